@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the distance-estimation raymarcher on B200.
+
+Metric: DE evaluations per second (CalculateDistance calls, counted on the
+device) of the FP32 batched (persistent wavefront) kernel, next to the plain
+FP64 kernel on the same frame, at stated error against the FP64 frame.
+Workload (default): Mandelbox s=-1.5, 1920x1080, camera A (0,-6,0) FOV 53,
+N=50, bailout 100, 5 binary steps, Lambert + hard shadow, 16 AO rays per hit.
+
+One step = one full frame rendered by one kernel launch.  Under torchrun each
+rank renders its own frame (own jitter stream): weak scaling, no collective on
+the data path; timing is max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DE evals/s & Mpix/s: FP32-batched vs plain FP64 kernel, 1 B200, fixed error"
+UNIT = "DE evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--engine", default="wavefront_fp32")
+    ap.add_argument("--baseline-engine", default="plain_fp64")
+    ap.add_argument("--workload", default="mandelbox_1080p_A")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name: str):
+    from mandelbulber2_b200 import configs
+
+    if name == "mandelbox_1080p_A":
+        sc, cam, p = configs.mandelbox_1080p("A")
+        desc = {"workload": "mandelbox s=-1.5 1920x1080 camera A (0,-6,0) fov 53, N=50, bailout 100, "
+                            "5 binary steps, lambert + hard shadow, 16 AO rays", "width": 1920, "height": 1080,
+                "formula": "mandelbox", "maxiter": 50, "ao_rays": 16}
+    elif name == "mandelbulb_512":
+        sc, cam, p = configs.mandelbulb_512()
+        desc = {"workload": "mandelbulb p=8 512x512 camera (0,-3,0) fov 53, N=250, bailout 10, 5 binary steps, "
+                            "lambert + hard shadow", "width": 512, "height": 512, "formula": "mandelbulb",
+                "maxiter": 250}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return sc, cam, p, desc
+
+
+# ---- clocks ---------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---- helpers ----------------------------------------------------------------------
+def l2_flush_buffer(torch, device):
+    return torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+
+def time_engine(r, torch, cam, p, bufs, engine, steps, warmup, flush, dist, world):
+    """Renders warmup + steps frames; returns (device seconds max over ranks, stats of the timed steps, per-step ms)."""
+    from mandelbulber2_b200.render import STATS_FIELDS, stats_dict
+
+    dev = r.device
+    stats = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        r.render_into(cam, p, bufs, stats, engine)
+    r.sync()
+    stats.zero_()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    for k in range(steps):
+        flush.fill_(float(k))  # L2 flush: a 256 MiB write between timed frames (outside the events)
+        evs[k][0].record(stream)
+        r.render_into(cam, p, bufs, stats, engine)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    r.sync()
+    if dist is not None:
+        dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    t = sum(ms) / 1e3
+    if dist is not None:
+        tt = torch.tensor([t], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return t, stats_dict(stats), ms
+
+
+def compare_frames(fast: dict, ref: dict) -> dict:
+    import numpy as np
+
+    hf, hr = fast["hit"].astype(bool), ref["hit"].astype(bool)
+    both = hf & hr
+    out = {"hit_mismatch": float((hf != hr).mean())}
+    if both.any():
+        rel = np.abs(fast["depth"][both] - ref["depth"][both]) / np.abs(ref["depth"][both])
+        out.update(depth_rel_median=float(np.median(rel)), depth_rel_p99=float(np.quantile(rel, 0.99)),
+                   depth_rel_max=float(rel.max()), frac_depth_rel_le_1e4=float((rel <= 1e-4).mean()))
+        nf, nr = fast["normal"][both].astype(np.float64), ref["normal"][both].astype(np.float64)
+        cos = np.clip((nf * nr).sum(1), -1, 1)
+        ang = np.degrees(np.arccos(cos))
+        out.update(normal_deg_median=float(np.median(ang)), normal_deg_p99=float(np.quantile(ang, 0.99)))
+    return out
+
+
+def load_json(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(sc, cam, p, seconds: float) -> dict:
+    """The oracle as the reference ships it (-O3 -ffast-math, OpenMP over rows,
+    all host threads) on a centred band of rows sized to about `seconds`."""
+    from oracle.oracle import Oracle
+
+    o = Oracle("fast")
+    threads = o.threads()
+    h = cam.height
+    rows = max(2, min(8, h))
+    while True:
+        r0 = h // 2 - rows // 2
+        t0 = time.perf_counter()
+        _, st = o.render(sc, cam, p, rows=(r0, r0 + rows), threads=threads, outputs=("depth",))
+        dt = time.perf_counter() - t0
+        if dt >= seconds * 0.5 or rows >= h:
+            break
+        rows = min(h, max(rows * 2, int(rows * seconds / max(dt, 1e-3))))
+    return {"value": st["de_evals"] / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"rows {r0}..{r0 + rows - 1} of the {cam.width}x{h} frame ({rows * cam.width} pixels), "
+                      f"{dt:.2f} s", "mpix_per_s": rows * cam.width / dt / 1e6,
+            "formula_iterations_per_s": st["formula_iterations"] / dt, "seconds": dt}
+
+
+def run_reference(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+
+    sc, cam, p, desc = workload(a.workload)
+    o = Oracle("fast")
+    threads = o.threads()
+    # bounded sample per step: a centred band of rows sized from a probe
+    rows = 8
+    r0 = cam.height // 2 - rows // 2
+    t0 = time.perf_counter()
+    o.render(sc, cam, p, rows=(r0, r0 + rows), threads=threads, outputs=("depth",))
+    probe = time.perf_counter() - t0
+    per_step = min(20.0, 150.0 / max(1, a.steps + a.warmup))
+    rows = int(max(8, min(cam.height, rows * per_step / max(probe, 1e-3))))
+    r0 = cam.height // 2 - rows // 2
+    for _ in range(a.warmup):
+        o.render(sc, cam, p, rows=(r0, r0 + min(rows, 8)), threads=threads, outputs=("depth",))
+    tot_de, tot_t = 0, 0.0
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        _, st = o.render(sc, cam, p, rows=(r0, r0 + rows), threads=threads, outputs=("depth",))
+        tot_t += time.perf_counter() - t0
+        tot_de += st["de_evals"]
+    v = tot_de / tot_t
+    sample = f"rows {r0}..{r0 + rows - 1} of {cam.width}x{cam.height} per step ({rows * cam.width} pixels)"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": tot_t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (procedural fractal, no dataset)",
+            "config": desc,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import numpy as np
+    import torch
+
+    from mandelbulber2_b200 import abi
+    from mandelbulber2_b200.render import Renderer, alloc_outputs, STATS_FIELDS
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    torch.cuda.set_device(local)
+    engines = {v: k for k, v in abi.ENGINE_NAMES.items()}
+    engine = engines[a.engine]
+    base_engine = engines[a.baseline_engine]
+
+    sc, cam, p, desc = workload(a.workload)
+    p.seed = rank  # each rank: its own frame (jitter stream)
+    r = Renderer(local)
+    r.set_scene(sc)
+    n = cam.width * cam.height
+    names = ("depth", "iters", "hit", "normal", "rgb8")
+    bufs = alloc_outputs(n, r.device, names)
+    flush = l2_flush_buffer(torch, r.device)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    t, st, ms = time_engine(r, torch, cam, p, bufs, engine, a.steps, a.warmup, flush, dist, world)
+    clk = clocks.stop()
+    de_total = torch.tensor([st["de_evals"], st["pixels"], st["formula_iterations"]], dtype=torch.float64,
+                            device=r.device)
+    if dist is not None:
+        dist.all_reduce(de_total)
+    de_all, pix_all, it_all = (float(x) for x in de_total.tolist())
+    value = de_all / t
+    fast_frame = {k: v.cpu().numpy() for k, v in bufs.items()}
+
+    # plain FP64 kernel on the same frame, and the error of the fast frame against it
+    base = None
+    err = None
+    if not a.no_baseline:
+        bbufs = alloc_outputs(n, r.device, names)
+        bsteps = max(1, min(a.steps, 3))
+        bt, bst, bms = time_engine(r, torch, cam, p, bbufs, base_engine, bsteps, 1, flush, dist, world)
+        btot = torch.tensor([bst["de_evals"]], dtype=torch.float64, device=r.device)
+        if dist is not None:
+            dist.all_reduce(btot)
+        base = {"engine": a.baseline_engine, "value": float(btot.item()) / bt, "unit": UNIT,
+                "ms_per_step": bt / bsteps * 1e3,
+                "mpix_per_s": n * world * bsteps / bt / 1e6}
+        err = compare_frames(fast_frame, {k: v.cpu().numpy() for k, v in bbufs.items()})
+        del bbufs
+
+    # end to end through the public API with host buffers: every step copies
+    # its inputs (the scene, camera and parameter structs, pinned) to the device
+    # and reads all outputs back to pinned host memory
+    hbufs = {k: torch.empty(v.shape, dtype=v.dtype, pin_memory=True) for k, v in bufs.items()}
+    in_bytes = C.sizeof(abi.Scene) + C.sizeof(abi.Camera) + C.sizeof(abi.RenderParams)
+    host_in = torch.empty(in_bytes, dtype=torch.uint8, pin_memory=True)
+    C.memmove(host_in.data_ptr(), C.addressof(sc), C.sizeof(abi.Scene))
+    C.memmove(host_in.data_ptr() + C.sizeof(abi.Scene), C.addressof(cam), C.sizeof(abi.Camera))
+    C.memmove(host_in.data_ptr() + C.sizeof(abi.Scene) + C.sizeof(abi.Camera), C.addressof(p),
+              C.sizeof(abi.RenderParams))
+    dev_in = torch.empty(in_bytes, dtype=torch.uint8, device=r.device)
+    stats = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=r.device)
+    e_steps = a.steps
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        dev_in.copy_(host_in, non_blocking=True)
+        r.set_scene(sc)
+        r.render_into(cam, p, bufs, stats, engine)
+        for k in bufs:
+            hbufs[k].copy_(bufs[k], non_blocking=True)
+        r.sync()
+    torch.cuda.synchronize()
+    te = time.perf_counter() - t0
+    if dist is not None:
+        tt = torch.tensor([te], dtype=torch.float64, device=r.device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    d2h = sum(v.numel() * v.element_size() for v in bufs.values())
+    e2e = {"value": de_all / a.steps * e_steps / te, "unit": UNIT, "h2d_bytes_per_step": in_bytes,
+           "d2h_bytes_per_step": d2h, "ms_per_step": te / e_steps * 1e3,
+           "api": "mbr_scene_set + mbr_render + D2H of depth/iters/hit/normal/rgb8 + mbr_sync"}
+
+    # roofline: algorithmic flops of the formula iterations (per-iteration
+    # counts from the op-counting oracle, profiles/opcount.json) per launch
+    # over the measured launch time, against the measured FP32 FMA peak
+    peak = C.c_double()
+    fp64_peak = C.c_double()
+    abi.load().mbr_fma_peak(0, 4096, None, C.byref(peak))
+    abi.load().mbr_fma_peak(1, 1024, None, C.byref(fp64_peak))
+    ops = load_json(os.path.join(ROOT, "profiles", "opcount.json")) or {}
+    per_iter = ops.get(desc["formula"], {}).get("flops_per_iteration")
+    launch_s = t / a.steps
+    roofline = None
+    if per_iter:
+        achieved = st["formula_iterations"] / a.steps * per_iter / launch_s / 1e12
+        pk = peak.value / 1e12
+        traffic = load_json(os.path.join(ROOT, "profiles", "traffic.json")) or {}
+        tr = traffic.get(a.engine, {}).get(a.workload)
+        roofline = {"bound": "fma", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
+                    "traffic": tr, "peak_source": "measured live: FFMA probe (mbr_fma_peak), FP32 non-tensor; "
+                                                  "MEASURED_PEAKS.json has no FP32 FMA figure",
+                    "flops_per_iteration": per_iter, "fp64_peak": fp64_peak.value / 1e12}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        try:
+            cpu = cpu_baseline(sc, cam, p, a.cpu_seconds)
+        except Exception as e:  # the baseline must not hide the GPU line
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if "fp32" in a.engine or "mixed" in a.engine else "f64",
+            "data": "synthetic (procedural fractal scene, no dataset)",
+            "config": dict(desc, engine=a.engine, parallelism=f"replicas x{world} (one frame per GPU)",
+                           l2="256 MiB buffer written between timed frames"),
+            "mpix_per_s": pix_all / t / 1e6, "formula_iterations_per_s": it_all / t,
+            "de_evals_per_frame": st["de_evals"] / a.steps, "stats_per_frame": {k: v / a.steps for k, v in st.items()},
+            "fp64_baseline": base, "speedup_vs_fp64": (value / base["value"]) if base else None,
+            "error_vs_fp64": err, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": a.steps, "clocks": clk, "per_step_ms": ms,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

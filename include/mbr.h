@@ -1,0 +1,356 @@
+/*
+ * mbr.h - C-ABI of the B200-native distance-estimation raymarcher.
+ *
+ * This library replaces the per-pixel work of mandelbulber2's cRenderWorker
+ * (src/render_worker.cpp:91-530) and everything beneath it on one GPU:
+ *   Compute<calcModeNormal>        src/compute_fractal.cpp:67-654
+ *   CalculateDistance(Simple)      src/calculate_distance.cpp:60-64, 225-516, 533-606
+ *   cRenderWorker::RayMarching     src/render_worker.cpp:708-951
+ *   CalculateNormals (fast path)   src/shader_calculate_normals.cpp:40-79
+ *   LightShading + AuxShadow       src/shader_light_shading.cpp:40-122,
+ *                                  src/shader_aux_shadow.cpp:39-323 (hard shadow)
+ *   AmbientOcclusion               src/shader_ambient_occlusion.cpp:41-120
+ *   GlobalIlumination + MC DOF     src/shader_global_illumination.cpp:41-209,
+ *                                  src/render_worker.cpp:1832-1862
+ *   cImage::CalculatePixel + 8 bit src/cimage.cpp:317-375, 460-469
+ *
+ * Only plain C types cross this boundary.  All buffers in mbr_outputs are
+ * caller-owned DEVICE pointers; streams are passed as `void*` (a cudaStream_t,
+ * NULL = legacy default stream).  A context is not thread-safe: use one
+ * context per host thread.  No call throws; every call returns an mbr_status
+ * and, on failure, mbr_last_error_string() describes the cause.
+ */
+#ifndef MBR_H_
+#define MBR_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MBR_ABI_VERSION 1
+
+/* Number of formula slots of one hybrid sequence (the reference's nine
+ * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
+#define MBR_MAX_FRACTALS 9
+/* Length of a hybrid sequence table: maxN * 5 with maxN = 250
+ * (src/hybrid_fractal_sequences.cpp:296-298). */
+#define MBR_SEQUENCE_LENGTH 1250
+
+typedef enum mbr_status {
+  MBR_OK = 0,
+  MBR_EINVAL = 1,        /* invalid argument (sizes, NULL pointers, ranges) */
+  MBR_ECUDA = 2,         /* a CUDA runtime call failed */
+  MBR_ETIMEOUT = 3,      /* a kernel watchdog budget ran out (status word set on device) */
+  MBR_ENOMEM = 4,        /* device allocation failed */
+  MBR_EUNSUPPORTED = 5   /* valid request that this build does not implement */
+} mbr_status;
+
+/* Formula ids, numerically equal to fractal::enumFractalFormula
+ * (formula/definition/all_fractal_list_enums.hpp:40-52). */
+typedef enum mbr_formula {
+  MBR_FORMULA_NONE = 0,
+  MBR_FORMULA_MANDELBULB = 2,   /* formula/definition/fractal_mandelbulb.cpp:29-43 */
+  MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
+  MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
+} mbr_formula;
+
+/* fractal::enumDEFunctionType (src/fractal_enums.h:47-60). */
+typedef enum mbr_de_function {
+  MBR_DE_FUNCTION_PREFERRED = 0,
+  MBR_DE_FUNCTION_LINEAR = 1,
+  MBR_DE_FUNCTION_LOGARITHMIC = 2
+} mbr_de_function;
+
+/* Which kernel renders a frame. */
+typedef enum mbr_engine {
+  /* One FP64 thread per pixel; FMA contraction allowed (the plain FP64 path). */
+  MBR_ENGINE_PLAIN_FP64 = 0,
+  /* Same kernel compiled without FMA contraction: every double operation is
+   * the IEEE-rounded operation the CPU reference performs. */
+  MBR_ENGINE_PLAIN_FP64_STRICT = 1,
+  /* One thread per pixel; formula iteration and march step in FP32, ray
+   * origin, accumulated t and the final hit bisection in FP64. */
+  MBR_ENGINE_PLAIN_MIXED = 2,
+  /* Persistent wavefront kernel: FP32 iteration, FP64 origin and t, per-lane
+   * ray refill, re-convergence of finished lanes every k iterations. */
+  MBR_ENGINE_WAVEFRONT_FP32 = 3,
+  /* The wavefront kernel with FP64 iteration (isolates scheduling gains). */
+  MBR_ENGINE_WAVEFRONT_FP64 = 4
+} mbr_engine;
+
+/* How the hit is refined after the march finds dist < threshold. */
+typedef enum mbr_refine {
+  /* Reference binary search: at most binary_steps halvings, stopped when
+   * threshold*(1-0.001*detail) < dist < threshold (render_worker.cpp:854-912). */
+  MBR_REFINE_REFERENCE = 0,
+  /* Bisection of F(t) = dist(t) - threshold(t) to convergence (64 halvings);
+   * makes depth a smooth function of the parameters (used by the adjoint). */
+  MBR_REFINE_ROOT = 1
+} mbr_refine;
+
+/* One formula slot: the subset of sFractal (src/fractal.h:888-940) and of
+ * cHybridFractalSequences::sFractalData (src/hybrid_fractal_sequences.h:33-54)
+ * that the three supported formulas read.  Angles are in degrees, as in the
+ * settings file; the library converts them like
+ * sFractal::RecalculateFractalParams (src/fractal.cpp:653-678). */
+typedef struct mbr_fractal {
+  int32_t formula;                 /* mbr_formula */
+  int32_t formula_iterations;      /* "formula_iterations", default 1 */
+  int32_t formula_start_iteration; /* default 0 */
+  int32_t formula_stop_iteration;  /* default 250 */
+  int32_t dont_add_c_constant;     /* default 0 */
+  int32_t check_for_bailout;       /* default 1 */
+  double formula_weight;           /* default 1.0 */
+  /* Mandelbulb: sFractalMandelbulb (src/fractal.h:227-234) */
+  double bulb_power;               /* "power", default 9 */
+  double bulb_alpha_angle_offset;  /* degrees, default 0 */
+  double bulb_beta_angle_offset;   /* degrees, default 0 */
+  /* Mandelbox: sFractalMandelbox (src/fractal.h:185-219); rotations off */
+  double mandelbox_scale;                 /* default 2 */
+  double mandelbox_folding_limit;         /* default 1 */
+  double mandelbox_folding_value;         /* default 2 */
+  double mandelbox_folding_min_radius;    /* default 0.5 */
+  double mandelbox_folding_fixed_radius;  /* default 1 */
+  double mandelbox_offset[3];             /* default (0,0,0) */
+  /* Menger sponge: sFractalTransformCommon::scale3 (default 3) */
+  double transf_scale3;
+} mbr_fractal;
+
+/* The fractal part of a scene: one fractal (or hybrid) object node with the
+ * general fractal parameters of src/initparameters.cpp:128-157 and the node
+ * parameters of :2102-2125.  The objects tree holds exactly this one node at
+ * the origin with unit scale (the reference's default scene). */
+typedef struct mbr_scene {
+  int32_t n_fractals;          /* 1..MBR_MAX_FRACTALS slots in use */
+  int32_t hybrid_fractal_enable;
+  int32_t formula_maxiter;     /* node "formula_maxiter", default 250 */
+  int32_t repeat_from;         /* 1-based, default 1 */
+  int32_t julia_mode;          /* default 0 */
+  int32_t use_default_bailout; /* default 1 */
+  int32_t delta_de_function;   /* mbr_de_function, default PREFERRED */
+  int32_t min_n;               /* "minN", default 1 */
+  int32_t iteration_threshold_mode; /* default 0 */
+  int32_t interior_mode;       /* default 0 */
+  double bailout;              /* used when use_default_bailout == 0; default 100 */
+  double julia_c[3];
+  double fractal_constant_factor[3]; /* default (1,1,1) */
+  double initial_waxis;        /* default 0 */
+  double linear_de_offset;     /* default 0 */
+  mbr_fractal fractal[MBR_MAX_FRACTALS];
+} mbr_scene;
+
+/* Camera in the reference's terms: camera/target/top vectors
+ * (cCameraTarget::SetCameraTargetTop, src/camera_target.cpp:86-130) or, when
+ * use_angles != 0, explicit yaw/pitch/roll in radians (viewAngle, as used by
+ * PrepareMainVectors, src/render_worker.cpp:539-564).  Only the three-point
+ * perspective (projection_3d.cpp:77-84) is supported. */
+typedef struct mbr_camera {
+  double camera[3];
+  double target[3];
+  double top[3];
+  double fov_deg;        /* "fov", default 53.13 */
+  int32_t width;
+  int32_t height;
+  int32_t use_angles;
+  int32_t reserved0;
+  double angles[3];      /* yaw, pitch, roll (radians) when use_angles != 0 */
+} mbr_camera;
+
+typedef struct mbr_render_params {
+  double detail_level;          /* default 1 */
+  double de_factor;             /* default 1 */
+  double view_distance_max;     /* default 50 */
+  double smoothness;            /* default 1 */
+  int32_t max_raymarching_steps;/* default 10000 */
+  int32_t binary_steps;         /* reference: 30 */
+  int32_t refine;               /* mbr_refine */
+  int32_t jitter;               /* 1: step *= 1 - Random(1000)/10000 from a per-pixel
+                                   Park-Miller stream (common_math.cpp:47-72); 0: off */
+  uint32_t seed;                /* jitter stream seed */
+  int32_t constant_de_threshold;/* default 0 */
+  double de_thresh;             /* "DE_thresh", default 0.01 */
+  /* shading of the level-0 ray */
+  int32_t shading_enable;       /* normals + directional light + shadow */
+  int32_t shadow_enable;        /* hard AuxShadow toward the light */
+  double light_direction[3];    /* direction TOWARD the light, normalised by the library */
+  double light_intensity;       /* default 1 */
+  double material_shading;      /* material "shading", default 1 */
+  double albedo;                /* constant surface colour, default 1 */
+  double ambient_intensity;     /* multiplies AO (or 1 when AO is off); default 0 */
+  int32_t ao_rays;              /* 0 = no AO; else cosine-hemisphere rays per hit */
+  uint32_t ao_seed;             /* PCG32 state seed of the AO stream (stream = pixel) */
+  double background[3];         /* colour of missed pixels */
+  /* Monte Carlo GI (path tracer) - used by mbr_render when gi_samples > 0 */
+  int32_t gi_samples;           /* samples per pixel */
+  int32_t gi_bounces;           /* diffuse bounces after the primary hit */
+  double gi_sky;                /* constant sky radiance */
+  double gi_sun;                /* sun radiance scale (directional, light_direction) */
+  double dof_aperture;          /* thin lens radius; 0 = pinhole */
+  double dof_focus;             /* focus distance */
+  uint32_t gi_seed;             /* PCG32 state seed (stream = pixel*spp + sample) */
+  int32_t reserved1;
+  /* image adjustments (sImageAdjustments, cimage.cpp:317-362) */
+  double brightness;            /* default 1 */
+  double contrast;              /* default 1 */
+  double gamma;                 /* default 1 */
+  double saturation;            /* default 1 */
+  int32_t hdr;                  /* default 0 */
+  int32_t reserved2;
+} mbr_render_params;
+
+/* Per-launch counters (src/statistics.h:42-70 mirrored).  A DE evaluation
+ * is one CalculateDistance call; formula_iterations sums its `iters`. */
+typedef struct mbr_stats {
+  unsigned long long de_evals;
+  unsigned long long formula_iterations;
+  unsigned long long march_steps;
+  unsigned long long binary_steps;
+  unsigned long long normal_evals;
+  unsigned long long shadow_evals;
+  unsigned long long ao_evals;
+  unsigned long long gi_evals;
+  unsigned long long pixels;
+  unsigned long long watchdog_trips;
+} mbr_stats;
+
+/* Caller-owned device buffers, each width*height elements (x3 for vectors),
+ * row-major, pixel (x,y) at y*width + x.  Any pointer may be NULL. */
+typedef struct mbr_outputs {
+  double *depth;      /* scan distance of the hit; 1e20 when nothing was hit */
+  int32_t *iters;     /* iters of the last DE evaluation of the primary march */
+  uint8_t *hit;       /* 1 when the primary ray found the surface */
+  float *normal;      /* world-space unit normal (0,0,0 on miss) */
+  float *shade;       /* Lambert term incl. shadow, before albedo/ambient */
+  float *ao;          /* ambient occlusion in [0,1] (1 when off) */
+  float *rgb;         /* linear colour */
+  uint8_t *rgb8;      /* 8-bit colour after CalculatePixel + ConvertTo8bitChar */
+  mbr_stats *stats;   /* device counters, ADDED to (caller zeroes them) */
+} mbr_outputs;
+
+typedef struct mbr_ctx mbr_ctx;
+typedef struct mbr_batch mbr_batch;
+
+/* ---- context ----------------------------------------------------------- */
+/* Library version string. */
+const char *mbr_version(void);
+/* Creates a context on `device`.  Replaces the per-render set-up of
+ * cRenderer::RenderImage (src/render_image.cpp:354-485). */
+mbr_status mbr_create(mbr_ctx **out, int device);
+void mbr_destroy(mbr_ctx *ctx);
+const char *mbr_last_error_string(const mbr_ctx *ctx);
+
+/* Fill structs with the reference defaults (src/initparameters.cpp). */
+void mbr_scene_defaults(mbr_scene *scene);
+void mbr_fractal_defaults(mbr_fractal *fractal, int formula);
+void mbr_camera_defaults(mbr_camera *camera);
+void mbr_render_params_defaults(mbr_render_params *params);
+
+/* Validates a scene and builds its hybrid sequence
+ * (cHybridFractalSequences::CreateSequences, hybrid_fractal_sequences.cpp:27-499)
+ * on the host, then uploads it.  Replaces cRenderJob's sequence set-up
+ * (src/render_job.cpp:300-351). */
+mbr_status mbr_scene_set(mbr_ctx *ctx, const mbr_scene *scene);
+
+/* Host helper: the camera rotation matrix (row-major 3x3) and view angles
+ * exactly as PrepareMainVectors builds mRot (render_worker.cpp:539-564). */
+mbr_status mbr_camera_rotation(const mbr_camera *camera, double mrot[9], double angles[3]);
+
+/* Host helper: the hybrid sequence table built for `scene` (length entries of
+ * slot indices) - the product of CreateSequence, exposed for testing. */
+mbr_status mbr_scene_sequence(const mbr_scene *scene, int32_t *seq_out, int32_t *length_out,
+                              int32_t *de_function_out, double *bailout_out);
+
+/* Renders one frame of the current scene: the body of cRenderWorker::doWork
+ * for every pixel (render_worker.cpp:126-525) on `stream`.  Asynchronous:
+ * returns after the launches are queued.  Call mbr_sync to wait and to read
+ * the watchdog status. */
+mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                      const mbr_outputs *out, int engine, void *stream);
+
+/* Waits for `stream` and reports a device watchdog trip (MBR_ETIMEOUT). */
+mbr_status mbr_sync(mbr_ctx *ctx, void *stream);
+
+/* Distance estimate at n points (device arrays, xyz interleaved): the
+ * reference's CalculateDistance, also what distance_engine.cl:42 computes.
+ * normal_mode selects sDistanceIn::normalCalculationMode. */
+mbr_status mbr_distance(mbr_ctx *ctx, const double *points, int64_t n, double detail_size,
+                        int normal_mode, double *dist, int32_t *iters, int engine, void *stream);
+
+/* ---- batches of render jobs (one persistent, graph-captured launch) ---- */
+typedef struct mbr_job {
+  mbr_camera camera;
+  int32_t scene_index;   /* into the scenes array of mbr_batch_create */
+  int32_t reserved0;
+  int64_t pixel_offset;  /* first pixel of this job in the batch outputs */
+} mbr_job;
+
+/* Builds the job table for n_jobs renders of uneven size and captures the
+ * launch into a CUDA graph.  Outputs are indexed pixel_offset + y*width + x.
+ * engine must be a WAVEFRONT engine. */
+mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_scenes,
+                            const mbr_job *jobs, int32_t n_jobs,
+                            const mbr_render_params *params, const mbr_outputs *out,
+                            int engine, void *stream, mbr_batch **batch);
+/* Replays the captured graph on `stream`. */
+mbr_status mbr_batch_launch(mbr_batch *batch, void *stream);
+void mbr_batch_destroy(mbr_batch *batch);
+
+/* Launch configuration of the wavefront kernel, chosen by the autotuner. */
+typedef struct mbr_tuning {
+  int32_t block_size;     /* threads per CTA */
+  int32_t ctas_per_sm;    /* persistent CTAs per SM */
+  int32_t refill_k;       /* re-converge finished lanes once <= k lanes still iterate */
+  int32_t queue_layout;   /* 0 = row-linear pixel queue, 1 = 8x4 tiles */
+} mbr_tuning;
+
+/* Sets / reads the wavefront launch configuration of the context. */
+mbr_status mbr_set_tuning(mbr_ctx *ctx, const mbr_tuning *tuning);
+mbr_status mbr_get_tuning(const mbr_ctx *ctx, mbr_tuning *tuning);
+
+/* Times the wavefront kernel over a grid of configurations on the given
+ * camera (outputs are scratch the caller provides) and keeps the fastest. */
+mbr_status mbr_autotune(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                        const mbr_outputs *out, int engine, void *stream, mbr_tuning *best);
+
+/* ---- adjoint ------------------------------------------------------------ */
+/* Parameters the adjoint differentiates, in this order. */
+enum {
+  MBR_GRAD_BULB_POWER = 0,
+  MBR_GRAD_MANDELBOX_SCALE = 1,
+  MBR_GRAD_MANDELBOX_MIN_R2 = 2,   /* w.r.t. min radius squared (mR2) */
+  MBR_GRAD_CAMERA_X = 3,           /* camera position at fixed view angles */
+  MBR_GRAD_CAMERA_Y = 4,
+  MBR_GRAD_CAMERA_Z = 5,
+  MBR_GRAD_YAW = 6,
+  MBR_GRAD_COUNT = 8               /* array length (last entry unused) */
+};
+
+/* Gradient of a per-pixel loss L(depth, shade) with respect to the
+ * MBR_GRAD_* parameters of slot 0 of the current (non-hybrid) scene and of
+ * the camera (given with use_angles = 1), by implicit differentiation at the
+ * hit: with F(t) = dist(o + t d) - threshold(t),
+ *   dt/dθ = -(∂dist/∂θ + ∇dist·∂p/∂θ) / (∇dist·d - ∂threshold/∂t).
+ * depth and hit are the forward outputs (rendered with MBR_REFINE_ROOT);
+ * dl_ddepth / dl_dshade are dL/d(depth) and dL/d(shade) per pixel (device,
+ * may be NULL = 0).  The shade term differentiates the central-difference
+ * normal of CalculateNormals through its six DE evaluations; the formula
+ * iteration is recomputed in forward-mode tangents.  grad (device, 8 doubles)
+ * is ADDED to.  `engine` selects FP64 (PLAIN_FP64) or FP32 (PLAIN_MIXED)
+ * recomputation. */
+mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                       const double *depth, const uint8_t *hit, const float *dl_ddepth,
+                       const float *dl_dshade, double *grad, int engine, void *stream);
+
+/* ---- measurement ------------------------------------------------------------ */
+/* FMA throughput of the current device (FLOP/s, an FMA counted as 2), FP32
+ * (fp64 = 0) or FP64: the roofline denominator for the DE kernels, which are
+ * bound by the FMA/SFU pipes.  Synchronous.  No counterpart in the reference. */
+mbr_status mbr_fma_peak(int fp64, int iters, void *stream, double *flops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBR_H_ */

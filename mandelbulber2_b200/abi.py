@@ -1,0 +1,180 @@
+"""ctypes mirror of ``include/mbr.h`` (the C-ABI of ``libmbr.so``).
+
+The structures below are field-for-field copies of the C structs; their sizes
+are checked against the C declarations by the CPU tests.  This module only
+loads the library; it performs no GPU work.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmbr.so")
+
+MBR_MAX_FRACTALS = 9
+MBR_SEQUENCE_LENGTH = 1250
+
+# mbr_status
+MBR_OK, MBR_EINVAL, MBR_ECUDA, MBR_ETIMEOUT, MBR_ENOMEM, MBR_EUNSUPPORTED = range(6)
+STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT", 4: "MBR_ENOMEM",
+                5: "MBR_EUNSUPPORTED"}
+
+# mbr_formula (fractal::enumFractalFormula)
+FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
+# mbr_de_function
+DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
+# mbr_engine
+ENGINE_PLAIN_FP64, ENGINE_PLAIN_FP64_STRICT, ENGINE_PLAIN_MIXED, ENGINE_WAVEFRONT_FP32, ENGINE_WAVEFRONT_FP64 = range(5)
+ENGINE_NAMES = {0: "plain_fp64", 1: "plain_fp64_strict", 2: "plain_mixed", 3: "wavefront_fp32", 4: "wavefront_fp64"}
+# mbr_refine
+REFINE_REFERENCE, REFINE_ROOT = 0, 1
+# gradient slots
+GRAD_BULB_POWER, GRAD_MANDELBOX_SCALE, GRAD_MANDELBOX_MIN_R2 = 0, 1, 2
+GRAD_CAMERA_X, GRAD_CAMERA_Y, GRAD_CAMERA_Z, GRAD_YAW, GRAD_COUNT = 3, 4, 5, 6, 8
+
+D3 = C.c_double * 3
+
+
+class Fractal(C.Structure):
+    _fields_ = [
+        ("formula", C.c_int32), ("formula_iterations", C.c_int32), ("formula_start_iteration", C.c_int32),
+        ("formula_stop_iteration", C.c_int32), ("dont_add_c_constant", C.c_int32), ("check_for_bailout", C.c_int32),
+        ("formula_weight", C.c_double),
+        ("bulb_power", C.c_double), ("bulb_alpha_angle_offset", C.c_double), ("bulb_beta_angle_offset", C.c_double),
+        ("mandelbox_scale", C.c_double), ("mandelbox_folding_limit", C.c_double),
+        ("mandelbox_folding_value", C.c_double), ("mandelbox_folding_min_radius", C.c_double),
+        ("mandelbox_folding_fixed_radius", C.c_double), ("mandelbox_offset", D3),
+        ("transf_scale3", C.c_double),
+    ]
+
+
+class Scene(C.Structure):
+    _fields_ = [
+        ("n_fractals", C.c_int32), ("hybrid_fractal_enable", C.c_int32), ("formula_maxiter", C.c_int32),
+        ("repeat_from", C.c_int32), ("julia_mode", C.c_int32), ("use_default_bailout", C.c_int32),
+        ("delta_de_function", C.c_int32), ("min_n", C.c_int32), ("iteration_threshold_mode", C.c_int32),
+        ("interior_mode", C.c_int32), ("bailout", C.c_double), ("julia_c", D3),
+        ("fractal_constant_factor", D3), ("initial_waxis", C.c_double), ("linear_de_offset", C.c_double),
+        ("fractal", Fractal * MBR_MAX_FRACTALS),
+    ]
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("camera", D3), ("target", D3), ("top", D3), ("fov_deg", C.c_double), ("width", C.c_int32),
+        ("height", C.c_int32), ("use_angles", C.c_int32), ("reserved0", C.c_int32), ("angles", D3),
+    ]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [
+        ("detail_level", C.c_double), ("de_factor", C.c_double), ("view_distance_max", C.c_double),
+        ("smoothness", C.c_double), ("max_raymarching_steps", C.c_int32), ("binary_steps", C.c_int32),
+        ("refine", C.c_int32), ("jitter", C.c_int32), ("seed", C.c_uint32), ("constant_de_threshold", C.c_int32),
+        ("de_thresh", C.c_double), ("shading_enable", C.c_int32), ("shadow_enable", C.c_int32),
+        ("light_direction", D3), ("light_intensity", C.c_double), ("material_shading", C.c_double),
+        ("albedo", C.c_double), ("ambient_intensity", C.c_double), ("ao_rays", C.c_int32),
+        ("ao_seed", C.c_uint32), ("background", D3), ("gi_samples", C.c_int32), ("gi_bounces", C.c_int32),
+        ("gi_sky", C.c_double), ("gi_sun", C.c_double), ("dof_aperture", C.c_double), ("dof_focus", C.c_double),
+        ("gi_seed", C.c_uint32), ("reserved1", C.c_int32), ("brightness", C.c_double), ("contrast", C.c_double),
+        ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("reserved2", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [(n, C.c_ulonglong) for n in (
+        "de_evals", "formula_iterations", "march_steps", "binary_steps", "normal_evals", "shadow_evals",
+        "ao_evals", "gi_evals", "pixels", "watchdog_trips")]
+
+
+class Outputs(C.Structure):
+    _fields_ = [
+        ("depth", C.c_void_p), ("iters", C.c_void_p), ("hit", C.c_void_p), ("normal", C.c_void_p),
+        ("shade", C.c_void_p), ("ao", C.c_void_p), ("rgb", C.c_void_p), ("rgb8", C.c_void_p),
+        ("stats", C.c_void_p),
+    ]
+
+
+class Job(C.Structure):
+    _fields_ = [("camera", Camera), ("scene_index", C.c_int32), ("reserved0", C.c_int32),
+                ("pixel_offset", C.c_int64)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("ctas_per_sm", C.c_int32), ("refill_k", C.c_int32),
+                ("queue_layout", C.c_int32)]
+
+
+# Every function the header declares: name -> (restype, argtypes).
+_P = C.c_void_p
+PROTOTYPES = {
+    "mbr_version": (C.c_char_p, []),
+    "mbr_create": (C.c_int, [C.POINTER(_P), C.c_int]),
+    "mbr_destroy": (None, [_P]),
+    "mbr_last_error_string": (C.c_char_p, [_P]),
+    "mbr_scene_defaults": (None, [C.POINTER(Scene)]),
+    "mbr_fractal_defaults": (None, [C.POINTER(Fractal), C.c_int]),
+    "mbr_camera_defaults": (None, [C.POINTER(Camera)]),
+    "mbr_render_params_defaults": (None, [C.POINTER(RenderParams)]),
+    "mbr_scene_set": (C.c_int, [_P, C.POINTER(Scene)]),
+    "mbr_camera_rotation": (C.c_int, [C.POINTER(Camera), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "mbr_scene_sequence": (C.c_int, [C.POINTER(Scene), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "mbr_render": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P]),
+    "mbr_sync": (C.c_int, [_P, _P]),
+    "mbr_distance": (C.c_int, [_P, _P, C.c_int64, C.c_double, C.c_int, _P, _P, C.c_int, _P]),
+    "mbr_batch_create": (C.c_int, [_P, C.POINTER(Scene), C.c_int32, C.POINTER(Job), C.c_int32,
+                                   C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P, C.POINTER(_P)]),
+    "mbr_batch_launch": (C.c_int, [_P, _P]),
+    "mbr_batch_destroy": (None, [_P]),
+    "mbr_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "mbr_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "mbr_autotune": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P,
+                               C.POINTER(Tuning)]),
+    "mbr_adjoint": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), _P, _P, _P, _P, _P, C.c_int, _P]),
+    "mbr_fma_peak": (C.c_int, [C.c_int, C.c_int, _P, C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None) -> C.CDLL:
+    """Loads libmbr.so (built in-tree) and declares its prototypes.
+
+    Raises RuntimeError when the library is missing: there is no fallback.
+    """
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"{p} is missing; build it with `python -m mandelbulber2_b200.build`")
+    lib = C.CDLL(p)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def scene_defaults(formula: int = FORMULA_MANDELBULB) -> Scene:
+    lib = load()
+    s = Scene()
+    lib.mbr_scene_defaults(C.byref(s))
+    lib.mbr_fractal_defaults(C.byref(s.fractal[0]), formula)
+    return s
+
+
+def camera_defaults() -> Camera:
+    c = Camera()
+    load().mbr_camera_defaults(C.byref(c))
+    return c
+
+
+def params_defaults() -> RenderParams:
+    p = RenderParams()
+    load().mbr_render_params_defaults(C.byref(p))
+    return p

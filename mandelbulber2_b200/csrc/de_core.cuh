@@ -1,0 +1,295 @@
+// de_core.cuh - distance estimation on the device: the formula iterations,
+// the Compute<calcModeNormal> loop and CalculateDistanceSimple, templated on
+// the scalar type T (double or float) and on the formula F (a fixed formula
+// id for single-formula scenes, 0 for the generic per-iteration dispatch that
+// hybrid sequences need).
+//
+// Reference semantics followed (file:line of mandelbulber2):
+//   cFractalMandelbulb::FormulaCode   formula/definition/fractal_mandelbulb.cpp:29-43
+//   cFractalMandelbox::FormulaCode    formula/definition/fractal_mandelbox.cpp:66-107
+//   cFractalMengerSponge::FormulaCode formula/definition/fractal_menger_sponge.cpp:30-71
+//   Compute<calcModeNormal>           src/compute_fractal.cpp:67-654
+//   CalculateDistanceSimple           src/calculate_distance.cpp:533-606
+// In FP64 every operation is written in the reference's order, so a build
+// without FMA contraction performs the same IEEE operations as the CPU code.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "mbr_device.h"
+
+namespace mbr {
+
+template <class T>
+__device__ __forceinline__ T P(const DevSlot &s, int i);
+template <>
+__device__ __forceinline__ double P<double>(const DevSlot &s, int i) {
+  return s.d[i];
+}
+template <>
+__device__ __forceinline__ float P<float>(const DevSlot &s, int i) {
+  return s.f[i];
+}
+
+template <class T>
+struct V4 {
+  T x, y, z, w;
+};
+
+// Scalar helpers with one spelling for both precisions.
+__device__ __forceinline__ double m_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float m_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double m_abs(double x) { return fabs(x); }
+__device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
+__device__ __forceinline__ double m_asin(double x) { return asin(x); }
+__device__ __forceinline__ float m_asin(float x) { return asinf(x); }
+__device__ __forceinline__ double m_atan2(double y, double x) { return atan2(y, x); }
+__device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
+__device__ __forceinline__ double m_pow(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float m_pow(float a, float b) { return powf(a, b); }
+__device__ __forceinline__ double m_log(double x) { return log(x); }
+__device__ __forceinline__ float m_log(float x) { return logf(x); }
+__device__ __forceinline__ void m_sincos(double x, double *s, double *c) { sincos(x, s, c); }
+__device__ __forceinline__ void m_sincos(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ double m_copysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float m_copysign(float a, float b) { return copysignf(a, b); }
+__device__ __forceinline__ bool m_finite(double x) { return isfinite(x); }
+__device__ __forceinline__ bool m_finite(float x) { return isfinite(x); }
+
+template <class T, bool W>
+__device__ __forceinline__ T len4(const V4<T> &v) {  // CVector4::Length
+  if (W) return m_sqrt(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
+  return m_sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+}
+template <class T, bool W>
+__device__ __forceinline__ bool nan4(const V4<T> &v) {  // CVector4::IsNotANumber
+  bool ok = m_finite(v.x) & m_finite(v.y) & m_finite(v.z);
+  if (W) ok = ok & m_finite(v.w);
+  return !ok;
+}
+
+// ---- formulas -----------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void f_mandelbulb(V4<T> &z, T r, T &DE, const DevSlot &s) {
+  const T power = P<T>(s, P_POWER);
+  const T th0 = m_asin(z.z / r) + P<T>(s, P_BETA);
+  const T ph0 = m_atan2(z.y, z.x) + P<T>(s, P_ALPHA);
+  T rp = m_pow(r, P<T>(s, P_POWER_M1));
+  const T th = th0 * power;
+  const T ph = ph0 * power;
+  T sth, cth, sph, cph;
+  m_sincos(th, &sth, &cth);
+  m_sincos(ph, &sph, &cph);
+  DE = (rp * DE) * power + T(1.0);
+  rp = rp * r;
+  z.x = cth * cph * rp;
+  z.y = cth * sph * rp;
+  z.z = sth * rp;
+}
+
+template <class T, bool W>
+__device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s) {
+  // box fold; the host requires folding_limit >= 0, so |z| > limit implies
+  // z != 0 and copysign(value, z) equals sign(z) * value exactly
+  const T limit = P<T>(s, P_MB_LIMIT), value = P<T>(s, P_MB_VALUE);
+  if (m_abs(z.x) > limit) z.x = m_copysign(value, z.x) - z.x;
+  if (m_abs(z.y) > limit) z.y = m_copysign(value, z.y) - z.y;
+  if (m_abs(z.z) > limit) z.z = m_copysign(value, z.z) - z.z;
+  T r2 = z.x * z.x + z.y * z.y + z.z * z.z;
+  if (W) r2 = r2 + z.w * z.w;
+  // FP64 always applies the offset, as the reference does; FP32 skips a zero
+  // offset (adding and subtracting +0 changes nothing but the sign of a zero)
+  const bool off = (sizeof(T) == 8) || s.has_offset != 0;
+  if (off) {
+    z.x = z.x + P<T>(s, P_MB_OFF_X);
+    z.y = z.y + P<T>(s, P_MB_OFF_Y);
+    z.z = z.z + P<T>(s, P_MB_OFF_Z);
+  }
+  if (r2 < P<T>(s, P_MB_MR2)) {
+    const T f1 = P<T>(s, P_MB_FACTOR1);
+    z.x = z.x * f1;
+    z.y = z.y * f1;
+    z.z = z.z * f1;
+    if (W) z.w = z.w * f1;
+    DE = DE * f1;
+  } else if (r2 < P<T>(s, P_MB_FR2)) {
+    const T t = P<T>(s, P_MB_FR2) / r2;
+    z.x = z.x * t;
+    z.y = z.y * t;
+    z.z = z.z * t;
+    if (W) z.w = z.w * t;
+    DE = DE * t;
+  }
+  if (off) {
+    z.x = z.x - P<T>(s, P_MB_OFF_X);
+    z.y = z.y - P<T>(s, P_MB_OFF_Y);
+    z.z = z.z - P<T>(s, P_MB_OFF_Z);
+  }
+  const T scale = P<T>(s, P_MB_SCALE);
+  z.x = z.x * scale;
+  z.y = z.y * scale;
+  z.z = z.z * scale;
+  if (W) z.w = z.w * scale;
+  DE = DE * P<T>(s, P_MB_ABS_SCALE) + T(1.0);
+}
+
+template <class T, bool W>
+__device__ __forceinline__ void f_menger(V4<T> &z, T &DE, const DevSlot &s) {
+  z.x = m_abs(z.x);
+  z.y = m_abs(z.y);
+  z.z = m_abs(z.z);
+  if (W) z.w = m_abs(z.w);
+  T tmp;
+  if (z.x < z.y) { tmp = z.y; z.y = z.x; z.x = tmp; }
+  if (z.x < z.z) { tmp = z.z; z.z = z.x; z.x = tmp; }
+  if (z.y < z.z) { tmp = z.z; z.z = z.y; z.y = tmp; }
+  const T s3 = P<T>(s, P_SCALE3);
+  z.x = z.x * s3;
+  z.y = z.y * s3;
+  z.z = z.z * s3;
+  if (W) z.w = z.w * s3;
+  z.x = z.x - T(2.0);
+  z.y = z.y - T(2.0);
+  if (z.z > T(1.0)) z.z = z.z - T(2.0);
+  DE = DE * s3;
+}
+
+template <class T, bool W>
+__device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s) {
+  switch (formula) {
+    case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
+    case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s); break;
+    default: f_menger<T, W>(z, DE, s); break;
+  }
+}
+
+// SmoothCVector (src/common_math.cpp:133-163)
+template <class T, bool W>
+__device__ __forceinline__ V4<T> smooth4(const V4<T> &v1, const V4<T> &v2, double k) {
+  if (k <= 0.0) return v1;
+  if (k >= 1.0) return v2;
+  const T kk = T(k), nk = T(1.0 - k);
+  const T l1 = len4<T, W>(v1), l2 = len4<T, W>(v2);
+  const T lenInterp = l1 * nk + l2 * kk;
+  V4<T> t{v1.x * nk + v2.x * kk, v1.y * nk + v2.y * kk, v1.z * nk + v2.z * kk, v1.w * nk + v2.w * kk};
+  const T lt = len4<T, W>(t);
+  if (lt > T(0.0)) return V4<T>{t.x / lt * lenInterp, t.y / lt * lenInterp, t.z / lt * lenInterp, t.w / lt * lenInterp};
+  return v1;
+}
+
+template <class T>
+__device__ __forceinline__ T cmul_of(const DevScene &sc, int k);
+template <>
+__device__ __forceinline__ double cmul_of<double>(const DevScene &sc, int k) {
+  return sc.cmul[k];
+}
+template <>
+__device__ __forceinline__ float cmul_of<float>(const DevScene &sc, int k) {
+  return sc.fcmul[k];
+}
+template <class T>
+__device__ __forceinline__ T juliac_of(const DevScene &sc, int k) {
+  return T(sc.julia_c[k] * sc.cmul[k]);
+}
+
+// Compute<calcModeNormal> + CalculateDistanceSimple (analytic branch).
+// F: fixed formula id (non-hybrid scene) or 0 (generic).  W: 4-D state.
+template <class T, int F, bool W>
+__device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
+                                           int *iters_out) {
+  const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
+  const int maxN = sc.formula_maxiter * mult;
+  V4<T> z{px, py, pz, W ? T(sc.w0) : T(0.0)};
+  const V4<T> c = z;
+  T r = len4<T, W>(z);
+  T DE = T(1.0);
+  V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)};
+  bool maxiter = true;
+  int i;
+  for (i = 0; i < maxN; i++) {
+    lastZ = z;
+    const int k = (F != 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]));
+    const DevSlot &s = sc.slot[k];
+    const V4<T> tempZ = z;
+    const T tempDE = DE;
+    if (F != 0) {
+      if (F == MBR_FORMULA_MANDELBULB) f_mandelbulb<T>(z, r, DE, s);
+      if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
+      if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
+    } else if (s.d[P_WEIGHT] > 0.0) {
+      formula_dispatch<T, W>(s.formula, z, r, DE, s);
+    }
+    if (s.add_c) {
+      if (sc.julia) {
+        z.x = z.x + juliac_of<T>(sc, 0);
+        z.y = z.y + juliac_of<T>(sc, 1);
+        z.z = z.z + juliac_of<T>(sc, 2);
+      } else {
+        z.x = z.x + c.x * cmul_of<T>(sc, 0);
+        z.y = z.y + c.y * cmul_of<T>(sc, 1);
+        z.z = z.z + c.z * cmul_of<T>(sc, 2);
+        if (W) z.w = z.w + c.w;
+      }
+    }
+    if (F == 0 && sc.is_hybrid) {
+      const double kw = s.d[P_WEIGHT];
+      if (kw < 1.0) {
+        z = smooth4<T, W>(tempZ, z, kw);
+        DE = DE * T(kw) + tempDE * T(1.0 - kw);
+      }
+    }
+    r = len4<T, W>(z);
+    if (nan4<T, W>(z)) {
+      z = lastZ;
+      r = len4<T, W>(z);
+      maxiter = true;
+      break;
+    }
+    if (s.check_bailout && r > P<T>(s, P_BAILOUT)) {
+      maxiter = false;
+      break;
+    }
+  }
+  // final DE (compute_fractal.cpp:495-621)
+  T distance;
+  if (DE > T(0.0)) {
+    // 1 linear r/DE, 2 log, 3 IFS, 4 hybrid linear with offset
+    const int fn = (F == 0 && sc.is_hybrid) ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
+    if (fn == 4) {
+      distance = (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
+    } else if (fn == 2) {
+      distance = (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
+    } else if (fn == 1) {
+      distance = r / DE;
+    } else if (fn == 3) {
+      distance = (r - T(2.0)) / DE;
+    } else {
+      distance = r;
+    }
+  } else {
+    distance = r;
+  }
+  const int iters = i + 1;
+  *iters_out = iters;
+  // CalculateDistanceSimple post-processing (calculate_distance.cpp:561-605)
+  bool mx = maxiter;
+  if (!sc.iter_thresh) mx = false;
+  if (normal_mode) mx = false;
+  if (mx) distance = T(0.0);
+  if (iters < sc.min_n && distance < detail) distance = detail;
+  if (sc.interior) {
+    if (!normal_mode) {
+      if (distance < T(0.5) * detail || maxiter) distance = detail;
+    } else {
+      if (distance < T(0.9) * detail) distance = detail - distance;
+    }
+  }
+  if (sc.iter_thresh && !normal_mode && !maxiter) {
+    if (distance < detail) distance = detail * T(1.01);
+  }
+  if (distance < T(0.0)) distance = T(0.0);
+  if (distance > T(10.0)) distance = T(10.0);
+  return distance;
+}
+
+}  // namespace mbr

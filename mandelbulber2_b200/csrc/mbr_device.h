@@ -1,0 +1,147 @@
+// mbr_device.h - data the host prepares for the kernels (host and device).
+//
+// A scene is flattened into DevScene: the hybrid sequence table and the
+// per-slot formula parameters in both FP64 and FP32, derived on the host once
+// (sFractal::RecalculateFractalParams, src/fractal.cpp:653-678, and
+// cHybridFractalSequences::CreateSequence, src/hybrid_fractal_sequences.cpp:289-499).
+// It is passed to the kernels by value (__grid_constant__), so every lane
+// reads it through the constant cache.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/mbr.h"
+
+namespace mbr {
+
+// Indices into DevSlot::d / DevSlot::f.
+enum SlotParam {
+  P_POWER = 0,      // bulb power
+  P_POWER_M1,       // power - 1
+  P_ALPHA,          // radians
+  P_BETA,
+  P_MB_SCALE,
+  P_MB_ABS_SCALE,
+  P_MB_LIMIT,
+  P_MB_VALUE,
+  P_MB_MR2,
+  P_MB_FR2,
+  P_MB_FACTOR1,     // fR2 / mR2
+  P_MB_OFF_X,
+  P_MB_OFF_Y,
+  P_MB_OFF_Z,
+  P_SCALE3,
+  P_BAILOUT,
+  P_WEIGHT,
+  P_COUNT
+};
+
+struct DevSlot {
+  int32_t formula;
+  int32_t add_c;
+  int32_t check_bailout;
+  int32_t has_offset;
+  double d[P_COUNT];
+  float f[P_COUNT];
+};
+
+struct DevScene {
+  int32_t n;
+  int32_t is_hybrid;
+  int32_t length;          // sequence length (entries of seq)
+  int32_t formula_maxiter;
+  int32_t min_n;
+  int32_t iter_thresh;
+  int32_t interior;
+  int32_t julia;
+  int32_t de_function;     // hybrid: enumDEFunctionType (1 linear, 2 log)
+  int32_t de_analytic;     // non-hybrid: enumDEAnalyticFunction (1 linear, 2 log, 3 IFS)
+  int32_t uniform_formula; // formula id when every iteration uses slot 0, else 0
+  int32_t has_w;           // initial w != 0 (4-D state needed)
+  double julia_c[3];
+  double cmul[3];
+  double w0;
+  double linear_de_offset;
+  float fjulia_c[3];
+  float fcmul[3];
+  float flinear_de_offset;
+  float pad0;
+  DevSlot slot[MBR_MAX_FRACTALS];
+  uint8_t seq[MBR_SEQUENCE_LENGTH];
+};
+
+// Everything about one frame that is not the scene: camera, march and
+// shading parameters, derived on the host.
+struct DevFrame {
+  double camera[3];
+  double mrot[9];      // PrepareMainVectors mRot, row-major
+  int32_t mrot_zero;   // CRotationMatrix::zero: RotateVector is the identity
+  int32_t width, height;
+  int32_t max_steps;
+  int32_t binary_steps;
+  int32_t refine;
+  int32_t jitter;
+  uint32_t seed;
+  double fov;          // 2 tan(fov/2)
+  double resolution;   // 1 / height
+  double aspect;
+  double detail_level;
+  double de_factor;
+  double view_distance_max;
+  double smoothness;
+  int32_t constant_de_threshold;
+  int32_t shading_enable;
+  int32_t shadow_enable;
+  int32_t ao_rays;
+  double de_thresh;
+  double light[3];     // unit vector toward the light
+  float light_intensity;
+  float material_shading;
+  float albedo;
+  float ambient;
+  float background[3];
+  uint32_t ao_seed;
+  int32_t gi_samples;
+  int32_t gi_bounces;
+  uint32_t gi_seed;
+  int32_t want_normal;
+  double gi_sky;
+  double gi_sun;
+  double dof_aperture;
+  double dof_focus;
+  float brightness, contrast, saturation;
+  int32_t hdr;
+  const uint16_t *gamma;  // 65536-entry table (device)
+};
+
+struct DevOutputs {
+  double *depth;
+  int32_t *iters;
+  uint8_t *hit;
+  float *normal;
+  float *shade;
+  float *ao;
+  float *rgb;
+  uint8_t *rgb8;
+  mbr_stats *stats;
+  int32_t *status;        // watchdog status word (device, context-owned)
+  int64_t pixel_offset;   // added to the pixel index when writing
+};
+
+// Counters a thread accumulates before one reduction per warp.
+struct Counters {
+  unsigned long long de, iters, march, binary, normal, shadow, ao, gi, pixels, watchdog;
+};
+
+// ---- launchers (one per translation unit) ---------------------------------
+// Plain per-pixel kernels: rows [0, height) of the frame.
+int launch_plain_fp64(const DevScene &sc, const DevFrame &fr, const DevOutputs &out, void *stream);
+int launch_plain_fp64_strict(const DevScene &sc, const DevFrame &fr, const DevOutputs &out, void *stream);
+int launch_plain_mixed(const DevScene &sc, const DevFrame &fr, const DevOutputs &out, void *stream);
+int launch_distance_fp64(const DevScene &sc, const double *pts, int64_t n, double detail, int normal_mode,
+                         double *dist, int32_t *iters, void *stream);
+int launch_distance_fp64_strict(const DevScene &sc, const double *pts, int64_t n, double detail, int normal_mode,
+                                double *dist, int32_t *iters, void *stream);
+int launch_distance_fp32(const DevScene &sc, const double *pts, int64_t n, double detail, int normal_mode,
+                         double *dist, int32_t *iters, void *stream);
+
+}  // namespace mbr

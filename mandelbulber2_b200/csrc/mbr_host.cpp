@@ -1,0 +1,705 @@
+// mbr_host.cpp - host side of the C-ABI (include/mbr.h): context, parameter
+// validation, the hybrid-sequence builder, camera set-up and kernel dispatch.
+//
+// The host work restates what cRenderJob / sParamRender / cHybridFractalSequences
+// / cRenderWorker::PrepareMainVectors do before the per-pixel loop:
+//   sequence table      src/hybrid_fractal_sequences.cpp:181-499
+//   derived parameters  src/fractal.cpp:653-678 (fR2, mR2, mboxFactor1, radians)
+//   camera rotation     src/camera_target.cpp:86-130, src/render_worker.cpp:539-564
+//   fov, resolution     src/projection_3d.cpp:140-159, src/render_job.cpp:477
+//   gamma table         src/cimage.cpp:366-375
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/mbr.h"
+#include "mbr_device.h"
+#include "mbr_internal.h"
+
+using namespace mbr;
+
+namespace {
+
+const double kPi = 3.14159265358979323846;
+
+struct FormulaMeta {
+  int de_function;   // enumDEFunctionType
+  int cpixel;        // 0 enabled by default, 1 disabled by default
+  double bailout;    // default bailout
+  int analytic;      // enumDEAnalyticFunction
+};
+// cAbstractFractal metadata of the three formula classes
+// (fractal_mandelbulb.cpp:16-27, fractal_mandelbox.cpp:18-29, fractal_menger_sponge.cpp:17-28)
+bool formula_meta(int formula, FormulaMeta *m) {
+  switch (formula) {
+    case MBR_FORMULA_MANDELBULB: *m = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
+    case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
+    default: return false;
+  }
+}
+
+bool finite3(const double *v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+}  // namespace
+
+struct mbr_ctx {
+  int device = 0;
+  std::string err;
+  bool has_scene = false;
+  DevScene scene;
+  mbr_scene scene_src;
+  uint16_t *d_gamma = nullptr;
+  double gamma_value = -1.0;
+  int32_t *d_status = nullptr;
+  mbr_tuning tuning{128, 4, 8, 1};
+  // scratch of the wavefront kernel (work counter + per-lane queue cursor)
+  unsigned long long *d_work = nullptr;
+  size_t work_words = 0;
+  void *adjoint_scratch = nullptr;
+};
+
+namespace mbr {
+
+mbr_status set_err(mbr_ctx *ctx, mbr_status st, const char *fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return st;
+}
+
+mbr_status cuda_err(mbr_ctx *ctx, int code, const char *what) {
+  if (code == 0) return MBR_OK;
+  return set_err(ctx, MBR_ECUDA, "%s: %s", what, cudaGetErrorString(cudaError_t(code)));
+}
+
+// ---- scene -------------------------------------------------------------------
+// Validates `sc` and flattens it into a DevScene.  Restates CollectSequenceData
+// and CreateSequence for the single fractal (or hybrid) node of the default
+// objects tree.
+mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
+  DevScene d;
+  std::memset(&d, 0, sizeof(d));
+  const bool hybrid = sc.hybrid_fractal_enable != 0;
+  const int n = hybrid ? sc.n_fractals : 1;
+  if (sc.n_fractals < 1 || sc.n_fractals > MBR_MAX_FRACTALS)
+    return set_err(ctx, MBR_EINVAL, "n_fractals must be in [1, %d], got %d", MBR_MAX_FRACTALS, sc.n_fractals);
+  if (sc.formula_maxiter < 1 || sc.formula_maxiter > 9999)
+    return set_err(ctx, MBR_EINVAL, "formula_maxiter must be in [1, 9999], got %d", sc.formula_maxiter);
+  if (sc.repeat_from < 1 || sc.repeat_from > MBR_MAX_FRACTALS)
+    return set_err(ctx, MBR_EINVAL, "repeat_from must be in [1, 9], got %d", sc.repeat_from);
+  if (sc.min_n < 0) return set_err(ctx, MBR_EINVAL, "min_n must be >= 0");
+  if (!sc.use_default_bailout && !(sc.bailout > 0.0))
+    return set_err(ctx, MBR_EINVAL, "bailout must be > 0");
+  if (!finite3(sc.julia_c) || !finite3(sc.fractal_constant_factor) || !std::isfinite(sc.initial_waxis) ||
+      !std::isfinite(sc.linear_de_offset))
+    return set_err(ctx, MBR_EINVAL, "non-finite scene vector");
+  if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED && sc.delta_de_function != MBR_DE_FUNCTION_LINEAR &&
+      sc.delta_de_function != MBR_DE_FUNCTION_LOGARITHMIC)
+    return set_err(ctx, MBR_EUNSUPPORTED, "delta_de_function %d is not supported (preferred, linear, log)",
+                   sc.delta_de_function);
+  d.n = n;
+  d.is_hybrid = hybrid ? 1 : 0;
+  double maxBailout = 0.0;
+  bool any = false;
+  for (int i = 0; i < n; i++) {
+    const mbr_fractal &f = sc.fractal[i];
+    DevSlot &s = d.slot[i];
+    s.formula = f.formula;
+    if (f.formula == MBR_FORMULA_NONE && hybrid) {
+      s.check_bailout = 1;
+      continue;
+    }
+    FormulaMeta m;
+    if (!formula_meta(f.formula, &m))
+      return set_err(ctx, MBR_EUNSUPPORTED, "slot %d: formula %d is not supported (2, 7, 8)", i, f.formula);
+    any = true;
+    if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
+    if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)
+      return set_err(ctx, MBR_EINVAL, "slot %d: negative start/stop iteration", i);
+    if (!(f.formula_weight >= 0.0 && f.formula_weight <= 1.0))
+      return set_err(ctx, MBR_EINVAL, "slot %d: formula_weight must be in [0, 1]", i);
+    if (f.formula == MBR_FORMULA_MANDELBULB && !std::isfinite(f.bulb_power))
+      return set_err(ctx, MBR_EINVAL, "slot %d: non-finite power", i);
+    if (f.formula == MBR_FORMULA_MANDELBOX) {
+      if (!(f.mandelbox_folding_limit >= 0.0))
+        return set_err(ctx, MBR_EINVAL, "slot %d: mandelbox_folding_limit must be >= 0", i);
+      if (!(f.mandelbox_folding_min_radius > 0.0) || !(f.mandelbox_folding_fixed_radius >= 0.0))
+        return set_err(ctx, MBR_EINVAL, "slot %d: mandelbox radii must be min > 0, fixed >= 0", i);
+      if (!std::isfinite(f.mandelbox_scale) || !std::isfinite(f.mandelbox_folding_value) || !finite3(f.mandelbox_offset))
+        return set_err(ctx, MBR_EINVAL, "slot %d: non-finite mandelbox parameter", i);
+    }
+    if (f.formula == MBR_FORMULA_MENGER_SPONGE && !std::isfinite(f.transf_scale3))
+      return set_err(ctx, MBR_EINVAL, "slot %d: non-finite scale3", i);
+    // checkForBailout and the c-constant rule (hybrid_fractal_sequences.cpp:199-215)
+    s.check_bailout = hybrid ? (f.check_for_bailout != 0) : 1;
+    bool addc = f.dont_add_c_constant == 0;
+    if (m.cpixel == 1) addc = !addc;
+    s.add_c = addc ? 1 : 0;
+    double bailout;
+    if (sc.use_default_bailout) {
+      bailout = m.bailout;
+      if (hybrid) maxBailout = std::max(maxBailout, m.bailout);
+    } else {
+      bailout = sc.bailout;
+    }
+    // sFractal::RecalculateFractalParams (fractal.cpp:673-678)
+    const double deg = 0.01745329251994329576923690768489;
+    double *p = s.d;
+    p[P_POWER] = f.bulb_power;
+    p[P_POWER_M1] = f.bulb_power - 1.0;
+    p[P_ALPHA] = f.bulb_alpha_angle_offset * deg;
+    p[P_BETA] = f.bulb_beta_angle_offset * deg;
+    p[P_MB_SCALE] = f.mandelbox_scale;
+    p[P_MB_ABS_SCALE] = std::fabs(f.mandelbox_scale);
+    p[P_MB_LIMIT] = f.mandelbox_folding_limit;
+    p[P_MB_VALUE] = f.mandelbox_folding_value;
+    p[P_MB_FR2] = f.mandelbox_folding_fixed_radius * f.mandelbox_folding_fixed_radius;
+    p[P_MB_MR2] = f.mandelbox_folding_min_radius * f.mandelbox_folding_min_radius;
+    p[P_MB_FACTOR1] = p[P_MB_FR2] / p[P_MB_MR2];
+    p[P_MB_OFF_X] = f.mandelbox_offset[0];
+    p[P_MB_OFF_Y] = f.mandelbox_offset[1];
+    p[P_MB_OFF_Z] = f.mandelbox_offset[2];
+    p[P_SCALE3] = f.transf_scale3;
+    p[P_BAILOUT] = bailout;
+    p[P_WEIGHT] = f.formula_weight;
+    s.has_offset = (f.mandelbox_offset[0] != 0.0 || f.mandelbox_offset[1] != 0.0 || f.mandelbox_offset[2] != 0.0);
+  }
+  if (!any) return set_err(ctx, MBR_EINVAL, "scene has no formula");
+  if (hybrid && sc.use_default_bailout)
+    for (int i = 0; i < n; i++) d.slot[i].d[P_BAILOUT] = maxBailout;
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < P_COUNT; k++) d.slot[i].f[k] = float(d.slot[i].d[k]);
+
+  // the sequence (hybrid_fractal_sequences.cpp:296-370)
+  int length = MBR_SEQUENCE_LENGTH;
+  const int repeatFromIndex = std::max(0, std::min(sc.repeat_from - 1, n - 1));
+  int k = 0, counter = 0, last = 0;
+  bool rapidEnd = false;
+  for (int i = 0; i < length; i++) {
+    counter++;
+    int search = 0;
+    while ((d.slot[k].formula == MBR_FORMULA_NONE || i < sc.fractal[k].formula_start_iteration ||
+            i > sc.fractal[k].formula_stop_iteration) &&
+           search < n) {
+      k++;
+      if (k >= n) k = repeatFromIndex;
+      search++;
+    }
+    if (search >= n) {
+      rapidEnd = true;
+      break;
+    }
+    d.seq[i] = uint8_t(k);
+    last = i;
+    const int iters = hybrid ? sc.fractal[k].formula_iterations : sc.fractal[0].formula_iterations;
+    if (counter >= iters) {
+      counter = 0;
+      k++;
+      if (k >= n) k = repeatFromIndex;
+    }
+  }
+  if (rapidEnd) length = last + 1;
+  d.length = length;
+
+  // DE function (hybrid_fractal_sequences.cpp:377-485)
+  if (hybrid) {
+    if (sc.delta_de_function == MBR_DE_FUNCTION_PREFERRED) {
+      int count[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < n; i++) {
+        FormulaMeta m;
+        if (formula_meta(d.slot[i].formula, &m)) count[m.de_function] += sc.fractal[i].formula_iterations;
+      }
+      int maxCount = -1;
+      for (int i = 1; i <= 6; i++)
+        if (count[i] > maxCount) {
+          maxCount = count[i];
+          d.de_function = i;
+        }
+    } else {
+      d.de_function = sc.delta_de_function;
+    }
+    d.de_analytic = (d.de_function == 2) ? 2 : 1;
+    d.uniform_formula = 0;
+  } else {
+    FormulaMeta m;
+    formula_meta(d.slot[0].formula, &m);
+    d.de_function = m.de_function;
+    d.de_analytic = m.analytic;
+    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {
+      d.de_function = sc.delta_de_function;
+      d.de_analytic = (d.de_function == 2) ? 2 : 1;
+    }
+    d.uniform_formula = d.slot[0].formula;
+  }
+  d.formula_maxiter = sc.formula_maxiter;
+  d.min_n = sc.min_n;
+  d.iter_thresh = sc.iteration_threshold_mode ? 1 : 0;
+  d.interior = sc.interior_mode ? 1 : 0;
+  d.julia = sc.julia_mode ? 1 : 0;
+  for (int i = 0; i < 3; i++) {
+    d.julia_c[i] = sc.julia_c[i];
+    d.cmul[i] = sc.fractal_constant_factor[i];
+    d.fjulia_c[i] = float(sc.julia_c[i] * sc.fractal_constant_factor[i]);
+    d.fcmul[i] = float(sc.fractal_constant_factor[i]);
+  }
+  d.w0 = sc.initial_waxis;
+  d.has_w = sc.initial_waxis != 0.0;
+  d.linear_de_offset = sc.linear_de_offset;
+  d.flinear_de_offset = float(sc.linear_de_offset);
+  *out = d;
+  return MBR_OK;
+}
+
+// cCameraTarget::SetCameraTargetTop + PrepareMainVectors (restated).
+struct HV {
+  double x, y, z;
+};
+static HV hadd(HV a, HV b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static HV hmul(HV a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static double hdot(HV a, HV b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static HV hcross(HV a, HV v) { return {a.y * v.z - a.z * v.y, -a.x * v.z + a.z * v.x, a.x * v.y - a.y * v.x}; }
+static HV hnorm(HV a) {
+  const double n = 1.0 / std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  return {a.x * n, a.y * n, a.z * n};
+}
+static HV hrotate_around(HV v, HV axis, double angle) {  // CVector3::RotateAroundVectorByAngle
+  HV r = hmul(v, std::cos(angle));
+  r = hadd(r, hmul(hcross(axis, v), std::sin(angle)));
+  r = hadd(r, hmul(hmul(axis, hdot(axis, v)), 1 - std::cos(angle)));
+  return r;
+}
+static double correct_angle(double a) { return std::fmod(a + 3 * kPi, 2 * kPi) - kPi; }
+static void mat3_mul(const double *a, const double *b, double *r) {
+  double t[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) t[i * 3 + j] = a[i * 3 + 0] * b[j] + a[i * 3 + 1] * b[3 + j] + a[i * 3 + 2] * b[6 + j];
+  std::memcpy(r, t, sizeof(t));
+}
+static void rotate_axis(double *m, bool *zero, int axis, double angle) {  // CRotationMatrix::RotateX/Y/Z
+  if (angle == 0.0) return;
+  double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double s = std::sin(angle), c = std::cos(angle);
+  if (axis == 0) { r[0] = 1.0; r[4] = c; r[8] = c; r[5] = -s; r[7] = s; }
+  if (axis == 1) { r[4] = 1.0; r[8] = c; r[0] = c; r[6] = -s; r[2] = s; }
+  if (axis == 2) { r[8] = 1.0; r[0] = c; r[4] = c; r[1] = -s; r[3] = s; }
+  mat3_mul(m, r, m);
+  *zero = false;
+}
+
+void camera_matrix(const mbr_camera &cam, double mrot[9], bool *zero, double angles[3]) {
+  double yaw, pitch, roll;
+  if (cam.use_angles) {
+    yaw = cam.angles[0];
+    pitch = cam.angles[1];
+    roll = cam.angles[2];
+  } else {
+    const HV c{cam.camera[0], cam.camera[1], cam.camera[2]};
+    const HV t{cam.target[0], cam.target[1], cam.target[2]};
+    HV fwd = (c.x == t.x && c.y == t.y && c.z == t.z) ? HV{0.0, 1.0, 0.0} : HV{t.x - c.x, t.y - c.y, t.z - c.z};
+    fwd = hnorm(fwd);
+    yaw = std::atan2(fwd.y, fwd.x) - 0.5 * kPi;
+    pitch = std::atan2(fwd.z, std::sqrt(fwd.x * fwd.x + fwd.y * fwd.y));
+    HV top = hnorm(HV{cam.top[0], cam.top[1], cam.top[2]});
+    top = hrotate_around(top, HV{0.0, 0.0, 1.0}, -yaw);
+    top = hrotate_around(top, HV{1.0, 0.0, 0.0}, -pitch);
+    roll = -std::atan2(top.z, top.x) + 0.5 * kPi;
+    yaw = correct_angle(yaw);
+    pitch = correct_angle(pitch);
+    roll = correct_angle(roll);
+  }
+  for (int i = 0; i < 9; i++) mrot[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  *zero = true;
+  rotate_axis(mrot, zero, 2, yaw);
+  rotate_axis(mrot, zero, 0, pitch);
+  rotate_axis(mrot, zero, 1, roll);
+  angles[0] = yaw;
+  angles[1] = pitch;
+  angles[2] = roll;
+}
+
+mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam) {
+  if (cam.width < 1 || cam.height < 1 || cam.width > 65535 || cam.height > 65535)
+    return set_err(ctx, MBR_EINVAL, "image size %dx%d out of range [1, 65535]", cam.width, cam.height);
+  if (!(cam.fov_deg > 0.0 && cam.fov_deg < 180.0))
+    return set_err(ctx, MBR_EINVAL, "fov_deg must be in (0, 180), got %g", cam.fov_deg);
+  if (!finite3(cam.camera) || !finite3(cam.target) || !finite3(cam.top) || !finite3(cam.angles))
+    return set_err(ctx, MBR_EINVAL, "non-finite camera vector");
+  if (!cam.use_angles && cam.top[0] == 0.0 && cam.top[1] == 0.0 && cam.top[2] == 0.0)
+    return set_err(ctx, MBR_EINVAL, "top vector is zero");
+  return MBR_OK;
+}
+
+mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out) {
+  mbr_status st = validate_camera(ctx, cam);
+  if (st != MBR_OK) return st;
+  if (!(p.detail_level > 0.0) || !(p.de_factor > 0.0) || !(p.view_distance_max > 0.0) || !(p.smoothness > 0.0))
+    return set_err(ctx, MBR_EINVAL, "detail_level, de_factor, view_distance_max and smoothness must be > 0");
+  if (p.max_raymarching_steps < 1 || p.max_raymarching_steps > 100000000)
+    return set_err(ctx, MBR_EINVAL, "max_raymarching_steps must be in [1, 1e8]");
+  if (p.binary_steps < 0 || p.binary_steps > 200) return set_err(ctx, MBR_EINVAL, "binary_steps must be in [0, 200]");
+  if (p.refine != MBR_REFINE_REFERENCE && p.refine != MBR_REFINE_ROOT)
+    return set_err(ctx, MBR_EINVAL, "unknown refine mode %d", p.refine);
+  if (p.ao_rays < 0 || p.ao_rays > 4096) return set_err(ctx, MBR_EINVAL, "ao_rays must be in [0, 4096]");
+  if (p.gi_samples < 0 || p.gi_samples > 65536 || p.gi_bounces < 0 || p.gi_bounces > 64)
+    return set_err(ctx, MBR_EINVAL, "gi_samples in [0, 65536] and gi_bounces in [0, 64] required");
+  if (p.gi_samples > 0 && p.dof_aperture > 0.0 && !(p.dof_focus > 0.0))
+    return set_err(ctx, MBR_EINVAL, "dof_focus must be > 0 with an aperture");
+  if (!(p.gamma > 0.0)) return set_err(ctx, MBR_EINVAL, "gamma must be > 0");
+  if (p.constant_de_threshold && !(p.de_thresh > 0.0)) return set_err(ctx, MBR_EINVAL, "de_thresh must be > 0");
+  const double *L = p.light_direction;
+  if (!finite3(L) || (L[0] == 0.0 && L[1] == 0.0 && L[2] == 0.0))
+    return set_err(ctx, MBR_EINVAL, "light_direction must be finite and non-zero");
+  DevFrame f;
+  std::memset(&f, 0, sizeof(f));
+  for (int i = 0; i < 3; i++) f.camera[i] = cam.camera[i];
+  bool zero;
+  double ang[3];
+  camera_matrix(cam, f.mrot, &zero, ang);
+  f.mrot_zero = zero ? 1 : 0;
+  f.width = cam.width;
+  f.height = cam.height;
+  f.max_steps = p.max_raymarching_steps;
+  f.binary_steps = p.binary_steps;
+  f.refine = p.refine;
+  f.jitter = p.jitter ? 1 : 0;
+  f.seed = p.seed;
+  f.fov = 2.0 * std::tan(cam.fov_deg / 360.0 * kPi);
+  f.resolution = 1.0 / cam.height;
+  f.aspect = double(cam.width) / cam.height;
+  f.detail_level = p.detail_level;
+  f.de_factor = p.de_factor;
+  f.view_distance_max = p.view_distance_max;
+  f.smoothness = p.smoothness;
+  f.constant_de_threshold = p.constant_de_threshold ? 1 : 0;
+  f.de_thresh = p.de_thresh;
+  f.shading_enable = p.shading_enable ? 1 : 0;
+  f.shadow_enable = p.shadow_enable ? 1 : 0;
+  f.ao_rays = p.ao_rays;
+  const HV l = hnorm(HV{L[0], L[1], L[2]});
+  f.light[0] = l.x;
+  f.light[1] = l.y;
+  f.light[2] = l.z;
+  f.light_intensity = float(p.light_intensity);
+  f.material_shading = float(p.material_shading);
+  f.albedo = float(p.albedo);
+  f.ambient = float(p.ambient_intensity);
+  for (int i = 0; i < 3; i++) f.background[i] = float(p.background[i]);
+  f.ao_seed = p.ao_seed;
+  f.gi_samples = p.gi_samples;
+  f.gi_bounces = p.gi_bounces;
+  f.gi_seed = p.gi_seed;
+  f.gi_sky = p.gi_sky;
+  f.gi_sun = p.gi_sun;
+  f.dof_aperture = p.dof_aperture;
+  f.dof_focus = p.dof_focus;
+  f.brightness = float(p.brightness);
+  f.contrast = float(p.contrast);
+  f.saturation = float(p.saturation);
+  f.hdr = p.hdr ? 1 : 0;
+  // gamma table (cImage::CalculateGammaTable), cached per context
+  if (ctx->gamma_value != p.gamma || !ctx->d_gamma) {
+    std::vector<uint16_t> t(65536);
+    for (int i = 0; i < 65536; i++) t[i] = uint16_t(int(powf(i / 65536.0f, 1.0f / float(p.gamma)) * 65535.0f));
+    if (!ctx->d_gamma) {
+      int e = int(cudaMalloc(&ctx->d_gamma, 65536 * sizeof(uint16_t)));
+      if (e) {
+        ctx->d_gamma = nullptr;
+        return set_err(ctx, MBR_ENOMEM, "cudaMalloc(gamma): %s", cudaGetErrorString(cudaError_t(e)));
+      }
+    }
+    int e = int(cudaMemcpy(ctx->d_gamma, t.data(), 65536 * sizeof(uint16_t), cudaMemcpyHostToDevice));
+    if (e) return cuda_err(ctx, e, "cudaMemcpy(gamma)");
+    ctx->gamma_value = p.gamma;
+  }
+  f.gamma = ctx->d_gamma;
+  *out = f;
+  return MBR_OK;
+}
+
+DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o) {
+  DevOutputs d;
+  d.depth = o.depth;
+  d.iters = o.iters;
+  d.hit = o.hit;
+  d.normal = o.normal;
+  d.shade = o.shade;
+  d.ao = o.ao;
+  d.rgb = o.rgb;
+  d.rgb8 = o.rgb8;
+  d.stats = o.stats;
+  d.status = ctx->d_status;
+  d.pixel_offset = 0;
+  return d;
+}
+
+const DevScene *ctx_scene(mbr_ctx *ctx) { return ctx->has_scene ? &ctx->scene : nullptr; }
+const mbr_scene *ctx_scene_src(mbr_ctx *ctx) { return ctx->has_scene ? &ctx->scene_src : nullptr; }
+mbr_tuning &ctx_tuning(mbr_ctx *ctx) { return ctx->tuning; }
+int32_t *ctx_status(mbr_ctx *ctx) { return ctx->d_status; }
+
+// Device scratch of the wavefront kernel, grown on demand (never shrunk).
+mbr_status ctx_work(mbr_ctx *ctx, size_t words, unsigned long long **out) {
+  if (ctx->work_words < words) {
+    if (ctx->d_work) cudaFree(ctx->d_work);
+    ctx->d_work = nullptr;
+    ctx->work_words = 0;
+    const int e = int(cudaMalloc(&ctx->d_work, words * sizeof(unsigned long long)));
+    if (e) return set_err(ctx, MBR_ENOMEM, "cudaMalloc(work): %s", cudaGetErrorString(cudaError_t(e)));
+    ctx->work_words = words;
+  }
+  *out = ctx->d_work;
+  return MBR_OK;
+}
+
+}  // namespace mbr
+
+// ============================================================================
+// C-ABI
+// ============================================================================
+extern "C" {
+
+const char *mbr_version(void) { return "mandelbulber2_b200 1.0 (sm_100a)"; }
+
+mbr_status mbr_create(mbr_ctx **out, int device) {
+  if (!out) return MBR_EINVAL;
+  *out = nullptr;
+  mbr_ctx *ctx = new (std::nothrow) mbr_ctx();
+  if (!ctx) return MBR_ENOMEM;
+  ctx->device = device;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    delete ctx;
+    return MBR_ECUDA;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete ctx;
+    return MBR_ECUDA;
+  }
+  if (cudaMalloc(&ctx->d_status, sizeof(int32_t)) != cudaSuccess) {
+    delete ctx;
+    return MBR_ENOMEM;
+  }
+  cudaMemset(ctx->d_status, 0, sizeof(int32_t));
+  mbr_scene_defaults(&ctx->scene_src);
+  *out = ctx;
+  return MBR_OK;
+}
+
+void mbr_destroy(mbr_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->d_gamma) cudaFree(ctx->d_gamma);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->d_work) cudaFree(ctx->d_work);
+  if (ctx->adjoint_scratch) cudaFree(ctx->adjoint_scratch);
+  delete ctx;
+}
+
+const char *mbr_last_error_string(const mbr_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void mbr_fractal_defaults(mbr_fractal *f, int formula) {
+  if (!f) return;
+  std::memset(f, 0, sizeof(*f));
+  // src/initparameters.cpp:701-750, 1010
+  f->formula = formula;
+  f->formula_iterations = 1;
+  f->formula_start_iteration = 0;
+  f->formula_stop_iteration = 250;
+  f->dont_add_c_constant = 0;
+  f->check_for_bailout = 1;
+  f->formula_weight = 1.0;
+  f->bulb_power = 9.0;
+  f->mandelbox_scale = 2.0;
+  f->mandelbox_folding_limit = 1.0;
+  f->mandelbox_folding_value = 2.0;
+  f->mandelbox_folding_min_radius = 0.5;
+  f->mandelbox_folding_fixed_radius = 1.0;
+  f->transf_scale3 = 3.0;
+}
+
+void mbr_scene_defaults(mbr_scene *s) {
+  if (!s) return;
+  std::memset(s, 0, sizeof(*s));
+  // src/initparameters.cpp:128-157 and the default node (:2102-2125)
+  s->n_fractals = 1;
+  s->formula_maxiter = 250;
+  s->repeat_from = 1;
+  s->use_default_bailout = 1;
+  s->delta_de_function = MBR_DE_FUNCTION_PREFERRED;
+  s->min_n = 1;
+  s->bailout = 100.0;
+  for (int i = 0; i < 3; i++) s->fractal_constant_factor[i] = 1.0;
+  mbr_fractal_defaults(&s->fractal[0], MBR_FORMULA_MANDELBULB);
+  for (int i = 1; i < MBR_MAX_FRACTALS; i++) mbr_fractal_defaults(&s->fractal[i], MBR_FORMULA_NONE);
+}
+
+void mbr_camera_defaults(mbr_camera *c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  // src/initparameters.cpp:113-120
+  c->camera[0] = 3.0;
+  c->camera[1] = -6.0;
+  c->camera[2] = 2.0;
+  c->top[2] = 1.0;
+  c->fov_deg = 53.13;
+  c->width = 800;
+  c->height = 600;
+}
+
+void mbr_render_params_defaults(mbr_render_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->detail_level = 1.0;
+  p->de_factor = 1.0;
+  p->view_distance_max = 50.0;
+  p->smoothness = 1.0;
+  p->max_raymarching_steps = 10000;
+  p->binary_steps = 30;
+  p->refine = MBR_REFINE_REFERENCE;
+  p->jitter = 1;
+  p->de_thresh = 0.01;
+  p->shading_enable = 1;
+  p->shadow_enable = 1;
+  p->light_direction[0] = 1.0;
+  p->light_direction[1] = -1.0;
+  p->light_direction[2] = 1.0;
+  p->light_intensity = 1.0;
+  p->material_shading = 1.0;
+  p->albedo = 1.0;
+  p->ambient_intensity = 0.0;
+  p->dof_focus = 3.0;
+  p->gi_sky = 0.3;
+  p->gi_sun = 3.0;
+  p->brightness = 1.0;
+  p->contrast = 1.0;
+  p->gamma = 1.0;
+  p->saturation = 1.0;
+}
+
+mbr_status mbr_scene_set(mbr_ctx *ctx, const mbr_scene *scene) {
+  if (!ctx || !scene) return set_err(ctx, MBR_EINVAL, "null argument");
+  DevScene d;
+  mbr_status st = build_scene(ctx, *scene, &d);
+  if (st != MBR_OK) return st;
+  ctx->scene = d;
+  ctx->scene_src = *scene;
+  ctx->has_scene = true;
+  return MBR_OK;
+}
+
+mbr_status mbr_camera_rotation(const mbr_camera *camera, double mrot[9], double angles[3]) {
+  if (!camera || !mrot || !angles) return MBR_EINVAL;
+  bool zero;
+  camera_matrix(*camera, mrot, &zero, angles);
+  return MBR_OK;
+}
+
+mbr_status mbr_scene_sequence(const mbr_scene *scene, int32_t *seq_out, int32_t *length_out,
+                              int32_t *de_function_out, double *bailout_out) {
+  if (!scene) return MBR_EINVAL;
+  DevScene d;
+  mbr_status st = build_scene(nullptr, *scene, &d);
+  if (st != MBR_OK) return st;
+  if (seq_out)
+    for (int i = 0; i < d.length; i++) seq_out[i] = d.seq[i];
+  if (length_out) *length_out = d.length;
+  if (de_function_out) *de_function_out = d.is_hybrid ? d.de_function : d.de_analytic;
+  if (bailout_out)
+    for (int i = 0; i < d.n; i++) bailout_out[i] = d.slot[i].d[P_BAILOUT];
+  return MBR_OK;
+}
+
+mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                      const mbr_outputs *out, int engine, void *stream) {
+  if (!ctx || !camera || !params || !out) return set_err(ctx, MBR_EINVAL, "null argument");
+  if (!ctx->has_scene) return set_err(ctx, MBR_EINVAL, "no scene set (call mbr_scene_set first)");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MBR_ECUDA, "cudaSetDevice failed");
+  DevFrame fr;
+  mbr_status st = build_frame(ctx, *camera, *params, &fr);
+  if (st != MBR_OK) return st;
+  fr.want_normal = out->normal != nullptr;
+  const DevOutputs d = dev_outputs(ctx, *out);
+  const bool fp32 = engine == MBR_ENGINE_PLAIN_MIXED || engine == MBR_ENGINE_WAVEFRONT_FP32;
+  if (fp32 && ctx->scene.has_w)
+    return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need initial_waxis == 0");
+  int e;
+  switch (engine) {
+    case MBR_ENGINE_PLAIN_FP64: e = launch_plain_fp64(ctx->scene, fr, d, stream); break;
+    case MBR_ENGINE_PLAIN_FP64_STRICT: e = launch_plain_fp64_strict(ctx->scene, fr, d, stream); break;
+    case MBR_ENGINE_PLAIN_MIXED: e = launch_plain_mixed(ctx->scene, fr, d, stream); break;
+    case MBR_ENGINE_WAVEFRONT_FP32:
+    case MBR_ENGINE_WAVEFRONT_FP64:
+      return render_wavefront(ctx, ctx->scene, fr, d, engine, stream);
+    default: return set_err(ctx, MBR_EINVAL, "unknown engine %d", engine);
+  }
+  return cuda_err(ctx, e, "kernel launch");
+}
+
+mbr_status mbr_sync(mbr_ctx *ctx, void *stream) {
+  if (!ctx) return MBR_EINVAL;
+  int e = int(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  if (e) return cuda_err(ctx, e, "cudaStreamSynchronize");
+  int32_t status = 0;
+  e = int(cudaMemcpy(&status, ctx->d_status, sizeof(status), cudaMemcpyDeviceToHost));
+  if (e) return cuda_err(ctx, e, "cudaMemcpy(status)");
+  if (status != 0) {
+    cudaMemset(ctx->d_status, 0, sizeof(int32_t));
+    return set_err(ctx, MBR_ETIMEOUT, "device watchdog tripped (status %d)", status);
+  }
+  return MBR_OK;
+}
+
+mbr_status mbr_distance(mbr_ctx *ctx, const double *points, int64_t n, double detail_size, int normal_mode,
+                        double *dist, int32_t *iters, int engine, void *stream) {
+  if (!ctx) return MBR_EINVAL;
+  if (!ctx->has_scene) return set_err(ctx, MBR_EINVAL, "no scene set");
+  if (n < 0 || (n > 0 && (!points || !dist))) return set_err(ctx, MBR_EINVAL, "bad point buffers");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MBR_ECUDA, "cudaSetDevice failed");
+  int e;
+  switch (engine) {
+    case MBR_ENGINE_PLAIN_FP64:
+    case MBR_ENGINE_WAVEFRONT_FP64:
+      e = launch_distance_fp64(ctx->scene, points, n, detail_size, normal_mode, dist, iters, stream);
+      break;
+    case MBR_ENGINE_PLAIN_FP64_STRICT:
+      e = launch_distance_fp64_strict(ctx->scene, points, n, detail_size, normal_mode, dist, iters, stream);
+      break;
+    case MBR_ENGINE_PLAIN_MIXED:
+    case MBR_ENGINE_WAVEFRONT_FP32:
+      if (ctx->scene.has_w) return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need initial_waxis == 0");
+      e = launch_distance_fp32(ctx->scene, points, n, detail_size, normal_mode, dist, iters, stream);
+      break;
+    default: return set_err(ctx, MBR_EINVAL, "unknown engine %d", engine);
+  }
+  return cuda_err(ctx, e, "distance kernel launch");
+}
+
+mbr_status mbr_set_tuning(mbr_ctx *ctx, const mbr_tuning *t) {
+  if (!ctx || !t) return MBR_EINVAL;
+  if (t->block_size < 32 || t->block_size > 1024 || t->block_size % 32 || t->ctas_per_sm < 1 ||
+      t->ctas_per_sm > 32 || t->refill_k < 0 || t->refill_k > 32 || t->queue_layout < 0 || t->queue_layout > 1)
+    return set_err(ctx, MBR_EINVAL, "tuning out of range");
+  ctx->tuning = *t;
+  return MBR_OK;
+}
+
+mbr_status mbr_get_tuning(const mbr_ctx *ctx, mbr_tuning *t) {
+  if (!ctx || !t) return MBR_EINVAL;
+  *t = ctx->tuning;
+  return MBR_OK;
+}
+
+}  // extern "C"

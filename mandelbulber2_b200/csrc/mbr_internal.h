@@ -1,0 +1,25 @@
+// mbr_internal.h - host-side helpers shared by the library's translation units.
+#pragma once
+#include "../../include/mbr.h"
+#include "mbr_device.h"
+
+namespace mbr {
+
+mbr_status set_err(mbr_ctx *ctx, mbr_status st, const char *fmt, ...);
+mbr_status cuda_err(mbr_ctx *ctx, int code, const char *what);
+mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out);
+mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out);
+mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam);
+void camera_matrix(const mbr_camera &cam, double mrot[9], bool *zero, double angles[3]);
+DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o);
+const DevScene *ctx_scene(mbr_ctx *ctx);
+const mbr_scene *ctx_scene_src(mbr_ctx *ctx);
+mbr_tuning &ctx_tuning(mbr_ctx *ctx);
+int32_t *ctx_status(mbr_ctx *ctx);
+mbr_status ctx_work(mbr_ctx *ctx, size_t words, unsigned long long **out);
+
+// wavefront.cu
+mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, const DevOutputs &out, int engine,
+                            void *stream);
+
+}  // namespace mbr

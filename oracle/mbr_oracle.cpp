@@ -1,0 +1,1412 @@
+// mbr_oracle.cpp - CPU restatement of mandelbulber2's distance-estimation
+// raymarching path.  TEST INFRASTRUCTURE ONLY: the parity checker for the CUDA
+// kernels and the timed CPU baseline.  The product never links or calls it.
+//
+// Every function follows the reference file:line it names.  Parity of the
+// restatement is pinned against the reference itself: the formula iterations,
+// the camera set-up and the Park-Miller generator are checked bit-for-bit
+// against the reference's own sources compiled into oracle/_ref (golden
+// vectors in tests/golden/, produced by tests/golden/make_golden.py).
+//
+// Built twice by oracle/Makefile: strict IEEE (-O2 -fno-fast-math
+// -ffp-contract=off, the parity oracle) and as the reference ships
+// (-O3 -ffast-math -fopenmp, qmake/common.pri:116-121, the timed baseline).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "../include/mbr.h"
+#include "oracle_scalar.hpp"
+
+namespace oracle {
+using std::asin;
+using std::atan2;
+using std::cos;
+using std::fabs;
+using std::isfinite;
+using std::log;
+using std::pow;
+using std::sin;
+using std::sqrt;
+
+thread_local OpTally g_tally;
+
+// ============================================================================
+// Formula metadata: the constructors of the three formula classes
+// (fractal_mandelbulb.cpp:16-27, fractal_mandelbox.cpp:18-29,
+//  fractal_menger_sponge.cpp:17-28).  fractal_enums.h:47-88 numbering.
+// ============================================================================
+struct FormulaInfo {
+  int de_function;      // enumDEFunctionType
+  int cpixel;           // enumCPixelAddition: 0 enabled by default, 1 disabled by default
+  double default_bailout;
+  int analytic;         // enumDEAnalyticFunction
+};
+static bool formula_info(int formula, FormulaInfo *fi) {
+  switch (formula) {
+    case MBR_FORMULA_MANDELBULB: *fi = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
+    case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
+    default: return false;
+  }
+}
+
+// ============================================================================
+// Hybrid sequence: cHybridFractalSequences::CollectSequenceData +
+// CreateSequence (hybrid_fractal_sequences.cpp:181-499) for one fractal or
+// hybrid node of the default objects tree.
+// ============================================================================
+struct Slot {
+  int formula = 0;
+  bool add_c = false, check_bailout = true;
+  double weight = 1.0, bailout = 10.0;
+  int iterations = 1, start = 0, stop = 250;
+  double power = 9, alpha = 0, beta = 0;
+  double mb_scale = 2, mb_limit = 1, mb_value = 2, mb_min = 0.5, mb_fixed = 1;
+  double mb_offset[3] = {0, 0, 0};
+  double scale3 = 3;
+};
+struct Seq {
+  bool is_hybrid = false, julia = false;
+  int length = 0, n = 0, formula_maxiter = 250, min_n = 1;
+  int de_function = 1, de_analytic = 1;
+  bool iter_thresh = false, interior = false;
+  double julia_c[3] = {0, 0, 0}, cmul[3] = {1, 1, 1}, w0 = 0, linear_de_offset = 0;
+  std::vector<int> seq;
+  Slot slot[MBR_MAX_FRACTALS];
+};
+
+// Returns false for scenes the restatement does not cover.
+static bool build_sequence(const mbr_scene &sc, Seq *out) {
+  Seq s;
+  const bool hybrid = sc.hybrid_fractal_enable != 0;
+  const int n = hybrid ? sc.n_fractals : 1;
+  if (n < 1 || n > MBR_MAX_FRACTALS) return false;
+  s.is_hybrid = hybrid;
+  s.n = n;
+  double maxBailout = 0.0;
+  for (int i = 0; i < n; i++) {
+    const mbr_fractal &f = sc.fractal[i];
+    Slot &sl = s.slot[i];
+    FormulaInfo fi;
+    if (hybrid && f.formula == MBR_FORMULA_NONE) {  // skipped by the sequence generator
+      sl.formula = MBR_FORMULA_NONE;
+      continue;
+    }
+    if (!formula_info(f.formula, &fi)) return false;
+    sl.formula = f.formula;
+    sl.iterations = f.formula_iterations;
+    sl.weight = f.formula_weight;
+    sl.start = f.formula_start_iteration;
+    sl.stop = f.formula_stop_iteration;
+    sl.check_bailout = f.check_for_bailout != 0;
+    if (!hybrid) sl.check_bailout = true;  // :201
+    // c-constant rule :204-215
+    bool addc = !(f.dont_add_c_constant != 0);
+    if (fi.cpixel == 1) addc = !addc;
+    sl.add_c = addc;
+    if (sc.use_default_bailout) {  // :217-224
+      if (hybrid) maxBailout = std::max(maxBailout, fi.default_bailout);
+      else sl.bailout = fi.default_bailout;
+    } else {
+      sl.bailout = sc.bailout;
+    }
+    // sFractal::RecalculateFractalParams (fractal.cpp:673-678)
+    sl.power = f.bulb_power;
+    sl.alpha = f.bulb_alpha_angle_offset * 0.01745329251994329576923690768489;
+    sl.beta = f.bulb_beta_angle_offset * 0.01745329251994329576923690768489;
+    sl.mb_scale = f.mandelbox_scale;
+    sl.mb_limit = f.mandelbox_folding_limit;
+    sl.mb_value = f.mandelbox_folding_value;
+    sl.mb_min = f.mandelbox_folding_min_radius;
+    sl.mb_fixed = f.mandelbox_folding_fixed_radius;
+    for (int k = 0; k < 3; k++) sl.mb_offset[k] = f.mandelbox_offset[k];
+    sl.scale3 = f.transf_scale3;
+  }
+  if (hybrid && sc.use_default_bailout)
+    for (int i = 0; i < n; i++) s.slot[i].bailout = maxBailout;  // :253-259
+  s.julia = sc.julia_mode != 0;
+  for (int k = 0; k < 3; k++) {
+    s.julia_c[k] = sc.julia_c[k];
+    s.cmul[k] = sc.fractal_constant_factor[k];
+  }
+  s.w0 = sc.initial_waxis;
+  s.formula_maxiter = sc.formula_maxiter;
+  s.min_n = sc.min_n;
+  s.iter_thresh = sc.iteration_threshold_mode != 0;
+  s.interior = sc.interior_mode != 0;
+  s.linear_de_offset = sc.linear_de_offset;
+
+  // sequence generation :296-370
+  const int maxN = 250;
+  s.length = maxN * 5;
+  s.seq.assign(s.length, 0);
+  int repeatFromIndex = std::max(0, std::min(sc.repeat_from - 1, n - 1));
+  int k = 0, counter = 0, last = 0;
+  bool rapidEnd = false;
+  for (int i = 0; i < s.length; i++) {
+    counter++;
+    int searchRepeatCount = 0;
+    while ((s.slot[k].formula == MBR_FORMULA_NONE || i < s.slot[k].start || i > s.slot[k].stop) &&
+           searchRepeatCount < n) {
+      k++;
+      if (k >= n) k = repeatFromIndex;
+      searchRepeatCount++;
+    }
+    if (searchRepeatCount >= n) {
+      rapidEnd = true;
+      break;
+    }
+    s.seq[i] = k;
+    last = i;
+    if (counter >= s.slot[k].iterations) {
+      counter = 0;
+      k++;
+      if (k >= n) k = repeatFromIndex;
+    }
+  }
+  if (rapidEnd) s.length = last + 1;
+  if (s.length <= 0) return false;
+
+  // DE function choice :377-485 (analytic formulas only)
+  if (hybrid) {
+    if (sc.delta_de_function == MBR_DE_FUNCTION_PREFERRED) {
+      int count[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int i = 0; i < n; i++) {
+        FormulaInfo fi;
+        if (formula_info(s.slot[i].formula, &fi)) count[fi.de_function] += s.slot[i].iterations;
+      }
+      int maxCount = -1;
+      for (int i = 1; i <= 6; i++)
+        if (count[i] > maxCount) {
+          maxCount = count[i];
+          s.de_function = i;
+        }
+    } else {
+      s.de_function = sc.delta_de_function;
+    }
+  } else {
+    FormulaInfo fi;
+    formula_info(s.slot[0].formula, &fi);
+    s.de_function = fi.de_function;
+    s.de_analytic = fi.analytic;
+    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {
+      s.de_function = sc.delta_de_function;
+      s.de_analytic = (s.de_function == 2) ? 2 : 1;
+    }
+  }
+  if (s.de_function != 1 && s.de_function != 2) return false;
+  *out = s;
+  return true;
+}
+
+// ============================================================================
+// Formula iterations, templated on the scalar.
+// ============================================================================
+template <class S>
+struct V4 {
+  S x, y, z, w;
+};
+template <class S>
+inline S len4(const V4<S> &v) {  // CVector4::Length (algebra.hpp:401)
+  return sqrt(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
+}
+template <class S>
+inline bool nan4(const V4<S> &v) {  // CVector4::IsNotANumber (algebra.hpp:444-451)
+  return !(static_cast<int>(isfinite(v.x)) & static_cast<int>(isfinite(v.y)) &
+           static_cast<int>(isfinite(v.z)) & static_cast<int>(isfinite(v.w)));
+}
+inline int sgn(double v) { return (0.0 < v) - (v < 0.0); }  // math_utilities.h:65-67
+
+// Formula parameters in the scalar type, so tangents can be seeded.
+template <class S>
+struct SlotT {
+  S power, alpha, beta;
+  S mb_scale, mb_limit, mb_value, mb_mR2, mb_fR2, mb_factor1;
+  S mb_off[3];
+  S scale3;
+};
+enum { TAN_POWER = 0, TAN_SCALE = 1, TAN_MR2 = 2, TAN_X = 3, TAN_Y = 4, TAN_Z = 5 };
+
+template <class S>
+S seeded(double v, int k, int want);
+template <>
+inline double seeded<double>(double v, int, int) { return v; }
+template <>
+inline OpCount seeded<OpCount>(double v, int, int) { return OpCount(v); }
+template <class S>
+S seeded(double v, int k, int want) {
+  return want ? S::seed(v, k) : S(v);
+}
+
+template <class S>
+SlotT<S> make_slot(const Slot &s, bool tangents) {
+  SlotT<S> t;
+  t.power = seeded<S>(s.power, TAN_POWER, tangents);
+  t.alpha = S(s.alpha);
+  t.beta = S(s.beta);
+  t.mb_scale = seeded<S>(s.mb_scale, TAN_SCALE, tangents);
+  t.mb_limit = S(s.mb_limit);
+  t.mb_value = S(s.mb_value);
+  // RecalculateFractalParams (fractal.cpp:673-675)
+  t.mb_fR2 = S(s.mb_fixed * s.mb_fixed);
+  t.mb_mR2 = seeded<S>(s.mb_min * s.mb_min, TAN_MR2, tangents);
+  t.mb_factor1 = t.mb_fR2 / t.mb_mR2;
+  for (int k = 0; k < 3; k++) t.mb_off[k] = S(s.mb_offset[k]);
+  t.scale3 = S(s.scale3);
+  return t;
+}
+
+// cFractalMandelbulb::FormulaCode (fractal_mandelbulb.cpp:29-43)
+template <class S>
+inline void formula_mandelbulb(V4<S> &z, const SlotT<S> &f, S &r, S &DE) {
+  const S th0 = asin(z.z / r) + f.beta;
+  const S ph0 = atan2(z.y, z.x) + f.alpha;
+  S rp = pow(r, f.power - 1.0);
+  const S th = th0 * f.power;
+  const S ph = ph0 * f.power;
+  const S cth = cos(th);
+  DE = (rp * DE) * f.power + 1.0;
+  rp = rp * r;
+  z.x = cth * cos(ph) * rp;
+  z.y = cth * sin(ph) * rp;
+  z.z = sin(th) * rp;
+}
+
+// cFractalMandelbox::FormulaCode, rotations disabled (fractal_mandelbox.cpp:66-107)
+template <class S>
+inline void formula_mandelbox(V4<S> &z, const SlotT<S> &f, S &DE) {
+  if (fabs(z.x) > f.mb_limit) z.x = S(double(sgn(val(z.x)))) * f.mb_value - z.x;
+  if (fabs(z.y) > f.mb_limit) z.y = S(double(sgn(val(z.y)))) * f.mb_value - z.y;
+  if (fabs(z.z) > f.mb_limit) z.z = S(double(sgn(val(z.z)))) * f.mb_value - z.z;
+  const S r2 = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+  z.x = z.x + f.mb_off[0];
+  z.y = z.y + f.mb_off[1];
+  z.z = z.z + f.mb_off[2];
+  z.w = z.w + 0.0;
+  if (r2 < f.mb_mR2) {
+    z.x = z.x * f.mb_factor1; z.y = z.y * f.mb_factor1; z.z = z.z * f.mb_factor1; z.w = z.w * f.mb_factor1;
+    DE = DE * f.mb_factor1;
+  } else if (r2 < f.mb_fR2) {
+    const S tglad_factor2 = f.mb_fR2 / r2;
+    z.x = z.x * tglad_factor2; z.y = z.y * tglad_factor2; z.z = z.z * tglad_factor2; z.w = z.w * tglad_factor2;
+    DE = DE * tglad_factor2;
+  }
+  z.x = z.x - f.mb_off[0];
+  z.y = z.y - f.mb_off[1];
+  z.z = z.z - f.mb_off[2];
+  z.w = z.w - 0.0;
+  z.x = z.x * f.mb_scale; z.y = z.y * f.mb_scale; z.z = z.z * f.mb_scale; z.w = z.w * f.mb_scale;
+  DE = DE * fabs(f.mb_scale) + 1.0;
+}
+
+// cFractalMengerSponge::FormulaCode (fractal_menger_sponge.cpp:30-71)
+template <class S>
+inline void formula_menger(V4<S> &z, const SlotT<S> &f, S &DE) {
+  z.x = fabs(z.x); z.y = fabs(z.y); z.z = fabs(z.z); z.w = fabs(z.w);
+  S temp;
+  if (z.x < z.y) { temp = z.y; z.y = z.x; z.x = temp; }
+  if (z.x < z.z) { temp = z.z; z.z = z.x; z.x = temp; }
+  if (z.y < z.z) { temp = z.z; z.z = z.y; z.y = temp; }
+  z.x = z.x * f.scale3; z.y = z.y * f.scale3; z.z = z.z * f.scale3; z.w = z.w * f.scale3;
+  z.x = z.x - 2.0;
+  z.y = z.y - 2.0;
+  if (z.z > 1.0) z.z = z.z - 2.0;
+  DE = DE * f.scale3;
+}
+
+// SmoothCVector (common_math.cpp:133-163)
+template <class S>
+inline V4<S> smooth4(const V4<S> &v1, const V4<S> &v2, double k) {
+  if (k <= 0.0) return v1;
+  if (k >= 1.0) return v2;
+  const double nk = 1.0 - k;
+  S l1 = len4(v1), l2 = len4(v2);
+  S lenInterp = l1 * nk + l2 * k;
+  V4<S> t{v1.x * nk + v2.x * k, v1.y * nk + v2.y * k, v1.z * nk + v2.z * k, v1.w * nk + v2.w * k};
+  S lt = len4(t);
+  if (lt > 0.0) return V4<S>{t.x / lt * lenInterp, t.y / lt * lenInterp, t.z / lt * lenInterp, t.w / lt * lenInterp};
+  return v1;
+}
+
+template <class S>
+struct FractalOut {
+  S distance;
+  int iters;
+  bool maxiter;
+};
+
+// Compute<calcModeNormal> (compute_fractal.cpp:67-654), without global
+// foldings (sCommonParams::foldings disabled) and colouring modes.
+template <class S>
+FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, int maxiterMultiplier,
+                      int forcedMaxiter) {
+  FractalOut<S> out;
+  V4<S> z{px, py, pz, S(0.0)};
+  z.w = S(seq.w0);
+  out.maxiter = true;
+  const V4<S> const_c = z;
+  S r = len4(z);
+  S DE = 1.0;
+  V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ;
+  int maxN = seq.formula_maxiter * maxiterMultiplier;
+  if (forcedMaxiter >= 0) maxN = forcedMaxiter;
+  int i;
+  for (i = 0; i < maxN; i++) {
+    lastGoodZ = lastZ;
+    lastZ = z;
+    const int sequence = (i < seq.length) ? seq.seq[i] : seq.seq[0];  // GetSequence
+    const Slot &sd = seq.slot[sequence];
+    const SlotT<S> &f = slots[sequence];
+    const V4<S> tempZ = z;
+    const S tempAuxDE = DE;
+    if (sd.weight > 0.0) {
+      switch (sd.formula) {
+        case MBR_FORMULA_MANDELBULB: formula_mandelbulb(z, f, r, DE); break;
+        case MBR_FORMULA_MANDELBOX: formula_mandelbox(z, f, DE); break;
+        case MBR_FORMULA_MENGER_SPONGE: formula_menger(z, f, DE); break;
+        default: {  // :228-238
+          out.distance = 10.0;
+          out.iters = 1;
+          out.maxiter = true;
+          return out;
+        }
+      }
+    }
+    if (sd.add_c) {  // :246-281
+      if (seq.julia) {
+        z.x = z.x + seq.julia_c[0] * seq.cmul[0];
+        z.y = z.y + seq.julia_c[1] * seq.cmul[1];
+        z.z = z.z + seq.julia_c[2] * seq.cmul[2];
+        z.w = z.w + 0.0;
+      } else {
+        z.x = z.x + const_c.x * seq.cmul[0];
+        z.y = z.y + const_c.y * seq.cmul[1];
+        z.z = z.z + const_c.z * seq.cmul[2];
+        z.w = z.w + const_c.w;
+      }
+    }
+    if (seq.is_hybrid) {  // :287-297
+      const double k = sd.weight;
+      if (k < 1.0) {
+        z = smooth4(tempZ, z, k);
+        const double kn = 1.0 - k;
+        DE = DE * k + tempAuxDE * kn;
+      }
+    }
+    r = len4(z);
+    if (nan4(z)) {  // :303-309
+      z = lastZ;
+      r = len4(z);
+      out.maxiter = true;
+      break;
+    }
+    if (sd.check_bailout) {  // :312-321
+      if (r > sd.bailout) {
+        out.maxiter = false;
+        break;
+      }
+    }
+    if (nan4(z)) {  // :487-491
+      z = lastGoodZ;
+      break;
+    }
+  }
+  // final DE :495-621
+  if (DE > 0.0) {
+    if (seq.is_hybrid) {
+      if (seq.de_function == 1)
+        out.distance = (r - seq.linear_de_offset) / DE;
+      else
+        out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0);
+    } else {
+      switch (seq.de_analytic) {
+        case 2: out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0); break;
+        case 1: out.distance = r / DE; break;
+        case 3: out.distance = (r - 2.0) / DE; break;
+        default: out.distance = r; break;
+      }
+    }
+  } else {
+    out.distance = r;
+  }
+  out.iters = i + 1;
+  return out;
+}
+
+// CalculateDistanceSimple, analytic branch (calculate_distance.cpp:533-606),
+// reached through CalculateDistanceFromObjectsTree (:225-516) for the single
+// identity-transform node (pointLocal == point, distance *= 1).
+template <class S>
+S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
+                int *iters_out) {
+  const int mult = (normalMode && seq.iter_thresh) ? 5 : 1;
+  FractalOut<S> fo = compute<S>(seq, slots, px, py, pz, mult, -1);
+  S distance = fo.distance;
+  bool maxiter = fo.maxiter;
+  if (iters_out) *iters_out = fo.iters;
+  if (!seq.iter_thresh) maxiter = false;
+  if (normalMode) maxiter = false;
+  if (maxiter) distance = 0.0;
+  if (fo.iters < seq.min_n && distance < detailSize) distance = detailSize;
+  if (seq.interior && !normalMode) {
+    if (distance < 0.5 * detailSize || fo.maxiter) distance = detailSize;
+  } else if (seq.interior && normalMode) {
+    if (distance < 0.9 * detailSize) distance = detailSize - distance;
+  }
+  if (seq.iter_thresh && !normalMode && !fo.maxiter) {
+    if (distance < detailSize) distance = detailSize * 1.01;
+  }
+  if (distance < 0.0) distance = 0.0;
+  if (distance > 10.0) distance = 10.0;
+  return distance;
+}
+
+// ============================================================================
+// Camera: cCameraTarget::SetCameraTargetTop (camera_target.cpp:86-130) and
+// cRenderWorker::PrepareMainVectors (render_worker.cpp:539-564).
+// ============================================================================
+struct D3 {
+  double x, y, z;
+};
+static inline D3 add(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline D3 sub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline D3 mul(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline double length(D3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static inline D3 cross(D3 a, D3 v) {  // algebra.hpp:188-195
+  return {a.y * v.z - a.z * v.y, -a.x * v.z + a.z * v.x, a.x * v.y - a.y * v.x};
+}
+static inline D3 normalize(D3 a) {  // algebra.hpp:204-211
+  const double n = 1.0 / length(a);
+  return {a.x * n, a.y * n, a.z * n};
+}
+static D3 rotate_around(D3 v, D3 axis, double angle) {  // algebra.cpp:70-76
+  D3 r = mul(v, cos(angle));
+  r = add(r, mul(cross(axis, v), sin(angle)));
+  r = add(r, mul(mul(axis, dot(axis, v)), 1 - cos(angle)));
+  return r;
+}
+static double correct_angle(double a) { return fmod(a + 3 * M_PI, 2 * M_PI) - M_PI; }  // camera_target.hpp:62
+
+struct Mat3 {
+  double m[9];  // row-major m11 m12 m13 / m21 ...
+  bool zero;
+};
+static void mat_mul(const double *a, const double *b, double *r) {  // algebra.cpp:152-166
+  double t[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      t[i * 3 + j] = a[i * 3 + 0] * b[0 * 3 + j] + a[i * 3 + 1] * b[1 * 3 + j] + a[i * 3 + 2] * b[2 * 3 + j];
+  std::memcpy(r, t, sizeof(t));
+}
+static void rot_axis(Mat3 &M, int axis, double angle) {  // algebra.cpp:198-247
+  if (angle == 0.0) return;
+  double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double s = sin(angle), c = cos(angle);
+  if (axis == 0) { r[0] = 1.0; r[4] = c; r[8] = c; r[5] = -s; r[7] = s; }
+  if (axis == 1) { r[4] = 1.0; r[8] = c; r[0] = c; r[6] = -s; r[2] = s; }
+  if (axis == 2) { r[8] = 1.0; r[0] = c; r[4] = c; r[1] = -s; r[3] = s; }
+  mat_mul(M.m, r, M.m);
+  M.zero = false;
+}
+static D3 rotate(const Mat3 &M, D3 v) {  // algebra.cpp:320-331, :168-175
+  if (M.zero) return v;
+  const double *m = M.m;
+  return {m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+          m[6] * v.x + m[7] * v.y + m[8] * v.z};
+}
+
+static void camera_setup(const mbr_camera &cam, Mat3 *M, double angles[3]) {
+  double yaw, pitch, roll;
+  if (cam.use_angles) {
+    yaw = cam.angles[0];
+    pitch = cam.angles[1];
+    roll = cam.angles[2];
+  } else {
+    const D3 c{cam.camera[0], cam.camera[1], cam.camera[2]};
+    const D3 t{cam.target[0], cam.target[1], cam.target[2]};
+    D3 fwd = (c.x == t.x && c.y == t.y && c.z == t.z) ? D3{0.0, 1.0, 0.0} : sub(t, c);
+    fwd = normalize(fwd);
+    yaw = atan2(fwd.y, fwd.x) - 0.5 * M_PI;                       // GetAlpha
+    pitch = atan2(fwd.z, sqrt(fwd.x * fwd.x + fwd.y * fwd.y));   // GetBeta
+    D3 top = normalize(D3{cam.top[0], cam.top[1], cam.top[2]});
+    top = rotate_around(top, D3{0.0, 0.0, 1.0}, -yaw);
+    top = rotate_around(top, D3{1.0, 0.0, 0.0}, -pitch);
+    roll = -atan2(top.z, top.x) + 0.5 * M_PI;
+    yaw = correct_angle(yaw);
+    pitch = correct_angle(pitch);
+    roll = correct_angle(roll);
+  }
+  Mat3 m;
+  for (int i = 0; i < 9; i++) m.m[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  m.zero = true;
+  rot_axis(m, 2, yaw);
+  rot_axis(m, 0, pitch);
+  rot_axis(m, 1, roll);
+  *M = m;
+  angles[0] = yaw;
+  angles[1] = pitch;
+  angles[2] = roll;
+}
+
+// ============================================================================
+// Random streams.
+// ============================================================================
+// Park-Miller without divisions (common_math.cpp:47-72), one state per ray.
+struct ParkMiller {
+  unsigned int s;
+  int next() {
+    unsigned int lo = 16807 * (s & 0xFFFF);
+    unsigned int hi = 16807 * (s >> 16);
+    lo += (hi & 0x7FFF) << 16;
+    hi >>= 15;
+    lo += hi;
+    if (lo > 2147483647) lo -= 2147483647;
+    return int(s = lo);
+  }
+  int random(int max) { return next() % (max + 1); }
+};
+// Per-ray seeding: a multiplicative hash of (ray, seed) into [1, 2^31-2],
+// then ten warm-up draws (the OpenCL engine warms its per-pixel seed the same
+// way, full_engine.cl:58-64).
+static ParkMiller pm_for_ray(uint64_t ray, uint32_t seed) {
+  uint64_t h = (ray + 1) * 0x9E3779B97F4A7C15ull ^ (uint64_t(seed) * 0xC2B2AE3D27D4EB4Full);
+  h ^= h >> 29;
+  ParkMiller pm;
+  pm.s = uint32_t(h % 2147483646ull) + 1u;
+  for (int i = 0; i < 10; i++) pm.next();
+  return pm;
+}
+
+// PCG32 (O'Neill 2014, pcg32_srandom_r / pcg32_random_r; XSH-RR output).
+struct Pcg32 {
+  uint64_t state, inc;
+  uint32_t next() {
+    uint64_t old = state;
+    state = old * 6364136223846793005ull + inc;
+    uint32_t xorshifted = uint32_t(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = uint32_t(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((-rot) & 31));
+  }
+  double uniform() { return double(next() >> 8) * (1.0 / 16777216.0); }  // [0,1), 24 bits
+};
+static Pcg32 pcg_init(uint64_t initstate, uint64_t initseq) {
+  Pcg32 p;
+  p.state = 0u;
+  p.inc = (initseq << 1u) | 1u;
+  p.next();
+  p.state += initstate;
+  p.next();
+  return p;
+}
+
+// Cosine-weighted direction about n (Malley's method), orthonormal basis by
+// Duff et al., "Building an Orthonormal Basis, Revisited" (JCGT 2017).
+static D3 cosine_dir(D3 n, double u1, double u2) {
+  const double r = sqrt(u1);
+  const double phi = 2.0 * M_PI * u2;
+  const double lx = r * cos(phi), ly = r * sin(phi);
+  const double lz = sqrt(std::max(0.0, 1.0 - u1));
+  const double sign = n.z >= 0.0 ? 1.0 : -1.0;
+  const double a = -1.0 / (sign + n.z);
+  const double b = n.x * n.y * a;
+  const D3 t{1.0 + sign * n.x * n.x * a, sign * b, -sign * n.x};
+  const D3 bb{b, sign + n.y * n.y * a, -n.y};
+  return {t.x * lx + bb.x * ly + n.x * lz, t.y * lx + bb.y * ly + n.y * lz, t.z * lx + bb.z * ly + n.z * lz};
+}
+
+// ============================================================================
+// Render state shared by the pixel pipeline.
+// ============================================================================
+struct Counters {
+  uint64_t de = 0, iters = 0, march = 0, binary = 0, normal = 0, shadow = 0, ao = 0, gi = 0, pixels = 0, watchdog = 0;
+};
+
+struct Renderer {
+  Seq seq;
+  std::vector<SlotT<double>> slots;
+  mbr_render_params p;
+  mbr_camera cam;
+  Mat3 M;
+  D3 camera;
+  double fov, resolution, aspect;
+  D3 light;
+  std::vector<int> gamma;
+  bool want_normal = false;
+
+  double de(D3 q, double detail, bool normalMode, int *iters, Counters &c) const {
+    int it = 0;
+    double d = calc_distance<double>(seq, slots.data(), q.x, q.y, q.z, detail, normalMode, &it);
+    c.de++;
+    c.iters += it;
+    if (iters) *iters = it;
+    return d;
+  }
+  // CalcDistThresh (render_worker.cpp:653-679), reduceDetail = 1
+  double dist_thresh(D3 q) const {
+    if (seq.iter_thresh) return length(sub(camera, q)) * resolution * fov;
+    if (p.constant_de_threshold) return p.de_thresh;
+    return length(sub(camera, q)) * resolution * fov / p.detail_level;
+  }
+  double calc_delta(D3 q) const { return length(sub(camera, q)) * resolution * fov; }  // :684-690
+
+  struct March {
+    bool found = false;
+    double depth = 0, dist = 0, thr = 0;
+    D3 point{0, 0, 0};
+    int iters = 0;
+    double prev_scan = 0;
+  };
+
+  // RayMarching (render_worker.cpp:708-951), minScan = 0, invertMode off.
+  March ray_marching(D3 start, D3 dir, double maxScan, ParkMiller &pm, Counters &c) const {
+    March o;
+    D3 point{1e30, 1e30, 1e30};
+    bool found = false, dead = false;
+    double scan = 0.0, dist = 0.0, step = 0.0, distThresh = 0.0, prevScan = 0.0;
+    const double search_accuracy = 0.001 * p.detail_level;
+    const double search_limit = 1.0 - search_accuracy;
+    int iters = 0;
+    const double dirLen = length(dir);
+    for (int i = 0; i < p.max_raymarching_steps; i++) {
+      D3 lastPoint = point;
+      point = add(start, mul(dir, scan));
+      if ((point.x == lastPoint.x && point.y == lastPoint.y && point.z == lastPoint.z) ||
+          !(isfinite(point.x) && isfinite(point.y) && isfinite(point.z))) {
+        found = true;
+        dead = true;
+        break;
+      }
+      distThresh = dist_thresh(point);
+      dist = de(point, distThresh, false, &iters, c);
+      c.march++;
+      if (dist < distThresh) {
+        found = true;
+        break;
+      }
+      const double jit = p.jitter ? (1.0 - pm.random(1000) / 10000.0) : 1.0;
+      if (seq.interior)
+        step = (dist - 0.8 * distThresh) * p.de_factor * jit;
+      else
+        step = (dist - 0.5 * distThresh) * p.de_factor * jit;
+      if (step > 3.0) step = 3.0;
+      prevScan = scan;
+      scan += step / dirLen;
+      if (scan > maxScan) break;
+    }
+    point = add(start, mul(dir, scan));
+    if (found && !dead) {
+      if (p.refine == MBR_REFINE_ROOT) {
+        // Bisection of F(t) = dist - thr on [previous scan, hit scan].
+        double lo = prevScan, hi = scan;
+        if (hi > lo) {
+          for (int i = 0; i < p.binary_steps; i++) {
+            const double mid = 0.5 * (lo + hi);
+            if (mid <= lo || mid >= hi) break;
+            const D3 q = add(start, mul(dir, mid));
+            const double thr = dist_thresh(q);
+            const double d = de(q, thr, false, &iters, c);
+            c.binary++;
+            if (d < thr) hi = mid; else lo = mid;
+          }
+          scan = hi;
+          point = add(start, mul(dir, scan));
+          distThresh = dist_thresh(point);
+          dist = de(point, distThresh, false, &iters, c);
+          c.binary++;
+        }
+      } else {
+        step *= 0.5;
+        for (int i = 0; i < p.binary_steps; i++) {
+          if (dist < distThresh && dist > distThresh * search_limit) break;
+          if (dist > distThresh) {
+            scan += step;
+            point = add(start, mul(dir, scan));
+          } else if (dist < distThresh * search_limit) {
+            scan -= step;
+            point = add(start, mul(dir, scan));
+          }
+          distThresh = dist_thresh(point);
+          dist = de(point, distThresh, false, &iters, c);
+          c.binary++;
+          step *= 0.5;
+        }
+      }
+    }
+    if (seq.iter_thresh) {  // :917-939
+      scan -= distThresh;
+      point = add(start, mul(dir, scan));
+      if (found) {
+        dist = de(point, distThresh, false, &iters, c);
+        c.binary++;
+      }
+    }
+    o.found = found;
+    o.dist = dist;
+    o.depth = scan;
+    o.thr = distThresh;
+    o.point = point;
+    o.iters = iters;
+    o.prev_scan = prevScan;
+    return o;
+  }
+
+  // CalculateNormals fast path (shader_calculate_normals.cpp:40-125)
+  D3 normals(D3 q, double thr, Counters &c, uint64_t *counter) const {
+    double delta = thr * p.smoothness;
+    if (seq.interior) delta = thr * 0.2 * p.smoothness;
+    const uint64_t before = c.de;
+    const double sx1 = de(add(q, D3{delta, 0.0, 0.0}), thr, true, nullptr, c);
+    const double sx2 = de(sub(q, D3{delta, 0.0, 0.0}), thr, true, nullptr, c);
+    const double sy1 = de(add(q, D3{0.0, delta, 0.0}), thr, true, nullptr, c);
+    const double sy2 = de(sub(q, D3{0.0, delta, 0.0}), thr, true, nullptr, c);
+    const double sz1 = de(add(q, D3{0.0, 0.0, delta}), thr, true, nullptr, c);
+    const double sz2 = de(sub(q, D3{0.0, 0.0, delta}), thr, true, nullptr, c);
+    *counter += c.de - before;
+    D3 n{sx1 - sx2, sy1 - sy2, sz1 - sz2};
+    if (fabs(n.x) < 1e-50 && fabs(n.y) < 1e-50 && fabs(n.z) < 1e-50)
+      n = D3{1.0, 0.0, 0.0};
+    else
+      n = normalize(n);
+    if (!(isfinite(n.x) && isfinite(n.y) && isfinite(n.z))) n = D3{1.0, 0.0, 0.0};
+    return n;
+  }
+
+  // AuxShadow, hard shadow of a non-penetrating directional light
+  // (shader_aux_shadow.cpp:39-323 with softShadowCone = 0, no fog/clouds/SSS;
+  //  distance = viewDistanceMax, light.cpp:281-291).
+  double aux_shadow(D3 q, double thr, D3 L, Counters &c, uint64_t *counter) const {
+    const double distance = p.view_distance_max;
+    double start = thr;
+    if (seq.interior) start = thr * p.de_factor;
+    double shadowTemp = 1.0;
+    int count = 0;
+    double step = thr;
+    const float dist_thresh = float(thr);
+    const uint64_t before = c.de;
+    for (double i = start; i < distance; i += step) {
+      const D3 point2 = add(q, mul(L, i));
+      const double dist = de(point2, thr, false, nullptr, c);
+      shadowTemp = 1.0 - 0.0;
+      if (dist < dist_thresh || shadowTemp < 0.0) {
+        shadowTemp = 0.0;
+        break;
+      }
+      step = std::min(dist, double(1e6f)) * p.de_factor;
+      step = std::max(step, 1e-15);
+      count++;
+      if (count > p.max_raymarching_steps) break;
+    }
+    *counter += c.de - before;
+    return shadowTemp;
+  }
+
+  // AmbientOcclusion march rule (shader_ambient_occlusion.cpp:41-120) along
+  // ao_rays cosine-hemisphere directions from PCG32(state ao_seed, stream pixel).
+  double ambient_occlusion(D3 q, D3 n, double thr, uint64_t pixel, Counters &c, uint64_t *counter) const {
+    const double start_dist = thr;
+    const double end_dist = calc_delta(q) / resolution;
+    const float dist_thresh = float(thr);
+    Pcg32 rng = pcg_init(p.ao_seed, pixel);
+    double sum = 0.0;
+    const uint64_t before = c.de;
+    for (int k = 0; k < p.ao_rays; k++) {
+      const double u1 = rng.uniform(), u2 = rng.uniform();
+      const D3 v = cosine_dir(n, u1, u2);
+      double dist = 0.0;
+      double shadowTemp = 1.0;
+      int steps = 0;  // cap: max_raymarching_steps evaluations per AO march
+      for (double r = start_dist; r < end_dist; r += dist * 2.0) {
+        if (steps >= p.max_raymarching_steps) {
+          c.watchdog++;
+          break;
+        }
+        steps++;
+        const D3 point2 = add(q, mul(v, r));
+        dist = de(point2, thr, false, nullptr, c);
+        if (dist < dist_thresh || shadowTemp < 0.0) {
+          shadowTemp -= (end_dist - r) / end_dist;
+          if (shadowTemp < 0.0) shadowTemp = 0.0;
+          break;
+        }
+      }
+      sum += shadowTemp;
+    }
+    *counter += c.de - before;
+    return sum / p.ao_rays;
+  }
+
+  // Image point and view direction of pixel (x, y): doWork (render_worker.cpp:155-163,
+  // 247, 326-327), region.hpp:66-71 with imageRegion (-0.5, 0.5, 0.5, -0.5),
+  // CalculateViewVector three-point (projection_3d.cpp:77-84, 87).
+  void image_point(double x, double y, double *ix, double *iy) const {
+    const double scaleX = 1.0 / double(cam.width);
+    const double scaleY = -1.0 / double(cam.height);
+    *ix = (scaleX * x + -0.5) * aspect;
+    *iy = scaleY * y + 0.5;
+  }
+  D3 view_vector(double ix, double iy) const {
+    D3 v{ix * fov, 1.0, iy * fov};
+    v = normalize(v);
+    return rotate(M, v);
+  }
+
+  struct PixelOut {
+    bool hit;
+    double depth;
+    int iters;
+    float normal[3];
+    float shade, ao, rgb[3];
+  };
+
+  void shade_pixel(const March &m, uint64_t pixel, Counters &c, PixelOut &po) const {
+    po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
+    po.shade = 0.0f;
+    po.ao = 1.0f;
+    if (!m.found) {
+      for (int k = 0; k < 3; k++) po.rgb[k] = float(p.background[k]);
+      return;
+    }
+    const bool need_normal = p.shading_enable || p.ao_rays > 0 || want_normal;
+    D3 n{1.0, 0.0, 0.0};
+    if (need_normal) {
+      n = normals(m.point, m.thr, c, &c.normal);
+      po.normal[0] = float(n.x);
+      po.normal[1] = float(n.y);
+      po.normal[2] = float(n.z);
+    }
+    float shade = 0.0f;
+    if (p.shading_enable) {  // LightShading (shader_light_shading.cpp:40-122), directional
+      const float intensity = float(p.light_intensity);
+      float s = float(dot(n, light));
+      if (s < 0) s = 0;
+      const float mshade = float(p.material_shading);
+      s = 1.0f - mshade + s * mshade;
+      s = s * intensity;
+      if (s > 500.0f) s = 500.0f;
+      float aux = 1.0f;
+      if (p.shadow_enable) {
+        if (s > 0.001f)
+          aux = float(aux_shadow(m.point, m.thr, light, c, &c.shadow));
+        else
+          aux = 0.0f;
+      }
+      shade = s * aux;
+    }
+    float ao = 1.0f;
+    if (p.ao_rays > 0) ao = float(ambient_occlusion(m.point, n, m.thr, pixel, c, &c.ao));
+    po.shade = shade;
+    po.ao = ao;
+    const float col = float(p.albedo) * (shade + float(p.ambient_intensity) * ao);
+    po.rgb[0] = po.rgb[1] = po.rgb[2] = col;
+  }
+
+  // One path of the Monte Carlo GI estimator: primary ray with MC pixel
+  // jitter (render_worker.cpp:228-232) and thin-lens DOF (MonteCarloDOF,
+  // :1832-1844), then diffuse bounces with the GI march rule
+  // (shader_global_illumination.cpp:75-125): scan from distThresh, step
+  // dist*DEFactor, a hit closer than 2*distThresh ends the path.
+  double gi_path(int x, int y, uint64_t pixel, int sample, Counters &c, March *first) const {
+    const uint64_t ray = pixel * uint64_t(p.gi_samples) + uint64_t(sample);
+    Pcg32 rng = pcg_init(p.gi_seed, ray);
+    const double ujx = rng.uniform(), ujy = rng.uniform(), ulr = rng.uniform(), ula = rng.uniform();
+    double ix, iy;
+    image_point(double(x), double(y), &ix, &iy);
+    ix = ix + (ujx - 0.5) / double(cam.width) * aspect;
+    iy = iy + (ujy - 0.5) / double(cam.height);
+    D3 view = view_vector(ix, iy);
+    D3 start = camera;
+    if (p.dof_aperture > 0.0) {
+      const double randR = p.dof_aperture * sqrt(ulr);
+      const double randAngle = 2.0 * M_PI * ula;
+      const D3 rv = rotate(M, D3{randR * sin(randAngle), 0.0, randR * cos(randAngle)});
+      view = sub(view, mul(rv, 1.0 / p.dof_focus));
+      start = add(camera, rv);
+    }
+    const D3 dir = normalize(view);
+    ParkMiller pm = pm_for_ray(ray, p.seed);
+    March m = ray_marching(start, dir, p.view_distance_max, pm, c);
+    if (first) *first = m;
+    // every DE evaluation after the primary march counts as a GI evaluation
+    const uint64_t after_primary = c.de;
+    uint64_t unused = 0;
+    double radiance = 0.0, throughput = 1.0;
+    if (!m.found) {
+      radiance = p.gi_sky;
+    } else {
+      D3 q = m.point;
+      double thr = m.thr;
+      D3 n = normals(q, thr, c, &unused);
+      for (int bounce = 0;; bounce++) {
+        const double ndl = dot(n, light);
+        if (ndl > 0.0) {
+          const double sh = aux_shadow(q, thr, light, c, &unused);
+          radiance += throughput * p.albedo * p.gi_sun * ndl * sh;
+        }
+        if (bounce >= p.gi_bounces) break;
+        throughput *= p.albedo;
+        const double u1 = rng.uniform(), u2 = rng.uniform();
+        const D3 d = cosine_dir(n, u1, u2);
+        bool found = false, ended = false;
+        int steps = 0;
+        double dist = 0.0;
+        for (double scan = thr; scan < p.view_distance_max; scan += dist * p.de_factor) {
+          if (steps >= p.max_raymarching_steps) break;
+          const D3 point = add(q, mul(d, scan));
+          const double t2 = dist_thresh(point);
+          dist = de(point, t2, false, nullptr, c);
+          if (dist < t2) {
+            if (scan < t2 * 2.0) {
+              ended = true;
+              break;
+            }
+            q = point;
+            thr = t2;
+            n = normals(q, thr, c, &unused);
+            found = true;
+            break;
+          }
+          steps++;
+        }
+        if (ended) break;
+        if (!found) {
+          radiance += throughput * p.gi_sky;
+          break;
+        }
+      }
+    }
+    c.gi += c.de - after_primary;
+    return radiance;
+  }
+};
+
+// cImage::CalculateGammaTable (cimage.cpp:366-375)
+static std::vector<int> gamma_table(double gamma) {
+  std::vector<int> t(65536);
+  for (int i = 0; i < 65536; i++) t[i] = int(powf(i / 65536.0f, 1.0f / float(gamma)) * 65535.0f);
+  return t;
+}
+
+// cImage::CalculatePixel (cimage.cpp:317-362) + ConvertTo8bitChar (:460-469)
+static void to_rgb8(const float *rgb, const mbr_render_params &p, const std::vector<int> &gamma, uint8_t *o) {
+  const float br = float(p.brightness), co = float(p.contrast), sat = float(p.saturation);
+  float R = rgb[0] * br, G = rgb[1] * br, B = rgb[2] * br;
+  R = (R - 0.5f) * co + 0.5f;
+  G = (G - 0.5f) * co + 0.5f;
+  B = (B - 0.5f) * co + 0.5f;
+  if (R < 0.0f) R = 0.0f;
+  if (G < 0.0f) G = 0.0f;
+  if (B < 0.0f) B = 0.0f;
+  if (p.hdr) {
+    R = tanhf(R);
+    G = tanhf(G);
+    B = tanhf(B);
+  }
+  const float rF = 0.299f, gF = .587f, bF = .114f;
+  const float V = sqrtf(R * R * rF + G * G * gF + B * B * bF);
+  R = V + (R - V) * sat;
+  G = V + (G - V) * sat;
+  B = V + (B - V) * sat;
+  R = std::min(std::max(R, 0.0f), 1.0f);
+  G = std::min(std::max(G, 0.0f), 1.0f);
+  B = std::min(std::max(B, 0.0f), 1.0f);
+  const uint16_t r16 = uint16_t(gamma[uint16_t(R * 65535.0f)]);
+  const uint16_t g16 = uint16_t(gamma[uint16_t(G * 65535.0f)]);
+  const uint16_t b16 = uint16_t(gamma[uint16_t(B * 65535.0f)]);
+  o[0] = uint8_t(r16 / 256);
+  o[1] = uint8_t(g16 / 256);
+  o[2] = uint8_t(b16 / 256);
+}
+
+static bool make_renderer(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
+                          Renderer *R) {
+  if (!build_sequence(*scene, &R->seq)) return false;
+  R->slots.clear();
+  for (int i = 0; i < R->seq.n; i++) R->slots.push_back(make_slot<double>(R->seq.slot[i], false));
+  R->p = *params;
+  R->cam = *cam;
+  double ang[3];
+  camera_setup(*cam, &R->M, ang);
+  R->camera = D3{cam->camera[0], cam->camera[1], cam->camera[2]};
+  R->fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);  // CalcFOV three-point (projection_3d.cpp:145-148)
+  R->resolution = 1.0 / cam->height;                // render_job.cpp:477
+  R->aspect = double(cam->width) / cam->height;     // render_worker.cpp:98
+  R->light = normalize(D3{params->light_direction[0], params->light_direction[1], params->light_direction[2]});
+  R->gamma = gamma_table(params->gamma);
+  return true;
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+// ============================================================================
+// C entry points (called through ctypes by tests/ and bench.py only).
+// ============================================================================
+extern "C" {
+
+typedef struct oracle_outputs {  // host buffers, same meaning as mbr_outputs
+  double *depth;
+  int32_t *iters;
+  uint8_t *hit;
+  float *normal;
+  float *shade;
+  float *ao;
+  float *rgb;
+  uint8_t *rgb8;
+} oracle_outputs;
+
+int oracle_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+// Renders rows [row0, row1) (all columns) of the frame.  Rows are handed to
+// threads one at a time, dynamically (the cScheduler line model,
+// scheduler.cpp:122-183).  Returns 0 on success.
+int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
+                  const oracle_outputs *out, int row0, int row1, int nthreads, mbr_stats *stats) {
+  Renderer R;
+  if (!make_renderer(scene, cam, params, &R)) return 1;
+  R.want_normal = out->normal != nullptr;
+  const int W = cam->width;
+  std::atomic<uint64_t> tot[10];
+  for (auto &t : tot) t = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    Counters c;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+    for (int y = row0; y < row1; y++) {
+      for (int x = 0; x < W; x++) {
+        const uint64_t pixel = uint64_t(y) * W + x;
+        Renderer::PixelOut po;
+        Renderer::March m;
+        if (params->gi_samples > 0) {
+          double acc = 0.0;
+          for (int s = 0; s < params->gi_samples; s++) {
+            Renderer::March mm;
+            acc += R.gi_path(x, y, pixel, s, c, s == 0 ? &m : &mm);
+          }
+          const float v = float(acc / params->gi_samples);
+          po.hit = m.found;
+          po.depth = m.found ? m.depth : 1e20;
+          po.iters = m.iters;
+          po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
+          po.shade = 0.0f;
+          po.ao = 1.0f;
+          po.rgb[0] = po.rgb[1] = po.rgb[2] = v;
+        } else {
+          double ix, iy;
+          R.image_point(double(x), double(y), &ix, &iy);
+          D3 dir = R.view_vector(ix, iy);
+          dir = normalize(dir);
+          ParkMiller pm = pm_for_ray(pixel, params->seed);
+          m = R.ray_marching(R.camera, dir, params->view_distance_max, pm, c);
+          R.shade_pixel(m, pixel, c, po);
+          po.hit = m.found;
+          po.depth = m.found ? m.depth : 1e20;
+          po.iters = m.iters;
+        }
+        c.pixels++;
+        const size_t o = size_t(pixel - uint64_t(row0) * W);
+        if (out->depth) out->depth[o] = po.depth;
+        if (out->iters) out->iters[o] = po.iters;
+        if (out->hit) out->hit[o] = po.hit ? 1 : 0;
+        if (out->normal) for (int k = 0; k < 3; k++) out->normal[o * 3 + k] = po.normal[k];
+        if (out->shade) out->shade[o] = po.shade;
+        if (out->ao) out->ao[o] = po.ao;
+        if (out->rgb) for (int k = 0; k < 3; k++) out->rgb[o * 3 + k] = po.rgb[k];
+        if (out->rgb8) to_rgb8(po.rgb, *params, R.gamma, &out->rgb8[o * 3]);
+      }
+    }
+    tot[0] += c.de; tot[1] += c.iters; tot[2] += c.march; tot[3] += c.binary; tot[4] += c.normal;
+    tot[5] += c.shadow; tot[6] += c.ao; tot[7] += c.gi; tot[8] += c.pixels; tot[9] += c.watchdog;
+  }
+  if (stats) {
+    stats->de_evals += tot[0]; stats->formula_iterations += tot[1]; stats->march_steps += tot[2];
+    stats->binary_steps += tot[3]; stats->normal_evals += tot[4]; stats->shadow_evals += tot[5];
+    stats->ao_evals += tot[6]; stats->gi_evals += tot[7]; stats->pixels += tot[8];
+    stats->watchdog_trips += tot[9];
+  }
+  return 0;
+}
+
+// CalculateDistance at n points (xyz interleaved).
+int oracle_distance(const mbr_scene *scene, const double *pts, int64_t n, double detail, int normal_mode,
+                    double *dist, int32_t *iters) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  std::vector<SlotT<double>> slots;
+  for (int i = 0; i < seq.n; i++) slots.push_back(make_slot<double>(seq.slot[i], false));
+  for (int64_t i = 0; i < n; i++) {
+    int it = 0;
+    dist[i] = calc_distance<double>(seq, slots.data(), pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], detail,
+                                    normal_mode != 0, &it);
+    if (iters) iters[i] = it;
+  }
+  return 0;
+}
+
+// Hybrid sequence of a scene (for cross-checking the library's host builder).
+int oracle_sequence(const mbr_scene *scene, int32_t *seq_out, int32_t *length, int32_t *de_function,
+                    double *bailout) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  for (int i = 0; i < seq.length; i++) seq_out[i] = seq.seq[i];
+  *length = seq.length;
+  *de_function = seq.is_hybrid ? seq.de_function : seq.de_analytic;
+  for (int i = 0; i < seq.n; i++) bailout[i] = seq.slot[i].bailout;
+  return 0;
+}
+
+// One formula iteration of slot `slot` at z (4 doubles in/out) with running
+// derivative *de and radius *r, exactly as Compute calls FormulaCode.
+int oracle_formula_step(const mbr_scene *scene, int slot, double *z, double *r, double *de) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  SlotT<double> f = make_slot<double>(seq.slot[slot], false);
+  V4<double> v{z[0], z[1], z[2], z[3]};
+  switch (seq.slot[slot].formula) {
+    case MBR_FORMULA_MANDELBULB: formula_mandelbulb(v, f, *r, *de); break;
+    case MBR_FORMULA_MANDELBOX: formula_mandelbox(v, f, *de); break;
+    case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, *de); break;
+    default: return 1;
+  }
+  z[0] = v.x; z[1] = v.y; z[2] = v.z; z[3] = v.w;
+  return 0;
+}
+
+// Camera rotation (row-major mRot, zero flag in mrot[9]) and view angles.
+int oracle_camera(const mbr_camera *cam, double *mrot10, double *angles) {
+  Mat3 M;
+  camera_setup(*cam, &M, angles);
+  for (int i = 0; i < 9; i++) mrot10[i] = M.m[i];
+  mrot10[9] = M.zero ? 1.0 : 0.0;
+  return 0;
+}
+
+// View direction (after both normalisations) of pixel (x, y).
+int oracle_view(const mbr_camera *cam, int x, int y, double *dir) {
+  Renderer R;
+  R.cam = *cam;
+  double ang[3];
+  camera_setup(*cam, &R.M, ang);
+  R.fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);
+  R.aspect = double(cam->width) / cam->height;
+  double ix, iy;
+  R.image_point(double(x), double(y), &ix, &iy);
+  D3 d = normalize(R.view_vector(ix, iy));
+  dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+  return 0;
+}
+
+// View direction (after both normalisations) of a normalised image point.
+int oracle_view_ip(const mbr_camera *cam, double ix, double iy, double *dir) {
+  Renderer R;
+  R.cam = *cam;
+  double ang[3];
+  camera_setup(*cam, &R.M, ang);
+  R.fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);
+  D3 d = normalize(R.view_vector(ix, iy));
+  dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+  return 0;
+}
+
+// Park-Miller draws: n values of Random(max) from the reference generator
+// state `seed` (seed = 0 selects the per-ray stream of ray `ray`).
+int oracle_park_miller(uint32_t seed, uint64_t ray, uint32_t ray_seed, int max, int n, int32_t *out) {
+  ParkMiller pm;
+  if (seed != 0) pm.s = seed; else pm = pm_for_ray(ray, ray_seed);
+  for (int i = 0; i < n; i++) out[i] = (max < 0) ? pm.next() : pm.random(max);
+  return 0;
+}
+
+int oracle_pcg32(uint64_t initstate, uint64_t initseq, int n, uint32_t *out) {
+  Pcg32 p = pcg_init(initstate, initseq);
+  for (int i = 0; i < n; i++) out[i] = p.next();
+  return 0;
+}
+
+// Operation counts of one formula iteration of `slot` at z (for the
+// roofline's algorithmic-work figure).  out: add, mul, div, sqrt, transc, cmp.
+int oracle_opcount(const mbr_scene *scene, int slot, const double *z, uint64_t *out) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  SlotT<OpCount> f = make_slot<OpCount>(seq.slot[slot], false);
+  g_tally = OpTally();
+  V4<OpCount> v{OpCount(z[0]), OpCount(z[1]), OpCount(z[2]), OpCount(z[3])};
+  OpCount DE(1.0);
+  OpCount r = len4(v);
+  g_tally = OpTally();
+  switch (seq.slot[slot].formula) {
+    case MBR_FORMULA_MANDELBULB: formula_mandelbulb(v, f, r, DE); break;
+    case MBR_FORMULA_MANDELBOX: formula_mandelbox(v, f, DE); break;
+    case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, DE); break;
+    default: return 1;
+  }
+  // the per-iteration work of Compute around the formula: c-add and |z|
+  if (seq.slot[slot].add_c) {
+    v.x = v.x + OpCount(z[0]) * seq.cmul[0];
+    v.y = v.y + OpCount(z[1]) * seq.cmul[1];
+    v.z = v.z + OpCount(z[2]) * seq.cmul[2];
+    v.w = v.w + OpCount(z[3]);
+  }
+  r = len4(v);
+  (void)(r > 10.0);
+  out[0] = g_tally.add; out[1] = g_tally.mul; out[2] = g_tally.div;
+  out[3] = g_tally.sqrt; out[4] = g_tally.transc; out[5] = g_tally.cmp;
+  return 0;
+}
+
+// Operation counts of whole CalculateDistance evaluations at n points
+// (xyz interleaved): out = add, mul, div, sqrt, transc, cmp, sum of iters, n,
+// essential add, essential mul.
+// The per-iteration algorithmic work of the roofline is (add + mul) / iters.
+int oracle_opcount_de(const mbr_scene *scene, const double *pts, int64_t n, double detail, uint64_t *out) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  std::vector<SlotT<OpCount>> slots;
+  for (int i = 0; i < seq.n; i++) slots.push_back(make_slot<OpCount>(seq.slot[i], false));
+  g_tally = OpTally();
+  uint64_t iters = 0;
+  for (int64_t i = 0; i < n; i++) {
+    int it = 0;
+    calc_distance<OpCount>(seq, slots.data(), OpCount::computed(pts[3 * i]), OpCount::computed(pts[3 * i + 1]),
+                           OpCount::computed(pts[3 * i + 2]),
+                           detail, false, &it);
+    iters += uint64_t(it);
+  }
+  out[0] = g_tally.add; out[1] = g_tally.mul; out[2] = g_tally.div;
+  out[3] = g_tally.sqrt; out[4] = g_tally.transc; out[5] = g_tally.cmp;
+  out[6] = iters; out[7] = uint64_t(n); out[8] = g_tally.e_add; out[9] = g_tally.e_mul;
+  return 0;
+}
+
+// Dual-number reference of the adjoint: for each pixel with hit[i] != 0, the
+// depth derivative dt/dθ (by the implicit function of F(t) = dist - thr at the
+// stored depth) and the derivative of the Lambert term max(N·L, 0) through the
+// six central-difference DE evaluations.  Parameters θ in MBR_GRAD_* order.
+// dt_dtheta / ds_dtheta: [n_pixels * MBR_GRAD_COUNT] (host).
+int oracle_pixel_gradients(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
+                           const double *depth, const uint8_t *hit, double *dt_dtheta, double *ds_dtheta,
+                           float *shade_out) {
+  Renderer R;
+  if (!make_renderer(scene, cam, params, &R)) return 1;
+  if (!cam->use_angles) return 2;
+  typedef Dual<6> DD;  // tangents: power, scale, mR2, x, y, z
+  const Seq &seq = R.seq;
+  std::vector<SlotT<DD>> slots;
+  for (int i = 0; i < seq.n; i++) slots.push_back(make_slot<DD>(seq.slot[i], true));
+  const int W = cam->width, H = cam->height;
+  const double c0 = R.resolution * R.fov / params->detail_level;  // thr = c0 * |cam - p|
+  // d(mRot)/d(yaw): mRot = Rz(yaw) Rx(pitch) Ry(roll)
+  const double yaw = cam->angles[0], pitch = cam->angles[1], roll = cam->angles[2];
+  double Rz_d[9] = {-sin(yaw), -cos(yaw), 0, cos(yaw), -sin(yaw), 0, 0, 0, 0};
+  Mat3 Rx, Ry;
+  for (int i = 0; i < 9; i++) Rx.m[i] = Ry.m[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  Rx.zero = Ry.zero = true;
+  rot_axis(Rx, 0, pitch);
+  rot_axis(Ry, 1, roll);
+  double dM[9];
+  mat_mul(Rz_d, Rx.m, dM);
+  mat_mul(dM, Ry.m, dM);
+  auto eval = [&](D3 q, double thr, bool nm, double *g) -> double {
+    DD x = DD::seed(q.x, TAN_X), y = DD::seed(q.y, TAN_Y), z = DD::seed(q.z, TAN_Z);
+    DD d = calc_distance<DD>(seq, slots.data(), x, y, z, thr, nm, nullptr);
+    for (int k = 0; k < 6; k++) g[k] = d.d[k];
+    return d.v;
+  };
+  for (int py = 0; py < H; py++) {
+    for (int px = 0; px < W; px++) {
+      const size_t i = size_t(py) * W + px;
+      double *dt = dt_dtheta + i * MBR_GRAD_COUNT;
+      double *ds = ds_dtheta + i * MBR_GRAD_COUNT;
+      for (int k = 0; k < MBR_GRAD_COUNT; k++) dt[k] = ds[k] = 0.0;
+      if (shade_out) shade_out[i] = 0.0f;
+      if (!hit[i]) continue;
+      double ix, iy;
+      R.image_point(double(px), double(py), &ix, &iy);
+      const D3 v0 = normalize(D3{ix * R.fov, 1.0, iy * R.fov});
+      const D3 dir = normalize(rotate(R.M, v0));
+      const double t = depth[i];
+      const D3 p = add(R.camera, mul(dir, t));
+      const double thr = R.dist_thresh(p);
+      double g[6];
+      eval(p, thr, false, g);
+      const D3 grad{g[3], g[4], g[5]};
+      // ∂p/∂θ at fixed t, for θ in MBR_GRAD order
+      D3 dp[MBR_GRAD_COUNT];
+      for (int k = 0; k < MBR_GRAD_COUNT; k++) dp[k] = D3{0, 0, 0};
+      dp[MBR_GRAD_CAMERA_X] = D3{1, 0, 0};
+      dp[MBR_GRAD_CAMERA_Y] = D3{0, 1, 0};
+      dp[MBR_GRAD_CAMERA_Z] = D3{0, 0, 1};
+      {  // d(dir)/d(yaw): dir = normalize(M v0); |M v0| = 1 for orthonormal M
+        const D3 w{dM[0] * v0.x + dM[1] * v0.y + dM[2] * v0.z, dM[3] * v0.x + dM[4] * v0.y + dM[5] * v0.z,
+                   dM[6] * v0.x + dM[7] * v0.y + dM[8] * v0.z};
+        dp[MBR_GRAD_YAW] = mul(w, t);
+      }
+      double dd[MBR_GRAD_COUNT] = {0};
+      dd[MBR_GRAD_BULB_POWER] = g[TAN_POWER];
+      dd[MBR_GRAD_MANDELBOX_SCALE] = g[TAN_SCALE];
+      dd[MBR_GRAD_MANDELBOX_MIN_R2] = g[TAN_MR2];
+      const double denom = dot(grad, dir) - c0;
+      for (int k = 0; k < MBR_GRAD_COUNT; k++) dt[k] = -(dd[k] + dot(grad, dp[k])) / denom;
+      // Lambert term through CalculateNormals
+      const double delta = thr * params->smoothness;
+      const D3 e[3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+      double gval[3];
+      double gder[3][MBR_GRAD_COUNT];
+      for (int a = 0; a < 3; a++) {
+        double gp[6], gm[6];
+        const double dpv = eval(add(p, mul(e[a], delta)), thr, true, gp);
+        const double dmv = eval(sub(p, mul(e[a], delta)), thr, true, gm);
+        gval[a] = dpv - dmv;
+        for (int k = 0; k < MBR_GRAD_COUNT; k++) {
+          // total dp/dθ = ∂p/∂θ + dir dt/dθ ; dδ/dθ = c0 * smoothness * dt/dθ (thr = c0 t)
+          const D3 dpt = add(dp[k], mul(dir, dt[k]));
+          const double ddelta = c0 * params->smoothness * dt[k];
+          double dplus = 0.0, dminus = 0.0;
+          if (k <= MBR_GRAD_MANDELBOX_MIN_R2) {
+            dplus += gp[k];
+            dminus += gm[k];
+          }
+          const D3 gpv{gp[3], gp[4], gp[5]}, gmv{gm[3], gm[4], gm[5]};
+          dplus += dot(gpv, add(dpt, mul(e[a], ddelta)));
+          dminus += dot(gmv, sub(dpt, mul(e[a], ddelta)));
+          gder[a][k] = dplus - dminus;
+        }
+      }
+      const double gl = sqrt(gval[0] * gval[0] + gval[1] * gval[1] + gval[2] * gval[2]);
+      const D3 N{gval[0] / gl, gval[1] / gl, gval[2] / gl};
+      const double s = dot(N, R.light);
+      if (shade_out) shade_out[i] = float(s > 0 ? s : 0);
+      if (s > 0.0) {
+        for (int k = 0; k < MBR_GRAD_COUNT; k++) {
+          const D3 dg{gder[0][k], gder[1][k], gder[2][k]};
+          // dN = (I - N N^T) dg / |g|
+          const double ndg = dot(N, dg);
+          const D3 dn = mul(sub(dg, mul(N, ndg)), 1.0 / gl);
+          ds[k] = dot(dn, R.light);
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

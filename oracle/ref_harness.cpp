@@ -1,0 +1,131 @@
+// ref_harness.cpp - C entry points around the REFERENCE's own compiled
+// sources (formula/definition/fractal_{mandelbulb,mandelbox,menger_sponge}.cpp,
+// src/camera_target.cpp, src/projection_3d.cpp, src/common_math.cpp,
+// src/algebra.cpp), built by oracle/build_ref.sh into oracle/_ref/libref.so.
+// Used only by tests/golden/make_golden.py and the CPU tests that pin the
+// oracle against the reference.
+#include <cstring>
+
+#include "formula/definition/all_fractal_definitions.h"
+#include "src/camera_target.hpp"
+#include "src/common_math.h"
+#include "src/fractal.h"
+#include "src/projection_3d.hpp"
+
+// cAbstractFractal's out-of-line members live in abstract_fractal.cpp, which
+// needs Qt; the formulas need only construction and the vtable.
+cAbstractFractal::cAbstractFractal() {}
+cAbstractFractal::~cAbstractFractal() {}
+std::string cAbstractFractal::getIconName() const { return std::string(); }
+std::string cAbstractFractal::getUiFilename() const { return std::string(); }
+std::string cAbstractFractal::getOpenCLFilename() const { return std::string(); }
+
+static sFractal g_fractal;  // zero-initialised static storage; rotations disabled
+
+extern "C" {
+
+// One FormulaCode call.  params: formula-specific doubles
+//   mandelbulb: power, alpha(rad), beta(rad)
+//   mandelbox:  scale, limit, value, minR, fixedR, offset x, y, z
+//   menger:     scale3
+// z: 4 doubles in/out; aux_r, aux_de in/out.  Returns 0 on success.
+int ref_formula_step(int formula, const double *params, double *z, double *aux_r, double *aux_de, int iter) {
+  sFractal &f = g_fractal;
+  sExtendedAux aux;
+  std::memset(&aux, 0, sizeof(aux));
+  aux.r = *aux_r;
+  aux.DE = *aux_de;
+  aux.i = iter;
+  aux.color = 1.0;
+  CVector4 v(z[0], z[1], z[2], z[3]);
+  if (formula == 2) {
+    f.bulb.power = params[0];
+    f.bulb.alphaAngleOffset = params[1];
+    f.bulb.betaAngleOffset = params[2];
+    static cFractalMandelbulb fm;
+    fm.FormulaCode(v, &f, aux);
+  } else if (formula == 8) {
+    f.mandelbox.scale = params[0];
+    f.mandelbox.foldingLimit = params[1];
+    f.mandelbox.foldingValue = params[2];
+    f.mandelbox.foldingSphericalMin = params[3];
+    f.mandelbox.foldingSphericalFixed = params[4];
+    f.mandelbox.offset = CVector4(params[5], params[6], params[7], 0.0);
+    f.mandelbox.rotationsEnabled = false;
+    f.mandelbox.mainRotationEnabled = false;
+    // sFractal::RecalculateFractalParams (fractal.cpp:673-675)
+    f.mandelbox.fR2 = f.mandelbox.foldingSphericalFixed * f.mandelbox.foldingSphericalFixed;
+    f.mandelbox.mR2 = f.mandelbox.foldingSphericalMin * f.mandelbox.foldingSphericalMin;
+    f.mandelbox.mboxFactor1 = f.mandelbox.fR2 / f.mandelbox.mR2;
+    static cFractalMandelbox fb;
+    fb.FormulaCode(v, &f, aux);
+  } else if (formula == 7) {
+    f.transformCommon.scale3 = params[0];
+    f.foldColor.auxColorEnabledFalse = false;
+    static cFractalMengerSponge fs;
+    fs.FormulaCode(v, &f, aux);
+  } else {
+    return 1;
+  }
+  z[0] = v.x;
+  z[1] = v.y;
+  z[2] = v.z;
+  z[3] = v.w;
+  *aux_r = aux.r;
+  *aux_de = aux.DE;
+  return 0;
+}
+
+// cCameraTarget(camera, target, top) + the mRot of PrepareMainVectors.
+// out: yaw, pitch, roll, then mRot row-major (9).
+int ref_camera(const double *cam, const double *target, const double *top, double *out) {
+  cCameraTarget ct(CVector3(cam[0], cam[1], cam[2]), CVector3(target[0], target[1], target[2]),
+                   CVector3(top[0], top[1], top[2]));
+  CVector3 a = ct.GetRotation();
+  CRotationMatrix m;
+  m.RotateZ(a.x);
+  m.RotateX(a.y);
+  m.RotateY(a.z);
+  out[0] = a.x;
+  out[1] = a.y;
+  out[2] = a.z;
+  CVector3 e[3] = {CVector3(1, 0, 0), CVector3(0, 1, 0), CVector3(0, 0, 1)};
+  for (int j = 0; j < 3; j++) {
+    CVector3 c = m.RotateVector(e[j]);
+    out[3 + 0 * 3 + j] = c.x;
+    out[3 + 1 * 3 + j] = c.y;
+    out[3 + 2 * 3 + j] = c.z;
+  }
+  return 0;
+}
+
+// View vector of normalised image point (x, y) through CalculateViewVector
+// (three-point) with the camera's mRot, then normalised as in doWork.
+int ref_view_vector(const double *cam, const double *target, const double *top, double fov_deg, double ix,
+                    double iy, double *out) {
+  cCameraTarget ct(CVector3(cam[0], cam[1], cam[2]), CVector3(target[0], target[1], target[2]),
+                   CVector3(top[0], top[1], top[2]));
+  CVector3 a = ct.GetRotation();
+  CRotationMatrix m;
+  m.RotateZ(a.x);
+  m.RotateX(a.y);
+  m.RotateY(a.z);
+  double fov = CalcFOV(fov_deg, params::perspThreePoint);
+  CVector3 v = CalculateViewVector(CVector2<double>(ix, iy), fov, params::perspThreePoint, m);
+  v.Normalize();
+  out[0] = v.x;
+  out[1] = v.y;
+  out[2] = v.z;
+  return 0;
+}
+
+double ref_calc_fov(double fov_deg) { return CalcFOV(fov_deg, params::perspThreePoint); }
+
+// n draws of Random(max) from gRandomSeed = seed (max < 0: RandomInt()).
+int ref_random(unsigned int seed, int max, int n, int *out) {
+  gRandomSeed = seed;
+  for (int i = 0; i < n; i++) out[i] = (max < 0) ? RandomInt() : Random(max);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+"""Generates the golden vectors of tests/golden/ from the REFERENCE's own
+sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
+
+  formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
+                    Mandelbox, Menger sponge) on seeded random points
+  camera_kat.json   cCameraTarget + PrepareMainVectors rotations and
+                    CalculateViewVector directions
+  random_kat.json   Park-Miller Random()/RandomInt() sequences
+
+Doubles are stored with float.hex() so the comparison is bit-exact.
+Run: python tests/golden/make_golden.py  (needs the reference tree to build libref.so)
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import Reference  # noqa: E402
+
+FORMULAS = [
+    # (name, formula id, params for ref_formula_step, scene fields)
+    ("mandelbulb_p8", 2, [8.0, 0.0, 0.0], {"bulb_power": 8.0}),
+    ("mandelbulb_p3_5", 2, [3.5, 0.0, 0.0], {"bulb_power": 3.5}),
+    ("mandelbulb_p8_angles", 2, [8.0, 10.0 * math.pi / 180.0, -20.0 * math.pi / 180.0],
+     {"bulb_power": 8.0, "bulb_alpha_angle_offset": 10.0, "bulb_beta_angle_offset": -20.0}),
+    ("mandelbox_m1_5", 8, [-1.5, 1.0, 2.0, 0.5, 1.0, 0.0, 0.0, 0.0],
+     {"mandelbox_scale": -1.5, "mandelbox_folding_min_radius": 0.5}),
+    ("mandelbox_2_offset", 8, [2.0, 1.0, 2.0, 0.5, 1.0, 0.1, -0.2, 0.05],
+     {"mandelbox_scale": 2.0, "mandelbox_offset": [0.1, -0.2, 0.05]}),
+    ("mandelbox_m2_2_minr", 8, [-2.2, 0.9, 1.8, 0.35, 1.1, 0.0, 0.0, 0.0],
+     {"mandelbox_scale": -2.2, "mandelbox_folding_limit": 0.9, "mandelbox_folding_value": 1.8,
+      "mandelbox_folding_min_radius": 0.35, "mandelbox_folding_fixed_radius": 1.1}),
+    ("menger_3", 7, [3.0], {"transf_scale3": 3.0}),
+]
+N_POINTS = 32
+N_STEPS = 6
+
+
+def hexs(a):
+    return [float(x).hex() for x in np.asarray(a, dtype=np.float64).ravel()]
+
+
+def formula_kats(ref: Reference) -> dict:
+    rng = np.random.default_rng(20241203)
+    out = {}
+    for name, fid, params, fields in FORMULAS:
+        cases = []
+        for _ in range(N_POINTS):
+            z = np.zeros(4)
+            z[:3] = rng.uniform(-1.5, 1.5, size=3)
+            r = math.sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2] + z[3] * z[3])
+            de = 1.0
+            steps = []
+            for i in range(N_STEPS):
+                zin, rin, dein = z.copy(), r, de
+                z, _, de = ref.formula_step(fid, params, z, r, de, i)
+                steps.append({"z_in": hexs(zin), "r_in": float(rin).hex(), "de_in": float(dein).hex(),
+                              "z_out": hexs(z), "de_out": float(de).hex()})
+                r = math.sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2] + z[3] * z[3])
+                if not math.isfinite(r) or r > 1e6:
+                    break
+            cases.append(steps)
+        out[name] = {"formula": fid, "fields": fields, "cases": cases}
+    return out
+
+
+CAMERAS = [
+    ((0.0, -3.0, 0.0), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0)),
+    ((0.0, -6.0, 0.0), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0)),
+    ((3.0, -6.0, 2.0), (0.0, 0.0, 0.0), (0.0, 0.0, 1.0)),
+    ((-2.1, 1.7, 0.9), (0.3, -0.2, 0.1), (0.0, 0.0, 1.0)),
+    ((1.0, 2.0, 3.0), (0.0, 0.0, 0.0), (0.2, 0.1, 1.0)),
+    ((0.5, -0.5, -3.5), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0)),
+]
+VIEW_POINTS = [(0.0, 0.0), (0.25, -0.1), (-0.4, 0.3), (0.7, 0.45), (-0.888, -0.5)]
+
+
+def camera_kats(ref: Reference) -> list:
+    out = []
+    for cam, tgt, top in CAMERAS:
+        r = ref.camera(cam, tgt, top)
+        views = []
+        for ix, iy in VIEW_POINTS:
+            views.append({"ix": float(ix).hex(), "iy": float(iy).hex(),
+                          "dir": hexs(ref.view_vector(cam, tgt, top, 53.0, ix, iy))})
+        out.append({"camera": cam, "target": tgt, "top": top, "angles": hexs(r[:3]), "mrot": hexs(r[3:]),
+                    "fov53": float(ref.lib.ref_calc_fov(53.0)).hex(), "views": views})
+    return out
+
+
+def random_kats(ref: Reference) -> list:
+    out = []
+    for seed in (1, 12345, 2147483646, 987654321):
+        out.append({"seed": seed, "max": -1, "values": ref.random(seed, 64, -1).tolist()})
+        out.append({"seed": seed, "max": 1000, "values": ref.random(seed, 64, 1000).tolist()})
+    return out
+
+
+def main() -> None:
+    ref = Reference()
+    with open(os.path.join(HERE, "formula_kat.json"), "w") as f:
+        json.dump(formula_kats(ref), f, separators=(",", ":"))
+    with open(os.path.join(HERE, "camera_kat.json"), "w") as f:
+        json.dump(camera_kats(ref), f, indent=1)
+    with open(os.path.join(HERE, "random_kat.json"), "w") as f:
+        json.dump(random_kats(ref), f)
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
