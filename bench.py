@@ -273,6 +273,11 @@ def main() -> None:
     p.seed = rank  # each rank: its own frame (jitter stream)
     r = Renderer(local)
     r.set_scene(sc)
+    tuning = None
+    if "wavefront" in a.engine:
+        t_ = r.autotune(cam, p, engine)  # the library's own autotuner picks the launch shape
+        tuning = {"block_size": t_.block_size, "ctas_per_sm": t_.ctas_per_sm, "refill_k": t_.refill_k,
+                  "queue_layout": t_.queue_layout}
     n = cam.width * cam.height
     names = ("depth", "iters", "hit", "normal", "rgb8")
     bufs = alloc_outputs(n, r.device, names)
@@ -376,7 +381,7 @@ def main() -> None:
             "dtype": "f32" if "fp32" in a.engine or "mixed" in a.engine else "f64",
             "data": "synthetic (procedural fractal scene, no dataset)",
             "config": dict(desc, engine=a.engine, parallelism=f"replicas x{world} (one frame per GPU)",
-                           l2="256 MiB buffer written between timed frames"),
+                           l2="256 MiB buffer written between timed frames", tuning=tuning),
             "mpix_per_s": pix_all / t / 1e6, "formula_iterations_per_s": it_all / t,
             "de_evals_per_frame": st["de_evals"] / a.steps, "stats_per_frame": {k: v / a.steps for k, v in st.items()},
             "fp64_baseline": base, "speedup_vs_fp64": (value / base["value"]) if base else None,

@@ -1,0 +1,193 @@
+// fast_formula.cuh - one formula iteration in FP32, written for the issue
+// slots of the B200 SM: the FMA pipe takes a warp instruction every cycle,
+// the ALU pipe every second cycle and the XU (MUFU) pipe every eighth, so
+// clamps and compares are expressed as saturating FMAs where possible.
+// Used by the wavefront kernels, whose lanes advance their distance
+// estimates a few iterations at a time.
+//
+// Rewrites of the reference formulas (equal in real arithmetic; in FP32 they
+// differ from a literal transcription by a few units in the last place):
+//  * Mandelbox box fold (fractal_mandelbox.cpp:91-105): when folding_value ==
+//    2*folding_limit (the reference default, 1 and 2), sign(z)*value - z for
+//    |z| > limit and z otherwise equals 2*clamp(z, -L, L) - z
+//    = 4L*sat(z/(2L) + 1/2) - 2L - z, with sat() the free [0,1] saturation.
+//  * Mandelbox sphere fold (:109-126): the factor (fR2/mR2 if r2 < mR2,
+//    fR2/r2 if r2 < fR2, else 1) equals clamp(fR2/r2, 1, fR2/mR2) whenever
+//    mR2 <= fR2, i.e. 1 + (F-1)*sat((fR2/r2 - 1)/(F-1)) with F = fR2/mR2; the
+//    scale and the c-addition fold into one FMA per axis.
+//  * Menger sponge sort (fractal_menger_sponge.cpp:34-56): the three
+//    conditional swaps are a sorting network, written with min/max.
+//  * bailout |z| > b is tested as |z|^2 > b^2; |z| is taken once, for the DE.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "mbr_device.h"
+
+namespace mbr {
+
+// FP32 parameters of a non-hybrid formula, as a lane holds them.
+struct FastParams {
+  int formula;     // MBR_FORMULA_*
+  int maxN;        // formula_maxiter
+  int de_fn;       // 1 linear, 2 log, 3 IFS
+  int box_simple;  // mandelbox: folding_value == 2*limit, mR2 < fR2, no offset
+  int add_c;       // slot adds the c constant
+  int julia;       // c is the Julia constant instead of the point
+  int min_n;       // minN
+  float bailout2;
+  float cm_x, cm_y, cm_z;        // fractal_constant_factor
+  float jc_x, jc_y, jc_z;        // julia_c * fractal_constant_factor
+  float p0, p1, p2, p3, p4, p5;  // formula specific (see load_fast_params)
+  float q0, q1, q2, q3, q4;      // derived constants of the simple Mandelbox path
+  float off_x, off_y, off_z;     // mandelbox offset (0 when absent)
+};
+
+// mandelbulb: p0 power, p1 power-1, p2 alpha, p3 beta
+// mandelbox:  p0 scale, p1 |scale|, p2 limit, p3 value, p4 fR2, p5 factor1 (fR2/mR2)
+//             simple path: q0 = 1/(2L), q1 = 4L, q2 = fR2/(F-1), q3 = F-1, q4 = -1/(F-1)
+// menger:     p0 scale3
+__host__ __device__ inline FastParams load_fast_params(const DevScene &sc) {
+  FastParams f;
+  const DevSlot &s = sc.slot[0];
+  f.formula = s.formula;
+  f.maxN = sc.formula_maxiter;
+  f.de_fn = sc.de_analytic;
+  f.bailout2 = s.f[P_BAILOUT] * s.f[P_BAILOUT];
+  f.add_c = s.add_c;
+  f.julia = sc.julia;
+  f.min_n = sc.min_n;
+  f.cm_x = sc.fcmul[0];
+  f.cm_y = sc.fcmul[1];
+  f.cm_z = sc.fcmul[2];
+  f.jc_x = sc.fjulia_c[0];
+  f.jc_y = sc.fjulia_c[1];
+  f.jc_z = sc.fjulia_c[2];
+  f.off_x = f.off_y = f.off_z = 0.0f;
+  f.box_simple = 0;
+  f.p0 = f.p1 = f.p2 = f.p3 = f.p4 = f.p5 = 0.0f;
+  f.q0 = f.q1 = f.q2 = f.q3 = f.q4 = 0.0f;
+  if (s.formula == MBR_FORMULA_MANDELBULB) {
+    f.p0 = s.f[P_POWER];
+    f.p1 = s.f[P_POWER_M1];
+    f.p2 = s.f[P_ALPHA];
+    f.p3 = s.f[P_BETA];
+  } else if (s.formula == MBR_FORMULA_MANDELBOX) {
+    f.p0 = s.f[P_MB_SCALE];
+    f.p1 = s.f[P_MB_ABS_SCALE];
+    f.p2 = s.f[P_MB_LIMIT];
+    f.p3 = s.f[P_MB_VALUE];
+    f.p4 = s.f[P_MB_FR2];
+    f.p5 = s.f[P_MB_FACTOR1];
+    const double L = s.d[P_MB_LIMIT], F = s.d[P_MB_FACTOR1];
+    f.box_simple = (s.d[P_MB_VALUE] == 2.0 * L && L > 0.0 && F > 1.0 && !s.has_offset) ? 1 : 0;
+    if (f.box_simple) {
+      f.q0 = float(1.0 / (2.0 * L));
+      f.q1 = float(4.0 * L);
+      f.q2 = float(s.d[P_MB_FR2] / (F - 1.0));
+      f.q3 = float(F - 1.0);
+      f.q4 = float(-1.0 / (F - 1.0));
+    }
+    if (s.has_offset) {
+      f.off_x = s.f[P_MB_OFF_X];
+      f.off_y = s.f[P_MB_OFF_Y];
+      f.off_z = s.f[P_MB_OFF_Z];
+    }
+  } else {
+    f.p0 = s.f[P_SCALE3];
+  }
+  return f;
+}
+
+struct Z3 {
+  float x, y, z;
+};
+
+// One Mandelbox iteration + c-addition.  c holds the (pre-multiplied) constant.
+template <bool SIMPLE>
+__device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, const FastParams &f) {
+  if (SIMPLE) {
+    const float L2 = 0.5f * f.q1;  // 2L
+    z.x = fmaf(f.q1, __saturatef(fmaf(z.x, f.q0, 0.5f)), -z.x) - L2;
+    z.y = fmaf(f.q1, __saturatef(fmaf(z.y, f.q0, 0.5f)), -z.y) - L2;
+    z.z = fmaf(f.q1, __saturatef(fmaf(z.z, f.q0, 0.5f)), -z.z) - L2;
+    const float r2 = fmaf(z.x, z.x, fmaf(z.y, z.y, z.z * z.z));
+    // factor = 1 + (F-1) * sat((fR2/r2 - 1) / (F-1))
+    const float fs = fmaf(f.q3, __saturatef(fmaf(f.q2, __fdividef(1.0f, r2), f.q4)), 1.0f);
+    const float s = fs * f.p0;
+    dr = fmaf(dr, fs * f.p1, 1.0f);
+    z.x = fmaf(z.x, s, c.x);
+    z.y = fmaf(z.y, s, c.y);
+    z.z = fmaf(z.z, s, c.z);
+  } else {
+    const float L = f.p2, V = f.p3;
+    if (fabsf(z.x) > L) z.x = copysignf(V, z.x) - z.x;
+    if (fabsf(z.y) > L) z.y = copysignf(V, z.y) - z.y;
+    if (fabsf(z.z) > L) z.z = copysignf(V, z.z) - z.z;
+    const float r2 = fmaf(z.x, z.x, fmaf(z.y, z.y, z.z * z.z));
+    z.x += f.off_x;
+    z.y += f.off_y;
+    z.z += f.off_z;
+    const float mR2 = f.p4 / f.p5;
+    float fs = 1.0f;
+    if (r2 < mR2) fs = f.p5;
+    else if (r2 < f.p4) fs = __fdividef(f.p4, r2);
+    z.x = z.x * fs - f.off_x;
+    z.y = z.y * fs - f.off_y;
+    z.z = z.z * fs - f.off_z;
+    dr = fmaf(dr * fs, f.p1, 1.0f);
+    z.x = fmaf(z.x, f.p0, c.x);
+    z.y = fmaf(z.y, f.p0, c.y);
+    z.z = fmaf(z.z, f.p0, c.z);
+  }
+}
+
+// One Mandelbulb iteration (asin latitude form of fractal_mandelbulb.cpp:32-42) + c-addition.
+__device__ __forceinline__ void it_mandelbulb(Z3 &z, float &dr, const Z3 &c, const FastParams &f, float r) {
+  const float th0 = asinf(z.z / r) + f.p3;
+  const float ph0 = atan2f(z.y, z.x) + f.p2;
+  float rp = __powf(r, f.p1);
+  float sth, cth, sph, cph;
+  sincosf(th0 * f.p0, &sth, &cth);
+  sincosf(ph0 * f.p0, &sph, &cph);
+  dr = fmaf(rp * dr, f.p0, 1.0f);
+  rp *= r;
+  z.x = fmaf(cth * cph, rp, c.x);
+  z.y = fmaf(cth * sph, rp, c.y);
+  z.z = fmaf(sth, rp, c.z);
+}
+
+// One Menger sponge iteration; c (zero unless the slot adds it) is added after.
+__device__ __forceinline__ void it_menger(Z3 &z, float &dr, const Z3 &c, const FastParams &f) {
+  const float ax = fabsf(z.x), ay = fabsf(z.y), az = fabsf(z.z);
+  const float a = fmaxf(ax, ay), b = fminf(ax, ay);
+  const float x = fmaxf(a, az), m = fminf(a, az);
+  const float y = fmaxf(b, m), zz = fminf(b, m);
+  const float s = f.p0;
+  z.x = fmaf(x, s, -2.0f);
+  z.y = fmaf(y, s, -2.0f);
+  float t = zz * s;
+  z.z = (t > 1.0f) ? t - 2.0f : t;
+  dr *= s;
+  if (f.add_c) {
+    z.x += c.x;
+    z.y += c.y;
+    z.z += c.z;
+  }
+}
+
+// Final distance of Compute + CalculateDistanceSimple clamps
+// (compute_fractal.cpp:561-621, calculate_distance.cpp:569, 604-605).
+__device__ __forceinline__ float final_de(const FastParams &f, float r2, float dr, int iters, float detail) {
+  const float r = sqrtf(r2);
+  float d;
+  if (!(dr > 0.0f)) d = r;
+  else if (f.de_fn == 2) d = (r > 1.0f) ? __fdividef(0.5f * r * __logf(r), dr) : 0.0f;
+  else if (f.de_fn == 3) d = __fdividef(r - 2.0f, dr);
+  else d = __fdividef(r, dr);
+  if (iters < f.min_n && d < detail) d = detail;
+  if (!(d == d)) d = 0.0f;  // a NaN orbit: treated as on the surface
+  return fminf(fmaxf(d, 0.0f), 10.0f);
+}
+
+}  // namespace mbr

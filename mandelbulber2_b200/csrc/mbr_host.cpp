@@ -59,7 +59,7 @@ struct mbr_ctx {
   uint16_t *d_gamma = nullptr;
   double gamma_value = -1.0;
   int32_t *d_status = nullptr;
-  mbr_tuning tuning{128, 4, 8, 1};
+  mbr_tuning tuning{128, 8, 16, 0};
   // scratch of the wavefront kernel (work counter + per-lane queue cursor)
   unsigned long long *d_work = nullptr;
   size_t work_words = 0;
@@ -689,7 +689,7 @@ mbr_status mbr_distance(mbr_ctx *ctx, const double *points, int64_t n, double de
 
 mbr_status mbr_set_tuning(mbr_ctx *ctx, const mbr_tuning *t) {
   if (!ctx || !t) return MBR_EINVAL;
-  if (t->block_size < 32 || t->block_size > 1024 || t->block_size % 32 || t->ctas_per_sm < 1 ||
+  if (t->block_size < 32 || t->block_size > 256 || t->block_size % 32 || t->ctas_per_sm < 1 ||
       t->ctas_per_sm > 32 || t->refill_k < 0 || t->refill_k > 32 || t->queue_layout < 0 || t->queue_layout > 1)
     return set_err(ctx, MBR_EINVAL, "tuning out of range");
   ctx->tuning = *t;

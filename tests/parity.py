@@ -26,7 +26,7 @@ def compare(gpu: dict, ora: dict) -> dict:
         out["depth_rel_p99"] = float(np.quantile(rel, 0.99))
         out["depth_rel_le_1e-9"] = float((rel <= 1e-9).mean())
         out["depth_rel_le_1e-4"] = float((rel <= 1e-4).mean())
-        if "normal" in gpu and "normal" in ora:
+        if "normal" in gpu and "normal" in ora and np.abs(ora["normal"][both]).sum() > 0:
             ng, no = gpu["normal"][both].astype(np.float64), ora["normal"][both].astype(np.float64)
             cos = np.clip((ng * no).sum(1) / np.maximum(np.linalg.norm(ng, axis=1) * np.linalg.norm(no, axis=1), 1e-30),
                           -1, 1)
