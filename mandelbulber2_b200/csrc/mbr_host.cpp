@@ -59,7 +59,7 @@ struct mbr_ctx {
   uint16_t *d_gamma = nullptr;
   double gamma_value = -1.0;
   int32_t *d_status = nullptr;
-  mbr_tuning tuning{128, 8, 16, 0};
+  mbr_tuning tuning{128, 12, 2, 0};  // fastest on the 1920x1080 Mandelbox of the autotuner grid
   // scratch of the wavefront kernel (work counter + per-lane queue cursor)
   unsigned long long *d_work = nullptr;
   size_t work_words = 0;

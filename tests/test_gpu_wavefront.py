@@ -54,7 +54,7 @@ def test_wavefront_vs_oracle(renderer, oracle, name):
 def test_wavefront_results_independent_of_tuning(renderer):
     sc, cam, p = configs.mandelbox_1080p("A", 160, 90)
     base = None
-    for t in [(128, 8, 16, 0), (64, 8, 0, 1), (256, 2, 24, 1), (128, 16, 4, 0)]:
+    for t in [(128, 12, 2, 0), (64, 8, 0, 1), (256, 2, 24, 1), (128, 16, 4, 0)]:
         renderer.set_tuning(*t)
         g, st = frame(renderer, sc, cam, p)
         if base is None:
@@ -63,7 +63,7 @@ def test_wavefront_results_independent_of_tuning(renderer):
         for k in base:
             assert np.array_equal(base[k], g[k]), (t, k)
         assert st == bst
-    renderer.set_tuning(128, 8, 16, 0)
+    renderer.set_tuning(128, 12, 2, 0)
 
 
 def test_batch_matches_single_renders(renderer):
