@@ -344,6 +344,35 @@ mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_
                        const double *depth, const uint8_t *hit, const float *dl_ddepth,
                        const float *dl_dshade, double *grad, int engine, void *stream);
 
+/* ---- allocation-free rendering ------------------------------------------------- */
+/* Size of the device scratch array that mbr_render_noalloc works in. */
+#define MBR_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+
+/* Renders one frame with the FP32 wavefront engine, like mbr_render with
+ * MBR_ENGINE_WAVEFRONT_FP32, without allocating any device memory and without
+ * a context.  No counterpart in the reference: it is for callers that cannot
+ * allocate device memory - applications whose device memory belongs to their
+ * own allocator or pool, or processes under a hard memory cap where a
+ * cudaMalloc during a frame could fail or synchronise the device.
+ *
+ * All scratch lives in one static device array of MBR_NOALLOC_SCRATCH_BYTES
+ * (64 MiB) that every GPU loading this library holds until the process exits.
+ * A frame needs 128 KiB + 512 B + pixels * (88 + 16 * (1 + tasks)) bytes, with
+ * tasks = ao_rays + 1 when the shadow march runs; larger frames are rejected
+ * with MBR_EINVAL and the limit in `err` (178,131 pixels with a shadow and 16
+ * AO rays, 644,012 with neither).  The caller passes the scene, camera,
+ * parameters and device output buffers as for mbr_render; `err` (may be NULL)
+ * receives a message of at most err_len bytes on failure.
+ *
+ * The first call on a device looks up the array's device address on the
+ * current device (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Every call shares the one array and keeps the previous
+ * call's contents; calls that overlap on the GPU (other streams, other
+ * threads) race on it, so serialise them.  Asynchronous: returns after the
+ * launches are queued on `stream`. */
+mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera, const mbr_render_params *params,
+                              const mbr_outputs *out, void *stream, char *err, size_t err_len);
+
 /* ---- measurement ------------------------------------------------------------ */
 /* FMA throughput of the current device (FLOP/s, an FMA counted as 2), FP32
  * (fp64 = 0) or FP64: the roofline denominator for the DE kernels, which are

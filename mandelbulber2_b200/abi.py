@@ -134,6 +134,8 @@ PROTOTYPES = {
                                C.POINTER(Tuning)]),
     "mbr_adjoint": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), _P, _P, _P, _P, _P, C.c_int, _P]),
     "mbr_fma_peak": (C.c_int, [C.c_int, C.c_int, _P, C.POINTER(C.c_double)]),
+    "mbr_render_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderParams),
+                                     C.POINTER(Outputs), _P, C.c_char_p, C.c_size_t]),
 }
 
 _lib = None

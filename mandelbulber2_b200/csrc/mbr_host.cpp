@@ -429,6 +429,22 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   return MBR_OK;
 }
 
+// Builds a frame exactly as build_frame does, with the gamma table in device
+// memory the caller already owns (`gamma_dev`, 65536 entries): the table is
+// uploaded when *gamma_value differs from params.gamma, and nothing is
+// allocated.  The error text, if any, goes to *err.
+mbr_status build_frame_owned_gamma(const mbr_camera &cam, const mbr_render_params &p, uint16_t *gamma_dev,
+                                   double *gamma_value, DevFrame *out, std::string *err) {
+  mbr_ctx tmp;  // holds no device memory of its own; nothing to release
+  tmp.d_gamma = gamma_dev;
+  tmp.gamma_value = *gamma_value;
+  const mbr_status st = build_frame(&tmp, cam, p, out);
+  *gamma_value = tmp.gamma_value;
+  tmp.d_gamma = nullptr;
+  if (err) *err = tmp.err;
+  return st;
+}
+
 DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o) {
   DevOutputs d;
   d.depth = o.depth;

@@ -1,5 +1,7 @@
 // mbr_internal.h - host-side helpers shared by the library's translation units.
 #pragma once
+#include <string>
+
 #include "../../include/mbr.h"
 #include "mbr_device.h"
 
@@ -12,6 +14,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
 mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam);
 void camera_matrix(const mbr_camera &cam, double mrot[9], bool *zero, double angles[3]);
 DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o);
+mbr_status build_frame_owned_gamma(const mbr_camera &cam, const mbr_render_params &p, uint16_t *gamma_dev,
+                                   double *gamma_value, DevFrame *out, std::string *err);
 const DevScene *ctx_scene(mbr_ctx *ctx);
 const mbr_scene *ctx_scene_src(mbr_ctx *ctx);
 mbr_tuning &ctx_tuning(mbr_ctx *ctx);

@@ -28,7 +28,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "fast_formula.cuh"
@@ -1068,3 +1071,124 @@ mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *, const mbr_render_params
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Allocation-free rendering
+//
+// For callers that cannot allocate device memory: a host application whose
+// device memory is owned by its own allocator or memory pool (which must not
+// be bypassed), or a process running under a hard memory cap, where a
+// cudaMalloc in the middle of a frame could fail or synchronise the device.
+// The wavefront pipeline's scratch (hit records, stage-S start records,
+// launch counters, the gamma table and the status word) lives in one
+// file-scope device array, part of this library's device image: every GPU
+// that loads the library holds it until the process exits.
+// ============================================================================
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MBR_NOALLOC_SCRATCH_BYTES];
+
+const size_t kGammaBytes = 65536 * sizeof(uint16_t);
+const size_t kHeadBytes = kGammaBytes + 256;  // gamma table, then the status word
+
+struct NoallocDevice {
+  bool ready = false;
+  unsigned char *base = nullptr;  // device address of g_noalloc_scratch on this device
+  double gamma_value = -1.0;      // gamma of the table currently in the array
+};
+const int kMaxDevices = 64;
+NoallocDevice g_noalloc[kMaxDevices];
+std::mutex g_noalloc_mutex;
+
+mbr_status noalloc_fail(char *err, size_t err_len, mbr_status st, const std::string &msg) {
+  if (err && err_len) std::snprintf(err, err_len, "%s", msg.c_str());
+  return st;
+}
+
+}  // namespace
+
+extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera,
+                                         const mbr_render_params *params, const mbr_outputs *out, void *stream,
+                                         char *err, size_t err_len) {
+  if (err && err_len) err[0] = '\0';
+  if (!scene || !camera || !params || !out) return noalloc_fail(err, err_len, MBR_EINVAL, "null argument");
+  int dev = 0;
+  int e = int(cudaGetDevice(&dev));
+  if (e || dev < 0 || dev >= kMaxDevices)
+    return noalloc_fail(err, err_len, MBR_ECUDA, "no current CUDA device");
+  // one-time set-up on this device: the device address of the scratch array
+  // (host code may not use the array's name as a device address)
+  NoallocDevice *nd = &g_noalloc[dev];
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!nd->ready) {
+      void *ptr = nullptr;
+      e = int(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+      if (e || !ptr)
+        return noalloc_fail(err, err_len, MBR_ECUDA,
+                            std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(cudaError_t(e)));
+      nd->base = static_cast<unsigned char *>(ptr);
+      nd->ready = true;
+    }
+  }
+  DevScene sc;
+  mbr_status st = build_scene(nullptr, *scene, &sc);
+  if (st != MBR_OK) return noalloc_fail(err, err_len, st, "invalid or unsupported scene (see mbr_scene_set)");
+  DevFrame fr;
+  std::string msg;
+  st = build_frame_owned_gamma(*camera, *params, reinterpret_cast<uint16_t *>(nd->base), &nd->gamma_value, &fr,
+                               &msg);
+  if (st != MBR_OK) return noalloc_fail(err, err_len, st, msg);
+  fr.want_normal = out->normal != nullptr;
+  if (sc.is_hybrid || sc.iter_thresh || sc.interior || sc.has_w || fr.gi_samples > 0 ||
+      fr.refine != MBR_REFINE_REFERENCE)
+    return noalloc_fail(err, err_len, MBR_EUNSUPPORTED,
+                        "the wavefront engine renders non-hybrid scenes without GI, root refinement, "
+                        "iteration threshold, interior mode or initial w");
+  const long long total = (long long)fr.width * fr.height;  // row-linear queue: no tile padding
+  const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
+  const size_t need = scratch_bytes(total, per);
+  const size_t have = size_t(MBR_NOALLOC_SCRATCH_BYTES) - kHeadBytes;
+  if (need > have) {
+    const size_t per_pixel = sizeof(HitRec) + sizeof(float4) * (1 + size_t(per));
+    char buf[320];
+    std::snprintf(buf, sizeof(buf),
+                  "frame of %lld pixels with %d shadow/AO tasks per hit needs %zu bytes of scratch; the "
+                  "allocation-free entry point has %zu (at most %zu pixels at this setting)",
+                  total, per, need, have, (have - 256) / per_pixel);
+    return noalloc_fail(err, err_len, MBR_EINVAL, buf);
+  }
+  Launch L;
+  std::memset(&L, 0, sizeof(L));
+  L.njobs = 1;
+  L.total = total;
+  scratch_layout(L, nd->base + kHeadBytes, total);
+  const mbr_tuning tu{128, 12, 2, 0};
+  L.refill_k = tu.refill_k;
+  L.layout = tu.queue_layout;
+  L.ao_rays = fr.ao_rays;
+  L.shadow_tasks = (fr.shading_enable && fr.shadow_enable) ? 1 : 0;
+  L.want_normal = fr.want_normal;
+  DevOutputs d;
+  d.depth = out->depth;
+  d.iters = out->iters;
+  d.hit = out->hit;
+  d.normal = out->normal;
+  d.shade = out->shade;
+  d.ao = out->ao;
+  d.rgb = out->rgb;
+  d.rgb8 = out->rgb8;
+  d.stats = out->stats;
+  d.status = reinterpret_cast<int32_t *>(nd->base + kGammaBytes);
+  d.pixel_offset = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the array keeps the previous call's contents: the status word starts at
+  // zero here and the launch counters are zeroed at the head of the pipeline
+  e = int(cudaMemsetAsync(d.status, 0, sizeof(int32_t), s));
+  if (e) return noalloc_fail(err, err_len, MBR_ECUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(cudaError_t(e)));
+  const WJob j0 = make_job(fr, 0, 0);
+  const FastParams fp = load_fast_params(sc);
+  e = launch_pipeline<false>(fast_kind(fp), tu, s, fr, fp, j0, L, d, total);
+  if (e) return noalloc_fail(err, err_len, MBR_ECUDA, std::string("wavefront launch: ") + cudaGetErrorString(cudaError_t(e)));
+  return MBR_OK;
+}
