@@ -34,6 +34,7 @@ UNITS = [
     ("plain_mixed.cu", []),
     ("wavefront.cu", []),
     ("probe.cu", []),
+    ("adjoint.cu", []),
 ]
 
 

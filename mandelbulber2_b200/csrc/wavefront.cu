@@ -1065,10 +1065,7 @@ done:
   return status;
 }
 
-mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *, const mbr_render_params *, const double *, const uint8_t *,
-                       const float *, const float *, double *, int, void *) {
-  return set_err(ctx, MBR_EUNSUPPORTED, "adjoint not built yet");
-}
+
 
 }  // extern "C"
 

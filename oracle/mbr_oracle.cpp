@@ -440,6 +440,16 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   return out;
 }
 
+// The gradient model of a non-escaping orbit (a point inside the set): its
+// distance estimate is ~0 and, to first order, constant - its exact
+// derivative through 50+ chaotic iterations is noise.  No-op for plain values.
+template <class S>
+inline void zero_tangents(S &) {}
+template <int N>
+inline void zero_tangents(Dual<N> &d) {
+  for (int i = 0; i < N; i++) d.d[i] = 0.0;
+}
+
 // CalculateDistanceSimple, analytic branch (calculate_distance.cpp:533-606),
 // reached through CalculateDistanceFromObjectsTree (:225-516) for the single
 // identity-transform node (pointLocal == point, distance *= 1).
@@ -449,6 +459,7 @@ S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double 
   const int mult = (normalMode && seq.iter_thresh) ? 5 : 1;
   FractalOut<S> fo = compute<S>(seq, slots, px, py, pz, mult, -1);
   S distance = fo.distance;
+  if (fo.maxiter) zero_tangents(distance);
   bool maxiter = fo.maxiter;
   if (iters_out) *iters_out = fo.iters;
   if (!seq.iter_thresh) maxiter = false;
@@ -1297,6 +1308,24 @@ int oracle_opcount_de(const mbr_scene *scene, const double *pts, int64_t n, doub
   return 0;
 }
 
+// CalculateDistance and its forward-mode tangents (power, scale, mR2, x, y, z)
+// at n points: out[7 i] = value, out[7 i + 1 + k] = tangent k.
+int oracle_de_tangents(const mbr_scene *scene, const double *pts, int64_t n, double detail, int normal_mode,
+                       double *out) {
+  Seq seq;
+  if (!build_sequence(*scene, &seq)) return 1;
+  typedef Dual<6> DD;
+  std::vector<SlotT<DD>> slots;
+  for (int i = 0; i < seq.n; i++) slots.push_back(make_slot<DD>(seq.slot[i], true));
+  for (int64_t i = 0; i < n; i++) {
+    DD x = DD::seed(pts[3 * i], TAN_X), y = DD::seed(pts[3 * i + 1], TAN_Y), z = DD::seed(pts[3 * i + 2], TAN_Z);
+    DD d = calc_distance<DD>(seq, slots.data(), x, y, z, detail, normal_mode != 0, nullptr);
+    out[7 * i] = d.v;
+    for (int k = 0; k < 6; k++) out[7 * i + 1 + k] = d.d[k];
+  }
+  return 0;
+}
+
 // Dual-number reference of the adjoint: for each pixel with hit[i] != 0, the
 // depth derivative dt/dθ (by the implicit function of F(t) = dist - thr at the
 // stored depth) and the derivative of the Lambert term max(N·L, 0) through the
@@ -1304,7 +1333,7 @@ int oracle_opcount_de(const mbr_scene *scene, const double *pts, int64_t n, doub
 // dt_dtheta / ds_dtheta: [n_pixels * MBR_GRAD_COUNT] (host).
 int oracle_pixel_gradients(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
                            const double *depth, const uint8_t *hit, double *dt_dtheta, double *ds_dtheta,
-                           float *shade_out) {
+                           double *shade_out) {
   Renderer R;
   if (!make_renderer(scene, cam, params, &R)) return 1;
   if (!cam->use_angles) return 2;
@@ -1337,7 +1366,7 @@ int oracle_pixel_gradients(const mbr_scene *scene, const mbr_camera *cam, const 
       double *dt = dt_dtheta + i * MBR_GRAD_COUNT;
       double *ds = ds_dtheta + i * MBR_GRAD_COUNT;
       for (int k = 0; k < MBR_GRAD_COUNT; k++) dt[k] = ds[k] = 0.0;
-      if (shade_out) shade_out[i] = 0.0f;
+      if (shade_out) shade_out[i] = 0.0;
       if (!hit[i]) continue;
       double ix, iy;
       R.image_point(double(px), double(py), &ix, &iy);
@@ -1347,7 +1376,11 @@ int oracle_pixel_gradients(const mbr_scene *scene, const mbr_camera *cam, const 
       const D3 p = add(R.camera, mul(dir, t));
       const double thr = R.dist_thresh(p);
       double g[6];
-      eval(p, thr, false, g);
+      const double dv = eval(p, thr, false, g);
+      // implicit differentiation needs F(t) = dist - thr = 0; a bisection
+      // that converged onto a jump of the distance estimate (an orbit's
+      // bailout iteration changing along the ray) leaves |F| large
+      if (std::fabs(dv - thr) > 1e-6 * thr) continue;
       const D3 grad{g[3], g[4], g[5]};
       // ∂p/∂θ at fixed t, for θ in MBR_GRAD order
       D3 dp[MBR_GRAD_COUNT];
@@ -1394,7 +1427,7 @@ int oracle_pixel_gradients(const mbr_scene *scene, const mbr_camera *cam, const 
       const double gl = sqrt(gval[0] * gval[0] + gval[1] * gval[1] + gval[2] * gval[2]);
       const D3 N{gval[0] / gl, gval[1] / gl, gval[2] / gl};
       const double s = dot(N, R.light);
-      if (shade_out) shade_out[i] = float(s > 0 ? s : 0);
+      if (shade_out) shade_out[i] = s > 0 ? s : 0.0;
       if (s > 0.0) {
         for (int k = 0; k < MBR_GRAD_COUNT; k++) {
           const D3 dg{gder[0][k], gder[1][k], gder[2][k]};

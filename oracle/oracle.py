@@ -56,6 +56,7 @@ class Oracle:
         L.oracle_pcg32.argtypes = [C.c_uint64, C.c_uint64, C.c_int, _P]
         L.oracle_opcount.argtypes = [C.POINTER(abi.Scene), C.c_int, _P, _P]
         L.oracle_opcount_de.argtypes = [C.POINTER(abi.Scene), _P, C.c_int64, C.c_double, _P]
+        L.oracle_de_tangents.argtypes = [C.POINTER(abi.Scene), _P, C.c_int64, C.c_double, C.c_int, _P]
         L.oracle_pixel_gradients.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Camera),
                                              C.POINTER(abi.RenderParams), _P, _P, _P, _P, _P]
         L.oracle_threads.restype = C.c_int
@@ -154,13 +155,23 @@ class Oracle:
         return dict(zip(("add", "mul", "div", "sqrt", "transc", "cmp", "iters", "evals", "e_add", "e_mul"),
                         out.tolist()))
 
+    def de_tangents(self, scene, pts: np.ndarray, detail: float, normal_mode: bool = False):
+        """Distance and its tangents (power, scale, mR2, x, y, z) at points: (n, 7)."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        out = np.zeros((pts.shape[0], 7), dtype=np.float64)
+        rc = self.lib.oracle_de_tangents(C.byref(scene), pts.ctypes.data, pts.shape[0], detail, int(normal_mode),
+                                         out.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle_de_tangents failed")
+        return out
+
     def pixel_gradients(self, scene, cam, params, depth: np.ndarray, hit: np.ndarray):
         n = cam.width * cam.height
         depth = np.ascontiguousarray(depth, dtype=np.float64)
         hit = np.ascontiguousarray(hit, dtype=np.uint8)
         dt = np.zeros((n, 8), dtype=np.float64)
         ds = np.zeros((n, 8), dtype=np.float64)
-        shade = np.zeros(n, dtype=np.float32)
+        shade = np.zeros(n, dtype=np.float64)
         rc = self.lib.oracle_pixel_gradients(C.byref(scene), C.byref(cam), C.byref(params), depth.ctypes.data,
                                              hit.ctypes.data, dt.ctypes.data, ds.ctypes.data, shade.ctypes.data)
         if rc != 0:
