@@ -41,14 +41,19 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default="wavefront_fp32")
     ap.add_argument("--baseline-engine", default="plain_fp64")
-    ap.add_argument("--workload", default="mandelbox_1080p_A")
+    ap.add_argument("--workload", default="mandelbox_1080p_A", choices=WORKLOADS)
+    ap.add_argument("--spp", type=int, default=16, help="GI samples per pixel (hybrid_gi_2160p)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
     return ap.parse_args()
 
 
-def workload(name: str):
+WORKLOADS = ("mandelbox_1080p_A", "mandelbox_1080p_B", "mandelbulb_512", "hybrid_gi_2160p", "batch_2048")
+
+
+def workload(name: str, spp: int = 16):
+    """Scene, camera, parameters and description of a frame workload."""
     from mandelbulber2_b200 import configs
 
     if name == "mandelbox_1080p_A":
@@ -56,14 +61,36 @@ def workload(name: str):
         desc = {"workload": "mandelbox s=-1.5 1920x1080 camera A (0,-6,0) fov 53, N=50, bailout 100, "
                             "5 binary steps, lambert + hard shadow, 16 AO rays", "width": 1920, "height": 1080,
                 "formula": "mandelbox", "maxiter": 50, "ao_rays": 16}
+    elif name == "mandelbox_1080p_B":
+        sc, cam, p = configs.mandelbox_1080p("A")  # camera B is placed from view A's centre hit in main()
+        desc = {"workload": "mandelbox s=-1.5 1920x1080 camera B: 1e-5 in front of view A's centre hit, fov 0.5, "
+                            "16 AO rays (deep zoom)", "width": 1920, "height": 1080, "formula": "mandelbox",
+                "maxiter": 50, "ao_rays": 16}
     elif name == "mandelbulb_512":
         sc, cam, p = configs.mandelbulb_512()
         desc = {"workload": "mandelbulb p=8 512x512 camera (0,-3,0) fov 53, N=250, bailout 10, 5 binary steps, "
                             "lambert + hard shadow", "width": 512, "height": 512, "formula": "mandelbulb",
                 "maxiter": 250}
+    elif name == "hybrid_gi_2160p":
+        sc, cam, p = configs.hybrid_gi_2160p(spp=spp)
+        desc = {"workload": f"hybrid mandelbulb(1-3)+menger(4-12) 3840x2160 monte carlo GI {spp} spp, 4 bounces, "
+                            "thin lens aperture 0.02 focus 3", "width": 3840, "height": 2160, "formula": "hybrid",
+                "spp": spp}
     else:
         raise SystemExit(f"unknown workload {name}")
     return sc, cam, p, desc
+
+
+def kernels_per_frame(engine: str, p) -> int:
+    """Kernel launches of one frame: the plain engines launch one kernel; the
+    wavefront pipeline launches stage P, N (normals wanted), D and S (shadow or
+    AO), the finish kernel and the pixel counter."""
+    if "wavefront" not in engine:
+        return 1
+    n = 4  # primary, normals (the bench asks for normals), finish, pixel count
+    if p.ao_rays > 0 or (p.shading_enable and p.shadow_enable):
+        n += 2  # directions, shadow/AO marches
+    return n
 
 
 # ---- clocks ---------------------------------------------------------------------
@@ -240,6 +267,93 @@ def run_reference(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_batch(a, torch, dist, world, rank, local) -> None:
+    """2048 render jobs of uneven size in one graph-captured wavefront launch,
+    against the plain FP64 kernel rendering the same jobs one by one."""
+    import numpy as np
+
+    from mandelbulber2_b200 import abi, configs
+    from mandelbulber2_b200.render import Renderer, STATS_FIELDS, alloc_outputs, outputs_struct, stats_dict
+    scenes, cams, offsets, total = configs.batch_jobs(2048, seed=7)
+    # jobs of this rank (weak scaling: every rank renders a full set of 2048 jobs)
+    p = configs.base_params(5, 20.0)
+    p.shading_enable = 0
+    p.shadow_enable = 0
+    p.ao_rays = 0
+    r = Renderer(local)
+    jobs = (abi.Job * len(cams))()
+    for i, c in enumerate(cams):
+        jobs[i].camera = c
+        jobs[i].scene_index = i
+        jobs[i].pixel_offset = offsets[i]
+    sc_arr = (abi.Scene * len(scenes))(*scenes)
+    names = ("depth", "normal")
+    bufs = alloc_outputs(total, r.device, names)
+    stats = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=r.device)
+    o = outputs_struct(bufs, stats)
+    b = C.c_void_p()
+    lib = abi.load()
+    st = lib.mbr_batch_create(r.ctx, sc_arr, len(scenes), jobs, len(cams), C.byref(p), C.byref(o),
+                              abi.ENGINE_WAVEFRONT_FP32, None, C.byref(b))
+    if st != abi.MBR_OK:
+        raise SystemExit(lib.mbr_last_error_string(r.ctx).decode())
+    s = torch.cuda.current_stream()
+    for _ in range(a.warmup):
+        lib.mbr_batch_launch(b, C.c_void_p(s.cuda_stream))
+    r.sync()
+    stats.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(a.steps):
+        lib.mbr_batch_launch(b, C.c_void_p(s.cuda_stream))
+    e1.record()
+    torch.cuda.synchronize()
+    r.sync()
+    t = e0.elapsed_time(e1) / 1e3
+    sd = stats_dict(stats)
+    fast = {k: v.cpu().numpy() for k, v in bufs.items()}
+    lib.mbr_batch_destroy(b)
+    # plain FP64, job by job (one launch per job)
+    base = None
+    if not a.no_baseline:
+        bstats = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=r.device)
+        torch.cuda.synchronize()
+        e0.record()
+        for i, (sc, cam) in enumerate(zip(scenes, cams)):
+            r.set_scene(sc)
+            n = cam.width * cam.height
+            view = {k: v[offsets[i]: offsets[i] + n] for k, v in bufs.items()}
+            r.render_into(cam, p, view, bstats, abi.ENGINE_PLAIN_FP64)
+        e1.record()
+        torch.cuda.synchronize()
+        bt = e0.elapsed_time(e1) / 1e3
+        bsd = stats_dict(bstats)
+        ref = {k: v.cpu().numpy() for k, v in bufs.items()}
+        hf, hr = fast["depth"] < 1e19, ref["depth"] < 1e19
+        both = hf & hr
+        rel = np.abs(fast["depth"][both] - ref["depth"][both]) / ref["depth"][both]
+        base = {"engine": "plain_fp64 (one launch per job)", "value": bsd["de_evals"] / bt, "unit": UNIT,
+                "seconds": bt, "hit_mismatch": float((hf != hr).mean()), "depth_rel_median": float(np.median(rel)),
+                "depth_rel_p99": float(np.quantile(rel, 0.99))}
+    value = sd["de_evals"] / t
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (procedural fractal scenes, no dataset)",
+                "config": {"workload": "2048 jobs, resolutions {64..1024}^2, cameras on a sphere r U[2.5,4], "
+                                       "mandelbulb (p U[2,12], N=100) / mandelbox (scale U[-2.5,-1.5] or U[1.5,3], "
+                                       "minR2 U[0.1,0.5], N=40), seed 7; outputs depth + normals",
+                           "pixels": total, "engine": "wavefront_fp32 batch (one graph launch)"},
+                "mpix_per_s": sd["pixels"] / t / 1e6, "stats_per_step": {k: v / a.steps for k, v in sd.items()},
+                "fp64_baseline": base, "speedup_vs_fp64": value / base["value"] if base else None,
+                "gpu_launches": a.steps * 4}
+        print(json.dumps(line), flush=True)
+    r.close()
+
+
 def main() -> None:
     a = parse()
     if a.impl == "reference":
@@ -266,13 +380,27 @@ def main() -> None:
         dist = tdist
     torch.cuda.set_device(local)
     engines = {v: k for k, v in abi.ENGINE_NAMES.items()}
+    if a.workload == "batch_2048":
+        run_batch(a, torch, dist, world, rank, local)
+        return
+    if a.workload == "hybrid_gi_2160p" and "wavefront" in a.engine:
+        a.engine = "plain_mixed"  # GI runs on the plain engines (FP32 march, FP64 origin and refinement)
     engine = engines[a.engine]
     base_engine = engines[a.baseline_engine]
 
-    sc, cam, p, desc = workload(a.workload)
+    sc, cam, p, desc = workload(a.workload, a.spp)
     p.seed = rank  # each rank: its own frame (jitter stream)
     r = Renderer(local)
     r.set_scene(sc)
+    if a.workload == "mandelbox_1080p_B":
+        # camera B: 1e-5 in front of the surface point hit by view A's centre ray
+        from mandelbulber2_b200 import configs
+
+        fa = r.render(cam, p, abi.ENGINE_PLAIN_FP64, outputs=("depth", "hit"))
+        cdepth = float(fa["depth"].cpu().numpy()[(cam.height // 2) * cam.width + cam.width // 2])
+        sc, cam, p = configs.mandelbox_1080p("B", centre_depth=cdepth)
+        p.seed = rank
+        desc["centre_depth"] = cdepth
     tuning = None
     if "wavefront" in a.engine:
         t_ = r.autotune(cam, p, engine)  # the library's own autotuner picks the launch shape
@@ -386,7 +514,7 @@ def main() -> None:
             "de_evals_per_frame": st["de_evals"] / a.steps, "stats_per_frame": {k: v / a.steps for k, v in st.items()},
             "fp64_baseline": base, "speedup_vs_fp64": (value / base["value"]) if base else None,
             "error_vs_fp64": err, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": a.steps, "clocks": clk, "per_step_ms": ms,
+            "gpu_launches": a.steps * kernels_per_frame(a.engine, p), "clocks": clk, "per_step_ms": ms,
         }
         print(json.dumps(line), flush=True)
     r.close()

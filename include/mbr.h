@@ -191,14 +191,16 @@ typedef struct mbr_render_params {
   double dof_aperture;          /* thin lens radius; 0 = pinhole */
   double dof_focus;             /* focus distance */
   uint32_t gi_seed;             /* PCG32 state seed (stream = pixel*spp + sample) */
-  int32_t reserved1;
+  int32_t row_begin;            /* render rows [row_begin, row_end) only (a band of the frame, for
+                                   sharding one frame over several GPUs); 0, 0 = the whole frame.
+                                   Pixels outside the band keep their buffer contents. */
   /* image adjustments (sImageAdjustments, cimage.cpp:317-362) */
   double brightness;            /* default 1 */
   double contrast;              /* default 1 */
   double gamma;                 /* default 1 */
   double saturation;            /* default 1 */
   int32_t hdr;                  /* default 0 */
-  int32_t reserved2;
+  int32_t row_end;              /* 0 = the last row */
 } mbr_render_params;
 
 /* Per-launch counters (src/statistics.h:42-70 mirrored).  A DE evaluation

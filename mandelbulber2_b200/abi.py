@@ -77,8 +77,8 @@ class RenderParams(C.Structure):
         ("albedo", C.c_double), ("ambient_intensity", C.c_double), ("ao_rays", C.c_int32),
         ("ao_seed", C.c_uint32), ("background", D3), ("gi_samples", C.c_int32), ("gi_bounces", C.c_int32),
         ("gi_sky", C.c_double), ("gi_sun", C.c_double), ("dof_aperture", C.c_double), ("dof_focus", C.c_double),
-        ("gi_seed", C.c_uint32), ("reserved1", C.c_int32), ("brightness", C.c_double), ("contrast", C.c_double),
-        ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("reserved2", C.c_int32),
+        ("gi_seed", C.c_uint32), ("row_begin", C.c_int32), ("brightness", C.c_double), ("contrast", C.c_double),
+        ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("row_end", C.c_int32),
     ]
 
 

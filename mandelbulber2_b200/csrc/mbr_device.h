@@ -76,6 +76,7 @@ struct DevFrame {
   double mrot[9];      // PrepareMainVectors mRot, row-major
   int32_t mrot_zero;   // CRotationMatrix::zero: RotateVector is the identity
   int32_t width, height;
+  int32_t row0, row1;  // rows rendered: [row0, row1)
   int32_t max_steps;
   int32_t binary_steps;
   int32_t refine;

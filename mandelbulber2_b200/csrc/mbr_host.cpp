@@ -359,6 +359,10 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
     return set_err(ctx, MBR_EINVAL, "dof_focus must be > 0 with an aperture");
   if (!(p.gamma > 0.0)) return set_err(ctx, MBR_EINVAL, "gamma must be > 0");
   if (p.constant_de_threshold && !(p.de_thresh > 0.0)) return set_err(ctx, MBR_EINVAL, "de_thresh must be > 0");
+  const int row_end = p.row_end == 0 ? cam.height : p.row_end;
+  if (p.row_begin < 0 || p.row_begin >= row_end || row_end > cam.height)
+    return set_err(ctx, MBR_EINVAL, "row band [%d, %d) outside the %d rows of the frame", p.row_begin, p.row_end,
+                   cam.height);
   const double *L = p.light_direction;
   if (!finite3(L) || (L[0] == 0.0 && L[1] == 0.0 && L[2] == 0.0))
     return set_err(ctx, MBR_EINVAL, "light_direction must be finite and non-zero");
@@ -371,6 +375,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.mrot_zero = zero ? 1 : 0;
   f.width = cam.width;
   f.height = cam.height;
+  f.row0 = p.row_begin;
+  f.row1 = row_end;
   f.max_steps = p.max_raymarching_steps;
   f.binary_steps = p.binary_steps;
   f.refine = p.refine;

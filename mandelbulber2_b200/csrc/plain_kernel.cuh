@@ -102,10 +102,10 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ DevS
   // a warp renders an 8x4 pixel tile, a block 16x8 pixels
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int x = blockIdx.x * 16 + (warp & 1) * 8 + (lane & 7);
-  const int y = blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
+  const int y = fr.row0 + blockIdx.y * 8 + (warp >> 1) * 4 + (lane >> 3);
   ThreadCount tc{0u, 0u};
   unsigned int n_march = 0, n_binary = 0, n_normal = 0, n_shadow = 0, n_ao = 0, n_gi = 0, trips = 0, n_pix = 0;
-  if (x < fr.width && y < fr.height) {
+  if (x < fr.width && y < fr.row1) {
     const unsigned long long pixel = (unsigned long long)y * fr.width + x;
     MarchOut m;
     float nrm[3] = {0.0f, 0.0f, 0.0f};
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128) distance_kernel(const __grid_constant__ D
 template <class T, class R, int V>
 int launch_plain_t(const DevScene &sc, const DevFrame &fr, const DevOutputs &out, void *stream) {
   const dim3 block(128);
-  const dim3 grid((fr.width + 15) / 16, (fr.height + 7) / 8);
+  const dim3 grid((fr.width + 15) / 16, (fr.row1 - fr.row0 + 7) / 8);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int F = sc.is_hybrid ? 0 : sc.uniform_formula;
   if (sc.has_w) {

@@ -49,6 +49,7 @@ struct WJob {
   double mrot[9];
   int32_t mrot_zero;
   int32_t width, height, tiles_x;
+  int32_t row0, rows;      // the job renders rows [row0, row0 + rows) of its frame
   long long first;         // first work item of this job in the pixel queue
   long long pixel_offset;  // first pixel of this job in the outputs
   double fov, aspect;
@@ -321,7 +322,8 @@ struct PrimaryStage {
       x = int(local % jb->width);
       y = int(local / jb->width);
     }
-    if (x >= jb->width || y >= jb->height) return false;  // padding of the last tile row/column
+    if (x >= jb->width || y >= jb->rows) return false;  // padding of the last tile row/column
+    y += jb->row0;
     ray = unsigned(y) * unsigned(jb->width) + unsigned(x);
     pix = jb->pixel_offset + (long long)ray;
     // camera ray (render_worker.cpp:155-163, 247, 326-327)
@@ -782,6 +784,8 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.width = fr.width;
   j.height = fr.height;
   j.tiles_x = (fr.width + 7) / 8;
+  j.row0 = fr.row0;
+  j.rows = fr.row1 - fr.row0;
   j.first = first;
   j.pixel_offset = pixel_offset;
   j.fov = fr.fov;
@@ -792,8 +796,8 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
 }
 
 static long long job_items(const WJob &j, int layout) {
-  if (layout == 1) return (long long)j.tiles_x * ((j.height + 3) / 4) * 32;
-  return (long long)j.width * j.height;
+  if (layout == 1) return (long long)j.tiles_x * ((j.rows + 3) / 4) * 32;
+  return (long long)j.width * j.rows;
 }
 
 static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr) {
@@ -891,7 +895,7 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   L.want_normal = fr.want_normal;
   const FastParams fp = load_fast_params(sc);
   const int e = launch_pipeline<false>(fast_kind(fp), tu, static_cast<cudaStream_t>(stream), fr, fp, j0, L, out,
-                                       (long long)fr.width * fr.height);
+                                       (long long)fr.width * (fr.row1 - fr.row0));
   return cuda_err(ctx, e, "wavefront launch");
 }
 
@@ -946,7 +950,7 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
     if (i == 0) fr0 = fr;
     wj[i] = make_job(fr, first, jb.pixel_offset);
     first += job_items(wj[i], tu.queue_layout);
-    pixels += (long long)fr.width * fr.height;
+    pixels += (long long)fr.width * (fr.row1 - fr.row0);
     fps[i] = load_fast_params(dsc[jb.scene_index]);
   }
   fr0.want_normal = outs->normal != nullptr;
@@ -1142,7 +1146,7 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
     return noalloc_fail(err, err_len, MBR_EUNSUPPORTED,
                         "the wavefront engine renders non-hybrid scenes without GI, root refinement, "
                         "iteration threshold, interior mode or initial w");
-  const long long total = (long long)fr.width * fr.height;  // row-linear queue: no tile padding
+  const long long total = (long long)fr.width * (fr.row1 - fr.row0);  // row-linear queue: no tile padding
   const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
   const size_t need = scratch_bytes(total, per);
   const size_t have = size_t(MBR_NOALLOC_SCRATCH_BYTES) - kHeadBytes;

@@ -123,3 +123,24 @@ def test_wavefront_rejects_unsupported(renderer):
     with pytest.raises(MbrError) as e:
         renderer.render(cam, p, WF)
     assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("engine", [abi.ENGINE_PLAIN_FP64, WF])
+def test_row_bands_compose_into_the_frame(renderer, engine):
+    """Two row bands rendered into one buffer give the whole frame (sharding a frame over GPUs)."""
+    from mandelbulber2_b200.shard import band_params, row_band
+
+    sc, cam, p = configs.mandelbox_1080p("A", 96, 54, ao_rays=4)
+    renderer.set_scene(sc)
+    whole = renderer.render(cam, p, engine, outputs=("depth", "iters", "hit", "normal", "rgb8"))
+    bufs = alloc_outputs(cam.width * cam.height, renderer.device, ("depth", "iters", "hit", "normal", "rgb8"))
+    total = 0
+    for rank in range(2):
+        r0, r1 = row_band(cam.height, 2, rank)
+        stats = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=renderer.device)
+        renderer.render_into(cam, band_params(p, r0, r1), bufs, stats, engine)
+        renderer.sync()
+        total += stats_dict(stats)["de_evals"]
+    for k in bufs:
+        assert np.array_equal(bufs[k].cpu().numpy(), whole[k].cpu().numpy()), k
+    assert total == whole.stats["de_evals"]
