@@ -1,0 +1,57 @@
+"""Small named render cases for profiling one kernel at a time (ncu -k ...).
+
+  python -m mandelbulber2_b200.profile_cases <case>
+
+cases: plain_fp64, plain_strict, plain_mixed, wavefront (Mandelbox s=-1.5,
+960x540, camera A, 16 AO rays; two frames), gi (hybrid Mandelbulb/Menger
+480x270, 2 spp), adjoint (Mandelbulb 256x256 forward + FP64 adjoint),
+distance (CalculateDistance at 2^20 random points).
+"""
+from __future__ import annotations
+
+import sys
+
+import torch
+
+from . import abi, configs
+from .render import STATS_FIELDS, Renderer, alloc_outputs
+
+FRAME_ENGINES = {"plain_fp64": abi.ENGINE_PLAIN_FP64, "plain_strict": abi.ENGINE_PLAIN_FP64_STRICT,
+                 "plain_mixed": abi.ENGINE_PLAIN_MIXED, "wavefront": abi.ENGINE_WAVEFRONT_FP32}
+
+
+def frame(r: Renderer, sc, cam, p, engine: int, reps: int = 2) -> dict:
+    r.set_scene(sc)
+    bufs = alloc_outputs(cam.width * cam.height, r.device, ("depth", "iters", "hit", "normal", "rgb8"))
+    st = torch.zeros(len(STATS_FIELDS), dtype=torch.int64, device=r.device)
+    for _ in range(reps):
+        r.render_into(cam, p, bufs, st, engine)
+    r.sync()
+    return bufs
+
+
+def run(case: str) -> None:
+    r = Renderer(0)
+    if case in FRAME_ENGINES:
+        sc, cam, p = configs.mandelbox_1080p("A", 960, 540)
+        frame(r, sc, cam, p, FRAME_ENGINES[case])
+    elif case == "gi":
+        sc, cam, p = configs.hybrid_gi_2160p(480, 270, spp=2)
+        frame(r, sc, cam, p, abi.ENGINE_PLAIN_MIXED, reps=1)
+    elif case == "adjoint":
+        sc, cam, p = configs.adjoint_256("mandelbulb", 256, 256)
+        b = frame(r, sc, cam, p, abi.ENGINE_PLAIN_MIXED, reps=1)
+        w = torch.ones(cam.width * cam.height, dtype=torch.float32, device=r.device)
+        r.adjoint(cam, p, b["depth"], b["hit"], w, w, abi.ENGINE_PLAIN_FP64)
+    elif case == "distance":
+        r.set_scene(configs.mandelbox_scene())
+        pts = torch.rand(1 << 20, 3, dtype=torch.float64, device=r.device) * 6 - 3
+        r.distance(pts, 1e-3, False, abi.ENGINE_PLAIN_FP64)
+    else:
+        raise SystemExit(f"unknown case {case}")
+    r.close()
+    print("ok", case)
+
+
+if __name__ == "__main__":
+    run(sys.argv[1])
