@@ -103,17 +103,39 @@ struct Z3 {
   float x, y, z;
 };
 
+// a*b + c clamped to [0, 1] in one FFMA.SAT (a separate saturate of an fmaf
+// result costs the ALU pipe another instruction)
+__device__ __forceinline__ float fma_sat(float a, float b, float c) {
+  float y;
+  asm("fma.rn.sat.f32 %0, %1, %2, %3;" : "=f"(y) : "f"(a), "f"(b), "f"(c));
+  return y;
+}
+
+// 1/x from the MUFU unit (max. 1 ulp; 0 -> +inf, flushes denormals)
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// sqrt(x) from the MUFU unit (max. 2 ulp; flushes denormals)
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // One Mandelbox iteration + c-addition.  c holds the (pre-multiplied) constant.
 template <bool SIMPLE>
 __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, const FastParams &f) {
   if (SIMPLE) {
     const float L2 = 0.5f * f.q1;  // 2L
-    z.x = fmaf(f.q1, __saturatef(fmaf(z.x, f.q0, 0.5f)), -z.x) - L2;
-    z.y = fmaf(f.q1, __saturatef(fmaf(z.y, f.q0, 0.5f)), -z.y) - L2;
-    z.z = fmaf(f.q1, __saturatef(fmaf(z.z, f.q0, 0.5f)), -z.z) - L2;
+    z.x = fmaf(f.q1, fma_sat(z.x, f.q0, 0.5f), -z.x) - L2;
+    z.y = fmaf(f.q1, fma_sat(z.y, f.q0, 0.5f), -z.y) - L2;
+    z.z = fmaf(f.q1, fma_sat(z.z, f.q0, 0.5f), -z.z) - L2;
     const float r2 = fmaf(z.x, z.x, fmaf(z.y, z.y, z.z * z.z));
-    // factor = 1 + (F-1) * sat((fR2/r2 - 1) / (F-1))
-    const float fs = fmaf(f.q3, __saturatef(fmaf(f.q2, __fdividef(1.0f, r2), f.q4)), 1.0f);
+    // factor = 1 + (F-1) * sat((fR2/r2 - 1) / (F-1)); r2 = 0 gives +inf -> factor F
+    const float fs = fmaf(f.q3, fma_sat(f.q2, rcp_approx(r2), f.q4), 1.0f);
     const float s = fs * f.p0;
     dr = fmaf(dr, fs * f.p1, 1.0f);
     z.x = fmaf(z.x, s, c.x);
@@ -179,7 +201,7 @@ __device__ __forceinline__ void it_menger(Z3 &z, float &dr, const Z3 &c, const F
 // Final distance of Compute + CalculateDistanceSimple clamps
 // (compute_fractal.cpp:561-621, calculate_distance.cpp:569, 604-605).
 __device__ __forceinline__ float final_de(const FastParams &f, float r2, float dr, int iters, float detail) {
-  const float r = sqrtf(r2);
+  const float r = sqrt_approx(r2);
   float d;
   if (!(dr > 0.0f)) d = r;
   else if (f.de_fn == 2) d = (r > 1.0f) ? __fdividef(0.5f * r * __logf(r), dr) : 0.0f;

@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "fast_formula.cuh"
+#include "fastdiv.h"
 #include "mbr_internal.h"
 #include "pixel_ops.cuh"
 
@@ -55,6 +56,7 @@ struct WJob {
   double fov, aspect;
   float c0;                // threshold per unit distance: resolution * fov / detail
   float fovf;              // fov (AO end distance = |camera - p| * fov)
+  FastDiv div_w, div_tx;   // divisions by width and tiles_x
 };
 
 // A surface hit, produced by stage P and completed by stages N and S.
@@ -101,6 +103,7 @@ struct Launch {
   int ao_rays;
   int shadow_tasks;        // 1 when the shadow march runs (shading && shadow)
   int want_normal;
+  FastDiv div_per;         // division by shadow_tasks + ao_rays (set by launch_pipeline)
 };
 
 __device__ __forceinline__ int job_of(const WJob *jobs, int n, long long idx) {
@@ -219,20 +222,32 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
     }
     if (!__any_sync(FULL, iterating)) break;
     const int k = drained ? 0 : refill_k;
-    // ---- formula iterations, two between votes, until <= k lanes still iterate
+    // ---- formula iterations, two between votes, until <= k lanes still iterate.
+    // A lane whose orbit ends leaves the loop by a branch, so the remaining
+    // lanes run the iteration without select instructions for finished ones;
+    // the vote counts the lanes still in the loop.
     const FastParams &fp = S.params();
     const int kind = S.kind();
-    do {
-#pragma unroll
-      for (int u = 0; u < 2; u++) {
-        if (iterating) {
-          iterate<FK>(kind, e.z, e.dr, e.c, fp, e.r2);
-          e.it++;
-          e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
-          if (!(e.r2 <= fp.bailout2) || e.it >= fp.maxN) iterating = false;
+    if (iterating) {
+      for (;;) {
+        iterate<FK>(kind, e.z, e.dr, e.c, fp, e.r2);
+        e.it++;
+        e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
+        if (!(e.r2 <= fp.bailout2) || e.it >= fp.maxN) {
+          iterating = false;
+          break;
         }
+        iterate<FK>(kind, e.z, e.dr, e.c, fp, e.r2);
+        e.it++;
+        e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
+        if (!(e.r2 <= fp.bailout2) || e.it >= fp.maxN) {
+          iterating = false;
+          break;
+        }
+        if (!more_than(__ballot_sync(__activemask(), 1), k)) break;
       }
-    } while (more_than(__ballot_sync(FULL, iterating), k));
+    }
+    __syncwarp();
     // ---- lanes whose estimate is done: distance, then the march step
     if (has && !iterating) {
       const bool bailed = e.r2 > fp.bailout2;
@@ -311,16 +326,18 @@ struct PrimaryStage {
       fp = L.fps[job];
       kd = fast_kind(fp);
     }
-    const long long local = idx - jb->first;
+    const unsigned long long local = (unsigned long long)(idx - jb->first);
     int x, y;
     if (L.layout == 1) {
-      const long long tile = local >> 5;
+      const unsigned long long tile = local >> 5;
       const int w = int(local & 31);
-      x = int(tile % jb->tiles_x) * 8 + (w & 7);
-      y = int(tile / jb->tiles_x) * 4 + (w >> 3);
+      const unsigned long long ty = fdiv(tile, jb->div_tx);
+      x = int(tile - ty * (unsigned long long)jb->tiles_x) * 8 + (w & 7);
+      y = int(ty) * 4 + (w >> 3);
     } else {
-      x = int(local % jb->width);
-      y = int(local / jb->width);
+      const unsigned long long yy = fdiv(local, jb->div_w);
+      x = int(local - yy * (unsigned long long)jb->width);
+      y = int(yy);
     }
     if (x >= jb->width || y >= jb->rows) return false;  // padding of the last tile row/column
     y += jb->row0;
@@ -610,8 +627,7 @@ struct ShadeStage {
   __device__ bool start(long long idx, float &qx, float &qy, float &qz) {
     const float4 dv = L.sdir[idx];
     if (dv.w == 0.0f) return false;  // resolved by the direction kernel
-    const int per = L.shadow_tasks + L.ao_rays;
-    const long long h = idx / per;
+    const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
     r = &L.hits[h];
     if (MULTI) {
       fp = L.fps[r->job];
@@ -677,7 +693,7 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
   const float vdm = float(fr.view_distance_max);
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
        idx += (long long)gridDim.x * blockDim.x) {
-    const long long h = idx / per;
+    const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
     const int k = int(idx - h * per);
     HitRec &r = L.hits[h];
     const float thr = r.thr;
@@ -792,6 +808,8 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.aspect = fr.aspect;
   j.c0 = float(fr.resolution * fr.fov / fr.detail_level);
   j.fovf = float(fr.fov);
+  j.div_w = make_fastdiv(j.width);
+  j.div_tx = make_fastdiv(j.tiles_x);
   return j;
 }
 
@@ -820,7 +838,9 @@ static int sm_count() {
 // The stage launches of one frame or batch, in stream order.
 template <bool MULTI>
 static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const DevFrame &fr, const FastParams &fp0,
-                           const WJob &j0, const Launch &L, const DevOutputs &out, long long pixels) {
+                           const WJob &j0, const Launch &L0, const DevOutputs &out, long long pixels) {
+  Launch L = L0;
+  L.div_per = make_fastdiv(std::max(1, L.shadow_tasks + L.ao_rays));
   const int sms = sm_count();
   const int grid = std::max(1, sms * tu.ctas_per_sm);
   const int block = tu.block_size;

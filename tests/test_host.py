@@ -3,6 +3,7 @@ construction, DE-function vote, bailout rules, camera set-up and argument
 validation.  CPU only."""
 import ctypes as C
 import math
+import os
 
 import numpy as np
 import pytest
@@ -123,3 +124,22 @@ def test_oracle_row_bands_compose(oracle):
     bot, _ = oracle.render(sc, cam, p, rows=(10, 24))
     for k in whole:
         assert np.array_equal(whole[k], np.concatenate([top[k], bot[k]])), k
+
+
+def test_fastdiv_exact(tmp_path):
+    """The multiply-high division of csrc/fastdiv.h equals integer division
+    for divisors 1..300, powers of two and their neighbours, 2^31-1, and
+    numerators up to 2^63-1 (edge cases, exact multiples, random)."""
+    import shutil
+    import subprocess
+
+    cxx = shutil.which("g++") or "/usr/bin/g++"
+    here = os.path.dirname(os.path.abspath(__file__))
+    csrc = os.path.join(os.path.dirname(here), "mandelbulber2_b200", "csrc")
+    exe = str(tmp_path / "fastdiv_check")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", csrc, os.path.join(here, "fastdiv_check.cpp"), "-o", exe],
+                   check=True)
+    out = subprocess.run([exe], capture_output=True, text=True)
+    bad, checked = map(int, out.stdout.split())
+    assert checked > 1_000_000
+    assert bad == 0 and out.returncode == 0
