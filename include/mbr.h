@@ -77,8 +77,16 @@ typedef enum mbr_engine {
   /* Persistent wavefront kernel: FP32 iteration, FP64 origin and t, per-lane
    * ray refill, re-convergence of finished lanes every k iterations. */
   MBR_ENGINE_WAVEFRONT_FP32 = 3,
-  /* The wavefront kernel with FP64 iteration (isolates scheduling gains). */
-  MBR_ENGINE_WAVEFRONT_FP64 = 4
+  /* The wavefront kernels with the formula iteration in FP64, in the
+   * reference's operation order, and the march arithmetic of the plain FP64
+   * kernel: for views whose hit threshold FP32 points cannot resolve. */
+  MBR_ENGINE_WAVEFRONT_FP64 = 4,
+  /* The wavefront kernels, FP32 or FP64 iteration chosen per frame (per job
+   * in a batch) on the device: FP64 when DE(camera) * (threshold per unit
+   * distance), a lower bound of the view's hit thresholds, is below 256 FP32
+   * units (2^-24) of the camera coordinates - deep zooms and cameras inside
+   * the solid. */
+  MBR_ENGINE_WAVEFRONT_AUTO = 5
 } mbr_engine;
 
 /* How the hit is refined after the march finds dist < threshold. */
@@ -290,8 +298,11 @@ typedef struct mbr_job {
 } mbr_job;
 
 /* Builds the job table for n_jobs renders of uneven size and captures the
- * launch into a CUDA graph.  Outputs are indexed pixel_offset + y*width + x.
- * engine must be a WAVEFRONT engine. */
+ * launch into a CUDA graph: one pipeline per formula kind and precision, each
+ * over its jobs with one persistent launch per stage.  Outputs are indexed
+ * pixel_offset + y*width + x.  engine must be a WAVEFRONT engine; with
+ * MBR_ENGINE_WAVEFRONT_AUTO the precision is chosen per job here (a
+ * synchronous device evaluation of DE at every camera). */
 mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_scenes,
                             const mbr_job *jobs, int32_t n_jobs,
                             const mbr_render_params *params, const mbr_outputs *out,
@@ -299,6 +310,10 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
 /* Replays the captured graph on `stream`. */
 mbr_status mbr_batch_launch(mbr_batch *batch, void *stream);
 void mbr_batch_destroy(mbr_batch *batch);
+/* Number of pipelines in the batch's graph (one per formula kind and
+ * precision) and, in *wide_jobs (may be NULL), how many jobs iterate in FP64;
+ * -1 for a NULL batch. */
+int32_t mbr_batch_groups(const mbr_batch *batch, int32_t *wide_jobs);
 
 /* Launch configuration of the wavefront kernel, chosen by the autotuner. */
 typedef struct mbr_tuning {

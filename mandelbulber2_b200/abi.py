@@ -25,8 +25,10 @@ FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
 # mbr_engine
-ENGINE_PLAIN_FP64, ENGINE_PLAIN_FP64_STRICT, ENGINE_PLAIN_MIXED, ENGINE_WAVEFRONT_FP32, ENGINE_WAVEFRONT_FP64 = range(5)
-ENGINE_NAMES = {0: "plain_fp64", 1: "plain_fp64_strict", 2: "plain_mixed", 3: "wavefront_fp32", 4: "wavefront_fp64"}
+ENGINE_PLAIN_FP64, ENGINE_PLAIN_FP64_STRICT, ENGINE_PLAIN_MIXED, ENGINE_WAVEFRONT_FP32, ENGINE_WAVEFRONT_FP64, \
+    ENGINE_WAVEFRONT_AUTO = range(6)
+ENGINE_NAMES = {0: "plain_fp64", 1: "plain_fp64_strict", 2: "plain_mixed", 3: "wavefront_fp32", 4: "wavefront_fp64",
+                5: "wavefront_auto"}
 # mbr_refine
 REFINE_REFERENCE, REFINE_ROOT = 0, 1
 # gradient slots
@@ -128,6 +130,7 @@ PROTOTYPES = {
                                    C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P, C.POINTER(_P)]),
     "mbr_batch_launch": (C.c_int, [_P, _P]),
     "mbr_batch_destroy": (None, [_P]),
+    "mbr_batch_groups": (C.c_int32, [_P, _P]),
     "mbr_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mbr_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mbr_autotune": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P,

@@ -664,6 +664,7 @@ mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_p
     case MBR_ENGINE_PLAIN_MIXED: e = launch_plain_mixed(ctx->scene, fr, d, stream); break;
     case MBR_ENGINE_WAVEFRONT_FP32:
     case MBR_ENGINE_WAVEFRONT_FP64:
+    case MBR_ENGINE_WAVEFRONT_AUTO:
       return render_wavefront(ctx, ctx->scene, fr, d, engine, stream);
     default: return set_err(ctx, MBR_EINVAL, "unknown engine %d", engine);
   }
@@ -694,6 +695,7 @@ mbr_status mbr_distance(mbr_ctx *ctx, const double *points, int64_t n, double de
   switch (engine) {
     case MBR_ENGINE_PLAIN_FP64:
     case MBR_ENGINE_WAVEFRONT_FP64:
+    case MBR_ENGINE_WAVEFRONT_AUTO:
       e = launch_distance_fp64(ctx->scene, points, n, detail_size, normal_mode, dist, iters, stream);
       break;
     case MBR_ENGINE_PLAIN_FP64_STRICT:

@@ -1,4 +1,4 @@
-// wavefront.cu - the batched FP32 form.
+// wavefront.cu - the batched wavefront form, with FP32 or FP64 iteration.
 //
 // A frame (or a batch of frames of uneven size) is rendered as a short
 // pipeline of persistent kernels, each over a homogeneous task space:
@@ -9,31 +9,47 @@
 //   stage N  one task per hit:    the six central-difference DE samples of
 //            CalculateNormals (src/shader_calculate_normals.cpp:40-125) and
 //            the Lambert term of LightShading (src/shader_light_shading.cpp:61-72)
+//   stage D  one thread per stage-S task: AO directions and start records
 //   stage S  (1 + ao_rays) tasks per hit: the hard AuxShadow march
 //            (src/shader_aux_shadow.cpp:94-321) and one AmbientOcclusion
 //            march per AO direction (src/shader_ambient_occlusion.cpp:60-110)
 //   stage F  one thread per hit: colour, 8-bit conversion, outputs
 //
-// Every march is a stream of distance requests p = origin + dir * t with t
-// and the origin in FP64 and the formula iteration in FP32.  In stages P, N
-// and S each lane holds one task; it runs two formula iterations between
-// warp votes and, once at most k lanes of the warp are still iterating, the
-// lanes whose estimate is done take their march step and start their next
-// request, or take the next task from the stage's device counter
-// (warp-aggregated atomicAdd).  Because a warp only ever runs one kind of
-// march, those steps stay converged and cheap, and divergent orbit lengths
-// and march lengths cost only the k-lane wait.  A batch walks a job table
-// (per-job camera, image size and formula parameters) with the same stages,
-// captured once into a CUDA graph.
+// Every march is a stream of distance requests p = origin + dir * t.  In
+// stages P, N and S each lane holds one task; it runs two formula iterations
+// between warp votes and, once at most k lanes of the warp are still
+// iterating, the lanes whose estimate is done take their march step and
+// start their next request, or take the next task from the stage's device
+// counter (warp-aggregated atomicAdd).  Because a warp only ever runs one
+// kind of march, those steps stay converged and cheap, and divergent orbit
+// lengths and march lengths cost only the k-lane wait.  A batch walks a job
+// table (per-job camera, image size and formula parameters) with the same
+// stages, captured once into a CUDA graph.
+//
+// Two precision policies share the stages:
+//   Prec32  the formula iteration in FP32 (fast_formula.cuh) with the ray
+//           origin, t and the refinement in FP64;
+//   Prec64  the formula iteration in FP64 in the reference's operation order
+//           (de_core.cuh) with the march arithmetic of the plain FP64 kernel.
+// FP32 points resolve distances down to about 2^-24 of their coordinates;
+// where the hit threshold of a view is not well above that (deep zooms, a
+// camera inside the solid) the FP32 estimate is noise at the scale the march
+// needs.  MBR_ENGINE_WAVEFRONT_AUTO chooses the policy per frame (per job in a
+// batch) from the distance estimate at the camera: no ray meets the surface
+// closer than that distance, so DE(camera) * threshold-per-unit-distance
+// bounds the smallest hit threshold of the view from below.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
+#include "de_core.cuh"
 #include "fast_formula.cuh"
 #include "fastdiv.h"
 #include "mbr_internal.h"
@@ -43,6 +59,12 @@ namespace mbr {
 
 // formula kinds of the iteration switch
 enum { FK_ANY = 0, FK_BULB = 2, FK_MENGER = 7, FK_BOX = 8, FK_BOX_SIMPLE = 108 };
+
+// Views whose smallest hit threshold is below this many FP32 units (2^-24)
+// of the camera coordinates iterate in FP64 under MBR_ENGINE_WAVEFRONT_AUTO.
+// The FP32 depth error grows about as 0.01 / (threshold in FP32 units); 256
+// keeps it near 1e-4 relative at the 99th percentile.
+const double kWideRatio = 256.0;
 
 // One render job of a launch: its camera, image size and place in the queue.
 struct WJob {
@@ -54,6 +76,7 @@ struct WJob {
   long long first;         // first work item of this job in the pixel queue
   long long pixel_offset;  // first pixel of this job in the outputs
   double fov, aspect;
+  double resolution, detail;  // CalcDistThresh factors (1/height, detail level)
   float c0;                // threshold per unit distance: resolution * fov / detail
   float fovf;              // fov (AO end distance = |camera - p| * fov)
   FastDiv div_w, div_tx;   // divisions by width and tiles_x
@@ -63,22 +86,21 @@ struct WJob {
 struct HitRec {
   double px, py, pz;  // hit point
   double depth;       // scan distance t of the hit
+  double thr;         // distThresh at the hit
   long long pix;      // output index
-  float thr;          // distThresh at the hit
   int iters;          // iters of the last primary DE evaluation
   float nx, ny, nz;   // normal
   float shade;        // Lambert term before the shadow
   float shadow;       // AuxShadow result
   int job;
   unsigned int ray;   // pixel index within its job (RNG streams)
-  int pad;
   // sum of the AO march results in 32.32 fixed point: integer atomics make
   // the sum independent of the order in which the AO marches finish
   unsigned long long ao_q;
 };
 
-__device__ __forceinline__ void ao_add(HitRec *r, float s) {
-  atomicAdd(&r->ao_q, (unsigned long long)(double(s) * 4294967296.0));
+__device__ __forceinline__ void ao_add(HitRec *r, double s) {
+  atomicAdd(&r->ao_q, (unsigned long long)(s * 4294967296.0));
 }
 
 // Device-side counters of one launch (in the context's scratch).
@@ -89,15 +111,48 @@ struct Counters4 {
   unsigned long long shade_next;   // stage S queue
 };
 
+// FP64 parameters of a non-hybrid formula: the slot's double parameters, read
+// by the reference-order formulas of de_core.cuh, and the Compute settings.
+struct WideParams {
+  DevSlot slot;
+  int formula, maxN, de_fn, min_n;
+  int julia, add_c, check_bailout, pad;
+  double bailout;
+  double jc[3];  // julia_c * fractal_constant_factor
+  double cm[3];  // fractal_constant_factor
+};
+
+__host__ __device__ inline WideParams load_wide_params(const DevScene &sc) {
+  WideParams w;
+  w.slot = sc.slot[0];
+  w.formula = sc.slot[0].formula;
+  w.maxN = sc.formula_maxiter;
+  w.de_fn = sc.de_analytic;
+  w.min_n = sc.min_n;
+  w.julia = sc.julia;
+  w.add_c = sc.slot[0].add_c;
+  w.check_bailout = sc.slot[0].check_bailout;
+  w.pad = 0;
+  w.bailout = sc.slot[0].d[P_BAILOUT];
+  for (int k = 0; k < 3; k++) {
+    w.jc[k] = sc.julia_c[k] * sc.cmul[k];
+    w.cm[k] = sc.cmul[k];
+  }
+  return w;
+}
+
 struct Launch {
   const WJob *jobs;        // njobs entries (device)
-  const FastParams *fps;   // per job (device)
+  const FastParams *fps;   // per job (device), FP32 policy
+  const WideParams *wps;   // per job (device), FP64 policy
   int njobs;
   long long total;         // pixel work items
   HitRec *hits;            // capacity: total
   float4 *sorg;            // per hit: FP32 hit point and threshold (stage S origins)
   float4 *sdir;            // per stage-S task: direction and end (w < 0: shadow, w == 0: no march)
   Counters4 *ctr;
+  const int *gate;         // MBR_ENGINE_WAVEFRONT_AUTO: the policy flag; null: always run
+  int gate_value;          // the flag value this pipeline runs under (0 FP32, 1 FP64)
   int refill_k;
   int layout;
   int ao_rays;
@@ -105,6 +160,10 @@ struct Launch {
   int want_normal;
   FastDiv div_per;         // division by shadow_tasks + ao_rays (set by launch_pipeline)
 };
+
+// True when this pipeline's kernels have nothing to do (the other precision
+// renders the frame).
+__device__ __forceinline__ bool gated_off(const Launch &L) { return L.gate && *L.gate != L.gate_value; }
 
 __device__ __forceinline__ int job_of(const WJob *jobs, int n, long long idx) {
   int lo = 0, hi = n - 1;
@@ -122,14 +181,14 @@ __host__ __device__ inline int fast_kind(const FastParams &f) {
   return FK_MENGER;
 }
 
-template <int FK>
-__device__ __forceinline__ void iterate(int kind, Z3 &z, float &dr, const Z3 &c, const FastParams &f, float r2) {
-  const int k = (FK == FK_ANY) ? kind : FK;
-  if (k == FK_BOX_SIMPLE) it_mandelbox<true>(z, dr, c, f);
-  else if (k == FK_BOX) it_mandelbox<false>(z, dr, c, f);
-  else if (k == FK_BULB) it_mandelbulb(z, dr, c, f, sqrtf(r2));
-  else it_menger(z, dr, c, f);
+__host__ __device__ inline int wide_kind(const WideParams &w) {
+  if (w.formula == MBR_FORMULA_MANDELBOX) return FK_BOX;
+  if (w.formula == MBR_FORMULA_MANDELBULB) return FK_BULB;
+  return FK_MENGER;
 }
+
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return fma(a, b, c); }
 
 // True when more than k bits of m are set.  k <= 2 takes the lowest set bit
 // off on the ALU pipe instead of a POPC on the (eighth-rate) XU pipe.
@@ -143,55 +202,161 @@ __device__ __forceinline__ bool more_than(unsigned m, int k) {
   return __popc(m) > k;
 }
 
-// Per-lane state of one distance estimate.
-struct DE {
-  Z3 z, c;
-  float dr, r2;
-  int it;
+// ============================================================================
+// Precision policies: the per-lane state of one distance estimate, its
+// start, one formula iteration and the final distance.
+// ============================================================================
+struct Prec32 {
+  typedef float D;  // distance and threshold arithmetic of the march
+  typedef FastParams Params;
+  enum { kWide = 0 };
+  struct State {
+    Z3 z, c;
+    float dr, r2;
+    int it;
+  };
+  __host__ __device__ static int kind(const Params &f) { return fast_kind(f); }
+  __device__ static const Params &job_params(const Launch &L, int job) { return L.fps[job]; }
+
+  __device__ static void start(State &e, const Params &fp, float qx, float qy, float qz) {
+    e.z.x = qx;
+    e.z.y = qy;
+    e.z.z = qz;
+    if (!fp.add_c) e.c = Z3{0.f, 0.f, 0.f};
+    else if (fp.julia) e.c = Z3{fp.jc_x, fp.jc_y, fp.jc_z};
+    else e.c = Z3{qx * fp.cm_x, qy * fp.cm_y, qz * fp.cm_z};
+    e.dr = 1.f;
+    e.it = 0;
+    e.r2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
+  }
+  __device__ static void start(State &e, const Params &fp, double qx, double qy, double qz) {
+    start(e, fp, float(qx), float(qy), float(qz));
+  }
+
+  // One iteration; false once the orbit is done (bailout or maxN).
+  template <int FK>
+  __device__ static bool step(int kind, State &e, const Params &fp) {
+    const int k = (FK == FK_ANY) ? kind : FK;
+    if (k == FK_BOX_SIMPLE) it_mandelbox<true>(e.z, e.dr, e.c, fp);
+    else if (k == FK_BOX) it_mandelbox<false>(e.z, e.dr, e.c, fp);
+    else if (k == FK_BULB) it_mandelbulb(e.z, e.dr, e.c, fp, sqrtf(e.r2));
+    else it_menger(e.z, e.dr, e.c, fp);
+    e.it++;
+    e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
+    return e.r2 <= fp.bailout2 && e.it < fp.maxN;
+  }
+
+  __device__ static float distance(const State &e, const Params &fp, float detail, int &iters) {
+    iters = (e.r2 > fp.bailout2) ? e.it : e.it + 1;
+    return final_de(fp, e.r2, e.dr, iters, detail);
+  }
 };
 
-__device__ __forceinline__ void de_start(DE &e, const FastParams &fp, double qx, double qy, double qz) {
-  e.z.x = float(qx);
-  e.z.y = float(qy);
-  e.z.z = float(qz);
-  if (!fp.add_c) e.c = Z3{0.f, 0.f, 0.f};
-  else if (fp.julia) e.c = Z3{fp.jc_x, fp.jc_y, fp.jc_z};
-  else e.c = Z3{e.z.x * fp.cm_x, e.z.y * fp.cm_y, e.z.z * fp.cm_z};
-  e.dr = 1.f;
-  e.it = 0;
-  e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
-}
+struct Prec64 {
+  typedef double D;
+  typedef WideParams Params;
+  enum { kWide = 1 };
+  struct State {
+    double zx, zy, zz, cx, cy, cz, dr, r;
+    int it, brk;  // iterations done; 1 when the loop ended by a break (bailout or NaN)
+  };
+  __host__ __device__ static int kind(const Params &w) { return wide_kind(w); }
+  __device__ static const Params &job_params(const Launch &L, int job) { return L.wps[job]; }
 
-__device__ __forceinline__ void de_start(DE &e, const FastParams &fp, float qx, float qy, float qz) {
-  e.z.x = qx;
-  e.z.y = qy;
-  e.z.z = qz;
-  if (!fp.add_c) e.c = Z3{0.f, 0.f, 0.f};
-  else if (fp.julia) e.c = Z3{fp.jc_x, fp.jc_y, fp.jc_z};
-  else e.c = Z3{qx * fp.cm_x, qy * fp.cm_y, qz * fp.cm_z};
-  e.dr = 1.f;
-  e.it = 0;
-  e.r2 = fmaf(qx, qx, fmaf(qy, qy, qz * qz));
-}
+  // Compute's start (compute_fractal.cpp:74-130): z = c = the point, DE = 1
+  __device__ static void start(State &e, const Params &, double qx, double qy, double qz) {
+    e.zx = qx;
+    e.zy = qy;
+    e.zz = qz;
+    e.cx = qx;
+    e.cy = qy;
+    e.cz = qz;
+    e.dr = 1.0;
+    e.r = len4<double, false>(V4<double>{qx, qy, qz, 0.0});
+    e.it = 0;
+    e.brk = 0;
+  }
+
+  // One pass of the Compute loop body for a non-hybrid scene, as
+  // calc_distance<double, F, false> runs it (compute_fractal.cpp:170-321).
+  template <int FK>
+  __device__ static bool step(int kind, State &e, const Params &fp) {
+    const int k = (FK == FK_ANY) ? kind : FK;
+    V4<double> z{e.zx, e.zy, e.zz, 0.0};
+    const V4<double> last = z;
+    double de = e.dr;
+    if (k == FK_BULB) f_mandelbulb<double>(z, e.r, de, fp.slot);
+    else if (k == FK_MENGER) f_menger<double, false>(z, de, fp.slot);
+    else f_mandelbox<double, false>(z, de, fp.slot);
+    if (fp.add_c) {
+      if (fp.julia) {
+        z.x = z.x + fp.jc[0];
+        z.y = z.y + fp.jc[1];
+        z.z = z.z + fp.jc[2];
+      } else {
+        z.x = z.x + e.cx * fp.cm[0];
+        z.y = z.y + e.cy * fp.cm[1];
+        z.z = z.z + e.cz * fp.cm[2];
+      }
+    }
+    e.it++;
+    e.dr = de;
+    if (nan4<double, false>(z)) {  // revert to the last finite orbit point
+      e.zx = last.x;
+      e.zy = last.y;
+      e.zz = last.z;
+      e.r = len4<double, false>(last);
+      e.brk = 1;
+      return false;
+    }
+    e.zx = z.x;
+    e.zy = z.y;
+    e.zz = z.z;
+    e.r = len4<double, false>(z);
+    if (fp.check_bailout && e.r > fp.bailout) {
+      e.brk = 1;
+      return false;
+    }
+    return e.it < fp.maxN;
+  }
+
+  // Final DE and CalculateDistanceSimple's clamps (compute_fractal.cpp:561-621,
+  // calculate_distance.cpp:569, 604-605).
+  __device__ static double distance(const State &e, const Params &fp, double detail, int &iters) {
+    iters = e.brk ? e.it : e.it + 1;
+    const double r = e.r, DE = e.dr;
+    double d;
+    if (DE > 0.0) {
+      if (fp.de_fn == 2) d = (r > 1.0) ? 0.5 * r * log(r) / DE : 0.0;
+      else if (fp.de_fn == 1) d = r / DE;
+      else if (fp.de_fn == 3) d = (r - 2.0) / DE;
+      else d = r;
+    } else {
+      d = r;
+    }
+    if (iters < fp.min_n && d < detail) d = detail;
+    if (d < 0.0) d = 0.0;
+    if (d > 10.0) d = 10.0;
+    return d;
+  }
+};
 
 // ============================================================================
 // The persistent skeleton: refill lanes from a task counter, iterate, step.
-// Stage provides (Real: the precision of its request points):
+// Stage provides (Real: the precision of its request points, D: of its distances):
 //   bool start(long long task, Real &qx, &qy, &qz)   - first request (false: nothing to march)
-//   bool step(float d, int iters, Real &qx, &qy, &qz) - consume a result; true: next request
-//   const FastParams &params()  - formula of the current task
-//   int kind()                  - formula kind (FK_ANY launches)
+//   bool step(D d, int iters, Real &qx, &qy, &qz)    - consume a result; true: next request
+//   const Params &params()  - formula of the current task
+//   int kind()              - formula kind (FK_ANY launches)
+//   D detail()              - detail size of the current request
 // ============================================================================
-template <int FK, class Stage>
+template <int FK, class P, class Stage>
 __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter, long long total, int refill_k,
                                           unsigned int *my_de, unsigned long long *my_iters) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lanemask_lt = (1u << lane) - 1u;
-  DE e;
-  e.it = 0;
-  e.r2 = 0.f;
-  e.dr = 1.f;
+  typename P::State e = {};
   bool has = false, iterating = false, drained = false;
   unsigned int de_n = 0;
   unsigned long long it_n = 0;
@@ -209,7 +374,7 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
         if (idx < total) {
           typename Stage::Real qx, qy, qz;
           if (S.start(idx, qx, qy, qz)) {
-            de_start(e, S.params(), qx, qy, qz);
+            P::start(e, S.params(), qx, qy, qz);
             has = true;
             iterating = true;
           }
@@ -226,21 +391,15 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
     // A lane whose orbit ends leaves the loop by a branch, so the remaining
     // lanes run the iteration without select instructions for finished ones;
     // the vote counts the lanes still in the loop.
-    const FastParams &fp = S.params();
+    const typename P::Params &fp = S.params();
     const int kind = S.kind();
     if (iterating) {
       for (;;) {
-        iterate<FK>(kind, e.z, e.dr, e.c, fp, e.r2);
-        e.it++;
-        e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
-        if (!(e.r2 <= fp.bailout2) || e.it >= fp.maxN) {
+        if (!P::template step<FK>(kind, e, fp)) {
           iterating = false;
           break;
         }
-        iterate<FK>(kind, e.z, e.dr, e.c, fp, e.r2);
-        e.it++;
-        e.r2 = fmaf(e.z.x, e.z.x, fmaf(e.z.y, e.z.y, e.z.z * e.z.z));
-        if (!(e.r2 <= fp.bailout2) || e.it >= fp.maxN) {
+        if (!P::template step<FK>(kind, e, fp)) {
           iterating = false;
           break;
         }
@@ -250,14 +409,13 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
     __syncwarp();
     // ---- lanes whose estimate is done: distance, then the march step
     if (has && !iterating) {
-      const bool bailed = e.r2 > fp.bailout2;
-      const int iters = bailed ? e.it : e.it + 1;
-      const float d = final_de(fp, e.r2, e.dr, iters, S.detail());
+      int iters;
+      const typename P::D d = P::distance(e, fp, S.detail(), iters);
       de_n++;
       it_n += (unsigned long long)iters;
       typename Stage::Real qx, qy, qz;
       if (S.step(d, iters, qx, qy, qz)) {
-        de_start(e, S.params(), qx, qy, qz);
+        P::start(e, S.params(), qx, qy, qz);
         iterating = true;
       } else {
         has = false;
@@ -291,40 +449,71 @@ __device__ __forceinline__ void flush_counts(const DevOutputs &out, unsigned int
 // ============================================================================
 // Stage P: primary march with binary refinement, one task per pixel.
 // ============================================================================
-template <bool MULTI>
+template <bool MULTI, class P>
 struct PrimaryStage {
   typedef double Real;
+  typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
   const DevOutputs &out;
   const WJob *jb;
-  FastParams fp;
+  typename P::Params fp;
   int kd;
   int job;
   // ray
-  double dx, dy, dz, ox, oy, oz, t, stp;
-  float thr, c0, dist_prev, search_limit;
+  double dx, dy, dz, ox, oy, oz, t, stp, dir_len;
+  double lx, ly, lz;  // previous request point (dead-ray check)
+  D thr, c0, dist_prev, search_limit;
   int phase, sub, count, last_iters;
   unsigned int pm, ray, binary_de;
   long long pix;
 
-  __device__ const FastParams &params() const { return fp; }
+  __device__ const typename P::Params &params() const { return fp; }
   __device__ int kind() const { return kd; }
-  __device__ float detail() const { return thr; }
+  __device__ D detail() const { return thr; }
+
+  // distThresh at the request point (render_worker.cpp:653-679): FP64 from
+  // |camera - q| as the plain kernel computes it; FP32 from t
+  __device__ void set_thr(double qx, double qy, double qz) {
+    if (fr.constant_de_threshold) {
+      thr = D(fr.de_thresh);
+    } else if (P::kWide) {
+      const double ax = jb->cam[0] - qx, ay = jb->cam[1] - qy, az = jb->cam[2] - qz;
+      const double l = sqrt(ax * ax + ay * ay + az * az);
+      thr = D(l * jb->resolution * jb->fov / jb->detail);
+    } else {
+      thr = D(float(t) * float(c0));
+    }
+  }
 
   __device__ void point(double &qx, double &qy, double &qz) {
-    thr = fr.constant_de_threshold ? float(fr.de_thresh) : float(t) * c0;
     qx = fma(dx, t, ox);
     qy = fma(dy, t, oy);
     qz = fma(dz, t, oz);
+    set_thr(qx, qy, qz);
+  }
+
+  // The next march point; false when the ray is stuck: the point did not
+  // move or is not finite (render_worker.cpp:747-756).
+  __device__ bool advance(double &qx, double &qy, double &qz) {
+    const double nx = fma(dx, t, ox), ny = fma(dy, t, oy), nz = fma(dz, t, oz);
+    if ((nx == lx && ny == ly && nz == lz) || !(isfinite(nx) && isfinite(ny) && isfinite(nz))) return false;
+    lx = nx;
+    ly = ny;
+    lz = nz;
+    qx = nx;
+    qy = ny;
+    qz = nz;
+    set_thr(qx, qy, qz);
+    return true;
   }
 
   __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
     if (MULTI) {
       job = job_of(L.jobs, L.njobs, idx);
       jb = &L.jobs[job];
-      fp = L.fps[job];
-      kd = fast_kind(fp);
+      fp = P::job_params(L, job);
+      kd = P::kind(fp);
     }
     const unsigned long long local = (unsigned long long)(idx - jb->first);
     int x, y;
@@ -364,18 +553,24 @@ struct PrimaryStage {
     dx = vx * n;
     dy = vy * n;
     dz = vz * n;
+    dir_len = sqrt(dx * dx + dy * dy + dz * dz);
     ox = jb->cam[0];
     oy = jb->cam[1];
     oz = jb->cam[2];
-    c0 = jb->c0;
+    c0 = D(jb->c0);
     t = 0.0;
     stp = 0.0;
     phase = 0;
     sub = 0;
     count = 0;
     last_iters = 0;
+    thr = D(0);
+    lx = ly = lz = 1e30;
     if (fr.jitter) pm = pm_for_ray(ray, fr.seed).s;
-    point(qx, qy, qz);
+    if (!advance(qx, qy, qz)) {  // a camera that is not finite: stuck at once
+      write_hit();
+      return false;
+    }
     return true;
   }
 
@@ -407,7 +602,7 @@ struct PrimaryStage {
     r.pz = fma(dz, t, oz);
     r.depth = t;
     r.pix = pix;
-    r.thr = thr;
+    r.thr = double(thr);
     r.iters = last_iters;
     r.nx = 1.f;
     r.ny = 0.f;
@@ -431,7 +626,7 @@ struct PrimaryStage {
     return true;
   }
 
-  __device__ bool step(float d, int iters, double &qx, double &qy, double &qz) {
+  __device__ bool step(D d, int iters, double &qx, double &qy, double &qz) {
     last_iters = iters;
     if (phase == 1) {
       binary_de++;
@@ -455,50 +650,61 @@ struct PrimaryStage {
       jit = 1.0 - p.random(1000) / 10000.0;
       pm = p.s;
     }
-    stp = double((d - 0.5f * thr) * float(fr.de_factor)) * jit;
-    if (stp > 3.0) stp = 3.0;
-    t += stp;
+    if (P::kWide) {
+      stp = (double(d) - 0.5 * double(thr)) * fr.de_factor * jit;
+      if (stp > 3.0) stp = 3.0;
+      t += stp / dir_len;
+    } else {
+      stp = double((float(d) - 0.5f * float(thr)) * float(fr.de_factor)) * jit;
+      if (stp > 3.0) stp = 3.0;
+      t += stp;
+    }
     if (t > fr.view_distance_max || count >= fr.max_steps) {
       write_miss();
       return false;
     }
-    point(qx, qy, qz);
+    if (!advance(qx, qy, qz)) {  // stuck: a hit where it stands, without refinement
+      write_hit();
+      return false;
+    }
     return true;
   }
 };
 
-template <int FK, bool MULTI>
+template <int FK, bool MULTI, class P>
 __global__ void __launch_bounds__(256) primary_kernel(const __grid_constant__ DevFrame fr,
-                                                      const __grid_constant__ FastParams fp0,
+                                                      const __grid_constant__ typename P::Params fp0,
                                                       const __grid_constant__ WJob job0,
                                                       const __grid_constant__ Launch L, DevOutputs out) {
-  PrimaryStage<MULTI> S{fr, L, out, &job0, fp0, fast_kind(fp0), 0};
-  S.search_limit = float(1.0 - 0.001 * fr.detail_level);
+  if (gated_off(L)) return;
+  PrimaryStage<MULTI, P> S{fr, L, out, &job0, fp0, P::kind(fp0), 0};
+  S.search_limit = typename P::D(1.0 - 0.001 * fr.detail_level);
   S.binary_de = 0;
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
-  run_stage<FK>(S, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_MARCH, my_de - S.binary_de, K_BINARY, S.binary_de);
 }
 
 // ============================================================================
 // Stage N: normals + Lambert term, one task per hit.
 // ============================================================================
-template <bool MULTI>
+template <bool MULTI, class P>
 struct NormalStage {
   typedef double Real;
+  typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
-  FastParams fp;
+  typename P::Params fp;
   int kd;
   HitRec *r;
   double ox, oy, oz, delta;
-  float thr, nx, ny, nz;
+  D thr, nx, ny, nz;
   int sub;
 
-  __device__ const FastParams &params() const { return fp; }
+  __device__ const typename P::Params &params() const { return fp; }
   __device__ int kind() const { return kd; }
-  __device__ float detail() const { return thr; }
+  __device__ D detail() const { return thr; }
 
   __device__ void point(double &qx, double &qy, double &qz) {
     const double dd = (sub & 1) ? -delta : delta;
@@ -511,24 +717,24 @@ struct NormalStage {
   __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
     r = &L.hits[idx];
     if (MULTI) {
-      fp = L.fps[r->job];
-      kd = fast_kind(fp);
+      fp = P::job_params(L, r->job);
+      kd = P::kind(fp);
     }
     ox = r->px;
     oy = r->py;
     oz = r->pz;
-    thr = r->thr;
-    delta = double(thr) * fr.smoothness;
+    thr = D(r->thr);
+    delta = r->thr * fr.smoothness;
     sub = 0;
-    nx = ny = nz = 0.f;
+    nx = ny = nz = D(0);
     point(qx, qy, qz);
     return true;
   }
 
-  __device__ bool step(float d, int, double &qx, double &qy, double &qz) {
+  __device__ bool step(D d, int, double &qx, double &qy, double &qz) {
     const bool neg = (sub & 1) != 0;
     const int axis = sub >> 1;
-    float &comp = (axis == 0) ? nx : ((axis == 1) ? ny : nz);
+    D &comp = (axis == 0) ? nx : ((axis == 1) ? ny : nz);
     comp = neg ? comp - d : d;
     sub++;
     if (sub < 6) {
@@ -536,26 +742,51 @@ struct NormalStage {
       return true;
     }
     // CalculateNormals tail (shader_calculate_normals.cpp:111-123)
-    if (fabsf(nx) < 1e-30f && fabsf(ny) < 1e-30f && fabsf(nz) < 1e-30f) {
-      nx = 1.f;
-      ny = nz = 0.f;
-    } else {
-      const float inv = rsqrtf(nx * nx + ny * ny + nz * nz);
-      nx *= inv;
-      ny *= inv;
-      nz *= inv;
-    }
-    if (!(isfinite(nx) && isfinite(ny) && isfinite(nz))) {
-      nx = 1.f;
-      ny = nz = 0.f;
-    }
-    r->nx = nx;
-    r->ny = ny;
-    r->nz = nz;
-    // LightShading, directional light (shader_light_shading.cpp:61-72)
+    float fx, fy, fz;
     float s = 0.f;
+    if (P::kWide) {
+      double ux = double(nx), uy = double(ny), uz = double(nz);
+      if (fabs(ux) < 1e-50 && fabs(uy) < 1e-50 && fabs(uz) < 1e-50) {
+        ux = 1.0;
+        uy = uz = 0.0;
+      } else {
+        const double inv = 1.0 / sqrt(ux * ux + uy * uy + uz * uz);
+        ux *= inv;
+        uy *= inv;
+        uz *= inv;
+      }
+      if (!(isfinite(ux) && isfinite(uy) && isfinite(uz))) {
+        ux = 1.0;
+        uy = uz = 0.0;
+      }
+      fx = float(ux);
+      fy = float(uy);
+      fz = float(uz);
+      if (fr.shading_enable) s = float(ux * fr.light[0] + uy * fr.light[1] + uz * fr.light[2]);
+    } else {
+      fx = float(nx);
+      fy = float(ny);
+      fz = float(nz);
+      if (fabsf(fx) < 1e-30f && fabsf(fy) < 1e-30f && fabsf(fz) < 1e-30f) {
+        fx = 1.f;
+        fy = fz = 0.f;
+      } else {
+        const float inv = rsqrtf(fx * fx + fy * fy + fz * fz);
+        fx *= inv;
+        fy *= inv;
+        fz *= inv;
+      }
+      if (!(isfinite(fx) && isfinite(fy) && isfinite(fz))) {
+        fx = 1.f;
+        fy = fz = 0.f;
+      }
+      if (fr.shading_enable) s = fx * float(fr.light[0]) + fy * float(fr.light[1]) + fz * float(fr.light[2]);
+    }
+    r->nx = fx;
+    r->ny = fy;
+    r->nz = fz;
+    // LightShading, directional light (shader_light_shading.cpp:61-72)
     if (fr.shading_enable) {
-      s = nx * float(fr.light[0]) + ny * float(fr.light[1]) + nz * float(fr.light[2]);
       if (s < 0) s = 0;
       s = 1.0f - fr.material_shading + s * fr.material_shading;
       s = s * fr.light_intensity;
@@ -566,15 +797,16 @@ struct NormalStage {
   }
 };
 
-template <int FK, bool MULTI>
+template <int FK, bool MULTI, class P>
 __global__ void __launch_bounds__(256) normal_kernel(const __grid_constant__ DevFrame fr,
-                                                     const __grid_constant__ FastParams fp0,
+                                                     const __grid_constant__ typename P::Params fp0,
                                                      const __grid_constant__ Launch L, DevOutputs out) {
-  NormalStage<MULTI> S{fr, L, fp0, fast_kind(fp0)};
+  if (gated_off(L)) return;
+  NormalStage<MULTI, P> S{fr, L, fp0, P::kind(fp0)};
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
   const long long total = (long long)L.ctr->hits;
-  run_stage<FK>(S, &L.ctr->normals_next, total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, &L.ctr->normals_next, total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_NORMAL, my_de, K_NORMAL, 0);
 }
 
@@ -599,78 +831,96 @@ __device__ __forceinline__ unsigned long long pcg_advance(unsigned long long sta
   return acc_mult * state + acc_plus;
 }
 
-template <bool MULTI>
+// The secondary marches run in the policy's precision: FP32 from the FP64
+// hit point rounded once (no FP64 conversions in the loop), or FP64 from the
+// hit point itself.  Their hit test uses the float-rounded distThresh, as the
+// reference's shaders do.
+template <bool MULTI, class P>
 struct ShadeStage {
-  // secondary rays start at the FP64 hit point, rounded once to FP32; their
-  // march runs in FP32 (no FP64 conversions in the loop)
-  typedef float Real;
+  typedef typename P::D Real;
+  typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
-  FastParams fp;
+  typename P::Params fp;
   int kd;
   HitRec *r;
-  float ox, oy, oz, t;
-  float dx, dy, dz, thr, end, vdm, dfac;
+  D ox, oy, oz, t;
+  D dx, dy, dz, end, vdm, dfac;
+  float thr;
   int count, mode;  // mode 0 shadow, 1 AO
   unsigned int shadow_de;
 
-  __device__ const FastParams &params() const { return fp; }
+  __device__ const typename P::Params &params() const { return fp; }
   __device__ int kind() const { return kd; }
-  __device__ float detail() const { return thr; }
+  __device__ D detail() const { return D(thr); }
 
-  __device__ void point(float &qx, float &qy, float &qz) {
-    qx = fmaf(dx, t, ox);
-    qy = fmaf(dy, t, oy);
-    qz = fmaf(dz, t, oz);
+  __device__ void point(D &qx, D &qy, D &qz) {
+    qx = fmadd(dx, t, ox);
+    qy = fmadd(dy, t, oy);
+    qz = fmadd(dz, t, oz);
   }
 
-  __device__ bool start(long long idx, float &qx, float &qy, float &qz) {
+  __device__ bool start(long long idx, D &qx, D &qy, D &qz) {
     const float4 dv = L.sdir[idx];
     if (dv.w == 0.0f) return false;  // resolved by the direction kernel
     const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
     r = &L.hits[h];
     if (MULTI) {
-      fp = L.fps[r->job];
-      kd = fast_kind(fp);
+      fp = P::job_params(L, r->job);
+      kd = P::kind(fp);
     }
-    const float4 o = L.sorg[h];
-    ox = o.x;
-    oy = o.y;
-    oz = o.z;
-    thr = o.w;
-    dx = dv.x;
-    dy = dv.y;
-    dz = dv.z;
+    if (P::kWide) {
+      ox = D(r->px);
+      oy = D(r->py);
+      oz = D(r->pz);
+      thr = float(r->thr);
+      t = D(r->thr);
+    } else {
+      const float4 o = L.sorg[h];
+      ox = D(o.x);
+      oy = D(o.y);
+      oz = D(o.z);
+      thr = o.w;
+      t = D(thr);
+    }
+    dx = D(dv.x);
+    dy = D(dv.y);
+    dz = D(dv.z);
     mode = dv.w < 0.0f ? 0 : 1;
-    end = mode ? dv.w : vdm;
+    end = mode ? D(dv.w) : vdm;
     count = 0;
-    t = thr;
     point(qx, qy, qz);
     return true;
   }
 
-  __device__ bool step(float d, int, float &qx, float &qy, float &qz) {
+  __device__ bool step(D d, int, D &qx, D &qy, D &qz) {
     count++;
     if (mode == 0) {
       shadow_de++;
-      if (d < thr) {
+      if (d < D(thr)) {
         r->shadow = 0.f;
         return false;
       }
-      t += fmaxf(fminf(d, 1e6f) * dfac, 1e-15f);
+      if (P::kWide) t += fmax(fmin(double(d), 1e6) * double(dfac), 1e-15);
+      else t += fmaxf(fminf(float(d), 1e6f) * float(dfac), 1e-15f);
       if (count > fr.max_steps || t >= vdm) {
         r->shadow = 1.f;
         return false;
       }
     } else {
-      if (d < thr) {
-        const float s = 1.0f - __fdividef(end - t, end);
-        ao_add(r, fmaxf(s, 0.0f));
+      if (d < D(thr)) {
+        if (P::kWide) {
+          const double s = 1.0 - (double(end) - double(t)) / double(end);
+          ao_add(r, fmax(s, 0.0));
+        } else {
+          const float s = 1.0f - __fdividef(float(end) - float(t), float(end));
+          ao_add(r, double(fmaxf(s, 0.0f)));
+        }
         return false;
       }
-      t = fmaf(2.0f, d, t);
+      t = fmadd(D(2), d, t);
       if (t >= end || count >= fr.max_steps) {
-        ao_add(r, 1.0f);
+        ao_add(r, 1.0);
         return false;
       }
     }
@@ -687,6 +937,7 @@ struct ShadeStage {
 template <bool MULTI>
 __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ DevFrame fr,
                                                         const __grid_constant__ Launch L) {
+  if (gated_off(L)) return;
   const long long nh = (long long)L.ctr->hits;
   const int per = L.shadow_tasks + L.ao_rays;
   const long long n = nh * per;
@@ -696,7 +947,7 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
     const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
     const int k = int(idx - h * per);
     HitRec &r = L.hits[h];
-    const float thr = r.thr;
+    const float thr = float(r.thr);
     if (k == 0) L.sorg[h] = make_float4(float(r.px), float(r.py), float(r.pz), thr);
     float4 dv;
     if (k < L.shadow_tasks) {
@@ -724,7 +975,7 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
       const float b = nx * ny * aa;
       const float end = float(r.depth) * (MULTI ? L.jobs[r.job].fovf : float(fr.fov));
       if (!(thr < end)) {
-        ao_add(&r, 1.0f);  // no room to march: unoccluded
+        ao_add(&r, 1.0);  // no room to march: unoccluded
         dv = make_float4(0.f, 0.f, 0.f, 0.f);
       } else {
         dv = make_float4(fmaf(1.0f + sg * nx * nx * aa, lx, fmaf(b, ly, nx * lz)),
@@ -736,18 +987,19 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
   }
 }
 
-template <int FK, bool MULTI>
+template <int FK, bool MULTI, class P>
 __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ DevFrame fr,
-                                                    const __grid_constant__ FastParams fp0,
+                                                    const __grid_constant__ typename P::Params fp0,
                                                     const __grid_constant__ Launch L, DevOutputs out) {
-  ShadeStage<MULTI> S{fr, L, fp0, fast_kind(fp0)};
+  if (gated_off(L)) return;
+  ShadeStage<MULTI, P> S{fr, L, fp0, P::kind(fp0)};
   S.shadow_de = 0;
-  S.vdm = float(fr.view_distance_max);
-  S.dfac = float(fr.de_factor);
+  S.vdm = typename P::D(fr.view_distance_max);
+  S.dfac = typename P::D(fr.de_factor);
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
   const long long total = (long long)L.ctr->hits * (long long)(L.shadow_tasks + L.ao_rays);
-  run_stage<FK>(S, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_AO, my_de - S.shadow_de, K_SHADOW, S.shadow_de);
 }
 
@@ -756,6 +1008,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ DevF
 // ============================================================================
 __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ DevFrame fr,
                                                      const __grid_constant__ Launch L, DevOutputs out) {
+  if (gated_off(L)) return;
   const long long nh = (long long)L.ctr->hits;
   for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < nh; h += (long long)gridDim.x * blockDim.x) {
     const HitRec &r = L.hits[h];
@@ -786,8 +1039,41 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Dev
 
 // Counts pixels (misses + hits) once per launch, from the stage-P queue size.
 __global__ void pixel_count_kernel(const __grid_constant__ Launch L, DevOutputs out, long long pixels) {
+  if (gated_off(L)) return;
   if (threadIdx.x == 0 && out.stats) atomicAdd(reinterpret_cast<unsigned long long *>(out.stats) + K_PIXELS,
                                                (unsigned long long)pixels);
+}
+
+// ============================================================================
+// Precision policy
+// ============================================================================
+// 1 when the smallest hit threshold of a view, bounded below by
+// DE(camera) * c0 (c0: threshold per unit distance), or the constant
+// threshold, is below kWideRatio FP32 units of the camera coordinates.
+__device__ __forceinline__ int wide_needed(const DevScene &sc, const double cam[3], double c0, int constant_thr,
+                                           double de_thresh) {
+  double thr_min = de_thresh;
+  if (!constant_thr) {
+    int it;
+    const double d0 = calc_distance<double, 0, false>(sc, cam[0], cam[1], cam[2], 0.0, false, &it);
+    thr_min = d0 * c0;
+  }
+  const double scale = fmax(fmax(fabs(cam[0]), fabs(cam[1])), fmax(fabs(cam[2]), 1.0));
+  return (thr_min < kWideRatio * scale * 0x1p-24) ? 1 : 0;
+}
+
+__global__ void policy_kernel(const __grid_constant__ DevScene sc, const __grid_constant__ DevFrame fr, int *gate) {
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    *gate = wide_needed(sc, fr.camera, fr.resolution * fr.fov / fr.detail_level, fr.constant_de_threshold,
+                        fr.de_thresh);
+}
+
+__global__ void batch_policy_kernel(const DevScene *scenes, const int *scene_of, const WJob *jobs, int n,
+                                    int constant_thr, double de_thresh, int *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n)
+    flags[i] = wide_needed(scenes[scene_of[i]], jobs[i].cam, jobs[i].resolution * jobs[i].fov / jobs[i].detail,
+                           constant_thr, de_thresh);
 }
 
 // ---- host side -------------------------------------------------------------------
@@ -806,6 +1092,8 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.pixel_offset = pixel_offset;
   j.fov = fr.fov;
   j.aspect = fr.aspect;
+  j.resolution = fr.resolution;
+  j.detail = fr.detail_level;
   j.c0 = float(fr.resolution * fr.fov / fr.detail_level);
   j.fovf = float(fr.fov);
   j.div_w = make_fastdiv(j.width);
@@ -835,12 +1123,15 @@ static int sm_count() {
   return sms;
 }
 
-// The stage launches of one frame or batch, in stream order.
-template <bool MULTI>
-static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const DevFrame &fr, const FastParams &fp0,
-                           const WJob &j0, const Launch &L0, const DevOutputs &out, long long pixels) {
+// The stage launches of one frame or batch under policy P, in stream order.
+template <bool MULTI, class P>
+static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const DevFrame &fr,
+                           const typename P::Params &fp0, const WJob &j0, const Launch &L0, const DevOutputs &out,
+                           long long pixels) {
   Launch L = L0;
   L.div_per = make_fastdiv(std::max(1, L.shadow_tasks + L.ao_rays));
+  L.gate_value = P::kWide;
+  if (P::kWide && fk == FK_BOX_SIMPLE) fk = FK_BOX;
   const int sms = sm_count();
   const int grid = std::max(1, sms * tu.ctas_per_sm);
   const int block = tu.block_size;
@@ -848,11 +1139,13 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
   if (e) return e;
 #define STAGE_LAUNCH(KERNEL, K, ...)                                                    \
   case K:                                                                               \
-    KERNEL<K, MULTI><<<grid, block, 0, st>>>(__VA_ARGS__);                              \
+    KERNEL<K, MULTI, P><<<grid, block, 0, st>>>(__VA_ARGS__);                           \
     break;
 #define STAGE(KERNEL, ...)                                                              \
   switch (fk) {                                                                         \
-    STAGE_LAUNCH(KERNEL, FK_BOX_SIMPLE, __VA_ARGS__)                                    \
+    case FK_BOX_SIMPLE:                                                                 \
+      if constexpr (!P::kWide) KERNEL<FK_BOX_SIMPLE, MULTI, P><<<grid, block, 0, st>>>(__VA_ARGS__); \
+      break;                                                                            \
     STAGE_LAUNCH(KERNEL, FK_BOX, __VA_ARGS__)                                           \
     STAGE_LAUNCH(KERNEL, FK_BULB, __VA_ARGS__)                                          \
     STAGE_LAUNCH(KERNEL, FK_MENGER, __VA_ARGS__)                                        \
@@ -874,7 +1167,8 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
 }
 
 // Scratch of a launch over `pixels` work items with `per` stage-S tasks per
-// hit: counters, hit records, FP32 origins and stage-S start records.
+// hit: counters and the policy flag, hit records, FP32 origins and stage-S
+// start records.
 static size_t scratch_bytes(long long pixels, int per) {
   return 256 + size_t(pixels) * (sizeof(HitRec) + sizeof(float4) * (1 + size_t(per)));
 }
@@ -882,15 +1176,22 @@ static size_t scratch_bytes(long long pixels, int per) {
 static void scratch_layout(Launch &L, void *base, long long pixels) {
   char *p = static_cast<char *>(base);
   L.ctr = reinterpret_cast<Counters4 *>(p);
+  L.gate = nullptr;
   L.hits = reinterpret_cast<HitRec *>(p + 256);
   L.sorg = reinterpret_cast<float4 *>(p + 256 + size_t(pixels) * sizeof(HitRec));
   L.sdir = L.sorg + pixels;
 }
 
+static int *scratch_gate(void *base) { return reinterpret_cast<int *>(static_cast<char *>(base) + 128); }
+
+static bool is_wavefront(int engine) {
+  return engine == MBR_ENGINE_WAVEFRONT_FP32 || engine == MBR_ENGINE_WAVEFRONT_FP64 ||
+         engine == MBR_ENGINE_WAVEFRONT_AUTO;
+}
+
 mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, const DevOutputs &out, int engine,
                             void *stream) {
-  if (engine != MBR_ENGINE_WAVEFRONT_FP32)
-    return set_err(ctx, MBR_EUNSUPPORTED, "the FP64 wavefront engine is not built; use MBR_ENGINE_PLAIN_FP64");
+  if (!is_wavefront(engine)) return set_err(ctx, MBR_EINVAL, "not a wavefront engine: %d", engine);
   mbr_status stt = check_supported(ctx, sc, fr);
   if (stt != MBR_OK) return stt;
   const mbr_tuning tu = ctx_tuning(ctx);
@@ -905,6 +1206,7 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   std::memset(&L, 0, sizeof(L));
   L.jobs = nullptr;
   L.fps = nullptr;
+  L.wps = nullptr;
   L.njobs = 1;
   L.total = total;
   scratch_layout(L, work, total);
@@ -914,8 +1216,20 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   L.shadow_tasks = (fr.shading_enable && fr.shadow_enable) ? 1 : 0;
   L.want_normal = fr.want_normal;
   const FastParams fp = load_fast_params(sc);
-  const int e = launch_pipeline<false>(fast_kind(fp), tu, static_cast<cudaStream_t>(stream), fr, fp, j0, L, out,
-                                       (long long)fr.width * (fr.row1 - fr.row0));
+  const WideParams wp = load_wide_params(sc);
+  const long long pixels = (long long)fr.width * (fr.row1 - fr.row0);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int e = 0;
+  if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {
+    int *gate = scratch_gate(work);
+    L.gate = gate;
+    policy_kernel<<<1, 32, 0, s>>>(sc, fr, gate);
+    e = int(cudaGetLastError());
+  }
+  if (!e && engine != MBR_ENGINE_WAVEFRONT_FP64)
+    e = launch_pipeline<false, Prec32>(fast_kind(fp), tu, s, fr, fp, j0, L, out, pixels);
+  if (!e && engine != MBR_ENGINE_WAVEFRONT_FP32)
+    e = launch_pipeline<false, Prec64>(wide_kind(wp), tu, s, fr, wp, j0, L, out, pixels);
   return cuda_err(ctx, e, "wavefront launch");
 }
 
@@ -926,15 +1240,54 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
 // ============================================================================
 using namespace mbr;
 
+// One pipeline of a batch: the jobs of one formula kind and one precision.
+struct BatchGroup {
+  int wide;              // 1: Prec64
+  int kind;              // FK_* of its jobs
+  int offset, count;     // jobs [offset, offset + count) of the batch's job table
+  long long items;       // work items of its pixel queue
+  long long pixels;
+};
+
 struct mbr_batch {
   mbr_ctx *ctx = nullptr;
   WJob *d_jobs = nullptr;
   FastParams *d_params = nullptr;
+  WideParams *d_wide = nullptr;
   void *d_scratch = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long total = 0;
+  std::vector<BatchGroup> groups;
 };
+
+// Precision flag of every job (AUTO): the policy kernel over the job table.
+static int batch_policy(const std::vector<DevScene> &dsc, const std::vector<int> &scene_of,
+                        const std::vector<WJob> &wj, const DevFrame &fr0, std::vector<int> *flags) {
+  const int n = int(wj.size());
+  DevScene *d_sc = nullptr;
+  int *d_of = nullptr, *d_fl = nullptr;
+  WJob *d_wj = nullptr;
+  int e = int(cudaMalloc(&d_sc, sizeof(DevScene) * dsc.size()));
+  if (!e) e = int(cudaMalloc(&d_of, sizeof(int) * n));
+  if (!e) e = int(cudaMalloc(&d_fl, sizeof(int) * n));
+  if (!e) e = int(cudaMalloc(&d_wj, sizeof(WJob) * n));
+  if (!e) e = int(cudaMemcpy(d_sc, dsc.data(), sizeof(DevScene) * dsc.size(), cudaMemcpyHostToDevice));
+  if (!e) e = int(cudaMemcpy(d_of, scene_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+  if (!e) e = int(cudaMemcpy(d_wj, wj.data(), sizeof(WJob) * n, cudaMemcpyHostToDevice));
+  if (!e) {
+    batch_policy_kernel<<<(n + 127) / 128, 128>>>(d_sc, d_of, d_wj, n, fr0.constant_de_threshold, fr0.de_thresh,
+                                                  d_fl);
+    e = int(cudaGetLastError());
+  }
+  flags->assign(n, 0);
+  if (!e) e = int(cudaMemcpy(flags->data(), d_fl, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  cudaFree(d_sc);
+  cudaFree(d_of);
+  cudaFree(d_fl);
+  cudaFree(d_wj);
+  return e;
+}
 
 extern "C" {
 
@@ -945,18 +1298,17 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
   *batch = nullptr;
   if (!ctx || !scenes || !jobs || !params || !outs || n_scenes < 1 || n_jobs < 1)
     return set_err(ctx, MBR_EINVAL, "null argument or empty batch");
-  if (engine != MBR_ENGINE_WAVEFRONT_FP32)
-    return set_err(ctx, MBR_EUNSUPPORTED, "batches run on MBR_ENGINE_WAVEFRONT_FP32");
+  if (!is_wavefront(engine)) return set_err(ctx, MBR_EUNSUPPORTED, "batches run on the wavefront engines");
   const mbr_tuning tu = ctx_tuning(ctx);
-  std::vector<FastParams> fps(n_jobs);
-  std::vector<WJob> wj(n_jobs);
   std::vector<DevScene> dsc(n_scenes);
   for (int i = 0; i < n_scenes; i++) {
     mbr_status st = build_scene(ctx, scenes[i], &dsc[i]);
     if (st != MBR_OK) return st;
   }
   DevFrame fr0;
-  long long first = 0, pixels = 0;
+  std::vector<WJob> wj(n_jobs);
+  std::vector<int> scene_of(n_jobs);
+  std::vector<long long> job_pixels(n_jobs);
   for (int i = 0; i < n_jobs; i++) {
     const mbr_job &jb = jobs[i];
     if (jb.scene_index < 0 || jb.scene_index >= n_scenes)
@@ -968,15 +1320,55 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
     st = check_supported(ctx, dsc[jb.scene_index], fr);
     if (st != MBR_OK) return st;
     if (i == 0) fr0 = fr;
-    wj[i] = make_job(fr, first, jb.pixel_offset);
-    first += job_items(wj[i], tu.queue_layout);
-    pixels += (long long)fr.width * (fr.row1 - fr.row0);
-    fps[i] = load_fast_params(dsc[jb.scene_index]);
+    wj[i] = make_job(fr, 0, jb.pixel_offset);
+    scene_of[i] = jb.scene_index;
+    job_pixels[i] = (long long)fr.width * (fr.row1 - fr.row0);
   }
   fr0.want_normal = outs->normal != nullptr;
+  // precision of every job
+  std::vector<int> wide(n_jobs, engine == MBR_ENGINE_WAVEFRONT_FP64 ? 1 : 0);
+  if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {
+    const int e = batch_policy(dsc, scene_of, wj, fr0, &wide);
+    if (e) return cuda_err(ctx, e, "batch precision policy");
+  }
+  // groups of one (precision, formula kind), each a contiguous run of the job table
+  std::map<std::pair<int, int>, std::vector<int>> by_group;
+  for (int i = 0; i < n_jobs; i++) {
+    const DevScene &sc = dsc[scene_of[i]];
+    const int kind = wide[i] ? wide_kind(load_wide_params(sc)) : fast_kind(load_fast_params(sc));
+    by_group[{wide[i], kind}].push_back(i);
+  }
   mbr_batch *b = new mbr_batch();
   b->ctx = ctx;
-  b->total = first;
+  std::vector<WJob> tab;
+  std::vector<FastParams> fps;
+  std::vector<WideParams> wps;
+  tab.reserve(n_jobs);
+  fps.reserve(n_jobs);
+  wps.reserve(n_jobs);
+  long long max_items = 0;
+  for (const auto &kv : by_group) {
+    BatchGroup g;
+    g.wide = kv.first.first;
+    g.kind = kv.first.second;
+    g.offset = int(tab.size());
+    g.count = int(kv.second.size());
+    g.items = 0;
+    g.pixels = 0;
+    for (int i : kv.second) {
+      WJob j = wj[i];
+      j.first = g.items;
+      g.items += job_items(j, tu.queue_layout);
+      g.pixels += job_pixels[i];
+      tab.push_back(j);
+      fps.push_back(load_fast_params(dsc[scene_of[i]]));
+      wps.push_back(load_wide_params(dsc[scene_of[i]]));
+    }
+    max_items = std::max(max_items, g.items);
+    b->groups.push_back(g);
+  }
+  b->total = 0;
+  for (const BatchGroup &g : b->groups) b->total += g.items;
   auto fail = [&](int e, const char *what) {
     mbr_batch_destroy(b);
     return cuda_err(ctx, e, what);
@@ -985,36 +1377,48 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
   if (e) return fail(e, "cudaMalloc(jobs)");
   e = int(cudaMalloc(&b->d_params, sizeof(FastParams) * n_jobs));
   if (e) return fail(e, "cudaMalloc(params)");
+  e = int(cudaMalloc(&b->d_wide, sizeof(WideParams) * n_jobs));
+  if (e) return fail(e, "cudaMalloc(wide params)");
   const int per = ((fr0.shading_enable && fr0.shadow_enable) ? 1 : 0) + fr0.ao_rays;
-  e = int(cudaMalloc(&b->d_scratch, scratch_bytes(first, per)));
+  e = int(cudaMalloc(&b->d_scratch, scratch_bytes(max_items, per)));
   if (e) return fail(e, "cudaMalloc(scratch)");
-  e = int(cudaMemcpy(b->d_jobs, wj.data(), sizeof(WJob) * n_jobs, cudaMemcpyHostToDevice));
+  e = int(cudaMemcpy(b->d_jobs, tab.data(), sizeof(WJob) * n_jobs, cudaMemcpyHostToDevice));
   if (e) return fail(e, "cudaMemcpy(jobs)");
   e = int(cudaMemcpy(b->d_params, fps.data(), sizeof(FastParams) * n_jobs, cudaMemcpyHostToDevice));
   if (e) return fail(e, "cudaMemcpy(params)");
-  Launch L;
-  std::memset(&L, 0, sizeof(L));
-  L.jobs = b->d_jobs;
-  L.fps = b->d_params;
-  L.njobs = n_jobs;
-  L.total = first;
-  scratch_layout(L, b->d_scratch, first);
-  L.refill_k = tu.refill_k;
-  L.layout = tu.queue_layout;
-  L.ao_rays = fr0.ao_rays;
-  L.shadow_tasks = (fr0.shading_enable && fr0.shadow_enable) ? 1 : 0;
-  L.want_normal = fr0.want_normal;
-  // capture the pipeline of one batch into a graph
+  e = int(cudaMemcpy(b->d_wide, wps.data(), sizeof(WideParams) * n_jobs, cudaMemcpyHostToDevice));
+  if (e) return fail(e, "cudaMemcpy(wide params)");
+  // capture the groups' pipelines of one batch into a graph
   cudaStream_t cs;
   e = int(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   if (e) return fail(e, "cudaStreamCreate");
   const DevOutputs d = dev_outputs(ctx, *outs);
   e = int(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   if (!e) {
-    const int le = launch_pipeline<true>(FK_ANY, tu, cs, fr0, fps[0], wj[0], L, d, pixels);
-    cudaGraph_t g = nullptr;
-    e = int(cudaStreamEndCapture(cs, &g));
-    b->graph = g;
+    int le = 0;
+    for (const BatchGroup &g : b->groups) {
+      Launch L;
+      std::memset(&L, 0, sizeof(L));
+      L.jobs = b->d_jobs + g.offset;
+      L.fps = b->d_params + g.offset;
+      L.wps = b->d_wide + g.offset;
+      L.njobs = g.count;
+      L.total = g.items;
+      scratch_layout(L, b->d_scratch, g.items);
+      L.refill_k = tu.refill_k;
+      L.layout = tu.queue_layout;
+      L.ao_rays = fr0.ao_rays;
+      L.shadow_tasks = (fr0.shading_enable && fr0.shadow_enable) ? 1 : 0;
+      L.want_normal = fr0.want_normal;
+      if (g.wide)
+        le = launch_pipeline<true, Prec64>(g.kind, tu, cs, fr0, wps[g.offset], tab[g.offset], L, d, g.pixels);
+      else
+        le = launch_pipeline<true, Prec32>(g.kind, tu, cs, fr0, fps[g.offset], tab[g.offset], L, d, g.pixels);
+      if (le) break;
+    }
+    cudaGraph_t gr = nullptr;
+    e = int(cudaStreamEndCapture(cs, &gr));
+    b->graph = gr;
     if (!e) e = le;
   }
   cudaStreamDestroy(cs);
@@ -1038,8 +1442,18 @@ void mbr_batch_destroy(mbr_batch *b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->d_jobs) cudaFree(b->d_jobs);
   if (b->d_params) cudaFree(b->d_params);
+  if (b->d_wide) cudaFree(b->d_wide);
   if (b->d_scratch) cudaFree(b->d_scratch);
   delete b;
+}
+
+int32_t mbr_batch_groups(const mbr_batch *b, int32_t *wide_jobs) {
+  if (!b) return -1;
+  int32_t w = 0;
+  for (const BatchGroup &g : b->groups)
+    if (g.wide) w += g.count;
+  if (wide_jobs) *wide_jobs = w;
+  return int32_t(b->groups.size());
 }
 
 // Times the wavefront pipeline on the given frame over block size x CTAs per
@@ -1088,8 +1502,6 @@ done:
   *best = ctx_tuning(ctx);
   return status;
 }
-
-
 
 }  // extern "C"
 
@@ -1209,7 +1621,7 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
   if (e) return noalloc_fail(err, err_len, MBR_ECUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(cudaError_t(e)));
   const WJob j0 = make_job(fr, 0, 0);
   const FastParams fp = load_fast_params(sc);
-  e = launch_pipeline<false>(fast_kind(fp), tu, s, fr, fp, j0, L, d, total);
+  e = launch_pipeline<false, Prec32>(fast_kind(fp), tu, s, fr, fp, j0, L, d, total);
   if (e) return noalloc_fail(err, err_len, MBR_ECUDA, std::string("wavefront launch: ") + cudaGetErrorString(cudaError_t(e)));
   return MBR_OK;
 }
