@@ -349,11 +349,30 @@ def run_batch(a, torch, dist, world, rank, local) -> None:
         hf, hr = fast["depth"] < 1e19, ref["depth"] < 1e19
         both = hf & hr
         rel = np.abs(fast["depth"][both] - ref["depth"][both]) / ref["depth"][both]
+        # jobs whose camera sits inside the solid: every pixel hits at a depth
+        # near 0, where a relative depth error compares rounding noise
+        inside = np.zeros(total, dtype=bool)
+        for i, cam in enumerate(cams):
+            n = cam.width * cam.height
+            d = ref["depth"][offsets[i]: offsets[i] + n]
+            h = d < 1e19
+            if h.any() and np.median(d[h]) < 1e-6:
+                inside[offsets[i]: offsets[i] + n] = True
+        out_both = both & ~inside
+        rel_out = np.abs(fast["depth"][out_both] - ref["depth"][out_both]) / ref["depth"][out_both]
         base = {"engine": "plain_fp64 (one launch per job)", "value": bsd["de_evals"] / bt, "unit": UNIT,
                 "seconds": bt, "mpix_per_s": bsd["pixels"] / bt / 1e6,
                 "hit_mismatch": float((hf != hr).mean()), "depth_rel_median": float(np.median(rel)),
                 "depth_rel_p99": float(np.quantile(rel, 0.99)),
-                "frac_depth_rel_le_1e4": float((rel <= 1e-4).mean())}
+                "frac_depth_rel_le_1e4": float((rel <= 1e-4).mean()),
+                "camera_outside_solid": {"pixels": int((~inside).sum()),
+                                         "hit_mismatch": float((hf != hr)[~inside].mean()),
+                                         "depth_rel_median": float(np.median(rel_out)),
+                                         "depth_rel_p99": float(np.quantile(rel_out, 0.99)),
+                                         "frac_depth_rel_le_1e4": float((rel_out <= 1e-4).mean())},
+                "camera_inside_solid": {"jobs": int(sum(1 for i, c in enumerate(cams)
+                                                        if inside[offsets[i]])),
+                                        "pixels": int(inside.sum())}}
     value = sd["de_evals"] / t
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -506,15 +525,22 @@ def main() -> None:
     per_iter = ops.get(desc["formula"], {}).get("flops_per_iteration")
     launch_s = t / a.steps
     roofline = None
+    # the precision the formula iteration ran in: FP64 engines, and the auto
+    # engine when its policy picked FP64 for this view
+    iter_fp64 = a.engine in ("plain_fp64", "plain_fp64_strict", "wavefront_fp64") or (
+        a.engine == "wavefront_auto" and r.choose_precision(cam, p) == 1)
     if per_iter:
         achieved = st["formula_iterations"] / a.steps * per_iter / launch_s / 1e12
-        pk = peak.value / 1e12
+        pk = (fp64_peak if iter_fp64 else peak).value / 1e12
         traffic = load_json(os.path.join(ROOT, "profiles", "traffic.json")) or {}
         tr = traffic.get(a.engine, {}).get(a.workload)
+        probe = "DFMA probe (mbr_fma_peak), FP64" if iter_fp64 else "FFMA probe (mbr_fma_peak), FP32 non-tensor"
         roofline = {"bound": "fma", "achieved": achieved, "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk,
-                    "traffic": tr, "peak_source": "measured live: FFMA probe (mbr_fma_peak), FP32 non-tensor; "
-                                                  "MEASURED_PEAKS.json has no FP32 FMA figure",
-                    "flops_per_iteration": per_iter, "fp64_peak": fp64_peak.value / 1e12}
+                    "traffic": tr, "peak_source": f"measured live: {probe}; MEASURED_PEAKS.json has no FMA "
+                                                  "figure for non-tensor arithmetic",
+                    "iteration_precision": "f64" if iter_fp64 else "f32",
+                    "flops_per_iteration": per_iter, "fp32_peak": peak.value / 1e12,
+                    "fp64_peak": fp64_peak.value / 1e12}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -527,7 +553,7 @@ def main() -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": t / a.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if "fp32" in a.engine or "mixed" in a.engine else "f64",
+            "dtype": "f64" if iter_fp64 else "f32",
             "data": "synthetic (procedural fractal scene, no dataset)",
             "config": dict(desc, engine=a.engine, parallelism=f"replicas x{world} (one frame per GPU)",
                            l2="256 MiB buffer written between timed frames", tuning=tuning),

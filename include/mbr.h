@@ -315,6 +315,12 @@ void mbr_batch_destroy(mbr_batch *batch);
  * -1 for a NULL batch. */
 int32_t mbr_batch_groups(const mbr_batch *batch, int32_t *wide_jobs);
 
+/* The precision MBR_ENGINE_WAVEFRONT_AUTO uses for the current scene seen
+ * from `camera` with `params`: *fp64 = 1 for FP64 iteration, 0 for FP32.
+ * Synchronous (one device evaluation of DE at the camera). */
+mbr_status mbr_choose_precision(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                                int32_t *fp64);
+
 /* Launch configuration of the wavefront kernel, chosen by the autotuner. */
 typedef struct mbr_tuning {
   int32_t block_size;     /* threads per CTA */

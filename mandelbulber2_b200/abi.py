@@ -131,6 +131,7 @@ PROTOTYPES = {
     "mbr_batch_launch": (C.c_int, [_P, _P]),
     "mbr_batch_destroy": (None, [_P]),
     "mbr_batch_groups": (C.c_int32, [_P, _P]),
+    "mbr_choose_precision": (C.c_int, [_P, _P, _P, _P]),
     "mbr_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mbr_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mbr_autotune": (C.c_int, [_P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(Outputs), C.c_int, _P,

@@ -468,6 +468,7 @@ DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o) {
 }
 
 const DevScene *ctx_scene(mbr_ctx *ctx) { return ctx->has_scene ? &ctx->scene : nullptr; }
+int ctx_device(mbr_ctx *ctx) { return ctx->device; }
 const mbr_scene *ctx_scene_src(mbr_ctx *ctx) { return ctx->has_scene ? &ctx->scene_src : nullptr; }
 mbr_tuning &ctx_tuning(mbr_ctx *ctx) { return ctx->tuning; }
 int32_t *ctx_status(mbr_ctx *ctx) { return ctx->d_status; }

@@ -17,6 +17,7 @@ DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o);
 mbr_status build_frame_owned_gamma(const mbr_camera &cam, const mbr_render_params &p, uint16_t *gamma_dev,
                                    double *gamma_value, DevFrame *out, std::string *err);
 const DevScene *ctx_scene(mbr_ctx *ctx);
+int ctx_device(mbr_ctx *ctx);
 const mbr_scene *ctx_scene_src(mbr_ctx *ctx);
 mbr_tuning &ctx_tuning(mbr_ctx *ctx);
 int32_t *ctx_status(mbr_ctx *ctx);

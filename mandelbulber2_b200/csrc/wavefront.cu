@@ -1447,6 +1447,28 @@ void mbr_batch_destroy(mbr_batch *b) {
   delete b;
 }
 
+mbr_status mbr_choose_precision(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
+                                int32_t *fp64) {
+  if (!ctx || !camera || !params || !fp64) return set_err(ctx, MBR_EINVAL, "null argument");
+  const DevScene *sc = ctx_scene(ctx);
+  if (!sc) return set_err(ctx, MBR_EINVAL, "no scene set (call mbr_scene_set first)");
+  if (cudaSetDevice(ctx_device(ctx)) != cudaSuccess) return set_err(ctx, MBR_ECUDA, "cudaSetDevice failed");
+  DevFrame fr;
+  mbr_status st = build_frame(ctx, *camera, *params, &fr);
+  if (st != MBR_OK) return st;
+  int *d_flag = nullptr;
+  int e = int(cudaMalloc(&d_flag, sizeof(int)));
+  if (e) return cuda_err(ctx, e, "cudaMalloc(flag)");
+  policy_kernel<<<1, 32>>>(*sc, fr, d_flag);
+  e = int(cudaGetLastError());
+  int flag = 0;
+  if (!e) e = int(cudaMemcpy(&flag, d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d_flag);
+  if (e) return cuda_err(ctx, e, "precision policy");
+  *fp64 = flag;
+  return MBR_OK;
+}
+
 int32_t mbr_batch_groups(const mbr_batch *b, int32_t *wide_jobs) {
   if (!b) return -1;
   int32_t w = 0;

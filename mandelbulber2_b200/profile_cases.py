@@ -2,10 +2,11 @@
 
   python -m mandelbulber2_b200.profile_cases <case>
 
-cases: plain_fp64, plain_strict, plain_mixed, wavefront (Mandelbox s=-1.5,
-960x540, camera A, 16 AO rays; two frames), gi (hybrid Mandelbulb/Menger
-480x270, 2 spp), adjoint (Mandelbulb 256x256 forward + FP64 adjoint),
-distance (CalculateDistance at 2^20 random points).
+cases: plain_fp64, plain_strict, plain_mixed, wavefront, wavefront64
+(Mandelbox s=-1.5, 960x540, camera A, 16 AO rays; two frames; wavefront64
+iterates in FP64), gi (hybrid Mandelbulb/Menger 480x270, 2 spp), adjoint
+(Mandelbulb 256x256 forward + FP64 adjoint), distance (CalculateDistance at
+2^20 random points).
 """
 from __future__ import annotations
 
@@ -17,7 +18,8 @@ from . import abi, configs
 from .render import STATS_FIELDS, Renderer, alloc_outputs
 
 FRAME_ENGINES = {"plain_fp64": abi.ENGINE_PLAIN_FP64, "plain_strict": abi.ENGINE_PLAIN_FP64_STRICT,
-                 "plain_mixed": abi.ENGINE_PLAIN_MIXED, "wavefront": abi.ENGINE_WAVEFRONT_FP32}
+                 "plain_mixed": abi.ENGINE_PLAIN_MIXED, "wavefront": abi.ENGINE_WAVEFRONT_FP32,
+                 "wavefront64": abi.ENGINE_WAVEFRONT_FP64}
 
 
 def frame(r: Renderer, sc, cam, p, engine: int, reps: int = 2) -> dict:

@@ -146,6 +146,12 @@ class Renderer:
         self.sync()
         return dist, iters
 
+    def choose_precision(self, camera: abi.Camera, params: abi.RenderParams) -> int:
+        """1 when MBR_ENGINE_WAVEFRONT_AUTO iterates this view in FP64, else 0."""
+        flag = C.c_int32(0)
+        self._check(self.lib.mbr_choose_precision(self.ctx, C.byref(camera), C.byref(params), C.byref(flag)))
+        return int(flag.value)
+
     def set_tuning(self, block_size: int, ctas_per_sm: int, refill_k: int, queue_layout: int) -> None:
         t = abi.Tuning(block_size, ctas_per_sm, refill_k, queue_layout)
         self._check(self.lib.mbr_set_tuning(self.ctx, C.byref(t)))
