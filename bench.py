@@ -106,16 +106,46 @@ def kernels_per_frame(engine: str, p) -> int:
 
 # ---- clocks ---------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons sampled every 2 ms during the timed
+    region through NVML (read-only queries; nvidia-smi's 100 ms period misses
+    timed regions of a few tens of milliseconds), with an nvidia-smi fallback."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, pci_bus_id: str | None = None):
         self.index = index
+        self.pci = pci_bus_id
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        h = None
+        if self.pci:
+            try:
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(self.pci)
+            except pynvml.NVMLError:
+                h = None
+        if h is None:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        return pynvml, h
 
     def start(self):
+        try:
+            self.nvml, self.handle = self._nvml_handle()
+            self.smax = float(self.nvml.nvmlDeviceGetMaxClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -125,11 +155,33 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml, self.handle
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop_flag.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((sm, [n for n, b in bits.items() if rs & b]))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            sm = [x[0] for x in self.samples]
+            reasons = sorted({r for x in self.samples for r in x[1]})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML, 2 ms period"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -138,7 +190,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
@@ -148,11 +199,19 @@ class ClockSampler:
                 smax = float(parts[2])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for n, v in zip(self.NAMES, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 100 ms period"}
+
+
+def pci_bus_id(torch, local: int) -> str | None:
+    try:
+        pr = torch.cuda.get_device_properties(local)
+        return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        return None
 
 
 # ---- helpers ----------------------------------------------------------------------
@@ -317,6 +376,8 @@ def run_batch(a, torch, dist, world, rank, local) -> None:
     r.sync()
     stats.zero_()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local, pci_bus_id(torch, local))
+    clocks.start()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -325,6 +386,7 @@ def run_batch(a, torch, dist, world, rank, local) -> None:
         lib.mbr_batch_launch(b, C.c_void_p(s.cuda_stream))
     e1.record()
     torch.cuda.synchronize()
+    clk = clocks.stop()
     r.sync()
     t = e0.elapsed_time(e1) / 1e3
     sd = stats_dict(stats)
@@ -387,7 +449,7 @@ def run_batch(a, torch, dist, world, rank, local) -> None:
                 "mpix_per_s": sd["pixels"] / t / 1e6, "stats_per_step": {k: v / a.steps for k, v in sd.items()},
                 "fp64_baseline": base, "speedup_vs_fp64": value / base["value"] if base else None,
                 "wall_speedup_vs_fp64": (base["seconds"] / (t / a.steps)) if base else None,
-                "gpu_launches": a.steps * n_groups * 4}
+                "gpu_launches": a.steps * n_groups * 4, "clocks": clk}
         print(json.dumps(line), flush=True)
     r.close()
 
@@ -451,7 +513,7 @@ def main() -> None:
     bufs = alloc_outputs(n, r.device, names)
     flush = l2_flush_buffer(torch, r.device)
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, pci_bus_id(torch, local))
     clocks.start()
     t, st, ms = time_engine(r, torch, cam, p, bufs, engine, a.steps, a.warmup, flush, dist, world)
     clk = clocks.stop()

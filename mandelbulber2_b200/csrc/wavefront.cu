@@ -350,9 +350,14 @@ struct Prec64 {
 //   int kind()              - formula kind (FK_ANY launches)
 //   D detail()              - detail size of the current request
 // ============================================================================
+// fpk: the formula parameters of a single-job launch, the kernel parameter
+// itself, so that the iteration reads its constants as constant-bank operands
+// (a copy held in the stage is read through indexed constant loads); batch
+// launches (Stage::kMulti) read the per-job copy the stage loads.
 template <int FK, class P, class Stage>
-__device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter, long long total, int refill_k,
-                                          unsigned int *my_de, unsigned long long *my_iters) {
+__device__ __forceinline__ void run_stage(Stage &S, const typename P::Params &fpk, unsigned long long *counter,
+                                          long long total, int refill_k, unsigned int *my_de,
+                                          unsigned long long *my_iters) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const unsigned lanemask_lt = (1u << lane) - 1u;
@@ -374,7 +379,7 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
         if (idx < total) {
           typename Stage::Real qx, qy, qz;
           if (S.start(idx, qx, qy, qz)) {
-            P::start(e, S.params(), qx, qy, qz);
+            P::start(e, Stage::kMulti ? S.params() : fpk, qx, qy, qz);
             has = true;
             iterating = true;
           }
@@ -391,7 +396,7 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
     // A lane whose orbit ends leaves the loop by a branch, so the remaining
     // lanes run the iteration without select instructions for finished ones;
     // the vote counts the lanes still in the loop.
-    const typename P::Params &fp = S.params();
+    const typename P::Params &fp = Stage::kMulti ? S.params() : fpk;
     const int kind = S.kind();
     if (iterating) {
       for (;;) {
@@ -415,7 +420,7 @@ __device__ __forceinline__ void run_stage(Stage &S, unsigned long long *counter,
       it_n += (unsigned long long)iters;
       typename Stage::Real qx, qy, qz;
       if (S.step(d, iters, qx, qy, qz)) {
-        P::start(e, S.params(), qx, qy, qz);
+        P::start(e, Stage::kMulti ? S.params() : fpk, qx, qy, qz);
         iterating = true;
       } else {
         has = false;
@@ -452,6 +457,7 @@ __device__ __forceinline__ void flush_counts(const DevOutputs &out, unsigned int
 template <bool MULTI, class P>
 struct PrimaryStage {
   typedef double Real;
+  static constexpr bool kMulti = MULTI;
   typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
@@ -682,7 +688,7 @@ __global__ void __launch_bounds__(256) primary_kernel(const __grid_constant__ De
   S.binary_de = 0;
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
-  run_stage<FK, P>(S, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, fp0, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_MARCH, my_de - S.binary_de, K_BINARY, S.binary_de);
 }
 
@@ -692,6 +698,7 @@ __global__ void __launch_bounds__(256) primary_kernel(const __grid_constant__ De
 template <bool MULTI, class P>
 struct NormalStage {
   typedef double Real;
+  static constexpr bool kMulti = MULTI;
   typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
@@ -806,7 +813,7 @@ __global__ void __launch_bounds__(256) normal_kernel(const __grid_constant__ Dev
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
   const long long total = (long long)L.ctr->hits;
-  run_stage<FK, P>(S, &L.ctr->normals_next, total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, fp0, &L.ctr->normals_next, total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_NORMAL, my_de, K_NORMAL, 0);
 }
 
@@ -838,6 +845,7 @@ __device__ __forceinline__ unsigned long long pcg_advance(unsigned long long sta
 template <bool MULTI, class P>
 struct ShadeStage {
   typedef typename P::D Real;
+  static constexpr bool kMulti = MULTI;
   typedef typename P::D D;
   const DevFrame &fr;
   const Launch &L;
@@ -999,7 +1007,7 @@ __global__ void __launch_bounds__(256) shade_kernel(const __grid_constant__ DevF
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
   const long long total = (long long)L.ctr->hits * (long long)(L.shadow_tasks + L.ao_rays);
-  run_stage<FK, P>(S, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
+  run_stage<FK, P>(S, fp0, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_AO, my_de - S.shadow_de, K_SHADOW, S.shadow_de);
 }
 
