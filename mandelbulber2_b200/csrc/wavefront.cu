@@ -116,10 +116,12 @@ struct Counters4 {
 struct WideParams {
   DevSlot slot;
   int formula, maxN, de_fn, min_n;
-  int julia, add_c, check_bailout, pad;
+  int julia, add_c, check_bailout, box_simple;  // box_simple: as FastParams::box_simple
   double bailout;
   double jc[3];  // julia_c * fractal_constant_factor
   double cm[3];  // fractal_constant_factor
+  // simple Mandelbox: folding limit, fR2, fR2/mR2, scale, |scale|, bailout^2
+  double lim, fr2, fmx, scale, ascale, bailout2;
 };
 
 __host__ __device__ inline WideParams load_wide_params(const DevScene &sc) {
@@ -132,12 +134,21 @@ __host__ __device__ inline WideParams load_wide_params(const DevScene &sc) {
   w.julia = sc.julia;
   w.add_c = sc.slot[0].add_c;
   w.check_bailout = sc.slot[0].check_bailout;
-  w.pad = 0;
   w.bailout = sc.slot[0].d[P_BAILOUT];
   for (int k = 0; k < 3; k++) {
     w.jc[k] = sc.julia_c[k] * sc.cmul[k];
     w.cm[k] = sc.cmul[k];
   }
+  const DevSlot &s = sc.slot[0];
+  const double L = s.d[P_MB_LIMIT], F = s.d[P_MB_FACTOR1];
+  w.box_simple = (s.formula == MBR_FORMULA_MANDELBOX && s.d[P_MB_VALUE] == 2.0 * L && L > 0.0 && F > 1.0 &&
+                  !s.has_offset) ? 1 : 0;
+  w.lim = L;
+  w.fr2 = s.d[P_MB_FR2];
+  w.fmx = F;
+  w.scale = s.d[P_MB_SCALE];
+  w.ascale = s.d[P_MB_ABS_SCALE];
+  w.bailout2 = w.bailout * w.bailout;
   return w;
 }
 
@@ -182,7 +193,7 @@ __host__ __device__ inline int fast_kind(const FastParams &f) {
 }
 
 __host__ __device__ inline int wide_kind(const WideParams &w) {
-  if (w.formula == MBR_FORMULA_MANDELBOX) return FK_BOX;
+  if (w.formula == MBR_FORMULA_MANDELBOX) return w.box_simple ? FK_BOX_SIMPLE : FK_BOX;
   if (w.formula == MBR_FORMULA_MANDELBULB) return FK_BULB;
   return FK_MENGER;
 }
@@ -279,9 +290,52 @@ struct Prec64 {
 
   // One pass of the Compute loop body for a non-hybrid scene, as
   // calc_distance<double, F, false> runs it (compute_fractal.cpp:170-321).
+  // The simple Mandelbox (folding value 2 * limit, no offset) runs the fold
+  // rewrites of fast_formula.cuh in FP64: box fold 2 clamp(z, -L, L) - z,
+  // sphere-fold factor clamp(fR2 / r2, 1, fR2 / mR2) with a correctly rounded
+  // reciprocal, scale and c-addition fused, bailout tested on |z|^2 and |z|
+  // taken once when the orbit ends; the result differs from the reference's
+  // operation order in the last bits only.
   template <int FK>
   __device__ static bool step(int kind, State &e, const Params &fp) {
     const int k = (FK == FK_ANY) ? kind : FK;
+    if (k == FK_BOX_SIMPLE) {
+      const double L = fp.lim;
+      const double x = fma(2.0, fmin(fmax(e.zx, -L), L), -e.zx);
+      const double y = fma(2.0, fmin(fmax(e.zy, -L), L), -e.zy);
+      const double z = fma(2.0, fmin(fmax(e.zz, -L), L), -e.zz);
+      const double r2 = fma(x, x, fma(y, y, z * z));
+      const double fs = fmin(fmax(fp.fr2 * __drcp_rn(r2), 1.0), fp.fmx);
+      const double s = fs * fp.scale;
+      e.dr = fma(e.dr, fs * fp.ascale, 1.0);
+      double ax = 0.0, ay = 0.0, az = 0.0;
+      if (fp.add_c) {
+        if (fp.julia) {
+          ax = fp.jc[0];
+          ay = fp.jc[1];
+          az = fp.jc[2];
+        } else {
+          ax = e.cx * fp.cm[0];
+          ay = e.cy * fp.cm[1];
+          az = e.cz * fp.cm[2];
+        }
+      }
+      e.zx = fma(x, s, ax);
+      e.zy = fma(y, s, ay);
+      e.zz = fma(z, s, az);
+      e.it++;
+      const double rr = fma(e.zx, e.zx, fma(e.zy, e.zy, e.zz * e.zz));
+      if (!(rr <= fp.bailout2) && fp.check_bailout) {
+        e.r = sqrt(rr);
+        e.brk = 1;
+        return false;
+      }
+      if (e.it >= fp.maxN) {
+        e.r = sqrt(rr);
+        return false;
+      }
+      return true;
+    }
     V4<double> z{e.zx, e.zy, e.zz, 0.0};
     const V4<double> last = z;
     double de = e.dr;
@@ -1139,7 +1193,6 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
   Launch L = L0;
   L.div_per = make_fastdiv(std::max(1, L.shadow_tasks + L.ao_rays));
   L.gate_value = P::kWide;
-  if (P::kWide && fk == FK_BOX_SIMPLE) fk = FK_BOX;
   const int sms = sm_count();
   const int grid = std::max(1, sms * tu.ctas_per_sm);
   const int block = tu.block_size;
@@ -1151,9 +1204,7 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
     break;
 #define STAGE(KERNEL, ...)                                                              \
   switch (fk) {                                                                         \
-    case FK_BOX_SIMPLE:                                                                 \
-      if constexpr (!P::kWide) KERNEL<FK_BOX_SIMPLE, MULTI, P><<<grid, block, 0, st>>>(__VA_ARGS__); \
-      break;                                                                            \
+    STAGE_LAUNCH(KERNEL, FK_BOX_SIMPLE, __VA_ARGS__)                                    \
     STAGE_LAUNCH(KERNEL, FK_BOX, __VA_ARGS__)                                           \
     STAGE_LAUNCH(KERNEL, FK_BULB, __VA_ARGS__)                                          \
     STAGE_LAUNCH(KERNEL, FK_MENGER, __VA_ARGS__)                                        \
