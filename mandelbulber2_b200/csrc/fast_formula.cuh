@@ -35,6 +35,7 @@ struct FastParams {
   int add_c;       // slot adds the c constant
   int julia;       // c is the Julia constant instead of the point
   int min_n;       // minN
+  int bulb_n;      // mandelbulb: the power when it is an integer 2..32 and both angle offsets are 0, else 0
   float bailout2;
   float cm_x, cm_y, cm_z;        // fractal_constant_factor
   float jc_x, jc_y, jc_z;        // julia_c * fractal_constant_factor
@@ -65,6 +66,7 @@ __host__ __device__ inline FastParams load_fast_params(const DevScene &sc) {
   f.jc_z = sc.fjulia_c[2];
   f.off_x = f.off_y = f.off_z = 0.0f;
   f.box_simple = 0;
+  f.bulb_n = 0;
   f.p0 = f.p1 = f.p2 = f.p3 = f.p4 = f.p5 = 0.0f;
   f.q0 = f.q1 = f.q2 = f.q3 = f.q4 = 0.0f;
   if (s.formula == MBR_FORMULA_MANDELBULB) {
@@ -72,6 +74,9 @@ __host__ __device__ inline FastParams load_fast_params(const DevScene &sc) {
     f.p1 = s.f[P_POWER_M1];
     f.p2 = s.f[P_ALPHA];
     f.p3 = s.f[P_BETA];
+    const double pw = s.d[P_POWER];
+    if (s.d[P_ALPHA] == 0.0 && s.d[P_BETA] == 0.0 && pw >= 2.0 && pw <= 32.0 && pw == double(int(pw)))
+      f.bulb_n = int(pw);
   } else if (s.formula == MBR_FORMULA_MANDELBOX) {
     f.p0 = s.f[P_MB_SCALE];
     f.p1 = s.f[P_MB_ABS_SCALE];
@@ -164,8 +169,68 @@ __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, cons
   }
 }
 
+// (re + i im)^n for n >= 1 by binary exponentiation.
+__device__ __forceinline__ void cpow_int(float &re, float &im, int n) {
+  float ar = re, ai = im;  // the result so far (the lowest set bit of n taken first)
+  while (!(n & 1)) {
+    const float t = fmaf(ar, ar, -ai * ai);
+    ai = 2.0f * ar * ai;
+    ar = t;
+    n >>= 1;
+  }
+  float br = ar, bi = ai;
+  n >>= 1;
+  while (n) {
+    const float t = fmaf(br, br, -bi * bi);
+    bi = 2.0f * br * bi;
+    br = t;
+    if (n & 1) {
+      const float u = fmaf(ar, br, -ai * bi);
+      ai = fmaf(ar, bi, ai * br);
+      ar = u;
+    }
+    n >>= 1;
+  }
+  re = ar;
+  im = ai;
+}
+
 // One Mandelbulb iteration (asin latitude form of fractal_mandelbulb.cpp:32-42) + c-addition.
+// With an integer power n and no angle offsets the angle multiplication is
+// De Moivre's: cos(n th) + i sin(n th) = (cos th + i sin th)^n with
+// cos th = rho/r, sin th = z/r (th = asin(z/r) lies in [-pi/2, pi/2]) and
+// cos ph = x/rho, sin ph = y/rho (ph = atan2(y, x)), rho = |(x, y)|; equal to
+// the transcendental form in real arithmetic, with no asin, atan2, sincos or pow.
 __device__ __forceinline__ void it_mandelbulb(Z3 &z, float &dr, const Z3 &c, const FastParams &f, float r) {
+  if (f.bulb_n) {
+    const int n = f.bulb_n;
+    const float ir = rcp_approx(r);
+    const float rho2 = fmaf(z.x, z.x, z.y * z.y);
+    float ct = sqrt_approx(rho2) * ir, st = z.z * ir;
+    float cp = 1.0f, sp = 0.0f;
+    if (rho2 > 0.0f) {
+      const float irho = rsqrtf(rho2);
+      cp = z.x * irho;
+      sp = z.y * irho;
+    }
+    cpow_int(ct, st, n);
+    cpow_int(cp, sp, n);
+    float rn = r;  // r^n
+    {
+      float b = r;
+      int m = n - 1;
+      while (m) {
+        if (m & 1) rn *= b;
+        b *= b;
+        m >>= 1;
+      }
+    }
+    dr = fmaf(rn * ir * dr, float(n), 1.0f);
+    z.x = fmaf(ct * cp, rn, c.x);
+    z.y = fmaf(ct * sp, rn, c.y);
+    z.z = fmaf(st, rn, c.z);
+    return;
+  }
   const float th0 = asinf(z.z / r) + f.p3;
   const float ph0 = atan2f(z.y, z.x) + f.p2;
   float rp = __powf(r, f.p1);
