@@ -40,8 +40,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--engine", default=None,
-                    help="default per workload: wavefront_fp32 (wide views), wavefront_auto (deep zoom, batch), "
-                         "plain_mixed (GI)")
+                    help="default per workload: wavefront_fp32 (wide views, GI), wavefront_auto (deep zoom, batch)")
     ap.add_argument("--baseline-engine", default="plain_fp64")
     ap.add_argument("--workload", default="mandelbox_1080p_A", choices=WORKLOADS)
     ap.add_argument("--spp", type=int, default=16, help="GI samples per pixel (hybrid_gi_2160p)")
@@ -84,7 +83,7 @@ def workload(name: str, spp: int = 16):
 
 
 DEFAULT_ENGINE = {"mandelbox_1080p_A": "wavefront_fp32", "mandelbox_1080p_B": "wavefront_auto",
-                  "mandelbulb_512": "wavefront_fp32", "hybrid_gi_2160p": "plain_mixed",
+                  "mandelbulb_512": "wavefront_fp32", "hybrid_gi_2160p": "wavefront_fp32",
                   "batch_2048": "wavefront_auto"}
 
 
@@ -96,6 +95,9 @@ def kernels_per_frame(engine: str, p) -> int:
     return at once."""
     if "wavefront" not in engine:
         return 1
+    if p.gi_samples > 0:
+        n = 3  # GI paths, colour, pixel count
+        return 1 + 2 * n if engine == "wavefront_auto" else n
     n = 4  # primary, normals (the bench asks for normals), finish, pixel count
     if p.ao_rays > 0 or (p.shading_enable and p.shadow_enable):
         n += 2  # directions, shadow/AO marches
@@ -263,9 +265,13 @@ def compare_frames(fast: dict, ref: dict) -> dict:
         out.update(depth_rel_median=float(np.median(rel)), depth_rel_p99=float(np.quantile(rel, 0.99)),
                    depth_rel_max=float(rel.max()), frac_depth_rel_le_1e4=float((rel <= 1e-4).mean()))
         nf, nr = fast["normal"][both].astype(np.float64), ref["normal"][both].astype(np.float64)
-        cos = np.clip((nf * nr).sum(1), -1, 1)
-        ang = np.degrees(np.arccos(cos))
-        out.update(normal_deg_median=float(np.median(ang)), normal_deg_p99=float(np.quantile(ang, 0.99)))
+        if np.abs(nr).sum() > 0:  # GI frames carry no normal output
+            cos = np.clip((nf * nr).sum(1), -1, 1)
+            ang = np.degrees(np.arccos(cos))
+            out.update(normal_deg_median=float(np.median(ang)), normal_deg_p99=float(np.quantile(ang, 0.99)))
+        if "rgb8" in fast and "rgb8" in ref:
+            mse = float(np.mean((fast["rgb8"].astype(np.float64) - ref["rgb8"].astype(np.float64)) ** 2))
+            out["psnr_rgb8"] = float("inf") if mse == 0 else 10.0 * np.log10(255.0 ** 2 / mse)
     return out
 
 
@@ -485,8 +491,6 @@ def main() -> None:
     if a.workload == "batch_2048":
         run_batch(a, torch, dist, world, rank, local)
         return
-    if a.workload == "hybrid_gi_2160p" and "wavefront" in a.engine:
-        a.engine = "plain_mixed"  # GI runs on the plain engines (FP32 march, FP64 origin and refinement)
     engine = engines[a.engine]
     base_engine = engines[a.baseline_engine]
 

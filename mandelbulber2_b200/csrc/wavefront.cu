@@ -170,6 +170,8 @@ struct Launch {
   int shadow_tasks;        // 1 when the shadow march runs (shading && shadow)
   int want_normal;
   FastDiv div_per;         // division by shadow_tasks + ao_rays (set by launch_pipeline)
+  unsigned long long *acc;  // GI: per pixel of the launch, summed radiance in 32.32 fixed point
+  FastDiv div_spp;          // GI: division by samples per pixel
 };
 
 // True when this pipeline's kernels have nothing to do (the other precision
@@ -231,7 +233,7 @@ __device__ __forceinline__ bool more_than(unsigned m, int k) {
 struct Prec32 {
   typedef float D;  // distance and threshold arithmetic of the march
   typedef FastParams Params;
-  enum { kWide = 0 };
+  enum { kWide = 0, kHyb = 0 };
   struct State {
     Z3 z, c;
     float dr, r2;
@@ -277,7 +279,7 @@ struct Prec32 {
 struct Prec64 {
   typedef double D;
   typedef WideParams Params;
-  enum { kWide = 1 };
+  enum { kWide = 1, kHyb = 0 };
   struct State {
     double zx, zy, zz, cx, cy, cz, dr, r;
     int it, brk;  // iterations done; 1 when the loop ended by a break (bailout or NaN)
@@ -402,6 +404,114 @@ struct Prec64 {
     if (iters < fp.min_n && d < detail) d = detail;
     if (d < 0.0) d = 0.0;
     if (d > 10.0) d = 10.0;
+    return d;
+  }
+};
+
+// Hybrid sequences (single-frame launches): the FP32 iteration of
+// calc_distance<float, 0, false> one pass at a time - the slot of iteration
+// i from the sequence table (CreateSequence), per-slot formula, c-addition,
+// weight blend, NaN revert and per-slot bailout (compute_fractal.cpp:170-321),
+// and the hybrid DE function of the final distance (:503-557).  The scene
+// lives in device memory (the launch scratch) and is read through a pointer.
+struct HybParams {
+  const DevScene *sc;
+};
+
+struct PrecHyb {
+  typedef float D;
+  typedef HybParams Params;
+  enum { kWide = 0, kHyb = 1 };
+  struct State {
+    float zx, zy, zz, cx, cy, cz, dr, r;
+    int it, brk;
+  };
+  __host__ __device__ static int kind(const Params &) { return FK_ANY; }
+
+  __device__ static void start(State &e, const Params &, float qx, float qy, float qz) {
+    e.zx = qx;
+    e.zy = qy;
+    e.zz = qz;
+    e.cx = qx;
+    e.cy = qy;
+    e.cz = qz;
+    e.dr = 1.0f;
+    e.r = len4<float, false>(V4<float>{qx, qy, qz, 0.0f});
+    e.it = 0;
+    e.brk = 0;
+  }
+  __device__ static void start(State &e, const Params &fp, double qx, double qy, double qz) {
+    start(e, fp, float(qx), float(qy), float(qz));
+  }
+
+  template <int FK>
+  __device__ static bool step(int, State &e, const Params &fp) {
+    const DevScene &sc = *fp.sc;
+    const int i = e.it;
+    const int k = (i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]);
+    const DevSlot &s = sc.slot[k];
+    V4<float> z{e.zx, e.zy, e.zz, 0.0f};
+    const V4<float> last = z;
+    const float tempDE = e.dr;
+    float de = e.dr;
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s);
+    if (s.add_c) {
+      if (sc.julia) {
+        z.x = z.x + juliac_of<float>(sc, 0);
+        z.y = z.y + juliac_of<float>(sc, 1);
+        z.z = z.z + juliac_of<float>(sc, 2);
+      } else {
+        z.x = z.x + e.cx * cmul_of<float>(sc, 0);
+        z.y = z.y + e.cy * cmul_of<float>(sc, 1);
+        z.z = z.z + e.cz * cmul_of<float>(sc, 2);
+      }
+    }
+    if (sc.is_hybrid) {
+      const double kw = s.d[P_WEIGHT];
+      if (kw < 1.0) {
+        z = smooth4<float, false>(last, z, kw);
+        de = de * float(kw) + tempDE * float(1.0 - kw);
+      }
+    }
+    e.it = i + 1;
+    e.dr = de;
+    if (nan4<float, false>(z)) {
+      e.zx = last.x;
+      e.zy = last.y;
+      e.zz = last.z;
+      e.r = len4<float, false>(last);
+      e.brk = 1;
+      return false;
+    }
+    e.zx = z.x;
+    e.zy = z.y;
+    e.zz = z.z;
+    e.r = len4<float, false>(z);
+    if (s.check_bailout && e.r > P<float>(s, P_BAILOUT)) {
+      e.brk = 1;
+      return false;
+    }
+    return e.it < sc.formula_maxiter;
+  }
+
+  __device__ static float distance(const State &e, const Params &fp, float detail, int &iters) {
+    const DevScene &sc = *fp.sc;
+    iters = e.brk ? e.it : e.it + 1;
+    const float r = e.r, DE = e.dr;
+    float d;
+    if (DE > 0.0f) {
+      const int fn = sc.is_hybrid ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
+      if (fn == 4) d = (r - sc.flinear_de_offset) / DE;
+      else if (fn == 2) d = (r > 1.0f) ? float(0.5f * r * logf(r) / DE) : 0.0f;
+      else if (fn == 1) d = r / DE;
+      else if (fn == 3) d = (r - 2.0f) / DE;
+      else d = r;
+    } else {
+      d = r;
+    }
+    if (iters < sc.min_n && d < detail) d = detail;
+    if (d < 0.0f) d = 0.0f;
+    if (d > 10.0f) d = 10.0f;
     return d;
   }
 };
@@ -584,7 +694,7 @@ struct PrimaryStage {
   }
 
   __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
-    if (MULTI) {
+    if constexpr (MULTI) {
       job = job_of(L.jobs, L.njobs, idx);
       jb = &L.jobs[job];
       fp = P::job_params(L, job);
@@ -792,7 +902,7 @@ struct NormalStage {
 
   __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
     r = &L.hits[idx];
-    if (MULTI) {
+    if constexpr (MULTI) {
       fp = P::job_params(L, r->job);
       kd = P::kind(fp);
     }
@@ -942,7 +1052,7 @@ struct ShadeStage {
     if (dv.w == 0.0f) return false;  // resolved by the direction kernel
     const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
     r = &L.hits[h];
-    if (MULTI) {
+    if constexpr (MULTI) {
       fp = P::job_params(L, r->job);
       kd = P::kind(fp);
     }
@@ -1153,6 +1263,372 @@ __global__ void batch_policy_kernel(const DevScene *scenes, const int *scene_of,
                            constant_thr, de_thresh);
 }
 
+// ============================================================================
+// Stage G: Monte Carlo GI paths (single-frame launches), one task per
+// (pixel, sample), numbered pixel-major.  A lane walks one path through the
+// phases of GlobalIlumination (src/shader_global_illumination.cpp:41-209) and
+// MonteCarloDOF (src/render_worker.cpp:1832-1862), as the plain kernel's
+// gi_path restates them: jittered thin-lens primary ray with the reference
+// march and binary search; at every vertex the six normal samples, a hard
+// sun-shadow march when the surface faces the sun, and a cosine bounce
+// marched with the GI step rule.  Random numbers come from the same PCG32
+// stream per (pixel, sample) and the same Park-Miller jitter stream as the
+// plain kernel's.  The path's radiance is added to its pixel in 32.32 fixed
+// point, so the sum does not depend on the order in which paths finish.
+// ============================================================================
+enum { G_MARCH = 0, G_BINARY, G_NORMAL, G_SHADOW, G_BOUNCE };
+
+template <class P>
+struct GIStage {
+  typedef double Real;
+  typedef typename P::D D;
+  static constexpr bool kMulti = false;
+  const DevFrame &fr;
+  const Launch &L;
+  const DevOutputs &out;
+  const WJob *jb;
+  typename P::Params fp;
+  int kd;
+  // path
+  unsigned long long ray;  // RNG stream id: frame pixel * samples + sample
+  long long pix;           // output index of the pixel
+  long long lpix;          // pixel of the launch (accumulator slot)
+  int sample, phase, bounce, sub, count, last_iters;
+  unsigned int pm;
+  Pcg32 rng;
+  double radiance, tp;
+  // current march
+  double ox, oy, oz, dx, dy, dz, t, stp, dir_len, thr;
+  double lx, ly, lz;  // previous primary request point (dead-ray check)
+  D dist_prev, search_limit;
+  // current vertex
+  double vx, vy, vz, vthr, nx, ny, nz, ndl;
+  unsigned int n_march, n_binary, n_gi;
+
+  __device__ const typename P::Params &params() const { return fp; }
+  __device__ int kind() const { return kd; }
+  __device__ D detail() const { return D(thr); }
+
+  // distThresh at q (render_worker.cpp:653-679), from the camera position
+  __device__ double thresh(double qx, double qy, double qz) const {
+    if (fr.constant_de_threshold) return fr.de_thresh;
+    const double ax = fr.camera[0] - qx, ay = fr.camera[1] - qy, az = fr.camera[2] - qz;
+    return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.detail_level;
+  }
+  __device__ void ray_point(double &qx, double &qy, double &qz) const {
+    qx = ox + dx * t;
+    qy = oy + dy * t;
+    qz = oz + dz * t;
+  }
+
+  __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
+    const unsigned long long spp = (unsigned long long)fr.gi_samples;
+    lpix = (long long)fdiv((unsigned long long)idx, L.div_spp);
+    sample = int((unsigned long long)idx - (unsigned long long)lpix * spp);
+    const unsigned long long yy = fdiv((unsigned long long)lpix, jb->div_w);
+    const int x = int((unsigned long long)lpix - yy * (unsigned long long)jb->width);
+    const int y = int(yy) + jb->row0;
+    const unsigned long long pixel = (unsigned long long)y * (unsigned long long)jb->width + (unsigned long long)x;
+    pix = jb->pixel_offset + (long long)pixel;
+    ray = pixel * spp + (unsigned long long)sample;
+    rng = pcg_init(fr.gi_seed, ray);
+    const double ujx = rng.uniform(), ujy = rng.uniform(), ulr = rng.uniform(), ula = rng.uniform();
+    double ix, iy;
+    image_point(fr, double(x), double(y), &ix, &iy);
+    ix = ix + (ujx - 0.5) / double(fr.width) * fr.aspect;
+    iy = iy + (ujy - 0.5) / double(fr.height);
+    D3 view = view_vector(fr, ix, iy);
+    const D3 cam = camera_of(fr);
+    D3 st = cam;
+    if (fr.dof_aperture > 0.0) {
+      const double randR = fr.dof_aperture * sqrt(ulr);
+      const double randAngle = 2.0 * 3.14159265358979323846 * ula;
+      double sa, ca;
+      sincos(randAngle, &sa, &ca);
+      const D3 rv = rotate(fr, D3{randR * sa, 0.0, randR * ca});
+      view = d3sub(view, d3mul(rv, 1.0 / fr.dof_focus));
+      st = d3add(cam, rv);
+    }
+    const D3 dir = d3norm(view);
+    ox = st.x;
+    oy = st.y;
+    oz = st.z;
+    dx = dir.x;
+    dy = dir.y;
+    dz = dir.z;
+    dir_len = d3len(dir);
+    pm = pm_for_ray(ray, fr.seed).s;
+    radiance = 0.0;
+    tp = 1.0;
+    bounce = 0;
+    phase = G_MARCH;
+    t = 0.0;
+    stp = 0.0;
+    count = 0;
+    sub = 0;
+    last_iters = 0;
+    thr = 0.0;
+    ray_point(qx, qy, qz);
+    if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) {  // stuck at once (render_worker.cpp:747-756)
+      if (sample == 0) {
+        if (out.depth) out.depth[pix] = t;
+        if (out.iters) out.iters[pix] = 0;
+        if (out.hit) out.hit[pix] = 1;
+      }
+      finish_path();
+      return false;
+    }
+    lx = qx;
+    ly = qy;
+    lz = qz;
+    thr = thresh(qx, qy, qz);
+    return true;
+  }
+
+  __device__ bool finish_path() {
+    atomicAdd(&L.acc[lpix], (unsigned long long)(radiance * 4294967296.0));
+    return false;
+  }
+
+  __device__ bool primary_miss() {
+    if (sample == 0) {
+      if (out.depth) out.depth[pix] = 1e20;
+      if (out.iters) out.iters[pix] = last_iters;
+      if (out.hit) out.hit[pix] = 0;
+    }
+    radiance = fr.gi_sky;
+    return finish_path();
+  }
+
+  // the primary ray found the surface at t: first vertex, then its normal
+  __device__ bool primary_hit(double &qx, double &qy, double &qz) {
+    ray_point(vx, vy, vz);
+    vthr = thr;
+    if (sample == 0) {
+      if (out.depth) out.depth[pix] = t;
+      if (out.iters) out.iters[pix] = last_iters;
+      if (out.hit) out.hit[pix] = 1;
+    }
+    return begin_normal(qx, qy, qz);
+  }
+
+  __device__ void normal_point(double &qx, double &qy, double &qz) const {
+    const double delta = vthr * fr.smoothness;
+    const double dd = (sub & 1) ? -delta : delta;
+    const int axis = sub >> 1;
+    qx = vx + (axis == 0 ? dd : 0.0);
+    qy = vy + (axis == 1 ? dd : 0.0);
+    qz = vz + (axis == 2 ? dd : 0.0);
+  }
+
+  __device__ bool begin_normal(double &qx, double &qy, double &qz) {
+    phase = G_NORMAL;
+    sub = 0;
+    nx = ny = nz = 0.0;
+    thr = vthr;
+    normal_point(qx, qy, qz);
+    return true;
+  }
+
+  __device__ bool after_shadow(double sh, double &qx, double &qy, double &qz) {
+    if (ndl > 0.0) radiance += tp * double(fr.albedo) * fr.gi_sun * ndl * sh;
+    if (bounce >= fr.gi_bounces) return finish_path();
+    tp *= double(fr.albedo);
+    const double u1 = rng.uniform(), u2 = rng.uniform();
+    const D3 d = cosine_dir(D3{nx, ny, nz}, u1, u2);
+    dx = d.x;
+    dy = d.y;
+    dz = d.z;
+    ox = vx;
+    oy = vy;
+    oz = vz;
+    phase = G_BOUNCE;
+    t = vthr;
+    count = 0;
+    if (!(t < fr.view_distance_max) || count >= fr.max_steps) {
+      radiance += tp * fr.gi_sky;
+      return finish_path();
+    }
+    ray_point(qx, qy, qz);
+    thr = thresh(qx, qy, qz);
+    return true;
+  }
+
+  // reference binary search step (render_worker.cpp:854-912)
+  __device__ bool binary_check(double &qx, double &qy, double &qz) {
+    if (sub >= fr.binary_steps || (double(dist_prev) < thr && double(dist_prev) > thr * double(search_limit)))
+      return primary_hit(qx, qy, qz);
+    if (double(dist_prev) > thr) t += stp;
+    else if (double(dist_prev) < thr * double(search_limit)) t -= stp;
+    ray_point(qx, qy, qz);
+    thr = thresh(qx, qy, qz);
+    return true;
+  }
+
+  __device__ bool step(D d, int iters, double &qx, double &qy, double &qz) {
+    switch (phase) {
+      case G_BINARY:
+        last_iters = iters;
+        n_binary++;
+        dist_prev = d;
+        stp *= 0.5;
+        sub++;
+        return binary_check(qx, qy, qz);
+      case G_MARCH: {
+        last_iters = iters;
+        n_march++;
+        count++;
+        if (double(d) < thr) {
+          stp *= 0.5;
+          sub = 0;
+          dist_prev = d;
+          phase = G_BINARY;
+          return binary_check(qx, qy, qz);
+        }
+        double jit = 1.0;
+        if (fr.jitter) {
+          ParkMiller p;
+          p.s = pm;
+          jit = 1.0 - p.random(1000) / 10000.0;
+          pm = p.s;
+        }
+        stp = (double(d) - 0.5 * thr) * fr.de_factor * jit;
+        if (stp > 3.0) stp = 3.0;
+        t += stp / dir_len;
+        if (t > fr.view_distance_max || count >= fr.max_steps) return primary_miss();
+        ray_point(qx, qy, qz);
+        if ((qx == lx && qy == ly && qz == lz) || !(isfinite(qx) && isfinite(qy) && isfinite(qz)))
+          return primary_hit(qx, qy, qz);
+        lx = qx;
+        ly = qy;
+        lz = qz;
+        thr = thresh(qx, qy, qz);
+        return true;
+      }
+      case G_NORMAL: {
+        n_gi++;
+        const bool neg = (sub & 1) != 0;
+        const int axis = sub >> 1;
+        double &comp = (axis == 0) ? nx : ((axis == 1) ? ny : nz);
+        comp = neg ? comp - double(d) : double(d);
+        sub++;
+        if (sub < 6) {
+          normal_point(qx, qy, qz);
+          return true;
+        }
+        // CalculateNormals tail (shader_calculate_normals.cpp:111-123)
+        if (fabs(nx) < 1e-50 && fabs(ny) < 1e-50 && fabs(nz) < 1e-50) {
+          nx = 1.0;
+          ny = nz = 0.0;
+        } else {
+          const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+          nx *= inv;
+          ny *= inv;
+          nz *= inv;
+        }
+        if (!(isfinite(nx) && isfinite(ny) && isfinite(nz))) {
+          nx = 1.0;
+          ny = nz = 0.0;
+        }
+        ndl = nx * fr.light[0] + ny * fr.light[1] + nz * fr.light[2];
+        if (!(ndl > 0.0)) return after_shadow(0.0, qx, qy, qz);
+        // hard AuxShadow toward the sun from the vertex (shader_aux_shadow.cpp:94-321)
+        phase = G_SHADOW;
+        t = vthr;
+        count = 0;
+        thr = vthr;
+        if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
+        ox = vx;
+        oy = vy;
+        oz = vz;
+        dx = fr.light[0];
+        dy = fr.light[1];
+        dz = fr.light[2];
+        ray_point(qx, qy, qz);
+        return true;
+      }
+      case G_SHADOW: {
+        n_gi++;
+        if (double(d) < double(float(vthr))) return after_shadow(0.0, qx, qy, qz);
+        const double s = fmax(fmin(double(d), 1000000.0) * fr.de_factor, 1e-15);
+        count++;
+        if (count > fr.max_steps) return after_shadow(1.0, qx, qy, qz);
+        t += s;
+        if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
+        ray_point(qx, qy, qz);
+        return true;
+      }
+      default: {  // G_BOUNCE: the GI march rule (shader_global_illumination.cpp:75-125)
+        n_gi++;
+        if (double(d) < thr) {
+          if (t < thr * 2.0) return finish_path();  // the bounce hit its own vertex
+          ray_point(vx, vy, vz);
+          vthr = thr;
+          bounce++;
+          return begin_normal(qx, qy, qz);
+        }
+        count++;
+        t += double(d) * fr.de_factor;
+        if (!(t < fr.view_distance_max) || count >= fr.max_steps) {
+          radiance += tp * fr.gi_sky;
+          return finish_path();
+        }
+        ray_point(qx, qy, qz);
+        thr = thresh(qx, qy, qz);
+        return true;
+      }
+    }
+  }
+};
+
+template <int FK, class P>
+__global__ void __launch_bounds__(256) gi_kernel(const __grid_constant__ DevFrame fr,
+                                                 const __grid_constant__ typename P::Params fp0,
+                                                 const __grid_constant__ WJob job0, const __grid_constant__ Launch L,
+                                                 DevOutputs out) {
+  if (gated_off(L)) return;
+  GIStage<P> S{fr, L, out, &job0, fp0, P::kind(fp0)};
+  S.search_limit = typename P::D(1.0 - 0.001 * fr.detail_level);
+  S.n_march = S.n_binary = S.n_gi = 0;
+  unsigned int my_de = 0;
+  unsigned long long my_iters = 0;
+  run_stage<FK, P>(S, fp0, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
+  flush_counts(out, my_de, my_iters, K_MARCH, S.n_march, K_BINARY, S.n_binary);
+  if (out.stats) {
+    const unsigned g = __reduce_add_sync(0xffffffffu, S.n_gi);
+    if ((threadIdx.x & 31) == 0 && g)
+      atomicAdd(reinterpret_cast<unsigned long long *>(out.stats) + K_GI, (unsigned long long)g);
+  }
+}
+
+// Stage F of a GI frame: the mean radiance of every pixel, its colour and the
+// outputs the plain kernel writes for GI (normal 0, shade 0, AO 1).
+__global__ void __launch_bounds__(256) gi_finish_kernel(const __grid_constant__ DevFrame fr,
+                                                        const __grid_constant__ WJob job0,
+                                                        const __grid_constant__ Launch L, DevOutputs out,
+                                                        long long pixels) {
+  if (gated_off(L)) return;
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels;
+       p += (long long)gridDim.x * blockDim.x) {
+    const long long pix = job0.pixel_offset + (long long)job0.row0 * job0.width + p;
+    const float v = float(double(L.acc[p]) * (1.0 / 4294967296.0) / double(fr.gi_samples));
+    float rgb[3] = {v, v, v};
+    if (out.normal) {
+      out.normal[3 * pix + 0] = 0.f;
+      out.normal[3 * pix + 1] = 0.f;
+      out.normal[3 * pix + 2] = 0.f;
+    }
+    if (out.shade) out.shade[pix] = 0.f;
+    if (out.ao) out.ao[pix] = 1.0f;
+    if (out.rgb) {
+      out.rgb[3 * pix + 0] = v;
+      out.rgb[3 * pix + 1] = v;
+      out.rgb[3 * pix + 2] = v;
+    }
+    if (out.rgb8) to_rgb8(fr, rgb, &out.rgb8[3 * pix]);
+  }
+}
+
 // ---- host side -------------------------------------------------------------------
 static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset) {
   WJob j;
@@ -1183,13 +1659,14 @@ static long long job_items(const WJob &j, int layout) {
   return (long long)j.width * j.rows;
 }
 
-static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr) {
-  if (sc.is_hybrid) return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: hybrid sequences use the plain engines");
+static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, bool batch) {
+  if (batch && (sc.is_hybrid || fr.gi_samples > 0))
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront batches: hybrid sequences and GI render one frame at a time");
   if (sc.iter_thresh || sc.interior || sc.has_w)
     return set_err(ctx, MBR_EUNSUPPORTED,
                    "wavefront engine: iteration_threshold_mode, interior_mode and initial_waxis != 0 use the plain engines");
-  if (fr.gi_samples > 0 || fr.refine != MBR_REFINE_REFERENCE)
-    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: GI and root refinement use the plain engines");
+  if (fr.refine != MBR_REFINE_REFERENCE)
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: root refinement uses the plain engines");
   return MBR_OK;
 }
 
@@ -1211,11 +1688,35 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
   const int sms = sm_count();
   const int grid = std::max(1, sms * tu.ctas_per_sm);
   const int block = tu.block_size;
+  if (P::kHyb) fk = FK_ANY;
   int e = int(cudaMemsetAsync(L.ctr, 0, sizeof(Counters4), st));
   if (e) return e;
+  if constexpr (!MULTI) {
+    if (fr.gi_samples > 0) {  // GI frame: stage G, then its colour stage
+      L.div_spp = make_fastdiv(fr.gi_samples);
+      e = int(cudaMemsetAsync(L.acc, 0, sizeof(unsigned long long) * size_t(pixels), st));
+      if (e) return e;
+      switch (fk) {
+#define GI_LAUNCH(K)                                                                            \
+  case K:                                                                                       \
+    if constexpr (!P::kHyb || K == FK_ANY) gi_kernel<K, P><<<grid, block, 0, st>>>(fr, fp0, j0, L, out); \
+    break;
+        GI_LAUNCH(FK_BOX_SIMPLE)
+        GI_LAUNCH(FK_BOX)
+        GI_LAUNCH(FK_BULB)
+        GI_LAUNCH(FK_MENGER)
+        GI_LAUNCH(FK_ANY)
+#undef GI_LAUNCH
+        default: return int(cudaErrorInvalidValue);
+      }
+      gi_finish_kernel<<<sms * 4, 256, 0, st>>>(fr, j0, L, out, pixels);
+      pixel_count_kernel<<<1, 32, 0, st>>>(L, out, pixels);
+      return int(cudaGetLastError());
+    }
+  }
 #define STAGE_LAUNCH(KERNEL, K, ...)                                                    \
   case K:                                                                               \
-    KERNEL<K, MULTI, P><<<grid, block, 0, st>>>(__VA_ARGS__);                           \
+    if constexpr (!P::kHyb || K == FK_ANY) KERNEL<K, MULTI, P><<<grid, block, 0, st>>>(__VA_ARGS__); \
     break;
 #define STAGE(KERNEL, ...)                                                              \
   switch (fk) {                                                                         \
@@ -1266,13 +1767,22 @@ static bool is_wavefront(int engine) {
 mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, const DevOutputs &out, int engine,
                             void *stream) {
   if (!is_wavefront(engine)) return set_err(ctx, MBR_EINVAL, "not a wavefront engine: %d", engine);
-  mbr_status stt = check_supported(ctx, sc, fr);
+  mbr_status stt = check_supported(ctx, sc, fr, false);
   if (stt != MBR_OK) return stt;
+  const bool gi = fr.gi_samples > 0, hyb = sc.is_hybrid != 0;
+  if (hyb && engine == MBR_ENGINE_WAVEFRONT_FP64)
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: hybrid sequences iterate in FP32 (MBR_ENGINE_WAVEFRONT_FP32 "
+                                          "or _AUTO); FP64 hybrids use MBR_ENGINE_PLAIN_FP64");
   const mbr_tuning tu = ctx_tuning(ctx);
   const WJob j0 = make_job(fr, 0, out.pixel_offset);
-  const long long total = job_items(j0, tu.queue_layout);
+  const long long pixels = (long long)fr.width * (fr.row1 - fr.row0);
+  const long long total = gi ? pixels * (long long)fr.gi_samples : job_items(j0, tu.queue_layout);
   const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
-  const size_t bytes = scratch_bytes(total, per);
+  // scratch: counters, then the GI accumulators or the hit records, then (a
+  // hybrid scene) the scene the iteration reads
+  const size_t main_bytes = gi ? 256 + sizeof(unsigned long long) * size_t(pixels) : scratch_bytes(total, per);
+  const size_t scene_at = (main_bytes + 255) / 256 * 256;
+  const size_t bytes = hyb ? scene_at + sizeof(DevScene) : main_bytes;
   unsigned long long *work = nullptr;
   stt = ctx_work(ctx, (bytes + 7) / 8, &work);
   if (stt != MBR_OK) return stt;
@@ -1283,7 +1793,12 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   L.wps = nullptr;
   L.njobs = 1;
   L.total = total;
-  scratch_layout(L, work, total);
+  if (gi) {
+    L.ctr = reinterpret_cast<Counters4 *>(work);
+    L.acc = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(work) + 256);
+  } else {
+    scratch_layout(L, work, total);
+  }
   L.refill_k = tu.refill_k;
   L.layout = tu.queue_layout;
   L.ao_rays = fr.ao_rays;
@@ -1291,9 +1806,14 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   L.want_normal = fr.want_normal;
   const FastParams fp = load_fast_params(sc);
   const WideParams wp = load_wide_params(sc);
-  const long long pixels = (long long)fr.width * (fr.row1 - fr.row0);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int e = 0;
+  if (hyb) {  // FP32 hybrid iteration reading the scene from the scratch
+    DevScene *d_sc = reinterpret_cast<DevScene *>(reinterpret_cast<char *>(work) + scene_at);
+    e = int(cudaMemcpyAsync(d_sc, &sc, sizeof(DevScene), cudaMemcpyHostToDevice, s));
+    if (!e) e = launch_pipeline<false, PrecHyb>(FK_ANY, tu, s, fr, HybParams{d_sc}, j0, L, out, pixels);
+    return cuda_err(ctx, e, "wavefront launch");
+  }
   if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {
     int *gate = scratch_gate(work);
     L.gate = gate;
@@ -1391,7 +1911,7 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
     DevFrame fr;
     mbr_status st = build_frame(ctx, jb.camera, *params, &fr);
     if (st != MBR_OK) return st;
-    st = check_supported(ctx, dsc[jb.scene_index], fr);
+    st = check_supported(ctx, dsc[jb.scene_index], fr, true);
     if (st != MBR_OK) return st;
     if (i == 0) fr0 = fr;
     wj[i] = make_job(fr, 0, jb.pixel_offset);

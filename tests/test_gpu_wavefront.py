@@ -118,7 +118,8 @@ def test_batch_matches_single_renders(renderer):
 def test_wavefront_rejects_unsupported(renderer):
     from mandelbulber2_b200.render import MbrError
 
-    sc, cam, p = configs.hybrid_gi_2160p(32, 18, spp=1)
+    sc, cam, p = configs.mandelbox_1080p("A", 32, 18)
+    p.refine = abi.REFINE_ROOT  # root refinement runs on the plain engines
     renderer.set_scene(sc)
     with pytest.raises(MbrError) as e:
         renderer.render(cam, p, WF)
