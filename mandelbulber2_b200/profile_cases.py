@@ -4,7 +4,9 @@
 
 cases: plain_fp64, plain_strict, plain_mixed, wavefront, wavefront64
 (Mandelbox s=-1.5, 960x540, camera A, 16 AO rays; two frames; wavefront64
-iterates in FP64), gi (hybrid Mandelbulb/Menger 480x270, 2 spp), adjoint
+iterates in FP64), gi and gi_wavefront (hybrid Mandelbulb/Menger 480x270,
+2 spp, on the plain mixed kernel and on the wavefront), hybrid_wavefront (the
+hybrid fractal, 480x270, Lambert + shadow + 4 AO rays), adjoint
 (Mandelbulb 256x256 forward + FP64 adjoint), distance (CalculateDistance at
 2^20 random points).
 """
@@ -37,9 +39,15 @@ def run(case: str) -> None:
     if case in FRAME_ENGINES:
         sc, cam, p = configs.mandelbox_1080p("A", 960, 540)
         frame(r, sc, cam, p, FRAME_ENGINES[case])
-    elif case == "gi":
+    elif case in ("gi", "gi_wavefront"):
         sc, cam, p = configs.hybrid_gi_2160p(480, 270, spp=2)
-        frame(r, sc, cam, p, abi.ENGINE_PLAIN_MIXED, reps=1)
+        frame(r, sc, cam, p, abi.ENGINE_PLAIN_MIXED if case == "gi" else abi.ENGINE_WAVEFRONT_FP32, reps=1)
+    elif case == "hybrid_wavefront":
+        sc = configs.hybrid_scene()
+        cam = configs.camera((0.0, -3.0, 0.5), width=480, height=270)
+        p = configs.base_params(5, 20.0)
+        p.ao_rays = 4
+        frame(r, sc, cam, p, abi.ENGINE_WAVEFRONT_FP32)
     elif case == "adjoint":
         sc, cam, p = configs.adjoint_256("mandelbulb", 256, 256)
         b = frame(r, sc, cam, p, abi.ENGINE_PLAIN_MIXED, reps=1)
