@@ -19,8 +19,8 @@
 // stages P, N and S each lane holds one task; it runs 2 to 12 formula
 // iterations (by formula) between warp votes and, once at most k lanes of the warp are still
 // iterating, the lanes whose estimate is done take their march step and
-// start their next request, or take the next task from the stage's device
-// counter (warp-aggregated atomicAdd).  Because a warp only ever runs one
+// start their next request, or take the next task from the warp's share of
+// the stage's queue (a chunk of tasks per atomicAdd on the stage's counter).  Because a warp only ever runs one
 // kind of march, those steps stay converged and cheap, and divergent orbit
 // lengths and march lengths cost only the k-lane wait.  A batch walks a job
 // table (per-job camera, image size and formula parameters) with the same
@@ -538,31 +538,43 @@ __device__ __forceinline__ void run_stage(Stage &S, const typename P::Params &fp
   const unsigned lanemask_lt = (1u << lane) - 1u;
   typename P::State e = {};
   bool has = false, iterating = false, drained = false;
+  long long q_next = 0, q_end = 0;  // the warp's unstarted tasks [q_next, q_end)
+  const long long warps = (long long)gridDim.x * (long long)(blockDim.x >> 5);
+  const int chunk = (int)min(64ll, max(1ll, total / (32ll * max(warps, 1ll))));
   unsigned int de_n = 0;
   unsigned long long it_n = 0;
   for (;;) {
-    // ---- refill lanes without a task
+    // ---- refill lanes without a task from the warp's share of the queue.
+    // A warp takes max(chunk, waiting lanes) tasks per atomic on the stage's
+    // counter; chunk grows with the tasks per resident warp (up to 64), so a
+    // large queue costs fewer atomics and dependent waits, while a small one
+    // keeps its tail balanced.
     unsigned need = __ballot_sync(FULL, !has && !drained);
     while (need) {
-      const int leader = __ffs(need) - 1;
-      unsigned long long base = 0ull;
-      if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(need));
-      base = __shfl_sync(FULL, base, leader);
-      bool empty = false;
-      if (!has && !drained) {
-        const long long idx = (long long)base + (long long)__popc(need & lanemask_lt);
-        if (idx < total) {
-          typename Stage::Real qx, qy, qz;
-          if (S.start(idx, qx, qy, qz)) {
-            P::start(e, Stage::kMulti ? S.params() : fpk, qx, qy, qz);
-            has = true;
-            iterating = true;
-          }
-        } else {
-          empty = true;
+      const int waiting = __popc(need);
+      if (q_next >= q_end) {
+        const int take_n = max(chunk, waiting);
+        unsigned long long base = 0ull;
+        if (lane == 0) base = atomicAdd(counter, (unsigned long long)take_n);
+        base = __shfl_sync(FULL, base, 0);
+        if ((long long)base >= total) {
+          drained = true;
+          break;
+        }
+        q_next = (long long)base;
+        q_end = min((long long)base + take_n, total);
+      }
+      const int take = (int)min((long long)waiting, q_end - q_next);
+      const int rank = __popc(need & lanemask_lt);
+      if (((need >> lane) & 1u) && rank < take) {
+        typename Stage::Real qx, qy, qz;
+        if (S.start(q_next + rank, qx, qy, qz)) {
+          P::start(e, Stage::kMulti ? S.params() : fpk, qx, qy, qz);
+          has = true;
+          iterating = true;
         }
       }
-      if (__any_sync(FULL, empty)) drained = true;
+      q_next += take;
       need = __ballot_sync(FULL, !has && !drained);
     }
     if (!__any_sync(FULL, iterating)) break;
@@ -1048,9 +1060,13 @@ struct ShadeStage {
   }
 
   __device__ bool start(long long idx, D &qx, D &qy, D &qz) {
-    const float4 dv = L.sdir[idx];
-    if (dv.w == 0.0f) return false;  // resolved by the direction kernel
+    // both start records are loaded before the first is tested: the origin's
+    // address depends on the task index only, so the two loads overlap
     const long long h = (long long)fdiv((unsigned long long)idx, L.div_per);
+    const float4 dv = L.sdir[idx];
+    float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!P::kWide) o = L.sorg[h];
+    if (dv.w == 0.0f) return false;  // resolved by the direction kernel
     r = &L.hits[h];
     if constexpr (MULTI) {
       fp = P::job_params(L, r->job);
@@ -1063,7 +1079,6 @@ struct ShadeStage {
       thr = float(r->thr);
       t = D(r->thr);
     } else {
-      const float4 o = L.sorg[h];
       ox = D(o.x);
       oy = D(o.y);
       oz = D(o.z);
