@@ -116,6 +116,22 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c) {
   return y;
 }
 
+// Blackwell's paired FP32 arithmetic (PTX fma.rn.f32x2): two lanes of an
+// FMA in one instruction on a 64-bit register pair
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long v;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(lo), "f"(hi));
+  return v;
+}
+__device__ __forceinline__ void unpack2(unsigned long long v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b, unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // 1/x from the MUFU unit (max. 1 ulp; 0 -> +inf, flushes denormals)
 __device__ __forceinline__ float rcp_approx(float x) {
   float y;
@@ -135,8 +151,10 @@ template <bool SIMPLE>
 __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, const FastParams &f) {
   if (SIMPLE) {
     const float L2 = 0.5f * f.q1;  // 2L
-    z.x = fmaf(f.q1, fma_sat(z.x, f.q0, 0.5f), -z.x) - L2;
-    z.y = fmaf(f.q1, fma_sat(z.y, f.q0, 0.5f), -z.y) - L2;
+    // x and y of the box fold in one f32x2 register pair: w = -z - 2L, then
+    // 4L * sat(...) + w - two paired FMAs where the scalar form issues four
+    const unsigned long long w = ffma2(pack2(z.x, z.y), pack2(-1.0f, -1.0f), pack2(-L2, -L2));
+    unpack2(ffma2(pack2(f.q1, f.q1), pack2(fma_sat(z.x, f.q0, 0.5f), fma_sat(z.y, f.q0, 0.5f)), w), z.x, z.y);
     z.z = fmaf(f.q1, fma_sat(z.z, f.q0, 0.5f), -z.z) - L2;
     const float r2 = fmaf(z.x, z.x, fmaf(z.y, z.y, z.z * z.z));
     // factor = 1 + (F-1) * sat((fR2/r2 - 1) / (F-1)); r2 = 0 gives +inf -> factor F
