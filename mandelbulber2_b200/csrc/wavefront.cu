@@ -170,8 +170,14 @@ struct Launch {
   int shadow_tasks;        // 1 when the shadow march runs (shading && shadow)
   int want_normal;
   FastDiv div_per;         // division by shadow_tasks + ao_rays (set by launch_pipeline)
-  unsigned long long *acc;  // GI: per pixel of the launch, summed radiance in 32.32 fixed point
-  FastDiv div_spp;          // GI: division by samples per pixel
+  // GI frames
+  double *path_rad;              // radiance of every path of the launch
+  HitRec *hits_next;             // the next level's vertex list
+  unsigned long long *next_hits; // its counter
+  FastDiv div_spp;               // division by samples per pixel
+  int level;                     // bounce level of the vertex list in `hits`
+  int row0;                      // first row of the launch
+  int normal_slot;               // stats counter of stage N (K_NORMAL; K_GI in GI frames)
 };
 
 // True when this pipeline's kernels have nothing to do (the other precision
@@ -1005,7 +1011,8 @@ __global__ void __launch_bounds__(256) normal_kernel(const __grid_constant__ Dev
   unsigned long long my_iters = 0;
   const long long total = (long long)L.ctr->hits;
   run_stage<FK, P>(S, fp0, &L.ctr->normals_next, total, L.refill_k, &my_de, &my_iters);
-  flush_counts(out, my_de, my_iters, K_NORMAL, my_de, K_NORMAL, 0);
+  const int slot = L.normal_slot ? L.normal_slot : K_NORMAL;
+  flush_counts(out, my_de, my_iters, slot, my_de, slot, 0);
 }
 
 // ============================================================================
@@ -1279,22 +1286,36 @@ __global__ void batch_policy_kernel(const DevScene *scenes, const int *scene_of,
 }
 
 // ============================================================================
-// Stage G: Monte Carlo GI paths (single-frame launches), one task per
-// (pixel, sample), numbered pixel-major.  A lane walks one path through the
-// phases of GlobalIlumination (src/shader_global_illumination.cpp:41-209) and
-// MonteCarloDOF (src/render_worker.cpp:1832-1862), as the plain kernel's
-// gi_path restates them: jittered thin-lens primary ray with the reference
-// march and binary search; at every vertex the six normal samples, a hard
-// sun-shadow march when the surface faces the sun, and a cosine bounce
-// marched with the GI step rule.  Random numbers come from the same PCG32
-// stream per (pixel, sample) and the same Park-Miller jitter stream as the
-// plain kernel's.  The path's radiance is added to its pixel in 32.32 fixed
-// point, so the sum does not depend on the order in which paths finish.
+// GI frames (single-frame launches).  Monte Carlo paths of GlobalIlumination
+// (src/shader_global_illumination.cpp:41-209) with MonteCarloDOF
+// (src/render_worker.cpp:1832-1862), as the plain kernel's gi_path restates
+// them, split into stages like the frame pipeline:
+//   stage GP  one task per path (pixel, sample), pixel-major: the jittered
+//             thin-lens primary ray, the reference march and binary search;
+//             a hit appends the path's first vertex to the level-0 list
+//   per level b = 0 .. bounces:
+//     stage N   the six normal samples of every vertex of level b
+//     stage GV  per vertex: the hard sun-shadow march when the surface faces
+//               the sun, its radiance term, then (b < bounces) the cosine
+//               bounce marched with the GI step rule; a hit appends the next
+//               vertex to the level-b+1 list, a miss adds the sky
+//   stage GF  per pixel: the path radiances summed in sample order.
+// Random numbers come from the same PCG32 stream per (pixel, sample) and the
+// same Park-Miller jitter stream as the plain kernel's: the bounce of level b
+// takes draws 4 + 2b and 5 + 2b, reached by jump-ahead.  A path's radiance
+// terms are added in the plain kernel's order by one thread at a time.
 // ============================================================================
-enum { G_MARCH = 0, G_BINARY, G_NORMAL, G_SHADOW, G_BOUNCE };
+enum { G_MARCH = 0, G_BINARY, G_SHADOW, G_BOUNCE };
+
+// distThresh at q (render_worker.cpp:653-679), from the camera position
+__device__ __forceinline__ double gi_thresh(const DevFrame &fr, double qx, double qy, double qz) {
+  if (fr.constant_de_threshold) return fr.de_thresh;
+  const double ax = fr.camera[0] - qx, ay = fr.camera[1] - qy, az = fr.camera[2] - qz;
+  return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.detail_level;
+}
 
 template <class P>
-struct GIStage {
+struct GIPrimaryStage {
   typedef double Real;
   typedef typename P::D D;
   static constexpr bool kMulti = false;
@@ -1304,32 +1325,19 @@ struct GIStage {
   const WJob *jb;
   typename P::Params fp;
   int kd;
-  // path
   unsigned long long ray;  // RNG stream id: frame pixel * samples + sample
   long long pix;           // output index of the pixel
-  long long lpix;          // pixel of the launch (accumulator slot)
-  int sample, phase, bounce, sub, count, last_iters;
+  long long path;          // path of the launch: pixel of the launch * samples + sample
+  int sample, phase, sub, count, last_iters;
   unsigned int pm;
-  Pcg32 rng;
-  double radiance, tp;
-  // current march
   double ox, oy, oz, dx, dy, dz, t, stp, dir_len, thr;
-  double lx, ly, lz;  // previous primary request point (dead-ray check)
+  double lx, ly, lz;  // previous request point (dead-ray check)
   D dist_prev, search_limit;
-  // current vertex
-  double vx, vy, vz, vthr, nx, ny, nz, ndl;
-  unsigned int n_march, n_binary, n_gi;
+  unsigned int n_march, n_binary;
 
   __device__ const typename P::Params &params() const { return fp; }
   __device__ int kind() const { return kd; }
   __device__ D detail() const { return D(thr); }
-
-  // distThresh at q (render_worker.cpp:653-679), from the camera position
-  __device__ double thresh(double qx, double qy, double qz) const {
-    if (fr.constant_de_threshold) return fr.de_thresh;
-    const double ax = fr.camera[0] - qx, ay = fr.camera[1] - qy, az = fr.camera[2] - qz;
-    return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.detail_level;
-  }
   __device__ void ray_point(double &qx, double &qy, double &qz) const {
     qx = ox + dx * t;
     qy = oy + dy * t;
@@ -1338,15 +1346,16 @@ struct GIStage {
 
   __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
     const unsigned long long spp = (unsigned long long)fr.gi_samples;
-    lpix = (long long)fdiv((unsigned long long)idx, L.div_spp);
-    sample = int((unsigned long long)idx - (unsigned long long)lpix * spp);
-    const unsigned long long yy = fdiv((unsigned long long)lpix, jb->div_w);
-    const int x = int((unsigned long long)lpix - yy * (unsigned long long)jb->width);
+    path = idx;
+    const unsigned long long lpix = fdiv((unsigned long long)idx, L.div_spp);
+    sample = int((unsigned long long)idx - lpix * spp);
+    const unsigned long long yy = fdiv(lpix, jb->div_w);
+    const int x = int(lpix - yy * (unsigned long long)jb->width);
     const int y = int(yy) + jb->row0;
     const unsigned long long pixel = (unsigned long long)y * (unsigned long long)jb->width + (unsigned long long)x;
     pix = jb->pixel_offset + (long long)pixel;
     ray = pixel * spp + (unsigned long long)sample;
-    rng = pcg_init(fr.gi_seed, ray);
+    Pcg32 rng = pcg_init(fr.gi_seed, ray);
     const double ujx = rng.uniform(), ujy = rng.uniform(), ulr = rng.uniform(), ula = rng.uniform();
     double ix, iy;
     image_point(fr, double(x), double(y), &ix, &iy);
@@ -1373,9 +1382,6 @@ struct GIStage {
     dz = dir.z;
     dir_len = d3len(dir);
     pm = pm_for_ray(ray, fr.seed).s;
-    radiance = 0.0;
-    tp = 1.0;
-    bounce = 0;
     phase = G_MARCH;
     t = 0.0;
     stp = 0.0;
@@ -1385,70 +1391,162 @@ struct GIStage {
     thr = 0.0;
     ray_point(qx, qy, qz);
     if (!(isfinite(qx) && isfinite(qy) && isfinite(qz))) {  // stuck at once (render_worker.cpp:747-756)
-      if (sample == 0) {
-        if (out.depth) out.depth[pix] = t;
-        if (out.iters) out.iters[pix] = 0;
-        if (out.hit) out.hit[pix] = 1;
-      }
-      finish_path();
+      hit();
       return false;
     }
     lx = qx;
     ly = qy;
     lz = qz;
-    thr = thresh(qx, qy, qz);
+    thr = gi_thresh(fr, qx, qy, qz);
     return true;
   }
 
-  __device__ bool finish_path() {
-    atomicAdd(&L.acc[lpix], (unsigned long long)(radiance * 4294967296.0));
-    return false;
-  }
-
-  __device__ bool primary_miss() {
+  __device__ bool miss() {
     if (sample == 0) {
       if (out.depth) out.depth[pix] = 1e20;
       if (out.iters) out.iters[pix] = last_iters;
       if (out.hit) out.hit[pix] = 0;
     }
-    radiance = fr.gi_sky;
-    return finish_path();
+    L.path_rad[path] = fr.gi_sky;
+    return false;
   }
 
-  // the primary ray found the surface at t: first vertex, then its normal
-  __device__ bool primary_hit(double &qx, double &qy, double &qz) {
-    ray_point(vx, vy, vz);
-    vthr = thr;
+  // the primary ray found the surface at t: the path's first vertex
+  __device__ bool hit() {
     if (sample == 0) {
       if (out.depth) out.depth[pix] = t;
       if (out.iters) out.iters[pix] = last_iters;
       if (out.hit) out.hit[pix] = 1;
     }
-    return begin_normal(qx, qy, qz);
+    L.path_rad[path] = 0.0;
+    const unsigned long long h = atomicAdd(&L.ctr->hits, 1ull);
+    HitRec &r = L.hits[h];
+    ray_point(r.px, r.py, r.pz);
+    r.depth = t;
+    r.thr = thr;
+    r.pix = path;
+    r.iters = last_iters;
+    r.nx = 1.f;
+    r.ny = r.nz = 0.f;
+    r.job = 0;
+    return false;
   }
 
-  __device__ void normal_point(double &qx, double &qy, double &qz) const {
-    const double delta = vthr * fr.smoothness;
-    const double dd = (sub & 1) ? -delta : delta;
-    const int axis = sub >> 1;
-    qx = vx + (axis == 0 ? dd : 0.0);
-    qy = vy + (axis == 1 ? dd : 0.0);
-    qz = vz + (axis == 2 ? dd : 0.0);
+  // reference binary search step (render_worker.cpp:854-912)
+  __device__ bool binary_check(double &qx, double &qy, double &qz) {
+    if (sub >= fr.binary_steps || (double(dist_prev) < thr && double(dist_prev) > thr * double(search_limit)))
+      return hit();
+    if (double(dist_prev) > thr) t += stp;
+    else if (double(dist_prev) < thr * double(search_limit)) t -= stp;
+    ray_point(qx, qy, qz);
+    thr = gi_thresh(fr, qx, qy, qz);
+    return true;
   }
 
-  __device__ bool begin_normal(double &qx, double &qy, double &qz) {
-    phase = G_NORMAL;
-    sub = 0;
-    nx = ny = nz = 0.0;
+  __device__ bool step(D d, int iters, double &qx, double &qy, double &qz) {
+    last_iters = iters;
+    if (phase == G_BINARY) {
+      n_binary++;
+      dist_prev = d;
+      stp *= 0.5;
+      sub++;
+      return binary_check(qx, qy, qz);
+    }
+    n_march++;
+    count++;
+    if (double(d) < thr) {
+      stp *= 0.5;
+      sub = 0;
+      dist_prev = d;
+      phase = G_BINARY;
+      return binary_check(qx, qy, qz);
+    }
+    double jit = 1.0;
+    if (fr.jitter) {
+      ParkMiller p;
+      p.s = pm;
+      jit = 1.0 - p.random(1000) / 10000.0;
+      pm = p.s;
+    }
+    stp = (double(d) - 0.5 * thr) * fr.de_factor * jit;
+    if (stp > 3.0) stp = 3.0;
+    t += stp / dir_len;
+    if (t > fr.view_distance_max || count >= fr.max_steps) return miss();
+    ray_point(qx, qy, qz);
+    if ((qx == lx && qy == ly && qz == lz) || !(isfinite(qx) && isfinite(qy) && isfinite(qz))) return hit();
+    lx = qx;
+    ly = qy;
+    lz = qz;
+    thr = gi_thresh(fr, qx, qy, qz);
+    return true;
+  }
+};
+
+template <class P>
+struct GIVertexStage {
+  typedef double Real;
+  typedef typename P::D D;
+  static constexpr bool kMulti = false;
+  const DevFrame &fr;
+  const Launch &L;
+  typename P::Params fp;
+  int kd;
+  long long path;
+  int phase, count;
+  double tp, vx, vy, vz, vthr, nx, ny, nz, ndl;
+  double ox, oy, oz, dx, dy, dz, t, thr;
+  unsigned int n_gi;
+
+  __device__ const typename P::Params &params() const { return fp; }
+  __device__ int kind() const { return kd; }
+  __device__ D detail() const { return D(thr); }
+  __device__ void ray_point(double &qx, double &qy, double &qz) const {
+    qx = ox + dx * t;
+    qy = oy + dy * t;
+    qz = oz + dz * t;
+  }
+
+  __device__ bool start(long long idx, double &qx, double &qy, double &qz) {
+    const HitRec &r = L.hits[idx];
+    path = r.pix;
+    vx = r.px;
+    vy = r.py;
+    vz = r.pz;
+    vthr = r.thr;
+    nx = double(r.nx);
+    ny = double(r.ny);
+    nz = double(r.nz);
+    ndl = nx * fr.light[0] + ny * fr.light[1] + nz * fr.light[2];
+    tp = 1.0;
+    for (int b = 0; b < L.level; b++) tp *= double(fr.albedo);
+    if (!(ndl > 0.0)) return after_shadow(0.0, qx, qy, qz);
+    // hard AuxShadow toward the sun from the vertex (shader_aux_shadow.cpp:94-321)
+    phase = G_SHADOW;
+    t = vthr;
+    count = 0;
     thr = vthr;
-    normal_point(qx, qy, qz);
+    if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
+    ox = vx;
+    oy = vy;
+    oz = vz;
+    dx = fr.light[0];
+    dy = fr.light[1];
+    dz = fr.light[2];
+    ray_point(qx, qy, qz);
     return true;
   }
 
   __device__ bool after_shadow(double sh, double &qx, double &qy, double &qz) {
-    if (ndl > 0.0) radiance += tp * double(fr.albedo) * fr.gi_sun * ndl * sh;
-    if (bounce >= fr.gi_bounces) return finish_path();
+    if (ndl > 0.0) L.path_rad[path] += tp * double(fr.albedo) * fr.gi_sun * ndl * sh;
+    if (L.level >= fr.gi_bounces) return false;
     tp *= double(fr.albedo);
+    // the bounce's two draws of the path's stream
+    const unsigned long long spp = (unsigned long long)fr.gi_samples;
+    const unsigned long long lpix = fdiv((unsigned long long)path, L.div_spp);
+    const unsigned long long sample = (unsigned long long)path - lpix * spp;
+    const unsigned long long ray = ((unsigned long long)L.row0 * (unsigned long long)fr.width + lpix) * spp + sample;
+    Pcg32 rng = pcg_init(fr.gi_seed, ray);
+    rng.state = pcg_advance(rng.state, rng.inc, 4ull + 2ull * (unsigned long long)L.level);
     const double u1 = rng.uniform(), u2 = rng.uniform();
     const D3 d = cosine_dir(D3{nx, ny, nz}, u1, u2);
     dx = d.x;
@@ -1461,172 +1559,97 @@ struct GIStage {
     t = vthr;
     count = 0;
     if (!(t < fr.view_distance_max) || count >= fr.max_steps) {
-      radiance += tp * fr.gi_sky;
-      return finish_path();
+      L.path_rad[path] += tp * fr.gi_sky;
+      return false;
     }
     ray_point(qx, qy, qz);
-    thr = thresh(qx, qy, qz);
+    thr = gi_thresh(fr, qx, qy, qz);
     return true;
   }
 
-  // reference binary search step (render_worker.cpp:854-912)
-  __device__ bool binary_check(double &qx, double &qy, double &qz) {
-    if (sub >= fr.binary_steps || (double(dist_prev) < thr && double(dist_prev) > thr * double(search_limit)))
-      return primary_hit(qx, qy, qz);
-    if (double(dist_prev) > thr) t += stp;
-    else if (double(dist_prev) < thr * double(search_limit)) t -= stp;
-    ray_point(qx, qy, qz);
-    thr = thresh(qx, qy, qz);
-    return true;
-  }
-
-  __device__ bool step(D d, int iters, double &qx, double &qy, double &qz) {
-    switch (phase) {
-      case G_BINARY:
-        last_iters = iters;
-        n_binary++;
-        dist_prev = d;
-        stp *= 0.5;
-        sub++;
-        return binary_check(qx, qy, qz);
-      case G_MARCH: {
-        last_iters = iters;
-        n_march++;
-        count++;
-        if (double(d) < thr) {
-          stp *= 0.5;
-          sub = 0;
-          dist_prev = d;
-          phase = G_BINARY;
-          return binary_check(qx, qy, qz);
-        }
-        double jit = 1.0;
-        if (fr.jitter) {
-          ParkMiller p;
-          p.s = pm;
-          jit = 1.0 - p.random(1000) / 10000.0;
-          pm = p.s;
-        }
-        stp = (double(d) - 0.5 * thr) * fr.de_factor * jit;
-        if (stp > 3.0) stp = 3.0;
-        t += stp / dir_len;
-        if (t > fr.view_distance_max || count >= fr.max_steps) return primary_miss();
-        ray_point(qx, qy, qz);
-        if ((qx == lx && qy == ly && qz == lz) || !(isfinite(qx) && isfinite(qy) && isfinite(qz)))
-          return primary_hit(qx, qy, qz);
-        lx = qx;
-        ly = qy;
-        lz = qz;
-        thr = thresh(qx, qy, qz);
-        return true;
-      }
-      case G_NORMAL: {
-        n_gi++;
-        const bool neg = (sub & 1) != 0;
-        const int axis = sub >> 1;
-        double &comp = (axis == 0) ? nx : ((axis == 1) ? ny : nz);
-        comp = neg ? comp - double(d) : double(d);
-        sub++;
-        if (sub < 6) {
-          normal_point(qx, qy, qz);
-          return true;
-        }
-        // CalculateNormals tail (shader_calculate_normals.cpp:111-123)
-        if (fabs(nx) < 1e-50 && fabs(ny) < 1e-50 && fabs(nz) < 1e-50) {
-          nx = 1.0;
-          ny = nz = 0.0;
-        } else {
-          const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
-          nx *= inv;
-          ny *= inv;
-          nz *= inv;
-        }
-        if (!(isfinite(nx) && isfinite(ny) && isfinite(nz))) {
-          nx = 1.0;
-          ny = nz = 0.0;
-        }
-        ndl = nx * fr.light[0] + ny * fr.light[1] + nz * fr.light[2];
-        if (!(ndl > 0.0)) return after_shadow(0.0, qx, qy, qz);
-        // hard AuxShadow toward the sun from the vertex (shader_aux_shadow.cpp:94-321)
-        phase = G_SHADOW;
-        t = vthr;
-        count = 0;
-        thr = vthr;
-        if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
-        ox = vx;
-        oy = vy;
-        oz = vz;
-        dx = fr.light[0];
-        dy = fr.light[1];
-        dz = fr.light[2];
-        ray_point(qx, qy, qz);
-        return true;
-      }
-      case G_SHADOW: {
-        n_gi++;
-        if (double(d) < double(float(vthr))) return after_shadow(0.0, qx, qy, qz);
-        const double s = fmax(fmin(double(d), 1000000.0) * fr.de_factor, 1e-15);
-        count++;
-        if (count > fr.max_steps) return after_shadow(1.0, qx, qy, qz);
-        t += s;
-        if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
-        ray_point(qx, qy, qz);
-        return true;
-      }
-      default: {  // G_BOUNCE: the GI march rule (shader_global_illumination.cpp:75-125)
-        n_gi++;
-        if (double(d) < thr) {
-          if (t < thr * 2.0) return finish_path();  // the bounce hit its own vertex
-          ray_point(vx, vy, vz);
-          vthr = thr;
-          bounce++;
-          return begin_normal(qx, qy, qz);
-        }
-        count++;
-        t += double(d) * fr.de_factor;
-        if (!(t < fr.view_distance_max) || count >= fr.max_steps) {
-          radiance += tp * fr.gi_sky;
-          return finish_path();
-        }
-        ray_point(qx, qy, qz);
-        thr = thresh(qx, qy, qz);
-        return true;
-      }
+  __device__ bool step(D d, int, double &qx, double &qy, double &qz) {
+    n_gi++;
+    if (phase == G_SHADOW) {
+      if (double(d) < double(float(vthr))) return after_shadow(0.0, qx, qy, qz);
+      const double s = fmax(fmin(double(d), 1000000.0) * fr.de_factor, 1e-15);
+      count++;
+      if (count > fr.max_steps) return after_shadow(1.0, qx, qy, qz);
+      t += s;
+      if (!(t < fr.view_distance_max)) return after_shadow(1.0, qx, qy, qz);
+      ray_point(qx, qy, qz);
+      return true;
     }
+    // G_BOUNCE: the GI march rule (shader_global_illumination.cpp:75-125)
+    if (double(d) < thr) {
+      if (t < thr * 2.0) return false;  // the bounce hit its own vertex
+      const unsigned long long h = atomicAdd(L.next_hits, 1ull);
+      HitRec &r = L.hits_next[h];
+      ray_point(r.px, r.py, r.pz);
+      r.depth = t;
+      r.thr = thr;
+      r.pix = path;
+      r.iters = 0;
+      r.nx = 1.f;
+      r.ny = r.nz = 0.f;
+      r.job = 0;
+      return false;
+    }
+    count++;
+    t += double(d) * fr.de_factor;
+    if (!(t < fr.view_distance_max) || count >= fr.max_steps) {
+      L.path_rad[path] += tp * fr.gi_sky;
+      return false;
+    }
+    ray_point(qx, qy, qz);
+    thr = gi_thresh(fr, qx, qy, qz);
+    return true;
   }
 };
 
 template <int FK, class P>
-__global__ void __launch_bounds__(256) gi_kernel(const __grid_constant__ DevFrame fr,
-                                                 const __grid_constant__ typename P::Params fp0,
-                                                 const __grid_constant__ WJob job0, const __grid_constant__ Launch L,
-                                                 DevOutputs out) {
+__global__ void __launch_bounds__(256) gi_primary_kernel(const __grid_constant__ DevFrame fr,
+                                                         const __grid_constant__ typename P::Params fp0,
+                                                         const __grid_constant__ WJob job0,
+                                                         const __grid_constant__ Launch L, DevOutputs out) {
   if (gated_off(L)) return;
-  GIStage<P> S{fr, L, out, &job0, fp0, P::kind(fp0)};
+  GIPrimaryStage<P> S{fr, L, out, &job0, fp0, P::kind(fp0)};
   S.search_limit = typename P::D(1.0 - 0.001 * fr.detail_level);
-  S.n_march = S.n_binary = S.n_gi = 0;
+  S.n_march = S.n_binary = 0;
   unsigned int my_de = 0;
   unsigned long long my_iters = 0;
   run_stage<FK, P>(S, fp0, &L.ctr->pixels_next, L.total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_MARCH, S.n_march, K_BINARY, S.n_binary);
-  if (out.stats) {
-    const unsigned g = __reduce_add_sync(0xffffffffu, S.n_gi);
-    if ((threadIdx.x & 31) == 0 && g)
-      atomicAdd(reinterpret_cast<unsigned long long *>(out.stats) + K_GI, (unsigned long long)g);
-  }
 }
 
-// Stage F of a GI frame: the mean radiance of every pixel, its colour and the
-// outputs the plain kernel writes for GI (normal 0, shade 0, AO 1).
+template <int FK, class P>
+__global__ void __launch_bounds__(256) gi_vertex_kernel(const __grid_constant__ DevFrame fr,
+                                                        const __grid_constant__ typename P::Params fp0,
+                                                        const __grid_constant__ Launch L, DevOutputs out) {
+  if (gated_off(L)) return;
+  GIVertexStage<P> S{fr, L, fp0, P::kind(fp0)};
+  S.n_gi = 0;
+  unsigned int my_de = 0;
+  unsigned long long my_iters = 0;
+  const long long total = (long long)L.ctr->hits;
+  run_stage<FK, P>(S, fp0, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
+  flush_counts(out, my_de, my_iters, K_GI, S.n_gi, K_GI, 0);
+}
+
+// Stage GF: the mean radiance of every pixel (its paths summed in sample
+// order, as the plain kernel sums them), its colour and the outputs the plain
+// kernel writes for GI (normal 0, shade 0, AO 1).
 __global__ void __launch_bounds__(256) gi_finish_kernel(const __grid_constant__ DevFrame fr,
                                                         const __grid_constant__ WJob job0,
                                                         const __grid_constant__ Launch L, DevOutputs out,
                                                         long long pixels) {
   if (gated_off(L)) return;
+  const int spp = fr.gi_samples;
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pixels;
        p += (long long)gridDim.x * blockDim.x) {
     const long long pix = job0.pixel_offset + (long long)job0.row0 * job0.width + p;
-    const float v = float(double(L.acc[p]) * (1.0 / 4294967296.0) / double(fr.gi_samples));
+    double acc = 0.0;
+    for (int s = 0; s < spp; s++) acc += L.path_rad[p * spp + s];
+    const float v = float(acc / double(spp));
     float rgb[3] = {v, v, v};
     if (out.normal) {
       out.normal[3 * pix + 0] = 0.f;
@@ -1707,23 +1730,52 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
   int e = int(cudaMemsetAsync(L.ctr, 0, sizeof(Counters4), st));
   if (e) return e;
   if constexpr (!MULTI) {
-    if (fr.gi_samples > 0) {  // GI frame: stage G, then its colour stage
+    if (fr.gi_samples > 0) {  // GI frame: stage GP, then per level stages N and GV, then GF
       L.div_spp = make_fastdiv(fr.gi_samples);
-      e = int(cudaMemsetAsync(L.acc, 0, sizeof(unsigned long long) * size_t(pixels), st));
+      L.row0 = fr.row0;
+      Counters4 *ctrs = L.ctr;
+      HitRec *lists[2] = {L.hits, L.hits_next};
+      e = int(cudaMemsetAsync(ctrs, 0, sizeof(Counters4) * size_t(fr.gi_bounces + 2), st));
       if (e) return e;
-      switch (fk) {
-#define GI_LAUNCH(K)                                                                            \
-  case K:                                                                                       \
-    if constexpr (!P::kHyb || K == FK_ANY) gi_kernel<K, P><<<grid, block, 0, st>>>(fr, fp0, j0, L, out); \
+#define GI_CASES(LAUNCH)         \
+  switch (fk) {                  \
+    LAUNCH(FK_BOX_SIMPLE)        \
+    LAUNCH(FK_BOX)               \
+    LAUNCH(FK_BULB)              \
+    LAUNCH(FK_MENGER)            \
+    LAUNCH(FK_ANY)               \
+    default: return int(cudaErrorInvalidValue); \
+  }
+      {
+        Launch Lp = L;
+        Lp.ctr = &ctrs[0];
+        Lp.hits = lists[0];
+#define GP_LAUNCH(K) \
+  case K:            \
+    if constexpr (!P::kHyb || K == FK_ANY) gi_primary_kernel<K, P><<<grid, block, 0, st>>>(fr, fp0, j0, Lp, out); \
     break;
-        GI_LAUNCH(FK_BOX_SIMPLE)
-        GI_LAUNCH(FK_BOX)
-        GI_LAUNCH(FK_BULB)
-        GI_LAUNCH(FK_MENGER)
-        GI_LAUNCH(FK_ANY)
-#undef GI_LAUNCH
-        default: return int(cudaErrorInvalidValue);
+        GI_CASES(GP_LAUNCH)
+#undef GP_LAUNCH
       }
+      for (int b = 0; b <= fr.gi_bounces; b++) {
+        Launch Lb = L;
+        Lb.ctr = &ctrs[b];
+        Lb.hits = lists[b & 1];
+        Lb.hits_next = lists[(b + 1) & 1];
+        Lb.next_hits = &ctrs[b + 1].hits;
+        Lb.level = b;
+        Lb.normal_slot = K_GI;
+#define GV_LAUNCH(K)                                                                                   \
+  case K:                                                                                              \
+    if constexpr (!P::kHyb || K == FK_ANY) {                                                           \
+      normal_kernel<K, false, P><<<grid, block, 0, st>>>(fr, fp0, Lb, out);                             \
+      gi_vertex_kernel<K, P><<<grid, block, 0, st>>>(fr, fp0, Lb, out);                                 \
+    }                                                                                                  \
+    break;
+        GI_CASES(GV_LAUNCH)
+#undef GV_LAUNCH
+      }
+#undef GI_CASES
       gi_finish_kernel<<<sms * 4, 256, 0, st>>>(fr, j0, L, out, pixels);
       pixel_count_kernel<<<1, 32, 0, st>>>(L, out, pixels);
       return int(cudaGetLastError());
@@ -1785,6 +1837,8 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   mbr_status stt = check_supported(ctx, sc, fr, false);
   if (stt != MBR_OK) return stt;
   const bool gi = fr.gi_samples > 0, hyb = sc.is_hybrid != 0;
+  if (gi && fr.gi_bounces > 120)
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: GI with more than 120 bounces uses the plain engines");
   if (hyb && engine == MBR_ENGINE_WAVEFRONT_FP64)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: hybrid sequences iterate in FP32 (MBR_ENGINE_WAVEFRONT_FP32 "
                                           "or _AUTO); FP64 hybrids use MBR_ENGINE_PLAIN_FP64");
@@ -1795,7 +1849,11 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
   // scratch: counters, then the GI accumulators or the hit records, then (a
   // hybrid scene) the scene the iteration reads
-  const size_t main_bytes = gi ? 256 + sizeof(unsigned long long) * size_t(pixels) : scratch_bytes(total, per);
+  // GI: a counter block per bounce level (4 KiB), the auto-engine flag, the
+  // path radiances and two vertex lists of one entry per path
+  const size_t gi_head = 4096 + 256;
+  const size_t main_bytes = gi ? gi_head + size_t(total) * (sizeof(double) + 2 * sizeof(HitRec))
+                               : scratch_bytes(total, per);
   const size_t scene_at = (main_bytes + 255) / 256 * 256;
   const size_t bytes = hyb ? scene_at + sizeof(DevScene) : main_bytes;
   unsigned long long *work = nullptr;
@@ -1809,8 +1867,11 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   L.njobs = 1;
   L.total = total;
   if (gi) {
-    L.ctr = reinterpret_cast<Counters4 *>(work);
-    L.acc = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(work) + 256);
+    char *w = reinterpret_cast<char *>(work);
+    L.ctr = reinterpret_cast<Counters4 *>(w);
+    L.path_rad = reinterpret_cast<double *>(w + gi_head);
+    L.hits = reinterpret_cast<HitRec *>(w + gi_head + sizeof(double) * size_t(total));
+    L.hits_next = L.hits + total;
   } else {
     scratch_layout(L, work, total);
   }
@@ -1830,7 +1891,7 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
     return cuda_err(ctx, e, "wavefront launch");
   }
   if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {
-    int *gate = scratch_gate(work);
+    int *gate = gi ? reinterpret_cast<int *>(reinterpret_cast<char *>(work) + 4096) : scratch_gate(work);
     L.gate = gate;
     policy_kernel<<<1, 32, 0, s>>>(sc, fr, gate);
     e = int(cudaGetLastError());
