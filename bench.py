@@ -90,13 +90,15 @@ DEFAULT_ENGINE = {"mandelbox_1080p_A": "wavefront_fp32", "mandelbox_1080p_B": "w
 def kernels_per_frame(engine: str, p) -> int:
     """Kernel launches of one frame: the plain engines launch one kernel; the
     wavefront pipeline launches stage P, N (normals wanted), D and S (shadow or
-    AO), the finish kernel and the pixel counter; the auto engine launches the
-    policy kernel and both pipelines, whose kernels of the precision not chosen
-    return at once."""
+    AO), the finish kernel and the pixel counter; a GI frame launches the
+    primary paths, per bounce level (bounces + 1 of them) the normal and vertex
+    stages, the per-pixel sum and the pixel counter; the auto engine launches
+    the policy kernel and both pipelines, whose kernels of the precision not
+    chosen return at once."""
     if "wavefront" not in engine:
         return 1
     if p.gi_samples > 0:
-        n = 3  # GI paths, colour, pixel count
+        n = 1 + 2 * (p.gi_bounces + 1) + 2
         return 1 + 2 * n if engine == "wavefront_auto" else n
     n = 4  # primary, normals (the bench asks for normals), finish, pixel count
     if p.ao_rays > 0 or (p.shading_enable and p.shadow_enable):
