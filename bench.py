@@ -43,11 +43,16 @@ def parse():
                     help="default per workload: wavefront_fp32 (wide views, GI), wavefront_auto (deep zoom, batch)")
     ap.add_argument("--baseline-engine", default="plain_fp64")
     ap.add_argument("--workload", default="mandelbox_1080p_A", choices=WORKLOADS)
+    ap.add_argument("--fract", default=None,
+                    help="render the scene of a mandelbulber2 settings file (.fract) instead of a named workload")
     ap.add_argument("--spp", type=int, default=16, help="GI samples per pixel (hybrid_gi_2160p)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-baseline", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.fract:
+        a.workload = "fract:" + a.fract
+    return a
 
 
 WORKLOADS = ("mandelbox_1080p_A", "mandelbox_1080p_B", "mandelbulb_512", "hybrid_gi_2160p", "batch_2048")
@@ -77,6 +82,21 @@ def workload(name: str, spp: int = 16):
         desc = {"workload": f"hybrid mandelbulb(1-3)+menger(4-12) 3840x2160 monte carlo GI {spp} spp, 4 bounces, "
                             "thin lens aperture 0.02 focus 3", "width": 3840, "height": 2160, "formula": "hybrid",
                 "spp": spp}
+    elif name.startswith("fract:"):
+        # a scene read from a settings file through mbr_fract_parse
+        from mandelbulber2_b200 import settings
+
+        path = name[len("fract:"):]
+        s = settings.load_from_file(path)
+        if not s.ok:
+            raise SystemExit(f"{path}: {s.report}")
+        sc, cam, p = s.scene, s.camera, s.params
+        used = range(sc.n_fractals) if sc.hybrid_fractal_enable else range(1)
+        names = {2: "mandelbulb", 7: "menger", 8: "mandelbox"}
+        forms = "+".join(names[sc.fractal[i].formula] for i in used if sc.fractal[i].formula in names)
+        desc = {"workload": f"settings file {os.path.basename(path)}: {forms} {cam.width}x{cam.height}, "
+                            f"N={sc.formula_maxiter}, {p.ao_rays} AO rays", "width": cam.width,
+                "height": cam.height, "formula": forms, "maxiter": sc.formula_maxiter, "ao_rays": p.ao_rays}
     else:
         raise SystemExit(f"unknown workload {name}")
     return sc, cam, p, desc
@@ -489,7 +509,7 @@ def main() -> None:
     torch.cuda.set_device(local)
     engines = {v: k for k, v in abi.ENGINE_NAMES.items()}
     if a.engine is None:
-        a.engine = DEFAULT_ENGINE[a.workload]
+        a.engine = DEFAULT_ENGINE.get(a.workload, "wavefront_auto")
     if a.workload == "batch_2048":
         run_batch(a, torch, dist, world, rank, local)
         return

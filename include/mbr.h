@@ -396,6 +396,27 @@ mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_
 mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera, const mbr_render_params *params,
                               const mbr_outputs *out, void *stream, char *err, size_t err_len);
 
+/* ---- settings files ------------------------------------------------------------ */
+/* Reads the text of a mandelbulber2 settings file (.fract, the flat form of
+ * versions up to 2.34 that the reference's example scenes use: header lines,
+ * [main_parameters], [fractal_N]) into a scene, a camera and render
+ * parameters.  Replaces, for the DE path, cSettings::LoadFromString + Decode
+ * (src/settings.cpp:513-527, 647-977) followed by the parameter structs the
+ * path reads (sParamRender, src/fractparams.cpp:42-362; sFractal,
+ * src/fractal.cpp:47-89).  Unlisted parameters keep the reference's defaults
+ * (src/initparameters.cpp).
+ *
+ * MBR_OK: everything that changes the geometry is representable.
+ * MBR_EUNSUPPORTED: the structs are filled, but the file uses geometry this
+ * path does not build (another formula, boolean combinations, primitives,
+ * transforms, forced delta DE, another projection); each is named in the
+ * report.  MBR_EINVAL: not a settings file, or a malformed value of a
+ * parameter read here.  The report (optional, NUL-terminated, truncated to
+ * report_size) also lists the shading parameters outside the path that were
+ * ignored, and how the main light and AO were mapped. */
+mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_camera *camera, mbr_render_params *params,
+                           char *report, int32_t report_size);
+
 /* ---- measurement ------------------------------------------------------------ */
 /* FMA throughput of the current device (FLOP/s, an FMA counted as 2), FP32
  * (fp64 = 0) or FP64: the roofline denominator for the DE kernels, which are

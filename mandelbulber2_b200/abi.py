@@ -140,6 +140,8 @@ PROTOTYPES = {
     "mbr_fma_peak": (C.c_int, [C.c_int, C.c_int, _P, C.POINTER(C.c_double)]),
     "mbr_render_noalloc": (C.c_int, [C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderParams),
                                      C.POINTER(Outputs), _P, C.c_char_p, C.c_size_t]),
+    "mbr_fract_parse": (C.c_int, [C.c_char_p, C.POINTER(Scene), C.POINTER(Camera), C.POINTER(RenderParams),
+                                  C.c_char_p, C.c_int32]),
 }
 
 _lib = None

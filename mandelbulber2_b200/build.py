@@ -29,6 +29,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # (source, extra flags)
 UNITS = [
     ("mbr_host.cpp", []),
+    ("fract_loader.cpp", []),
     ("plain_fp64.cu", []),
     ("plain_fp64_strict.cu", ["--fmad=false"]),
     ("plain_mixed.cu", []),

@@ -1,0 +1,706 @@
+// fract_loader.cpp - a mandelbulber2 settings file (.fract text) read into
+// the structs of this path: mbr_scene, mbr_camera, mbr_render_params.
+//
+// The reference loads settings in cSettings::LoadFromString and Decode
+// (src/settings.cpp:513-527, 647-977), line by line in DecodeOneLine
+// (:1015-1240), with version-dependent renames in Compatibility (:1262-1492)
+// and Compatibility2 (:1494-1754), and then migrates files older than 2.35
+// to its objects tree (MigrateToObjectsTree, :2551-2953).  All example
+// scenes the reference ships are of that older, flat form:
+//
+//   # Mandelbulber settings file
+//   # version 2.33
+//   # only modified parameters            (or "all parameters")
+//   [main_parameters]
+//   name value;                           (comma or point decimals, vectors space-separated)
+//   [fractal_1]
+//   name value;
+//
+// This reader restates that flat form for the parameters the DE path reads:
+// formulas and the hybrid sequence, the iteration and bailout settings,
+// camera, raymarching quality, the main light, AO and the 8-bit conversion.
+// Geometry this path does not build (other formulas, boolean combinations,
+// primitives, transforms, forced delta DE, other projections) makes the call
+// return MBR_EUNSUPPORTED with each item named in the report; shading
+// parameters outside the path (materials, fog, glow, reflections, textures,
+// further lights) are counted and listed as ignored.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mbr.h"
+
+namespace {
+
+const int kSlots = MBR_MAX_FRACTALS;
+
+std::string trim(const std::string &s) {
+  size_t a = 0, b = s.size();
+  while (a < b && (s[a] == ' ' || s[a] == '\t' || s[a] == '\r' || s[a] == '\n' || s[a] == '\v' || s[a] == '\f')) a++;
+  while (b > a && (s[b - 1] == ' ' || s[b - 1] == '\t' || s[b - 1] == '\r' || s[b - 1] == '\n' || s[b - 1] == '\v' ||
+                   s[b - 1] == '\f'))
+    b--;
+  return s.substr(a, b - a);
+}
+
+std::string strip_quotes(const std::string &s) {
+  if (s.size() >= 2 && ((s.front() == '"' && s.back() == '"') || (s.front() == '\'' && s.back() == '\'')))
+    return trim(s.substr(1, s.size() - 2));
+  return s;
+}
+
+bool starts_with(const std::string &s, const char *p) { return s.compare(0, std::strlen(p), p) == 0; }
+
+// One "name value;" line (DecodeOneLine, settings.cpp:1017-1043): the name
+// ends at the first space, the value at the first semicolon; enclosing
+// quotes are removed from both.  Whatever follows the semicolon (an
+// animation script) is not read.
+bool split_line(const std::string &line, std::string &name, std::string &value) {
+  const size_t sp = line.find(' ');
+  const size_t sc = line.find(';');
+  if (sp == std::string::npos || sc == std::string::npos || sc <= sp) return false;
+  name = strip_quotes(trim(line.substr(0, sp)));
+  value = strip_quotes(trim(line.substr(sp + 1, sc - sp - 1)));
+  return true;
+}
+
+// Numbers are written with the saving locale's decimal separator: a comma
+// reads as a point (everyLocaleDouble, settings.cpp:2063-2073).
+bool parse_double(const std::string &v, double &out) {
+  std::string t = trim(v);
+  for (char &c : t)
+    if (c == ',') c = '.';
+  if (t.empty()) return false;
+  char *end = nullptr;
+  const double d = std::strtod(t.c_str(), &end);
+  if (end == t.c_str() || *end != '\0') return false;
+  out = d;
+  return true;
+}
+
+bool parse_int(const std::string &v, int &out) {
+  double d;
+  if (!parse_double(v, d) || d != std::floor(d) || std::fabs(d) > 2147483647.0) return false;
+  out = int(d);
+  return true;
+}
+
+bool parse_bool(const std::string &v, int &out) {
+  const std::string t = trim(v);
+  if (t == "true" || t == "1") out = 1;
+  else if (t == "false" || t == "0") out = 0;
+  else return false;
+  return true;
+}
+
+bool parse_vec3(const std::string &v, double out[3]) {
+  std::vector<std::string> parts;
+  std::string cur;
+  for (char c : v) {
+    if (c == ' ' || c == '\t') {
+      if (!cur.empty()) parts.push_back(cur);
+      cur.clear();
+    } else {
+      cur += c;
+    }
+  }
+  if (!cur.empty()) parts.push_back(cur);
+  if (parts.size() != 3) return false;
+  for (int i = 0; i < 3; i++)
+    if (!parse_double(parts[i], out[i])) return false;
+  return true;
+}
+
+// "name_K" with K in 1..9: the base name and the 0-based slot.
+bool indexed(const std::string &name, std::string &base, int &slot) {
+  const size_t u = name.rfind('_');
+  if (u == std::string::npos || u + 1 >= name.size()) return false;
+  int k = 0;
+  for (size_t i = u + 1; i < name.size(); i++) {
+    if (name[i] < '0' || name[i] > '9') return false;
+    k = k * 10 + (name[i] - '0');
+    if (k > 99) return false;
+  }
+  if (k < 1 || k > kSlots) return false;
+  base = name.substr(0, u);
+  slot = k - 1;
+  return true;
+}
+
+struct V3 {
+  double x, y, z;
+};
+V3 v3(const double a[3]) { return V3{a[0], a[1], a[2]}; }
+V3 add(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+V3 sub(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 mul(V3 a, double s) { return V3{a.x * s, a.y * s, a.z * s}; }
+double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V3 cross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+double length(V3 a) { return std::sqrt(dot(a, a)); }
+V3 normalize(V3 a) {
+  const double l = length(a);
+  return l > 0.0 ? mul(a, 1.0 / l) : a;
+}
+// Rodrigues' rotation of v about the unit axis a (CVector3::RotateAroundVectorByAngle, algebra.cpp:71-77)
+V3 rotate_about(V3 v, V3 a, double angle) {
+  V3 r = mul(v, std::cos(angle));
+  r = add(r, mul(cross(a, v), std::sin(angle)));
+  return add(r, mul(a, dot(a, v) * (1.0 - std::cos(angle))));
+}
+// atan2 angles of CVector3::GetAlpha / GetBeta (algebra.hpp)
+double get_alpha(V3 v) { return std::atan2(v.y, v.x); }
+double get_beta(V3 v) { return std::atan2(v.z, std::sqrt(v.x * v.x + v.y * v.y)); }
+
+// The camera frame of cCameraTarget::SetCameraTargetTop (camera_target.cpp:88-126).
+void camera_frame(V3 camera, V3 target, V3 top_in, V3 &forward, V3 &top, V3 &right) {
+  const bool same = camera.x == target.x && camera.y == target.y && camera.z == target.z;
+  forward = normalize(same ? V3{0.0, 1.0, 0.0} : sub(target, camera));
+  const double yaw = get_alpha(forward) - 0.5 * M_PI;
+  const double pitch = get_beta(forward);
+  V3 t = normalize(top_in);
+  t = rotate_about(t, V3{0.0, 0.0, 1.0}, -yaw);
+  t = rotate_about(t, V3{1.0, 0.0, 0.0}, -pitch);
+  const double roll = -std::atan2(t.z, t.x) + 0.5 * M_PI;
+  // CorrectAngle only wraps into (-pi, pi]; the rotations below are periodic
+  top = V3{0.0, 0.0, 1.0};
+  top = rotate_about(top, V3{0.0, 1.0, 0.0}, roll);
+  top = rotate_about(top, V3{1.0, 0.0, 0.0}, pitch);
+  top = rotate_about(top, V3{0.0, 0.0, 1.0}, yaw);
+  right = cross(forward, top);
+}
+
+// CRotationMatrix::SetRotation(CVector3) = RotateZ(x) RotateX(y) RotateY(z) applied to v
+// (algebra.cpp:265-271; RotateZ/X/Y post-multiply the matrix by the axis rotation).
+V3 rotate_zxy(V3 v, V3 angles) {
+  // M = Rz(a) * Rx(b) * Ry(c); M v = Rz(a) (Rx(b) (Ry(c) v))
+  const double ca = std::cos(angles.x), sa = std::sin(angles.x);
+  const double cb = std::cos(angles.y), sb = std::sin(angles.y);
+  const double cc = std::cos(angles.z), sc = std::sin(angles.z);
+  V3 r{cc * v.x + sc * v.z, v.y, -sc * v.x + cc * v.z};  // Ry(c)
+  r = V3{r.x, cb * r.y - sb * r.z, sb * r.y + cb * r.z};  // Rx(b)
+  return V3{ca * r.x - sa * r.y, sa * r.x + ca * r.y, r.z};  // Rz(a)
+}
+
+struct Reader {
+  double version = 0.0;
+  std::vector<std::string> unsupported, ignored, notes, errors;
+
+  // main parameters (defaults: initparameters.cpp)
+  int N = 250;
+  int hybrid = 0, boolean_ops = 0;
+  int formula[kSlots];
+  int slot_enable[kSlots];
+  int ao_enabled = 0, ao_mode = 2;
+  double ao_intensity = 1.0;
+  // light 1 (initparameters.cpp:1895-1950)
+  int light_enabled = 1, light_shadows = 1, light_penetrating = 1, light_relative = 1, light_use_target = 0;
+  int light_type = 0;  // 0 directional
+  int light_defined = 0;
+  double light_rot[3] = {-45.0, 45.0, 0.0};
+  double light_alpha = -45.0, light_beta = 45.0;
+  double light_soft_cone = 1.0, light_intensity = 1.0, all_lights_intensity = 1.0;
+  double light_pos[3] = {0.0, 0.0, 0.0}, light_target[3] = {0.0, 0.0, 0.0};
+
+  Reader() {
+    for (int i = 0; i < kSlots; i++) {
+      formula[i] = i == 0 ? MBR_FORMULA_MANDELBULB : MBR_FORMULA_NONE;
+      slot_enable[i] = 1;
+    }
+  }
+
+  void bad(const std::string &name, const std::string &value) { errors.push_back(name + " '" + value + "'"); }
+};
+
+// Renames of older files that reach the keys read here (Compatibility,
+// settings.cpp:1283-1466).
+void compatibility(const Reader &R, std::string &name, std::string &value) {
+  const double v = R.version;
+  if (v <= 2.04 && name == "fractal_constant_factor") {
+    const std::string t = trim(value);
+    if (t.find(' ') == std::string::npos) value = t + " " + t + " " + t;
+  }
+  if (v <= 2.06 && name == "linear_DE_mode") {
+    name = "delta_DE_function";
+    value = "1";
+  }
+  if (v < 2.09 && name == "delta_DE_function") {
+    if (value == "0") value = "2";
+    else if (value == "2") value = "0";
+  }
+  if (v < 2.25) {
+    struct Ren {
+      const char *from, *to;
+    };
+    static const Ren ren[] = {{"main_light_intensity", "light1_intensity"},
+                              {"main_light_alpha", "light1_alpha"},
+                              {"main_light_beta", "light1_beta"},
+                              {"penetrating_lights", "light1_penetrating"},
+                              {"shadows_enabled", "light1_cast_shadows"},
+                              {"shadows_cone_angle", "light1_soft_shadow_cone"},
+                              {"main_light_enable", "light1_enabled"},
+                              {"main_light_position_relative", "light1_relative_position"}};
+    for (const Ren &r : ren)
+      if (name == r.from) name = r.to;
+  }
+}
+
+void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &name, const std::string &value) {
+  mbr_fractal &f = sc->fractal[slot];
+  double d;
+  int b;
+  double v[3];
+  if (name == "power") {
+    if (parse_double(value, d)) f.bulb_power = d; else R.bad(name, value);
+  } else if (name == "alpha_angle_offset") {
+    if (parse_double(value, d)) f.bulb_alpha_angle_offset = d; else R.bad(name, value);
+  } else if (name == "beta_angle_offset") {
+    if (parse_double(value, d)) f.bulb_beta_angle_offset = d; else R.bad(name, value);
+  } else if (name == "mandelbox_scale") {
+    if (parse_double(value, d)) f.mandelbox_scale = d; else R.bad(name, value);
+  } else if (name == "mandelbox_folding_limit") {
+    if (parse_double(value, d)) f.mandelbox_folding_limit = d; else R.bad(name, value);
+  } else if (name == "mandelbox_folding_value") {
+    if (parse_double(value, d)) f.mandelbox_folding_value = d; else R.bad(name, value);
+  } else if (name == "mandelbox_folding_min_radius") {
+    if (parse_double(value, d)) f.mandelbox_folding_min_radius = d; else R.bad(name, value);
+  } else if (name == "mandelbox_folding_fixed_radius") {
+    if (parse_double(value, d)) f.mandelbox_folding_fixed_radius = d; else R.bad(name, value);
+  } else if (name == "mandelbox_offset") {
+    if (parse_vec3(value, v)) std::memcpy(f.mandelbox_offset, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "transf_scale_3") {
+    if (parse_double(value, d)) f.transf_scale3 = d; else R.bad(name, value);
+  } else if (name == "mandelbox_rotations_enabled" || name == "mandelbox_main_rotation_enabled") {
+    // only an unsupported feature when the slot is a Mandelbox in use (checked later)
+    if (parse_bool(value, b) && b) R.notes.push_back("slot:" + std::to_string(slot) + ":" + name);
+  } else if (name == "formula_iterations") {
+    if (parse_int(value, b)) f.formula_iterations = b; else R.bad(name, value);
+  } else if (name == "formula_weight") {
+    if (parse_double(value, d)) f.formula_weight = d; else R.bad(name, value);
+  } else if (name == "formula_start_iteration") {
+    if (parse_int(value, b)) f.formula_start_iteration = b; else R.bad(name, value);
+  } else if (name == "formula_stop_iteration") {
+    if (parse_int(value, b)) f.formula_stop_iteration = b; else R.bad(name, value);
+  } else {
+    R.ignored.push_back("fractal_" + std::to_string(slot + 1) + "." + name);
+  }
+}
+
+bool nonzero3(const double v[3]) { return v[0] != 0.0 || v[1] != 0.0 || v[2] != 0.0; }
+
+void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_params *p, std::string name,
+                     std::string value) {
+  compatibility(R, name, value);
+  double d;
+  int b;
+  double v[3];
+  std::string base;
+  int slot;
+  // per-slot parameters of the flat form: formula_K, formula_iterations_K, ...
+  if (indexed(name, base, slot)) {
+    mbr_fractal &f = sc->fractal[slot];
+    if (base == "formula") {
+      if (parse_int(value, b)) R.formula[slot] = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "formula_iterations") {
+      if (parse_int(value, b)) f.formula_iterations = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "formula_weight") {
+      if (parse_double(value, d)) f.formula_weight = d; else R.bad(name, value);
+      return;
+    }
+    if (base == "formula_start_iteration") {
+      if (parse_int(value, b)) f.formula_start_iteration = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "formula_stop_iteration") {
+      if (parse_int(value, b)) f.formula_stop_iteration = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "dont_add_c_constant") {
+      if (parse_bool(value, b)) f.dont_add_c_constant = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "check_for_bailout") {
+      if (parse_bool(value, b)) f.check_for_bailout = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "fractal_enable") {
+      if (parse_bool(value, b)) R.slot_enable[slot] = b; else R.bad(name, value);
+      return;
+    }
+    if (base == "formula_position" || base == "formula_rotation" || base == "formula_repeat") {
+      if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (formula transform)");
+      return;
+    }
+    if (base == "formula_scale") {
+      if (parse_double(value, d) && d != 1.0) R.unsupported.push_back(name + " (formula transform)");
+      return;
+    }
+    // julia_mode_K, julia_c_K, fractal_constant_factor_K, initial_waxis_K,
+    // formula_maxiter_K, boolean_operator_K: read by the boolean combination only
+    if (base == "julia_mode" || base == "julia_c" || base == "fractal_constant_factor" ||
+        base == "initial_waxis" || base == "formula_maxiter" || base == "boolean_operator" ||
+        base == "formula_material_id") {
+      R.ignored.push_back(name);
+      return;
+    }
+  }
+  if (starts_with(name, "primitive_")) {
+    R.unsupported.push_back(name + " (primitive object)");
+    return;
+  }
+  if (starts_with(name, "node_")) {
+    R.unsupported.push_back(name + " (objects tree)");
+    return;
+  }
+  // formula and sequence
+  if (name == "N") {
+    if (parse_int(value, b)) R.N = b; else R.bad(name, value);
+  } else if (name == "minN") {
+    if (parse_int(value, b)) sc->min_n = b; else R.bad(name, value);
+  } else if (name == "bailout") {
+    if (parse_double(value, d)) sc->bailout = d; else R.bad(name, value);
+  } else if (name == "use_default_bailout") {
+    if (parse_bool(value, b)) sc->use_default_bailout = b; else R.bad(name, value);
+  } else if (name == "repeat_from") {
+    if (parse_int(value, b)) sc->repeat_from = b; else R.bad(name, value);
+  } else if (name == "hybrid_fractal_enable") {
+    if (parse_bool(value, b)) R.hybrid = b; else R.bad(name, value);
+  } else if (name == "boolean_operators") {
+    if (parse_bool(value, b)) R.boolean_ops = b; else R.bad(name, value);
+  } else if (name == "julia_mode") {
+    if (parse_bool(value, b)) sc->julia_mode = b; else R.bad(name, value);
+  } else if (name == "julia_c") {
+    if (parse_vec3(value, v)) std::memcpy(sc->julia_c, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "fractal_constant_factor") {
+    if (parse_vec3(value, v)) std::memcpy(sc->fractal_constant_factor, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "initial_waxis") {
+    if (parse_double(value, d)) sc->initial_waxis = d; else R.bad(name, value);
+  } else if (name == "linear_DE_offset") {
+    if (parse_double(value, d)) sc->linear_de_offset = d; else R.bad(name, value);
+  } else if (name == "delta_DE_function") {
+    if (parse_int(value, b) && b >= 0 && b <= 2) sc->delta_de_function = b;
+    else if (parse_int(value, b)) R.unsupported.push_back(name + " " + value + " (DE function)");
+    else R.bad(name, value);
+  } else if (name == "delta_DE_method") {
+    // 0 preferred (analytic for the three formulas), 1 forced delta, 2 forced analytic
+    if (parse_int(value, b)) {
+      if (b == 1) R.unsupported.push_back(name + " 1 (forced delta DE)");
+    } else {
+      R.bad(name, value);
+    }
+  } else if (name == "iteration_threshold_mode") {
+    if (parse_bool(value, b)) sc->iteration_threshold_mode = b; else R.bad(name, value);
+  } else if (name == "interior_mode") {
+    if (parse_bool(value, b)) sc->interior_mode = b; else R.bad(name, value);
+  } else if (name == "fractal_position" || name == "fractal_rotation" || name == "repeat") {
+    if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (fractal transform)");
+  } else if (name == "formula_code") {
+    R.unsupported.push_back(name + " (custom formula code)");
+  // camera and image
+  } else if (name == "camera") {
+    if (parse_vec3(value, v)) std::memcpy(cam->camera, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "target") {
+    if (parse_vec3(value, v)) std::memcpy(cam->target, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "camera_top") {
+    if (parse_vec3(value, v)) std::memcpy(cam->top, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "fov") {
+    if (parse_double(value, d)) cam->fov_deg = d; else R.bad(name, value);
+  } else if (name == "image_width") {
+    if (parse_int(value, b)) cam->width = b; else R.bad(name, value);
+  } else if (name == "image_height") {
+    if (parse_int(value, b)) cam->height = b; else R.bad(name, value);
+  } else if (name == "perspective_type") {
+    if (!(value == "three_point" || value == "0")) R.unsupported.push_back(name + " " + value + " (projection)");
+  } else if (name == "legacy_coordinate_system") {
+    if (parse_bool(value, b) && b) R.unsupported.push_back(name + " (camera axes)");
+  } else if (name == "camera_rotation" || name == "camera_distance_to_target") {
+    // derived from camera, target and top by the reference itself
+  // raymarching quality
+  } else if (name == "detail_level") {
+    if (parse_double(value, d)) p->detail_level = d; else R.bad(name, value);
+  } else if (name == "DE_factor") {
+    if (parse_double(value, d)) p->de_factor = d; else R.bad(name, value);
+  } else if (name == "view_distance_max") {
+    if (parse_double(value, d)) p->view_distance_max = d; else R.bad(name, value);
+  } else if (name == "smoothness") {
+    if (parse_double(value, d)) p->smoothness = d; else R.bad(name, value);
+  } else if (name == "max_raymarching_steps") {
+    if (parse_int(value, b)) p->max_raymarching_steps = b; else R.bad(name, value);
+  } else if (name == "constant_DE_threshold") {
+    if (parse_bool(value, b)) p->constant_de_threshold = b; else R.bad(name, value);
+  } else if (name == "DE_thresh") {
+    if (parse_double(value, d)) p->de_thresh = d; else R.bad(name, value);
+  // 8-bit conversion (cImage::CalculatePixel)
+  } else if (name == "brightness") {
+    if (parse_double(value, d)) p->brightness = d; else R.bad(name, value);
+  } else if (name == "contrast") {
+    if (parse_double(value, d)) p->contrast = d; else R.bad(name, value);
+  } else if (name == "gamma") {
+    if (parse_double(value, d)) p->gamma = d; else R.bad(name, value);
+  } else if (name == "saturation") {
+    if (parse_double(value, d)) p->saturation = d; else R.bad(name, value);
+  } else if (name == "hdr") {
+    if (parse_bool(value, b)) p->hdr = b; else R.bad(name, value);
+  // the main light
+  } else if (starts_with(name, "light1_")) {
+    R.light_defined = 1;
+    const std::string k = name.substr(7);
+    if (k == "enabled") {
+      if (parse_bool(value, b)) R.light_enabled = b; else R.bad(name, value);
+    } else if (k == "cast_shadows") {
+      if (parse_bool(value, b)) R.light_shadows = b; else R.bad(name, value);
+    } else if (k == "penetrating") {
+      if (parse_bool(value, b)) R.light_penetrating = b; else R.bad(name, value);
+    } else if (k == "relative_position") {
+      if (parse_bool(value, b)) R.light_relative = b; else R.bad(name, value);
+    } else if (k == "use_target_point") {
+      if (parse_bool(value, b)) R.light_use_target = b; else R.bad(name, value);
+    } else if (k == "type") {
+      if (value == "directional" || value == "0") R.light_type = 0;
+      else R.light_type = 1;
+    } else if (k == "rotation") {
+      if (parse_vec3(value, v)) std::memcpy(R.light_rot, v, sizeof(v)); else R.bad(name, value);
+    } else if (k == "alpha") {
+      if (parse_double(value, d)) R.light_alpha = d; else R.bad(name, value);
+    } else if (k == "beta") {
+      if (parse_double(value, d)) R.light_beta = d; else R.bad(name, value);
+    } else if (k == "intensity") {
+      if (parse_double(value, d)) R.light_intensity = d; else R.bad(name, value);
+    } else if (k == "soft_shadow_cone") {
+      if (parse_double(value, d)) R.light_soft_cone = d; else R.bad(name, value);
+    } else if (k == "position") {
+      if (parse_vec3(value, v)) std::memcpy(R.light_pos, v, sizeof(v)); else R.bad(name, value);
+    } else if (k == "target") {
+      if (parse_vec3(value, v)) std::memcpy(R.light_target, v, sizeof(v)); else R.bad(name, value);
+    } else {
+      R.ignored.push_back(name);
+    }
+  } else if (name == "all_lights_intensity") {  // multiplies every light's intensity (light.cpp:77-83)
+    if (parse_double(value, d)) R.all_lights_intensity = d; else R.bad(name, value);
+  } else if (name == "mat1_shading") {
+    if (parse_double(value, d)) p->material_shading = d; else R.bad(name, value);
+  // ambient occlusion
+  } else if (name == "ambient_occlusion_enabled") {
+    if (parse_bool(value, b)) R.ao_enabled = b; else R.bad(name, value);
+  } else if (name == "ambient_occlusion_mode") {
+    if (value == "fast") R.ao_mode = 0;
+    else if (value == "multiple_rays") R.ao_mode = 1;
+    else if (value == "screen_space") R.ao_mode = 2;
+    else if (parse_int(value, b)) R.ao_mode = b;
+    else R.bad(name, value);
+  } else if (name == "ambient_occlusion") {
+    if (parse_double(value, d)) R.ao_intensity = d; else R.bad(name, value);
+  } else {
+    R.ignored.push_back(name);
+  }
+}
+
+void append(std::string &out, const std::string &s) {
+  out += s;
+  out += '\n';
+}
+
+}  // namespace
+
+extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_camera *camera,
+                                      mbr_render_params *params, char *report, int32_t report_size) {
+  if (!text || !scene || !camera || !params) return MBR_EINVAL;
+  Reader R;
+  std::string rep;
+  auto finish = [&](mbr_status st) {
+    if (report && report_size > 0) {
+      const size_t n = std::min(rep.size(), size_t(report_size - 1));
+      std::memcpy(report, rep.data(), n);
+      report[n] = '\0';
+    }
+    return st;
+  };
+
+  // lines split at \n, \r\n or \r of the trimmed text (settings.cpp:656-665)
+  std::vector<std::string> lines;
+  {
+    const std::string all = trim(std::string(text));
+    std::string cur;
+    for (size_t i = 0; i < all.size(); i++) {
+      const char c = all[i];
+      if (c == '\r' || c == '\n') {
+        lines.push_back(cur);
+        cur.clear();
+        if (c == '\r' && i + 1 < all.size() && all[i + 1] == '\n') i++;
+      } else {
+        cur += c;
+      }
+    }
+    lines.push_back(cur);
+  }
+  // header (DecodeHeader, settings.cpp:540-601)
+  if (lines.size() < 3) {
+    append(rep, "error: not a Mandelbulber settings file (no header)");
+    return finish(MBR_EINVAL);
+  }
+  if (lines[0].find("Mandelbulber settings file") == std::string::npos) {
+    append(rep, "error: not a Mandelbulber settings file (wrong header)");
+    return finish(MBR_EINVAL);
+  }
+  const size_t vp = lines[1].rfind("version");
+  if (vp == std::string::npos || !parse_double(lines[1].substr(vp + 7), R.version)) {
+    append(rep, "error: no version number in the header");
+    return finish(MBR_EINVAL);
+  }
+  if (lines[2].find("all parameters") == std::string::npos &&
+      lines[2].find("only modified parameters") == std::string::npos) {
+    append(rep, "error: the header names no settings format (all / only modified parameters)");
+    return finish(MBR_EINVAL);
+  }
+
+  // defaults (initparameters.cpp): scene and fractal slots, camera, quality, light 1
+  mbr_scene_defaults(scene);
+  mbr_camera_defaults(camera);
+  mbr_render_params_defaults(params);
+  const double top0[3] = {-0.1277753, 0.2555506, 0.958314};  // camera_top (initparameters.cpp:116)
+  std::memcpy(camera->top, top0, sizeof(top0));
+  params->ambient_intensity = 0.0;
+  params->ao_rays = 0;
+
+  std::string section;
+  std::vector<std::pair<int, std::pair<std::string, std::string>>> fractal_lines;
+  for (size_t l = 3; l < lines.size(); l++) {
+    const std::string &line = lines[l];
+    if (!line.empty() && line.front() == '[' && line.back() == ']') {  // CheckSection (settings.cpp:1247-1255)
+      section = line.substr(1, line.size() - 2);
+      continue;
+    }
+    if (section == "description" || section == "frames" || section == "keyframes") continue;
+    const std::string t = trim(line);
+    if (t.empty()) continue;
+    std::string name, value;
+    if (!split_line(t, name, value)) {
+      if (section == "main_parameters" || starts_with(section, "fractal_")) R.errors.push_back("line " + std::to_string(l + 1) + ": '" + t + "'");
+      continue;
+    }
+    if (section == "main_parameters") {
+      read_main_param(R, scene, camera, params, name, value);
+    } else if (starts_with(section, "fractal_")) {
+      int k = 0;
+      if (std::sscanf(section.c_str() + 8, "%d", &k) == 1 && k >= 1 && k <= kSlots)
+        fractal_lines.push_back({k - 1, {name, value}});
+      else
+        R.ignored.push_back(section + "." + name);
+    } else {
+      R.ignored.push_back((section.empty() ? std::string("?") : section) + "." + name);
+    }
+  }
+  for (const auto &fl : fractal_lines) read_fractal_param(R, scene, fl.first, fl.second.first, fl.second.second);
+
+  if (!R.errors.empty()) {
+    for (const std::string &e : R.errors) append(rep, "error: malformed value or line: " + e);
+    return finish(MBR_EINVAL);
+  }
+
+  // formulas: a single fractal renders slot 1; a hybrid iterates every slot
+  // whose formula is not none (MigrateToObjectsTree, settings.cpp:2716-2830)
+  if (R.boolean_ops) R.unsupported.push_back("boolean_operators (boolean combination of fractals)");
+  scene->hybrid_fractal_enable = R.hybrid;
+  int last = 0;
+  for (int i = 0; i < kSlots; i++) {
+    scene->fractal[i].formula = R.formula[i];
+    if (R.formula[i] != MBR_FORMULA_NONE) last = i + 1;
+  }
+  scene->n_fractals = R.hybrid ? (last > 0 ? last : 1) : 1;
+  for (int i = 0; i < scene->n_fractals; i++) {
+    const int f = R.formula[i];
+    if (!R.hybrid && i > 0) break;
+    if (f == MBR_FORMULA_NONE) continue;
+    if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE)
+      R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
+                              " (formula not built here: 2 Mandelbulb, 7 Menger sponge, 8 Mandelbox are)");
+    if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
+    if (f == MBR_FORMULA_MANDELBOX)
+      for (const std::string &n : R.notes)
+        if (starts_with(n, ("slot:" + std::to_string(i) + ":").c_str()))
+          R.unsupported.push_back("fractal_" + std::to_string(i + 1) + "." + n.substr(n.rfind(':') + 1) +
+                                  " (Mandelbox rotations)");
+  }
+  if (!R.hybrid && R.formula[0] == MBR_FORMULA_NONE) R.unsupported.push_back("formula_1 0 (no fractal)");
+  // the node's iteration limit is the main N (CopyFractalParams, settings.cpp:2494-2501; the hybrid root :2775-2778)
+  scene->formula_maxiter = R.N;
+
+  // light 1 direction (cLight::Set, light.cpp:90-190): files before 2.25 give
+  // alpha and beta; rotation is scaled by pi/180.8 as the reference does
+  if (R.version < 2.25 && R.light_defined) {
+    R.light_rot[0] = R.light_alpha;
+    R.light_rot[1] = R.light_beta;
+    R.light_rot[2] = 0.0;
+  }
+  params->shading_enable = R.light_enabled;
+  params->shadow_enable = R.light_enabled && R.light_shadows;
+  params->light_intensity = R.light_intensity * R.all_lights_intensity;
+  if (R.light_type != 0) {
+    append(rep, "note: light1 is not directional; the path lights with a directional light from its default rotation");
+  }
+  {
+    V3 rot = mul(v3(R.light_rot), M_PI / 180.8);
+    rot = V3{rot.x, -rot.y, rot.z};  // directional
+    V3 dir;
+    if (R.light_relative) {
+      V3 fwd, top, right;
+      camera_frame(v3(camera->camera), v3(camera->target), v3(camera->top), fwd, top, right);
+      if (R.light_use_target && R.light_type == 0) {
+        const V3 c = v3(camera->camera);
+        const V3 dp = v3(R.light_pos), dt = v3(R.light_target);
+        const V3 pos = add(c, add(add(mul(fwd, dp.z), mul(top, dp.y)), mul(right, dp.x)));
+        const V3 tgt = add(c, add(add(mul(fwd, dt.z), mul(top, dt.y)), mul(right, dt.x)));
+        dir = sub(pos, tgt);
+        dir = length(dir) > 0.0 ? normalize(dir) : mul(fwd, -1.0);
+      } else {
+        dir = mul(fwd, -1.0);
+        dir = rotate_about(dir, fwd, rot.z);
+        dir = rotate_about(dir, right, rot.y);
+        dir = rotate_about(dir, top, rot.x);
+      }
+    } else if (R.light_use_target && R.light_type == 0) {
+      dir = sub(v3(R.light_pos), v3(R.light_target));
+      dir = length(dir) > 0.0 ? normalize(dir) : V3{1.0, 0.0, 0.0};
+    } else {
+      dir = rotate_zxy(V3{0.0, -1.0, 0.0}, rot);
+    }
+    params->light_direction[0] = dir.x;
+    params->light_direction[1] = dir.y;
+    params->light_direction[2] = dir.z;
+  }
+  if (R.light_enabled && R.light_shadows && R.light_penetrating)
+    append(rep, "note: light1_penetrating: the shadow march runs to view_distance_max (non-penetrating)");
+  if (R.light_enabled && R.light_shadows && R.light_soft_cone > 0.0)
+    append(rep, "note: light1_soft_shadow_cone: the shadow is hard");
+
+  // ambient occlusion: the multiple-rays mode maps onto 16 cosine-hemisphere
+  // rays per hit; the fast and screen-space modes are not on this path
+  if (R.ao_enabled) {
+    if (R.ao_mode == 1) {
+      params->ao_rays = 16;
+      params->ambient_intensity = R.ao_intensity;
+      append(rep, "note: ambient_occlusion (multiple rays): 16 cosine-hemisphere rays per hit");
+    } else {
+      append(rep, std::string("note: ambient_occlusion mode ") + (R.ao_mode == 0 ? "fast" : "screen space") +
+                      " is not on this path; AO off");
+    }
+  }
+
+  for (const std::string &u : R.unsupported) append(rep, "unsupported: " + u);
+  if (!R.ignored.empty()) {
+    std::string s = "ignored: " + std::to_string(R.ignored.size()) + " parameters outside the DE path:";
+    for (size_t i = 0; i < R.ignored.size(); i++) s += " " + R.ignored[i];
+    append(rep, s);
+  }
+  char head[96];
+  std::snprintf(head, sizeof(head), "version %.2f, %s\n", R.version, R.hybrid ? "hybrid" : "single fractal");
+  rep = std::string(head) + rep;
+  return finish(R.unsupported.empty() ? MBR_OK : MBR_EUNSUPPORTED);
+}

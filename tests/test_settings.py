@@ -1,0 +1,246 @@
+"""Settings files (.fract) read by mbr_fract_parse, on the CPU.
+
+The fixtures under tests/golden/settings/ are scenes written for these tests
+in the reference's flat settings format (header, [main_parameters],
+[fractal_N], comma decimals).  The expected values restate the reference's
+rules: defaults from initparameters.cpp, the renames of Compatibility for old
+versions (settings.cpp:1283-1466), N as the iteration limit of the fractal
+node (settings.cpp:2494-2501, 2775-2778), and the main light's direction from
+cLight (light.cpp:90-190, rotation scaled by pi/180.8).  When the reference
+tree is present, every example scene it ships is read as well.
+"""
+import glob
+import math
+import os
+
+import numpy as np
+import pytest
+
+from mandelbulber2_b200 import abi, settings
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = os.path.join(HERE, "golden", "settings")
+EXAMPLES = "/root/reference/mandelbulber2/deploy/share/mandelbulber2/examples"
+
+HEADER = "# Mandelbulber settings file\n# version 2.33\n# only modified parameters\n"
+
+
+def rot_about(v, a, ang):
+    v, a = np.asarray(v, float), np.asarray(a, float)
+    return v * math.cos(ang) + np.cross(a, v) * math.sin(ang) + a * np.dot(a, v) * (1 - math.cos(ang))
+
+
+def camera_frame(cam, tgt, top):
+    """cCameraTarget::SetCameraTargetTop (camera_target.cpp:88-126)."""
+    f = np.asarray(tgt, float) - np.asarray(cam, float)
+    f = f / np.linalg.norm(f)
+    yaw = math.atan2(f[1], f[0]) - 0.5 * math.pi
+    pitch = math.atan2(f[2], math.sqrt(f[0] ** 2 + f[1] ** 2))
+    t = np.asarray(top, float) / np.linalg.norm(top)
+    t = rot_about(t, [0, 0, 1], -yaw)
+    t = rot_about(t, [1, 0, 0], -pitch)
+    roll = -math.atan2(t[2], t[0]) + 0.5 * math.pi
+    up = rot_about([0, 0, 1], [0, 1, 0], roll)
+    up = rot_about(up, [1, 0, 0], pitch)
+    up = rot_about(up, [0, 0, 1], yaw)
+    return f, up, np.cross(f, up)
+
+
+def relative_light(cam, tgt, top, rotation_deg):
+    """Directional light 1 relative to the camera (light.cpp:90-160)."""
+    r = np.asarray(rotation_deg, float) / 180.8 * math.pi * np.array([1.0, -1.0, 1.0])
+    f, up, right = camera_frame(cam, tgt, top)
+    d = -f
+    d = rot_about(d, f, r[2])
+    d = rot_about(d, right, r[1])
+    d = rot_about(d, up, r[0])
+    return d
+
+
+def test_mandelbox_with_ao():
+    s = settings.load_from_file(os.path.join(FIX, "box_ao.fract"))
+    assert s.status == abi.MBR_OK, s.report
+    sc, cam, p = s.scene, s.camera, s.params
+    assert sc.n_fractals == 1 and not sc.hybrid_fractal_enable
+    f = sc.fractal[0]
+    assert f.formula == abi.FORMULA_MANDELBOX
+    assert f.mandelbox_scale == -1.73 and f.mandelbox_folding_min_radius == 0.4
+    assert f.mandelbox_folding_limit == 1.0 and f.mandelbox_folding_value == 2.0  # defaults
+    assert sc.formula_maxiter == 40
+    assert list(cam.camera) == [0.5, -5.5, 1.4] and list(cam.target) == [0.0, 0.0, 0.1]
+    assert list(cam.top) == [0.05, 0.2, 0.97]
+    assert (cam.width, cam.height) == (96, 54) and cam.fov_deg == 53.13
+    assert p.detail_level == 1.5 and p.de_factor == 0.9 and p.view_distance_max == 25.0
+    assert p.ao_rays == 16 and p.ambient_intensity == 0.8
+    assert p.shading_enable == 1 and p.shadow_enable == 1
+    want = relative_light(cam.camera, cam.target, cam.top, [30, -20, 0])
+    np.testing.assert_allclose(list(p.light_direction), want, rtol=0, atol=1e-12)
+    assert "volumetric_fog_enabled" in s.report and "mat1_specular" in s.report
+    assert "penetrating" not in s.report and "hard" not in s.report
+
+
+def test_hybrid_sequence():
+    s = settings.load_from_file(os.path.join(FIX, "hybrid_bulb_menger.fract"))
+    assert s.status == abi.MBR_OK, s.report
+    sc = s.scene
+    assert sc.hybrid_fractal_enable == 1 and sc.n_fractals == 2
+    assert sc.fractal[0].formula == abi.FORMULA_MANDELBULB and sc.fractal[0].formula_iterations == 3
+    assert sc.fractal[0].bulb_power == 8.0
+    assert sc.fractal[1].formula == abi.FORMULA_MENGER_SPONGE and sc.fractal[1].formula_iterations == 9
+    assert sc.formula_maxiter == 12
+    assert s.params.view_distance_max == 20.0  # quoted name and value
+    # the default light: rotation (-45, 45, 0) relative to the camera
+    want = relative_light(s.camera.camera, s.camera.target, s.camera.top, [-45, 45, 0])
+    np.testing.assert_allclose(list(s.params.light_direction), want, rtol=0, atol=1e-12)
+    # penetrating shadows and the soft cone are the reference's defaults, mapped with a note
+    assert "penetrating" in s.report and "hard" in s.report
+    # the sequence the library builds: 3 bulb passes, then 9 Menger passes
+    lib = abi.load()
+    import ctypes as C
+
+    seq = (C.c_int32 * abi.MBR_SEQUENCE_LENGTH)()
+    n, fn, bo = C.c_int32(), C.c_int32(), C.c_double()
+    assert lib.mbr_scene_sequence(C.byref(sc), seq, C.byref(n), C.byref(fn), C.byref(bo)) == abi.MBR_OK
+    assert list(seq[:12]) == [0, 0, 0] + [1] * 9
+
+
+def test_legacy_renames():
+    s = settings.load_from_file(os.path.join(FIX, "legacy_light.fract"))
+    assert s.status == abi.MBR_OK, s.report
+    sc, p = s.scene, s.params
+    assert sc.fractal[0].formula == abi.FORMULA_MANDELBULB and sc.fractal[0].bulb_power == 6.0
+    assert sc.delta_de_function == 2  # before 2.09 the values 0 and 2 were swapped
+    assert list(sc.fractal_constant_factor) == [1.1, 1.1, 1.1]  # a scalar before 2.05
+    assert p.shading_enable == 1 and p.shadow_enable == 0  # shadows_enabled -> light1_cast_shadows
+    # main_light_alpha / beta -> light1 rotation (alpha, beta, 0) (settings.cpp:1420-1421, 1643-1649)
+    want = relative_light(s.camera.camera, s.camera.target, s.camera.top, [10, -35, 0])
+    np.testing.assert_allclose(list(p.light_direction), want, rtol=0, atol=1e-12)
+    assert sc.formula_maxiter == 250  # N's default
+
+
+def test_light_rotation_zero_points_back_along_the_view():
+    txt = HEADER + "[main_parameters]\ncamera 1 -5 2;\ntarget 0 0 0;\ncamera_top 0 0 1;\nlight1_rotation 0 0 0;\n"
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    f = np.array([-1.0, 5.0, -2.0]) / math.sqrt(30.0)
+    np.testing.assert_allclose(list(s.params.light_direction), -f, atol=1e-15)
+
+
+def test_absolute_light_rotation():
+    txt = HEADER + ("[main_parameters]\nlight1_relative_position false;\nlight1_rotation 20 10 5;\n")
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    a, b, c = np.array([20.0, -10.0, 5.0]) / 180.8 * math.pi
+    rz = np.array([[math.cos(a), -math.sin(a), 0], [math.sin(a), math.cos(a), 0], [0, 0, 1]])
+    rx = np.array([[1, 0, 0], [0, math.cos(b), -math.sin(b)], [0, math.sin(b), math.cos(b)]])
+    ry = np.array([[math.cos(c), 0, math.sin(c)], [0, 1, 0], [-math.sin(c), 0, math.cos(c)]])
+    want = rz @ rx @ ry @ np.array([0.0, -1.0, 0.0])
+    np.testing.assert_allclose(list(s.params.light_direction), want, atol=1e-15)
+
+
+def test_defaults_of_an_empty_file():
+    s = settings.load_from_string(HEADER + "[main_parameters]\n")
+    assert s.ok, s.report
+    sc, cam, p = s.scene, s.camera, s.params
+    assert sc.fractal[0].formula == abi.FORMULA_MANDELBULB and sc.fractal[0].bulb_power == 9.0
+    assert sc.formula_maxiter == 250 and sc.bailout == 100.0 and sc.use_default_bailout == 1
+    assert list(cam.camera) == [3.0, -6.0, 2.0] and list(cam.target) == [0.0, 0.0, 0.0]
+    assert list(cam.top) == [-0.1277753, 0.2555506, 0.958314]
+    assert (cam.width, cam.height) == (800, 600) and cam.fov_deg == 53.13
+    assert p.detail_level == 1.0 and p.view_distance_max == 50.0 and p.max_raymarching_steps == 10000
+    assert p.ao_rays == 0 and p.binary_steps == 30
+
+
+@pytest.mark.parametrize("text,what", [
+    ("[main_parameters]\nformula_1 8;\n", "no header"),
+    ("# some other file\n# version 2.3\n# only modified parameters\n", "wrong header"),
+    ("# Mandelbulber settings file\n# no number here\n# only modified parameters\n", "version"),
+    ("# Mandelbulber settings file\n# version 2.33\n# something\n", "format"),
+    (HEADER + "[main_parameters]\ncamera 1 2;\n", "malformed"),
+    (HEADER + "[main_parameters]\ndetail_level fast;\n", "malformed"),
+    (HEADER + "[main_parameters]\nformula_1 8\n", "malformed"),
+])
+def test_invalid_files(text, what):
+    s = settings.load_from_string(text)
+    assert s.status == abi.MBR_EINVAL, (what, s.report)
+    assert "error" in s.report
+
+
+def test_unsupported_geometry_is_named():
+    txt = HEADER + ("[main_parameters]\nformula_1 103;\n")
+    s = settings.load_from_string(txt)
+    assert s.status == abi.MBR_EUNSUPPORTED
+    assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
+    txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_sphere_1_enabled true;\nboolean_operators true;\n"
+                    "perspective_type fish_eye;\ndelta_DE_method 1;\n[fractal_1]\nmandelbox_rotations_enabled true;\n")
+    s = settings.load_from_string(txt)
+    assert s.status == abi.MBR_EUNSUPPORTED
+    u = " | ".join(s.unsupported())
+    for key in ("primitive_sphere_1_enabled", "boolean_operators", "perspective_type fish_eye",
+                "delta_DE_method 1", "mandelbox_rotations_enabled"):
+        assert key in u, (key, s.report)
+    # a slot that a single-fractal scene does not iterate may name any formula
+    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
+    assert s.ok, s.report
+
+
+def test_report_is_truncated_safely():
+    import ctypes as C
+
+    lib = abi.load()
+    sc, cam, p = abi.Scene(), abi.Camera(), abi.RenderParams()
+    buf = C.create_string_buffer(8)
+    txt = (HEADER + "[main_parameters]\nfog_color_1 1 2 3;\n").encode()
+    assert lib.mbr_fract_parse(txt, C.byref(sc), C.byref(cam), C.byref(p), buf, 8) == abi.MBR_OK
+    assert len(buf.value) == 7
+    assert lib.mbr_fract_parse(txt, C.byref(sc), C.byref(cam), C.byref(p), None, 0) == abi.MBR_OK
+    assert lib.mbr_fract_parse(None, C.byref(sc), C.byref(cam), C.byref(p), None, 0) == abi.MBR_EINVAL
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
+def test_reference_examples():
+    """Every example scene the reference ships is read: none is malformed, and a
+    scene is accepted exactly when the formulas it iterates are built here and
+    none of the unsupported features appears."""
+    files = sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.fract"), recursive=True))
+    assert len(files) > 150
+    ok = 0
+    for path in files:
+        s = settings.load_from_file(path)
+        assert s.status in (abi.MBR_OK, abi.MBR_EUNSUPPORTED), (path, s.report)
+        sc = s.scene
+        used = range(sc.n_fractals) if sc.hybrid_fractal_enable else range(1)
+        formulas = {sc.fractal[i].formula for i in used} - {0}
+        if s.ok:
+            ok += 1
+            assert formulas <= {2, 7, 8}, (path, formulas)
+            assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
+        elif not formulas <= {2, 7, 8}:
+            assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
+    assert ok >= 60, ok
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
+def test_reference_examples_render_on_the_oracle(oracle):
+    """Three accepted example scenes (one per formula) rendered small by the
+    oracle from the parsed structs: the fractal is in view."""
+    names = {"mandelbox001.fract": 8, "iteration fog.fract": 7, "mandelbulb001.fract": 2}
+    seen = 0
+    for name, formula in names.items():
+        path = os.path.join(EXAMPLES, name)
+        if not os.path.exists(path):
+            continue
+        s = settings.load_from_file(path)
+        if not s.ok or s.scene.fractal[0].formula != formula:
+            continue
+        cam = s.camera
+        aspect = cam.width / cam.height
+        cam.height = 18
+        cam.width = max(8, int(round(18 * aspect)))
+        p = s.params
+        p.ao_rays = 0
+        out, st = oracle.render(s.scene, cam, p)
+        frac = float(np.mean(out["hit"]))
+        assert 0.02 < frac <= 1.0, (name, frac)
+        seen += 1
+    assert seen >= 1
