@@ -150,20 +150,30 @@ typedef struct mbr_scene {
   mbr_fractal fractal[MBR_MAX_FRACTALS];
 } mbr_scene;
 
+/* params::enumPerspectiveType (src/projection_3d.hpp:44-50): the view
+ * vector of CalculateViewVector (src/projection_3d.cpp:40-89). */
+typedef enum mbr_projection {
+  MBR_PROJECTION_THREE_POINT = 0,     /* normalize(x fov, 1, y fov), fov = 2 tan(FOV/2) */
+  MBR_PROJECTION_FISH_EYE = 1,        /* angle from the axis = |image point| * FOV (radians) */
+  MBR_PROJECTION_EQUIRECTANGULAR = 2, /* longitude x FOV/2, latitude y FOV/2 */
+  /* fish eye whose pixels more than 90 degrees off the axis are not traced:
+   * black, depth 1e20, no hit (render_worker.cpp:165-170, 321) */
+  MBR_PROJECTION_FISH_EYE_CUT = 3
+} mbr_projection;
+
 /* Camera in the reference's terms: camera/target/top vectors
  * (cCameraTarget::SetCameraTargetTop, src/camera_target.cpp:86-130) or, when
  * use_angles != 0, explicit yaw/pitch/roll in radians (viewAngle, as used by
- * PrepareMainVectors, src/render_worker.cpp:539-564).  Only the three-point
- * perspective (projection_3d.cpp:77-84) is supported. */
+ * PrepareMainVectors, src/render_worker.cpp:539-564), and the projection. */
 typedef struct mbr_camera {
   double camera[3];
   double target[3];
   double top[3];
-  double fov_deg;        /* "fov", default 53.13 */
+  double fov_deg;        /* "fov", default 53.13; (0, 180) three-point, (0, 720] the others */
   int32_t width;
   int32_t height;
   int32_t use_angles;
-  int32_t reserved0;
+  int32_t perspective_type; /* mbr_projection, default three-point */
   double angles[3];      /* yaw, pitch, roll (radians) when use_angles != 0 */
 } mbr_camera;
 
@@ -409,8 +419,7 @@ mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera, 
  * MBR_OK: everything that changes the geometry is representable.
  * MBR_EUNSUPPORTED: the structs are filled, but the file uses geometry this
  * path does not build (another formula, boolean combinations, primitives,
- * transforms, forced delta DE, another projection); each is named in the
- * report.  MBR_EINVAL: not a settings file, or a malformed value of a
+ * transforms, forced delta DE); each is named in the report.  MBR_EINVAL: not a settings file, or a malformed value of a
  * parameter read here.  The report (optional, NUL-terminated, truncated to
  * report_size) also lists the shading parameters outside the path that were
  * ignored, and how the main light and AO were mapped. */

@@ -22,6 +22,7 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 
 # mbr_formula (fractal::enumFractalFormula)
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
+PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
 # mbr_engine
@@ -65,7 +66,7 @@ class Scene(C.Structure):
 class Camera(C.Structure):
     _fields_ = [
         ("camera", D3), ("target", D3), ("top", D3), ("fov_deg", C.c_double), ("width", C.c_int32),
-        ("height", C.c_int32), ("use_angles", C.c_int32), ("reserved0", C.c_int32), ("angles", D3),
+        ("height", C.c_int32), ("use_angles", C.c_int32), ("perspective_type", C.c_int32), ("angles", D3),
     ]
 
 

@@ -20,7 +20,7 @@
 // formulas and the hybrid sequence, the iteration and bailout settings,
 // camera, raymarching quality, the main light, AO and the 8-bit conversion.
 // Geometry this path does not build (other formulas, boolean combinations,
-// primitives, transforms, forced delta DE, other projections) makes the call
+// primitives, transforms, forced delta DE) makes the call
 // return MBR_EUNSUPPORTED with each item named in the report; shading
 // parameters outside the path (materials, fog, glow, reflections, textures,
 // further lights) are counted and listed as ignored.
@@ -416,8 +416,12 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     if (parse_int(value, b)) cam->width = b; else R.bad(name, value);
   } else if (name == "image_height") {
     if (parse_int(value, b)) cam->height = b; else R.bad(name, value);
-  } else if (name == "perspective_type") {
-    if (!(value == "three_point" || value == "0")) R.unsupported.push_back(name + " " + value + " (projection)");
+  } else if (name == "perspective_type") {  // enumeration names of initparameters.cpp:121-122
+    if (value == "three_point" || value == "0") cam->perspective_type = MBR_PROJECTION_THREE_POINT;
+    else if (value == "fish_eye" || value == "1") cam->perspective_type = MBR_PROJECTION_FISH_EYE;
+    else if (value == "equirectangular" || value == "2") cam->perspective_type = MBR_PROJECTION_EQUIRECTANGULAR;
+    else if (value == "fish_eye_cut" || value == "3") cam->perspective_type = MBR_PROJECTION_FISH_EYE_CUT;
+    else R.bad(name, value);
   } else if (name == "legacy_coordinate_system") {
     if (parse_bool(value, b) && b) R.unsupported.push_back(name + " (camera axes)");
   } else if (name == "camera_rotation" || name == "camera_distance_to_target") {

@@ -82,7 +82,7 @@ struct DevFrame {
   int32_t refine;
   int32_t jitter;
   uint32_t seed;
-  double fov;          // 2 tan(fov/2)
+  double fov;          // CalcFOV: 2 tan(FOV/2) three-point, FOV in radians otherwise
   double resolution;   // 1 / height
   double aspect;
   double detail_level;
@@ -105,6 +105,7 @@ struct DevFrame {
   int32_t gi_bounces;
   uint32_t gi_seed;
   int32_t want_normal;
+  int32_t persp;       // mbr_projection
   double gi_sky;
   double gi_sun;
   double dof_aperture;

@@ -333,8 +333,12 @@ void camera_matrix(const mbr_camera &cam, double mrot[9], bool *zero, double ang
 mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam) {
   if (cam.width < 1 || cam.height < 1 || cam.width > 65535 || cam.height > 65535)
     return set_err(ctx, MBR_EINVAL, "image size %dx%d out of range [1, 65535]", cam.width, cam.height);
-  if (!(cam.fov_deg > 0.0 && cam.fov_deg < 180.0))
-    return set_err(ctx, MBR_EINVAL, "fov_deg must be in (0, 180), got %g", cam.fov_deg);
+  if (cam.perspective_type < MBR_PROJECTION_THREE_POINT || cam.perspective_type > MBR_PROJECTION_FISH_EYE_CUT)
+    return set_err(ctx, MBR_EINVAL, "unknown perspective_type %d", cam.perspective_type);
+  if (cam.perspective_type == MBR_PROJECTION_THREE_POINT && !(cam.fov_deg > 0.0 && cam.fov_deg < 180.0))
+    return set_err(ctx, MBR_EINVAL, "fov_deg must be in (0, 180) for the three-point projection, got %g", cam.fov_deg);
+  if (cam.perspective_type != MBR_PROJECTION_THREE_POINT && !(cam.fov_deg > 0.0 && cam.fov_deg <= 720.0))
+    return set_err(ctx, MBR_EINVAL, "fov_deg must be in (0, 720], got %g", cam.fov_deg);
   if (!finite3(cam.camera) || !finite3(cam.target) || !finite3(cam.top) || !finite3(cam.angles))
     return set_err(ctx, MBR_EINVAL, "non-finite camera vector");
   if (!cam.use_angles && cam.top[0] == 0.0 && cam.top[1] == 0.0 && cam.top[2] == 0.0)
@@ -382,7 +386,10 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.refine = p.refine;
   f.jitter = p.jitter ? 1 : 0;
   f.seed = p.seed;
-  f.fov = 2.0 * std::tan(cam.fov_deg / 360.0 * kPi);
+  // CalcFOV (projection_3d.cpp:140-159)
+  f.persp = cam.perspective_type;
+  f.fov = cam.perspective_type == MBR_PROJECTION_THREE_POINT ? 2.0 * std::tan(cam.fov_deg / 360.0 * kPi)
+                                                              : cam.fov_deg / 180.0 * kPi;
   f.resolution = 1.0 / cam.height;
   f.aspect = double(cam.width) / cam.height;
   f.detail_level = p.detail_level;

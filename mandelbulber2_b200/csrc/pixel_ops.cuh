@@ -118,8 +118,29 @@ __device__ __forceinline__ void image_point(const DevFrame &fr, double x, double
   *ix = (scaleX * x + -0.5) * fr.aspect;
   *iy = scaleY * y + 0.5;
 }
+// CalculateViewVector (projection_3d.cpp:40-89) before the camera rotation:
+// the view vector of image point (ix, iy) (aspect applied), with fov from
+// CalcFOV.  Three-point: (x fov, 1, y fov); fish eye: at angle |v| fov from
+// the axis; equirectangular: longitude x fov/2, latitude y fov/2.
+__device__ __forceinline__ D3 projection_dir(int persp, double fov, double ix, double iy) {
+  if (persp == MBR_PROJECTION_FISH_EYE || persp == MBR_PROJECTION_FISH_EYE_CUT) {
+    const double r = sqrt(ix * ix + iy * iy);
+    if (r == 0.0) return D3{0.0, 1.0, 0.0};
+    return D3{ix / r * sin(r * fov), cos(r * fov), iy / r * sin(r * fov)};
+  }
+  if (persp == MBR_PROJECTION_EQUIRECTANGULAR) {
+    const double vx = ix * 0.5, vy = iy * 0.5;
+    return D3{sin(fov * vx) * cos(fov * vy), cos(fov * vx) * cos(fov * vy), sin(fov * vy)};
+  }
+  return D3{ix * fov, 1.0, iy * fov};
+}
+// Fish-eye cut: an image point more than 90 degrees off the axis is not
+// traced (render_worker.cpp:165-170, 321); its pixel is black, with no hit.
+__device__ __forceinline__ bool hemisphere_cut(int persp, double fov, double ix, double iy) {
+  return persp == MBR_PROJECTION_FISH_EYE_CUT && sqrt(ix * ix + iy * iy) > 3.14159265358979323846 * 0.5 / fov;
+}
 __device__ __forceinline__ D3 view_vector(const DevFrame &fr, double ix, double iy) {
-  return rotate(fr, d3norm(D3{ix * fr.fov, 1.0, iy * fr.fov}));
+  return rotate(fr, d3norm(projection_dir(fr.persp, fr.fov, ix, iy)));
 }
 __device__ __forceinline__ D3 camera_of(const DevFrame &fr) { return {fr.camera[0], fr.camera[1], fr.camera[2]}; }
 __device__ __forceinline__ double dist_thresh(const DevScene &sc, const DevFrame &fr, D3 q) {

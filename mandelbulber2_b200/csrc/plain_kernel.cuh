@@ -110,7 +110,14 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ DevS
     MarchOut m;
     float nrm[3] = {0.0f, 0.0f, 0.0f};
     float shade = 0.0f, ao = 1.0f, rgb[3];
-    if (fr.gi_samples > 0) {
+    double cx, cy;
+    image_point(fr, double(x), double(y), &cx, &cy);
+    if (hemisphere_cut(fr.persp, fr.fov, cx, cy)) {
+      m.found = false;
+      m.depth = 1e20;
+      m.iters = 0;
+      rgb[0] = rgb[1] = rgb[2] = 0.0f;
+    } else if (fr.gi_samples > 0) {
       double acc = 0.0;
       for (int s = 0; s < fr.gi_samples; s++) {
         MarchOut mm;

@@ -73,6 +73,7 @@ struct WJob {
   int32_t mrot_zero;
   int32_t width, height, tiles_x;
   int32_t row0, rows;      // the job renders rows [row0, row0 + rows) of its frame
+  int32_t persp;           // mbr_projection
   long long first;         // first work item of this job in the pixel queue
   long long pixel_offset;  // first pixel of this job in the outputs
   double fov, aspect;
@@ -739,6 +740,17 @@ struct PrimaryStage {
     const double ix = (1.0 / double(jb->width) * double(x) + -0.5) * jb->aspect;
     const double iy = -1.0 / double(jb->height) * double(y) + 0.5;
     double vx = ix * jb->fov, vy = 1.0, vz = iy * jb->fov;
+    if (jb->persp != MBR_PROJECTION_THREE_POINT) {
+      if (hemisphere_cut(jb->persp, jb->fov, ix, iy)) {
+        last_iters = 0;
+        write_miss(true);
+        return false;
+      }
+      const D3 v = projection_dir(jb->persp, jb->fov, ix, iy);
+      vx = v.x;
+      vy = v.y;
+      vz = v.z;
+    }
     double n = 1.0 / sqrt(vx * vx + vy * vy + vz * vz);
     vx *= n;
     vy *= n;
@@ -777,8 +789,10 @@ struct PrimaryStage {
     return true;
   }
 
-  __device__ void write_miss() {
+  // cut: a fish-eye-cut pixel, not traced and black
+  __device__ void write_miss(bool cut = false) {
     float rgb[3] = {fr.background[0], fr.background[1], fr.background[2]};
+    if (cut) rgb[0] = rgb[1] = rgb[2] = 0.0f;
     if (out.depth) out.depth[pix] = 1e20;
     if (out.iters) out.iters[pix] = last_iters;
     if (out.hit) out.hit[pix] = 0;
@@ -1359,6 +1373,16 @@ struct GIPrimaryStage {
     const double ujx = rng.uniform(), ujy = rng.uniform(), ulr = rng.uniform(), ula = rng.uniform();
     double ix, iy;
     image_point(fr, double(x), double(y), &ix, &iy);
+    if (hemisphere_cut(fr.persp, fr.fov, ix, iy)) {  // not traced: black, no hit
+      last_iters = 0;
+      if (sample == 0) {
+        if (out.depth) out.depth[pix] = 1e20;
+        if (out.iters) out.iters[pix] = 0;
+        if (out.hit) out.hit[pix] = 0;
+      }
+      L.path_rad[path] = 0.0;
+      return false;
+    }
     ix = ix + (ujx - 0.5) / double(fr.width) * fr.aspect;
     iy = iy + (ujy - 0.5) / double(fr.height);
     D3 view = view_vector(fr, ix, iy);
@@ -1685,6 +1709,7 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.first = first;
   j.pixel_offset = pixel_offset;
   j.fov = fr.fov;
+  j.persp = fr.persp;
   j.aspect = fr.aspect;
   j.resolution = fr.resolution;
   j.detail = fr.detail_level;

@@ -640,6 +640,12 @@ struct Counters {
   uint64_t de = 0, iters = 0, march = 0, binary = 0, normal = 0, shadow = 0, ao = 0, gi = 0, pixels = 0, watchdog = 0;
 };
 
+// CalcFOV (projection_3d.cpp:140-159)
+inline double calc_fov(const mbr_camera &c) {
+  if (c.perspective_type == MBR_PROJECTION_THREE_POINT) return 2.0 * tan(c.fov_deg / 360.0 * M_PI);
+  return c.fov_deg / 180.0 * M_PI;
+}
+
 struct Renderer {
   Seq seq;
   std::vector<SlotT<double>> slots;
@@ -863,10 +869,28 @@ struct Renderer {
     *ix = (scaleX * x + -0.5) * aspect;
     *iy = scaleY * y + 0.5;
   }
+  // CalculateViewVector (projection_3d.cpp:40-89) for the camera's projection
   D3 view_vector(double ix, double iy) const {
-    D3 v{ix * fov, 1.0, iy * fov};
+    D3 v;
+    if (cam.perspective_type == MBR_PROJECTION_FISH_EYE || cam.perspective_type == MBR_PROJECTION_FISH_EYE_CUT) {
+      const double r = sqrt(ix * ix + iy * iy);
+      if (r == 0.0) {
+        v = D3{0.0, 1.0, 0.0};
+      } else {
+        v = D3{ix / r * sin(r * fov), cos(r * fov), iy / r * sin(r * fov)};
+      }
+    } else if (cam.perspective_type == MBR_PROJECTION_EQUIRECTANGULAR) {
+      const double vx = ix * 0.5, vy = iy * 0.5;
+      v = D3{sin(fov * vx) * cos(fov * vy), cos(fov * vx) * cos(fov * vy), sin(fov * vy)};
+    } else {
+      v = D3{ix * fov, 1.0, iy * fov};
+    }
     v = normalize(v);
     return rotate(M, v);
+  }
+  // fish-eye cut: image points beyond 90 degrees are not traced (render_worker.cpp:165-170, 321)
+  bool hemisphere_cut(double ix, double iy) const {
+    return cam.perspective_type == MBR_PROJECTION_FISH_EYE_CUT && sqrt(ix * ix + iy * iy) > M_PI * 0.5 / fov;
   }
 
   struct PixelOut {
@@ -1046,7 +1070,7 @@ static bool make_renderer(const mbr_scene *scene, const mbr_camera *cam, const m
   double ang[3];
   camera_setup(*cam, &R->M, ang);
   R->camera = D3{cam->camera[0], cam->camera[1], cam->camera[2]};
-  R->fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);  // CalcFOV three-point (projection_3d.cpp:145-148)
+  R->fov = calc_fov(*cam);
   R->resolution = 1.0 / cam->height;                // render_job.cpp:477
   R->aspect = double(cam->width) / cam->height;     // render_worker.cpp:98
   R->light = normalize(D3{params->light_direction[0], params->light_direction[1], params->light_direction[2]});
@@ -1107,7 +1131,17 @@ int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_rende
         const uint64_t pixel = uint64_t(y) * W + x;
         Renderer::PixelOut po;
         Renderer::March m;
-        if (params->gi_samples > 0) {
+        double cx, cy;
+        R.image_point(double(x), double(y), &cx, &cy);
+        if (R.hemisphere_cut(cx, cy)) {  // black, depth 1e20, no hit
+          po.hit = false;
+          po.depth = 1e20;
+          po.iters = 0;
+          po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
+          po.shade = 0.0f;
+          po.ao = 1.0f;
+          po.rgb[0] = po.rgb[1] = po.rgb[2] = 0.0f;
+        } else if (params->gi_samples > 0) {
           double acc = 0.0;
           for (int s = 0; s < params->gi_samples; s++) {
             Renderer::March mm;
@@ -1217,7 +1251,7 @@ int oracle_view(const mbr_camera *cam, int x, int y, double *dir) {
   R.cam = *cam;
   double ang[3];
   camera_setup(*cam, &R.M, ang);
-  R.fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);
+  R.fov = calc_fov(*cam);
   R.aspect = double(cam->width) / cam->height;
   double ix, iy;
   R.image_point(double(x), double(y), &ix, &iy);
@@ -1232,7 +1266,7 @@ int oracle_view_ip(const mbr_camera *cam, double ix, double iy, double *dir) {
   R.cam = *cam;
   double ang[3];
   camera_setup(*cam, &R.M, ang);
-  R.fov = 2.0 * tan(cam->fov_deg / 360.0 * M_PI);
+  R.fov = calc_fov(*cam);
   D3 d = normalize(R.view_vector(ix, iy));
   dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
   return 0;

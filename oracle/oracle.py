@@ -193,6 +193,9 @@ class Reference:
         L.ref_view_vector.argtypes = [_P, _P, _P, C.c_double, C.c_double, C.c_double, _P]
         L.ref_calc_fov.restype = C.c_double
         L.ref_calc_fov.argtypes = [C.c_double]
+        L.ref_view_vector_p.argtypes = [_P, _P, _P, C.c_double, C.c_int, C.c_double, C.c_double, _P]
+        L.ref_calc_fov_p.restype = C.c_double
+        L.ref_calc_fov_p.argtypes = [C.c_double, C.c_int]
         L.ref_random.argtypes = [C.c_uint, C.c_int, C.c_int, _P]
 
     @staticmethod
@@ -219,6 +222,13 @@ class Reference:
         a = [np.array(v, dtype=np.float64) for v in (cam, target, top)]
         self.lib.ref_view_vector(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, fov_deg, ix, iy,
                                  out.ctypes.data)
+        return out
+
+    def view_vector_p(self, cam, target, top, fov_deg, persp, ix, iy):
+        out = np.zeros(3, dtype=np.float64)
+        a = [np.array(v, dtype=np.float64) for v in (cam, target, top)]
+        self.lib.ref_view_vector_p(a[0].ctypes.data, a[1].ctypes.data, a[2].ctypes.data, fov_deg, persp, ix, iy,
+                                   out.ctypes.data)
         return out
 
     def random(self, seed: int, n: int, max_: int = -1):

@@ -121,6 +121,29 @@ int ref_view_vector(const double *cam, const double *target, const double *top, 
 
 double ref_calc_fov(double fov_deg) { return CalcFOV(fov_deg, params::perspThreePoint); }
 
+// The same for projection `persp` (params::enumPerspectiveType): CalcFOV and
+// CalculateViewVector of that projection, then normalised as in doWork.
+int ref_view_vector_p(const double *cam, const double *target, const double *top, double fov_deg, int persp,
+                      double ix, double iy, double *out) {
+  cCameraTarget ct(CVector3(cam[0], cam[1], cam[2]), CVector3(target[0], target[1], target[2]),
+                   CVector3(top[0], top[1], top[2]));
+  CVector3 a = ct.GetRotation();
+  CRotationMatrix m;
+  m.RotateZ(a.x);
+  m.RotateX(a.y);
+  m.RotateY(a.z);
+  const params::enumPerspectiveType pt = params::enumPerspectiveType(persp);
+  double fov = CalcFOV(fov_deg, pt);
+  CVector3 v = CalculateViewVector(CVector2<double>(ix, iy), fov, pt, m);
+  v.Normalize();
+  out[0] = v.x;
+  out[1] = v.y;
+  out[2] = v.z;
+  return 0;
+}
+
+double ref_calc_fov_p(double fov_deg, int persp) { return CalcFOV(fov_deg, params::enumPerspectiveType(persp)); }
+
 // n draws of Random(max) from gRandomSeed = seed (max < 0: RandomInt()).
 int ref_random(unsigned int seed, int max, int n, int *out) {
   gRandomSeed = seed;

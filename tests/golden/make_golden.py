@@ -3,6 +3,8 @@ sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
 
   formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
                     Mandelbox, Menger sponge) on seeded random points
+  projection_kat.json  CalcFOV + CalculateViewVector of the fish-eye,
+                    equirectangular and fish-eye-cut projections
   camera_kat.json   cCameraTarget + PrepareMainVectors rotations and
                     CalculateViewVector directions
   random_kat.json   Park-Miller Random()/RandomInt() sequences
@@ -96,6 +98,24 @@ def camera_kats(ref: Reference) -> list:
     return out
 
 
+# (projection, FOV degrees): fish eye below and beyond a hemisphere,
+# equirectangular over the full sphere, fish-eye cut
+PROJECTIONS = [(1, 120.0), (1, 200.0), (2, 360.0), (2, 90.0), (3, 180.0)]
+
+
+def projection_kats(ref: Reference) -> list:
+    out = []
+    for cam, tgt, top in CAMERAS[:4]:
+        for persp, fov in PROJECTIONS:
+            views = []
+            for ix, iy in VIEW_POINTS:
+                views.append({"ix": float(ix).hex(), "iy": float(iy).hex(),
+                              "dir": hexs(ref.view_vector_p(cam, tgt, top, fov, persp, ix, iy))})
+            out.append({"camera": cam, "target": tgt, "top": top, "perspective_type": persp, "fov_deg": fov,
+                        "fov": float(ref.lib.ref_calc_fov_p(fov, persp)).hex(), "views": views})
+    return out
+
+
 def random_kats(ref: Reference) -> list:
     out = []
     for seed in (1, 12345, 2147483646, 987654321):
@@ -110,6 +130,8 @@ def main() -> None:
         json.dump(formula_kats(ref), f, separators=(",", ":"))
     with open(os.path.join(HERE, "camera_kat.json"), "w") as f:
         json.dump(camera_kats(ref), f, indent=1)
+    with open(os.path.join(HERE, "projection_kat.json"), "w") as f:
+        json.dump(projection_kats(ref), f, indent=1)
     with open(os.path.join(HERE, "random_kat.json"), "w") as f:
         json.dump(random_kats(ref), f)
     print("golden vectors written to", HERE)

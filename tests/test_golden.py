@@ -89,6 +89,20 @@ def test_camera_kat_library_host():
         assert m == fh(c["mrot"])
 
 
+def test_projection_kat_oracle(oracle):
+    """Fish-eye, equirectangular and fish-eye-cut view vectors of the oracle
+    equal the reference's CalcFOV + CalculateViewVector bit for bit."""
+    kats = load("projection_kat.json")
+    assert {k["perspective_type"] for k in kats} == {1, 2, 3}
+    for c in kats:
+        cam = _cam(c)
+        cam.fov_deg = c["fov_deg"]
+        cam.perspective_type = c["perspective_type"]
+        for v in c["views"]:
+            d = oracle.view_ip(cam, fh(v["ix"]), fh(v["iy"]))
+            assert list(d) == fh(v["dir"]), (c["perspective_type"], c["fov_deg"], v)
+
+
 def test_fov_kat():
     for c in load("camera_kat.json"):
         assert 2.0 * math.tan(53.0 / 360.0 * math.pi) == fh(c["fov53"])

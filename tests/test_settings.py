@@ -172,16 +172,25 @@ def test_unsupported_geometry_is_named():
     assert s.status == abi.MBR_EUNSUPPORTED
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_sphere_1_enabled true;\nboolean_operators true;\n"
-                    "perspective_type fish_eye;\ndelta_DE_method 1;\n[fractal_1]\nmandelbox_rotations_enabled true;\n")
+                    "legacy_coordinate_system true;\ndelta_DE_method 1;\n[fractal_1]\n"
+                    "mandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
-    for key in ("primitive_sphere_1_enabled", "boolean_operators", "perspective_type fish_eye",
+    for key in ("primitive_sphere_1_enabled", "boolean_operators", "legacy_coordinate_system",
                 "delta_DE_method 1", "mandelbox_rotations_enabled"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
     s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
     assert s.ok, s.report
+
+
+@pytest.mark.parametrize("value,want", [("three_point", 0), ("fish_eye", 1), ("equirectangular", 2),
+                                        ("fish_eye_cut", 3), ("2", 2)])
+def test_projection(value, want):
+    s = settings.load_from_string(HEADER + f"[main_parameters]\nperspective_type {value};\nfov 200;\n")
+    assert s.ok, s.report
+    assert s.camera.perspective_type == want and s.camera.fov_deg == 200.0
 
 
 def test_report_is_truncated_safely():
