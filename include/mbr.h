@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MBR_ABI_VERSION 1
+#define MBR_ABI_VERSION 2
 
 /* Number of formula slots of one hybrid sequence (the reference's nine
  * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
@@ -116,7 +116,7 @@ typedef struct mbr_fractal {
   double bulb_power;               /* "power", default 9 */
   double bulb_alpha_angle_offset;  /* degrees, default 0 */
   double bulb_beta_angle_offset;   /* degrees, default 0 */
-  /* Mandelbox: sFractalMandelbox (src/fractal.h:185-219); rotations off */
+  /* Mandelbox: sFractalMandelbox (src/fractal.h:185-219) */
   double mandelbox_scale;                 /* default 2 */
   double mandelbox_folding_limit;         /* default 1 */
   double mandelbox_folding_value;         /* default 2 */
@@ -125,6 +125,19 @@ typedef struct mbr_fractal {
   double mandelbox_offset[3];             /* default (0,0,0) */
   /* Menger sponge: sFractalTransformCommon::scale3 (default 3) */
   double transf_scale3;
+  /* Mandelbox rotations (sFractalMandelbox rotationsEnabled, rotation[2][3],
+   * mainRotationEnabled, rotationMain: src/fractal.h:185-219; matrices as in
+   * src/fractal.cpp:663-671).  Angles in degrees; a vector (x, y, z) is the
+   * rotation RotateZ(z) RotateY(y) RotateX(x).  With rotations on, axis k of
+   * the box fold is folded in the frame of rotation_neg[k] (the side above
+   * the limit) or rotation_pos[k] (the side below it)
+   * (formula/definition/fractal_mandelbox.cpp:33-63); the main rotation turns
+   * z after the sphere fold (:103).  Only in a scene that is not a hybrid. */
+  int32_t mandelbox_rotations_enabled;      /* default 0 */
+  int32_t mandelbox_main_rotation_enabled;  /* default 0 */
+  double mandelbox_rotation_neg[3][3];      /* "mandelbox_rotation_neg_1..3" */
+  double mandelbox_rotation_pos[3][3];      /* "mandelbox_rotation_pos_1..3" */
+  double mandelbox_rotation_main[3];        /* "mandelbox_rotation_main" */
 } mbr_fractal;
 
 /* The fractal part of a scene: one fractal (or hybrid) object node with the

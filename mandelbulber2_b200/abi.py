@@ -49,6 +49,8 @@ class Fractal(C.Structure):
         ("mandelbox_folding_value", C.c_double), ("mandelbox_folding_min_radius", C.c_double),
         ("mandelbox_folding_fixed_radius", C.c_double), ("mandelbox_offset", D3),
         ("transf_scale3", C.c_double),
+        ("mandelbox_rotations_enabled", C.c_int32), ("mandelbox_main_rotation_enabled", C.c_int32),
+        ("mandelbox_rotation_neg", D3 * 3), ("mandelbox_rotation_pos", D3 * 3), ("mandelbox_rotation_main", D3),
     ]
 
 

@@ -385,6 +385,8 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
     return set_err(ctx, MBR_EINVAL, "the adjoint differentiates a camera given by position and angles (use_angles = 1)");
   if (camera->perspective_type != MBR_PROJECTION_THREE_POINT)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the three-point projection");
+  if (sc->mbrot.folds || sc->mbrot.main)
+    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the Mandelbox without rotations");
   if (sc->is_hybrid || sc->has_w || sc->iter_thresh || sc->interior ||
       (sc->slot[0].formula != MBR_FORMULA_MANDELBULB && sc->slot[0].formula != MBR_FORMULA_MANDELBOX))
     return set_err(ctx, MBR_EUNSUPPORTED,

@@ -87,14 +87,56 @@ __device__ __forceinline__ void f_mandelbulb(V4<T> &z, T r, T &DE, const DevSlot
   z.z = sth * rp;
 }
 
+// CRotationMatrix::RotateVector on the xyz of a 4-vector (algebra.cpp:333-344,
+// 168-175), or with the transpose (rotinv, fractal.cpp:670)
+template <class T>
+__device__ __forceinline__ V4<T> mb_turn(const double *m, bool transpose, const V4<T> &v) {
+  V4<T> r = v;
+  if (!transpose) {
+    r.x = T(m[0]) * v.x + T(m[1]) * v.y + T(m[2]) * v.z;
+    r.y = T(m[3]) * v.x + T(m[4]) * v.y + T(m[5]) * v.z;
+    r.z = T(m[6]) * v.x + T(m[7]) * v.y + T(m[8]) * v.z;
+  } else {
+    r.x = T(m[0]) * v.x + T(m[3]) * v.y + T(m[6]) * v.z;
+    r.y = T(m[1]) * v.x + T(m[4]) * v.y + T(m[7]) * v.z;
+    r.z = T(m[2]) * v.x + T(m[5]) * v.y + T(m[8]) * v.z;
+  }
+  return r;
+}
+
+template <class T>
+__device__ __forceinline__ T &v4_axis(V4<T> &v, int dim) {
+  return dim == 0 ? v.x : (dim == 1 ? v.y : v.z);
+}
+
+// rot: the scene's Mandelbox rotations (nullptr or zero flags: none)
 template <class T, bool W>
-__device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s) {
+__device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s, const MbRot *rot) {
   // box fold; the host requires folding_limit >= 0, so |z| > limit implies
   // z != 0 and copysign(value, z) equals sign(z) * value exactly
   const T limit = P<T>(s, P_MB_LIMIT), value = P<T>(s, P_MB_VALUE);
-  if (m_abs(z.x) > limit) z.x = m_copysign(value, z.x) - z.x;
-  if (m_abs(z.y) > limit) z.y = m_copysign(value, z.y) - z.y;
-  if (m_abs(z.z) > limit) z.z = m_copysign(value, z.z) - z.z;
+  if (rot && rot->folds) {
+    // each axis folded in the frame of rot[0][dim] above the limit, else of
+    // rot[1][dim] below minus the limit, then turned back
+    // (fractal_mandelbox.cpp:33-63)
+    for (int dim = 0; dim < 3; dim++) {
+      V4<T> zr = rot->zero[0][dim] ? z : mb_turn<T>(rot->m[0][dim], false, z);
+      if (v4_axis(zr, dim) > limit) {
+        v4_axis(zr, dim) = value - v4_axis(zr, dim);
+        z = mb_turn<T>(rot->m[0][dim], true, zr);
+      } else {
+        zr = rot->zero[1][dim] ? z : mb_turn<T>(rot->m[1][dim], false, z);
+        if (v4_axis(zr, dim) < -limit) {
+          v4_axis(zr, dim) = -value - v4_axis(zr, dim);
+          z = mb_turn<T>(rot->m[1][dim], true, zr);
+        }
+      }
+    }
+  } else {
+    if (m_abs(z.x) > limit) z.x = m_copysign(value, z.x) - z.x;
+    if (m_abs(z.y) > limit) z.y = m_copysign(value, z.y) - z.y;
+    if (m_abs(z.z) > limit) z.z = m_copysign(value, z.z) - z.z;
+  }
   T r2 = z.x * z.x + z.y * z.y + z.z * z.z;
   if (W) r2 = r2 + z.w * z.w;
   // FP64 always applies the offset, as the reference does; FP32 skips a zero
@@ -125,6 +167,7 @@ __device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s) {
     z.y = z.y - P<T>(s, P_MB_OFF_Y);
     z.z = z.z - P<T>(s, P_MB_OFF_Z);
   }
+  if (rot && rot->main && !rot->main_zero) z = mb_turn<T>(rot->mm, false, z);  // :103
   const T scale = P<T>(s, P_MB_SCALE);
   z.x = z.x * scale;
   z.y = z.y * scale;
@@ -155,10 +198,11 @@ __device__ __forceinline__ void f_menger(V4<T> &z, T &DE, const DevSlot &s) {
 }
 
 template <class T, bool W>
-__device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s) {
+__device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
+                                                 const MbRot *rot) {
   switch (formula) {
     case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
-    case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s); break;
+    case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s, rot); break;
     default: f_menger<T, W>(z, DE, s); break;
   }
 }
@@ -214,10 +258,10 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
     const T tempDE = DE;
     if (F != 0) {
       if (F == MBR_FORMULA_MANDELBULB) f_mandelbulb<T>(z, r, DE, s);
-      if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
+      if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s, &sc.mbrot);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W>(s.formula, z, r, DE, s);
+      formula_dispatch<T, W>(s.formula, z, r, DE, s, &sc.mbrot);
     }
     if (s.add_c) {
       if (sc.julia) {

@@ -42,6 +42,12 @@ struct FastParams {
   float p0, p1, p2, p3, p4, p5;  // formula specific (see load_fast_params)
   float q0, q1, q2, q3, q4;      // derived constants of the simple Mandelbox path
   float off_x, off_y, off_z;     // mandelbox offset (0 when absent)
+  // mandelbox rotations (MbRot in FP32; the simple path is off when any is on)
+  int rot_folds;                 // box fold in rotated frames
+  int rot_main;                  // main rotation (enabled and not the identity)
+  int rot_zero[2][3];            // rot[fold][axis] is the identity
+  float rot_m[2][3][9];          // rot[fold][axis], row-major; rotinv is the transpose
+  float rot_mm[9];               // main rotation
 };
 
 // mandelbulb: p0 power, p1 power-1, p2 alpha, p3 beta
@@ -67,6 +73,14 @@ __host__ __device__ inline FastParams load_fast_params(const DevScene &sc) {
   f.off_x = f.off_y = f.off_z = 0.0f;
   f.box_simple = 0;
   f.bulb_n = 0;
+  f.rot_folds = sc.mbrot.folds;
+  f.rot_main = (sc.mbrot.main && !sc.mbrot.main_zero) ? 1 : 0;
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 3; b++) {
+      f.rot_zero[a][b] = sc.mbrot.zero[a][b];
+      for (int k = 0; k < 9; k++) f.rot_m[a][b][k] = float(sc.mbrot.m[a][b][k]);
+    }
+  for (int k = 0; k < 9; k++) f.rot_mm[k] = float(sc.mbrot.mm[k]);
   f.p0 = f.p1 = f.p2 = f.p3 = f.p4 = f.p5 = 0.0f;
   f.q0 = f.q1 = f.q2 = f.q3 = f.q4 = 0.0f;
   if (s.formula == MBR_FORMULA_MANDELBULB) {
@@ -85,7 +99,8 @@ __host__ __device__ inline FastParams load_fast_params(const DevScene &sc) {
     f.p4 = s.f[P_MB_FR2];
     f.p5 = s.f[P_MB_FACTOR1];
     const double L = s.d[P_MB_LIMIT], F = s.d[P_MB_FACTOR1];
-    f.box_simple = (s.d[P_MB_VALUE] == 2.0 * L && L > 0.0 && F > 1.0 && !s.has_offset) ? 1 : 0;
+    f.box_simple = (s.d[P_MB_VALUE] == 2.0 * L && L > 0.0 && F > 1.0 && !s.has_offset && !sc.mbrot.folds &&
+                    !sc.mbrot.main) ? 1 : 0;
     if (f.box_simple) {
       f.q0 = float(1.0 / (2.0 * L));
       f.q1 = float(4.0 * L);
@@ -146,6 +161,16 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return y;
 }
 
+// z turned by the row-major matrix m, or by its transpose
+__device__ __forceinline__ Z3 turn3(const float *m, bool transpose, const Z3 &v) {
+  if (!transpose)
+    return Z3{fmaf(m[0], v.x, fmaf(m[1], v.y, m[2] * v.z)), fmaf(m[3], v.x, fmaf(m[4], v.y, m[5] * v.z)),
+              fmaf(m[6], v.x, fmaf(m[7], v.y, m[8] * v.z))};
+  return Z3{fmaf(m[0], v.x, fmaf(m[3], v.y, m[6] * v.z)), fmaf(m[1], v.x, fmaf(m[4], v.y, m[7] * v.z)),
+            fmaf(m[2], v.x, fmaf(m[5], v.y, m[8] * v.z))};
+}
+__device__ __forceinline__ float &z3_axis(Z3 &v, int dim) { return dim == 0 ? v.x : (dim == 1 ? v.y : v.z); }
+
 // One Mandelbox iteration + c-addition.  c holds the (pre-multiplied) constant.
 template <bool SIMPLE>
 __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, const FastParams &f) {
@@ -166,9 +191,25 @@ __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, cons
     z.z = fmaf(z.z, s, c.z);
   } else {
     const float L = f.p2, V = f.p3;
-    if (fabsf(z.x) > L) z.x = copysignf(V, z.x) - z.x;
-    if (fabsf(z.y) > L) z.y = copysignf(V, z.y) - z.y;
-    if (fabsf(z.z) > L) z.z = copysignf(V, z.z) - z.z;
+    if (f.rot_folds) {  // fractal_mandelbox.cpp:33-63
+      for (int dim = 0; dim < 3; dim++) {
+        Z3 zr = f.rot_zero[0][dim] ? z : turn3(f.rot_m[0][dim], false, z);
+        if (z3_axis(zr, dim) > L) {
+          z3_axis(zr, dim) = V - z3_axis(zr, dim);
+          z = turn3(f.rot_m[0][dim], true, zr);
+        } else {
+          zr = f.rot_zero[1][dim] ? z : turn3(f.rot_m[1][dim], false, z);
+          if (z3_axis(zr, dim) < -L) {
+            z3_axis(zr, dim) = -V - z3_axis(zr, dim);
+            z = turn3(f.rot_m[1][dim], true, zr);
+          }
+        }
+      }
+    } else {
+      if (fabsf(z.x) > L) z.x = copysignf(V, z.x) - z.x;
+      if (fabsf(z.y) > L) z.y = copysignf(V, z.y) - z.y;
+      if (fabsf(z.z) > L) z.z = copysignf(V, z.z) - z.z;
+    }
     const float r2 = fmaf(z.x, z.x, fmaf(z.y, z.y, z.z * z.z));
     z.x += f.off_x;
     z.y += f.off_y;
@@ -180,6 +221,7 @@ __device__ __forceinline__ void it_mandelbox(Z3 &z, float &dr, const Z3 &c, cons
     z.x = z.x * fs - f.off_x;
     z.y = z.y * fs - f.off_y;
     z.z = z.z * fs - f.off_z;
+    if (f.rot_main) z = turn3(f.rot_mm, false, z);  // :103
     dr = fmaf(dr * fs, f.p1, 1.0f);
     z.x = fmaf(z.x, f.p0, c.x);
     z.y = fmaf(z.y, f.p0, c.y);

@@ -273,9 +273,17 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
     if (parse_vec3(value, v)) std::memcpy(f.mandelbox_offset, v, sizeof(v)); else R.bad(name, value);
   } else if (name == "transf_scale_3") {
     if (parse_double(value, d)) f.transf_scale3 = d; else R.bad(name, value);
-  } else if (name == "mandelbox_rotations_enabled" || name == "mandelbox_main_rotation_enabled") {
-    // only an unsupported feature when the slot is a Mandelbox in use (checked later)
-    if (parse_bool(value, b) && b) R.notes.push_back("slot:" + std::to_string(slot) + ":" + name);
+  } else if (name == "mandelbox_rotations_enabled") {
+    if (parse_bool(value, b)) f.mandelbox_rotations_enabled = b; else R.bad(name, value);
+  } else if (name == "mandelbox_main_rotation_enabled") {
+    if (parse_bool(value, b)) f.mandelbox_main_rotation_enabled = b; else R.bad(name, value);
+  } else if (name == "mandelbox_rotation_main") {
+    if (parse_vec3(value, v)) std::memcpy(f.mandelbox_rotation_main, v, sizeof(v)); else R.bad(name, value);
+  } else if ((starts_with(name, "mandelbox_rotation_neg_") || starts_with(name, "mandelbox_rotation_pos_")) &&
+             name.size() == 24 && name[23] >= '1' && name[23] <= '3') {
+    // rotation[0][k] = mandelbox_rotation_neg_(k+1), rotation[1][k] = ..._pos_(k+1) (fractal.cpp:69-73)
+    double *dst = (name[19] == 'n' ? f.mandelbox_rotation_neg : f.mandelbox_rotation_pos)[name[23] - '1'];
+    if (parse_vec3(value, v)) std::memcpy(dst, v, sizeof(v)); else R.bad(name, value);
   } else if (name == "formula_iterations") {
     if (parse_int(value, b)) f.formula_iterations = b; else R.bad(name, value);
   } else if (name == "formula_weight") {
@@ -626,11 +634,9 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
                               " (formula not built here: 2 Mandelbulb, 7 Menger sponge, 8 Mandelbox are)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
-    if (f == MBR_FORMULA_MANDELBOX)
-      for (const std::string &n : R.notes)
-        if (starts_with(n, ("slot:" + std::to_string(i) + ":").c_str()))
-          R.unsupported.push_back("fractal_" + std::to_string(i + 1) + "." + n.substr(n.rfind(':') + 1) +
-                                  " (Mandelbox rotations)");
+    if (f == MBR_FORMULA_MANDELBOX && R.hybrid &&
+        (scene->fractal[i].mandelbox_rotations_enabled || scene->fractal[i].mandelbox_main_rotation_enabled))
+      R.unsupported.push_back("fractal_" + std::to_string(i + 1) + " rotations (Mandelbox rotations in a hybrid)");
   }
   if (!R.hybrid && R.formula[0] == MBR_FORMULA_NONE) R.unsupported.push_back("formula_1 0 (no fractal)");
   // the node's iteration limit is the main N (CopyFractalParams, settings.cpp:2494-2501; the hybrid root :2775-2778)

@@ -44,6 +44,21 @@ struct DevSlot {
   float f[P_COUNT];
 };
 
+// Mandelbox rotations of slot 0 of a single-fractal scene (sFractalMandelbox
+// rot, rotinv, mainRot; fractal.cpp:663-671): row-major matrices built on the
+// host from the angles.  rotinv is the transpose of rot and is applied as
+// such; zero marks a matrix whose angles were all 0 (CRotationMatrix::zero:
+// RotateVector returns its argument).
+struct MbRot {
+  int32_t folds;        // rotationsEnabled: the box fold in rotated frames
+  int32_t main;         // mainRotationEnabled
+  int32_t zero[2][3];   // rot[fold][axis].zero
+  int32_t main_zero;    // mainRot.zero
+  int32_t pad;
+  double m[2][3][9];    // rot[fold][axis]: fold 0 from mandelbox_rotation_neg, 1 from _pos
+  double mm[9];         // mainRot
+};
+
 struct DevScene {
   int32_t n;
   int32_t is_hybrid;
@@ -66,6 +81,7 @@ struct DevScene {
   float flinear_de_offset;
   float pad0;
   DevSlot slot[MBR_MAX_FRACTALS];
+  MbRot mbrot;             // zero (no rotations) unless slot 0 is a rotated Mandelbox
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 

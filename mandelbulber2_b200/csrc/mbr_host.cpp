@@ -85,6 +85,32 @@ mbr_status cuda_err(mbr_ctx *ctx, int code, const char *what) {
   return set_err(ctx, MBR_ECUDA, "%s: %s", what, cudaGetErrorString(cudaError_t(code)));
 }
 
+// The matrix of CRotationMatrix::SetRotation2(angles_deg * M_PI_180)
+// (fractal.cpp:663, 669; algebra.cpp:296-302, 198-247): from the identity,
+// rotations about z, y and x by the vector's z, y and x angles, each
+// multiplied onto the right and skipped for a zero angle; *zero is set when
+// all three are zero (RotateVector then returns its argument unchanged).
+static void mandelbox_rotation(const double deg[3], double m[9], bool *zero) {
+  const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
+  for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  *zero = true;
+  for (int axis = 2; axis >= 0; axis--) {
+    const double a = deg[axis] * k;
+    if (a == 0.0) continue;
+    const double sn = std::sin(a), cs = std::cos(a);
+    double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (axis == 0) { r[0] = 1.0; r[4] = cs; r[8] = cs; r[5] = -sn; r[7] = sn; }
+    if (axis == 1) { r[4] = 1.0; r[8] = cs; r[0] = cs; r[6] = -sn; r[2] = sn; }
+    if (axis == 2) { r[8] = 1.0; r[0] = cs; r[4] = cs; r[1] = -sn; r[3] = sn; }
+    double t[9];
+    for (int row = 0; row < 3; row++)
+      for (int col = 0; col < 3; col++)
+        t[row * 3 + col] = m[row * 3 + 0] * r[col] + m[row * 3 + 1] * r[3 + col] + m[row * 3 + 2] * r[6 + col];
+    std::memcpy(m, t, sizeof(t));
+    *zero = false;
+  }
+}
+
 // ---- scene -------------------------------------------------------------------
 // Validates `sc` and flattens it into a DevScene.  Restates CollectSequenceData
 // and CreateSequence for the single fractal (or hybrid) node of the default
@@ -110,6 +136,29 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
       sc.delta_de_function != MBR_DE_FUNCTION_LOGARITHMIC)
     return set_err(ctx, MBR_EUNSUPPORTED, "delta_de_function %d is not supported (preferred, linear, log)",
                    sc.delta_de_function);
+  // Mandelbox rotations: slot 0 of a single-fractal scene
+  for (int i = 0; i < (hybrid ? n : 1); i++) {
+    const mbr_fractal &f = sc.fractal[i];
+    const bool rot = f.mandelbox_rotations_enabled || f.mandelbox_main_rotation_enabled;
+    if (!rot || f.formula != MBR_FORMULA_MANDELBOX) continue;
+    if (hybrid)
+      return set_err(ctx, MBR_EUNSUPPORTED, "Mandelbox rotations are supported in single-fractal scenes only");
+    bool ok = finite3(f.mandelbox_rotation_main);
+    for (int a = 0; a < 3; a++) ok = ok && finite3(f.mandelbox_rotation_neg[a]) && finite3(f.mandelbox_rotation_pos[a]);
+    if (!ok) return set_err(ctx, MBR_EINVAL, "non-finite Mandelbox rotation angle");
+    MbRot &r = d.mbrot;
+    r.folds = f.mandelbox_rotations_enabled ? 1 : 0;
+    r.main = f.mandelbox_main_rotation_enabled ? 1 : 0;
+    bool zero;
+    for (int a = 0; a < 3; a++) {
+      mandelbox_rotation(f.mandelbox_rotation_neg[a], r.m[0][a], &zero);
+      r.zero[0][a] = zero ? 1 : 0;
+      mandelbox_rotation(f.mandelbox_rotation_pos[a], r.m[1][a], &zero);
+      r.zero[1][a] = zero ? 1 : 0;
+    }
+    mandelbox_rotation(f.mandelbox_rotation_main, r.mm, &zero);
+    r.main_zero = zero ? 1 : 0;
+  }
   d.n = n;
   d.is_hybrid = hybrid ? 1 : 0;
   double maxBailout = 0.0;

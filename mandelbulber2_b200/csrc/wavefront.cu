@@ -123,6 +123,7 @@ struct WideParams {
   double cm[3];  // fractal_constant_factor
   // simple Mandelbox: folding limit, fR2, fR2/mR2, scale, |scale|, bailout^2
   double lim, fr2, fmx, scale, ascale, bailout2;
+  MbRot rot;  // Mandelbox rotations (the simple form is off when any is on)
 };
 
 __host__ __device__ inline WideParams load_wide_params(const DevScene &sc) {
@@ -142,8 +143,9 @@ __host__ __device__ inline WideParams load_wide_params(const DevScene &sc) {
   }
   const DevSlot &s = sc.slot[0];
   const double L = s.d[P_MB_LIMIT], F = s.d[P_MB_FACTOR1];
+  w.rot = sc.mbrot;
   w.box_simple = (s.formula == MBR_FORMULA_MANDELBOX && s.d[P_MB_VALUE] == 2.0 * L && L > 0.0 && F > 1.0 &&
-                  !s.has_offset) ? 1 : 0;
+                  !s.has_offset && !sc.mbrot.folds && !sc.mbrot.main) ? 1 : 0;
   w.lim = L;
   w.fr2 = s.d[P_MB_FR2];
   w.fmx = F;
@@ -361,7 +363,7 @@ struct Prec64 {
     double de = e.dr;
     if (k == FK_BULB) f_mandelbulb<double>(z, e.r, de, fp.slot);
     else if (k == FK_MENGER) f_menger<double, false>(z, de, fp.slot);
-    else f_mandelbox<double, false>(z, de, fp.slot);
+    else f_mandelbox<double, false>(z, de, fp.slot, &fp.rot);
     if (fp.add_c) {
       if (fp.julia) {
         z.x = z.x + fp.jc[0];
@@ -461,7 +463,7 @@ struct PrecHyb {
     const V4<float> last = z;
     const float tempDE = e.dr;
     float de = e.dr;
-    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s);
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s, &sc.mbrot);
     if (s.add_c) {
       if (sc.julia) {
         z.x = z.x + juliac_of<float>(sc, 0);

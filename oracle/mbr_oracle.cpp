@@ -71,6 +71,9 @@ struct Slot {
   double mb_scale = 2, mb_limit = 1, mb_value = 2, mb_min = 0.5, mb_fixed = 1;
   double mb_offset[3] = {0, 0, 0};
   double scale3 = 3;
+  bool mb_rot = false, mb_main = false;       // rotationsEnabled, mainRotationEnabled
+  double mb_rot_deg[2][3][3] = {};            // rotation[fold][axis]: neg (fold 0), pos (fold 1), degrees
+  double mb_main_deg[3] = {0, 0, 0};          // rotationMain, degrees
 };
 struct Seq {
   bool is_hybrid = false, julia = false;
@@ -128,6 +131,15 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     sl.mb_fixed = f.mandelbox_folding_fixed_radius;
     for (int k = 0; k < 3; k++) sl.mb_offset[k] = f.mandelbox_offset[k];
     sl.scale3 = f.transf_scale3;
+    // fractal.cpp:67-80: rotation[0][i] = mandelbox_rotation_neg_i, rotation[1][i] = ..._pos_i
+    sl.mb_rot = f.mandelbox_rotations_enabled != 0;
+    sl.mb_main = f.mandelbox_main_rotation_enabled != 0;
+    for (int a = 0; a < 3; a++)
+      for (int k = 0; k < 3; k++) {
+        sl.mb_rot_deg[0][a][k] = f.mandelbox_rotation_neg[a][k];
+        sl.mb_rot_deg[1][a][k] = f.mandelbox_rotation_pos[a][k];
+      }
+    for (int k = 0; k < 3; k++) sl.mb_main_deg[k] = f.mandelbox_rotation_main[k];
   }
   if (hybrid && sc.use_default_bailout)
     for (int i = 0; i < n; i++) s.slot[i].bailout = maxBailout;  // :253-259
@@ -224,6 +236,33 @@ inline bool nan4(const V4<S> &v) {  // CVector4::IsNotANumber (algebra.hpp:444-4
 }
 inline int sgn(double v) { return (0.0 < v) - (v < 0.0); }  // math_utilities.h:65-67
 
+// CRotationMatrix::SetRotation2(angles * M_PI_180) (fractal.cpp:663, 669;
+// algebra.cpp:296-302, 198-247): from the identity, RotateZ(z), RotateY(y),
+// RotateX(x), each post-multiplying the matrix and skipped for a zero angle;
+// `zero` stays set (RotateVector is the identity) when all three are zero.
+inline void mb_rotation(const double deg[3], double m[9], bool *zero) {
+  const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
+  for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  *zero = true;
+  const double ang[3] = {deg[2] * k, deg[1] * k, deg[0] * k};
+  const int axis[3] = {2, 1, 0};
+  for (int j = 0; j < 3; j++) {
+    const double a = ang[j];
+    if (a == 0.0) continue;
+    double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double sn = sin(a), cs = cos(a);
+    if (axis[j] == 0) { r[0] = 1.0; r[4] = cs; r[8] = cs; r[5] = -sn; r[7] = sn; }
+    if (axis[j] == 1) { r[4] = 1.0; r[8] = cs; r[0] = cs; r[6] = -sn; r[2] = sn; }
+    if (axis[j] == 2) { r[8] = 1.0; r[0] = cs; r[4] = cs; r[1] = -sn; r[3] = sn; }
+    double t[9];
+    for (int row = 0; row < 3; row++)
+      for (int col = 0; col < 3; col++)
+        t[row * 3 + col] = m[row * 3 + 0] * r[0 * 3 + col] + m[row * 3 + 1] * r[1 * 3 + col] + m[row * 3 + 2] * r[2 * 3 + col];
+    std::memcpy(m, t, sizeof(t));
+    *zero = false;
+  }
+}
+
 // Formula parameters in the scalar type, so tangents can be seeded.
 template <class S>
 struct SlotT {
@@ -231,6 +270,11 @@ struct SlotT {
   S mb_scale, mb_limit, mb_value, mb_mR2, mb_fR2, mb_factor1;
   S mb_off[3];
   S scale3;
+  bool mb_rot, mb_main;
+  double mb_rm[2][3][9];  // rot[fold][axis]; rotinv is its transpose (fractal.cpp:670)
+  bool mb_rz[2][3];       // rot[fold][axis].zero
+  double mb_mm[9];        // mainRot
+  bool mb_mz;             // mainRot.zero
 };
 enum { TAN_POWER = 0, TAN_SCALE = 1, TAN_MR2 = 2, TAN_X = 3, TAN_Y = 4, TAN_Z = 5 };
 
@@ -260,7 +304,31 @@ SlotT<S> make_slot(const Slot &s, bool tangents) {
   t.mb_factor1 = t.mb_fR2 / t.mb_mR2;
   for (int k = 0; k < 3; k++) t.mb_off[k] = S(s.mb_offset[k]);
   t.scale3 = S(s.scale3);
+  t.mb_rot = s.mb_rot;
+  t.mb_main = s.mb_main;
+  for (int f = 0; f < 2; f++)
+    for (int a = 0; a < 3; a++) mb_rotation(s.mb_rot_deg[f][a], t.mb_rm[f][a], &t.mb_rz[f][a]);
+  mb_rotation(s.mb_main_deg, t.mb_mm, &t.mb_mz);
   return t;
+}
+
+// CRotationMatrix::RotateVector of a CVector4: xyz turned, w kept
+// (algebra.cpp:333-344, 168-175); `transpose` applies the matrix's transpose
+// (rotinv, whose zero flag Transpose() clears: algebra.cpp:398-411).
+template <class S>
+inline V4<S> mb_turn(const double *m, bool zero, bool transpose, const V4<S> &v) {
+  if (zero && !transpose) return v;
+  V4<S> r = v;
+  if (!transpose) {
+    r.x = S(m[0]) * v.x + S(m[1]) * v.y + S(m[2]) * v.z;
+    r.y = S(m[3]) * v.x + S(m[4]) * v.y + S(m[5]) * v.z;
+    r.z = S(m[6]) * v.x + S(m[7]) * v.y + S(m[8]) * v.z;
+  } else {
+    r.x = S(m[0]) * v.x + S(m[3]) * v.y + S(m[6]) * v.z;
+    r.y = S(m[1]) * v.x + S(m[4]) * v.y + S(m[7]) * v.z;
+    r.z = S(m[2]) * v.x + S(m[5]) * v.y + S(m[8]) * v.z;
+  }
+  return r;
 }
 
 // cFractalMandelbulb::FormulaCode (fractal_mandelbulb.cpp:29-43)
@@ -279,12 +347,32 @@ inline void formula_mandelbulb(V4<S> &z, const SlotT<S> &f, S &r, S &DE) {
   z.z = sin(th) * rp;
 }
 
-// cFractalMandelbox::FormulaCode, rotations disabled (fractal_mandelbox.cpp:66-107)
+// cFractalMandelbox::FormulaCode (fractal_mandelbox.cpp:31-107)
 template <class S>
 inline void formula_mandelbox(V4<S> &z, const SlotT<S> &f, S &DE) {
-  if (fabs(z.x) > f.mb_limit) z.x = S(double(sgn(val(z.x)))) * f.mb_value - z.x;
-  if (fabs(z.y) > f.mb_limit) z.y = S(double(sgn(val(z.y)))) * f.mb_value - z.y;
-  if (fabs(z.z) > f.mb_limit) z.z = S(double(sgn(val(z.z)))) * f.mb_value - z.z;
+  if (f.mb_rot) {
+    // each axis folded in the frame of rot[0][dim] (above the limit), else
+    // of rot[1][dim] (below minus the limit), and turned back (:33-63)
+    for (int dim = 0; dim < 3; dim++) {
+      V4<S> zr = mb_turn(f.mb_rm[0][dim], f.mb_rz[0][dim], false, z);
+      S &a = dim == 0 ? zr.x : (dim == 1 ? zr.y : zr.z);
+      if (a > f.mb_limit) {
+        a = f.mb_value - a;
+        z = mb_turn(f.mb_rm[0][dim], false, true, zr);
+      } else {
+        zr = mb_turn(f.mb_rm[1][dim], f.mb_rz[1][dim], false, z);
+        S &b = dim == 0 ? zr.x : (dim == 1 ? zr.y : zr.z);
+        if (b < -f.mb_limit) {
+          b = -f.mb_value - b;
+          z = mb_turn(f.mb_rm[1][dim], false, true, zr);
+        }
+      }
+    }
+  } else {
+    if (fabs(z.x) > f.mb_limit) z.x = S(double(sgn(val(z.x)))) * f.mb_value - z.x;
+    if (fabs(z.y) > f.mb_limit) z.y = S(double(sgn(val(z.y)))) * f.mb_value - z.y;
+    if (fabs(z.z) > f.mb_limit) z.z = S(double(sgn(val(z.z)))) * f.mb_value - z.z;
+  }
   const S r2 = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
   z.x = z.x + f.mb_off[0];
   z.y = z.y + f.mb_off[1];
@@ -302,6 +390,7 @@ inline void formula_mandelbox(V4<S> &z, const SlotT<S> &f, S &DE) {
   z.y = z.y - f.mb_off[1];
   z.z = z.z - f.mb_off[2];
   z.w = z.w - 0.0;
+  if (f.mb_main) z = mb_turn(f.mb_mm, f.mb_mz, false, z);  // :103
   z.x = z.x * f.mb_scale; z.y = z.y * f.mb_scale; z.z = z.z * f.mb_scale; z.w = z.w * f.mb_scale;
   DE = DE * fabs(f.mb_scale) + 1.0;
 }

@@ -193,6 +193,7 @@ class Reference:
         L.ref_view_vector.argtypes = [_P, _P, _P, C.c_double, C.c_double, C.c_double, _P]
         L.ref_calc_fov.restype = C.c_double
         L.ref_calc_fov.argtypes = [C.c_double]
+        L.ref_mandelbox_rot_step.argtypes = [_P, _P, _P, _P, C.c_int]
         L.ref_view_vector_p.argtypes = [_P, _P, _P, C.c_double, C.c_int, C.c_double, C.c_double, _P]
         L.ref_calc_fov_p.restype = C.c_double
         L.ref_calc_fov_p.argtypes = [C.c_double, C.c_int]
@@ -209,6 +210,15 @@ class Reference:
         rc = self.lib.ref_formula_step(formula, p.ctypes.data, zz.ctypes.data, C.addressof(rr), C.addressof(dd), i)
         if rc != 0:
             raise RuntimeError("ref_formula_step failed")
+        return zz, rr.value, dd.value
+
+    def mandelbox_rot_step(self, params, z, r: float, de: float, i: int = 0):
+        p = np.array(params, dtype=np.float64)
+        assert p.size == 31
+        zz = np.array(z, dtype=np.float64)
+        rr, dd = C.c_double(r), C.c_double(de)
+        if self.lib.ref_mandelbox_rot_step(p.ctypes.data, zz.ctypes.data, C.addressof(rr), C.addressof(dd), i) != 0:
+            raise RuntimeError("ref_mandelbox_rot_step failed")
         return zz, rr.value, dd.value
 
     def camera(self, cam, target, top):

@@ -76,6 +76,57 @@ int ref_formula_step(int formula, const double *params, double *z, double *aux_r
   return 0;
 }
 
+// One cFractalMandelbox::FormulaCode step with rotations.  params: the eight
+// Mandelbox parameters of ref_formula_step, then rotationsEnabled,
+// mainRotationEnabled, rotation[0][0..2] (mandelbox_rotation_neg_1..3, 9
+// degrees), rotation[1][0..2] (mandelbox_rotation_pos_1..3, 9 degrees) and
+// rotationMain (3 degrees): 31 values.  The matrices are built as
+// sFractal::RecalculateFractalParams builds them (fractal.cpp:663-671).
+int ref_mandelbox_rot_step(const double *params, double *z, double *aux_r, double *aux_de, int iter) {
+  sFractal &f = g_fractal;
+  sExtendedAux aux;
+  std::memset(&aux, 0, sizeof(aux));
+  aux.r = *aux_r;
+  aux.DE = *aux_de;
+  aux.i = iter;
+  aux.color = 1.0;
+  CVector4 v(z[0], z[1], z[2], z[3]);
+  f.mandelbox.scale = params[0];
+  f.mandelbox.foldingLimit = params[1];
+  f.mandelbox.foldingValue = params[2];
+  f.mandelbox.foldingSphericalMin = params[3];
+  f.mandelbox.foldingSphericalFixed = params[4];
+  f.mandelbox.offset = CVector4(params[5], params[6], params[7], 0.0);
+  f.mandelbox.rotationsEnabled = params[8] != 0.0;
+  f.mandelbox.mainRotationEnabled = params[9] != 0.0;
+  for (int fold = 0; fold < 2; fold++)
+    for (int axis = 0; axis < 3; axis++) {
+      const double *a = params + 10 + fold * 9 + axis * 3;
+      f.mandelbox.rotation[fold][axis] = CVector3(a[0], a[1], a[2]);
+    }
+  f.mandelbox.rotationMain = CVector3(params[28], params[29], params[30]);
+  f.mandelbox.mainRot.SetRotation2(f.mandelbox.rotationMain * M_PI_180);
+  for (int fold = 0; fold < MANDELBOX_FOLDS; ++fold)
+    for (int axis = 0; axis < 3; ++axis) {
+      f.mandelbox.rot[fold][axis].SetRotation2(f.mandelbox.rotation[fold][axis] * M_PI_180);
+      f.mandelbox.rotinv[fold][axis] = f.mandelbox.rot[fold][axis].Transpose();
+    }
+  f.mandelbox.fR2 = f.mandelbox.foldingSphericalFixed * f.mandelbox.foldingSphericalFixed;
+  f.mandelbox.mR2 = f.mandelbox.foldingSphericalMin * f.mandelbox.foldingSphericalMin;
+  f.mandelbox.mboxFactor1 = f.mandelbox.fR2 / f.mandelbox.mR2;
+  static cFractalMandelbox fb;
+  fb.FormulaCode(v, &f, aux);
+  f.mandelbox.rotationsEnabled = false;
+  f.mandelbox.mainRotationEnabled = false;
+  z[0] = v.x;
+  z[1] = v.y;
+  z[2] = v.z;
+  z[3] = v.w;
+  *aux_r = aux.r;
+  *aux_de = aux.DE;
+  return 0;
+}
+
 // cCameraTarget(camera, target, top) + the mRot of PrepareMainVectors.
 // out: yaw, pitch, roll, then mRot row-major (9).
 int ref_camera(const double *cam, const double *target, const double *top, double *out) {

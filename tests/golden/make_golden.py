@@ -2,7 +2,8 @@
 sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
 
   formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
-                    Mandelbox, Menger sponge) on seeded random points
+                    Mandelbox with and without rotations, Menger sponge)
+                    on seeded random points
   projection_kat.json  CalcFOV + CalculateViewVector of the fish-eye,
                     equirectangular and fish-eye-cut projections
   camera_kat.json   cCameraTarget + PrepareMainVectors rotations and
@@ -42,6 +43,26 @@ FORMULAS = [
       "mandelbox_folding_min_radius": 0.35, "mandelbox_folding_fixed_radius": 1.1}),
     ("menger_3", 7, [3.0], {"transf_scale3": 3.0}),
 ]
+# Mandelbox with rotations (fractal_mandelbox.cpp:33-63, 103): the eight
+# parameters above, rotationsEnabled, mainRotationEnabled, the neg and pos
+# rotation vectors of the three axes and the main rotation, in degrees.
+_NEG = [[10.0, 0.0, -5.0], [0.0, 25.0, 0.0], [-15.0, 5.0, 30.0]]
+_POS = [[0.0, -20.0, 0.0], [12.0, 0.0, 7.0], [0.0, 0.0, 0.0]]
+_MAIN = [3.0, -17.0, 41.0]
+ROT_FORMULAS = [
+    ("mandelbox_m1_5_rotations", [-1.5, 1.0, 2.0, 0.5, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0] + sum(_NEG, []) + sum(_POS, [])
+     + [0.0, 0.0, 0.0],
+     {"mandelbox_scale": -1.5, "mandelbox_rotations_enabled": 1, "mandelbox_rotation_neg": _NEG,
+      "mandelbox_rotation_pos": _POS}),
+    ("mandelbox_2_main_rotation", [2.0, 1.0, 2.0, 0.5, 1.0, 0.1, -0.2, 0.05, 0.0, 1.0] + [0.0] * 18 + _MAIN,
+     {"mandelbox_scale": 2.0, "mandelbox_offset": [0.1, -0.2, 0.05], "mandelbox_main_rotation_enabled": 1,
+      "mandelbox_rotation_main": _MAIN}),
+    ("mandelbox_m2_both_rotations", [-2.0, 1.0, 2.0, 0.4, 1.0, 0.0, 0.0, 0.0, 1.0, 1.0] + sum(_NEG, [])
+     + sum(_POS, []) + _MAIN,
+     {"mandelbox_scale": -2.0, "mandelbox_folding_min_radius": 0.4, "mandelbox_rotations_enabled": 1,
+      "mandelbox_main_rotation_enabled": 1, "mandelbox_rotation_neg": _NEG, "mandelbox_rotation_pos": _POS,
+      "mandelbox_rotation_main": _MAIN}),
+]
 N_POINTS = 32
 N_STEPS = 6
 
@@ -53,7 +74,8 @@ def hexs(a):
 def formula_kats(ref: Reference) -> dict:
     rng = np.random.default_rng(20241203)
     out = {}
-    for name, fid, params, fields in FORMULAS:
+    entries = [(n, f, p, fl, False) for n, f, p, fl in FORMULAS] + [(n, 8, p, fl, True) for n, p, fl in ROT_FORMULAS]
+    for name, fid, params, fields, rot in entries:
         cases = []
         for _ in range(N_POINTS):
             z = np.zeros(4)
@@ -63,7 +85,10 @@ def formula_kats(ref: Reference) -> dict:
             steps = []
             for i in range(N_STEPS):
                 zin, rin, dein = z.copy(), r, de
-                z, _, de = ref.formula_step(fid, params, z, r, de, i)
+                if rot:
+                    z, _, de = ref.mandelbox_rot_step(params, z, r, de, i)
+                else:
+                    z, _, de = ref.formula_step(fid, params, z, r, de, i)
                 steps.append({"z_in": hexs(zin), "r_in": float(rin).hex(), "de_in": float(dein).hex(),
                               "z_out": hexs(z), "de_out": float(de).hex()})
                 r = math.sqrt(z[0] * z[0] + z[1] * z[1] + z[2] * z[2] + z[3] * z[3])

@@ -34,7 +34,10 @@ def scene_for(formula, fields):
     s = abi.scene_defaults(formula)
     f = s.fractal[0]
     for k, v in fields.items():
-        if isinstance(v, list):
+        if isinstance(v, list) and isinstance(v[0], list):
+            for i, row in enumerate(v):
+                getattr(f, k)[i][:] = row
+        elif isinstance(v, list):
             getattr(f, k)[:] = v
         else:
             setattr(f, k, v)

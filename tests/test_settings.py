@@ -172,17 +172,30 @@ def test_unsupported_geometry_is_named():
     assert s.status == abi.MBR_EUNSUPPORTED
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_sphere_1_enabled true;\nboolean_operators true;\n"
-                    "legacy_coordinate_system true;\ndelta_DE_method 1;\n[fractal_1]\n"
-                    "mandelbox_rotations_enabled true;\n")
+                    "legacy_coordinate_system true;\ndelta_DE_method 1;\nhybrid_fractal_enable true;\n"
+                    "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
     for key in ("primitive_sphere_1_enabled", "boolean_operators", "legacy_coordinate_system",
-                "delta_DE_method 1", "mandelbox_rotations_enabled"):
+                "delta_DE_method 1", "Mandelbox rotations in a hybrid"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
     s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
     assert s.ok, s.report
+
+
+def test_mandelbox_rotations():
+    txt = HEADER + ("[main_parameters]\nformula_1 8;\n[fractal_1]\nmandelbox_rotations_enabled true;\n"
+                    "mandelbox_main_rotation_enabled true;\nmandelbox_rotation_neg_2 10 0 -5,5;\n"
+                    "mandelbox_rotation_pos_3 0 20 0;\nmandelbox_rotation_main 3 -17 41;\n")
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    f = s.scene.fractal[0]
+    assert f.mandelbox_rotations_enabled == 1 and f.mandelbox_main_rotation_enabled == 1
+    assert list(f.mandelbox_rotation_neg[1]) == [10.0, 0.0, -5.5] and list(f.mandelbox_rotation_neg[0]) == [0.0] * 3
+    assert list(f.mandelbox_rotation_pos[2]) == [0.0, 20.0, 0.0]
+    assert list(f.mandelbox_rotation_main) == [3.0, -17.0, 41.0]
 
 
 @pytest.mark.parametrize("value,want", [("three_point", 0), ("fish_eye", 1), ("equirectangular", 2),
