@@ -53,6 +53,8 @@ typedef enum mbr_status {
 typedef enum mbr_formula {
   MBR_FORMULA_NONE = 0,
   MBR_FORMULA_MANDELBULB = 2,   /* formula/definition/fractal_mandelbulb.cpp:29-43 */
+  MBR_FORMULA_MANDELBULB_POWER2 = 3, /* formula/definition/fractal_mandelbulb_power2.cpp:30-45 */
+  MBR_FORMULA_HYPERCOMPLEX = 4, /* formula/definition/fractal_hypercomplex.cpp:30-45; 4-D: plain FP64 engines */
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
   MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
 } mbr_formula;

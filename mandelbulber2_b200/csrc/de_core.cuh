@@ -197,12 +197,45 @@ __device__ __forceinline__ void f_menger(V4<T> &z, T &DE, const DevSlot &s) {
   DE = DE * s3;
 }
 
+// cFractalMandelbulbPower2::FormulaCode (fractal_mandelbulb_power2.cpp:30-45)
+template <class T>
+__device__ __forceinline__ void f_bulb_pow2(V4<T> &z, T r, T &DE) {
+  DE = DE * T(2.0) * r;
+  const T x2 = z.x * z.x;
+  const T y2 = z.y * z.y;
+  const T z2 = z.z * z.z;
+  const T temp = T(1.0) - z2 / (x2 + y2);
+  const T nx = (x2 - y2) * temp;
+  const T ny = T(2.0) * z.x * z.y * temp;
+  const T nz = T(-2.0) * z.z * m_sqrt(x2 + y2);
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+}
+
+// cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45): the
+// 4-D state is always carried (the host sets has_w for this formula)
+template <class T>
+__device__ __forceinline__ void f_hypercomplex(V4<T> &z, T r, T &DE) {
+  DE = DE * T(2.0) * r;
+  const T nx = z.x * z.x - z.y * z.y - z.z * z.z - z.w * z.w;
+  const T ny = T(2.0) * z.x * z.y - T(2.0) * z.w * z.z;
+  const T nz = T(2.0) * z.x * z.z - T(2.0) * z.y * z.w;
+  const T nw = T(2.0) * z.x * z.w - T(2.0) * z.y * z.z;
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+  z.w = nw;
+}
+
 template <class T, bool W>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
                                                  const MbRot *rot) {
   switch (formula) {
     case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
     case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s, rot); break;
+    case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
+    case MBR_FORMULA_HYPERCOMPLEX: f_hypercomplex<T>(z, r, DE); break;
     default: f_menger<T, W>(z, DE, s); break;
   }
 }

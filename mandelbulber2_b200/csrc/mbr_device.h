@@ -71,7 +71,9 @@ struct DevScene {
   int32_t de_function;     // hybrid: enumDEFunctionType (1 linear, 2 log)
   int32_t de_analytic;     // non-hybrid: enumDEAnalyticFunction (1 linear, 2 log, 3 IFS)
   int32_t uniform_formula; // formula id when every iteration uses slot 0, else 0
-  int32_t has_w;           // initial w != 0 (4-D state needed)
+  int32_t has_w;           // initial w != 0 or a 4-D formula (4-D state needed)
+  int32_t generic;         // a slot's formula has no specialised FP32/FP64 form (reference-order iteration only)
+  int32_t pad1;
   double julia_c[3];
   double cmul[3];
   double w0;

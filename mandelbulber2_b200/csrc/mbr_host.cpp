@@ -35,11 +35,14 @@ struct FormulaMeta {
   double bailout;    // default bailout
   int analytic;      // enumDEAnalyticFunction
 };
-// cAbstractFractal metadata of the three formula classes
-// (fractal_mandelbulb.cpp:16-27, fractal_mandelbox.cpp:18-29, fractal_menger_sponge.cpp:17-28)
+// cAbstractFractal metadata of the formula classes (fractal_mandelbulb.cpp:16-27,
+// fractal_mandelbulb_power2.cpp:17-28, fractal_hypercomplex.cpp:17-28,
+// fractal_mandelbox.cpp:18-29, fractal_menger_sponge.cpp:17-28)
 bool formula_meta(int formula, FormulaMeta *m) {
   switch (formula) {
     case MBR_FORMULA_MANDELBULB: *m = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_MANDELBULB_POWER2: *m = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_HYPERCOMPLEX: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -306,6 +309,13 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   }
   d.w0 = sc.initial_waxis;
   d.has_w = sc.initial_waxis != 0.0;
+  for (int i = 0; i < n; i++) {
+    const int f = d.slot[i].formula;
+    if (f == MBR_FORMULA_HYPERCOMPLEX) d.has_w = 1;  // z.w evolves from w = 0
+    if (f != MBR_FORMULA_NONE && f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX &&
+        f != MBR_FORMULA_MENGER_SPONGE)
+      d.generic = 1;
+  }
   d.linear_de_offset = sc.linear_de_offset;
   d.flinear_de_offset = float(sc.linear_de_offset);
   *out = d;
@@ -713,7 +723,8 @@ mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_p
   const DevOutputs d = dev_outputs(ctx, *out);
   const bool fp32 = engine == MBR_ENGINE_PLAIN_MIXED || engine == MBR_ENGINE_WAVEFRONT_FP32;
   if (fp32 && ctx->scene.has_w)
-    return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need initial_waxis == 0");
+    return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need a 3-D state: initial_waxis == 0 and no hypercomplex "
+                                          "formula");
   int e;
   switch (engine) {
     case MBR_ENGINE_PLAIN_FP64: e = launch_plain_fp64(ctx->scene, fr, d, stream); break;

@@ -1728,8 +1728,10 @@ static long long job_items(const WJob &j, int layout) {
 }
 
 static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, bool batch) {
-  if (batch && (sc.is_hybrid || fr.gi_samples > 0))
-    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront batches: hybrid sequences and GI render one frame at a time");
+  if (batch && (sc.is_hybrid || sc.generic || fr.gi_samples > 0))
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "wavefront batches: hybrid sequences, formulas without a specialised form and GI render one frame "
+                   "at a time");
   if (sc.iter_thresh || sc.interior || sc.has_w)
     return set_err(ctx, MBR_EUNSUPPORTED,
                    "wavefront engine: iteration_threshold_mode, interior_mode and initial_waxis != 0 use the plain engines");
@@ -1866,12 +1868,14 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   if (!is_wavefront(engine)) return set_err(ctx, MBR_EINVAL, "not a wavefront engine: %d", engine);
   mbr_status stt = check_supported(ctx, sc, fr, false);
   if (stt != MBR_OK) return stt;
-  const bool gi = fr.gi_samples > 0, hyb = sc.is_hybrid != 0;
+  // hybrids and formulas without a specialised form iterate in the reference's order (PrecHyb)
+  const bool gi = fr.gi_samples > 0, hyb = sc.is_hybrid != 0 || sc.generic != 0;
   if (gi && fr.gi_bounces > 120)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: GI with more than 120 bounces uses the plain engines");
   if (hyb && engine == MBR_ENGINE_WAVEFRONT_FP64)
-    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: hybrid sequences iterate in FP32 (MBR_ENGINE_WAVEFRONT_FP32 "
-                                          "or _AUTO); FP64 hybrids use MBR_ENGINE_PLAIN_FP64");
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: hybrid sequences and formulas other than the Mandelbulb, "
+                                          "Mandelbox and Menger sponge iterate in FP32 (MBR_ENGINE_WAVEFRONT_FP32 or "
+                                          "_AUTO); in FP64 they use MBR_ENGINE_PLAIN_FP64");
   const mbr_tuning tu = ctx_tuning(ctx);
   const WJob j0 = make_job(fr, 0, out.pixel_offset);
   const long long pixels = (long long)fr.width * (fr.row1 - fr.row0);
@@ -2295,11 +2299,11 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
                                &msg);
   if (st != MBR_OK) return noalloc_fail(err, err_len, st, msg);
   fr.want_normal = out->normal != nullptr;
-  if (sc.is_hybrid || sc.iter_thresh || sc.interior || sc.has_w || fr.gi_samples > 0 ||
+  if (sc.is_hybrid || sc.generic || sc.iter_thresh || sc.interior || sc.has_w || fr.gi_samples > 0 ||
       fr.refine != MBR_REFINE_REFERENCE)
     return noalloc_fail(err, err_len, MBR_EUNSUPPORTED,
-                        "the wavefront engine renders non-hybrid scenes without GI, root refinement, "
-                        "iteration threshold, interior mode or initial w");
+                        "the wavefront engine renders non-hybrid Mandelbulb, Mandelbox and Menger scenes without GI, "
+                        "root refinement, iteration threshold, interior mode or initial w");
   const long long total = (long long)fr.width * (fr.row1 - fr.row0);  // row-linear queue: no tile padding
   const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
   const size_t need = scratch_bytes(total, per);

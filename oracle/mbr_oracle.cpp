@@ -51,6 +51,8 @@ struct FormulaInfo {
 static bool formula_info(int formula, FormulaInfo *fi) {
   switch (formula) {
     case MBR_FORMULA_MANDELBULB: *fi = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_MANDELBULB_POWER2: *fi = {2, 0, 10.0, 2}; return true;  // fractal_mandelbulb_power2.cpp:17-28
+    case MBR_FORMULA_HYPERCOMPLEX: *fi = {2, 0, 10.0, 2}; return true;      // fractal_hypercomplex.cpp:17-28
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -395,6 +397,36 @@ inline void formula_mandelbox(V4<S> &z, const SlotT<S> &f, S &DE) {
   DE = DE * fabs(f.mb_scale) + 1.0;
 }
 
+// cFractalMandelbulbPower2::FormulaCode (fractal_mandelbulb_power2.cpp:30-45)
+template <class S>
+inline void formula_bulb_pow2(V4<S> &z, const S &r, S &DE) {
+  DE = DE * 2.0 * r;
+  const S x2 = z.x * z.x;
+  const S y2 = z.y * z.y;
+  const S z2 = z.z * z.z;
+  const S temp = 1.0 - z2 / (x2 + y2);
+  const S nx = (x2 - y2) * temp;
+  const S ny = 2.0 * z.x * z.y * temp;
+  const S nz = -2.0 * z.z * sqrt(x2 + y2);
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+}
+
+// cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45)
+template <class S>
+inline void formula_hypercomplex(V4<S> &z, const S &r, S &DE) {
+  DE = DE * 2.0 * r;
+  const S nx = z.x * z.x - z.y * z.y - z.z * z.z - z.w * z.w;
+  const S ny = 2.0 * z.x * z.y - 2.0 * z.w * z.z;
+  const S nz = 2.0 * z.x * z.z - 2.0 * z.y * z.w;
+  const S nw = 2.0 * z.x * z.w - 2.0 * z.y * z.z;
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+  z.w = nw;
+}
+
 // cFractalMengerSponge::FormulaCode (fractal_menger_sponge.cpp:30-71)
 template <class S>
 inline void formula_menger(V4<S> &z, const SlotT<S> &f, S &DE) {
@@ -460,6 +492,8 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_MANDELBULB: formula_mandelbulb(z, f, r, DE); break;
         case MBR_FORMULA_MANDELBOX: formula_mandelbox(z, f, DE); break;
         case MBR_FORMULA_MENGER_SPONGE: formula_menger(z, f, DE); break;
+        case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(z, r, DE); break;
+        case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(z, r, DE); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
@@ -1319,6 +1353,8 @@ int oracle_formula_step(const mbr_scene *scene, int slot, double *z, double *r, 
     case MBR_FORMULA_MANDELBULB: formula_mandelbulb(v, f, *r, *de); break;
     case MBR_FORMULA_MANDELBOX: formula_mandelbox(v, f, *de); break;
     case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, *de); break;
+    case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, *r, *de); break;
+    case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, *r, *de); break;
     default: return 1;
   }
   z[0] = v.x; z[1] = v.y; z[2] = v.z; z[3] = v.w;
@@ -1391,6 +1427,8 @@ int oracle_opcount(const mbr_scene *scene, int slot, const double *z, uint64_t *
     case MBR_FORMULA_MANDELBULB: formula_mandelbulb(v, f, r, DE); break;
     case MBR_FORMULA_MANDELBOX: formula_mandelbox(v, f, DE); break;
     case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, DE); break;
+    case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, r, DE); break;
+    case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, r, DE); break;
     default: return 1;
   }
   // the per-iteration work of Compute around the formula: c-add and |z|

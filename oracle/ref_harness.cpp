@@ -59,6 +59,12 @@ int ref_formula_step(int formula, const double *params, double *z, double *aux_r
     f.mandelbox.mboxFactor1 = f.mandelbox.fR2 / f.mandelbox.mR2;
     static cFractalMandelbox fb;
     fb.FormulaCode(v, &f, aux);
+  } else if (formula == 3) {
+    static cFractalMandelbulbPower2 fp2;
+    fp2.FormulaCode(v, &f, aux);
+  } else if (formula == 4) {
+    static cFractalHypercomplex fh;
+    fh.FormulaCode(v, &f, aux);
   } else if (formula == 7) {
     f.transformCommon.scale3 = params[0];
     f.foldColor.auxColorEnabledFalse = false;

@@ -2,7 +2,8 @@
 sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
 
   formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
-                    Mandelbox with and without rotations, Menger sponge)
+                    Mandelbox with and without rotations, Menger sponge,
+                    Mandelbulb power 2, hypercomplex)
                     on seeded random points
   projection_kat.json  CalcFOV + CalculateViewVector of the fish-eye,
                     equirectangular and fish-eye-cut projections
@@ -42,6 +43,8 @@ FORMULAS = [
      {"mandelbox_scale": -2.2, "mandelbox_folding_limit": 0.9, "mandelbox_folding_value": 1.8,
       "mandelbox_folding_min_radius": 0.35, "mandelbox_folding_fixed_radius": 1.1}),
     ("menger_3", 7, [3.0], {"transf_scale3": 3.0}),
+    ("mandelbulb_power2", 3, [], {}),
+    ("hypercomplex", 4, [], {}),
 ]
 # Mandelbox with rotations (fractal_mandelbox.cpp:33-63, 103): the eight
 # parameters above, rotationsEnabled, mainRotationEnabled, the neg and pos

@@ -1,0 +1,79 @@
+"""Mandelbulb power 2 (formula 3) and hypercomplex (formula 4), the two
+formulas beyond the Mandelbulb, Mandelbox and Menger sponge.  They iterate in
+the reference's operation order (de_core.cuh), on the plain engines and, for
+the 3-D power-2 bulb, on the FP32 wavefront through the reference-order
+policy.  The oracle's steps equal the reference's FormulaCode bit for bit
+(tests/golden/formula_kat.json); both formulas use only +, -, *, / and sqrt,
+so the strict FP64 kernel is held to bit-exactness against the oracle.
+"""
+import numpy as np
+import pytest
+
+from mandelbulber2_b200 import abi, configs
+
+from .parity import compare
+
+pytestmark = pytest.mark.gpu
+NAMES = ("depth", "iters", "hit", "normal", "ao", "rgb8")
+
+
+def scene(formula):
+    sc = abi.scene_defaults(formula)
+    sc.formula_maxiter = 30
+    cam = configs.camera((0.3, -1.8, 0.6), width=96, height=64)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    return sc, cam, p
+
+
+def check(renderer, sc, cam, p, o, ost, engine, name):
+    fr = renderer.render(cam, p, engine, outputs=NAMES)
+    g = {k: v.cpu().numpy() for k, v in fr.buffers.items()}
+    m = compare(g, o)
+    print(name, abi.ENGINE_NAMES[engine], m)
+    if engine == abi.ENGINE_PLAIN_FP64_STRICT:
+        for k in NAMES:
+            assert np.array_equal(g[k], o[k]), (name, k)
+        assert fr.stats == ost
+    elif engine == abi.ENGINE_PLAIN_FP64:
+        assert m["hit_iters_match"] >= 0.999, m
+        assert m["depth_rel_le_1e-9"] >= 0.999, m
+    else:
+        assert m["hit_mismatch"] <= 0.005, m
+        assert m["depth_rel_median"] <= 1e-4, m
+
+
+def test_mandelbulb_power2(renderer, oracle):
+    sc, cam, p = scene(abi.FORMULA_MANDELBULB_POWER2)
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.1 < float(np.mean(o["hit"])) < 0.95
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED,
+                   abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
+        check(renderer, sc, cam, p, o, ost, engine, "power2")
+
+
+def test_hypercomplex(renderer, oracle):
+    from mandelbulber2_b200.render import MbrError
+
+    sc, cam, p = scene(abi.FORMULA_HYPERCOMPLEX)
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.1 < float(np.mean(o["hit"])) < 0.95
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64):
+        check(renderer, sc, cam, p, o, ost, engine, "hypercomplex")
+    # the 4-D state runs on the plain FP64 engines only
+    for engine in (abi.ENGINE_PLAIN_MIXED, abi.ENGINE_WAVEFRONT_FP32):
+        with pytest.raises(MbrError) as e:
+            renderer.render(cam, p, engine, outputs=NAMES)
+        assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+def test_generic_formulas_refused_where_not_built(renderer):
+    from mandelbulber2_b200.render import MbrError
+
+    sc, cam, p = scene(abi.FORMULA_MANDELBULB_POWER2)
+    renderer.set_scene(sc)
+    with pytest.raises(MbrError) as e:
+        renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP64, outputs=NAMES)
+    assert e.value.status == abi.MBR_EUNSUPPORTED
