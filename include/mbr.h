@@ -55,6 +55,7 @@ typedef enum mbr_formula {
   MBR_FORMULA_MANDELBULB = 2,   /* formula/definition/fractal_mandelbulb.cpp:29-43 */
   MBR_FORMULA_MANDELBULB_POWER2 = 3, /* formula/definition/fractal_mandelbulb_power2.cpp:30-45 */
   MBR_FORMULA_HYPERCOMPLEX = 4, /* formula/definition/fractal_hypercomplex.cpp:30-45; 4-D: plain FP64 engines */
+  MBR_FORMULA_KALEIDOSCOPIC_IFS = 10, /* formula/definition/fractal_kaleidoscopic_ifs.cpp:30-85 */
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
   MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
 } mbr_formula;
@@ -140,6 +141,24 @@ typedef struct mbr_fractal {
   double mandelbox_rotation_neg[3][3];      /* "mandelbox_rotation_neg_1..3" */
   double mandelbox_rotation_pos[3][3];      /* "mandelbox_rotation_pos_1..3" */
   double mandelbox_rotation_main[3];        /* "mandelbox_rotation_main" */
+  /* Kaleidoscopic IFS (formula 10): sFractalIFS (src/fractal.h:155-174),
+   * read as in src/fractal.cpp:96-115, 655-661.  Angles in degrees; a vector
+   * (x, y, z) is the rotation RotateZ(x) RotateY(y) RotateX(z).  Only in a
+   * scene that is not a hybrid. */
+  int32_t ifs_abs_x, ifs_abs_y, ifs_abs_z;   /* "IFS_abs_x/y/z", default 0 */
+  int32_t ifs_rotation_enabled;              /* default 0 */
+  int32_t ifs_edge_enabled;                  /* default 0 */
+  int32_t ifs_menger_sponge_mode;            /* default 0 */
+  int32_t ifs_enabled[9];                    /* "IFS_enabled_0..8", default 0 */
+  int32_t ifs_reserved;
+  double ifs_scale;                          /* default 2 */
+  double ifs_rotation[3];                    /* main rotation, default 0 */
+  double ifs_offset[3];                      /* default (1, 0, 0) */
+  double ifs_edge[3];                        /* default 0 */
+  double ifs_direction[9][3];                /* "IFS_direction_0..8", default (1, 0, 0) */
+  double ifs_rotations[9][3];                /* default 0 */
+  double ifs_distance[9];                    /* default 0 */
+  double ifs_intensity[9];                   /* default 1 */
 } mbr_fractal;
 
 /* The fractal part of a scene: one fractal (or hybrid) object node with the

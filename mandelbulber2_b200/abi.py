@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 
 # mbr_formula (fractal::enumFractalFormula)
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
-FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX = 3, 4
+FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS = 3, 4, 10
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
@@ -52,6 +52,12 @@ class Fractal(C.Structure):
         ("transf_scale3", C.c_double),
         ("mandelbox_rotations_enabled", C.c_int32), ("mandelbox_main_rotation_enabled", C.c_int32),
         ("mandelbox_rotation_neg", D3 * 3), ("mandelbox_rotation_pos", D3 * 3), ("mandelbox_rotation_main", D3),
+        ("ifs_abs_x", C.c_int32), ("ifs_abs_y", C.c_int32), ("ifs_abs_z", C.c_int32),
+        ("ifs_rotation_enabled", C.c_int32), ("ifs_edge_enabled", C.c_int32), ("ifs_menger_sponge_mode", C.c_int32),
+        ("ifs_enabled", C.c_int32 * 9), ("ifs_reserved", C.c_int32),
+        ("ifs_scale", C.c_double), ("ifs_rotation", D3), ("ifs_offset", D3), ("ifs_edge", D3),
+        ("ifs_direction", D3 * 9), ("ifs_rotations", D3 * 9), ("ifs_distance", C.c_double * 9),
+        ("ifs_intensity", C.c_double * 9),
     ]
 
 

@@ -228,14 +228,64 @@ __device__ __forceinline__ void f_hypercomplex(V4<T> &z, T r, T &DE) {
   z.w = nw;
 }
 
+// cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
+// over the enabled vectors of the scene's IFS block; the 4-vector terms with
+// w keep the reference's operations (its direction and offset have w = 0)
+template <class T>
+__device__ __forceinline__ void f_ifs(V4<T> &z, T &DE, const IfsBlock &b) {
+  if (b.abs_x) z.x = m_abs(z.x);
+  if (b.abs_y) z.y = m_abs(z.y);
+  if (b.abs_z) z.z = m_abs(z.z);
+  for (int k = 0; k < b.n; k++) {
+    if (!b.rot_zero[k]) z = mb_turn<T>(b.rot[k], false, z);
+    const T dx = T(b.dir[k][0]), dy = T(b.dir[k][1]), dz = T(b.dir[k][2]);
+    const T len = z.x * dx + z.y * dy + z.z * dz + z.w * T(0.0);
+    if (len < T(b.dist[k])) {
+      const T f = T(2.0) * (len - T(b.dist[k])) * T(b.inten[k]);
+      z.x = z.x - dx * f;
+      z.y = z.y - dy * f;
+      z.z = z.z - dz * f;
+      z.w = z.w - T(0.0) * f;
+    }
+  }
+  const T ox = T(b.offset[0]), oy = T(b.offset[1]), oz = T(b.offset[2]);
+  if (b.rot_on) {
+    V4<T> t{z.x - ox, z.y - oy, z.z - oz, z.w - T(0.0)};
+    if (!b.main_zero) t = mb_turn<T>(b.main, false, t);
+    z = V4<T>{t.x + ox, t.y + oy, t.z + oz, t.w + T(0.0)};
+  }
+  if (b.edge_on) {
+    if (b.edge[0] > 0.0) z.x = T(b.edge[0]) - m_abs(T(b.edge[0]) - z.x);
+    if (b.edge[1] > 0.0) z.y = T(b.edge[1]) - m_abs(T(b.edge[1]) - z.y);
+    if (b.edge[2] > 0.0) z.z = T(b.edge[2]) - m_abs(T(b.edge[2]) - z.z);
+  }
+  const T sc = T(b.scale);
+  z.x = z.x * sc;
+  z.y = z.y * sc;
+  z.z = z.z * sc;
+  z.w = z.w * sc;
+  if (b.menger) {
+    z.x = z.x - ox * (sc - T(1.0));
+    z.y = z.y - oy * (sc - T(1.0));
+    if (z.z > T(0.5) * oz * (sc - T(1.0))) z.z = z.z - oz * (sc - T(1.0));
+  } else {
+    z.x = z.x - ox * (sc - T(1.0));
+    z.y = z.y - oy * (sc - T(1.0));
+    z.z = z.z - oz * (sc - T(1.0));
+    z.w = z.w - T(0.0) * (sc - T(1.0));
+  }
+  DE = DE * m_abs(sc);
+}
+
 template <class T, bool W>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
-                                                 const MbRot *rot) {
+                                                 const MbRot *rot, const IfsBlock *ifs) {
   switch (formula) {
     case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
     case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s, rot); break;
     case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
     case MBR_FORMULA_HYPERCOMPLEX: f_hypercomplex<T>(z, r, DE); break;
+    case MBR_FORMULA_KALEIDOSCOPIC_IFS: f_ifs<T>(z, DE, *ifs); break;
     default: f_menger<T, W>(z, DE, s); break;
   }
 }
@@ -294,7 +344,7 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
       if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s, &sc.mbrot);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W>(s.formula, z, r, DE, s, &sc.mbrot);
+      formula_dispatch<T, W>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs);
     }
     if (s.add_c) {
       if (sc.julia) {

@@ -284,6 +284,49 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
     // rotation[0][k] = mandelbox_rotation_neg_(k+1), rotation[1][k] = ..._pos_(k+1) (fractal.cpp:69-73)
     double *dst = (name[19] == 'n' ? f.mandelbox_rotation_neg : f.mandelbox_rotation_pos)[name[23] - '1'];
     if (parse_vec3(value, v)) std::memcpy(dst, v, sizeof(v)); else R.bad(name, value);
+  } else if (starts_with(name, "IFS_")) {  // kaleidoscopic IFS (initparameters.cpp:724-743)
+    const std::string k = name.substr(4);
+    // indexed vector parameters: IFS_direction_0 .. IFS_enabled_8
+    int idx = -1;
+    std::string base = k;
+    const size_t u = k.rfind('_');
+    if (u != std::string::npos && u + 2 == k.size() && k[u + 1] >= '0' && k[u + 1] <= '8') {
+      idx = k[u + 1] - '0';
+      base = k.substr(0, u);
+    }
+    if (idx >= 0 && base == "direction") {
+      if (parse_vec3(value, v)) std::memcpy(f.ifs_direction[idx], v, sizeof(v)); else R.bad(name, value);
+    } else if (idx >= 0 && base == "rotations") {
+      if (parse_vec3(value, v)) std::memcpy(f.ifs_rotations[idx], v, sizeof(v)); else R.bad(name, value);
+    } else if (idx >= 0 && base == "distance") {
+      if (parse_double(value, d)) f.ifs_distance[idx] = d; else R.bad(name, value);
+    } else if (idx >= 0 && base == "intensity") {
+      if (parse_double(value, d)) f.ifs_intensity[idx] = d; else R.bad(name, value);
+    } else if (idx >= 0 && base == "enabled") {
+      if (parse_bool(value, b)) f.ifs_enabled[idx] = b; else R.bad(name, value);
+    } else if (k == "scale") {
+      if (parse_double(value, d)) f.ifs_scale = d; else R.bad(name, value);
+    } else if (k == "rotation") {
+      if (parse_vec3(value, v)) std::memcpy(f.ifs_rotation, v, sizeof(v)); else R.bad(name, value);
+    } else if (k == "rotation_enabled") {
+      if (parse_bool(value, b)) f.ifs_rotation_enabled = b; else R.bad(name, value);
+    } else if (k == "offset") {
+      if (parse_vec3(value, v)) std::memcpy(f.ifs_offset, v, sizeof(v)); else R.bad(name, value);
+    } else if (k == "edge") {
+      if (parse_vec3(value, v)) std::memcpy(f.ifs_edge, v, sizeof(v)); else R.bad(name, value);
+    } else if (k == "edge_enabled") {
+      if (parse_bool(value, b)) f.ifs_edge_enabled = b; else R.bad(name, value);
+    } else if (k == "abs_x") {
+      if (parse_bool(value, b)) f.ifs_abs_x = b; else R.bad(name, value);
+    } else if (k == "abs_y") {
+      if (parse_bool(value, b)) f.ifs_abs_y = b; else R.bad(name, value);
+    } else if (k == "abs_z") {
+      if (parse_bool(value, b)) f.ifs_abs_z = b; else R.bad(name, value);
+    } else if (k == "menger_sponge_mode") {
+      if (parse_bool(value, b)) f.ifs_menger_sponge_mode = b; else R.bad(name, value);
+    } else {
+      R.ignored.push_back("fractal_" + std::to_string(slot + 1) + "." + name);
+    }
   } else if (name == "formula_iterations") {
     if (parse_int(value, b)) f.formula_iterations = b; else R.bad(name, value);
   } else if (name == "formula_weight") {
@@ -631,10 +674,12 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     if (!R.hybrid && i > 0) break;
     if (f == MBR_FORMULA_NONE) continue;
     if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE &&
-        f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX)
+        f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
                               " (formula not built here: 2 Mandelbulb, 3 Mandelbulb power 2, 4 hypercomplex, "
-                              "7 Menger sponge, 8 Mandelbox are)");
+                              "7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS are)");
+    if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && R.hybrid)
+      R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in a hybrid)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
     if (f == MBR_FORMULA_MANDELBOX && R.hybrid &&
         (scene->fractal[i].mandelbox_rotations_enabled || scene->fractal[i].mandelbox_main_rotation_enabled))

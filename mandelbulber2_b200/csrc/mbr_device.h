@@ -59,6 +59,25 @@ struct MbRot {
   double mm[9];         // mainRot
 };
 
+// Kaleidoscopic IFS of slot 0 of a single-fractal scene (sFractalIFS,
+// fractal.h:155-174): the enabled vectors in order, with their rotation
+// matrices (SetRotation3), twice-normalised directions, distances and
+// intensities, built on the host (fractal.cpp:96-115, 655-661).
+struct IfsBlock {
+  int32_t abs_x, abs_y, abs_z, menger;
+  int32_t rot_on, edge_on, n, main_zero;
+  int32_t rot_zero[9];
+  int32_t pad;
+  double scale;
+  double offset[3];
+  double edge[3];
+  double main[9];       // mainRot, row-major
+  double rot[9][9];     // rot of the k-th enabled vector
+  double dir[9][3];
+  double dist[9];
+  double inten[9];
+};
+
 struct DevScene {
   int32_t n;
   int32_t is_hybrid;
@@ -84,6 +103,7 @@ struct DevScene {
   float pad0;
   DevSlot slot[MBR_MAX_FRACTALS];
   MbRot mbrot;             // zero (no rotations) unless slot 0 is a rotated Mandelbox
+  IfsBlock ifs;            // slot 0 of a kaleidoscopic IFS scene
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 

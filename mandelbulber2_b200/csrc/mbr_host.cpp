@@ -43,6 +43,7 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_MANDELBULB: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_MANDELBULB_POWER2: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_HYPERCOMPLEX: *m = {2, 0, 10.0, 2}; return true;
+    case MBR_FORMULA_KALEIDOSCOPIC_IFS: *m = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -93,12 +94,14 @@ mbr_status cuda_err(mbr_ctx *ctx, int code, const char *what) {
 // rotations about z, y and x by the vector's z, y and x angles, each
 // multiplied onto the right and skipped for a zero angle; *zero is set when
 // all three are zero (RotateVector then returns its argument unchanged).
-static void mandelbox_rotation(const double deg[3], double m[9], bool *zero) {
+// set3: CRotationMatrix::SetRotation3 instead (algebra.cpp:304-310):
+// rotations about z, y and x by the vector's x, y and z angles.
+static void mandelbox_rotation(const double deg[3], double m[9], bool *zero, bool set3 = false) {
   const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
   for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0 : 0.0;
   *zero = true;
   for (int axis = 2; axis >= 0; axis--) {
-    const double a = deg[axis] * k;
+    const double a = deg[set3 ? 2 - axis : axis] * k;
     if (a == 0.0) continue;
     const double sn = std::sin(a), cs = std::cos(a);
     double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -161,6 +164,47 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     }
     mandelbox_rotation(f.mandelbox_rotation_main, r.mm, &zero);
     r.main_zero = zero ? 1 : 0;
+  }
+  // kaleidoscopic IFS: slot 0 of a single-fractal scene
+  for (int i = 0; i < (hybrid ? n : 1); i++) {
+    const mbr_fractal &f = sc.fractal[i];
+    if (f.formula != MBR_FORMULA_KALEIDOSCOPIC_IFS) continue;
+    if (hybrid) return set_err(ctx, MBR_EUNSUPPORTED, "the kaleidoscopic IFS is supported in single-fractal scenes only");
+    IfsBlock &b = d.ifs;
+    b.abs_x = f.ifs_abs_x ? 1 : 0;
+    b.abs_y = f.ifs_abs_y ? 1 : 0;
+    b.abs_z = f.ifs_abs_z ? 1 : 0;
+    b.menger = f.ifs_menger_sponge_mode ? 1 : 0;
+    b.rot_on = f.ifs_rotation_enabled ? 1 : 0;
+    b.edge_on = f.ifs_edge_enabled ? 1 : 0;
+    b.scale = f.ifs_scale;
+    for (int k = 0; k < 3; k++) {
+      b.offset[k] = f.ifs_offset[k];
+      b.edge[k] = f.ifs_edge[k];
+    }
+    bool zero;
+    mandelbox_rotation(f.ifs_rotation, b.main, &zero, true);
+    b.main_zero = zero ? 1 : 0;
+    b.n = 0;
+    for (int v = 0; v < 9; v++) {
+      if (!f.ifs_enabled[v]) continue;
+      const int j = b.n++;
+      mandelbox_rotation(f.ifs_rotations[v], b.rot[j], &zero, true);
+      b.rot_zero[j] = zero ? 1 : 0;
+      // CVector4(direction, 0), normalised when read and again when derived (fractal.cpp:110-115, 660)
+      double x = f.ifs_direction[v][0], y = f.ifs_direction[v][1], z = f.ifs_direction[v][2];
+      for (int rep = 0; rep < 2; rep++) {
+        const double norm = 1.0 / std::sqrt(x * x + y * y + z * z + 0.0 * 0.0);
+        x = x * norm;
+        y = y * norm;
+        z = z * norm;
+      }
+      b.dir[j][0] = x;
+      b.dir[j][1] = y;
+      b.dir[j][2] = z;
+      b.dist[j] = f.ifs_distance[v];
+      b.inten[j] = f.ifs_intensity[v];
+    }
   }
   d.n = n;
   d.is_hybrid = hybrid ? 1 : 0;
@@ -617,6 +661,13 @@ void mbr_fractal_defaults(mbr_fractal *f, int formula) {
   f->mandelbox_folding_min_radius = 0.5;
   f->mandelbox_folding_fixed_radius = 1.0;
   f->transf_scale3 = 3.0;
+  // IFS (initparameters.cpp:724-743)
+  f->ifs_scale = 2.0;
+  f->ifs_offset[0] = 1.0;
+  for (int i = 0; i < 9; i++) {
+    f->ifs_direction[i][0] = 1.0;
+    f->ifs_intensity[i] = 1.0;
+  }
 }
 
 void mbr_scene_defaults(mbr_scene *s) {

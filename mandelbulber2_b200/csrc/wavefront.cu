@@ -463,7 +463,7 @@ struct PrecHyb {
     const V4<float> last = z;
     const float tempDE = e.dr;
     float de = e.dr;
-    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s, &sc.mbrot);
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs);
     if (s.add_c) {
       if (sc.julia) {
         z.x = z.x + juliac_of<float>(sc, 0);

@@ -53,6 +53,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_MANDELBULB: *fi = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_MANDELBULB_POWER2: *fi = {2, 0, 10.0, 2}; return true;  // fractal_mandelbulb_power2.cpp:17-28
     case MBR_FORMULA_HYPERCOMPLEX: *fi = {2, 0, 10.0, 2}; return true;      // fractal_hypercomplex.cpp:17-28
+    case MBR_FORMULA_KALEIDOSCOPIC_IFS: *fi = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -76,6 +77,7 @@ struct Slot {
   bool mb_rot = false, mb_main = false;       // rotationsEnabled, mainRotationEnabled
   double mb_rot_deg[2][3][3] = {};            // rotation[fold][axis]: neg (fold 0), pos (fold 1), degrees
   double mb_main_deg[3] = {0, 0, 0};          // rotationMain, degrees
+  mbr_fractal ifs = {};                       // the IFS_* parameters (fractal.cpp:96-115)
 };
 struct Seq {
   bool is_hybrid = false, julia = false;
@@ -142,6 +144,7 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
         sl.mb_rot_deg[1][a][k] = f.mandelbox_rotation_pos[a][k];
       }
     for (int k = 0; k < 3; k++) sl.mb_main_deg[k] = f.mandelbox_rotation_main[k];
+    sl.ifs = f;
   }
   if (hybrid && sc.use_default_bailout)
     for (int i = 0; i < n; i++) s.slot[i].bailout = maxBailout;  // :253-259
@@ -242,11 +245,12 @@ inline int sgn(double v) { return (0.0 < v) - (v < 0.0); }  // math_utilities.h:
 // algebra.cpp:296-302, 198-247): from the identity, RotateZ(z), RotateY(y),
 // RotateX(x), each post-multiplying the matrix and skipped for a zero angle;
 // `zero` stays set (RotateVector is the identity) when all three are zero.
-inline void mb_rotation(const double deg[3], double m[9], bool *zero) {
+// set3: SetRotation3 instead (algebra.cpp:304-310): RotateZ(x), RotateY(y), RotateX(z).
+inline void mb_rotation(const double deg[3], double m[9], bool *zero, bool set3 = false) {
   const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
   for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0 : 0.0;
   *zero = true;
-  const double ang[3] = {deg[2] * k, deg[1] * k, deg[0] * k};
+  const double ang[3] = {deg[set3 ? 0 : 2] * k, deg[1] * k, deg[set3 ? 2 : 0] * k};
   const int axis[3] = {2, 1, 0};
   for (int j = 0; j < 3; j++) {
     const double a = ang[j];
@@ -277,6 +281,9 @@ struct SlotT {
   bool mb_rz[2][3];       // rot[fold][axis].zero
   double mb_mm[9];        // mainRot
   bool mb_mz;             // mainRot.zero
+  // kaleidoscopic IFS (sFractalIFS after RecalculateFractalParams, fractal.cpp:655-661)
+  bool ifs_abs[3], ifs_enabled[9], ifs_menger, ifs_rot_on, ifs_edge_on, ifs_main_zero, ifs_rot_zero[9];
+  double ifs_scale, ifs_offset[3], ifs_edge[3], ifs_main[9], ifs_rot[9][9], ifs_dir[9][3], ifs_dist[9], ifs_int[9];
 };
 enum { TAN_POWER = 0, TAN_SCALE = 1, TAN_MR2 = 2, TAN_X = 3, TAN_Y = 4, TAN_Z = 5 };
 
@@ -311,6 +318,32 @@ SlotT<S> make_slot(const Slot &s, bool tangents) {
   for (int f = 0; f < 2; f++)
     for (int a = 0; a < 3; a++) mb_rotation(s.mb_rot_deg[f][a], t.mb_rm[f][a], &t.mb_rz[f][a]);
   mb_rotation(s.mb_main_deg, t.mb_mm, &t.mb_mz);
+  const mbr_fractal &f = s.ifs;
+  t.ifs_abs[0] = f.ifs_abs_x != 0;
+  t.ifs_abs[1] = f.ifs_abs_y != 0;
+  t.ifs_abs[2] = f.ifs_abs_z != 0;
+  t.ifs_menger = f.ifs_menger_sponge_mode != 0;
+  t.ifs_rot_on = f.ifs_rotation_enabled != 0;
+  t.ifs_edge_on = f.ifs_edge_enabled != 0;
+  t.ifs_scale = f.ifs_scale;
+  for (int k = 0; k < 3; k++) {
+    t.ifs_offset[k] = f.ifs_offset[k];
+    t.ifs_edge[k] = f.ifs_edge[k];
+  }
+  mb_rotation(f.ifs_rotation, t.ifs_main, &t.ifs_main_zero, true);
+  for (int i = 0; i < 9; i++) {
+    t.ifs_enabled[i] = f.ifs_enabled[i] != 0;
+    mb_rotation(f.ifs_rotations[i], t.ifs_rot[i], &t.ifs_rot_zero[i], true);
+    // CVector4(direction, 0).Normalize() when read and again in RecalculateFractalParams
+    double d[4] = {f.ifs_direction[i][0], f.ifs_direction[i][1], f.ifs_direction[i][2], 0.0};
+    for (int rep = 0; rep < 2; rep++) {
+      const double norm = 1.0 / sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3]);
+      for (int c = 0; c < 4; c++) d[c] = d[c] * norm;
+    }
+    for (int c = 0; c < 3; c++) t.ifs_dir[i][c] = d[c];
+    t.ifs_dist[i] = f.ifs_distance[i];
+    t.ifs_int[i] = f.ifs_intensity[i];
+  }
   return t;
 }
 
@@ -427,6 +460,54 @@ inline void formula_hypercomplex(V4<S> &z, const S &r, S &DE) {
   z.w = nw;
 }
 
+// cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
+template <class S>
+inline void formula_ifs(V4<S> &z, const SlotT<S> &f, S &DE) {
+  if (f.ifs_abs[0]) z.x = fabs(z.x);
+  if (f.ifs_abs[1]) z.y = fabs(z.y);
+  if (f.ifs_abs[2]) z.z = fabs(z.z);
+  for (int i = 0; i < 9; i++) {
+    if (!f.ifs_enabled[i]) continue;
+    z = mb_turn(f.ifs_rot[i], f.ifs_rot_zero[i], false, z);
+    const double *d = f.ifs_dir[i];
+    const S length = z.x * d[0] + z.y * d[1] + z.z * d[2] + z.w * 0.0;  // CVector4::Dot, direction w = 0
+    if (length < f.ifs_dist[i]) {
+      const S k = 2.0 * (length - f.ifs_dist[i]) * f.ifs_int[i];
+      z.x = z.x - d[0] * k;
+      z.y = z.y - d[1] * k;
+      z.z = z.z - d[2] * k;
+      z.w = z.w - 0.0 * k;
+    }
+  }
+  const double *o = f.ifs_offset;
+  if (f.ifs_rot_on) {
+    V4<S> t{z.x - o[0], z.y - o[1], z.z - o[2], z.w - 0.0};
+    t = mb_turn(f.ifs_main, f.ifs_main_zero, false, t);
+    z = V4<S>{t.x + o[0], t.y + o[1], t.z + o[2], t.w + 0.0};
+  }
+  if (f.ifs_edge_on) {
+    if (f.ifs_edge[0] > 0.0) z.x = f.ifs_edge[0] - fabs(f.ifs_edge[0] - z.x);
+    if (f.ifs_edge[1] > 0.0) z.y = f.ifs_edge[1] - fabs(f.ifs_edge[1] - z.y);
+    if (f.ifs_edge[2] > 0.0) z.z = f.ifs_edge[2] - fabs(f.ifs_edge[2] - z.z);
+  }
+  const double sc = f.ifs_scale;
+  z.x = z.x * sc;
+  z.y = z.y * sc;
+  z.z = z.z * sc;
+  z.w = z.w * sc;
+  if (f.ifs_menger) {
+    z.x = z.x - o[0] * (sc - 1.0);
+    z.y = z.y - o[1] * (sc - 1.0);
+    if (z.z > 0.5 * o[2] * (sc - 1.0)) z.z = z.z - o[2] * (sc - 1.0);
+  } else {
+    z.x = z.x - o[0] * (sc - 1.0);
+    z.y = z.y - o[1] * (sc - 1.0);
+    z.z = z.z - o[2] * (sc - 1.0);
+    z.w = z.w - 0.0 * (sc - 1.0);
+  }
+  DE = DE * fabs(sc);
+}
+
 // cFractalMengerSponge::FormulaCode (fractal_menger_sponge.cpp:30-71)
 template <class S>
 inline void formula_menger(V4<S> &z, const SlotT<S> &f, S &DE) {
@@ -494,6 +575,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_MENGER_SPONGE: formula_menger(z, f, DE); break;
         case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(z, r, DE); break;
         case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(z, r, DE); break;
+        case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(z, f, DE); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
@@ -1355,6 +1437,7 @@ int oracle_formula_step(const mbr_scene *scene, int slot, double *z, double *r, 
     case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, *de); break;
     case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, *r, *de); break;
     case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, *r, *de); break;
+    case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(v, f, *de); break;
     default: return 1;
   }
   z[0] = v.x; z[1] = v.y; z[2] = v.z; z[3] = v.w;
@@ -1429,6 +1512,7 @@ int oracle_opcount(const mbr_scene *scene, int slot, const double *z, uint64_t *
     case MBR_FORMULA_MENGER_SPONGE: formula_menger(v, f, DE); break;
     case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, r, DE); break;
     case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, r, DE); break;
+    case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(v, f, DE); break;
     default: return 1;
   }
   // the per-iteration work of Compute around the formula: c-add and |z|

@@ -194,6 +194,7 @@ class Reference:
         L.ref_calc_fov.restype = C.c_double
         L.ref_calc_fov.argtypes = [C.c_double]
         L.ref_mandelbox_rot_step.argtypes = [_P, _P, _P, _P, C.c_int]
+        L.ref_ifs_step.argtypes = [_P, _P, _P, _P, C.c_int]
         L.ref_view_vector_p.argtypes = [_P, _P, _P, C.c_double, C.c_int, C.c_double, C.c_double, _P]
         L.ref_calc_fov_p.restype = C.c_double
         L.ref_calc_fov_p.argtypes = [C.c_double, C.c_int]
@@ -219,6 +220,15 @@ class Reference:
         rr, dd = C.c_double(r), C.c_double(de)
         if self.lib.ref_mandelbox_rot_step(p.ctypes.data, zz.ctypes.data, C.addressof(rr), C.addressof(dd), i) != 0:
             raise RuntimeError("ref_mandelbox_rot_step failed")
+        return zz, rr.value, dd.value
+
+    def ifs_step(self, params, z, r: float, de: float, i: int = 0):
+        p = np.array(params, dtype=np.float64)
+        assert p.size == 97
+        zz = np.array(z, dtype=np.float64)
+        rr, dd = C.c_double(r), C.c_double(de)
+        if self.lib.ref_ifs_step(p.ctypes.data, zz.ctypes.data, C.addressof(rr), C.addressof(dd), i) != 0:
+            raise RuntimeError("ref_ifs_step failed")
         return zz, rr.value, dd.value
 
     def camera(self, cam, target, top):

@@ -82,6 +82,57 @@ int ref_formula_step(int formula, const double *params, double *z, double *aux_r
   return 0;
 }
 
+// One cFractalKaleidoscopicIfs::FormulaCode step.  params (97 values):
+// scale, rotationEnabled, rotation (3, degrees), offset (3), edgeEnabled,
+// edge (3), absX, absY, absZ, mengerSpongeMode, then for each of the nine
+// vectors: enabled, direction (3), rotations (3, degrees), distance,
+// intensity.  Directions and matrices are derived as sFractal's constructor
+// and RecalculateFractalParams derive them (fractal.cpp:96-115, 655-661).
+int ref_ifs_step(const double *params, double *z, double *aux_r, double *aux_de, int iter) {
+  sFractal &f = g_fractal;
+  sExtendedAux aux;
+  std::memset(&aux, 0, sizeof(aux));
+  aux.r = *aux_r;
+  aux.DE = *aux_de;
+  aux.i = iter;
+  aux.color = 1.0;
+  CVector4 v(z[0], z[1], z[2], z[3]);
+  sFractalIFS &I = f.IFS;
+  I.scale = params[0];
+  I.rotationEnabled = params[1] != 0.0;
+  I.rotation = CVector3(params[2], params[3], params[4]);
+  I.offset = CVector4(CVector3(params[5], params[6], params[7]), 0.0);
+  I.edgeEnabled = params[8] != 0.0;
+  I.edge = CVector3(params[9], params[10], params[11]);
+  I.absX = params[12] != 0.0;
+  I.absY = params[13] != 0.0;
+  I.absZ = params[14] != 0.0;
+  I.mengerSpongeMode = params[15] != 0.0;
+  for (int i = 0; i < IFS_VECTOR_COUNT; i++) {
+    const double *q = params + 16 + 9 * i;
+    I.enabled[i] = q[0] != 0.0;
+    I.direction[i] = CVector4(CVector3(q[1], q[2], q[3]), 0.0);
+    I.rotations[i] = CVector3(q[4], q[5], q[6]);
+    I.distance[i] = q[7];
+    I.intensity[i] = q[8];
+    I.direction[i].Normalize();
+  }
+  I.mainRot.SetRotation3(I.rotation * M_PI_180);
+  for (int i = 0; i < IFS_VECTOR_COUNT; i++) {
+    I.rot[i].SetRotation3(I.rotations[i] * M_PI_180);
+    I.direction[i].Normalize();
+  }
+  static cFractalKaleidoscopicIfs fk;
+  fk.FormulaCode(v, &f, aux);
+  z[0] = v.x;
+  z[1] = v.y;
+  z[2] = v.z;
+  z[3] = v.w;
+  *aux_r = aux.r;
+  *aux_de = aux.DE;
+  return 0;
+}
+
 // One cFractalMandelbox::FormulaCode step with rotations.  params: the eight
 // Mandelbox parameters of ref_formula_step, then rotationsEnabled,
 // mainRotationEnabled, rotation[0][0..2] (mandelbox_rotation_neg_1..3, 9

@@ -3,7 +3,7 @@ sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
 
   formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
                     Mandelbox with and without rotations, Menger sponge,
-                    Mandelbulb power 2, hypercomplex)
+                    Mandelbulb power 2, hypercomplex, kaleidoscopic IFS)
                     on seeded random points
   projection_kat.json  CalcFOV + CalculateViewVector of the fish-eye,
                     equirectangular and fish-eye-cut projections
@@ -70,6 +70,36 @@ N_POINTS = 32
 N_STEPS = 6
 
 
+# Kaleidoscopic IFS: (name, ref_ifs_step parameters, scene fields)
+def _ifs(scale, rot_on, rotation, offset, edge_on, edge, absxyz, menger, vectors):
+    p = [scale, rot_on] + rotation + offset + [edge_on] + edge + absxyz + [menger]
+    fields = {"ifs_scale": scale, "ifs_rotation_enabled": rot_on, "ifs_rotation": rotation, "ifs_offset": offset,
+              "ifs_edge_enabled": edge_on, "ifs_edge": edge, "ifs_abs_x": absxyz[0], "ifs_abs_y": absxyz[1],
+              "ifs_abs_z": absxyz[2], "ifs_menger_sponge_mode": menger, "ifs_enabled": [0] * 9,
+              "ifs_direction": [[1.0, 0.0, 0.0] for _ in range(9)], "ifs_rotations": [[0.0] * 3 for _ in range(9)],
+              "ifs_distance": [0.0] * 9, "ifs_intensity": [1.0] * 9}
+    for i in range(9):
+        en, d, r, dist, inten = vectors.get(i, (0, [1.0, 0.0, 0.0], [0.0, 0.0, 0.0], 0.0, 1.0))
+        p += [en] + d + r + [dist, inten]
+        fields["ifs_enabled"][i] = en
+        fields["ifs_direction"][i] = d
+        fields["ifs_rotations"][i] = r
+        fields["ifs_distance"][i] = dist
+        fields["ifs_intensity"][i] = inten
+    return p, fields
+
+
+IFS_FORMULAS = [
+    ("ifs_menger_mode", *_ifs(3.0, 0, [0.0, 0.0, 0.0], [1.0, 1.0, 1.0], 0, [0.0] * 3, [1, 1, 1], 1,
+                              {0: (1, [1.0, -1.0, 0.0], [0.0, 0.0, 0.0], 0.0, 1.0),
+                               1: (1, [0.0, 1.0, -1.0], [0.0, 0.0, 0.0], 0.0, 1.0),
+                               2: (1, [1.0, 0.0, -1.0], [0.0, 0.0, 0.0], 0.0, 1.0)})),
+    ("ifs_rotated_edges", *_ifs(2.2, 1, [45.0, 0.0, 12.0], [1.0, 0.5, 0.3], 1, [0.8, 0.0, 0.6], [1, 0, 1], 0,
+                                {3: (1, [0.0, 0.71, -0.71], [10.0, -5.0, 20.0], 0.1, 0.9),
+                                 7: (1, [1.0, 1.0, 1.0], [0.0, 30.0, 0.0], -0.2, 1.0)})),
+]
+
+
 def hexs(a):
     return [float(x).hex() for x in np.asarray(a, dtype=np.float64).ravel()]
 
@@ -77,7 +107,8 @@ def hexs(a):
 def formula_kats(ref: Reference) -> dict:
     rng = np.random.default_rng(20241203)
     out = {}
-    entries = [(n, f, p, fl, False) for n, f, p, fl in FORMULAS] + [(n, 8, p, fl, True) for n, p, fl in ROT_FORMULAS]
+    entries = ([(n, f, p, fl, False) for n, f, p, fl in FORMULAS] + [(n, 8, p, fl, True) for n, p, fl in ROT_FORMULAS]
+               + [(n, 10, p, fl, "ifs") for n, p, fl in IFS_FORMULAS])
     for name, fid, params, fields, rot in entries:
         cases = []
         for _ in range(N_POINTS):
@@ -88,7 +119,9 @@ def formula_kats(ref: Reference) -> dict:
             steps = []
             for i in range(N_STEPS):
                 zin, rin, dein = z.copy(), r, de
-                if rot:
+                if rot == "ifs":
+                    z, _, de = ref.ifs_step(params, z, r, de, i)
+                elif rot:
                     z, _, de = ref.mandelbox_rot_step(params, z, r, de, i)
                 else:
                     z, _, de = ref.formula_step(fid, params, z, r, de, i)

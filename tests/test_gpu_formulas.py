@@ -1,10 +1,12 @@
-"""Mandelbulb power 2 (formula 3) and hypercomplex (formula 4), the two
-formulas beyond the Mandelbulb, Mandelbox and Menger sponge.  They iterate in
+"""Mandelbulb power 2 (formula 3), hypercomplex (formula 4) and the
+kaleidoscopic IFS (formula 10), the formulas beyond the Mandelbulb, Mandelbox
+and Menger sponge.  They iterate in
 the reference's operation order (de_core.cuh), on the plain engines and, for
-the 3-D power-2 bulb, on the FP32 wavefront through the reference-order
-policy.  The oracle's steps equal the reference's FormulaCode bit for bit
-(tests/golden/formula_kat.json); both formulas use only +, -, *, / and sqrt,
-so the strict FP64 kernel is held to bit-exactness against the oracle.
+the 3-D ones, on the FP32 wavefront through the reference-order policy.  The
+oracle's steps equal the reference's FormulaCode bit for bit
+(tests/golden/formula_kat.json); the formulas use only +, -, *, /, sqrt and
+fabs (the IFS matrices are built on the host), so the strict FP64 kernel is
+held to bit-exactness against the oracle.
 """
 import numpy as np
 import pytest
@@ -77,3 +79,32 @@ def test_generic_formulas_refused_where_not_built(renderer):
     with pytest.raises(MbrError) as e:
         renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP64, outputs=NAMES)
     assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+def ifs_scene():
+    sc = abi.scene_defaults(abi.FORMULA_KALEIDOSCOPIC_IFS)
+    f = sc.fractal[0]
+    f.ifs_scale = 3.0
+    f.ifs_offset[:] = [1.0, 1.0, 1.0]
+    f.ifs_menger_sponge_mode = 1
+    f.ifs_abs_x = f.ifs_abs_y = f.ifs_abs_z = 1
+    for i, d in ((5, [1.0, -1.0, 0.0]), (6, [1.0, 0.0, -1.0]), (7, [0.39, 1.0, -1.0])):
+        f.ifs_enabled[i] = 1
+        f.ifs_direction[i][:] = d
+    f.ifs_rotation_enabled = 1
+    f.ifs_rotation[:] = [20.0, 0.0, 10.0]
+    sc.formula_maxiter = 20
+    cam = configs.camera((1.2, -2.2, 1.5), width=96, height=64)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    return sc, cam, p
+
+
+def test_kaleidoscopic_ifs(renderer, oracle):
+    sc, cam, p = ifs_scene()
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.1 < float(np.mean(o["hit"])) < 0.95
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED,
+                   abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
+        check(renderer, sc, cam, p, o, ost, engine, "ifs")
