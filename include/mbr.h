@@ -209,6 +209,11 @@ typedef struct mbr_camera {
   int32_t use_angles;
   int32_t perspective_type; /* mbr_projection, default three-point */
   double angles[3];      /* yaw, pitch, roll (radians) when use_angles != 0 */
+  /* "legacy_coordinate_system": the image region runs from y = -0.5 at the
+   * top row to +0.5 at the bottom instead of +0.5 to -0.5
+   * (cRenderJob::PrepareData, src/render_job.cpp:308-315); default 0 */
+  int32_t legacy_coordinate_system;
+  int32_t reserved1;
 } mbr_camera;
 
 typedef struct mbr_render_params {

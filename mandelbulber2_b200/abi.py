@@ -76,6 +76,7 @@ class Camera(C.Structure):
     _fields_ = [
         ("camera", D3), ("target", D3), ("top", D3), ("fov_deg", C.c_double), ("width", C.c_int32),
         ("height", C.c_int32), ("use_angles", C.c_int32), ("perspective_type", C.c_int32), ("angles", D3),
+        ("legacy_coordinate_system", C.c_int32), ("reserved1", C.c_int32),
     ]
 
 

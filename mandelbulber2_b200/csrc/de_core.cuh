@@ -109,13 +109,15 @@ __device__ __forceinline__ T &v4_axis(V4<T> &v, int dim) {
   return dim == 0 ? v.x : (dim == 1 ? v.y : v.z);
 }
 
-// rot: the scene's Mandelbox rotations (nullptr or zero flags: none)
-template <class T, bool W>
-__device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s, const MbRot *rot) {
+// ROT: the rotation code is compiled in (rot: the scene's rotations; zero
+// flags: none); kernels of scenes without rotations are built without it, so
+// its registers do not lower their occupancy
+template <class T, bool W, bool ROT = false>
+__device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s, const MbRot *rot = nullptr) {
   // box fold; the host requires folding_limit >= 0, so |z| > limit implies
   // z != 0 and copysign(value, z) equals sign(z) * value exactly
   const T limit = P<T>(s, P_MB_LIMIT), value = P<T>(s, P_MB_VALUE);
-  if (rot && rot->folds) {
+  if (ROT && rot->folds) {
     // each axis folded in the frame of rot[0][dim] above the limit, else of
     // rot[1][dim] below minus the limit, then turned back
     // (fractal_mandelbox.cpp:33-63)
@@ -167,7 +169,7 @@ __device__ __forceinline__ void f_mandelbox(V4<T> &z, T &DE, const DevSlot &s, c
     z.y = z.y - P<T>(s, P_MB_OFF_Y);
     z.z = z.z - P<T>(s, P_MB_OFF_Z);
   }
-  if (rot && rot->main && !rot->main_zero) z = mb_turn<T>(rot->mm, false, z);  // :103
+  if (ROT && rot->main && !rot->main_zero) z = mb_turn<T>(rot->mm, false, z);  // :103
   const T scale = P<T>(s, P_MB_SCALE);
   z.x = z.x * scale;
   z.y = z.y * scale;
@@ -277,16 +279,27 @@ __device__ __forceinline__ void f_ifs(V4<T> &z, T &DE, const IfsBlock &b) {
   DE = DE * m_abs(sc);
 }
 
-template <class T, bool W>
+// EXT: the formulas beyond the three specialised ones and the Mandelbox
+// rotations are compiled in; kernels of scenes that use none of them (hybrids
+// of the three included) are built without that code.
+template <class T, bool W, bool EXT = false>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
                                                  const MbRot *rot, const IfsBlock *ifs) {
-  switch (formula) {
-    case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
-    case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s, rot); break;
-    case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
-    case MBR_FORMULA_HYPERCOMPLEX: f_hypercomplex<T>(z, r, DE); break;
-    case MBR_FORMULA_KALEIDOSCOPIC_IFS: f_ifs<T>(z, DE, *ifs); break;
-    default: f_menger<T, W>(z, DE, s); break;
+  if constexpr (EXT) {
+    switch (formula) {
+      case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
+      case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W, true>(z, DE, s, rot); break;
+      case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
+      case MBR_FORMULA_HYPERCOMPLEX: f_hypercomplex<T>(z, r, DE); break;
+      case MBR_FORMULA_KALEIDOSCOPIC_IFS: f_ifs<T>(z, DE, *ifs); break;
+      default: f_menger<T, W>(z, DE, s); break;
+    }
+  } else {
+    switch (formula) {
+      case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
+      case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W>(z, DE, s); break;
+      default: f_menger<T, W>(z, DE, s); break;
+    }
   }
 }
 
@@ -320,7 +333,9 @@ __device__ __forceinline__ T juliac_of(const DevScene &sc, int k) {
 }
 
 // Compute<calcModeNormal> + CalculateDistanceSimple (analytic branch).
-// F: fixed formula id (non-hybrid scene) or 0 (generic).  W: 4-D state.
+// F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
+// the three specialised formulas) or F_EXT (generic with every formula and
+// the Mandelbox rotations).  W: 4-D state.
 template <class T, int F, bool W>
 __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
                                            int *iters_out) {
@@ -335,16 +350,16 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
   int i;
   for (i = 0; i < maxN; i++) {
     lastZ = z;
-    const int k = (F != 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]));
+    const int k = (F > 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]));
     const DevSlot &s = sc.slot[k];
     const V4<T> tempZ = z;
     const T tempDE = DE;
-    if (F != 0) {
+    if (F > 0) {
       if (F == MBR_FORMULA_MANDELBULB) f_mandelbulb<T>(z, r, DE, s);
-      if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s, &sc.mbrot);
+      if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs);
+      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs);
     }
     if (s.add_c) {
       if (sc.julia) {
@@ -358,7 +373,7 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
         if (W) z.w = z.w + c.w;
       }
     }
-    if (F == 0 && sc.is_hybrid) {
+    if (F <= 0 && sc.is_hybrid) {
       const double kw = s.d[P_WEIGHT];
       if (kw < 1.0) {
         z = smooth4<T, W>(tempZ, z, kw);
@@ -381,7 +396,7 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
   T distance;
   if (DE > T(0.0)) {
     // 1 linear r/DE, 2 log, 3 IFS, 4 hybrid linear with offset
-    const int fn = (F == 0 && sc.is_hybrid) ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
+    const int fn = (F <= 0 && sc.is_hybrid) ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
     if (fn == 4) {
       distance = (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
     } else if (fn == 2) {

@@ -474,7 +474,7 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     else if (value == "fish_eye_cut" || value == "3") cam->perspective_type = MBR_PROJECTION_FISH_EYE_CUT;
     else R.bad(name, value);
   } else if (name == "legacy_coordinate_system") {
-    if (parse_bool(value, b) && b) R.unsupported.push_back(name + " (camera axes)");
+    if (parse_bool(value, b)) cam->legacy_coordinate_system = b; else R.bad(name, value);
   } else if (name == "camera_rotation" || name == "camera_distance_to_target") {
     // derived from camera, target and top by the reference itself
   // raymarching quality

@@ -78,6 +78,14 @@ struct IfsBlock {
   double inten[9];
 };
 
+// The F template value of the generic iteration that carries every formula
+// and the Mandelbox rotations (de_core.cuh calc_distance).
+constexpr int F_EXT = -1;
+
+// Whether a scene needs that iteration.
+struct DevScene;
+__host__ __device__ inline bool scene_extended(const DevScene &sc);
+
 struct DevScene {
   int32_t n;
   int32_t is_hybrid;
@@ -106,6 +114,10 @@ struct DevScene {
   IfsBlock ifs;            // slot 0 of a kaleidoscopic IFS scene
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
+
+__host__ __device__ inline bool scene_extended(const DevScene &sc) {
+  return sc.generic || sc.mbrot.folds || sc.mbrot.main;
+}
 
 // Everything about one frame that is not the scene: camera, march and
 // shading parameters, derived on the host.
@@ -144,6 +156,7 @@ struct DevFrame {
   uint32_t gi_seed;
   int32_t want_normal;
   int32_t persp;       // mbr_projection
+  int32_t legacy_y;    // legacy coordinate system: image y runs -0.5 (top) to +0.5
   double gi_sky;
   double gi_sun;
   double dof_aperture;

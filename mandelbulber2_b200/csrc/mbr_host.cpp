@@ -491,6 +491,7 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.seed = p.seed;
   // CalcFOV (projection_3d.cpp:140-159)
   f.persp = cam.perspective_type;
+  f.legacy_y = cam.legacy_coordinate_system ? 1 : 0;
   f.fov = cam.perspective_type == MBR_PROJECTION_THREE_POINT ? 2.0 * std::tan(cam.fov_deg / 360.0 * kPi)
                                                               : cam.fov_deg / 180.0 * kPi;
   f.resolution = 1.0 / cam.height;

@@ -112,11 +112,14 @@ __device__ __forceinline__ D3 rotate(const DevFrame &fr, D3 v) {  // CRotationMa
   return {m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
           m[6] * v.x + m[7] * v.y + m[8] * v.z};
 }
+// cRegion::transpose from the screen to the image region (region.hpp:66-71):
+// (-0.5, 0.5, 0.5, -0.5), or (-0.5, -0.5, 0.5, 0.5) in the legacy coordinate
+// system (render_job.cpp:308-315)
 __device__ __forceinline__ void image_point(const DevFrame &fr, double x, double y, double *ix, double *iy) {
   const double scaleX = 1.0 / double(fr.width);
-  const double scaleY = -1.0 / double(fr.height);
+  const double scaleY = (fr.legacy_y ? 1.0 : -1.0) / double(fr.height);
   *ix = (scaleX * x + -0.5) * fr.aspect;
-  *iy = scaleY * y + 0.5;
+  *iy = scaleY * y + (fr.legacy_y ? -0.5 : 0.5);
 }
 // CalculateViewVector (projection_3d.cpp:40-89) before the camera rotation:
 // the view vector of image point (ix, iy) (aspect applied), with fov from

@@ -223,10 +223,17 @@ int launch_plain_t(const DevScene &sc, const DevFrame &fr, const DevOutputs &out
   const dim3 block(128);
   const dim3 grid((fr.width + 15) / 16, (fr.row1 - fr.row0 + 7) / 8);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool ext = scene_extended(sc);
   const int F = sc.is_hybrid ? 0 : sc.uniform_formula;
   if (sc.has_w) {
-    if constexpr (sizeof(T) == 8) plain_kernel<T, R, 0, true, V><<<grid, block, 0, s>>>(sc, fr, out);
-    else return int(cudaErrorInvalidValue);
+    if constexpr (sizeof(T) == 8) {
+      if (ext) plain_kernel<T, R, F_EXT, true, V><<<grid, block, 0, s>>>(sc, fr, out);
+      else plain_kernel<T, R, 0, true, V><<<grid, block, 0, s>>>(sc, fr, out);
+    } else {
+      return int(cudaErrorInvalidValue);
+    }
+  } else if (ext) {
+    plain_kernel<T, R, F_EXT, false, V><<<grid, block, 0, s>>>(sc, fr, out);
   } else {
     switch (F) {
       case MBR_FORMULA_MANDELBULB: plain_kernel<T, R, MBR_FORMULA_MANDELBULB, false, V><<<grid, block, 0, s>>>(sc, fr, out); break;
@@ -245,9 +252,16 @@ int launch_distance_t(const DevScene &sc, const double *pts, int64_t n, double d
   const dim3 block(128);
   const dim3 grid(unsigned((n + 127) / 128));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool ext = scene_extended(sc);
   if (sc.has_w) {
-    if constexpr (sizeof(T) == 8) distance_kernel<T, 0, true, V><<<grid, block, 0, s>>>(sc, pts, n, detail, normal_mode, dist, iters);
-    else return int(cudaErrorInvalidValue);
+    if constexpr (sizeof(T) == 8) {
+      if (ext) distance_kernel<T, F_EXT, true, V><<<grid, block, 0, s>>>(sc, pts, n, detail, normal_mode, dist, iters);
+      else distance_kernel<T, 0, true, V><<<grid, block, 0, s>>>(sc, pts, n, detail, normal_mode, dist, iters);
+    } else {
+      return int(cudaErrorInvalidValue);
+    }
+  } else if (ext) {
+    distance_kernel<T, F_EXT, false, V><<<grid, block, 0, s>>>(sc, pts, n, detail, normal_mode, dist, iters);
   } else {
     distance_kernel<T, 0, false, V><<<grid, block, 0, s>>>(sc, pts, n, detail, normal_mode, dist, iters);
   }

@@ -74,6 +74,7 @@ struct WJob {
   int32_t width, height, tiles_x;
   int32_t row0, rows;      // the job renders rows [row0, row0 + rows) of its frame
   int32_t persp;           // mbr_projection
+  int32_t legacy_y;        // legacy coordinate system (image y flipped)
   long long first;         // first work item of this job in the pixel queue
   long long pixel_offset;  // first pixel of this job in the outputs
   double fov, aspect;
@@ -363,7 +364,7 @@ struct Prec64 {
     double de = e.dr;
     if (k == FK_BULB) f_mandelbulb<double>(z, e.r, de, fp.slot);
     else if (k == FK_MENGER) f_menger<double, false>(z, de, fp.slot);
-    else f_mandelbox<double, false>(z, de, fp.slot, &fp.rot);
+    else f_mandelbox<double, false, true>(z, de, fp.slot, &fp.rot);
     if (fp.add_c) {
       if (fp.julia) {
         z.x = z.x + fp.jc[0];
@@ -427,7 +428,10 @@ struct HybParams {
   const DevScene *sc;
 };
 
-struct PrecHyb {
+// EXT: every formula and the Mandelbox rotations (scene_extended scenes);
+// hybrids of the three specialised formulas use the lighter PrecHyb.
+template <bool EXT>
+struct PrecHybT {
   typedef float D;
   typedef HybParams Params;
   enum { kWide = 0, kHyb = 1 };
@@ -463,7 +467,7 @@ struct PrecHyb {
     const V4<float> last = z;
     const float tempDE = e.dr;
     float de = e.dr;
-    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs);
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs);
     if (s.add_c) {
       if (sc.julia) {
         z.x = z.x + juliac_of<float>(sc, 0);
@@ -524,6 +528,7 @@ struct PrecHyb {
     return d;
   }
 };
+typedef PrecHybT<false> PrecHyb;
 
 // ============================================================================
 // The persistent skeleton: refill lanes from a task counter, iterate, step.
@@ -740,7 +745,8 @@ struct PrimaryStage {
     pix = jb->pixel_offset + (long long)ray;
     // camera ray (render_worker.cpp:155-163, 247, 326-327)
     const double ix = (1.0 / double(jb->width) * double(x) + -0.5) * jb->aspect;
-    const double iy = -1.0 / double(jb->height) * double(y) + 0.5;
+    const double iy = jb->legacy_y ? 1.0 / double(jb->height) * double(y) + -0.5
+                                   : -1.0 / double(jb->height) * double(y) + 0.5;
     double vx = ix * jb->fov, vy = 1.0, vz = iy * jb->fov;
     if (jb->persp != MBR_PROJECTION_THREE_POINT) {
       if (hemisphere_cut(jb->persp, jb->fov, ix, iy)) {
@@ -1280,7 +1286,7 @@ __device__ __forceinline__ int wide_needed(const DevScene &sc, const double cam[
   double thr_min = de_thresh;
   if (!constant_thr) {
     int it;
-    const double d0 = calc_distance<double, 0, false>(sc, cam[0], cam[1], cam[2], 0.0, false, &it);
+    const double d0 = calc_distance<double, F_EXT, false>(sc, cam[0], cam[1], cam[2], 0.0, false, &it);
     thr_min = d0 * c0;
   }
   const double scale = fmax(fmax(fabs(cam[0]), fabs(cam[1])), fmax(fabs(cam[2]), 1.0));
@@ -1712,6 +1718,7 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.pixel_offset = pixel_offset;
   j.fov = fr.fov;
   j.persp = fr.persp;
+  j.legacy_y = fr.legacy_y;
   j.aspect = fr.aspect;
   j.resolution = fr.resolution;
   j.detail = fr.detail_level;
@@ -1921,7 +1928,10 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   if (hyb) {  // FP32 hybrid iteration reading the scene from the scratch
     DevScene *d_sc = reinterpret_cast<DevScene *>(reinterpret_cast<char *>(work) + scene_at);
     e = int(cudaMemcpyAsync(d_sc, &sc, sizeof(DevScene), cudaMemcpyHostToDevice, s));
-    if (!e) e = launch_pipeline<false, PrecHyb>(FK_ANY, tu, s, fr, HybParams{d_sc}, j0, L, out, pixels);
+    if (!e)
+      e = scene_extended(sc)
+              ? launch_pipeline<false, PrecHybT<true>>(FK_ANY, tu, s, fr, HybParams{d_sc}, j0, L, out, pixels)
+              : launch_pipeline<false, PrecHyb>(FK_ANY, tu, s, fr, HybParams{d_sc}, j0, L, out, pixels);
     return cuda_err(ctx, e, "wavefront launch");
   }
   if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {

@@ -1068,11 +1068,13 @@ struct Renderer {
   // Image point and view direction of pixel (x, y): doWork (render_worker.cpp:155-163,
   // 247, 326-327), region.hpp:66-71 with imageRegion (-0.5, 0.5, 0.5, -0.5),
   // CalculateViewVector three-point (projection_3d.cpp:77-84, 87).
+  // legacy coordinate system: imageRegion (-0.5, -0.5, 0.5, 0.5) (render_job.cpp:308-315)
   void image_point(double x, double y, double *ix, double *iy) const {
+    const bool legacy = cam.legacy_coordinate_system != 0;
     const double scaleX = 1.0 / double(cam.width);
-    const double scaleY = -1.0 / double(cam.height);
+    const double scaleY = (legacy ? 1.0 : -1.0) / double(cam.height);
     *ix = (scaleX * x + -0.5) * aspect;
-    *iy = scaleY * y + 0.5;
+    *iy = scaleY * y + (legacy ? -0.5 : 0.5);
   }
   // CalculateViewVector (projection_3d.cpp:40-89) for the camera's projection
   D3 view_vector(double ix, double iy) const {

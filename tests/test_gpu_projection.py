@@ -97,3 +97,29 @@ def test_projection_arguments(renderer):
     cam.perspective_type = 7
     with pytest.raises(MbrError):
         renderer.render(cam, p)
+
+
+def test_legacy_coordinate_system(renderer, oracle):
+    """The legacy image region (y from -0.5 at the top to +0.5 at the bottom,
+    render_job.cpp:308-315): every engine against the oracle, and the frame
+    is the ordinary one upside down."""
+    sc = configs.mandelbulb_scene(8.0, 20)
+    cam = configs.camera((0.4, -2.2, 0.9), width=64, height=48)
+    p = configs.base_params(5, 20.0)
+    renderer.set_scene(sc)
+    plain, _ = oracle.render(sc, cam, p)
+    cam.legacy_coordinate_system = 1
+    o, ost = oracle.render(sc, cam, p)
+    hp = plain["hit"].reshape(48, 64)
+    ho = o["hit"].reshape(48, 64)
+    assert np.mean(ho[1:][::-1] == hp[1:]) >= 0.99 and not np.array_equal(ho, hp)
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_MIXED, abi.ENGINE_WAVEFRONT_FP32,
+                   abi.ENGINE_WAVEFRONT_FP64):
+        fr = renderer.render(cam, p, engine, outputs=NAMES)
+        g = {k: v.cpu().numpy() for k, v in fr.buffers.items()}
+        m = compare(g, o)
+        print("legacy", abi.ENGINE_NAMES[engine], m)
+        if engine == abi.ENGINE_PLAIN_FP64_STRICT:
+            assert m["hit_iters_match"] >= 0.999 and m["depth_rel_le_1e-9"] >= 0.999, m
+        else:
+            assert m["hit_mismatch"] <= 0.005 and m["depth_rel_median"] <= 1e-4, m

@@ -172,12 +172,12 @@ def test_unsupported_geometry_is_named():
     assert s.status == abi.MBR_EUNSUPPORTED
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_sphere_1_enabled true;\nboolean_operators true;\n"
-                    "legacy_coordinate_system true;\ndelta_DE_method 1;\nhybrid_fractal_enable true;\n"
+                    "delta_DE_method 1;\nhybrid_fractal_enable true;\n"
                     "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
-    for key in ("primitive_sphere_1_enabled", "boolean_operators", "legacy_coordinate_system",
+    for key in ("primitive_sphere_1_enabled", "boolean_operators",
                 "delta_DE_method 1", "Mandelbox rotations in a hybrid"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
@@ -196,6 +196,12 @@ def test_mandelbox_rotations():
     assert list(f.mandelbox_rotation_neg[1]) == [10.0, 0.0, -5.5] and list(f.mandelbox_rotation_neg[0]) == [0.0] * 3
     assert list(f.mandelbox_rotation_pos[2]) == [0.0, 20.0, 0.0]
     assert list(f.mandelbox_rotation_main) == [3.0, -17.0, 41.0]
+
+
+def test_legacy_coordinate_system():
+    s = settings.load_from_string(HEADER + "[main_parameters]\nlegacy_coordinate_system true;\n")
+    assert s.ok, s.report
+    assert s.camera.legacy_coordinate_system == 1
 
 
 @pytest.mark.parametrize("value,want", [("three_point", 0), ("fish_eye", 1), ("equirectangular", 2),
