@@ -272,3 +272,25 @@ def test_reference_examples_render_on_the_oracle(oracle):
         assert 0.02 < frac <= 1.0, (name, frac)
         seen += 1
     assert seen >= 1
+
+
+def test_malformed_text_never_crashes():
+    """Random and truncated settings texts: the reader returns a status and a
+    report for every one, and never reads past the text."""
+    import random
+
+    rng = random.Random(5)
+    base = open(os.path.join(FIX, "box_ao.fract")).read()
+    pieces = ["camera", "formula_1", "IFS_direction_3", "mandelbox_rotation_neg_2", "fov", ";", " ", ",", "[",
+              "]", "fractal_9", "fractal_12", "\n", "\r\n", "true", "1e308", "-0", "nan", "\"", "'", "0,5 1 2"]
+    statuses = set()
+    for k in range(400):
+        if k % 2:
+            t = base[: rng.randrange(len(base))]
+        else:
+            t = HEADER + "".join(rng.choice(pieces) for _ in range(rng.randrange(1, 60)))
+        s = settings.load_from_string(t)
+        statuses.add(s.status)
+        assert s.status in (abi.MBR_OK, abi.MBR_EINVAL, abi.MBR_EUNSUPPORTED)
+        assert isinstance(s.report, str)
+    assert abi.MBR_EINVAL in statuses
