@@ -56,6 +56,7 @@ typedef enum mbr_formula {
   MBR_FORMULA_MANDELBULB_POWER2 = 3, /* formula/definition/fractal_mandelbulb_power2.cpp:30-45 */
   MBR_FORMULA_HYPERCOMPLEX = 4, /* formula/definition/fractal_hypercomplex.cpp:30-45; 4-D: plain FP64 engines */
   MBR_FORMULA_KALEIDOSCOPIC_IFS = 10, /* formula/definition/fractal_kaleidoscopic_ifs.cpp:30-85 */
+  MBR_FORMULA_XENODREAMBUIE = 11, /* formula/definition/fractal_xenodreambuie.cpp:30-49; Mandelbulb parameters */
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
   MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
 } mbr_formula;

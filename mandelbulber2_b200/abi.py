@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 
 # mbr_formula (fractal::enumFractalFormula)
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
-FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS = 3, 4, 10
+FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS, FORMULA_XENODREAMBUIE = 3, 4, 10, 11
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2

@@ -43,6 +43,8 @@ __device__ __forceinline__ double m_abs(double x) { return fabs(x); }
 __device__ __forceinline__ float m_abs(float x) { return fabsf(x); }
 __device__ __forceinline__ double m_asin(double x) { return asin(x); }
 __device__ __forceinline__ float m_asin(float x) { return asinf(x); }
+__device__ __forceinline__ double m_acos(double x) { return acos(x); }
+__device__ __forceinline__ float m_acos(float x) { return acosf(x); }
 __device__ __forceinline__ double m_atan2(double y, double x) { return atan2(y, x); }
 __device__ __forceinline__ float m_atan2(float y, float x) { return atan2f(y, x); }
 __device__ __forceinline__ double m_pow(double a, double b) { return pow(a, b); }
@@ -215,6 +217,27 @@ __device__ __forceinline__ void f_bulb_pow2(V4<T> &z, T r, T &DE) {
   z.z = nz;
 }
 
+// cFractalXenodreambuie::FormulaCode (fractal_xenodreambuie.cpp:30-49): the
+// Mandelbulb's parameters, azimuth from atan2 + beta, polar angle from acos
+// + alpha reflected into [-pi/2, pi/2]
+template <class T>
+__device__ __forceinline__ void f_xenodreambuie(V4<T> &z, T r, T &DE, const DevSlot &s) {
+  const T power = P<T>(s, P_POWER);
+  T rp = m_pow(r, P<T>(s, P_POWER_M1));
+  DE = rp * DE * power + T(1.0);
+  rp = rp * r;
+  const T th = (m_atan2(z.y, z.x) + P<T>(s, P_BETA)) * power;
+  T ph = m_acos(z.z / r) + P<T>(s, P_ALPHA);
+  if (m_abs(ph) > T(0.5 * 3.14159265358979323846)) ph = m_copysign(T(3.14159265358979323846), ph) - ph;
+  ph = ph * power;
+  T sth, cth, sph, cph;
+  m_sincos(th, &sth, &cth);
+  m_sincos(ph, &sph, &cph);
+  z.x = rp * cth * sph;
+  z.y = rp * sth * sph;
+  z.z = rp * cph;
+}
+
 // cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45): the
 // 4-D state is always carried (the host sets has_w for this formula)
 template <class T>
@@ -292,6 +315,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
       case MBR_FORMULA_HYPERCOMPLEX: f_hypercomplex<T>(z, r, DE); break;
       case MBR_FORMULA_KALEIDOSCOPIC_IFS: f_ifs<T>(z, DE, *ifs); break;
+      case MBR_FORMULA_XENODREAMBUIE: f_xenodreambuie<T>(z, r, DE, s); break;
       default: f_menger<T, W>(z, DE, s); break;
     }
   } else {

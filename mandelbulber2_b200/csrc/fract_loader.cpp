@@ -674,10 +674,11 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     if (!R.hybrid && i > 0) break;
     if (f == MBR_FORMULA_NONE) continue;
     if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE &&
-        f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS)
+        f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS &&
+        f != MBR_FORMULA_XENODREAMBUIE)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
                               " (formula not built here: 2 Mandelbulb, 3 Mandelbulb power 2, 4 hypercomplex, "
-                              "7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS are)");
+                              "7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie are)");
     if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && R.hybrid)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in a hybrid)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");

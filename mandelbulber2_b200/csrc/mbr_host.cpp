@@ -44,6 +44,7 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_MANDELBULB_POWER2: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_HYPERCOMPLEX: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: *m = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
+    case MBR_FORMULA_XENODREAMBUIE: *m = {2, 0, 10.0, 2}; return true;       // fractal_xenodreambuie.cpp:17-28
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
     default: return false;

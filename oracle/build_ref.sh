@@ -17,7 +17,7 @@ CXX=${CXX:-g++}
 FLAGS="-std=c++17 -O2 -fno-fast-math -ffp-contract=off -fPIC -I$MB -I$MB/src -I$MB/formula/definition -I$HERE/ref_shim"
 SRCS="$MB/formula/definition/fractal_mandelbulb.cpp $MB/formula/definition/fractal_mandelbox.cpp \
 $MB/formula/definition/fractal_menger_sponge.cpp $MB/formula/definition/fractal_mandelbulb_power2.cpp \
-$MB/formula/definition/fractal_hypercomplex.cpp $MB/formula/definition/fractal_kaleidoscopic_ifs.cpp \
+$MB/formula/definition/fractal_hypercomplex.cpp $MB/formula/definition/fractal_kaleidoscopic_ifs.cpp $MB/formula/definition/fractal_xenodreambuie.cpp \
 $MB/src/camera_target.cpp $MB/src/projection_3d.cpp \
 $MB/src/common_math.cpp $MB/src/algebra.cpp $HERE/ref_harness.cpp"
 $CXX $FLAGS -shared -o "$OUT/libref.so" $SRCS

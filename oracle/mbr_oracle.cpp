@@ -25,6 +25,7 @@
 #include "oracle_scalar.hpp"
 
 namespace oracle {
+using std::acos;
 using std::asin;
 using std::atan2;
 using std::cos;
@@ -54,6 +55,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_MANDELBULB_POWER2: *fi = {2, 0, 10.0, 2}; return true;  // fractal_mandelbulb_power2.cpp:17-28
     case MBR_FORMULA_HYPERCOMPLEX: *fi = {2, 0, 10.0, 2}; return true;      // fractal_hypercomplex.cpp:17-28
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: *fi = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
+    case MBR_FORMULA_XENODREAMBUIE: *fi = {2, 0, 10.0, 2}; return true;       // fractal_xenodreambuie.cpp:17-28
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -446,6 +448,22 @@ inline void formula_bulb_pow2(V4<S> &z, const S &r, S &DE) {
   z.z = nz;
 }
 
+// cFractalXenodreambuie::FormulaCode (fractal_xenodreambuie.cpp:30-49)
+template <class S>
+inline void formula_xenodreambuie(V4<S> &z, const SlotT<S> &f, const S &r, S &DE) {
+  S rp = pow(r, f.power - 1.0);
+  DE = rp * DE * f.power + 1.0;
+  rp = rp * r;
+  const S th = (atan2(z.y, z.x) + f.beta) * f.power;
+  S ph = acos(z.z / r) + f.alpha;
+  if (fabs(ph) > 0.5 * M_PI) ph = double(sgn(val(ph))) * M_PI - ph;  // sign(ph) * M_PI - ph
+  ph = ph * f.power;
+  const S sph = sin(ph);
+  z.x = rp * cos(th) * sph;
+  z.y = rp * sin(th) * sph;
+  z.z = rp * cos(ph);
+}
+
 // cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45)
 template <class S>
 inline void formula_hypercomplex(V4<S> &z, const S &r, S &DE) {
@@ -576,6 +594,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(z, r, DE); break;
         case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(z, r, DE); break;
         case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(z, f, DE); break;
+        case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(z, f, r, DE); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
@@ -1440,6 +1459,7 @@ int oracle_formula_step(const mbr_scene *scene, int slot, double *z, double *r, 
     case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, *r, *de); break;
     case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, *r, *de); break;
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(v, f, *de); break;
+    case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(v, f, *r, *de); break;
     default: return 1;
   }
   z[0] = v.x; z[1] = v.y; z[2] = v.z; z[3] = v.w;
@@ -1515,6 +1535,7 @@ int oracle_opcount(const mbr_scene *scene, int slot, const double *z, uint64_t *
     case MBR_FORMULA_MANDELBULB_POWER2: formula_bulb_pow2(v, r, DE); break;
     case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, r, DE); break;
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(v, f, DE); break;
+    case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(v, f, r, DE); break;
     default: return 1;
   }
   // the per-iteration work of Compute around the formula: c-add and |z|

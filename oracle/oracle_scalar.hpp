@@ -63,6 +63,8 @@ template <int N> inline Dual<N> cos(const Dual<N> &a) { return dual_apply<N, voi
 template <int N> inline Dual<N> log(const Dual<N> &a) { return dual_apply<N, void>(a, std::log(a.v), 1.0 / a.v); }
 template <int N> inline Dual<N> asin(const Dual<N> &a) {
   return dual_apply<N, void>(a, std::asin(a.v), 1.0 / std::sqrt(1.0 - a.v * a.v)); }
+template <int N> inline Dual<N> acos(const Dual<N> &a) {
+  return dual_apply<N, void>(a, std::acos(a.v), -1.0 / std::sqrt(1.0 - a.v * a.v)); }
 template <int N> inline Dual<N> atan2(const Dual<N> &y, const Dual<N> &x) {
   Dual<N> r; r.v = std::atan2(y.v, x.v); double q = x.v * x.v + y.v * y.v;
   for (int i = 0; i < N; i++) r.d[i] = (x.v * y.d[i] - y.v * x.d[i]) / q; return r; }
@@ -134,6 +136,7 @@ inline OpCount sin(OpCount a) { g_tally.transc++; return OpCount::computed(std::
 inline OpCount cos(OpCount a) { g_tally.transc++; return OpCount::computed(std::cos(a.v)); }
 inline OpCount log(OpCount a) { g_tally.transc++; return OpCount::computed(std::log(a.v)); }
 inline OpCount asin(OpCount a) { g_tally.transc++; return OpCount::computed(std::asin(a.v)); }
+inline OpCount acos(OpCount a) { g_tally.transc++; return OpCount::computed(std::acos(a.v)); }
 inline OpCount atan2(OpCount y, OpCount x) { g_tally.transc++; return OpCount::computed(std::atan2(y.v, x.v)); }
 inline OpCount pow(OpCount a, OpCount b) { g_tally.transc++; return OpCount::computed(std::pow(a.v, b.v)); }
 inline bool isfinite(OpCount a) { return std::isfinite(a.v); }

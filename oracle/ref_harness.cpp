@@ -65,6 +65,12 @@ int ref_formula_step(int formula, const double *params, double *z, double *aux_r
   } else if (formula == 4) {
     static cFractalHypercomplex fh;
     fh.FormulaCode(v, &f, aux);
+  } else if (formula == 11) {
+    f.bulb.power = params[0];
+    f.bulb.alphaAngleOffset = params[1];
+    f.bulb.betaAngleOffset = params[2];
+    static cFractalXenodreambuie fx;
+    fx.FormulaCode(v, &f, aux);
   } else if (formula == 7) {
     f.transformCommon.scale3 = params[0];
     f.foldColor.auxColorEnabledFalse = false;

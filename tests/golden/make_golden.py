@@ -3,7 +3,8 @@ sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
 
   formula_kat.json  chains of cFractal*::FormulaCode calls (Mandelbulb,
                     Mandelbox with and without rotations, Menger sponge,
-                    Mandelbulb power 2, hypercomplex, kaleidoscopic IFS)
+                    Mandelbulb power 2, hypercomplex, kaleidoscopic IFS,
+                    xenodreambuie)
                     on seeded random points
   projection_kat.json  CalcFOV + CalculateViewVector of the fish-eye,
                     equirectangular and fish-eye-cut projections
@@ -45,6 +46,9 @@ FORMULAS = [
     ("menger_3", 7, [3.0], {"transf_scale3": 3.0}),
     ("mandelbulb_power2", 3, [], {}),
     ("hypercomplex", 4, [], {}),
+    ("xenodreambuie_p5", 11, [5.0, 0.0, 0.0], {"bulb_power": 5.0}),
+    ("xenodreambuie_p3_angles", 11, [3.0, 15.0 * math.pi / 180.0, -30.0 * math.pi / 180.0],
+     {"bulb_power": 3.0, "bulb_alpha_angle_offset": 15.0, "bulb_beta_angle_offset": -30.0}),
 ]
 # Mandelbox with rotations (fractal_mandelbox.cpp:33-63, 103): the eight
 # parameters above, rotationsEnabled, mainRotationEnabled, the neg and pos

@@ -108,3 +108,29 @@ def test_kaleidoscopic_ifs(renderer, oracle):
     for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED,
                    abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
         check(renderer, sc, cam, p, o, ost, engine, "ifs")
+
+
+def test_xenodreambuie(renderer, oracle):
+    """Formula 11: transcendental, so FP64 is held to the FP64 bar (not
+    bit-exactness) and FP32 to the FP32 bar."""
+    sc = abi.scene_defaults(abi.FORMULA_XENODREAMBUIE)
+    sc.fractal[0].bulb_power = 5.0
+    sc.formula_maxiter = 30
+    cam = configs.camera((0.5, -2.4, 0.9), width=96, height=64)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    renderer.set_scene(sc)
+    o, _ = oracle.render(sc, cam, p)
+    assert 0.1 < float(np.mean(o["hit"])) < 0.95
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED,
+                   abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
+        fr = renderer.render(cam, p, engine, outputs=NAMES)
+        g = {k: v.cpu().numpy() for k, v in fr.buffers.items()}
+        m = compare(g, o)
+        print("xenodreambuie", abi.ENGINE_NAMES[engine], m)
+        if engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64):
+            assert m["hit_iters_match"] >= 0.999, m
+            assert m["depth_rel_le_1e-9"] >= 0.999, m
+        else:
+            assert m["hit_mismatch"] <= 0.005, m
+            assert m["depth_rel_median"] <= 1e-4, m

@@ -241,9 +241,9 @@ def test_reference_examples():
         formulas = {sc.fractal[i].formula for i in used} - {0}
         if s.ok:
             ok += 1
-            assert formulas <= {2, 3, 4, 7, 8, 10}, (path, formulas)
+            assert formulas <= {2, 3, 4, 7, 8, 10, 11}, (path, formulas)
             assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
-        elif not formulas <= {2, 3, 4, 7, 8, 10}:
+        elif not formulas <= {2, 3, 4, 7, 8, 10, 11}:
             assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
     assert ok >= 60, ok
 
