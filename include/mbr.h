@@ -259,6 +259,11 @@ typedef struct mbr_render_params {
   double saturation;            /* default 1 */
   int32_t hdr;                  /* default 0 */
   int32_t row_end;              /* 0 = the last row */
+  /* the main light's shadow (cLight, light.cpp:87; AuxShadow,
+   * shader_aux_shadow.cpp:55-77, 142-151, 266-301): */
+  double soft_shadow_cone;      /* "soft_shadow_cone", degrees; default 1; 0 = hard shadow */
+  int32_t penetrating;          /* "penetrating": march only |camera - p| * fov and darken by depth; default 1 */
+  int32_t reserved2;
 } mbr_render_params;
 
 /* Per-launch counters (src/statistics.h:42-70 mirrored).  A DE evaluation

@@ -81,6 +81,10 @@ def base_params(binary_steps: int = 5, view_distance_max: float = 20.0) -> abi.R
     p.seed = 0
     p.shading_enable = 1
     p.shadow_enable = 1
+    # the benchmark configurations use a hard, non-penetrating shadow
+    # (the library's defaults are the reference's: a 1 degree soft cone, penetrating)
+    p.soft_shadow_cone = 0.0
+    p.penetrating = 0
     p.light_direction[:] = list(SUN)
     p.light_intensity = 1.0
     p.material_shading = 1.0

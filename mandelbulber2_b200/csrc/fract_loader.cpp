@@ -733,10 +733,12 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     params->light_direction[1] = dir.y;
     params->light_direction[2] = dir.z;
   }
-  if (R.light_enabled && R.light_shadows && R.light_penetrating)
-    append(rep, "note: light1_penetrating: the shadow march runs to view_distance_max (non-penetrating)");
-  if (R.light_enabled && R.light_shadows && R.light_soft_cone > 0.0)
-    append(rep, "note: light1_soft_shadow_cone: the shadow is hard");
+  params->penetrating = R.light_penetrating;
+  params->soft_shadow_cone = R.light_soft_cone;
+  if (!(R.light_soft_cone >= 0.0 && R.light_soft_cone < 90.0)) {
+    params->soft_shadow_cone = R.light_soft_cone < 0.0 ? 0.0 : 89.0;
+    append(rep, "note: light1_soft_shadow_cone outside [0, 90) degrees: clamped");
+  }
 
   // ambient occlusion: the multiple-rays mode maps onto 16 cosine-hemisphere
   // rays per hit; the fast and screen-space modes are not on this path

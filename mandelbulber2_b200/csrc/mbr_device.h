@@ -145,6 +145,9 @@ struct DevFrame {
   int32_t ao_rays;
   double de_thresh;
   double light[3];     // unit vector toward the light
+  double soft_range;   // tan(soft shadow cone); 0: hard shadow
+  int32_t penetrating; // shadow march to |camera - p| * fov, darkened by depth
+  int32_t pad2;
   float light_intensity;
   float material_shading;
   float albedo;

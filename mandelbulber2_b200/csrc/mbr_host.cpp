@@ -471,6 +471,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   if (p.row_begin < 0 || p.row_begin >= row_end || row_end > cam.height)
     return set_err(ctx, MBR_EINVAL, "row band [%d, %d) outside the %d rows of the frame", p.row_begin, p.row_end,
                    cam.height);
+  if (!(p.soft_shadow_cone >= 0.0 && p.soft_shadow_cone < 90.0))
+    return set_err(ctx, MBR_EINVAL, "soft_shadow_cone must be in [0, 90) degrees, got %g", p.soft_shadow_cone);
   const double *L = p.light_direction;
   if (!finite3(L) || (L[0] == 0.0 && L[1] == 0.0 && L[2] == 0.0))
     return set_err(ctx, MBR_EINVAL, "light_direction must be finite and non-zero");
@@ -505,6 +507,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.de_thresh = p.de_thresh;
   f.shading_enable = p.shading_enable ? 1 : 0;
   f.shadow_enable = p.shadow_enable ? 1 : 0;
+  f.soft_range = std::tan(p.soft_shadow_cone / 180.0 * kPi);  // light.cpp:87, shader_aux_shadow.cpp:64
+  f.penetrating = p.penetrating ? 1 : 0;
   f.ao_rays = p.ao_rays;
   const HV l = hnorm(HV{L[0], L[1], L[2]});
   f.light[0] = l.x;
@@ -729,6 +733,9 @@ void mbr_render_params_defaults(mbr_render_params *p) {
   p->contrast = 1.0;
   p->gamma = 1.0;
   p->saturation = 1.0;
+  // light 1 (initparameters.cpp:1901, 1919)
+  p->soft_shadow_cone = 1.0;
+  p->penetrating = 1;
 }
 
 mbr_status mbr_scene_set(mbr_ctx *ctx, const mbr_scene *scene) {

@@ -13,7 +13,7 @@
 //   RayMarching               src/render_worker.cpp:708-951
 //   CalculateNormals          src/shader_calculate_normals.cpp:40-125
 //   LightShading              src/shader_light_shading.cpp:40-122
-//   AuxShadow (hard)          src/shader_aux_shadow.cpp:39-323
+//   AuxShadow (hard, soft)    src/shader_aux_shadow.cpp:39-323
 //   AmbientOcclusion          src/shader_ambient_occlusion.cpp:41-120
 //   GlobalIlumination march   src/shader_global_illumination.cpp:75-125
 //   MonteCarloDOF             src/render_worker.cpp:1832-1844
@@ -301,10 +301,14 @@ __device__ D3 normals(const DevScene &sc, const DevFrame &fr, D3 q, double thr, 
 
 template <class T, int F, bool W>
 __device__ double aux_shadow(const DevScene &sc, const DevFrame &fr, D3 q, double thr, D3 L, ThreadCount &tc) {
-  const double distance = fr.view_distance_max;
+  // a penetrating directional light marches delta / resolution (light.cpp:277-290)
+  const bool pen = fr.penetrating != 0;
+  const double distance = pen ? calc_delta(fr, q) / fr.resolution : fr.view_distance_max;
+  const bool soft = fr.soft_range > 0.0 && !sc.interior && !sc.iter_thresh;  // bSoft (:71-74)
   double start = thr;
   if (sc.interior) start = thr * fr.de_factor;
   double shadowTemp = 1.0;
+  double maxSoft = 0.0;
   int count = 0;
   double step = thr;
   const float dist_thresh_f = float(thr);
@@ -312,8 +316,22 @@ __device__ double aux_shadow(const DevScene &sc, const DevFrame &fr, D3 q, doubl
   for (double i = start; i < distance; i += step) {
     const D3 point2 = d3ray(q, L, i);
     const double dist = de_eval<T, F, W>(sc, point2, thr, false, &it, tc);
-    if (dist < double(dist_thresh_f)) {
-      shadowTemp = 0.0;
+    if (soft) {  // :142-151
+      double angle = (dist - double(dist_thresh_f)) / i;
+      if (angle < 0) angle = 0;
+      if (dist < double(dist_thresh_f)) angle = 0;
+      double softShadow = 1.0 - angle / fr.soft_range;
+      if (pen) softShadow *= (distance - i) / distance;
+      if (softShadow < 0) softShadow = 0;
+      if (softShadow > maxSoft) maxSoft = softShadow;
+    }
+    if (dist < double(dist_thresh_f)) {  // :266-280
+      if (pen) {
+        shadowTemp -= (distance - i) / distance;
+        if (shadowTemp < 0.0) shadowTemp = 0.0;
+      } else {
+        shadowTemp = 0.0;
+      }
       break;
     }
     step = fmin(dist, 1000000.0) * fr.de_factor;
@@ -321,7 +339,7 @@ __device__ double aux_shadow(const DevScene &sc, const DevFrame &fr, D3 q, doubl
     count++;
     if (count > fr.max_steps) break;
   }
-  return shadowTemp;
+  return soft ? 1.0 - maxSoft : shadowTemp;
 }
 
 // AO march rule of the reference along cosine-hemisphere directions; each

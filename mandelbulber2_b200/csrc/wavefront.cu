@@ -1062,6 +1062,13 @@ __device__ __forceinline__ unsigned long long pcg_advance(unsigned long long sta
 // hit point rounded once (no FP64 conversions in the loop), or FP64 from the
 // hit point itself.  Their hit test uses the float-rounded distThresh, as the
 // reference's shaders do.
+// The march length of a penetrating directional light's shadow: delta /
+// resolution at the hit, i.e. |camera - p| * fov (light.cpp:277-290)
+__device__ __forceinline__ double shadow_distance(const DevFrame &fr, double px, double py, double pz) {
+  const double ax = fr.camera[0] - px, ay = fr.camera[1] - py, az = fr.camera[2] - pz;
+  return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.resolution;
+}
+
 template <bool MULTI, class P>
 struct ShadeStage {
   typedef typename P::D Real;
@@ -1074,6 +1081,7 @@ struct ShadeStage {
   HitRec *r;
   D ox, oy, oz, t;
   D dx, dy, dz, end, vdm, dfac;
+  D maxsoft;  // soft shadow: the largest 1 - angle / range so far (shader_aux_shadow.cpp:142-151)
   float thr;
   int count, mode;  // mode 0 shadow, 1 AO
   unsigned int shadow_de;
@@ -1119,6 +1127,8 @@ struct ShadeStage {
     dz = D(dv.z);
     mode = dv.w < 0.0f ? 0 : 1;
     end = mode ? D(dv.w) : vdm;
+    if (!mode && fr.penetrating) end = D(shadow_distance(fr, double(ox), double(oy), double(oz)));
+    maxsoft = D(0);
     count = 0;
     point(qx, qy, qz);
     return true;
@@ -1128,14 +1138,29 @@ struct ShadeStage {
     count++;
     if (mode == 0) {
       shadow_de++;
+      const bool soft = fr.soft_range > 0.0;
+      if (soft) {
+        D angle = (d - D(thr)) / t;
+        if (angle < D(0)) angle = D(0);
+        if (d < D(thr)) angle = D(0);
+        D sft = D(1) - angle / D(fr.soft_range);
+        if (fr.penetrating) sft = sft * ((end - t) / end);
+        if (sft < D(0)) sft = D(0);
+        if (sft > maxsoft) maxsoft = sft;
+      }
       if (d < D(thr)) {
-        r->shadow = 0.f;
+        D v = D(0);
+        if (fr.penetrating) {
+          v = D(1) - (end - t) / end;
+          if (v < D(0)) v = D(0);
+        }
+        r->shadow = float(soft ? D(1) - maxsoft : v);
         return false;
       }
       if (P::kWide) t += fmax(fmin(double(d), 1e6) * double(dfac), 1e-15);
       else t += fmaxf(fminf(float(d), 1e6f) * float(dfac), 1e-15f);
-      if (count > fr.max_steps || t >= vdm) {
-        r->shadow = 1.f;
+      if (count > fr.max_steps || t >= end) {
+        r->shadow = soft ? float(D(1) - maxsoft) : 1.f;
         return false;
       }
     } else {
@@ -1185,7 +1210,7 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
       if (!(r.shade > 0.001f)) {
         r.shadow = 0.f;
         dv = make_float4(0.f, 0.f, 0.f, 0.f);
-      } else if (!(thr < vdm)) {
+      } else if (!(thr < (fr.penetrating ? float(shadow_distance(fr, r.px, r.py, r.pz)) : vdm))) {
         r.shadow = 1.f;
         dv = make_float4(0.f, 0.f, 0.f, 0.f);
       } else {

@@ -1024,10 +1024,15 @@ struct Renderer {
   // (shader_aux_shadow.cpp:39-323 with softShadowCone = 0, no fog/clouds/SSS;
   //  distance = viewDistanceMax, light.cpp:281-291).
   double aux_shadow(D3 q, double thr, D3 L, Counters &c, uint64_t *counter) const {
-    const double distance = p.view_distance_max;
+    // directional light: a penetrating one marches delta / resolution (light.cpp:277-290)
+    const bool pen = p.penetrating != 0;
+    const double distance = pen ? calc_delta(q) / resolution : p.view_distance_max;
+    const double softRange = tan(p.soft_shadow_cone / 180.0 * M_PI);  // light.cpp:87, :64
+    const bool bSoft = !seq.iter_thresh && !seq.interior && softRange > 0.0;  // :71-74
     double start = thr;
     if (seq.interior) start = thr * p.de_factor;
     double shadowTemp = 1.0;
+    double maxSoft = 0.0;
     int count = 0;
     double step = thr;
     const float dist_thresh = float(thr);
@@ -1035,9 +1040,23 @@ struct Renderer {
     for (double i = start; i < distance; i += step) {
       const D3 point2 = add(q, mul(L, i));
       const double dist = de(point2, thr, false, nullptr, c);
+      if (bSoft) {  // :142-151
+        double angle = (dist - dist_thresh) / i;
+        if (angle < 0) angle = 0;
+        if (dist < dist_thresh) angle = 0;
+        double softShadow = 1.0 - angle / softRange;
+        if (pen) softShadow *= (distance - i) / distance;
+        if (softShadow < 0) softShadow = 0;
+        if (softShadow > maxSoft) maxSoft = softShadow;
+      }
       shadowTemp = 1.0 - 0.0;
-      if (dist < dist_thresh || shadowTemp < 0.0) {
-        shadowTemp = 0.0;
+      if (dist < dist_thresh || shadowTemp < 0.0) {  // :266-280
+        if (pen) {
+          shadowTemp -= (distance - i) / distance;
+          if (shadowTemp < 0.0) shadowTemp = 0.0;
+        } else {
+          shadowTemp = 0.0;
+        }
         break;
       }
       step = std::min(dist, double(1e6f)) * p.de_factor;
@@ -1046,7 +1065,7 @@ struct Renderer {
       if (count > p.max_raymarching_steps) break;
     }
     *counter += c.de - before;
-    return shadowTemp;
+    return bSoft ? 1.0 - maxSoft : shadowTemp;
   }
 
   // AmbientOcclusion march rule (shader_ambient_occlusion.cpp:41-120) along

@@ -76,7 +76,7 @@ def test_mandelbox_with_ao():
     want = relative_light(cam.camera, cam.target, cam.top, [30, -20, 0])
     np.testing.assert_allclose(list(p.light_direction), want, rtol=0, atol=1e-12)
     assert "volumetric_fog_enabled" in s.report and "mat1_specular" in s.report
-    assert "penetrating" not in s.report and "hard" not in s.report
+    assert p.penetrating == 0 and p.soft_shadow_cone == 0.0  # light1_penetrating false, cone 0
 
 
 def test_hybrid_sequence():
@@ -92,8 +92,8 @@ def test_hybrid_sequence():
     # the default light: rotation (-45, 45, 0) relative to the camera
     want = relative_light(s.camera.camera, s.camera.target, s.camera.top, [-45, 45, 0])
     np.testing.assert_allclose(list(s.params.light_direction), want, rtol=0, atol=1e-12)
-    # penetrating shadows and the soft cone are the reference's defaults, mapped with a note
-    assert "penetrating" in s.report and "hard" in s.report
+    # penetrating shadows with a 1 degree soft cone are the reference's defaults
+    assert s.params.penetrating == 1 and s.params.soft_shadow_cone == 1.0
     # the sequence the library builds: 3 bulb passes, then 9 Menger passes
     lib = abi.load()
     import ctypes as C
