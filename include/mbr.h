@@ -8,7 +8,7 @@
  *   cRenderWorker::RayMarching     src/render_worker.cpp:708-951
  *   CalculateNormals (fast path)   src/shader_calculate_normals.cpp:40-79
  *   LightShading + AuxShadow       src/shader_light_shading.cpp:40-122,
- *                                  src/shader_aux_shadow.cpp:39-323 (hard shadow)
+ *                                  src/shader_aux_shadow.cpp:39-323 (hard, soft, penetrating)
  *   AmbientOcclusion               src/shader_ambient_occlusion.cpp:41-120
  *   GlobalIlumination + MC DOF     src/shader_global_illumination.cpp:41-209,
  *                                  src/render_worker.cpp:1832-1862
