@@ -263,7 +263,12 @@ typedef struct mbr_render_params {
    * shader_aux_shadow.cpp:55-77, 142-151, 266-301): */
   double soft_shadow_cone;      /* "soft_shadow_cone", degrees; default 1; 0 = hard shadow */
   int32_t penetrating;          /* "penetrating": march only |camera - p| * fov and darken by depth; default 1 */
-  int32_t reserved2;
+  /* fast ambient occlusion (ambient_occlusion_mode "fast": FastAmbientOcclusion,
+   * src/shader_fast_ambient_occlusion.cpp:40-65): quality^2 - 1 distance
+   * samples along the normal instead of the ao_rays marches */
+  int32_t ao_fast;              /* default 0 */
+  int32_t ao_quality;           /* "ambient_occlusion_quality", default 4, 1..10 */
+  double ao_fast_tune;          /* "ambient_occlusion_fast_tune", default 1 */
 } mbr_render_params;
 
 /* Per-launch counters (src/statistics.h:42-70 mirrored).  A DE evaluation

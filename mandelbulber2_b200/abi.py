@@ -92,7 +92,8 @@ class RenderParams(C.Structure):
         ("gi_sky", C.c_double), ("gi_sun", C.c_double), ("dof_aperture", C.c_double), ("dof_focus", C.c_double),
         ("gi_seed", C.c_uint32), ("row_begin", C.c_int32), ("brightness", C.c_double), ("contrast", C.c_double),
         ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("row_end", C.c_int32),
-        ("soft_shadow_cone", C.c_double), ("penetrating", C.c_int32), ("reserved2", C.c_int32),
+        ("soft_shadow_cone", C.c_double), ("penetrating", C.c_int32), ("ao_fast", C.c_int32),
+        ("ao_quality", C.c_int32), ("ao_fast_tune", C.c_double),
     ]
 
 

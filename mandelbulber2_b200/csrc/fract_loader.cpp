@@ -196,6 +196,8 @@ struct Reader {
   int slot_enable[kSlots];
   int ao_enabled = 0, ao_mode = 2;
   double ao_intensity = 1.0;
+  int ao_quality = 4;
+  double ao_fast_tune = 1.0;
   // light 1 (initparameters.cpp:1895-1950)
   int light_enabled = 1, light_shadows = 1, light_penetrating = 1, light_relative = 1, light_use_target = 0;
   int light_type = 0;  // 0 directional
@@ -550,6 +552,10 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     else if (value == "screen_space") R.ao_mode = 2;
     else if (parse_int(value, b)) R.ao_mode = b;
     else R.bad(name, value);
+  } else if (name == "ambient_occlusion_quality") {
+    if (parse_int(value, b)) R.ao_quality = b; else R.bad(name, value);
+  } else if (name == "ambient_occlusion_fast_tune") {
+    if (parse_double(value, d)) R.ao_fast_tune = d; else R.bad(name, value);
   } else if (name == "ambient_occlusion") {
     if (parse_double(value, d)) R.ao_intensity = d; else R.bad(name, value);
   } else {
@@ -741,15 +747,21 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
   }
 
   // ambient occlusion: the multiple-rays mode maps onto 16 cosine-hemisphere
-  // rays per hit; the fast and screen-space modes are not on this path
+  // rays per hit, the fast mode onto its quality^2 - 1 samples along the
+  // normal (quality and fast tune in the reference's ranges,
+  // initparameters.cpp:215-216); the screen-space mode is not on this path
   if (R.ao_enabled) {
     if (R.ao_mode == 1) {
       params->ao_rays = 16;
       params->ambient_intensity = R.ao_intensity;
       append(rep, "note: ambient_occlusion (multiple rays): 16 cosine-hemisphere rays per hit");
+    } else if (R.ao_mode == 0) {
+      params->ao_fast = 1;
+      params->ao_quality = std::min(10, std::max(1, R.ao_quality));
+      params->ao_fast_tune = std::isfinite(R.ao_fast_tune) ? std::min(1e5, std::max(1e-5, R.ao_fast_tune)) : 1.0;
+      params->ambient_intensity = R.ao_intensity;
     } else {
-      append(rep, std::string("note: ambient_occlusion mode ") + (R.ao_mode == 0 ? "fast" : "screen space") +
-                      " is not on this path; AO off");
+      append(rep, "note: ambient_occlusion mode screen space is not on this path; AO off");
     }
   }
 

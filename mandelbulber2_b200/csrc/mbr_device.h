@@ -147,7 +147,10 @@ struct DevFrame {
   double light[3];     // unit vector toward the light
   double soft_range;   // tan(soft shadow cone); 0: hard shadow
   int32_t penetrating; // shadow march to |camera - p| * fov, darkened by depth
+  int32_t ao_fast;     // fast AO: quality^2 - 1 samples along the normal
+  int32_t ao_quality;
   int32_t pad2;
+  double ao_fast_tune;
   float light_intensity;
   float material_shading;
   float albedo;

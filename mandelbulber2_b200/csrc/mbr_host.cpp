@@ -471,6 +471,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   if (p.row_begin < 0 || p.row_begin >= row_end || row_end > cam.height)
     return set_err(ctx, MBR_EINVAL, "row band [%d, %d) outside the %d rows of the frame", p.row_begin, p.row_end,
                    cam.height);
+  if (p.ao_fast && (p.ao_quality < 1 || p.ao_quality > 10 || !std::isfinite(p.ao_fast_tune)))
+    return set_err(ctx, MBR_EINVAL, "fast AO needs ao_quality in [1, 10] and a finite ao_fast_tune");
   if (!(p.soft_shadow_cone >= 0.0 && p.soft_shadow_cone < 90.0))
     return set_err(ctx, MBR_EINVAL, "soft_shadow_cone must be in [0, 90) degrees, got %g", p.soft_shadow_cone);
   const double *L = p.light_direction;
@@ -509,6 +511,9 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.shadow_enable = p.shadow_enable ? 1 : 0;
   f.soft_range = std::tan(p.soft_shadow_cone / 180.0 * kPi);  // light.cpp:87, shader_aux_shadow.cpp:64
   f.penetrating = p.penetrating ? 1 : 0;
+  f.ao_fast = (p.ao_fast && p.gi_samples == 0) ? 1 : 0;
+  f.ao_quality = p.ao_quality;
+  f.ao_fast_tune = p.ao_fast_tune;
   f.ao_rays = p.ao_rays;
   const HV l = hnorm(HV{L[0], L[1], L[2]});
   f.light[0] = l.x;
@@ -736,6 +741,9 @@ void mbr_render_params_defaults(mbr_render_params *p) {
   // light 1 (initparameters.cpp:1901, 1919)
   p->soft_shadow_cone = 1.0;
   p->penetrating = 1;
+  // initparameters.cpp:214-216
+  p->ao_quality = 4;
+  p->ao_fast_tune = 1.0;
 }
 
 mbr_status mbr_scene_set(mbr_ctx *ctx, const mbr_scene *scene) {

@@ -15,6 +15,7 @@
 //   LightShading              src/shader_light_shading.cpp:40-122
 //   AuxShadow (hard, soft)    src/shader_aux_shadow.cpp:39-323
 //   AmbientOcclusion          src/shader_ambient_occlusion.cpp:41-120
+//   FastAmbientOcclusion      src/shader_fast_ambient_occlusion.cpp:40-65
 //   GlobalIlumination march   src/shader_global_illumination.cpp:75-125
 //   MonteCarloDOF             src/render_worker.cpp:1832-1844
 //   CalculatePixel + 8 bit    src/cimage.cpp:317-375, 460-469
@@ -344,34 +345,58 @@ __device__ double aux_shadow(const DevScene &sc, const DevFrame &fr, D3 q, doubl
 
 // AO march rule of the reference along cosine-hemisphere directions; each
 // march is capped at max_steps evaluations (counted as a watchdog trip).
+// Fast AO (fr.ao_fast) runs through the same loop, so that the kernel holds
+// one inlined distance estimate for both: quality^2 - 1 samples at
+// i^2 * distThresh along the normal, each clamped to twice the previous one,
+// summed in float as 2^-i (scan - fast_tune * dist) / distThresh, giving
+// ao = max(0, 1 - 0.2 sum).
 template <class T, int F, bool W>
 __device__ double ambient_occlusion(const DevScene &sc, const DevFrame &fr, D3 q, D3 n, double thr,
                                     unsigned long long pixel, ThreadCount &tc, unsigned int *trips) {
+  const bool fast = fr.ao_fast != 0;
   const double start_dist = thr;
   const double end_dist = calc_delta(fr, q) / fr.resolution;
   const float dist_thresh_f = float(thr);
+  const int rays = fast ? 1 : fr.ao_rays;
+  const int samples = fr.ao_quality * fr.ao_quality;
   Pcg32 rng = pcg_init(fr.ao_seed, pixel);
   double sum = 0.0;
   int it;
-  for (int k = 0; k < fr.ao_rays; k++) {
-    const double u1 = rng.uniform(), u2 = rng.uniform();
-    const D3 v = cosine_dir(n, u1, u2);
+  for (int k = 0; k < rays; k++) {
+    D3 v = n;
+    if (!fast) {
+      const double u1 = rng.uniform(), u2 = rng.uniform();
+      v = cosine_dir(n, u1, u2);
+    }
     double dist = 0.0;
-    double shadowTemp = 1.0;
+    double shadowTemp = fast ? 1e20 : 1.0;  // fast: the previous (clamped) sample
     int steps = 0;
-    for (double r = start_dist; r < end_dist; r += dist * 2.0) {
-      if (steps >= fr.max_steps) {
+    for (double r = start_dist; fast ? steps + 1 < samples : r < end_dist;) {
+      if (steps >= fr.max_steps && !fast) {
         (*trips)++;
         break;
       }
       steps++;
       const D3 point2 = d3ray(q, v, r);
       dist = de_eval<T, F, W>(sc, point2, thr, false, &it, tc);
+      if (fast) {  // sum holds the float sum
+        if (dist > shadowTemp * 2) dist = shadowTemp * 2.0;
+        shadowTemp = dist;
+        sum = double(float(sum + ldexp(1.0, -steps) * (r - fr.ao_fast_tune * dist) / thr));
+        r = double((steps + 1) * (steps + 1)) * thr;
+        continue;
+      }
       if (dist < double(dist_thresh_f)) {
         shadowTemp -= (end_dist - r) / end_dist;
         if (shadowTemp < 0.0) shadowTemp = 0.0;
         break;
       }
+      r += dist * 2.0;
+    }
+    if (fast) {
+      float ao = 1.0f - 0.2f * float(sum);
+      if (ao < 0) ao = 0;
+      return ao;
     }
     sum += shadowTemp;
   }

@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ DevS
       m = ray_marching<T, R, F, W>(sc, fr, camera_of(fr), dir, pm, tc, &n_march, &n_binary);
       if (m.found) {
         D3 n{1.0, 0.0, 0.0};
-        if (fr.shading_enable || fr.ao_rays > 0 || fr.want_normal) {
+        if (fr.shading_enable || fr.ao_rays > 0 || fr.ao_fast || fr.want_normal) {
           const unsigned int d0 = tc.de;
           n = normals<T, F, W>(sc, fr, m.point, m.thr, tc);
           n_normal += tc.de - d0;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ DevS
           }
           shade = s * aux;
         }
-        if (fr.ao_rays > 0) {
+        if (fr.ao_rays > 0 || fr.ao_fast) {
           const unsigned int d0 = tc.de;
           ao = float(ambient_occlusion<T, F, W>(sc, fr, m.point, n, m.thr, pixel, tc, &trips));
           n_ao += tc.de - d0;

@@ -170,7 +170,8 @@ struct Launch {
   int gate_value;          // the flag value this pipeline runs under (0 FP32, 1 FP64)
   int refill_k;
   int layout;
-  int ao_rays;
+  int ao_rays;             // AO tasks per hit (1 for fast AO)
+  int ao_fast;             // fast AO: the AO task samples along the normal
   int shadow_tasks;        // 1 when the shadow march runs (shading && shadow)
   int want_normal;
   FastDiv div_per;         // division by shadow_tasks + ao_rays (set by launch_pipeline)
@@ -183,6 +184,9 @@ struct Launch {
   int row0;                      // first row of the launch
   int normal_slot;               // stats counter of stage N (K_NORMAL; K_GI in GI frames)
 };
+
+// Stage-S AO tasks per hit: the AO marches, or the one fast-AO task.
+static inline int ao_tasks(const DevFrame &fr) { return fr.ao_fast ? 1 : fr.ao_rays; }
 
 // True when this pipeline's kernels have nothing to do (the other precision
 // renders the frame).
@@ -1063,10 +1067,15 @@ __device__ __forceinline__ unsigned long long pcg_advance(unsigned long long sta
 // hit point itself.  Their hit test uses the float-rounded distThresh, as the
 // reference's shaders do.
 // The march length of a penetrating directional light's shadow: delta /
-// resolution at the hit, i.e. |camera - p| * fov (light.cpp:277-290)
-__device__ __forceinline__ double shadow_distance(const DevFrame &fr, double px, double py, double pz) {
-  const double ax = fr.camera[0] - px, ay = fr.camera[1] - py, az = fr.camera[2] - pz;
-  return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.resolution;
+// resolution at the hit, i.e. |camera - p| * fov (light.cpp:277-290), with
+// the camera of the hit's own job
+template <bool MULTI>
+__device__ __forceinline__ double shadow_distance(const DevFrame &fr, const Launch &L, const HitRec &r) {
+  const double *cam = MULTI ? L.jobs[r.job].cam : fr.camera;
+  const double res = MULTI ? L.jobs[r.job].resolution : fr.resolution;
+  const double fov = MULTI ? L.jobs[r.job].fov : fr.fov;
+  const double ax = cam[0] - r.px, ay = cam[1] - r.py, az = cam[2] - r.pz;
+  return sqrt(ax * ax + ay * ay + az * az) * res * fov / res;
 }
 
 template <bool MULTI, class P>
@@ -1081,9 +1090,11 @@ struct ShadeStage {
   HitRec *r;
   D ox, oy, oz, t;
   D dx, dy, dz, end, vdm, dfac;
-  D maxsoft;  // soft shadow: the largest 1 - angle / range so far (shader_aux_shadow.cpp:142-151)
+  // soft shadow: the largest 1 - angle / range so far (shader_aux_shadow.cpp:142-151);
+  // fast AO: the previous (clamped) distance sample
+  D maxsoft;
   float thr;
-  int count, mode;  // mode 0 shadow, 1 AO
+  int count, mode;  // mode 0 shadow, 1 AO march, 2 fast AO (end: its float sum)
   unsigned int shadow_de;
 
   __device__ const typename P::Params &params() const { return fp; }
@@ -1125,10 +1136,14 @@ struct ShadeStage {
     dx = D(dv.x);
     dy = D(dv.y);
     dz = D(dv.z);
-    mode = dv.w < 0.0f ? 0 : 1;
-    end = mode ? D(dv.w) : vdm;
-    if (!mode && fr.penetrating) end = D(shadow_distance(fr, double(ox), double(oy), double(oz)));
+    mode = dv.w < 0.0f ? 0 : (L.ao_fast ? 2 : 1);
+    end = mode == 1 ? D(dv.w) : vdm;
+    if (!mode && fr.penetrating) end = D(shadow_distance<MULTI>(fr, L, *r));
     maxsoft = D(0);
+    if (mode == 2) {  // first sample at 1 * distThresh along the normal
+      end = D(0);
+      maxsoft = D(1e20);
+    }
     count = 0;
     point(qx, qy, qz);
     return true;
@@ -1163,6 +1178,25 @@ struct ShadeStage {
         r->shadow = soft ? float(D(1) - maxsoft) : 1.f;
         return false;
       }
+    } else if (mode == 2) {
+      // FastAmbientOcclusion (shader_fast_ambient_occlusion.cpp:40-65): sample
+      // i = count at scan t = i^2 distThresh; the sum is kept in float
+      D dist = d;
+      if (dist > maxsoft * D(2)) dist = maxsoft * D(2);
+      maxsoft = dist;
+      const D delta = P::kWide ? D(r->thr) : D(thr);
+      if (P::kWide)
+        end = D(float(double(end) + ldexp(1.0, -count) * (double(t) - fr.ao_fast_tune * double(dist)) / double(delta)));
+      else
+        end = D(float(end) + ldexpf(1.0f, -count) * (float(t) - float(fr.ao_fast_tune) * float(dist)) / float(delta));
+      const int i = count + 1;
+      if (i >= fr.ao_quality * fr.ao_quality) {
+        float ao = 1.0f - 0.2f * float(end);
+        if (ao < 0.0f) ao = 0.0f;
+        r->ao_q = (unsigned long long)__float_as_uint(ao);
+        return false;
+      }
+      t = D(i * i) * delta;
     } else {
       if (d < D(thr)) {
         if (P::kWide) {
@@ -1210,12 +1244,14 @@ __global__ void __launch_bounds__(256) direction_kernel(const __grid_constant__ 
       if (!(r.shade > 0.001f)) {
         r.shadow = 0.f;
         dv = make_float4(0.f, 0.f, 0.f, 0.f);
-      } else if (!(thr < (fr.penetrating ? float(shadow_distance(fr, r.px, r.py, r.pz)) : vdm))) {
+      } else if (!(thr < (fr.penetrating ? float(shadow_distance<MULTI>(fr, L, r)) : vdm))) {
         r.shadow = 1.f;
         dv = make_float4(0.f, 0.f, 0.f, 0.f);
       } else {
         dv = make_float4(float(fr.light[0]), float(fr.light[1]), float(fr.light[2]), -1.0f);
       }
+    } else if (L.ao_fast) {
+      dv = make_float4(r.nx, r.ny, r.nz, 1.0f);  // fast AO: samples along the normal
     } else {
       const int a = k - L.shadow_tasks;
       Pcg32 g = pcg_init(fr.ao_seed, (unsigned long long)r.ray);
@@ -1270,7 +1306,9 @@ __global__ void __launch_bounds__(256) finish_kernel(const __grid_constant__ Dev
     const HitRec &r = L.hits[h];
     const long long pix = r.pix;
     const float shade = r.shade * r.shadow;
-    const float ao = (L.ao_rays > 0) ? float(double(r.ao_q) * (1.0 / 4294967296.0) / double(L.ao_rays)) : 1.0f;
+    const float ao = L.ao_fast        ? __uint_as_float((unsigned int)r.ao_q)
+                     : (L.ao_rays > 0) ? float(double(r.ao_q) * (1.0 / 4294967296.0) / double(L.ao_rays))
+                                       : 1.0f;
     const float col = fr.albedo * (shade + fr.ambient * ao);
     float rgb[3] = {col, col, col};
     if (out.depth) out.depth[pix] = r.depth;
@@ -1912,7 +1950,7 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   const WJob j0 = make_job(fr, 0, out.pixel_offset);
   const long long pixels = (long long)fr.width * (fr.row1 - fr.row0);
   const long long total = gi ? pixels * (long long)fr.gi_samples : job_items(j0, tu.queue_layout);
-  const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
+  const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + ao_tasks(fr);
   // scratch: counters, then the GI accumulators or the hit records, then (a
   // hybrid scene) the scene the iteration reads
   // GI: a counter block per bounce level (4 KiB), the auto-engine flag, the
@@ -1943,7 +1981,8 @@ mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr
   }
   L.refill_k = tu.refill_k;
   L.layout = tu.queue_layout;
-  L.ao_rays = fr.ao_rays;
+  L.ao_rays = ao_tasks(fr);
+  L.ao_fast = fr.ao_fast;
   L.shadow_tasks = (fr.shading_enable && fr.shadow_enable) ? 1 : 0;
   L.want_normal = fr.want_normal;
   const FastParams fp = load_fast_params(sc);
@@ -2118,7 +2157,7 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
   if (e) return fail(e, "cudaMalloc(params)");
   e = int(cudaMalloc(&b->d_wide, sizeof(WideParams) * n_jobs));
   if (e) return fail(e, "cudaMalloc(wide params)");
-  const int per = ((fr0.shading_enable && fr0.shadow_enable) ? 1 : 0) + fr0.ao_rays;
+  const int per = ((fr0.shading_enable && fr0.shadow_enable) ? 1 : 0) + ao_tasks(fr0);
   e = int(cudaMalloc(&b->d_scratch, scratch_bytes(max_items, per)));
   if (e) return fail(e, "cudaMalloc(scratch)");
   e = int(cudaMemcpy(b->d_jobs, tab.data(), sizeof(WJob) * n_jobs, cudaMemcpyHostToDevice));
@@ -2146,7 +2185,8 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
       scratch_layout(L, b->d_scratch, g.items);
       L.refill_k = tu.refill_k;
       L.layout = tu.queue_layout;
-      L.ao_rays = fr0.ao_rays;
+      L.ao_rays = ao_tasks(fr0);
+      L.ao_fast = fr0.ao_fast;
       L.shadow_tasks = (fr0.shading_enable && fr0.shadow_enable) ? 1 : 0;
       L.want_normal = fr0.want_normal;
       if (g.wide)
@@ -2340,7 +2380,7 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
                         "the wavefront engine renders non-hybrid Mandelbulb, Mandelbox and Menger scenes without GI, "
                         "root refinement, iteration threshold, interior mode or initial w");
   const long long total = (long long)fr.width * (fr.row1 - fr.row0);  // row-linear queue: no tile padding
-  const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + fr.ao_rays;
+  const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + ao_tasks(fr);
   const size_t need = scratch_bytes(total, per);
   const size_t have = size_t(MBR_NOALLOC_SCRATCH_BYTES) - kHeadBytes;
   if (need > have) {
@@ -2360,7 +2400,8 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
   const mbr_tuning tu{128, 12, 2, 0};
   L.refill_k = tu.refill_k;
   L.layout = tu.queue_layout;
-  L.ao_rays = fr.ao_rays;
+  L.ao_rays = ao_tasks(fr);
+  L.ao_fast = fr.ao_fast;
   L.shadow_tasks = (fr.shading_enable && fr.shadow_enable) ? 1 : 0;
   L.want_normal = fr.want_normal;
   DevOutputs d;

@@ -1103,6 +1103,28 @@ struct Renderer {
     return sum / p.ao_rays;
   }
 
+  // FastAmbientOcclusion (shader_fast_ambient_occlusion.cpp:40-65): quality^2 - 1
+  // distance samples at i^2 * distThresh along the normal, each clamped to twice
+  // the previous one; the float sum of 2^-i (scan - fastTune * dist) / distThresh
+  // gives ao = max(0, 1 - 0.2 sum).
+  double fast_ao(D3 q, D3 n, double thr, Counters &c, uint64_t *counter) const {
+    const uint64_t before = c.de;
+    float aoTemp = 0.0f;
+    double lastDist = 1e20;
+    const int samples = p.ao_quality * p.ao_quality;
+    for (int i = 1; i < samples; i++) {
+      const double scan = double(i * i) * thr;
+      double dist = de(add(q, mul(n, scan)), thr, false, nullptr, c);
+      if (dist > lastDist * 2) dist = lastDist * 2.0;
+      lastDist = dist;
+      aoTemp += std::ldexp(1.0, -i) * (scan - p.ao_fast_tune * dist) / thr;
+    }
+    *counter += c.de - before;
+    float ao = 1.0f - 0.2f * aoTemp;
+    if (ao < 0) ao = 0;
+    return ao;
+  }
+
   // Image point and view direction of pixel (x, y): doWork (render_worker.cpp:155-163,
   // 247, 326-327), region.hpp:66-71 with imageRegion (-0.5, 0.5, 0.5, -0.5),
   // CalculateViewVector three-point (projection_3d.cpp:77-84, 87).
@@ -1154,7 +1176,8 @@ struct Renderer {
       for (int k = 0; k < 3; k++) po.rgb[k] = float(p.background[k]);
       return;
     }
-    const bool need_normal = p.shading_enable || p.ao_rays > 0 || want_normal;
+    const bool fast = p.ao_fast && p.gi_samples == 0;
+    const bool need_normal = p.shading_enable || p.ao_rays > 0 || fast || want_normal;
     D3 n{1.0, 0.0, 0.0};
     if (need_normal) {
       n = normals(m.point, m.thr, c, &c.normal);
@@ -1181,7 +1204,8 @@ struct Renderer {
       shade = s * aux;
     }
     float ao = 1.0f;
-    if (p.ao_rays > 0) ao = float(ambient_occlusion(m.point, n, m.thr, pixel, c, &c.ao));
+    if (fast) ao = float(fast_ao(m.point, n, m.thr, c, &c.ao));
+    else if (p.ao_rays > 0) ao = float(ambient_occlusion(m.point, n, m.thr, pixel, c, &c.ao));
     po.shade = shade;
     po.ao = ao;
     const float col = float(p.albedo) * (shade + float(p.ambient_intensity) * ao);

@@ -66,7 +66,11 @@ def test_wavefront_results_independent_of_tuning(renderer):
     renderer.set_tuning(128, 12, 2, 0)
 
 
-def test_batch_matches_single_renders(renderer):
+@pytest.mark.parametrize("lighting", ["hard_ao_rays", "penetrating_soft_fast_ao"])
+def test_batch_matches_single_renders(renderer, lighting):
+    """Every job of a batch renders its frame as a render of its own would;
+    the second case uses the camera-dependent parts of the shading (the
+    penetrating shadow's march length and the fast AO's samples)."""
     lib = abi.load()
     scenes = [configs.mandelbulb_scene(8.0, 100), configs.mandelbox_scene(-1.5, 0.5, 40),
               configs.mandelbox_scene(2.2, 0.4, 40), configs.mandelbulb_scene(5.5, 100)]
@@ -77,6 +81,13 @@ def test_batch_matches_single_renders(renderer):
     p = configs.base_params(5, 20.0)
     p.ao_rays = 4
     p.ao_seed = 9
+    if lighting == "penetrating_soft_fast_ao":
+        p.penetrating = 1
+        p.soft_shadow_cone = 1.0
+        p.ao_rays = 0
+        p.ao_fast = 1
+        p.ao_quality = 4
+        p.ambient_intensity = 0.5
     jobs = (abi.Job * len(cams))()
     off = 0
     offs = []

@@ -204,6 +204,31 @@ def test_legacy_coordinate_system():
     assert s.camera.legacy_coordinate_system == 1
 
 
+@pytest.mark.parametrize("quality,tune,want_q,want_t", [("3", "0,5", 3, 0.5), ("50", "0", 10, 1e-5),
+                                                        (None, None, 4, 1.0)])
+def test_fast_ambient_occlusion(quality, tune, want_q, want_t):
+    """ambient_occlusion_mode fast maps onto the fast AO with the quality and
+    fast tune clamped to the reference's ranges (initparameters.cpp:215-216)."""
+    txt = HEADER + "[main_parameters]\nambient_occlusion_enabled true;\nambient_occlusion_mode fast;\n"
+    txt += "ambient_occlusion 0,7;\n"
+    if quality is not None:
+        txt += f"ambient_occlusion_quality {quality};\nambient_occlusion_fast_tune {tune};\n"
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    p = s.params
+    assert p.ao_fast == 1 and p.ao_rays == 0 and p.ambient_intensity == 0.7
+    assert p.ao_quality == want_q and p.ao_fast_tune == want_t
+    assert "ambient_occlusion" not in s.report
+
+
+def test_screen_space_ao_is_noted_and_off():
+    txt = HEADER + "[main_parameters]\nambient_occlusion_enabled true;\nambient_occlusion_mode screen_space;\n"
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    assert s.params.ao_fast == 0 and s.params.ao_rays == 0
+    assert "screen space is not on this path" in s.report
+
+
 @pytest.mark.parametrize("value,want", [("three_point", 0), ("fish_eye", 1), ("equirectangular", 2),
                                         ("fish_eye_cut", 3), ("2", 2)])
 def test_projection(value, want):
