@@ -38,6 +38,8 @@ extern "C" {
 /* Length of a hybrid sequence table: maxN * 5 with maxN = 250
  * (src/hybrid_fractal_sequences.cpp:296-298). */
 #define MBR_SEQUENCE_LENGTH 1250
+/* primitives joined to the fractal by union (at most this many) */
+#define MBR_MAX_PRIMITIVES 8
 
 typedef enum mbr_status {
   MBR_OK = 0,
@@ -162,6 +164,50 @@ typedef struct mbr_fractal {
   double ifs_intensity[9];                   /* default 1 */
 } mbr_fractal;
 
+/* Primitive kinds (fractal::enumObjectType primitives, src/primitive.cpp) */
+typedef enum mbr_primitive_type {
+  MBR_PRIMITIVE_PLANE = 1,     /* z = 0, solid below (sPrimitivePlane, :459-465) */
+  MBR_PRIMITIVE_BOX = 2,       /* size, rounding (sPrimitiveBox, :467-497) */
+  MBR_PRIMITIVE_SPHERE = 3,    /* radius (sPrimitiveSphere, :499-511) */
+  MBR_PRIMITIVE_WATER = 4,     /* wavy plane (sPrimitiveWater, :572-638) */
+  MBR_PRIMITIVE_TORUS = 5,     /* radius, tube radius, their L-powers (sPrimitiveTorus, :640-655) */
+  MBR_PRIMITIVE_CYLINDER = 6,  /* radius, height, caps (sPrimitiveCylinder, :522-537) */
+  MBR_PRIMITIVE_CIRCLE = 7,    /* flat disc of radius (sPrimitiveCircle, :539-545) */
+  MBR_PRIMITIVE_RECTANGLE = 8  /* flat width x height (sPrimitiveRectangle, :513-520) */
+} mbr_primitive_type;
+
+/* One primitive (the legacy primitive_<type>_<n>_* parameters,
+ * src/initparameters.cpp:1313-1420) and its node transform (position,
+ * rotation in degrees as CRotationMatrix::SetRotation2, uniform scale,
+ * repeat period; src/objects_tree.cpp:290-385). */
+typedef struct mbr_primitive {
+  int32_t type;               /* mbr_primitive_type */
+  int32_t empty;              /* hollow: |distance| */
+  int32_t limits_enable;      /* clip to the box [limits_min, limits_max] (local frame) */
+  int32_t caps;               /* cylinder: closed ends, default 1 */
+  int32_t iterations;         /* water: wave octaves, default 5 */
+  int32_t frame_no;           /* water: animation frame ("frame_no"), default 0 */
+  double position[3];
+  double rotation[3];         /* degrees */
+  double scale;               /* default 1 */
+  double repeat[3];           /* tiling period, 0 = none */
+  double size[3];             /* box: default (1,1,1) */
+  double radius;              /* sphere, torus, cylinder, circle: default 1 */
+  double height;              /* cylinder, rectangle: default 1 */
+  double width;               /* rectangle: default 1 */
+  double tube_radius;         /* torus: default 0.2 */
+  double radius_lpow;         /* torus: L-power exponent log2, default 1 */
+  double tube_radius_lpow;    /* torus: default 1 */
+  double rounding;            /* box: default 1e-15 */
+  double wall_thickness;      /* default 0 */
+  double limits_min[3];       /* default (-0.7,-0.7,-0.7) */
+  double limits_max[3];       /* default (0.7,0.7,0.7) */
+  double relative_amplitude;  /* water: default 0.2 */
+  double length;              /* water: default 0.1 */
+  double anim_speed;          /* water: default 1 */
+  double anim_progression_speed; /* water: default 1 */
+} mbr_primitive;
+
 /* The fractal part of a scene: one fractal (or hybrid) object node with the
  * general fractal parameters of src/initparameters.cpp:128-157 and the node
  * parameters of :2102-2125.  The objects tree holds exactly this one node at
@@ -183,6 +229,12 @@ typedef struct mbr_scene {
   double initial_waxis;        /* default 0 */
   double linear_de_offset;     /* default 0 */
   mbr_fractal fractal[MBR_MAX_FRACTALS];
+  /* primitives joined to the fractal by union (boolean operator OR, the
+   * default of a primitive): the distance is the smallest of the fractal's
+   * and theirs (objects-tree walk, src/calculate_distance.cpp:225-516) */
+  int32_t n_primitives;        /* 0..MBR_MAX_PRIMITIVES, default 0 */
+  int32_t reserved_prim;
+  mbr_primitive primitive[MBR_MAX_PRIMITIVES];
 } mbr_scene;
 
 /* params::enumPerspectiveType (src/projection_3d.hpp:44-50): the view
@@ -315,6 +367,7 @@ const char *mbr_last_error_string(const mbr_ctx *ctx);
 /* Fill structs with the reference defaults (src/initparameters.cpp). */
 void mbr_scene_defaults(mbr_scene *scene);
 void mbr_fractal_defaults(mbr_fractal *fractal, int formula);
+void mbr_primitive_defaults(mbr_primitive *primitive, int type);
 void mbr_camera_defaults(mbr_camera *camera);
 void mbr_render_params_defaults(mbr_render_params *params);
 

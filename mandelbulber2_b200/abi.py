@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libmbr.so")
 
 MBR_MAX_FRACTALS = 9
 MBR_SEQUENCE_LENGTH = 1250
+MBR_MAX_PRIMITIVES = 8
 
 # mbr_status
 MBR_OK, MBR_EINVAL, MBR_ECUDA, MBR_ETIMEOUT, MBR_ENOMEM, MBR_EUNSUPPORTED = range(6)
@@ -24,6 +25,9 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
 FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS, FORMULA_XENODREAMBUIE = 3, 4, 10, 11
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
+# mbr_primitive_type
+(PRIMITIVE_PLANE, PRIMITIVE_BOX, PRIMITIVE_SPHERE, PRIMITIVE_WATER, PRIMITIVE_TORUS, PRIMITIVE_CYLINDER,
+ PRIMITIVE_CIRCLE, PRIMITIVE_RECTANGLE) = range(1, 9)
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
 # mbr_engine
@@ -61,6 +65,18 @@ class Fractal(C.Structure):
     ]
 
 
+class Primitive(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("empty", C.c_int32), ("limits_enable", C.c_int32), ("caps", C.c_int32),
+        ("iterations", C.c_int32), ("frame_no", C.c_int32), ("position", D3), ("rotation", D3),
+        ("scale", C.c_double), ("repeat", D3), ("size", D3), ("radius", C.c_double), ("height", C.c_double),
+        ("width", C.c_double), ("tube_radius", C.c_double), ("radius_lpow", C.c_double),
+        ("tube_radius_lpow", C.c_double), ("rounding", C.c_double), ("wall_thickness", C.c_double),
+        ("limits_min", D3), ("limits_max", D3), ("relative_amplitude", C.c_double), ("length", C.c_double),
+        ("anim_speed", C.c_double), ("anim_progression_speed", C.c_double),
+    ]
+
+
 class Scene(C.Structure):
     _fields_ = [
         ("n_fractals", C.c_int32), ("hybrid_fractal_enable", C.c_int32), ("formula_maxiter", C.c_int32),
@@ -69,6 +85,7 @@ class Scene(C.Structure):
         ("interior_mode", C.c_int32), ("bailout", C.c_double), ("julia_c", D3),
         ("fractal_constant_factor", D3), ("initial_waxis", C.c_double), ("linear_de_offset", C.c_double),
         ("fractal", Fractal * MBR_MAX_FRACTALS),
+        ("n_primitives", C.c_int32), ("reserved_prim", C.c_int32), ("primitive", Primitive * MBR_MAX_PRIMITIVES),
     ]
 
 
@@ -130,6 +147,7 @@ PROTOTYPES = {
     "mbr_last_error_string": (C.c_char_p, [_P]),
     "mbr_scene_defaults": (None, [C.POINTER(Scene)]),
     "mbr_fractal_defaults": (None, [C.POINTER(Fractal), C.c_int]),
+    "mbr_primitive_defaults": (None, [C.POINTER(Primitive), C.c_int]),
     "mbr_camera_defaults": (None, [C.POINTER(Camera)]),
     "mbr_render_params_defaults": (None, [C.POINTER(RenderParams)]),
     "mbr_scene_set": (C.c_int, [_P, C.POINTER(Scene)]),
@@ -187,6 +205,12 @@ def scene_defaults(formula: int = FORMULA_MANDELBULB) -> Scene:
     lib.mbr_scene_defaults(C.byref(s))
     lib.mbr_fractal_defaults(C.byref(s.fractal[0]), formula)
     return s
+
+
+def primitive_defaults(kind: int) -> Primitive:
+    q = Primitive()
+    load().mbr_primitive_defaults(C.byref(q), kind)
+    return q
 
 
 def camera_defaults() -> Camera:

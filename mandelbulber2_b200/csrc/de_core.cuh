@@ -356,6 +356,121 @@ __device__ __forceinline__ T juliac_of(const DevScene &sc, int k) {
   return T(sc.julia_c[k] * sc.cmul[k]);
 }
 
+// std::max(a, b) of the reference: b when a < b, else a.
+template <class T>
+__device__ __forceinline__ T smax(T a, T b) {
+  return (a < b) ? b : a;
+}
+
+// One component of CVector3::repeatMod (algebra.hpp:106-115): ((p - v/2) % v
+// + v) % v - v/2, with % the fmod of a positive period.
+template <class T>
+__device__ __forceinline__ T repeat_mod(T p, T v) {
+  T t = p - v * T(0.5);
+  if (v > T(0.0)) t = fmod(t, v);
+  t = t + v;
+  if (v > T(0.0)) t = fmod(t, v);
+  return t - v * T(0.5);
+}
+
+// Primitive distances (src/primitive.cpp) at a world point: the node's
+// world-to-local transform and repeat (calculate_distance.cpp:268-282), the
+// primitive's local distance, times the node's scale (:398-401).
+template <class T>
+__device__ __noinline__ T prim_distance(const DevPrim &q, T wx, T wy, T wz) {
+  T x = T(q.m[0]) * wx + T(q.m[1]) * wy + T(q.m[2]) * wz + T(q.m[3]);
+  T y = T(q.m[4]) * wx + T(q.m[5]) * wy + T(q.m[6]) * wz + T(q.m[7]);
+  T z = T(q.m[8]) * wx + T(q.m[9]) * wy + T(q.m[10]) * wz + T(q.m[11]);
+  if (q.has_repeat) {
+    x = repeat_mod(x, T(q.repeat[0]));
+    y = repeat_mod(y, T(q.repeat[1]));
+    z = repeat_mod(z, T(q.repeat[2]));
+  }
+  T d;
+  bool limits = q.limits != 0;
+  switch (q.type) {
+    case MBR_PRIMITIVE_PLANE:
+      d = z;
+      break;
+    case MBR_PRIMITIVE_BOX:
+      if (q.empty) {
+        d = T(-1e10);
+        d = smax(T(fabs(x) - T(q.size[0]) * T(0.5)), d);
+        d = smax(T(fabs(y) - T(q.size[1]) * T(0.5)), d);
+        d = smax(T(fabs(z) - T(q.size[2]) * T(0.5)), d);
+        d = fabs(d);
+      } else {
+        const T bx = smax(T(fabs(x) - T(q.size[0]) * T(0.5)), T(0.0));
+        const T by = smax(T(fabs(y) - T(q.size[1]) * T(0.5)), T(0.0));
+        const T bz = smax(T(fabs(z) - T(q.size[2]) * T(0.5)), T(0.0));
+        d = sqrt(bx * bx + by * by + bz * bz) - T(q.rounding);
+      }
+      break;
+    case MBR_PRIMITIVE_SPHERE:
+      d = sqrt(x * x + y * y + z * z) - T(q.radius);
+      break;
+    case MBR_PRIMITIVE_CYLINDER:
+      d = sqrt(x * x + y * y) - T(q.radius);
+      if (!q.caps) d = fabs(d);
+      d = smax(T(fabs(z) - T(q.height) * T(0.5)), d);
+      break;
+    case MBR_PRIMITIVE_CIRCLE:
+      d = smax(T(fabs(z)), T(sqrt(x * x + y * y) - T(q.radius)));
+      break;
+    case MBR_PRIMITIVE_RECTANGLE: {
+      const T bx = smax(T(fabs(x) - T(q.width) * T(0.5)), T(0.0));
+      const T by = smax(T(fabs(y) - T(q.height) * T(0.5)), T(0.0));
+      const T bz = fabs(z);
+      d = sqrt(bx * bx + by * by + bz * bz);
+      break;
+    }
+    case MBR_PRIMITIVE_TORUS: {
+      const T pr = T(q.pow_r), pt = T(q.pow_t);
+      const T d1 = pow(pow(x, pr) + pow(y, pr), T(1.0) / pr) - T(q.radius);
+      d = pow(pow(d1, pt) + pow(z, pt), T(1.0) / pt) - T(q.tube);
+      break;
+    }
+    default: {  // MBR_PRIMITIVE_WATER: sPrimitiveWater::PrimitiveDistanceWater (primitive.cpp:572-638)
+      const T amplitude = T(q.amp), len = T(q.length);
+      d = z;
+      if (d < amplitude * T(10.0)) {
+        const double phase = q.phase;
+        const T k = T(0.23);
+        T waveX = T(0.0), waveY = T(0.0);
+        T p = T(1.0), p2 = T(0.05);
+        x = x + T(q.xshift);
+        for (int i = 1; i <= q.iterations; i++) {
+          const float p3 = float(p * p2);
+          const float shift = float(phase / (double(i) / 2.697 + 1.0));
+          const T wxt = sin(T(i) + T(0.4) * waveX * T(p3) + sin(k * y / len * T(p3) + T(shift) * T(0.134) * T(p3)) +
+                            x / len * T(p3) + T(shift * p3)) /
+                        p;
+          const T wyt = cos(T(i) + T(0.4) * waveY * T(p3) + sin(x / len * T(p3) + T(shift) * T(0.0179) * T(p3)) +
+                            k * y / len * T(p3) + T(shift) * T(0.023) * T(p3)) /
+                        p;
+          waveX = waveX + wxt;
+          waveY = waveY + wyt;
+          p2 = p2 + (T(1.0) - p2 + T(0.5) * sin(T(shift) * T(0.0323))) * T(0.7);
+          p = p * T(1.872);
+        }
+        d = d + (waveX + waveY) * amplitude;
+      }
+      break;
+    }
+  }
+  if (q.type != MBR_PRIMITIVE_CIRCLE && q.type != MBR_PRIMITIVE_RECTANGLE) {
+    if (q.empty && q.type != MBR_PRIMITIVE_BOX) d = fabs(d);
+    d = smax(T(d - T(q.wall)), T(0.0));
+  }
+  if (limits) {
+    const T lx = smax(T(x - T(q.lmax[0])), T(T(q.lmin[0]) - x));
+    const T ly = smax(T(y - T(q.lmax[1])), T(T(q.lmin[1]) - y));
+    const T lz = smax(T(z - T(q.lmax[2])), T(T(q.lmin[2]) - z));
+    d = smax(d, smax(smax(lx, ly), lz));
+  }
+  return d * T(q.abs_scale);
+}
+
 // Compute<calcModeNormal> + CalculateDistanceSimple (analytic branch).
 // F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
 // the three specialised formulas) or F_EXT (generic with every formula and
@@ -455,6 +570,12 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
   }
   if (distance < T(0.0)) distance = T(0.0);
   if (distance > T(10.0)) distance = T(10.0);
+  if (F == F_EXT) {  // the union with the primitives (booleanAdd, calculate_distance.cpp:166-201)
+    for (int k = 0; k < sc.n_prims; k++) {
+      const T pd = prim_distance<T>(sc.prim[k], px, py, pz);
+      if (pd < distance) distance = pd;
+    }
+  }
   return distance;
 }
 

@@ -19,8 +19,10 @@
 // This reader restates that flat form for the parameters the DE path reads:
 // formulas and the hybrid sequence, the iteration and bailout settings,
 // camera, raymarching quality, the main light, AO and the 8-bit conversion.
-// Geometry this path does not build (other formulas, boolean combinations,
-// primitives, transforms, forced delta DE) makes the call
+// Primitives joined by union (plane, box, sphere, water, torus, cylinder,
+// circle, rectangle) are read into mbr_scene.primitive.  Geometry this path
+// does not build (other formulas, boolean combinations, other primitives or
+// operators, transforms, forced delta DE) makes the call
 // return MBR_EUNSUPPORTED with each item named in the report; shading
 // parameters outside the path (materials, fog, glow, reflections, textures,
 // further lights) are counted and listed as ignored.
@@ -185,8 +187,21 @@ V3 rotate_zxy(V3 v, V3 angles) {
   return V3{ca * r.x - sa * r.y, sa * r.x + ca * r.y, r.z};  // Rz(a)
 }
 
+// A legacy primitive_<type>_<n>_* block (settings.cpp:1058-1080, initparameters.cpp:1313-1420)
+struct PrimRead {
+  std::string key;  // "<type>_<n>"
+  int type = 0;     // mbr_primitive_type, 0: a kind not built here
+  std::string type_name;
+  int enabled = 0;  // InitPrimitiveParams: "_enabled" false
+  int boolean_operator = 1;  // primBooleanOperatorOR
+  int smooth = 0;
+  mbr_primitive q;
+};
+
 struct Reader {
   double version = 0.0;
+  std::vector<PrimRead> prims;
+  int frame_no = 0;
   std::vector<std::string> unsupported, ignored, notes, errors;
 
   // main parameters (defaults: initparameters.cpp)
@@ -247,6 +262,101 @@ void compatibility(const Reader &R, std::string &name, std::string &value) {
                               {"main_light_position_relative", "light1_relative_position"}};
     for (const Ren &r : ren)
       if (name == r.from) name = r.to;
+  }
+}
+
+// primitive_<type>_<n>_<param> (the legacy flat form; cPrimitives::PrimitiveNameToEnum)
+void read_primitive_param(Reader &R, const std::string &full, const std::string &value) {
+  const std::string rest = full.substr(10);  // after "primitive_"
+  const size_t u1 = rest.find('_');
+  const size_t u2 = (u1 == std::string::npos) ? u1 : rest.find('_', u1 + 1);
+  int index = 0;
+  if (u2 == std::string::npos || !parse_int(rest.substr(u1 + 1, u2 - u1 - 1), index)) {
+    R.unsupported.push_back(full + " (primitive parameter)");
+    return;
+  }
+  const std::string tname = rest.substr(0, u1), key = rest.substr(0, u2);
+  std::string param = rest.substr(u2 + 1);
+  // settings.cpp:1365-1372: before 2.13 the water's "amplitude" is its relative amplitude
+  if (R.version < 2.13 && tname == "water" && param == "amplitude") param = "relative_amplitude";
+  PrimRead *pr = nullptr;
+  for (PrimRead &x : R.prims)
+    if (x.key == key) pr = &x;
+  if (!pr) {
+    static const struct {
+      const char *name;
+      int type;
+    } kinds[] = {{"plane", MBR_PRIMITIVE_PLANE},       {"box", MBR_PRIMITIVE_BOX},
+                 {"sphere", MBR_PRIMITIVE_SPHERE},     {"water", MBR_PRIMITIVE_WATER},
+                 {"torus", MBR_PRIMITIVE_TORUS},       {"cylinder", MBR_PRIMITIVE_CYLINDER},
+                 {"circle", MBR_PRIMITIVE_CIRCLE},     {"rectangle", MBR_PRIMITIVE_RECTANGLE},
+                 {"cone", 0},                          {"prism", 0},
+                 {"ellipsoid", 0}};
+    int type = -1;
+    for (const auto &k : kinds)
+      if (tname == k.name) type = k.type;
+    if (type < 0) {
+      R.unsupported.push_back(full + " (unknown primitive)");
+      return;
+    }
+    R.prims.push_back(PrimRead());
+    pr = &R.prims.back();
+    pr->key = key;
+    pr->type = type;
+    pr->type_name = tname;
+    mbr_primitive_defaults(&pr->q, type);
+  }
+  mbr_primitive &q = pr->q;
+  double d;
+  int b;
+  double v[3];
+  auto vec = [&](double *dst) {
+    if (parse_vec3(value, v)) std::memcpy(dst, v, sizeof(v)); else R.bad(full, value);
+  };
+  auto num = [&](double &dst) {
+    if (parse_double(value, d)) dst = d; else R.bad(full, value);
+  };
+  auto flag = [&](int32_t &dst) {
+    if (parse_bool(value, b)) dst = b; else R.bad(full, value);
+  };
+  if (param == "enabled") {
+    if (parse_bool(value, b)) pr->enabled = b; else R.bad(full, value);
+  } else if (param == "position") vec(q.position);
+  else if (param == "rotation") vec(q.rotation);
+  else if (param == "repeat") vec(q.repeat);
+  else if (param == "size") vec(q.size);
+  else if (param == "limits_min") vec(q.limits_min);
+  else if (param == "limits_max") vec(q.limits_max);
+  else if (param == "scale") num(q.scale);
+  else if (param == "radius") num(q.radius);
+  else if (param == "height") num(q.height);
+  else if (param == "width") num(q.width);
+  else if (param == "tube_radius") num(q.tube_radius);
+  else if (param == "radius_lpow") num(q.radius_lpow);
+  else if (param == "tube_radius_lpow") num(q.tube_radius_lpow);
+  else if (param == "rounding") num(q.rounding);
+  else if (param == "wall_thickness") num(q.wall_thickness);
+  else if (param == "relative_amplitude") num(q.relative_amplitude);
+  else if (param == "length") num(q.length);
+  else if (param == "anim_speed") num(q.anim_speed);
+  else if (param == "anim_progression_speed") num(q.anim_progression_speed);
+  else if (param == "empty") flag(q.empty);
+  else if (param == "limits_enable") flag(q.limits_enable);
+  else if (param == "caps") flag(q.caps);
+  else if (param == "iterations") {
+    if (parse_int(value, b)) q.iterations = b; else R.bad(full, value);
+  } else if (param == "boolean_operator") {
+    if (parse_int(value, b)) pr->boolean_operator = b; else R.bad(full, value);
+  } else if (param == "smooth_de_combine_enable") {
+    if (parse_bool(value, b)) pr->smooth = b; else R.bad(full, value);
+  } else if (param == "wave_from_objects_enable" || param == "wave_from_objects_relative_amplitude") {
+    // the water's distance from other objects is 1e20 in the objects-tree walk
+    // (calculate_distance.cpp:385-396): the wave from objects has no effect
+    R.ignored.push_back(full);
+  } else {
+    // material, colour, reflection, name, object id, calculation order,
+    // smooth-combine distance: shading or tree bookkeeping
+    R.ignored.push_back(full);
   }
 }
 
@@ -405,7 +515,11 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     }
   }
   if (starts_with(name, "primitive_")) {
-    R.unsupported.push_back(name + " (primitive object)");
+    read_primitive_param(R, name, value);
+    return;
+  }
+  if (name == "frame_no") {
+    if (!parse_int(value, b)) R.bad(name, value); else R.frame_no = b;
     return;
   }
   if (starts_with(name, "node_")) {
@@ -693,6 +807,40 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
       R.unsupported.push_back("fractal_" + std::to_string(i + 1) + " rotations (Mandelbox rotations in a hybrid)");
   }
   if (!R.hybrid && R.formula[0] == MBR_FORMULA_NONE) R.unsupported.push_back("formula_1 0 (no fractal)");
+  // enabled primitives join the fractal by union (MigrateToObjectsTree, settings.cpp:2866-2940)
+  scene->n_primitives = 0;
+  for (const PrimRead &pr : R.prims) {
+    if (!pr.enabled) continue;
+    const std::string nm = "primitive_" + pr.key;
+    if (pr.type == 0) {
+      R.unsupported.push_back(nm + " (primitive " + pr.type_name + " not built here)");
+      continue;
+    }
+    if (pr.boolean_operator != 1) {
+      R.unsupported.push_back(nm + "_boolean_operator " + std::to_string(pr.boolean_operator) +
+                              " (primitive combined other than by union)");
+      continue;
+    }
+    if (pr.smooth) {
+      R.unsupported.push_back(nm + "_smooth_de_combine_enable (smooth union)");
+      continue;
+    }
+    if (pr.type == MBR_PRIMITIVE_WATER && pr.q.length == 0.0) {
+      R.unsupported.push_back(nm + "_length 0 (water of zero wave length)");
+      continue;
+    }
+    if (scene->n_primitives == MBR_MAX_PRIMITIVES) {
+      R.unsupported.push_back(nm + " (more than " + std::to_string(MBR_MAX_PRIMITIVES) + " primitives)");
+      continue;
+    }
+    if (pr.q.iterations < 0 || pr.q.iterations > 100) {
+      R.unsupported.push_back(nm + "_iterations " + std::to_string(pr.q.iterations) + " (outside 0..100)");
+      continue;
+    }
+    mbr_primitive q = pr.q;
+    q.frame_no = R.frame_no;
+    scene->primitive[scene->n_primitives++] = q;
+  }
   // the node's iteration limit is the main N (CopyFractalParams, settings.cpp:2494-2501; the hybrid root :2775-2778)
   scene->formula_maxiter = R.N;
 

@@ -86,6 +86,24 @@ constexpr int F_EXT = -1;
 struct DevScene;
 __host__ __device__ inline bool scene_extended(const DevScene &sc);
 
+// One primitive of the union in the form its distance reads: the node's
+// world-to-local matrix and scale (objects_tree.cpp:290-385,
+// CMatrix44::InverseAffine) and the primitive's own fields (primitive.cpp),
+// built on the host.
+struct DevPrim {
+  int32_t type, empty, limits, caps;
+  int32_t iterations, has_repeat;
+  double m[12];         // worldToLocalMatrix rows 1-3: m11 m12 m13 m14, m21 ...
+  double abs_scale;     // |world scale|: a local distance times this is a world distance
+  double repeat[3];     // repeat period / abs_scale
+  double size[3];       // box
+  double radius, height, width, tube;
+  double pow_r, pow_t;  // torus: pow(2, radius_lpow), pow(2, tube_radius_lpow)
+  double rounding, wall;
+  double lmin[3], lmax[3];
+  double amp, length, phase, xshift;  // water: length * relative amplitude, animation phase and drift
+};
+
 struct DevScene {
   int32_t n;
   int32_t is_hybrid;
@@ -112,11 +130,14 @@ struct DevScene {
   DevSlot slot[MBR_MAX_FRACTALS];
   MbRot mbrot;             // zero (no rotations) unless slot 0 is a rotated Mandelbox
   IfsBlock ifs;            // slot 0 of a kaleidoscopic IFS scene
+  int32_t n_prims;         // primitives joined by union (F_EXT iteration only)
+  int32_t pad2;
+  DevPrim prim[MBR_MAX_PRIMITIVES];
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 
 __host__ __device__ inline bool scene_extended(const DevScene &sc) {
-  return sc.generic || sc.mbrot.folds || sc.mbrot.main;
+  return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0;
 }
 
 // Everything about one frame that is not the scene: camera, march and

@@ -118,6 +118,91 @@ static void mandelbox_rotation(const double deg[3], double m[9], bool *zero, boo
   }
 }
 
+static void rotate_axis(double *m, bool *zero, int axis, double angle);
+
+// A primitive's node as the distance reads it: localToWorld = [R^T s | t] with
+// R from SetRotation2(rotation * pi/180), accumulated under identity parents,
+// then InverseAffine (objects_tree.cpp:290-385, algebra.cpp:477-576).
+static bool build_prim(const mbr_primitive &q, DevPrim *o) {
+  std::memset(o, 0, sizeof(*o));
+  const bool finite = finite3(q.position) && finite3(q.rotation) && finite3(q.repeat) && finite3(q.size) &&
+                      finite3(q.limits_min) && finite3(q.limits_max) && std::isfinite(q.scale) &&
+                      std::isfinite(q.radius) && std::isfinite(q.height) && std::isfinite(q.width) &&
+                      std::isfinite(q.tube_radius) && std::isfinite(q.radius_lpow) &&
+                      std::isfinite(q.tube_radius_lpow) && std::isfinite(q.rounding) &&
+                      std::isfinite(q.wall_thickness) && std::isfinite(q.relative_amplitude) &&
+                      std::isfinite(q.length) && std::isfinite(q.anim_speed) &&
+                      std::isfinite(q.anim_progression_speed);
+  if (!finite || !(std::fabs(q.scale) > 1e-12) || q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_RECTANGLE ||
+      q.iterations < 0 || q.iterations > 100)
+    return false;
+  if (q.type == MBR_PRIMITIVE_WATER && !(q.length != 0.0)) return false;
+  double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  bool zero = true;
+  const double k = kPi / 180.0;
+  rotate_axis(R, &zero, 2, q.rotation[2] * k);
+  rotate_axis(R, &zero, 1, q.rotation[1] * k);
+  rotate_axis(R, &zero, 0, q.rotation[0] * k);
+  const double sc = q.scale;
+  const double L[16] = {R[0] * sc, R[3] * sc, R[6] * sc, q.position[0],  //
+                        R[1] * sc, R[4] * sc, R[7] * sc, q.position[1],  //
+                        R[2] * sc, R[5] * sc, R[8] * sc, q.position[2],  //
+                        0.0,       0.0,       0.0,       1.0};
+  static const double I[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  double W[16];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++)
+      W[r * 4 + c] = I[r * 4 + 0] * L[c] + I[r * 4 + 1] * L[4 + c] + I[r * 4 + 2] * L[8 + c] + I[r * 4 + 3] * L[12 + c];
+  const double ws = std::sqrt(W[0] * W[0] + W[1] * W[1] + W[2] * W[2]);
+  const double s2 = ws * ws;
+  if (ws > 1e-12) {
+    o->m[0] = W[0] / s2;
+    o->m[1] = W[4] / s2;
+    o->m[2] = W[8] / s2;
+    o->m[4] = W[1] / s2;
+    o->m[5] = W[5] / s2;
+    o->m[6] = W[9] / s2;
+    o->m[8] = W[2] / s2;
+    o->m[9] = W[6] / s2;
+    o->m[10] = W[10] / s2;
+  }
+  const double tx = W[3], ty = W[7], tz = W[11];
+  o->m[3] = -(W[0] * tx + W[4] * ty + W[8] * tz) / s2;
+  o->m[7] = -(W[1] * tx + W[5] * ty + W[9] * tz) / s2;
+  o->m[11] = -(W[2] * tx + W[6] * ty + W[10] * tz) / s2;
+  o->abs_scale = std::fabs(ws);
+  for (int i = 0; i < 3; i++) o->repeat[i] = q.repeat[i] / o->abs_scale;
+  o->has_repeat = std::sqrt(o->repeat[0] * o->repeat[0] + o->repeat[1] * o->repeat[1] + o->repeat[2] * o->repeat[2]) > 0.0;
+  o->type = q.type;
+  o->empty = q.empty ? 1 : 0;
+  // the plane, circle and rectangle have no limits box (primitive.cpp:459-465, 513-520, 539-545)
+  o->limits = (q.limits_enable && q.type != MBR_PRIMITIVE_PLANE && q.type != MBR_PRIMITIVE_CIRCLE &&
+               q.type != MBR_PRIMITIVE_RECTANGLE)
+                  ? 1
+                  : 0;
+  o->caps = q.caps ? 1 : 0;
+  o->iterations = q.iterations;
+  for (int i = 0; i < 3; i++) {
+    o->size[i] = q.size[i];
+    o->lmin[i] = q.limits_min[i];
+    o->lmax[i] = q.limits_max[i];
+  }
+  o->radius = q.radius;
+  o->height = q.height;
+  o->width = q.width;
+  o->tube = q.tube_radius;
+  o->pow_r = std::pow(2.0, q.radius_lpow);
+  o->pow_t = std::pow(2.0, q.tube_radius_lpow);
+  o->rounding = q.rounding;
+  o->wall = q.wall_thickness;
+  // water (primitive.cpp:172-191, 583-603)
+  o->amp = q.length * q.relative_amplitude;
+  o->length = q.length;
+  o->phase = -q.anim_speed * double(q.frame_no) * 0.1;
+  o->xshift = o->phase * 0.05 * (q.anim_progression_speed * 3.0 - 3.0);
+  return true;
+}
+
 // ---- scene -------------------------------------------------------------------
 // Validates `sc` and flattens it into a DevScene.  Restates CollectSequenceData
 // and CreateSequence for the single fractal (or hybrid) node of the default
@@ -363,6 +448,16 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   }
   d.linear_de_offset = sc.linear_de_offset;
   d.flinear_de_offset = float(sc.linear_de_offset);
+  if (sc.n_primitives < 0 || sc.n_primitives > MBR_MAX_PRIMITIVES)
+    return set_err(ctx, MBR_EINVAL, "n_primitives must be in [0, %d], got %d", MBR_MAX_PRIMITIVES, sc.n_primitives);
+  for (int k = 0; k < sc.n_primitives; k++)
+    if (!build_prim(sc.primitive[k], &d.prim[k]))
+      return set_err(ctx, MBR_EINVAL,
+                     "primitive %d: type must be 1..8, every value finite, |scale| > 1e-12, iterations in "
+                     "[0, 100] and a water length != 0",
+                     k);
+  d.n_prims = sc.n_primitives;
+  if (d.n_prims > 0) d.generic = 1;  // the union is evaluated by the reference-order iteration only
   *out = d;
   return MBR_OK;
 }
@@ -653,6 +748,33 @@ void mbr_destroy(mbr_ctx *ctx) {
 }
 
 const char *mbr_last_error_string(const mbr_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void mbr_primitive_defaults(mbr_primitive *q, int type) {
+  if (!q) return;
+  std::memset(q, 0, sizeof(*q));
+  // InitPrimitiveParams (src/initparameters.cpp:1313-1420) and the legacy
+  // node transform defaults (src/settings.cpp:2217-2241)
+  q->type = type;
+  q->caps = 1;
+  q->iterations = 5;
+  q->scale = 1.0;
+  for (int i = 0; i < 3; i++) {
+    q->size[i] = 1.0;
+    q->limits_min[i] = -0.7;
+    q->limits_max[i] = 0.7;
+  }
+  q->radius = 1.0;
+  q->height = 1.0;
+  q->width = 1.0;
+  q->tube_radius = 0.2;
+  q->radius_lpow = 1.0;
+  q->tube_radius_lpow = 1.0;
+  q->rounding = 1e-15;
+  q->relative_amplitude = 0.2;
+  q->length = 0.1;
+  q->anim_speed = 1.0;
+  q->anim_progression_speed = 1.0;
+}
 
 void mbr_fractal_defaults(mbr_fractal *f, int formula) {
   if (!f) return;

@@ -529,6 +529,12 @@ struct PrecHybT {
     if (iters < sc.min_n && d < detail) d = detail;
     if (d < 0.0f) d = 0.0f;
     if (d > 10.0f) d = 10.0f;
+    if (EXT) {  // the union with the primitives, at the request point c
+      for (int k = 0; k < sc.n_prims; k++) {
+        const float pd = prim_distance<float>(sc.prim[k], e.cx, e.cy, e.cz);
+        if (pd < d) d = pd;
+      }
+    }
     return d;
   }
 };

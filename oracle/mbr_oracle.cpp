@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -81,7 +82,16 @@ struct Slot {
   double mb_main_deg[3] = {0, 0, 0};          // rotationMain, degrees
   mbr_fractal ifs = {};                       // the IFS_* parameters (fractal.cpp:96-115)
 };
+// A primitive of the union with its node transform (objects_tree.cpp:290-385).
+struct OPrim {
+  mbr_primitive q;
+  double w2l[12];  // worldToLocalMatrix rows 1-3 (CMatrix44::InverseAffine, algebra.cpp:528-576)
+  double abs_scale;
+  double repeat[3];  // node repeat / absScale (calculate_distance.cpp:277-282)
+};
+
 struct Seq {
+  std::vector<OPrim> prims;
   bool is_hybrid = false, julia = false;
   int length = 0, n = 0, formula_maxiter = 250, min_n = 1;
   int de_function = 1, de_analytic = 1;
@@ -90,6 +100,8 @@ struct Seq {
   std::vector<int> seq;
   Slot slot[MBR_MAX_FRACTALS];
 };
+
+static bool build_prim(const mbr_primitive &q, OPrim *o);
 
 // Returns false for scenes the restatement does not cover.
 static bool build_sequence(const mbr_scene &sc, Seq *out) {
@@ -221,6 +233,12 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     }
   }
   if (s.de_function != 1 && s.de_function != 2) return false;
+  if (sc.n_primitives < 0 || sc.n_primitives > MBR_MAX_PRIMITIVES) return false;
+  for (int k = 0; k < sc.n_primitives; k++) {
+    OPrim op;
+    if (!build_prim(sc.primitive[k], &op)) return false;
+    s.prims.push_back(op);
+  }
   *out = s;
   return true;
 }
@@ -248,8 +266,8 @@ inline int sgn(double v) { return (0.0 < v) - (v < 0.0); }  // math_utilities.h:
 // RotateX(x), each post-multiplying the matrix and skipped for a zero angle;
 // `zero` stays set (RotateVector is the identity) when all three are zero.
 // set3: SetRotation3 instead (algebra.cpp:304-310): RotateZ(x), RotateY(y), RotateX(z).
-inline void mb_rotation(const double deg[3], double m[9], bool *zero, bool set3 = false) {
-  const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
+inline void mb_rotation(const double deg[3], double m[9], bool *zero, bool set3 = false,
+                        double k = 0.01745329251994329576923690768489 /* M_PI_180, fractal.h:45-46 */) {
   for (int i = 0; i < 9; i++) m[i] = (i % 4 == 0) ? 1.0 : 0.0;
   *zero = true;
   const double ang[3] = {deg[set3 ? 0 : 2] * k, deg[1] * k, deg[set3 ? 2 : 0] * k};
@@ -269,6 +287,166 @@ inline void mb_rotation(const double deg[3], double m[9], bool *zero, bool set3 
     std::memcpy(m, t, sizeof(t));
     *zero = false;
   }
+}
+
+// The legacy settings put every enabled primitive in a node under identity
+// boolean groups (settings.cpp:2551-2940); the node's localToWorld is
+// [R^T s | position] with R = SetRotation2(rotation * M_PI / 180), its world
+// matrix identity * localToWorld (algebra.cpp:477-500), and the distance
+// reads InverseAffine of that (objects_tree.cpp:290-385).
+static bool build_prim(const mbr_primitive &q, OPrim *o) {
+  if (q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_RECTANGLE) return false;
+  o->q = q;
+  double R[9];
+  bool zero;
+  mb_rotation(q.rotation, R, &zero, false, M_PI / 180.0);
+  const double s = q.scale;
+  double L[4][4] = {{R[0] * s, R[3] * s, R[6] * s, q.position[0]},
+                    {R[1] * s, R[4] * s, R[7] * s, q.position[1]},
+                    {R[2] * s, R[5] * s, R[8] * s, q.position[2]},
+                    {0.0, 0.0, 0.0, 1.0}};
+  double W[4][4];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      const double I[4] = {r == 0 ? 1.0 : 0.0, r == 1 ? 1.0 : 0.0, r == 2 ? 1.0 : 0.0, r == 3 ? 1.0 : 0.0};
+      W[r][c] = I[0] * L[0][c] + I[1] * L[1][c] + I[2] * L[2][c] + I[3] * L[3][c];
+    }
+  const double ws = sqrt(W[0][0] * W[0][0] + W[0][1] * W[0][1] + W[0][2] * W[0][2]);
+  const double sSq = ws * ws;
+  double *m = o->w2l;
+  for (int i = 0; i < 12; i++) m[i] = 0.0;
+  if (ws > 1e-12) {
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) m[r * 4 + c] = W[c][r] / sSq;
+  }
+  for (int r = 0; r < 3; r++) m[r * 4 + 3] = -(W[0][r] * W[0][3] + W[1][r] * W[1][3] + W[2][r] * W[2][3]) / sSq;
+  o->abs_scale = fabs(ws);
+  for (int i = 0; i < 3; i++) o->repeat[i] = q.repeat[i] / o->abs_scale;
+  return true;
+}
+
+// std::max
+static inline double dmax(double a, double b) { return (a < b) ? b : a; }
+
+// Limits box of a primitive (primitive.cpp, e.g. :490-495)
+static inline double limit_box(const mbr_primitive &q, double x, double y, double z, double dist) {
+  if (!q.limits_enable) return dist;
+  const double ax = dmax(x - q.limits_max[0], q.limits_min[0] - x);
+  const double ay = dmax(y - q.limits_max[1], q.limits_min[1] - y);
+  const double az = dmax(z - q.limits_max[2], q.limits_min[2] - z);
+  return dmax(dist, dmax(dmax(ax, ay), az));
+}
+
+// The primitive's distance at a world point: node transform and repeat
+// (calculate_distance.cpp:268-282), PrimitiveDistance (primitive.cpp:459-686;
+// the water's distance from another object is the leaf's initial 1e20,
+// :385-396, so its wave-from-objects terms vanish), times the node scale.
+static double prim_distance(const OPrim &op, double wx, double wy, double wz) {
+  const mbr_primitive &q = op.q;
+  const double *m = op.w2l;
+  double x = m[0] * wx + m[1] * wy + m[2] * wz + m[3];
+  double y = m[4] * wx + m[5] * wy + m[6] * wz + m[7];
+  double z = m[8] * wx + m[9] * wy + m[10] * wz + m[11];
+  const double *v = op.repeat;
+  if (sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) > 0.0) {  // CVector3::repeatMod (algebra.hpp:106-115)
+    double *c[3] = {&x, &y, &z};
+    for (int i = 0; i < 3; i++) {
+      double t = *c[i] - v[i] * 0.5;
+      t = (v[i] > 0.0) ? fmod(t, v[i]) : t;
+      t = t + v[i];
+      t = (v[i] > 0.0) ? fmod(t, v[i]) : t;
+      *c[i] = t - v[i] * 0.5;
+    }
+  }
+  double dist = 0.0;
+  switch (q.type) {
+    case MBR_PRIMITIVE_PLANE:  // :459-465
+      dist = z;
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      break;
+    case MBR_PRIMITIVE_BOX: {  // :467-497
+      double boxDist = -1e10;
+      if (q.empty) {
+        boxDist = dmax(fabs(x) - q.size[0] * 0.5, boxDist);
+        boxDist = dmax(fabs(y) - q.size[1] * 0.5, boxDist);
+        boxDist = dmax(fabs(z) - q.size[2] * 0.5, boxDist);
+        boxDist = fabs(boxDist);
+      } else {
+        const double bx = dmax(fabs(x) - q.size[0] * 0.5, 0.0);
+        const double by = dmax(fabs(y) - q.size[1] * 0.5, 0.0);
+        const double bz = dmax(fabs(z) - q.size[2] * 0.5, 0.0);
+        boxDist = sqrt(bx * bx + by * by + bz * bz) - q.rounding;
+      }
+      boxDist = dmax(boxDist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, boxDist);
+      break;
+    }
+    case MBR_PRIMITIVE_SPHERE:  // :499-511
+      dist = sqrt(x * x + y * y + z * z) - q.radius;
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, dist);
+      break;
+    case MBR_PRIMITIVE_RECTANGLE: {  // :513-520
+      const double bx = dmax(fabs(x) - q.width * 0.5, 0.0);
+      const double by = dmax(fabs(y) - q.height * 0.5, 0.0);
+      const double bz = fabs(z);
+      dist = sqrt(bx * bx + by * by + bz * bz);
+      break;
+    }
+    case MBR_PRIMITIVE_CYLINDER:  // :522-537
+      dist = sqrt(x * x + y * y) - q.radius;
+      if (!q.caps) dist = fabs(dist);
+      dist = dmax(fabs(z) - q.height * 0.5, dist);
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, dist);
+      break;
+    case MBR_PRIMITIVE_CIRCLE:  // :539-545
+      dist = dmax(fabs(z), sqrt(x * x + y * y) - q.radius);
+      break;
+    case MBR_PRIMITIVE_TORUS: {  // :640-655, CVector2::LengthPow (algebra.hpp:538)
+      const double pr = pow(2, q.radius_lpow), pt = pow(2, q.tube_radius_lpow);
+      const double d1 = pow(pow(x, pr) + pow(y, pr), 1.0 / pr) - q.radius;
+      dist = pow(pow(d1, pt) + pow(z, pt), 1.0 / pt) - q.tube_radius;
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, dist);
+      break;
+    }
+    case MBR_PRIMITIVE_WATER: {  // :572-638
+      const double length = q.length;
+      const double amplitude = length * q.relative_amplitude;
+      double planeDistance = z;
+      if (planeDistance < amplitude * 10.0) {
+        const double phase = -q.anim_speed * q.frame_no * 0.1;
+        const double k = 0.23;
+        double waveX = 0.0, waveY = -0.0, p = 1.0, p2 = 0.05;
+        x += phase * 0.05 * (q.anim_progression_speed * 3.0 - 3.0);
+        for (int i = 1; i <= q.iterations; i++) {
+          const float p3 = p * p2;
+          const float shift = phase / (i / 2.697 + 1.0);
+          const double waveXTemp =
+              sin(i + 0.4 * (waveX)*p3 + sin(k * y / length * p3 + shift * 0.134 * p3) + x / length * p3 + shift * p3) / p;
+          const double waveYTemp =
+              cos(i + 0.4 * (waveY)*p3 + sin(x / length * p3 + shift * 0.0179 * p3) + k * y / length * p3 +
+                  shift * 0.023 * p3) /
+              p;
+          waveX += waveXTemp;
+          waveY += waveYTemp;
+          p2 = p2 + (1.0 - p2 + 0.5 * sin(shift * 0.0323)) * 0.7;
+          p *= 1.872;
+        }
+        planeDistance += (waveX + waveY) * amplitude;
+      }
+      planeDistance = q.empty ? fabs(planeDistance) : planeDistance;
+      planeDistance = dmax(planeDistance - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, planeDistance);
+      break;
+    }
+  }
+  return dist * op.abs_scale;
 }
 
 // Formula parameters in the scalar type, so tangents can be seeded.
@@ -700,6 +878,12 @@ S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double 
   }
   if (distance < 0.0) distance = 0.0;
   if (distance > 10.0) distance = 10.0;
+  if constexpr (std::is_same<S, double>::value) {  // booleanAdd with the primitives (calculate_distance.cpp:166-201)
+    for (const OPrim &op : seq.prims) {
+      const double pd = prim_distance(op, px, py, pz);
+      if (pd < distance) distance = pd;
+    }
+  }
   return distance;
 }
 

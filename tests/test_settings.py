@@ -79,6 +79,41 @@ def test_mandelbox_with_ao():
     assert p.penetrating == 0 and p.soft_shadow_cone == 0.0  # light1_penetrating false, cone 0
 
 
+def test_primitives():
+    """Enabled primitives join the fractal by union; a water of a file before
+    2.13 reads its amplitude as the relative amplitude (settings.cpp:1365-1372);
+    a disabled primitive of a kind not built here is skipped."""
+    s = settings.load_from_file(os.path.join(FIX, "box_primitives.fract"))
+    assert s.ok, s.report
+    sc = s.scene
+    assert sc.n_primitives == 3
+    w, sp, bx = sc.primitive[0], sc.primitive[1], sc.primitive[2]
+    assert w.type == abi.PRIMITIVE_WATER and list(w.position) == [0.0, 0.0, -2.2] and list(w.rotation) == [0, 0, 15]
+    assert w.relative_amplitude == 0.25 and w.length == 0.4 and w.iterations == 4 and w.anim_speed == 1.0
+    assert sp.type == abi.PRIMITIVE_SPHERE and sp.radius == 0.7 and list(sp.position) == [2.1, 0.6, -0.4]
+    assert bx.type == abi.PRIMITIVE_BOX and list(bx.size) == [0.8, 1.2, 0.6] and bx.rounding == 0.05
+    assert list(bx.rotation) == [10.0, 0.0, 35.0] and bx.scale == 1.0 and list(bx.repeat) == [0.0] * 3
+    assert "primitive_water_1_material_id" in s.report  # ignored: a material
+
+
+@pytest.mark.parametrize("lines,what", [
+    ("primitive_cone_1_enabled true;\n", "primitive cone not built here"),
+    ("primitive_sphere_1_enabled true;\nprimitive_sphere_1_boolean_operator 2;\n", "other than by union"),
+    ("primitive_box_1_enabled true;\nprimitive_box_1_smooth_de_combine_enable true;\n", "smooth union"),
+])
+def test_primitives_not_built_here(lines, what):
+    s = settings.load_from_string(HEADER + "[main_parameters]\n" + lines)
+    assert s.status == abi.MBR_EUNSUPPORTED and any(what in u for u in s.unsupported()), s.report
+
+
+def test_nine_primitives_are_too_many():
+    txt = HEADER + "[main_parameters]\n" + "".join(
+        f"primitive_sphere_{i}_enabled true;\nprimitive_sphere_{i}_position {i} 0 0;\n" for i in range(1, 10))
+    s = settings.load_from_string(txt)
+    assert s.status == abi.MBR_EUNSUPPORTED and s.scene.n_primitives == 8
+    assert any("more than 8 primitives" in u for u in s.unsupported())
+
+
 def test_hybrid_sequence():
     s = settings.load_from_file(os.path.join(FIX, "hybrid_bulb_menger.fract"))
     assert s.status == abi.MBR_OK, s.report
@@ -171,13 +206,13 @@ def test_unsupported_geometry_is_named():
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
-    txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_sphere_1_enabled true;\nboolean_operators true;\n"
+    txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nboolean_operators true;\n"
                     "delta_DE_method 1;\nhybrid_fractal_enable true;\n"
                     "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
-    for key in ("primitive_sphere_1_enabled", "boolean_operators",
+    for key in ("primitive_prism_1 (primitive prism not built here)", "boolean_operators",
                 "delta_DE_method 1", "Mandelbox rotations in a hybrid"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
@@ -270,7 +305,7 @@ def test_reference_examples():
             assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
         elif not formulas <= {2, 3, 4, 7, 8, 10, 11}:
             assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
-    assert ok >= 60, ok
+    assert ok >= 180, ok
 
 
 @pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
