@@ -16,7 +16,8 @@ FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "settin
 NAMES = ("depth", "iters", "hit", "normal", "ao", "rgb8")
 
 
-@pytest.mark.parametrize("name", ["box_ao.fract", "hybrid_bulb_menger.fract", "legacy_light.fract"])
+@pytest.mark.parametrize("name", ["box_ao.fract", "hybrid_bulb_menger.fract", "legacy_light.fract",
+                                  "box_primitives.fract"])
 def test_settings_scene_vs_oracle(renderer, oracle, name):
     s = settings.load_from_file(os.path.join(FIX, name))
     assert s.ok, s.report
