@@ -566,6 +566,9 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     if (parse_bool(value, b)) sc->iteration_threshold_mode = b; else R.bad(name, value);
   } else if (name == "interior_mode") {
     if (parse_bool(value, b)) sc->interior_mode = b; else R.bad(name, value);
+  } else if (name == "all_primitives_position" || name == "all_primitives_rotation") {
+    // the transform of the group that holds the primitives (settings.cpp:3113-3117)
+    if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (primitive group transform)");
   } else if (name == "fractal_position" || name == "fractal_rotation" || name == "repeat") {
     if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (fractal transform)");
   } else if (name == "formula_code") {

@@ -100,6 +100,7 @@ def test_primitives():
     ("primitive_cone_1_enabled true;\n", "primitive cone not built here"),
     ("primitive_sphere_1_enabled true;\nprimitive_sphere_1_boolean_operator 2;\n", "other than by union"),
     ("primitive_box_1_enabled true;\nprimitive_box_1_smooth_de_combine_enable true;\n", "smooth union"),
+    ("primitive_box_1_enabled true;\nall_primitives_rotation 0 0 10;\n", "primitive group transform"),
 ])
 def test_primitives_not_built_here(lines, what):
     s = settings.load_from_string(HEADER + "[main_parameters]\n" + lines)
