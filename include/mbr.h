@@ -173,7 +173,10 @@ typedef enum mbr_primitive_type {
   MBR_PRIMITIVE_TORUS = 5,     /* radius, tube radius, their L-powers (sPrimitiveTorus, :640-655) */
   MBR_PRIMITIVE_CYLINDER = 6,  /* radius, height, caps (sPrimitiveCylinder, :522-537) */
   MBR_PRIMITIVE_CIRCLE = 7,    /* flat disc of radius (sPrimitiveCircle, :539-545) */
-  MBR_PRIMITIVE_RECTANGLE = 8  /* flat width x height (sPrimitiveRectangle, :513-520) */
+  MBR_PRIMITIVE_RECTANGLE = 8, /* flat width x height (sPrimitiveRectangle, :513-520) */
+  MBR_PRIMITIVE_CONE = 9,      /* radius, height, caps (sPrimitiveCone, :547-564) */
+  MBR_PRIMITIVE_PRISM = 10,    /* prism angle, triangle height, height (sPrimitivePrism, :657-668) */
+  MBR_PRIMITIVE_ELLIPSOID = 11 /* size (sPrimitiveEllipsoid, :670-686) */
 } mbr_primitive_type;
 
 /* One primitive (the legacy primitive_<type>_<n>_* parameters,
@@ -191,21 +194,23 @@ typedef struct mbr_primitive {
   double rotation[3];         /* degrees */
   double scale;               /* default 1 */
   double repeat[3];           /* tiling period, 0 = none */
-  double size[3];             /* box: default (1,1,1) */
-  double radius;              /* sphere, torus, cylinder, circle: default 1 */
-  double height;              /* cylinder, rectangle: default 1 */
+  double size[3];             /* box: default (1,1,1); ellipsoid: default (1,0.5,0.5) */
+  double radius;              /* sphere, torus, cylinder, circle, cone: default 1 */
+  double height;              /* cylinder, rectangle, cone, prism: default 1 */
   double width;               /* rectangle: default 1 */
   double tube_radius;         /* torus: default 0.2 */
   double radius_lpow;         /* torus: L-power exponent log2, default 1 */
   double tube_radius_lpow;    /* torus: default 1 */
   double rounding;            /* box: default 1e-15 */
   double wall_thickness;      /* default 0 */
-  double limits_min[3];       /* default (-0.7,-0.7,-0.7) */
-  double limits_max[3];       /* default (0.7,0.7,0.7) */
+  double limits_min[3];       /* default (-0.7,-0.7,-0.7); ellipsoid (-1.4,-0.7,-0.7) */
+  double limits_max[3];       /* default (0.7,0.7,0.7); ellipsoid (1.4,0.7,0.7) */
   double relative_amplitude;  /* water: default 0.2 */
   double length;              /* water: default 0.1 */
   double anim_speed;          /* water: default 1 */
   double anim_progression_speed; /* water: default 1 */
+  double prism_angle;         /* prism: degrees, default 60 */
+  double triangle_height;     /* prism ("trangle_height"): default 1 */
 } mbr_primitive;
 
 /* The fractal part of a scene: one fractal (or hybrid) object node with the

@@ -27,7 +27,7 @@ FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS, FORM
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_primitive_type
 (PRIMITIVE_PLANE, PRIMITIVE_BOX, PRIMITIVE_SPHERE, PRIMITIVE_WATER, PRIMITIVE_TORUS, PRIMITIVE_CYLINDER,
- PRIMITIVE_CIRCLE, PRIMITIVE_RECTANGLE) = range(1, 9)
+ PRIMITIVE_CIRCLE, PRIMITIVE_RECTANGLE, PRIMITIVE_CONE, PRIMITIVE_PRISM, PRIMITIVE_ELLIPSOID) = range(1, 12)
 # mbr_de_function
 DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
 # mbr_engine
@@ -73,7 +73,8 @@ class Primitive(C.Structure):
         ("width", C.c_double), ("tube_radius", C.c_double), ("radius_lpow", C.c_double),
         ("tube_radius_lpow", C.c_double), ("rounding", C.c_double), ("wall_thickness", C.c_double),
         ("limits_min", D3), ("limits_max", D3), ("relative_amplitude", C.c_double), ("length", C.c_double),
-        ("anim_speed", C.c_double), ("anim_progression_speed", C.c_double),
+        ("anim_speed", C.c_double), ("anim_progression_speed", C.c_double), ("prism_angle", C.c_double),
+        ("triangle_height", C.c_double),
     ]
 
 

@@ -430,6 +430,28 @@ __device__ __noinline__ T prim_distance(const DevPrim &q, T wx, T wy, T wz) {
       d = pow(pow(d1, pt) + pow(z, pt), T(1.0) / pt) - T(q.tube);
       break;
     }
+    case MBR_PRIMITIVE_CONE: {  // primitive.cpp:547-564 (the shifted z also feeds the limits)
+      z = z - T(q.height);
+      const T r = sqrt(x * x + y * y);
+      d = T(q.wn[0]) * r + T(q.wn[1]) * z;
+      if (!q.caps) d = fabs(d);
+      d = smax(T(-z - T(q.height)), d);
+      break;
+    }
+    case MBR_PRIMITIVE_PRISM: {  // primitive.cpp:657-668
+      const T ax = fabs(x), az = fabs(z), tri = T(q.tri);
+      d = smax(T(az - T(q.height)), T(smax(T(ax * T(q.pn[1]) + y * T(q.pn[2])), T(-y + tri)) - tri));
+      break;
+    }
+    case MBR_PRIMITIVE_ELLIPSOID: {  // primitive.cpp:670-686: k0 and k1 are floats there
+      const T sx = T(q.size[0]), sy = T(q.size[1]), sz = T(q.size[2]);
+      const T ux = x / sx, uy = y / sy, uz = z / sz;
+      const T vx = x / (sx * sx), vy = y / (sy * sy), vz = z / (sz * sz);
+      const float k0 = float(sqrt(ux * ux + uy * uy + uz * uz));
+      const float k1 = float(sqrt(vx * vx + vy * vy + vz * vz));
+      d = T(double(k0) * (double(k0) - 1.0) / double(k1));
+      break;
+    }
     default: {  // MBR_PRIMITIVE_WATER: sPrimitiveWater::PrimitiveDistanceWater (primitive.cpp:572-638)
       const T amplitude = T(q.amp), len = T(q.length);
       d = z;

@@ -20,7 +20,7 @@
 // formulas and the hybrid sequence, the iteration and bailout settings,
 // camera, raymarching quality, the main light, AO and the 8-bit conversion.
 // Primitives joined by union (plane, box, sphere, water, torus, cylinder,
-// circle, rectangle) are read into mbr_scene.primitive.  Geometry this path
+// circle, rectangle, cone, prism, ellipsoid) are read into mbr_scene.primitive.  Geometry this path
 // does not build (other formulas, boolean combinations, other primitives or
 // operators, transforms, forced delta DE) makes the call
 // return MBR_EUNSUPPORTED with each item named in the report; shading
@@ -290,8 +290,8 @@ void read_primitive_param(Reader &R, const std::string &full, const std::string 
                  {"sphere", MBR_PRIMITIVE_SPHERE},     {"water", MBR_PRIMITIVE_WATER},
                  {"torus", MBR_PRIMITIVE_TORUS},       {"cylinder", MBR_PRIMITIVE_CYLINDER},
                  {"circle", MBR_PRIMITIVE_CIRCLE},     {"rectangle", MBR_PRIMITIVE_RECTANGLE},
-                 {"cone", 0},                          {"prism", 0},
-                 {"ellipsoid", 0}};
+                 {"cone", MBR_PRIMITIVE_CONE},         {"prism", MBR_PRIMITIVE_PRISM},
+                 {"ellipsoid", MBR_PRIMITIVE_ELLIPSOID}};
     int type = -1;
     for (const auto &k : kinds)
       if (tname == k.name) type = k.type;
@@ -340,6 +340,8 @@ void read_primitive_param(Reader &R, const std::string &full, const std::string 
   else if (param == "length") num(q.length);
   else if (param == "anim_speed") num(q.anim_speed);
   else if (param == "anim_progression_speed") num(q.anim_progression_speed);
+  else if (param == "prism_angle") num(q.prism_angle);
+  else if (param == "trangle_height") num(q.triangle_height);  // the reference's key
   else if (param == "empty") flag(q.empty);
   else if (param == "limits_enable") flag(q.limits_enable);
   else if (param == "caps") flag(q.caps);
@@ -815,10 +817,6 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
   for (const PrimRead &pr : R.prims) {
     if (!pr.enabled) continue;
     const std::string nm = "primitive_" + pr.key;
-    if (pr.type == 0) {
-      R.unsupported.push_back(nm + " (primitive " + pr.type_name + " not built here)");
-      continue;
-    }
     if (pr.boolean_operator != 1) {
       R.unsupported.push_back(nm + "_boolean_operator " + std::to_string(pr.boolean_operator) +
                               " (primitive combined other than by union)");
@@ -830,6 +828,14 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     }
     if (pr.type == MBR_PRIMITIVE_WATER && pr.q.length == 0.0) {
       R.unsupported.push_back(nm + "_length 0 (water of zero wave length)");
+      continue;
+    }
+    if (pr.type == MBR_PRIMITIVE_CONE && pr.q.height == 0.0) {
+      R.unsupported.push_back(nm + "_height 0 (flat cone)");
+      continue;
+    }
+    if (pr.type == MBR_PRIMITIVE_ELLIPSOID && !(pr.q.size[0] != 0.0 && pr.q.size[1] != 0.0 && pr.q.size[2] != 0.0)) {
+      R.unsupported.push_back(nm + "_size with a zero axis");
       continue;
     }
     if (scene->n_primitives == MBR_MAX_PRIMITIVES) {

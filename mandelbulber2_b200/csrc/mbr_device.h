@@ -102,6 +102,8 @@ struct DevPrim {
   double rounding, wall;
   double lmin[3], lmax[3];
   double amp, length, phase, xshift;  // water: length * relative amplitude, animation phase and drift
+  double wn[2];         // cone: the unit wall normal (1, radius / height) normalised
+  double pn[3], tri;    // prism: (sin a, cos a, sin a) of half its angle a, triangle height * sin a
 };
 
 struct DevScene {

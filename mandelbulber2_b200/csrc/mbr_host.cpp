@@ -132,10 +132,13 @@ static bool build_prim(const mbr_primitive &q, DevPrim *o) {
                       std::isfinite(q.tube_radius_lpow) && std::isfinite(q.rounding) &&
                       std::isfinite(q.wall_thickness) && std::isfinite(q.relative_amplitude) &&
                       std::isfinite(q.length) && std::isfinite(q.anim_speed) &&
-                      std::isfinite(q.anim_progression_speed);
-  if (!finite || !(std::fabs(q.scale) > 1e-12) || q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_RECTANGLE ||
+                      std::isfinite(q.anim_progression_speed) && std::isfinite(q.prism_angle) &&
+                      std::isfinite(q.triangle_height);
+  if (!finite || !(std::fabs(q.scale) > 1e-12) || q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_ELLIPSOID ||
       q.iterations < 0 || q.iterations > 100)
     return false;
+  if (q.type == MBR_PRIMITIVE_CONE && !(q.height != 0.0)) return false;
+  if (q.type == MBR_PRIMITIVE_ELLIPSOID && !(q.size[0] != 0.0 && q.size[1] != 0.0 && q.size[2] != 0.0)) return false;
   if (q.type == MBR_PRIMITIVE_WATER && !(q.length != 0.0)) return false;
   double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   bool zero = true;
@@ -175,9 +178,9 @@ static bool build_prim(const mbr_primitive &q, DevPrim *o) {
   o->has_repeat = std::sqrt(o->repeat[0] * o->repeat[0] + o->repeat[1] * o->repeat[1] + o->repeat[2] * o->repeat[2]) > 0.0;
   o->type = q.type;
   o->empty = q.empty ? 1 : 0;
-  // the plane, circle and rectangle have no limits box (primitive.cpp:459-465, 513-520, 539-545)
+  // the plane, circle, rectangle and prism have no limits box (primitive.cpp:459-465, 513-520, 539-545, 657-668)
   o->limits = (q.limits_enable && q.type != MBR_PRIMITIVE_PLANE && q.type != MBR_PRIMITIVE_CIRCLE &&
-               q.type != MBR_PRIMITIVE_RECTANGLE)
+               q.type != MBR_PRIMITIVE_RECTANGLE && q.type != MBR_PRIMITIVE_PRISM)
                   ? 1
                   : 0;
   o->caps = q.caps ? 1 : 0;
@@ -200,6 +203,23 @@ static bool build_prim(const mbr_primitive &q, DevPrim *o) {
   o->length = q.length;
   o->phase = -q.anim_speed * double(q.frame_no) * 0.1;
   o->xshift = o->phase * 0.05 * (q.anim_progression_speed * 3.0 - 3.0);
+  // cone: wallNormal = (1, radius / height), CVector2::Normalize (primitive.cpp:222-237, algebra.hpp:566-572)
+  o->wn[0] = 1.0;
+  o->wn[1] = q.type == MBR_PRIMITIVE_CONE ? q.radius / q.height : 0.0;
+  {
+    const double norm = 1.0 / std::sqrt(o->wn[0] * o->wn[0] + o->wn[1] * o->wn[1]);
+    o->wn[0] = o->wn[0] * norm;
+    o->wn[1] = o->wn[1] * norm;
+  }
+  // prism (primitive.cpp:380-393): half height, half angle, triangle height
+  if (q.type == MBR_PRIMITIVE_PRISM) {
+    o->height = q.height / 2.0;
+    const double a = q.prism_angle * kPi / 180.0 / 2.0;
+    o->tri = q.triangle_height * std::sin(a);
+    o->pn[0] = std::sin(a);
+    o->pn[1] = std::cos(a);
+    o->pn[2] = std::sin(a);
+  }
   return true;
 }
 
@@ -774,6 +794,13 @@ void mbr_primitive_defaults(mbr_primitive *q, int type) {
   q->length = 0.1;
   q->anim_speed = 1.0;
   q->anim_progression_speed = 1.0;
+  q->prism_angle = 60.0;
+  q->triangle_height = 1.0;
+  if (type == MBR_PRIMITIVE_ELLIPSOID) {
+    q->size[1] = q->size[2] = 0.5;
+    q->limits_min[0] = -1.4;
+    q->limits_max[0] = 1.4;
+  }
 }
 
 void mbr_fractal_defaults(mbr_fractal *f, int formula) {

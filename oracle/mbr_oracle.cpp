@@ -295,7 +295,7 @@ inline void mb_rotation(const double deg[3], double m[9], bool *zero, bool set3 
 // matrix identity * localToWorld (algebra.cpp:477-500), and the distance
 // reads InverseAffine of that (objects_tree.cpp:290-385).
 static bool build_prim(const mbr_primitive &q, OPrim *o) {
-  if (q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_RECTANGLE) return false;
+  if (q.type < MBR_PRIMITIVE_PLANE || q.type > MBR_PRIMITIVE_ELLIPSOID) return false;
   o->q = q;
   double R[9];
   bool zero;
@@ -410,6 +410,42 @@ static double prim_distance(const OPrim &op, double wx, double wy, double wz) {
       const double pr = pow(2, q.radius_lpow), pt = pow(2, q.tube_radius_lpow);
       const double d1 = pow(pow(x, pr) + pow(y, pr), 1.0 / pr) - q.radius;
       dist = pow(pow(d1, pt) + pow(z, pt), 1.0 / pt) - q.tube_radius;
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, dist);
+      break;
+    }
+    case MBR_PRIMITIVE_CONE: {  // :222-237 (wallNormal), :547-564
+      double wx2 = 1.0, wy2 = q.radius / q.height;
+      const double norm = 1.0 / sqrt(wx2 * wx2 + wy2 * wy2);
+      wx2 = wx2 * norm;
+      wy2 = wy2 * norm;
+      z -= q.height;
+      const double qq = sqrt(x * x + y * y);
+      dist = wx2 * qq + wy2 * z;
+      if (!q.caps) dist = fabs(dist);
+      dist = dmax(-z - q.height, dist);
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      dist = limit_box(q, x, y, z, dist);
+      break;
+    }
+    case MBR_PRIMITIVE_PRISM: {  // :380-393, :657-668
+      const double height = q.height / 2.0;
+      const double prismAngle = q.prism_angle * M_PI / 180.0 / 2.0;
+      const double triangleHeight = q.triangle_height * sin(prismAngle);
+      const double ny = cos(prismAngle), nz = sin(prismAngle);
+      dist = dmax(fabs(z) - height, dmax(fabs(x) * ny + y * nz, -y + triangleHeight) - triangleHeight);
+      dist = q.empty ? fabs(dist) : dist;
+      dist = dmax(dist - q.wall_thickness, 0.0);
+      break;
+    }
+    case MBR_PRIMITIVE_ELLIPSOID: {  // :670-686
+      const float k0 = sqrt((x / q.size[0]) * (x / q.size[0]) + (y / q.size[1]) * (y / q.size[1]) +
+                            (z / q.size[2]) * (z / q.size[2]));
+      const double s0 = q.size[0] * q.size[0], s1 = q.size[1] * q.size[1], s2 = q.size[2] * q.size[2];
+      const float k1 = sqrt((x / s0) * (x / s0) + (y / s1) * (y / s1) + (z / s2) * (z / s2));
+      dist = k0 * (k0 - 1.0) / k1;
       dist = q.empty ? fabs(dist) : dist;
       dist = dmax(dist - q.wall_thickness, 0.0);
       dist = limit_box(q, x, y, z, dist);

@@ -77,6 +77,25 @@ def test_ieee_primitives_vs_oracle(renderer, oracle):
     check_engines(renderer, sc, cam, p, o, ost, True, "ieee")
 
 
+def test_cone_prism_ellipsoid_vs_oracle(renderer, oracle):
+    """Cone and prism (host-built wall normals) and the ellipsoid (float
+    k0, k1 as in the reference) use IEEE operations only: strict bit-exact."""
+    sc, cam, p = scene_with([
+        prim(abi.PRIMITIVE_PLANE, position=[0, 0, -2.2]),
+        prim(abi.PRIMITIVE_CONE, position=[2.3, -1.2, -0.9], radius=0.5, height=1.0, rotation=[0, 10, 0]),
+        prim(abi.PRIMITIVE_PRISM, position=[-2.3, -1.2, -0.6], prism_angle=70.0, triangle_height=0.8, height=0.6,
+             rotation=[90, 0, 20]),
+        prim(abi.PRIMITIVE_ELLIPSOID, position=[0.0, -2.4, 1.0], size=[0.6, 0.3, 0.3], rotation=[0, 0, 30])])
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    for k in range(1, 4):  # every object changes the frame
+        s2 = abi.Scene.from_buffer_copy(sc)
+        s2.primitive[k].position[:] = [0.0, 0.0, 100.0]  # moved out of view
+        o2, _ = oracle.render(s2, cam, p)
+        assert np.mean(np.abs(o2["depth"] - o["depth"]) > 1e-6) > 0.002, k
+    check_engines(renderer, sc, cam, p, o, ost, True, "cone+prism+ellipsoid")
+
+
 def test_water_and_torus_vs_oracle(renderer, oracle):
     sc, cam, p = scene_with([
         prim(abi.PRIMITIVE_WATER, position=[0, 0, -1.9], rotation=[0, 0, 15], length=0.4, relative_amplitude=0.25,
@@ -107,8 +126,10 @@ def test_primitives_refused_where_not_built(renderer):
     with pytest.raises(MbrError) as e:
         renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP64, outputs=NAMES)
     assert e.value.status == abi.MBR_EUNSUPPORTED
-    bad = abi.Scene.from_buffer_copy(sc)
-    bad.primitive[0].scale = 0.0
-    with pytest.raises(MbrError) as e:
-        renderer.set_scene(bad)
-    assert e.value.status == abi.MBR_EINVAL
+    for field, kind, value in (("scale", abi.PRIMITIVE_PLANE, 0.0), ("height", abi.PRIMITIVE_CONE, 0.0)):
+        bad = abi.Scene.from_buffer_copy(sc)
+        bad.primitive[0] = prim(kind)
+        setattr(bad.primitive[0], field, value)
+        with pytest.raises(MbrError) as e:
+            renderer.set_scene(bad)
+        assert e.value.status == abi.MBR_EINVAL

@@ -94,6 +94,21 @@ def test_flat_and_round_shapes(oracle):
     np.testing.assert_allclose(d, [2.0, 2.0, 2.0, 3.0, math.hypot(2.0, 1.5) - 0.5, 0.0], rtol=0, atol=1e-9)
 
 
+def test_cone_prism_ellipsoid(oracle):
+    sc = with_prims(prim(abi.PRIMITIVE_CONE, position=[0, 0, 30], radius=1.0, height=2.0),
+                    prim(abi.PRIMITIVE_PRISM, position=[30, 0, 0], prism_angle=60.0, triangle_height=1.0, height=1.0),
+                    prim(abi.PRIMITIVE_ELLIPSOID, position=[-30, 0, 0], size=[2, 1, 1]))
+    d = dist(oracle, sc, [[0, 0, 35], [0, 0, 29], [30, 0, 3], [30, -2, 0], [-27, 0, 0]])
+    # above the apex: the distance to the wall's plane; below: to the base
+    np.testing.assert_allclose(d, [3 / math.sqrt(5), 1.0, 2.5, 2.0, 1.0], rtol=0, atol=1e-7)
+    cone = prim(abi.PRIMITIVE_CONE)
+    assert cone.radius == 1.0 and cone.height == 1.0 and cone.caps == 1
+    e = abi.primitive_defaults(abi.PRIMITIVE_ELLIPSOID)
+    assert list(e.size) == [1.0, 0.5, 0.5] and list(e.limits_max) == [1.4, 0.7, 0.7]
+    p = abi.primitive_defaults(abi.PRIMITIVE_PRISM)
+    assert p.prism_angle == 60.0 and p.triangle_height == 1.0
+
+
 def test_water_is_a_wavy_plane(oracle):
     sc = with_prims(prim(abi.PRIMITIVE_WATER, position=[0, 0, -2], length=0.5, relative_amplitude=0.2))
     rng = np.random.default_rng(3)

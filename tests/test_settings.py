@@ -82,7 +82,7 @@ def test_mandelbox_with_ao():
 def test_primitives():
     """Enabled primitives join the fractal by union; a water of a file before
     2.13 reads its amplitude as the relative amplitude (settings.cpp:1365-1372);
-    a disabled primitive of a kind not built here is skipped."""
+    a disabled primitive is skipped."""
     s = settings.load_from_file(os.path.join(FIX, "box_primitives.fract"))
     assert s.ok, s.report
     sc = s.scene
@@ -97,7 +97,7 @@ def test_primitives():
 
 
 @pytest.mark.parametrize("lines,what", [
-    ("primitive_cone_1_enabled true;\n", "primitive cone not built here"),
+    ("primitive_blob_1_enabled true;\n", "unknown primitive"),
     ("primitive_sphere_1_enabled true;\nprimitive_sphere_1_boolean_operator 2;\n", "other than by union"),
     ("primitive_box_1_enabled true;\nprimitive_box_1_smooth_de_combine_enable true;\n", "smooth union"),
     ("primitive_box_1_enabled true;\nall_primitives_rotation 0 0 10;\n", "primitive group transform"),
@@ -207,13 +207,14 @@ def test_unsupported_geometry_is_named():
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
-    txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nboolean_operators true;\n"
+    txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nprimitive_prism_1_boolean_operator 0;\n"
+                    "boolean_operators true;\n"
                     "delta_DE_method 1;\nhybrid_fractal_enable true;\n"
                     "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
-    for key in ("primitive_prism_1 (primitive prism not built here)", "boolean_operators",
+    for key in ("primitive_prism_1_boolean_operator 0", "boolean_operators",
                 "delta_DE_method 1", "Mandelbox rotations in a hybrid"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
