@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MBR_ABI_VERSION 2
+#define MBR_ABI_VERSION 3
 
 /* Number of formula slots of one hybrid sequence (the reference's nine
  * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
@@ -326,6 +326,19 @@ typedef struct mbr_render_params {
   int32_t ao_fast;              /* default 0 */
   int32_t ao_quality;           /* "ambient_occlusion_quality", default 4, 1..10 */
   double ao_fast_tune;          /* "ambient_occlusion_fast_tune", default 1 */
+  /* "advanced_quality" (sParamRender, src/fractparams.cpp:48-50, 112-113,
+   * 214-215): CalcDistThresh clamps the threshold to [detail_size_min,
+   * detail_size_max] (src/render_worker.cpp:671-675), and RayMarching limits
+   * each step by the absolute and relative bounds below instead of step <= 3
+   * (:819-834).  Defaults from src/initparameters.cpp:159-165. */
+  int32_t advanced_quality;     /* default 0 */
+  int32_t reserved_aq;
+  double detail_size_min;       /* default 1e-12 */
+  double detail_size_max;       /* default 1 */
+  double abs_min_marching_step; /* default 1e-15 */
+  double abs_max_marching_step; /* default 3 */
+  double rel_min_marching_step; /* default 1e-2 (times the threshold) */
+  double rel_max_marching_step; /* default 1e4 (times the threshold) */
 } mbr_render_params;
 
 /* Per-launch counters (src/statistics.h:42-70 mirrored).  A DE evaluation
@@ -398,7 +411,11 @@ mbr_status mbr_scene_sequence(const mbr_scene *scene, int32_t *seq_out, int32_t 
 mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_params *params,
                       const mbr_outputs *out, int engine, void *stream);
 
-/* Waits for `stream` and reports a device watchdog trip (MBR_ETIMEOUT). */
+/* Waits for `stream` and reads (and clears) the context's device status word:
+ * MBR_ETIMEOUT when a kernel's bounded loop ran out of its budget since the
+ * last mbr_sync - an AO march that reached max_raymarching_steps (the
+ * reference's AO march has no cap; the march is ended as unoccluded and
+ * counted in mbr_stats.watchdog_trips).  The frame itself is complete. */
 mbr_status mbr_sync(mbr_ctx *ctx, void *stream);
 
 /* Distance estimate at n points (device arrays, xyz interleaved): the
@@ -432,6 +449,15 @@ void mbr_batch_destroy(mbr_batch *batch);
  * precision) and, in *wide_jobs (may be NULL), how many jobs iterate in FP64;
  * -1 for a NULL batch. */
 int32_t mbr_batch_groups(const mbr_batch *batch, int32_t *wide_jobs);
+
+/* Host helper (no device call): the layout of the wavefront engines' scratch
+ * for a launch over `pixels` work items with `tasks_per_hit` shadow/AO tasks
+ * per hit.  offsets[0..2] receive the byte offsets of the hit records, the
+ * FP32 start records and the shadow/AO direction records; *total_bytes the
+ * size.  Both record regions start on a 16-byte boundary for every pixel
+ * count.  No counterpart in the reference (exposed for testing). */
+mbr_status mbr_wavefront_scratch_layout(int64_t pixels, int32_t tasks_per_hit, uint64_t offsets[3],
+                                        uint64_t *total_bytes);
 
 /* The precision MBR_ENGINE_WAVEFRONT_AUTO uses for the current scene seen
  * from `camera` with `params`: *fp64 = 1 for FP64 iteration, 0 for FP32.
@@ -499,9 +525,10 @@ mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_
  * All scratch lives in one static device array of MBR_NOALLOC_SCRATCH_BYTES
  * (64 MiB) that every GPU loading this library holds until the process exits.
  * A frame needs 128 KiB + 512 B + pixels * (88 + 16 * (1 + tasks)) bytes, with
- * tasks = ao_rays + 1 when the shadow march runs; larger frames are rejected
- * with MBR_EINVAL and the limit in `err` (178,131 pixels with a shadow and 16
- * AO rays, 644,012 with neither).  The caller passes the scene, camera,
+ * tasks = ao_rays + 1 when the shadow march runs and the 88-byte hit records
+ * rounded up to a multiple of 256 bytes; larger frames are rejected with
+ * MBR_EINVAL and the limit in `err` (178,130 pixels with a shadow and 16 AO
+ * rays, 644,011 with neither).  The caller passes the scene, camera,
  * parameters and device output buffers as for mbr_render; `err` (may be NULL)
  * receives a message of at most err_len bytes on failure.
  *

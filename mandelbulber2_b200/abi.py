@@ -112,6 +112,10 @@ class RenderParams(C.Structure):
         ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("row_end", C.c_int32),
         ("soft_shadow_cone", C.c_double), ("penetrating", C.c_int32), ("ao_fast", C.c_int32),
         ("ao_quality", C.c_int32), ("ao_fast_tune", C.c_double),
+        ("advanced_quality", C.c_int32), ("reserved_aq", C.c_int32), ("detail_size_min", C.c_double),
+        ("detail_size_max", C.c_double), ("abs_min_marching_step", C.c_double),
+        ("abs_max_marching_step", C.c_double), ("rel_min_marching_step", C.c_double),
+        ("rel_max_marching_step", C.c_double),
     ]
 
 
@@ -163,6 +167,8 @@ PROTOTYPES = {
     "mbr_batch_launch": (C.c_int, [_P, _P]),
     "mbr_batch_destroy": (None, [_P]),
     "mbr_batch_groups": (C.c_int32, [_P, _P]),
+    "mbr_wavefront_scratch_layout": (C.c_int, [C.c_int64, C.c_int32, C.POINTER(C.c_uint64),
+                                               C.POINTER(C.c_uint64)]),
     "mbr_choose_precision": (C.c_int, [_P, _P, _P, _P]),
     "mbr_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "mbr_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),

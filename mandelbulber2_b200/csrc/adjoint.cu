@@ -385,6 +385,9 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
     return set_err(ctx, MBR_EINVAL, "the adjoint differentiates a camera given by position and angles (use_angles = 1)");
   if (camera->perspective_type != MBR_PROJECTION_THREE_POINT)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the three-point projection");
+  if (params->advanced_quality || params->constant_de_threshold)
+    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers thresholds proportional to the distance (no advanced "
+                                          "quality clamps, no constant threshold)");
   if (sc->mbrot.folds || sc->mbrot.main)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the Mandelbox without rotations");
   if (sc->n_prims > 0) return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers scenes without primitives");
@@ -396,7 +399,7 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
   if (engine != MBR_ENGINE_PLAIN_FP64 && engine != MBR_ENGINE_PLAIN_MIXED)
     return set_err(ctx, MBR_EINVAL, "adjoint engine must be MBR_ENGINE_PLAIN_FP64 or MBR_ENGINE_PLAIN_MIXED");
   DevFrame fr;
-  mbr_status st = build_frame(ctx, *camera, *params, &fr);
+  mbr_status st = build_frame(ctx, *camera, *params, &fr, stream);
   if (st != MBR_OK) return st;
   // d(mRot)/d(yaw) with mRot = Rz(yaw) Rx(pitch) Ry(roll) (PrepareMainVectors)
   AdjointFrame af;

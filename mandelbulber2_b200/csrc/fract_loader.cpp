@@ -609,6 +609,32 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     if (parse_double(value, d)) p->smoothness = d; else R.bad(name, value);
   } else if (name == "max_raymarching_steps") {
     if (parse_int(value, b)) p->max_raymarching_steps = b; else R.bad(name, value);
+  } else if (name == "advanced_quality") {  // CalcDistThresh clamps, RayMarching step limits
+    if (parse_bool(value, b)) p->advanced_quality = b; else R.bad(name, value);
+  } else if (name == "detail_size_min") {
+    if (parse_double(value, d)) p->detail_size_min = d; else R.bad(name, value);
+  } else if (name == "detail_size_max") {
+    if (parse_double(value, d)) p->detail_size_max = d; else R.bad(name, value);
+  } else if (name == "abs_min_marching_step") {
+    if (parse_double(value, d)) p->abs_min_marching_step = d; else R.bad(name, value);
+  } else if (name == "abs_max_marching_step") {
+    if (parse_double(value, d)) p->abs_max_marching_step = d; else R.bad(name, value);
+  } else if (name == "rel_min_marching_step") {
+    if (parse_double(value, d)) p->rel_min_marching_step = d; else R.bad(name, value);
+  } else if (name == "rel_max_marching_step") {
+    if (parse_double(value, d)) p->rel_max_marching_step = d; else R.bad(name, value);
+  } else if (name == "limits_enabled" || name == "box_folding" || name == "spherical_folding" ||
+             name == "stereo_enabled" || name == "slow_shading") {
+    // switches that change the geometry (the limit box, calculate_distance.cpp:261-275;
+    // the global folds, compute_fractal.cpp:190-202), the image plane (stereo,
+    // render_worker.cpp:107-108, 158-161, 268) or the normals (iteration-count normals,
+    // shader_calculate_normals.cpp:82-109): refused when on
+    if (!parse_bool(value, b)) R.bad(name, value);
+    else if (b) R.unsupported.push_back(name + " true (" +
+                                        (name == "limits_enabled" ? std::string("limit box")
+                                         : name == "stereo_enabled" ? std::string("stereo image")
+                                         : name == "slow_shading" ? std::string("iteration-count normals")
+                                                                  : std::string("global folding")) + ")");
   } else if (name == "constant_DE_threshold") {
     if (parse_bool(value, b)) p->constant_de_threshold = b; else R.bad(name, value);
   } else if (name == "DE_thresh") {

@@ -193,6 +193,18 @@ struct DevFrame {
   float brightness, contrast, saturation;
   int32_t hdr;
   const uint16_t *gamma;  // 65536-entry table (device)
+  // advanced quality: threshold clamps and march step limits (render_worker.cpp:671-675, 819-834)
+  int32_t adv_quality;
+  int32_t pad3;
+  double detail_size_min, detail_size_max;
+  double abs_step_min, abs_step_max, rel_step_min, rel_step_max;
+};
+
+// Bits of the device status word (DevOutputs::status), read and cleared by
+// mbr_sync: a bounded loop ran out of its budget.  The frame is complete;
+// the loops that ran out were ended as the watchdog rule says.
+enum DevStatus {
+  STATUS_AO_MARCH_CAP = 1,  // an AO march reached max_raymarching_steps (ended unoccluded)
 };
 
 struct DevOutputs {

@@ -62,6 +62,8 @@ struct mbr_ctx {
   DevScene scene;
   mbr_scene scene_src;
   uint16_t *d_gamma = nullptr;
+  uint16_t *h_gamma = nullptr;      // pinned staging table of the gamma copies
+  cudaEvent_t gamma_evt = nullptr;  // recorded after the last gamma copy
   double gamma_value = -1.0;
   int32_t *d_status = nullptr;
   mbr_tuning tuning{128, 12, 2, 0};  // fastest on the 1920x1080 Mandelbox of the autotuner grid
@@ -565,7 +567,7 @@ mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam) {
   return MBR_OK;
 }
 
-mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out) {
+mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out, void *stream) {
   mbr_status st = validate_camera(ctx, cam);
   if (st != MBR_OK) return st;
   if (!(p.detail_level > 0.0) || !(p.de_factor > 0.0) || !(p.view_distance_max > 0.0) || !(p.smoothness > 0.0))
@@ -588,6 +590,12 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
                    cam.height);
   if (p.ao_fast && (p.ao_quality < 1 || p.ao_quality > 10 || !std::isfinite(p.ao_fast_tune)))
     return set_err(ctx, MBR_EINVAL, "fast AO needs ao_quality in [1, 10] and a finite ao_fast_tune");
+  if (p.advanced_quality &&
+      !(std::isfinite(p.detail_size_min) && std::isfinite(p.detail_size_max) && p.abs_min_marching_step > 0.0 &&
+        p.abs_max_marching_step > 0.0 && p.rel_min_marching_step > 0.0 && p.rel_max_marching_step > 0.0 &&
+        std::isfinite(p.abs_min_marching_step) && std::isfinite(p.abs_max_marching_step) &&
+        std::isfinite(p.rel_min_marching_step) && std::isfinite(p.rel_max_marching_step)))
+    return set_err(ctx, MBR_EINVAL, "advanced quality needs finite detail sizes and finite marching step limits > 0");
   if (!(p.soft_shadow_cone >= 0.0 && p.soft_shadow_cone < 90.0))
     return set_err(ctx, MBR_EINVAL, "soft_shadow_cone must be in [0, 90) degrees, got %g", p.soft_shadow_cone);
   const double *L = p.light_direction;
@@ -615,7 +623,8 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.fov = cam.perspective_type == MBR_PROJECTION_THREE_POINT ? 2.0 * std::tan(cam.fov_deg / 360.0 * kPi)
                                                               : cam.fov_deg / 180.0 * kPi;
   f.resolution = 1.0 / cam.height;
-  f.aspect = double(cam.width) / cam.height;
+  // the image plane of an equirectangular view spans 2:1 (render_worker.cpp:98-100)
+  f.aspect = cam.perspective_type == MBR_PROJECTION_EQUIRECTANGULAR ? 2.0 : double(cam.width) / cam.height;
   f.detail_level = p.detail_level;
   f.de_factor = p.de_factor;
   f.view_distance_max = p.view_distance_max;
@@ -651,19 +660,39 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.contrast = float(p.contrast);
   f.saturation = float(p.saturation);
   f.hdr = p.hdr ? 1 : 0;
-  // gamma table (cImage::CalculateGammaTable), cached per context
+  f.adv_quality = p.advanced_quality ? 1 : 0;
+  f.detail_size_min = p.detail_size_min;
+  f.detail_size_max = p.detail_size_max;
+  f.abs_step_min = p.abs_min_marching_step;
+  f.abs_step_max = p.abs_max_marching_step;
+  f.rel_step_min = p.rel_min_marching_step;
+  f.rel_step_max = p.rel_max_marching_step;
+  // gamma table (cImage::CalculateGammaTable), cached per context.  A new
+  // table is copied on `stream`, so frames queued earlier on that stream
+  // still read the table they were built with.  The staging buffer is
+  // pinned; before it is refilled, the host waits for its previous copy.
   if (ctx->gamma_value != p.gamma || !ctx->d_gamma) {
-    std::vector<uint16_t> t(65536);
-    for (int i = 0; i < 65536; i++) t[i] = uint16_t(int(powf(i / 65536.0f, 1.0f / float(p.gamma)) * 65535.0f));
+    const size_t bytes = 65536 * sizeof(uint16_t);
     if (!ctx->d_gamma) {
-      int e = int(cudaMalloc(&ctx->d_gamma, 65536 * sizeof(uint16_t)));
+      int e = int(cudaMalloc(&ctx->d_gamma, bytes));
       if (e) {
         ctx->d_gamma = nullptr;
         return set_err(ctx, MBR_ENOMEM, "cudaMalloc(gamma): %s", cudaGetErrorString(cudaError_t(e)));
       }
     }
-    int e = int(cudaMemcpy(ctx->d_gamma, t.data(), 65536 * sizeof(uint16_t), cudaMemcpyHostToDevice));
-    if (e) return cuda_err(ctx, e, "cudaMemcpy(gamma)");
+    if (!ctx->h_gamma) {
+      int e = int(cudaMallocHost(&ctx->h_gamma, bytes));
+      if (!e) e = int(cudaEventCreateWithFlags(&ctx->gamma_evt, cudaEventDisableTiming));
+      if (e) return set_err(ctx, MBR_ENOMEM, "gamma staging buffer: %s", cudaGetErrorString(cudaError_t(e)));
+    } else if (ctx->gamma_evt) {
+      const int e = int(cudaEventSynchronize(ctx->gamma_evt));
+      if (e) return cuda_err(ctx, e, "cudaEventSynchronize(gamma)");
+    }
+    uint16_t *t = ctx->h_gamma;
+    for (int i = 0; i < 65536; i++) t[i] = uint16_t(int(powf(i / 65536.0f, 1.0f / float(p.gamma)) * 65535.0f));
+    int e = int(cudaMemcpyAsync(ctx->d_gamma, t, bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream)));
+    if (!e && ctx->gamma_evt) e = int(cudaEventRecord(ctx->gamma_evt, static_cast<cudaStream_t>(stream)));
+    if (e) return cuda_err(ctx, e, "cudaMemcpyAsync(gamma)");
     ctx->gamma_value = p.gamma;
   }
   f.gamma = ctx->d_gamma;
@@ -672,17 +701,23 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
 }
 
 // Builds a frame exactly as build_frame does, with the gamma table in device
-// memory the caller already owns (`gamma_dev`, 65536 entries): the table is
-// uploaded when *gamma_value differs from params.gamma, and nothing is
-// allocated.  The error text, if any, goes to *err.
+// memory the caller already owns (`gamma_dev`, 65536 entries) and a host
+// staging table the caller owns too (`gamma_host`, 65536 entries, pageable):
+// the table is copied on `stream` when *gamma_value differs from
+// params.gamma, and nothing is allocated.  A copy from pageable memory has
+// read its source when cudaMemcpyAsync returns, so the staging table may be
+// refilled by the next call.  The error text, if any, goes to *err.
 mbr_status build_frame_owned_gamma(const mbr_camera &cam, const mbr_render_params &p, uint16_t *gamma_dev,
-                                   double *gamma_value, DevFrame *out, std::string *err) {
-  mbr_ctx tmp;  // holds no device memory of its own; nothing to release
+                                   uint16_t *gamma_host, double *gamma_value, DevFrame *out, void *stream,
+                                   std::string *err) {
+  mbr_ctx tmp;  // holds no memory of its own; nothing to release
   tmp.d_gamma = gamma_dev;
+  tmp.h_gamma = gamma_host;
   tmp.gamma_value = *gamma_value;
-  const mbr_status st = build_frame(&tmp, cam, p, out);
+  const mbr_status st = build_frame(&tmp, cam, p, out, stream);
   *gamma_value = tmp.gamma_value;
   tmp.d_gamma = nullptr;
+  tmp.h_gamma = nullptr;
   if (err) *err = tmp.err;
   return st;
 }
@@ -761,6 +796,11 @@ void mbr_destroy(mbr_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->d_gamma) cudaFree(ctx->d_gamma);
+  if (ctx->gamma_evt) {
+    cudaEventSynchronize(ctx->gamma_evt);
+    cudaEventDestroy(ctx->gamma_evt);
+  }
+  if (ctx->h_gamma) cudaFreeHost(ctx->h_gamma);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->d_work) cudaFree(ctx->d_work);
   if (ctx->adjoint_scratch) cudaFree(ctx->adjoint_scratch);
@@ -893,6 +933,14 @@ void mbr_render_params_defaults(mbr_render_params *p) {
   // initparameters.cpp:214-216
   p->ao_quality = 4;
   p->ao_fast_tune = 1.0;
+  // initparameters.cpp:159-165
+  p->advanced_quality = 0;
+  p->abs_max_marching_step = 3.0;
+  p->abs_min_marching_step = 1e-15;
+  p->rel_max_marching_step = 1e4;
+  p->rel_min_marching_step = 1e-2;
+  p->detail_size_max = 1.0;
+  p->detail_size_min = 1e-12;
 }
 
 mbr_status mbr_scene_set(mbr_ctx *ctx, const mbr_scene *scene) {
@@ -934,7 +982,7 @@ mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_p
   if (!ctx->has_scene) return set_err(ctx, MBR_EINVAL, "no scene set (call mbr_scene_set first)");
   if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, MBR_ECUDA, "cudaSetDevice failed");
   DevFrame fr;
-  mbr_status st = build_frame(ctx, *camera, *params, &fr);
+  mbr_status st = build_frame(ctx, *camera, *params, &fr, stream);
   if (st != MBR_OK) return st;
   fr.want_normal = out->normal != nullptr;
   const DevOutputs d = dev_outputs(ctx, *out);
@@ -964,7 +1012,13 @@ mbr_status mbr_sync(mbr_ctx *ctx, void *stream) {
   e = int(cudaMemcpy(&status, ctx->d_status, sizeof(status), cudaMemcpyDeviceToHost));
   if (e) return cuda_err(ctx, e, "cudaMemcpy(status)");
   if (status != 0) {
-    cudaMemset(ctx->d_status, 0, sizeof(int32_t));
+    e = int(cudaMemset(ctx->d_status, 0, sizeof(int32_t)));
+    if (e) return cuda_err(ctx, e, "cudaMemset(status)");
+    if (status & STATUS_AO_MARCH_CAP)
+      return set_err(ctx, MBR_ETIMEOUT,
+                     "device watchdog: an AO march reached max_raymarching_steps and was ended as unoccluded "
+                     "(status %d; the frame is complete, stats.watchdog_trips counts the marches)",
+                     status);
     return set_err(ctx, MBR_ETIMEOUT, "device watchdog tripped (status %d)", status);
   }
   return MBR_OK;

@@ -10,12 +10,14 @@ namespace mbr {
 mbr_status set_err(mbr_ctx *ctx, mbr_status st, const char *fmt, ...);
 mbr_status cuda_err(mbr_ctx *ctx, int code, const char *what);
 mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out);
-mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out);
+// The gamma table, when it changes, is copied on `stream`.
+mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_params &p, DevFrame *out, void *stream);
 mbr_status validate_camera(mbr_ctx *ctx, const mbr_camera &cam);
 void camera_matrix(const mbr_camera &cam, double mrot[9], bool *zero, double angles[3]);
 DevOutputs dev_outputs(mbr_ctx *ctx, const mbr_outputs &o);
 mbr_status build_frame_owned_gamma(const mbr_camera &cam, const mbr_render_params &p, uint16_t *gamma_dev,
-                                   double *gamma_value, DevFrame *out, std::string *err);
+                                   uint16_t *gamma_host, double *gamma_value, DevFrame *out, void *stream,
+                                   std::string *err);
 const DevScene *ctx_scene(mbr_ctx *ctx);
 int ctx_device(mbr_ctx *ctx);
 const mbr_scene *ctx_scene_src(mbr_ctx *ctx);

@@ -147,14 +147,46 @@ __device__ __forceinline__ D3 view_vector(const DevFrame &fr, double ix, double 
   return rotate(fr, d3norm(projection_dir(fr.persp, fr.fov, ix, iy)));
 }
 __device__ __forceinline__ D3 camera_of(const DevFrame &fr) { return {fr.camera[0], fr.camera[1], fr.camera[2]}; }
+// The tail of CalcDistThresh (render_worker.cpp:669-677): an equirectangular
+// view halves the threshold, then advanced quality clamps it to
+// [detail_size_min, detail_size_max]; reduceDetail is 1 outside progressive
+// previews (render_job.cpp:1177-1182).
+__device__ __forceinline__ double thresh_tail(const DevFrame &fr, int persp, double distThresh) {
+  if (persp == MBR_PROJECTION_EQUIRECTANGULAR) distThresh *= 0.5;
+  if (fr.adv_quality) {
+    if (distThresh > fr.detail_size_max) distThresh = fr.detail_size_max;
+    if (distThresh < fr.detail_size_min) distThresh = fr.detail_size_min;
+  }
+  return distThresh;
+}
 __device__ __forceinline__ double dist_thresh(const DevScene &sc, const DevFrame &fr, D3 q) {
   const double l = d3len(d3sub(camera_of(fr), q));
-  if (sc.iter_thresh) return l * fr.resolution * fr.fov;
-  if (fr.constant_de_threshold) return fr.de_thresh;
-  return l * fr.resolution * fr.fov / fr.detail_level;
+  double t;
+  if (sc.iter_thresh) t = l * fr.resolution * fr.fov;
+  else if (fr.constant_de_threshold) t = fr.de_thresh;
+  else t = l * fr.resolution * fr.fov / fr.detail_level;
+  return thresh_tail(fr, fr.persp, t);
 }
+// CalcDelta (render_worker.cpp:684-690)
 __device__ __forceinline__ double calc_delta(const DevFrame &fr, D3 q) {
-  return d3len(d3sub(camera_of(fr), q)) * fr.resolution * fr.fov;
+  double delta = d3len(d3sub(camera_of(fr), q)) * fr.resolution * fr.fov;
+  if (fr.persp == MBR_PROJECTION_EQUIRECTANGULAR) delta *= 0.5;
+  return delta;
+}
+// The limits of one march step (render_worker.cpp:819-834): with advanced
+// quality the absolute and threshold-relative bounds, else step <= 3.
+__device__ __forceinline__ double step_limit(const DevFrame &fr, double step, double distThresh) {
+  if (fr.adv_quality) {
+    if (step > fr.abs_step_max) step = fr.abs_step_max;
+    if (step < fr.abs_step_min) step = fr.abs_step_min;
+    if (distThresh > fr.abs_step_min) {
+      if (step > fr.rel_step_max * distThresh) step = fr.rel_step_max * distThresh;
+    }
+    if (step < fr.rel_step_min * distThresh) step = fr.rel_step_min * distThresh;
+  } else if (step > 3.0) {
+    step = 3.0;
+  }
+  return step;
 }
 
 // Per-thread counters: DE evaluations and summed iterations live in
@@ -217,7 +249,7 @@ __device__ MarchOut ray_marching(const DevScene &sc, const DevFrame &fr, D3 star
       step = (dist - 0.8 * distThresh) * fr.de_factor * jit;
     else
       step = (dist - 0.5 * distThresh) * fr.de_factor * jit;
-    if (step > 3.0) step = 3.0;
+    step = step_limit(fr, step, distThresh);
     prevScan = scan;
     scan += step / dirLen;
     if (scan > fr.view_distance_max) break;

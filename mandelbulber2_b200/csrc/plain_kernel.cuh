@@ -191,6 +191,10 @@ __global__ void __launch_bounds__(128) plain_kernel(const __grid_constant__ DevS
     if (out.rgb8) to_rgb8(fr, rgb, &out.rgb8[3 * o]);
     n_pix = 1;
   }
+  if (out.status) {  // the watchdog status word: any AO march that reached its cap
+    const unsigned int t = __reduce_add_sync(0xffffffffu, trips);
+    if (lane == 0 && t) atomicOr(out.status, int(STATUS_AO_MARCH_CAP));
+  }
   if (out.stats) {
     const unsigned int vals[K_COUNT] = {tc.de, tc.iters, n_march, n_binary, n_normal, n_shadow, n_ao, n_gi, n_pix, trips};
 #pragma unroll

@@ -79,8 +79,9 @@ struct WJob {
   long long pixel_offset;  // first pixel of this job in the outputs
   double fov, aspect;
   double resolution, detail;  // CalcDistThresh factors (1/height, detail level)
-  float c0;                // threshold per unit distance: resolution * fov / detail
-  float fovf;              // fov (AO end distance = |camera - p| * fov)
+  float c0;                // threshold per unit distance: resolution * fov / detail (halved: equirectangular)
+  float fovf;              // AO end distance per unit distance: fov (halved: equirectangular)
+  float cthr;              // constant threshold (halved: equirectangular)
   FastDiv div_w, div_tx;   // divisions by width and tiles_x
 };
 
@@ -695,15 +696,26 @@ struct PrimaryStage {
 
   // distThresh at the request point (render_worker.cpp:653-679): FP64 from
   // |camera - q| as the plain kernel computes it; FP32 from t
+  // with the tail of thresh_tail: an equirectangular view halves it (in the
+  // FP32 form inside c0 and `cthr`), advanced quality clamps it
   __device__ void set_thr(double qx, double qy, double qz) {
-    if (fr.constant_de_threshold) {
-      thr = D(fr.de_thresh);
-    } else if (P::kWide) {
-      const double ax = jb->cam[0] - qx, ay = jb->cam[1] - qy, az = jb->cam[2] - qz;
-      const double l = sqrt(ax * ax + ay * ay + az * az);
-      thr = D(l * jb->resolution * jb->fov / jb->detail);
+    if (P::kWide) {
+      double v;
+      if (fr.constant_de_threshold) {
+        v = fr.de_thresh;
+      } else {
+        const double ax = jb->cam[0] - qx, ay = jb->cam[1] - qy, az = jb->cam[2] - qz;
+        const double l = sqrt(ax * ax + ay * ay + az * az);
+        v = l * jb->resolution * jb->fov / jb->detail;
+      }
+      thr = D(thresh_tail(fr, jb->persp, v));
     } else {
-      thr = D(float(t) * float(c0));
+      float v = fr.constant_de_threshold ? jb->cthr : float(t) * float(c0);
+      if (fr.adv_quality) {
+        if (v > float(fr.detail_size_max)) v = float(fr.detail_size_max);
+        if (v < float(fr.detail_size_min)) v = float(fr.detail_size_min);
+      }
+      thr = D(v);
     }
   }
 
@@ -887,11 +899,12 @@ struct PrimaryStage {
     }
     if (P::kWide) {
       stp = (double(d) - 0.5 * double(thr)) * fr.de_factor * jit;
-      if (stp > 3.0) stp = 3.0;
+      stp = step_limit(fr, stp, double(thr));
       t += stp / dir_len;
     } else {
       stp = double((float(d) - 0.5f * float(thr)) * float(fr.de_factor)) * jit;
-      if (stp > 3.0) stp = 3.0;
+      if (fr.adv_quality) stp = step_limit(fr, stp, double(thr));
+      else if (stp > 3.0) stp = 3.0;
       t += stp;
     }
     if (t > fr.view_distance_max || count >= fr.max_steps) {
@@ -1080,8 +1093,11 @@ __device__ __forceinline__ double shadow_distance(const DevFrame &fr, const Laun
   const double *cam = MULTI ? L.jobs[r.job].cam : fr.camera;
   const double res = MULTI ? L.jobs[r.job].resolution : fr.resolution;
   const double fov = MULTI ? L.jobs[r.job].fov : fr.fov;
+  const int persp = MULTI ? L.jobs[r.job].persp : fr.persp;
   const double ax = cam[0] - r.px, ay = cam[1] - r.py, az = cam[2] - r.pz;
-  return sqrt(ax * ax + ay * ay + az * az) * res * fov / res;
+  double delta = sqrt(ax * ax + ay * ay + az * az) * res * fov;  // CalcDelta
+  if (persp == MBR_PROJECTION_EQUIRECTANGULAR) delta *= 0.5;
+  return delta / res;
 }
 
 // FAST: the AO task is the fast AO (a separate instantiation, so the march
@@ -1104,6 +1120,7 @@ struct ShadeStage {
   float thr;
   int count, mode;  // mode 0 shadow, 1 AO march, 2 fast AO (end: its float sum)
   unsigned int shadow_de;
+  unsigned int trips;  // AO marches that reached max_raymarching_steps (watchdog)
 
   __device__ const typename P::Params &params() const { return fp; }
   __device__ int kind() const { return kd; }
@@ -1218,6 +1235,7 @@ struct ShadeStage {
       }
       t = fmadd(D(2), d, t);
       if (t >= end || count >= fr.max_steps) {
+        if (!(t >= end)) trips++;  // the cap ended it: a watchdog trip
         ao_add(r, 1.0);
         return false;
       }
@@ -1293,6 +1311,7 @@ __device__ __forceinline__ void shade_body(const DevFrame &fr, const typename P:
   if (gated_off(L)) return;
   ShadeStage<MULTI, P, FAST> S{fr, L, fp0, P::kind(fp0)};
   S.shadow_de = 0;
+  S.trips = 0;
   S.vdm = typename P::D(fr.view_distance_max);
   S.dfac = typename P::D(fr.de_factor);
   unsigned int my_de = 0;
@@ -1300,6 +1319,11 @@ __device__ __forceinline__ void shade_body(const DevFrame &fr, const typename P:
   const long long total = (long long)L.ctr->hits * (long long)(L.shadow_tasks + L.ao_rays);
   run_stage<FK, P>(S, fp0, &L.ctr->shade_next, total, L.refill_k, &my_de, &my_iters);
   flush_counts(out, my_de, my_iters, K_AO, my_de - S.shadow_de, K_SHADOW, S.shadow_de);
+  const unsigned int trips = __reduce_add_sync(0xffffffffu, S.trips);
+  if ((threadIdx.x & 31) == 0 && trips) {
+    if (out.stats) atomicAdd(reinterpret_cast<unsigned long long *>(out.stats) + K_WATCHDOG, (unsigned long long)trips);
+    if (out.status) atomicOr(out.status, int(STATUS_AO_MARCH_CAP));
+  }
 }
 
 template <int FK, bool MULTI, class P>
@@ -1365,31 +1389,33 @@ __global__ void pixel_count_kernel(const __grid_constant__ Launch L, DevOutputs 
 // ============================================================================
 // 1 when the smallest hit threshold of a view, bounded below by
 // DE(camera) * c0 (c0: threshold per unit distance), or the constant
-// threshold, is below kWideRatio FP32 units of the camera coordinates.
-__device__ __forceinline__ int wide_needed(const DevScene &sc, const double cam[3], double c0, int constant_thr,
-                                           double de_thresh) {
-  double thr_min = de_thresh;
-  if (!constant_thr) {
+// threshold, is below kWideRatio FP32 units of the camera coordinates.  The
+// bound passes through the threshold's tail (equirectangular halving,
+// advanced-quality clamps) as every threshold of the view does.
+__device__ __forceinline__ int wide_needed(const DevScene &sc, const DevFrame &fr, const double cam[3], double c0,
+                                           int persp) {
+  double thr_min = fr.de_thresh;
+  if (!fr.constant_de_threshold) {
     int it;
     const double d0 = calc_distance<double, F_EXT, false>(sc, cam[0], cam[1], cam[2], 0.0, false, &it);
     thr_min = d0 * c0;
   }
+  thr_min = thresh_tail(fr, persp, thr_min);
   const double scale = fmax(fmax(fabs(cam[0]), fabs(cam[1])), fmax(fabs(cam[2]), 1.0));
   return (thr_min < kWideRatio * scale * 0x1p-24) ? 1 : 0;
 }
 
 __global__ void policy_kernel(const __grid_constant__ DevScene sc, const __grid_constant__ DevFrame fr, int *gate) {
   if (blockIdx.x == 0 && threadIdx.x == 0)
-    *gate = wide_needed(sc, fr.camera, fr.resolution * fr.fov / fr.detail_level, fr.constant_de_threshold,
-                        fr.de_thresh);
+    *gate = wide_needed(sc, fr, fr.camera, fr.resolution * fr.fov / fr.detail_level, fr.persp);
 }
 
 __global__ void batch_policy_kernel(const DevScene *scenes, const int *scene_of, const WJob *jobs, int n,
-                                    int constant_thr, double de_thresh, int *flags) {
+                                    const __grid_constant__ DevFrame fr, int *flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n)
-    flags[i] = wide_needed(scenes[scene_of[i]], jobs[i].cam, jobs[i].resolution * jobs[i].fov / jobs[i].detail,
-                           constant_thr, de_thresh);
+    flags[i] = wide_needed(scenes[scene_of[i]], fr, jobs[i].cam, jobs[i].resolution * jobs[i].fov / jobs[i].detail,
+                           jobs[i].persp);
 }
 
 // ============================================================================
@@ -1416,9 +1442,9 @@ enum { G_MARCH = 0, G_BINARY, G_SHADOW, G_BOUNCE };
 
 // distThresh at q (render_worker.cpp:653-679), from the camera position
 __device__ __forceinline__ double gi_thresh(const DevFrame &fr, double qx, double qy, double qz) {
-  if (fr.constant_de_threshold) return fr.de_thresh;
+  if (fr.constant_de_threshold) return thresh_tail(fr, fr.persp, fr.de_thresh);
   const double ax = fr.camera[0] - qx, ay = fr.camera[1] - qy, az = fr.camera[2] - qz;
-  return sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.detail_level;
+  return thresh_tail(fr, fr.persp, sqrt(ax * ax + ay * ay + az * az) * fr.resolution * fr.fov / fr.detail_level);
 }
 
 template <class P>
@@ -1586,7 +1612,7 @@ struct GIPrimaryStage {
       pm = p.s;
     }
     stp = (double(d) - 0.5 * thr) * fr.de_factor * jit;
-    if (stp > 3.0) stp = 3.0;
+    stp = step_limit(fr, stp, thr);
     t += stp / dir_len;
     if (t > fr.view_distance_max || count >= fr.max_steps) return miss();
     ray_point(qx, qy, qz);
@@ -1807,8 +1833,11 @@ static WJob make_job(const DevFrame &fr, long long first, long long pixel_offset
   j.aspect = fr.aspect;
   j.resolution = fr.resolution;
   j.detail = fr.detail_level;
-  j.c0 = float(fr.resolution * fr.fov / fr.detail_level);
-  j.fovf = float(fr.fov);
+  // CalcDistThresh and CalcDelta halve both for an equirectangular view (render_worker.cpp:669, 688)
+  const double half = fr.persp == MBR_PROJECTION_EQUIRECTANGULAR ? 0.5 : 1.0;
+  j.c0 = float(fr.resolution * fr.fov / fr.detail_level * half);
+  j.fovf = float(fr.fov * half);
+  j.cthr = float(fr.de_thresh * half);
   j.div_w = make_fastdiv(j.width);
   j.div_tx = make_fastdiv(j.tiles_x);
   return j;
@@ -1937,19 +1966,32 @@ static int launch_pipeline(int fk, const mbr_tuning &tu, cudaStream_t st, const 
 }
 
 // Scratch of a launch over `pixels` work items with `per` stage-S tasks per
-// hit: counters and the policy flag, hit records, FP32 origins and stage-S
-// start records.
+// hit: counters and the policy flag (256 B), hit records, FP32 origins and
+// stage-S start records.  A HitRec is 88 bytes, so the hit region is rounded
+// up to a multiple of 256 bytes: the float4 records after it then start on a
+// 16-byte boundary for every pixel count, odd ones included.
+static size_t hit_region_bytes(long long pixels) { return (size_t(pixels) * sizeof(HitRec) + 255) / 256 * 256; }
+
 static size_t scratch_bytes(long long pixels, int per) {
-  return 256 + size_t(pixels) * (sizeof(HitRec) + sizeof(float4) * (1 + size_t(per)));
+  return 256 + hit_region_bytes(pixels) + size_t(pixels) * sizeof(float4) * (1 + size_t(per));
+}
+
+// Byte offsets of the hit records, the FP32 origins and the stage-S records.
+static void scratch_offsets(long long pixels, size_t off[3]) {
+  off[0] = 256;
+  off[1] = 256 + hit_region_bytes(pixels);
+  off[2] = off[1] + size_t(pixels) * sizeof(float4);
 }
 
 static void scratch_layout(Launch &L, void *base, long long pixels) {
   char *p = static_cast<char *>(base);
+  size_t off[3];
+  scratch_offsets(pixels, off);
   L.ctr = reinterpret_cast<Counters4 *>(p);
   L.gate = nullptr;
-  L.hits = reinterpret_cast<HitRec *>(p + 256);
-  L.sorg = reinterpret_cast<float4 *>(p + 256 + size_t(pixels) * sizeof(HitRec));
-  L.sdir = L.sorg + pixels;
+  L.hits = reinterpret_cast<HitRec *>(p + off[0]);
+  L.sorg = reinterpret_cast<float4 *>(p + off[1]);
+  L.sdir = reinterpret_cast<float4 *>(p + off[2]);
 }
 
 static int *scratch_gate(void *base) { return reinterpret_cast<int *>(static_cast<char *>(base) + 128); }
@@ -2080,8 +2122,7 @@ static int batch_policy(const std::vector<DevScene> &dsc, const std::vector<int>
   if (!e) e = int(cudaMemcpy(d_of, scene_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   if (!e) e = int(cudaMemcpy(d_wj, wj.data(), sizeof(WJob) * n, cudaMemcpyHostToDevice));
   if (!e) {
-    batch_policy_kernel<<<(n + 127) / 128, 128>>>(d_sc, d_of, d_wj, n, fr0.constant_de_threshold, fr0.de_thresh,
-                                                  d_fl);
+    batch_policy_kernel<<<(n + 127) / 128, 128>>>(d_sc, d_of, d_wj, n, fr0, d_fl);
     e = int(cudaGetLastError());
   }
   flags->assign(n, 0);
@@ -2119,7 +2160,7 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
       return set_err(ctx, MBR_EINVAL, "job %d: scene_index %d out of range", i, jb.scene_index);
     if (jb.pixel_offset < 0) return set_err(ctx, MBR_EINVAL, "job %d: negative pixel_offset", i);
     DevFrame fr;
-    mbr_status st = build_frame(ctx, jb.camera, *params, &fr);
+    mbr_status st = build_frame(ctx, jb.camera, *params, &fr, stream);
     if (st != MBR_OK) return st;
     st = check_supported(ctx, dsc[jb.scene_index], fr, true);
     if (st != MBR_OK) return st;
@@ -2129,6 +2170,10 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
     job_pixels[i] = (long long)fr.width * (fr.row1 - fr.row0);
   }
   fr0.want_normal = outs->normal != nullptr;
+  {  // the gamma table was copied on `stream`; the graph may be launched on another
+    const int e = int(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    if (e) return cuda_err(ctx, e, "cudaStreamSynchronize");
+  }
   // precision of every job
   std::vector<int> wide(n_jobs, engine == MBR_ENGINE_WAVEFRONT_FP64 ? 1 : 0);
   if (engine == MBR_ENGINE_WAVEFRONT_AUTO) {
@@ -2230,7 +2275,6 @@ mbr_status mbr_batch_create(mbr_ctx *ctx, const mbr_scene *scenes, int32_t n_sce
   if (e) return fail(e, "graph capture");
   e = int(cudaGraphInstantiate(&b->exec, b->graph, 0));
   if (e) return fail(e, "cudaGraphInstantiate");
-  (void)stream;
   *batch = b;
   return MBR_OK;
 }
@@ -2259,7 +2303,7 @@ mbr_status mbr_choose_precision(mbr_ctx *ctx, const mbr_camera *camera, const mb
   if (!sc) return set_err(ctx, MBR_EINVAL, "no scene set (call mbr_scene_set first)");
   if (cudaSetDevice(ctx_device(ctx)) != cudaSuccess) return set_err(ctx, MBR_ECUDA, "cudaSetDevice failed");
   DevFrame fr;
-  mbr_status st = build_frame(ctx, *camera, *params, &fr);
+  mbr_status st = build_frame(ctx, *camera, *params, &fr, nullptr);
   if (st != MBR_OK) return st;
   int *d_flag = nullptr;
   int e = int(cudaMalloc(&d_flag, sizeof(int)));
@@ -2271,6 +2315,16 @@ mbr_status mbr_choose_precision(mbr_ctx *ctx, const mbr_camera *camera, const mb
   cudaFree(d_flag);
   if (e) return cuda_err(ctx, e, "precision policy");
   *fp64 = flag;
+  return MBR_OK;
+}
+
+mbr_status mbr_wavefront_scratch_layout(int64_t pixels, int32_t tasks_per_hit, uint64_t offsets[3],
+                                        uint64_t *total_bytes) {
+  if (pixels < 0 || tasks_per_hit < 0 || !offsets || !total_bytes) return MBR_EINVAL;
+  size_t off[3];
+  scratch_offsets(pixels, off);
+  for (int i = 0; i < 3; i++) offsets[i] = off[i];
+  *total_bytes = scratch_bytes(pixels, tasks_per_hit);
   return MBR_OK;
 }
 
@@ -2381,10 +2435,19 @@ struct NoallocDevice {
 const int kMaxDevices = 64;
 NoallocDevice g_noalloc[kMaxDevices];
 std::mutex g_noalloc_mutex;
+uint16_t g_noalloc_gamma_host[65536];  // host staging table of the gamma copies
 
 mbr_status noalloc_fail(char *err, size_t err_len, mbr_status st, const std::string &msg) {
   if (err && err_len) std::snprintf(err, err_len, "%s", msg.c_str());
   return st;
+}
+
+// The largest pixel count whose scratch fits in `have` bytes.
+long long noalloc_max_pixels(int per, size_t have) {
+  const size_t per_pixel = sizeof(HitRec) + sizeof(float4) * (1 + size_t(per));
+  long long n = (long long)((have - 256 - 255) / per_pixel);  // the hit region rounds up by < 256 bytes
+  while (scratch_bytes(n + 1, per) <= have) n++;
+  return n;
 }
 
 }  // namespace
@@ -2418,8 +2481,11 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
   if (st != MBR_OK) return noalloc_fail(err, err_len, st, "invalid or unsupported scene (see mbr_scene_set)");
   DevFrame fr;
   std::string msg;
-  st = build_frame_owned_gamma(*camera, *params, reinterpret_cast<uint16_t *>(nd->base), &nd->gamma_value, &fr,
-                               &msg);
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);  // the host staging table is shared
+    st = build_frame_owned_gamma(*camera, *params, reinterpret_cast<uint16_t *>(nd->base), g_noalloc_gamma_host,
+                                 &nd->gamma_value, &fr, stream, &msg);
+  }
   if (st != MBR_OK) return noalloc_fail(err, err_len, st, msg);
   fr.want_normal = out->normal != nullptr;
   if (sc.is_hybrid || sc.generic || sc.iter_thresh || sc.interior || sc.has_w || fr.gi_samples > 0 ||
@@ -2432,12 +2498,11 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
   const size_t need = scratch_bytes(total, per);
   const size_t have = size_t(MBR_NOALLOC_SCRATCH_BYTES) - kHeadBytes;
   if (need > have) {
-    const size_t per_pixel = sizeof(HitRec) + sizeof(float4) * (1 + size_t(per));
     char buf[320];
     std::snprintf(buf, sizeof(buf),
                   "frame of %lld pixels with %d shadow/AO tasks per hit needs %zu bytes of scratch; the "
-                  "allocation-free entry point has %zu (at most %zu pixels at this setting)",
-                  total, per, need, have, (have - 256) / per_pixel);
+                  "allocation-free entry point has %zu (at most %lld pixels at this setting)",
+                  total, per, need, have, noalloc_max_pixels(per, have));
     return noalloc_fail(err, err_len, MBR_EINVAL, buf);
   }
   Launch L;

@@ -1112,11 +1112,27 @@ struct Renderer {
   }
   // CalcDistThresh (render_worker.cpp:653-679), reduceDetail = 1
   double dist_thresh(D3 q) const {
-    if (seq.iter_thresh) return length(sub(camera, q)) * resolution * fov;
-    if (p.constant_de_threshold) return p.de_thresh;
-    return length(sub(camera, q)) * resolution * fov / p.detail_level;
+    double distThresh;
+    if (seq.iter_thresh) {
+      distThresh = length(sub(camera, q)) * resolution * fov;
+    } else {
+      if (p.constant_de_threshold)
+        distThresh = p.de_thresh;
+      else
+        distThresh = length(sub(camera, q)) * resolution * fov / p.detail_level;
+    }
+    if (cam.perspective_type == MBR_PROJECTION_EQUIRECTANGULAR) distThresh *= 0.5;  // :669
+    if (p.advanced_quality) {  // :671-675
+      if (distThresh > p.detail_size_max) distThresh = p.detail_size_max;
+      if (distThresh < p.detail_size_min) distThresh = p.detail_size_min;
+    }
+    return distThresh;
   }
-  double calc_delta(D3 q) const { return length(sub(camera, q)) * resolution * fov; }  // :684-690
+  double calc_delta(D3 q) const {  // :684-690
+    double delta = length(sub(camera, q)) * resolution * fov;
+    if (cam.perspective_type == MBR_PROJECTION_EQUIRECTANGULAR) delta *= 0.5f;
+    return delta;
+  }
 
   struct March {
     bool found = false;
@@ -1157,7 +1173,16 @@ struct Renderer {
         step = (dist - 0.8 * distThresh) * p.de_factor * jit;
       else
         step = (dist - 0.5 * distThresh) * p.de_factor * jit;
-      if (step > 3.0) step = 3.0;
+      if (p.advanced_quality) {  // :819-834
+        if (step > p.abs_max_marching_step) step = p.abs_max_marching_step;
+        if (step < p.abs_min_marching_step) step = p.abs_min_marching_step;
+        if (distThresh > p.abs_min_marching_step) {
+          if (step > p.rel_max_marching_step * distThresh) step = p.rel_max_marching_step * distThresh;
+        }
+        if (step < p.rel_min_marching_step * distThresh) step = p.rel_min_marching_step * distThresh;
+      } else {
+        if (step > 3.0) step = 3.0;
+      }
       prevScan = scan;
       scan += step / dirLen;
       if (scan > maxScan) break;
@@ -1562,6 +1587,7 @@ static bool make_renderer(const mbr_scene *scene, const mbr_camera *cam, const m
   R->fov = calc_fov(*cam);
   R->resolution = 1.0 / cam->height;                // render_job.cpp:477
   R->aspect = double(cam->width) / cam->height;     // render_worker.cpp:98
+  if (cam->perspective_type == MBR_PROJECTION_EQUIRECTANGULAR) R->aspect = 2.0;  // :100
   R->light = normalize(D3{params->light_direction[0], params->light_direction[1], params->light_direction[2]});
   R->gamma = gamma_table(params->gamma);
   return true;
@@ -1746,6 +1772,7 @@ int oracle_view(const mbr_camera *cam, int x, int y, double *dir) {
   camera_setup(*cam, &R.M, ang);
   R.fov = calc_fov(*cam);
   R.aspect = double(cam->width) / cam->height;
+  if (cam->perspective_type == MBR_PROJECTION_EQUIRECTANGULAR) R.aspect = 2.0;  // render_worker.cpp:100
   double ix, iy;
   R.image_point(double(x), double(y), &ix, &iy);
   D3 d = normalize(R.view_vector(ix, iy));

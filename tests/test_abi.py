@@ -81,3 +81,42 @@ def test_create_without_gpu_fails_loudly():
 
     with pytest.raises(RuntimeError):
         Renderer(0)
+
+
+def _layout(pixels, per):
+    off = (C.c_uint64 * 3)()
+    total = C.c_uint64()
+    assert abi.load().mbr_wavefront_scratch_layout(pixels, per, off, C.byref(total)) == abi.MBR_OK
+    return list(off), total.value
+
+
+@pytest.mark.parametrize("pixels", [0, 1, 2, 3, 7, 99 * 55, 99 * 99, 1001 * 751, 1920 * 1080, 178131, 3840 * 2160])
+@pytest.mark.parametrize("per", [0, 1, 5, 17])
+def test_wavefront_scratch_records_are_16_byte_aligned(pixels, per):
+    """The float4 start and direction records follow the 88-byte hit records:
+    both regions must start on a 16-byte boundary for odd pixel counts too."""
+    off, total = _layout(pixels, per)
+    assert off[0] == 256
+    assert all(o % 16 == 0 for o in off), off
+    assert off[1] >= off[0] + 88 * pixels and off[1] - (off[0] + 88 * pixels) < 256
+    assert off[2] == off[1] + 16 * pixels
+    assert total == off[2] + 16 * pixels * per
+
+
+def test_noalloc_pixel_limits_match_the_header():
+    """The largest frames the allocation-free entry point accepts (documented
+    in mbr.h: 178,130 pixels with a shadow and 16 AO rays, 644,011 with
+    neither), from the scratch layout and the static array's size."""
+    have = 64 * 1024 * 1024 - (65536 * 2 + 256)
+    for per, documented in ((17, 178130), (0, 644011)):
+        assert _layout(documented, per)[1] <= have
+        assert _layout(documented + 1, per)[1] > have
+    assert b"178,130" in open(HEADER, "rb").read() and b"644,011" in open(HEADER, "rb").read()
+
+
+def test_advanced_quality_defaults():
+    p = abi.params_defaults()
+    assert p.advanced_quality == 0
+    assert (p.detail_size_min, p.detail_size_max) == (1e-12, 1.0)
+    assert (p.abs_min_marching_step, p.abs_max_marching_step) == (1e-15, 3.0)
+    assert (p.rel_min_marching_step, p.rel_max_marching_step) == (1e-2, 1e4)

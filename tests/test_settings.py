@@ -20,7 +20,10 @@ from mandelbulber2_b200 import abi, settings
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIX = os.path.join(HERE, "golden", "settings")
-EXAMPLES = "/root/reference/mandelbulber2/deploy/share/mandelbulber2/examples"
+# the reference's example scenes: read when MANDELBULBER2_SOURCE names the
+# reference's mandelbulber2 directory (the tests are skipped otherwise)
+_SRC = os.environ.get("MANDELBULBER2_SOURCE", "")
+EXAMPLES = os.path.join(_SRC, "deploy", "share", "mandelbulber2", "examples") if _SRC else ""
 
 HEADER = "# Mandelbulber settings file\n# version 2.33\n# only modified parameters\n"
 
@@ -287,11 +290,13 @@ def test_report_is_truncated_safely():
     assert lib.mbr_fract_parse(None, C.byref(sc), C.byref(cam), C.byref(p), None, 0) == abi.MBR_EINVAL
 
 
-@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
+@pytest.mark.skipif(not EXAMPLES or not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
 def test_reference_examples():
     """Every example scene the reference ships is read: none is malformed, and a
     scene is accepted exactly when the formulas it iterates are built here and
-    none of the unsupported features appears."""
+    none of the unsupported features appears.  Switches that change the
+    geometry, the march or the normals and are not built (the limit box, the
+    global folds, stereo, iteration-count normals) turn a scene away."""
     files = sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.fract"), recursive=True))
     assert len(files) > 150
     ok = 0
@@ -301,16 +306,20 @@ def test_reference_examples():
         sc = s.scene
         used = range(sc.n_fractals) if sc.hybrid_fractal_enable else range(1)
         formulas = {sc.fractal[i].formula for i in used} - {0}
+        text = open(path, errors="replace").read()
+        for key in ("limits_enabled", "box_folding", "spherical_folding", "stereo_enabled", "slow_shading"):
+            if f"\n{key} true;" in text:
+                assert not s.ok and any(u.startswith(key + " true") for u in s.unsupported()), (path, key)
         if s.ok:
             ok += 1
             assert formulas <= {2, 3, 4, 7, 8, 10, 11}, (path, formulas)
             assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
         elif not formulas <= {2, 3, 4, 7, 8, 10, 11}:
             assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
-    assert ok >= 180, ok
+    assert ok >= 150, ok
 
 
-@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
+@pytest.mark.skipif(not EXAMPLES or not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
 def test_reference_examples_render_on_the_oracle(oracle):
     """Three accepted example scenes (one per formula) rendered small by the
     oracle from the parsed structs: the fractal is in view."""

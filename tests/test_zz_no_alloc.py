@@ -21,9 +21,10 @@ pytestmark = pytest.mark.gpu
 NAMES = ("depth", "iters", "hit", "normal", "shade", "ao", "rgb", "rgb8")
 
 
-def test_noalloc_matches_mbr_render_on_two_calls(renderer):
+@pytest.mark.parametrize("size", [(160, 90), (99, 55)])  # 99 x 55: an odd pixel count
+def test_noalloc_matches_mbr_render_on_two_calls(renderer, size):
     lib = abi.load()
-    sc, cam, p = configs.mandelbox_1080p("A", 160, 90)
+    sc, cam, p = configs.mandelbox_1080p("A", *size)
     renderer.set_scene(sc)
     ref = renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP32, outputs=NAMES)
     want = {k: v.cpu().numpy() for k, v in ref.buffers.items()}
@@ -59,4 +60,33 @@ def test_noalloc_rejects_frames_beyond_its_scratch():
     err = C.create_string_buffer(512)
     st = lib.mbr_render_noalloc(C.byref(sc), C.byref(cam), C.byref(p), C.byref(o), None, err, len(err))
     assert st == abi.MBR_EINVAL
-    assert b"at most 178131 pixels" in err.value, err.value
+    assert b"at most 178130 pixels" in err.value, err.value
+
+
+def test_noalloc_gamma_tables_stay_ordered_on_the_stream(renderer):
+    """Two frames with different gamma values queued back to back on one
+    non-blocking stream: each must be coloured with its own table."""
+    lib = abi.load()
+    sc, cam, p = configs.mandelbox_1080p("A", 96, 64)
+    renderer.set_scene(sc)
+    gammas = (0.6, 1.7)
+    want = []
+    for g in gammas:
+        p.gamma = g
+        want.append(renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP32, outputs=("rgb8",)).buffers["rgb8"].cpu().numpy())
+    s = torch.cuda.Stream()
+    err = C.create_string_buffer(512)
+    bufs = []
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        for g in gammas:
+            p.gamma = g
+            b = alloc_outputs(cam.width * cam.height, renderer.device, ("rgb8",))
+            o = outputs_struct(b, None)
+            st = lib.mbr_render_noalloc(C.byref(sc), C.byref(cam), C.byref(p), C.byref(o), C.c_void_p(s.cuda_stream),
+                                        err, len(err))
+            assert st == abi.MBR_OK, err.value
+            bufs.append(b)
+    s.synchronize()
+    for b, w in zip(bufs, want):
+        assert np.mean(b["rgb8"].cpu().numpy() == w) >= 0.999
