@@ -206,11 +206,33 @@ def load(path: str | None = None) -> C.CDLL:
     return lib
 
 
+# Where the struct defaults come from: this library's mbr_*_defaults, or
+# another library exporting the same functions under another prefix (a CPU
+# program that must not load libmbr.so, see use_defaults_from).
+_defaults_src = None  # (library, prefix)
+
+
+def use_defaults_from(lib: C.CDLL | None, prefix: str = "mbr_") -> None:
+    """Takes the struct defaults from `lib`'s <prefix>scene_defaults,
+    fractal_defaults, camera_defaults and render_params_defaults (same
+    signatures as mbr_*); None restores libmbr.so."""
+    global _defaults_src
+    _defaults_src = None if lib is None else (lib, prefix)
+
+
+def _defaults_fn(name: str):
+    lib, prefix = _defaults_src if _defaults_src is not None else (load(), "mbr_")
+    return getattr(lib, prefix + name)
+
+
+def fractal_defaults(f: Fractal, formula: int) -> None:
+    _defaults_fn("fractal_defaults")(C.byref(f), formula)
+
+
 def scene_defaults(formula: int = FORMULA_MANDELBULB) -> Scene:
-    lib = load()
     s = Scene()
-    lib.mbr_scene_defaults(C.byref(s))
-    lib.mbr_fractal_defaults(C.byref(s.fractal[0]), formula)
+    _defaults_fn("scene_defaults")(C.byref(s))
+    fractal_defaults(s.fractal[0], formula)
     return s
 
 
@@ -222,11 +244,16 @@ def primitive_defaults(kind: int) -> Primitive:
 
 def camera_defaults() -> Camera:
     c = Camera()
-    load().mbr_camera_defaults(C.byref(c))
+    _defaults_fn("camera_defaults")(C.byref(c))
     return c
 
 
 def params_defaults() -> RenderParams:
     p = RenderParams()
-    load().mbr_render_params_defaults(C.byref(p))
+    _defaults_fn("render_params_defaults")(C.byref(p))
     return p
+
+
+def library_loaded() -> bool:
+    """True once this process has loaded libmbr.so through load()."""
+    return _lib is not None

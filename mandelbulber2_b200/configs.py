@@ -51,7 +51,7 @@ def hybrid_scene() -> abi.Scene:
     s.formula_maxiter = 12
     s.fractal[0].bulb_power = 8.0
     s.fractal[0].formula_iterations = 3
-    abi.load().mbr_fractal_defaults(s.fractal[1], abi.FORMULA_MENGER_SPONGE)
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MENGER_SPONGE)
     s.fractal[1].formula_iterations = 9
     s.fractal[1].transf_scale3 = 3.0
     return s
@@ -102,13 +102,14 @@ def mandelbulb_512(width: int = 512, height: int = 512, binary_steps: int = 5):
 
 
 def mandelbox_1080p(view: str = "A", width: int = 1920, height: int = 1080, ao_rays: int = 16,
-                    centre_depth: float | None = None):
+                    centre_depth: float | None = None, camera_rotation=None):
     """Mandelbox s=-1.5, limit 1, min r 0.5 (mR2 0.25), fixed r 1, N=50, bailout 100, r/|dr|.
 
     View A: camera (0,-6,0) aimed at the origin, FOV 53.  View B: camera 1e-5 in
     front of the surface point that view A's centre ray hits (`centre_depth`
     along that ray), same direction, FOV 0.5.  AO: 16 cosine rays from PCG32
-    (state 1234, stream = pixel).
+    (state 1234, stream = pixel).  `camera_rotation(camera) -> (mRot, angles)`
+    places the centre ray (default: the library's mbr_camera_rotation).
     """
     sc = mandelbox_scene(-1.5, 0.5, 50)
     p = base_params(5, 20.0)
@@ -121,16 +122,17 @@ def mandelbox_1080p(view: str = "A", width: int = 1920, height: int = 1080, ao_r
         return sc, cam_a, p
     if centre_depth is None:
         raise ValueError("view B needs the depth of view A's centre ray")
-    d = centre_ray(cam_a)
+    d = centre_ray(cam_a, camera_rotation)
     hit = np.array(cam_a.camera[:]) + d * centre_depth
     pos = hit - d * 1e-5
     cam_b = camera(tuple(pos), target=tuple(hit + d), fov=0.5, width=width, height=height)
     return sc, cam_b, p
 
 
-def centre_ray(cam: abi.Camera) -> np.ndarray:
+def centre_ray(cam: abi.Camera, camera_rotation=None) -> np.ndarray:
     """Unit direction of the ray through the image centre (pixel W/2, H/2)."""
-    from .render import camera_rotation
+    if camera_rotation is None:
+        from .render import camera_rotation
 
     m, _ = camera_rotation(cam)
     fov = 2.0 * math.tan(cam.fov_deg / 360.0 * math.pi)

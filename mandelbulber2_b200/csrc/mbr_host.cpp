@@ -633,7 +633,9 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.de_thresh = p.de_thresh;
   f.shading_enable = p.shading_enable ? 1 : 0;
   f.shadow_enable = p.shadow_enable ? 1 : 0;
-  f.soft_range = std::tan(p.soft_shadow_cone / 180.0 * kPi);  // light.cpp:87, shader_aux_shadow.cpp:64
+  // cLight::softShadowCone is a float (light.h:113, light.cpp:87): the
+  // tangent of shader_aux_shadow.cpp:64 is the float one
+  f.soft_range = double(std::tan(float(p.soft_shadow_cone / 180.0 * kPi)));
   f.penetrating = p.penetrating ? 1 : 0;
   f.ao_fast = (p.ao_fast && p.gi_samples == 0) ? 1 : 0;
   f.ao_quality = p.ao_quality;
@@ -893,7 +895,9 @@ void mbr_camera_defaults(mbr_camera *c) {
   c->camera[0] = 3.0;
   c->camera[1] = -6.0;
   c->camera[2] = 2.0;
-  c->top[2] = 1.0;
+  c->top[0] = -0.1277753;
+  c->top[1] = 0.2555506;
+  c->top[2] = 0.958314;
   c->fov_deg = 53.13;
   c->width = 800;
   c->height = 600;

@@ -1272,7 +1272,10 @@ struct Renderer {
     // directional light: a penetrating one marches delta / resolution (light.cpp:277-290)
     const bool pen = p.penetrating != 0;
     const double distance = pen ? calc_delta(q) / resolution : p.view_distance_max;
-    const double softRange = tan(p.soft_shadow_cone / 180.0 * M_PI);  // light.cpp:87, :64
+    // cLight::softShadowCone is a float (light.h:113, light.cpp:87), so the
+    // tangent is the float one (shader_aux_shadow.cpp:64)
+    const float cone = float(p.soft_shadow_cone / 180.0 * M_PI);
+    const double softRange = std::tan(cone);
     const bool bSoft = !seq.iter_thresh && !seq.interior && softRange > 0.0;  // :71-74
     double start = thr;
     if (seq.interior) start = thr * p.de_factor;
@@ -1411,12 +1414,14 @@ struct Renderer {
     int iters;
     float normal[3];
     float shade, ao, rgb[3];
+    float shadow;  // the AuxShadow factor (1: lit; 0 when the surface faces away)
   };
 
   void shade_pixel(const March &m, uint64_t pixel, Counters &c, PixelOut &po) const {
     po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
     po.shade = 0.0f;
     po.ao = 1.0f;
+    po.shadow = 1.0f;
     if (!m.found) {
       for (int k = 0; k < 3; k++) po.rgb[k] = float(p.background[k]);
       return;
@@ -1447,6 +1452,7 @@ struct Renderer {
           aux = 0.0f;
       }
       shade = s * aux;
+      po.shadow = aux;
     }
     float ao = 1.0f;
     if (fast) ao = float(fast_ao(m.point, n, m.thr, c, &c.ao));
@@ -1611,7 +1617,98 @@ typedef struct oracle_outputs {  // host buffers, same meaning as mbr_outputs
   float *ao;
   float *rgb;
   uint8_t *rgb8;
+  float *shadow;  // the main light's AuxShadow factor per pixel (may be NULL)
 } oracle_outputs;
+
+// The reference's defaults (src/initparameters.cpp) for the C-ABI structs,
+// so that the CPU legs of the benchmark fill their parameters without the
+// product library.  tests/test_oracle_defaults.py holds them equal to the
+// library's mbr_*_defaults.
+void oracle_fractal_defaults(mbr_fractal *f, int formula) {
+  std::memset(f, 0, sizeof(*f));
+  f->formula = formula;
+  f->formula_iterations = 1;     // initparameters.cpp:2109-2125 (node defaults)
+  f->formula_stop_iteration = 250;
+  f->check_for_bailout = 1;
+  f->formula_weight = 1.0;
+  f->bulb_power = 9.0;           // :717
+  f->mandelbox_scale = 2.0;      // :746-750
+  f->mandelbox_folding_limit = 1.0;
+  f->mandelbox_folding_value = 2.0;
+  f->mandelbox_folding_min_radius = 0.5;
+  f->mandelbox_folding_fixed_radius = 1.0;
+  f->transf_scale3 = 3.0;        // :1010
+  f->ifs_scale = 2.0;            // :724-743
+  f->ifs_offset[0] = 1.0;
+  for (int i = 0; i < 9; i++) {
+    f->ifs_direction[i][0] = 1.0;
+    f->ifs_intensity[i] = 1.0;
+  }
+}
+
+void oracle_scene_defaults(mbr_scene *s) {
+  std::memset(s, 0, sizeof(*s));
+  s->n_fractals = 1;             // :128-157, node :2102-2125
+  s->formula_maxiter = 250;
+  s->repeat_from = 1;
+  s->use_default_bailout = 1;
+  s->min_n = 1;
+  s->bailout = 100.0;
+  for (int i = 0; i < 3; i++) s->fractal_constant_factor[i] = 1.0;
+  oracle_fractal_defaults(&s->fractal[0], MBR_FORMULA_MANDELBULB);
+  for (int i = 1; i < MBR_MAX_FRACTALS; i++) oracle_fractal_defaults(&s->fractal[i], MBR_FORMULA_NONE);
+}
+
+void oracle_camera_defaults(mbr_camera *c) {
+  std::memset(c, 0, sizeof(*c));
+  c->camera[0] = 3.0;            // :113-120
+  c->camera[1] = -6.0;
+  c->camera[2] = 2.0;
+  c->top[0] = -0.1277753;
+  c->top[1] = 0.2555506;
+  c->top[2] = 0.958314;
+  c->fov_deg = 53.13;
+  c->width = 800;                // :173-174
+  c->height = 600;
+}
+
+void oracle_render_params_defaults(mbr_render_params *p) {
+  std::memset(p, 0, sizeof(*p));
+  p->detail_level = 1.0;         // :133-167
+  p->de_factor = 1.0;
+  p->view_distance_max = 50.0;
+  p->smoothness = 1.0;
+  p->max_raymarching_steps = 10000;
+  p->binary_steps = 30;          // render_worker.cpp:854
+  p->refine = MBR_REFINE_REFERENCE;
+  p->jitter = 1;
+  p->de_thresh = 0.01;
+  p->shading_enable = 1;
+  p->shadow_enable = 1;
+  p->light_direction[0] = 1.0;
+  p->light_direction[1] = -1.0;
+  p->light_direction[2] = 1.0;
+  p->light_intensity = 1.0;
+  p->material_shading = 1.0;
+  p->albedo = 1.0;
+  p->dof_focus = 3.0;
+  p->gi_sky = 0.3;
+  p->gi_sun = 3.0;
+  p->brightness = 1.0;           // :208-212
+  p->contrast = 1.0;
+  p->gamma = 1.0;
+  p->saturation = 1.0;
+  p->soft_shadow_cone = 1.0;     // light 1, :1901, 1919
+  p->penetrating = 1;
+  p->ao_quality = 4;             // :214-216
+  p->ao_fast_tune = 1.0;
+  p->abs_max_marching_step = 3.0;  // :159-165
+  p->abs_min_marching_step = 1e-15;
+  p->rel_max_marching_step = 1e4;
+  p->rel_min_marching_step = 1e-2;
+  p->detail_size_max = 1.0;
+  p->detail_size_min = 1e-12;
+}
 
 int oracle_threads(void) {
 #ifdef _OPENMP
@@ -1624,6 +1721,14 @@ int oracle_threads(void) {
 // Renders rows [row0, row1) (all columns) of the frame.  Rows are handed to
 // threads one at a time, dynamically (the cScheduler line model,
 // scheduler.cpp:122-183).  Returns 0 on success.
+//
+// params->jitter == 2 (the oracle only): the march jitter draws from ONE
+// Park-Miller state seeded with params->seed and consumed in pixel order
+// (rows top to bottom, pixels left to right), as the reference's
+// process-global Random() is consumed by one render thread without
+// progressive passes (common_math.cpp:47-72; render_worker.cpp:126-134,
+// 811-815).  It renders on one thread, so that golden frames of the
+// reference's own render worker can be reproduced bit for bit.
 int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
                   const oracle_outputs *out, int row0, int row1, int nthreads, mbr_stats *stats) {
   Renderer R;
@@ -1632,6 +1737,10 @@ int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_rende
   const int W = cam->width;
   std::atomic<uint64_t> tot[10];
   for (auto &t : tot) t = 0;
+  const bool global_stream = params->jitter == 2;
+  ParkMiller gpm;
+  gpm.s = params->seed;
+  if (global_stream) nthreads = 1;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel
@@ -1655,6 +1764,7 @@ int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_rende
           po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
           po.shade = 0.0f;
           po.ao = 1.0f;
+          po.shadow = 1.0f;
           po.rgb[0] = po.rgb[1] = po.rgb[2] = 0.0f;
         } else if (params->gi_samples > 0) {
           double acc = 0.0;
@@ -1669,14 +1779,16 @@ int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_rende
           po.normal[0] = po.normal[1] = po.normal[2] = 0.0f;
           po.shade = 0.0f;
           po.ao = 1.0f;
+          po.shadow = 1.0f;
           po.rgb[0] = po.rgb[1] = po.rgb[2] = v;
         } else {
           double ix, iy;
           R.image_point(double(x), double(y), &ix, &iy);
           D3 dir = R.view_vector(ix, iy);
           dir = normalize(dir);
-          ParkMiller pm = pm_for_ray(pixel, params->seed);
+          ParkMiller pm = global_stream ? gpm : pm_for_ray(pixel, params->seed);
           m = R.ray_marching(R.camera, dir, params->view_distance_max, pm, c);
+          if (global_stream) gpm = pm;
           R.shade_pixel(m, pixel, c, po);
           po.hit = m.found;
           po.depth = m.found ? m.depth : 1e20;
@@ -1692,6 +1804,7 @@ int oracle_render(const mbr_scene *scene, const mbr_camera *cam, const mbr_rende
         if (out->ao) out->ao[o] = po.ao;
         if (out->rgb) for (int k = 0; k < 3; k++) out->rgb[o * 3 + k] = po.rgb[k];
         if (out->rgb8) to_rgb8(po.rgb, *params, R.gamma, &out->rgb8[o * 3]);
+        if (out->shadow) out->shadow[o] = po.shadow;
       }
     }
     tot[0] += c.de; tot[1] += c.iters; tot[2] += c.march; tot[3] += c.binary; tot[4] += c.normal;

@@ -20,7 +20,8 @@ _P = C.c_void_p
 
 
 class OracleOutputs(C.Structure):
-    _fields_ = [(n, C.c_void_p) for n in ("depth", "iters", "hit", "normal", "shade", "ao", "rgb", "rgb8")]
+    _fields_ = [(n, C.c_void_p) for n in ("depth", "iters", "hit", "normal", "shade", "ao", "rgb", "rgb8",
+                                          "shadow")]
 
 
 def build() -> None:
@@ -60,16 +61,31 @@ class Oracle:
         L.oracle_pixel_gradients.argtypes = [C.POINTER(abi.Scene), C.POINTER(abi.Camera),
                                              C.POINTER(abi.RenderParams), _P, _P, _P, _P, _P]
         L.oracle_threads.restype = C.c_int
+        L.oracle_scene_defaults.argtypes = [C.POINTER(abi.Scene)]
+        L.oracle_fractal_defaults.argtypes = [C.POINTER(abi.Fractal), C.c_int]
+        L.oracle_camera_defaults.argtypes = [C.POINTER(abi.Camera)]
+        L.oracle_render_params_defaults.argtypes = [C.POINTER(abi.RenderParams)]
+        for f in ("oracle_scene_defaults", "oracle_fractal_defaults", "oracle_camera_defaults",
+                  "oracle_render_params_defaults"):
+            getattr(L, f).restype = None
 
     def threads(self) -> int:
         return self.lib.oracle_threads()
+
+    def camera_rotation(self, cam):
+        """(mRot row-major as a list of 9, [yaw, pitch, roll]) of PrepareMainVectors."""
+        m = (C.c_double * 10)()
+        ang = (C.c_double * 3)()
+        self.lib.oracle_camera(C.byref(cam), m, ang)
+        return list(m)[:9], list(ang)
 
     def render(self, scene, cam, params, rows=None, threads: int = 0,
                outputs=("depth", "iters", "hit", "normal", "shade", "ao", "rgb", "rgb8")):
         r0, r1 = rows if rows is not None else (0, cam.height)
         n = (r1 - r0) * cam.width
         spec = {"depth": (np.float64, 1), "iters": (np.int32, 1), "hit": (np.uint8, 1), "normal": (np.float32, 3),
-                "shade": (np.float32, 1), "ao": (np.float32, 1), "rgb": (np.float32, 3), "rgb8": (np.uint8, 3)}
+                "shade": (np.float32, 1), "ao": (np.float32, 1), "rgb": (np.float32, 3), "rgb8": (np.uint8, 3),
+                "shadow": (np.float32, 1)}
         bufs = {}
         o = OracleOutputs()
         for k in outputs:

@@ -1,0 +1,2 @@
+#pragma once
+#include "qshim_core.h"

@@ -12,6 +12,16 @@ sources, compiled unchanged into oracle/_ref/libref.so by oracle/build_ref.sh:
                     CalculateViewVector directions
   random_kat.json   Park-Miller Random()/RandomInt() sequences
 
+and, from the reference's sources for the whole path compiled into
+oracle/_ref/librefpipe.so (parameter containers with the reference's
+defaults, objects tree, sequences, Compute, CalculateDistance, the render
+worker with its shaders, cImage):
+
+  pipeline_kat.json CalculateDistance and the hybrid sequence of the scene
+                    variants of pipeline_cases.cases() at seeded points
+  render_kat.json   small frames of pipeline_cases.render_cases() rendered by
+                    cRenderWorker::doWork: z-buffer, world normals, shadows
+
 Doubles are stored with float.hex() so the comparison is bit-exact.
 Run: python tests/golden/make_golden.py  (needs the reference tree to build libref.so)
 """
@@ -29,6 +39,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle.oracle import Reference  # noqa: E402
+from tests.golden.pipeline_cases import cases, render_cases  # noqa: E402
 
 FORMULAS = [
     # (name, formula id, params for ref_formula_step, scene fields)
@@ -189,6 +200,52 @@ def random_kats(ref: Reference) -> list:
     return out
 
 
+def pipeline_kats() -> dict:
+    """CalculateDistance (both normal modes, two detail sizes) at 48 seeded
+    points per scene, and the scene's sequence."""
+    from oracle.refpipe import RefPipeline
+
+    rng = np.random.default_rng(20241)
+    out = {}
+    for name, sc in cases().items():
+        r = RefPipeline()
+        r.configure(sc)
+        pts = rng.uniform(-2.0, 2.0, size=(48, 3))
+        entry = {"points": [hexs(p) for p in pts], "runs": []}
+        for nm in (0, 1):
+            for det in (1e-3, 0.05):
+                d, it = r.distance(pts, det, bool(nm))
+                entry["runs"].append({"normal_mode": nm, "detail": det.hex(), "dist": hexs(d),
+                                      "iters": [int(x) for x in it]})
+        entry["sequence"] = r.sequence()
+        out[name] = entry
+        r.close()
+    return out
+
+
+def _pack(a: np.ndarray) -> str:
+    import base64
+    import zlib
+
+    return base64.b64encode(zlib.compress(np.ascontiguousarray(a).astype("<f4").tobytes(), 9)).decode()
+
+
+def render_kats() -> dict:
+    from oracle.refpipe import RefPipeline
+
+    out = {}
+    for name, sc, cam, p in render_cases():
+        r = RefPipeline()
+        r.configure(sc, cam, p)
+        r.prepare()
+        light = r.light_direction(0)
+        z, nw, sh, _ = r.render(cam.width, cam.height, seed=1)
+        out[name] = {"width": cam.width, "height": cam.height, "seed": 1, "light": [float(v).hex() for v in light],
+                     "zbuffer": _pack(z), "normal_world": _pack(nw), "shadow": _pack(sh[:, 0])}
+        r.close()
+    return out
+
+
 def main() -> None:
     ref = Reference()
     with open(os.path.join(HERE, "formula_kat.json"), "w") as f:
@@ -199,6 +256,13 @@ def main() -> None:
         json.dump(projection_kats(ref), f, indent=1)
     with open(os.path.join(HERE, "random_kat.json"), "w") as f:
         json.dump(random_kats(ref), f)
+    from oracle.refpipe import available
+
+    if available():
+        with open(os.path.join(HERE, "pipeline_kat.json"), "w") as f:
+            json.dump(pipeline_kats(), f, separators=(",", ":"))
+        with open(os.path.join(HERE, "render_kat.json"), "w") as f:
+            json.dump(render_kats(), f, indent=1)
     print("golden vectors written to", HERE)
 
 

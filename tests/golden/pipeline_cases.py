@@ -1,0 +1,179 @@
+"""Scene variants whose distance estimates are pinned against the reference's
+own CalculateDistance (oracle/_ref/librefpipe.so, built from the reference's
+sources): every formula built here, the Mandelbox rotations, julia mode and
+the c constant factor, the DE-function and bailout switches, minN, interior
+and iteration-threshold modes, and hybrid sequences with weights, start/stop
+iterations, repeat_from, check_for_bailout and the c-constant rule.  Shared
+by make_golden.py (which writes the fixture) and tests/test_golden.py.
+"""
+from mandelbulber2_b200 import abi, configs
+
+
+def _box(**kw):
+    s = configs.mandelbox_scene(kw.pop("scale", -1.5), kw.pop("min_r", 0.5), kw.pop("maxiter", 50))
+    return s
+
+
+def cases():
+    out = {}
+    out["bulb_p8"] = configs.mandelbulb_scene(8.0, 250)
+    s = configs.mandelbulb_scene(5.0, 60)
+    s.fractal[0].bulb_alpha_angle_offset = 12.0
+    s.fractal[0].bulb_beta_angle_offset = -7.0
+    out["bulb_p5_angles"] = s
+    s = configs.mandelbulb_scene(8.0, 40)
+    s.julia_mode = 1
+    s.julia_c[:] = [0.3, -0.2, 0.1]
+    out["bulb_julia"] = s
+    s = configs.mandelbulb_scene(8.0, 40)
+    s.fractal_constant_factor[:] = [1.2, 1.0, 0.9]
+    out["bulb_cmul"] = s
+    s = configs.mandelbulb_scene(8.0, 40)
+    s.delta_de_function = abi.DE_LINEAR
+    out["bulb_linear_de"] = s
+    out["box_s-1.5"] = configs.mandelbox_scene(-1.5, 0.5, 50)
+    s = configs.mandelbox_scene(2.0, 0.5, 30)
+    s.fractal[0].mandelbox_offset[:] = [0.1, -0.2, 0.05]
+    out["box_s2_offset"] = s
+    s = configs.mandelbox_scene(-1.8, 0.45, 30)
+    f = s.fractal[0]
+    f.mandelbox_rotations_enabled = 1
+    f.mandelbox_rotation_neg[0][:] = [10.0, 0.0, 5.0]
+    f.mandelbox_rotation_pos[1][:] = [0.0, -8.0, 0.0]
+    f.mandelbox_rotation_pos[2][:] = [3.0, 4.0, -6.0]
+    out["box_rotated_folds"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.fractal[0].mandelbox_main_rotation_enabled = 1
+    s.fractal[0].mandelbox_rotation_main[:] = [15.0, -10.0, 25.0]
+    out["box_main_rotation"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.min_n = 4
+    s.use_default_bailout = 0
+    s.bailout = 40.0
+    s.linear_de_offset = 0.05
+    out["box_minn_bailout_offset"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.interior_mode = 1
+    out["box_interior"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.iteration_threshold_mode = 1
+    out["box_iter_thresh"] = s
+    out["menger_12"] = configs.menger_scene(12)
+    s = configs.menger_scene(8)
+    s.fractal[0].transf_scale3 = 2.6
+    s.fractal[0].dont_add_c_constant = 1
+    out["menger_s2.6_addc"] = s
+    s = abi.scene_defaults(abi.FORMULA_MANDELBULB_POWER2)
+    s.formula_maxiter = 40
+    out["bulb_power2"] = s
+    s = abi.scene_defaults(abi.FORMULA_HYPERCOMPLEX)
+    s.formula_maxiter = 40
+    out["hypercomplex"] = s
+    s = abi.scene_defaults(abi.FORMULA_XENODREAMBUIE)
+    s.formula_maxiter = 40
+    s.fractal[0].bulb_power = 5.0
+    out["xenodreambuie_p5"] = s
+    s = abi.scene_defaults(abi.FORMULA_KALEIDOSCOPIC_IFS)
+    s.formula_maxiter = 30
+    f = s.fractal[0]
+    f.ifs_menger_sponge_mode = 1
+    f.ifs_scale = 3.0
+    f.ifs_rotation_enabled = 1
+    f.ifs_rotation[:] = [5.0, 10.0, 0.0]
+    out["ifs_menger_mode"] = s
+    s = abi.scene_defaults(abi.FORMULA_KALEIDOSCOPIC_IFS)
+    s.formula_maxiter = 30
+    f = s.fractal[0]
+    f.ifs_abs_x = f.ifs_abs_y = f.ifs_abs_z = 1
+    for k, d in enumerate(([1.0, 1.0, 0.0], [0.0, 1.0, 1.0], [1.0, 0.0, 1.0])):
+        f.ifs_enabled[k] = 1
+        f.ifs_direction[k][:] = d
+        f.ifs_distance[k] = 0.1 * (k + 1)
+        f.ifs_rotations[k][:] = [k * 7.0, 0.0, -k * 3.0]
+    out["ifs_vectors"] = s
+    out["hybrid_bulb3_menger9"] = configs.hybrid_scene()
+    s = configs.hybrid_scene()
+    s.fractal[0].formula_weight = 0.6
+    s.fractal[1].formula_start_iteration = 2
+    s.fractal[1].formula_stop_iteration = 10
+    s.formula_maxiter = 20
+    out["hybrid_weight_startstop"] = s
+    s = abi.scene_defaults(abi.FORMULA_MANDELBOX)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 3
+    s.formula_maxiter = 24
+    s.fractal[0].mandelbox_scale = -1.6
+    s.fractal[0].formula_iterations = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBULB)
+    s.fractal[1].bulb_power = 4.0
+    s.fractal[1].check_for_bailout = 0
+    abi.fractal_defaults(s.fractal[2], abi.FORMULA_MENGER_SPONGE)
+    s.fractal[2].formula_iterations = 3
+    s.fractal[2].dont_add_c_constant = 1
+    s.repeat_from = 2
+    out["hybrid_box_bulb_menger_repeat2"] = s
+    return out
+
+
+def render_cases():
+    """Small frames rendered by the reference's own render worker (one
+    thread, lines in order) with the march jitter drawn from the global
+    Park-Miller stream seeded with 1: (name, scene, camera, params).  The
+    light is the reference's default main light (its direction is taken from
+    the reference and stored with each frame); shading is Lambert with a hard
+    or soft, penetrating or not, shadow; AO and specular highlights are off."""
+    out = []
+
+    def params(**kw):
+        p = configs.base_params(30, kw.pop("vdm", 20.0))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    sc, cam, p = configs.mandelbulb_512(40, 30, binary_steps=30)
+    out.append(("bulb_p8", sc, cam, p))
+    sc, cam, p = configs.mandelbox_1080p("A", 48, 27, ao_rays=0)
+    p.binary_steps = 30
+    out.append(("box_view_a", sc, cam, p))
+    out.append(("menger", configs.menger_scene(12), configs.camera((0.0, -3.0, 0.5), width=32, height=32),
+                params()))
+    out.append(("hybrid_bulb_menger", configs.hybrid_scene(), configs.camera((0.0, -3.0, 0.0), width=40, height=30),
+                params()))
+    cam = configs.camera((0.15, -1.4, 0.3), fov=360.0, width=48, height=36)
+    cam.perspective_type = abi.PROJECTION_EQUIRECTANGULAR
+    out.append(("bulb_equirectangular_4x3", configs.mandelbulb_scene(8.0, 20), cam, params()))
+    sc, cam, p = configs.mandelbox_1080p("A", 48, 27, ao_rays=0)
+    p.binary_steps = 30
+    p.advanced_quality = 1
+    p.detail_size_max = 0.01
+    p.detail_size_min = 0.004
+    p.abs_max_marching_step = 0.4
+    p.rel_min_marching_step = 0.6
+    out.append(("box_advanced_quality", sc, cam, p))
+    out.append(("bulb_soft_penetrating", configs.mandelbulb_scene(8.0, 40),
+                configs.camera((0.4, -2.4, 0.6), width=32, height=24), params(soft_shadow_cone=10.0, penetrating=1)))
+    cases_ = cases()
+    out.append(("box_rotated_folds", cases_["box_rotated_folds"], configs.camera((0.0, -5.0, 1.0), width=40, height=24),
+                params()))
+    cam = configs.camera((0.1, -2.2, 0.4), fov=160.0, width=32, height=32)
+    cam.perspective_type = abi.PROJECTION_FISH_EYE
+    out.append(("bulb_fish_eye", configs.mandelbulb_scene(8.0, 20), cam, params()))
+    cam = configs.camera((0.4, -2.2, 0.9), width=32, height=24)
+    cam.legacy_coordinate_system = 1
+    out.append(("bulb_legacy_coordinates", configs.mandelbulb_scene(8.0, 20), cam, params()))
+    out.append(("box_constant_threshold", configs.mandelbox_scene(-1.5, 0.5, 30),
+                configs.camera((0.0, -6.0, 0.0), width=40, height=24), params(constant_de_threshold=1, de_thresh=0.02)))
+    s = abi.scene_defaults(abi.FORMULA_KALEIDOSCOPIC_IFS)
+    s.formula_maxiter = 30
+    f = s.fractal[0]
+    f.ifs_scale = 3.0
+    f.ifs_offset[:] = [1.0, 1.0, 1.0]
+    f.ifs_menger_sponge_mode = 1
+    f.ifs_abs_x = f.ifs_abs_y = f.ifs_abs_z = 1
+    for k, d in enumerate(([1.0, -1.0, 0.0], [0.0, 1.0, -1.0], [1.0, 0.0, -1.0])):
+        f.ifs_enabled[k] = 1
+        f.ifs_direction[k][:] = d
+    f.ifs_rotation_enabled = 1
+    f.ifs_rotation[:] = [20.0, 0.0, 10.0]
+    out.append(("ifs_menger", s, configs.camera((1.2, -2.2, 1.5), width=32, height=24), params()))
+    return out
