@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MBR_ABI_VERSION 3
+#define MBR_ABI_VERSION 4
 
 /* Number of formula slots of one hybrid sequence (the reference's nine
  * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
@@ -240,6 +240,25 @@ typedef struct mbr_scene {
   int32_t n_primitives;        /* 0..MBR_MAX_PRIMITIVES, default 0 */
   int32_t reserved_prim;
   mbr_primitive primitive[MBR_MAX_PRIMITIVES];
+  /* "limits_enabled": outside the box [limit_min, limit_max] by more than the
+   * detail size, CalculateDistance returns the distance to the box without
+   * iterating (src/calculate_distance.cpp:261-275); a soft shadow ignores
+   * samples outside it (src/shader_aux_shadow.cpp:130-147) */
+  int32_t limits_enabled;      /* default 0 */
+  /* the global folds applied before every formula iteration
+   * (src/compute_fractal.cpp:190-202, formula/definition/
+   * legacy_fractal_transforrms.cpp:43-103): "box_folding" with
+   * box_folding_limit / _value, "spherical_folding" with
+   * spherical_folding_inner / _outer */
+  int32_t box_folding;         /* default 0 */
+  int32_t spherical_folding;   /* default 0 */
+  int32_t reserved_folds;
+  double limit_min[3];         /* default (-10, -10, -10) */
+  double limit_max[3];         /* default (10, 10, 10) */
+  double box_folding_limit;    /* default 1 */
+  double box_folding_value;    /* default 2 */
+  double spherical_folding_inner; /* default 0.5 */
+  double spherical_folding_outer; /* default 1 */
 } mbr_scene;
 
 /* params::enumPerspectiveType (src/projection_3d.hpp:44-50): the view

@@ -87,6 +87,10 @@ class Scene(C.Structure):
         ("fractal_constant_factor", D3), ("initial_waxis", C.c_double), ("linear_de_offset", C.c_double),
         ("fractal", Fractal * MBR_MAX_FRACTALS),
         ("n_primitives", C.c_int32), ("reserved_prim", C.c_int32), ("primitive", Primitive * MBR_MAX_PRIMITIVES),
+        ("limits_enabled", C.c_int32), ("box_folding", C.c_int32), ("spherical_folding", C.c_int32),
+        ("reserved_folds", C.c_int32), ("limit_min", D3), ("limit_max", D3), ("box_folding_limit", C.c_double),
+        ("box_folding_value", C.c_double), ("spherical_folding_inner", C.c_double),
+        ("spherical_folding_outer", C.c_double),
     ]
 
 

@@ -390,7 +390,8 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
                                           "quality clamps, no constant threshold)");
   if (sc->mbrot.folds || sc->mbrot.main)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the Mandelbox without rotations");
-  if (sc->n_prims > 0) return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers scenes without primitives");
+  if (sc->n_prims > 0 || sc->limits || sc->gbox || sc->gsph)
+    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers scenes without primitives, limit box or global folds");
   if (sc->is_hybrid || sc->has_w || sc->iter_thresh || sc->interior ||
       (sc->slot[0].formula != MBR_FORMULA_MANDELBULB && sc->slot[0].formula != MBR_FORMULA_MANDELBOX))
     return set_err(ctx, MBR_EUNSUPPORTED,

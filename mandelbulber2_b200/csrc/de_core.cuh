@@ -497,9 +497,69 @@ __device__ __noinline__ T prim_distance(const DevPrim &q, T wx, T wy, T wz) {
 // F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
 // the three specialised formulas) or F_EXT (generic with every formula and
 // the Mandelbox rotations).  W: 4-D state.
+// The limit box of CalculateDistance (calculate_distance.cpp:261-275): the
+// largest of the per-axis distances outside [lim_min, lim_max].
+template <class T>
+__device__ __forceinline__ T limit_box_distance(const DevScene &sc, T px, T py, T pz) {
+  const bool f = sizeof(T) == 4;
+  const T bx0 = px - T(f ? sc.flim_max[0] : sc.lim_max[0]), bx1 = -(px - T(f ? sc.flim_min[0] : sc.lim_min[0]));
+  const T by0 = py - T(f ? sc.flim_max[1] : sc.lim_max[1]), by1 = -(py - T(f ? sc.flim_min[1] : sc.lim_min[1]));
+  const T bz0 = pz - T(f ? sc.flim_max[2] : sc.lim_max[2]), bz1 = -(pz - T(f ? sc.flim_min[2] : sc.lim_min[2]));
+  const T bx = (bx0 < bx1) ? bx1 : bx0, by = (by0 < by1) ? by1 : by0, bz = (bz0 < bz1) ? bz1 : bz0;
+  T m = bx;
+  if (m < by) m = by;
+  if (m < bz) m = bz;
+  return m;
+}
+
+// The global folds before a formula iteration (compute_fractal.cpp:190-202):
+// BoxFolding and SphericalFolding (legacy_fractal_transforrms.cpp:43-103),
+// each followed by r = |z|.
+template <class T, bool W>
+__device__ __forceinline__ void global_folds(const DevScene &sc, V4<T> &z, T &r, T &DE) {
+  const bool f = sizeof(T) == 4;
+  if (sc.gbox) {
+    const T lim = T(f ? sc.fgbox_limit : sc.gbox_limit), val = T(f ? sc.fgbox_value : sc.gbox_value);
+    if (z.x > lim) z.x = val - z.x;
+    else if (z.x < -lim) z.x = -val - z.x;
+    if (z.y > lim) z.y = val - z.y;
+    else if (z.y < -lim) z.y = -val - z.y;
+    if (z.z > lim) z.z = val - z.z;
+    else if (z.z < -lim) z.z = -val - z.z;
+    r = len4<T, W>(z);
+  }
+  if (sc.gsph) {
+    const T fR2 = T(f ? sc.fgsph_fr2 : sc.gsph_fr2), mR2 = T(f ? sc.fgsph_mr2 : sc.gsph_mr2);
+    const T r2 = r * r;
+    const T f1 = fR2 / mR2;
+    if (r2 < mR2) {
+      z.x = z.x * f1;
+      z.y = z.y * f1;
+      z.z = z.z * f1;
+      if (W) z.w = z.w * f1;
+      DE = DE * f1;
+    } else if (r2 < fR2) {
+      const T f2 = fR2 / r2;
+      z.x = z.x * f2;
+      z.y = z.y * f2;
+      z.z = z.z * f2;
+      if (W) z.w = z.w * f2;
+      DE = DE * f2;
+    }
+    r = len4<T, W>(z);
+  }
+}
+
 template <class T, int F, bool W>
 __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
                                            int *iters_out) {
+  if (F == F_EXT && sc.limits) {  // outside the limit box: its distance, no iteration
+    const T lbd = limit_box_distance<T>(sc, px, py, pz);
+    if (lbd > detail) {
+      *iters_out = 0;
+      return lbd;
+    }
+  }
   const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
   const int maxN = sc.formula_maxiter * mult;
   V4<T> z{px, py, pz, W ? T(sc.w0) : T(0.0)};
@@ -513,6 +573,7 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
     lastZ = z;
     const int k = (F > 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]));
     const DevSlot &s = sc.slot[k];
+    if (F == F_EXT) global_folds<T, W>(sc, z, r, DE);
     const V4<T> tempZ = z;
     const T tempDE = DE;
     if (F > 0) {

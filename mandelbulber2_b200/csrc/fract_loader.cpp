@@ -623,18 +623,32 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     if (parse_double(value, d)) p->rel_min_marching_step = d; else R.bad(name, value);
   } else if (name == "rel_max_marching_step") {
     if (parse_double(value, d)) p->rel_max_marching_step = d; else R.bad(name, value);
-  } else if (name == "limits_enabled" || name == "box_folding" || name == "spherical_folding" ||
-             name == "stereo_enabled" || name == "slow_shading") {
-    // switches that change the geometry (the limit box, calculate_distance.cpp:261-275;
-    // the global folds, compute_fractal.cpp:190-202), the image plane (stereo,
-    // render_worker.cpp:107-108, 158-161, 268) or the normals (iteration-count normals,
+  } else if (name == "limits_enabled") {  // the limit box (calculate_distance.cpp:261-275)
+    if (parse_bool(value, b)) sc->limits_enabled = b; else R.bad(name, value);
+  } else if (name == "limit_min") {
+    if (parse_vec3(value, v)) std::memcpy(sc->limit_min, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "limit_max") {
+    if (parse_vec3(value, v)) std::memcpy(sc->limit_max, v, sizeof(v)); else R.bad(name, value);
+  } else if (name == "box_folding") {  // the global folds (compute_fractal.cpp:190-202)
+    if (parse_bool(value, b)) sc->box_folding = b; else R.bad(name, value);
+  } else if (name == "box_folding_limit") {
+    if (parse_double(value, d)) sc->box_folding_limit = d; else R.bad(name, value);
+  } else if (name == "box_folding_value") {
+    if (parse_double(value, d)) sc->box_folding_value = d; else R.bad(name, value);
+  } else if (name == "spherical_folding") {
+    if (parse_bool(value, b)) sc->spherical_folding = b; else R.bad(name, value);
+  } else if (name == "spherical_folding_inner") {
+    if (parse_double(value, d)) sc->spherical_folding_inner = d; else R.bad(name, value);
+  } else if (name == "spherical_folding_outer") {
+    if (parse_double(value, d)) sc->spherical_folding_outer = d; else R.bad(name, value);
+  } else if (name == "stereo_enabled" || name == "slow_shading") {
+    // switches that change the image plane (stereo, render_worker.cpp:107-108,
+    // 158-161, 268) or the normals (iteration-count normals,
     // shader_calculate_normals.cpp:82-109): refused when on
     if (!parse_bool(value, b)) R.bad(name, value);
     else if (b) R.unsupported.push_back(name + " true (" +
-                                        (name == "limits_enabled" ? std::string("limit box")
-                                         : name == "stereo_enabled" ? std::string("stereo image")
-                                         : name == "slow_shading" ? std::string("iteration-count normals")
-                                                                  : std::string("global folding")) + ")");
+                                        (name == "stereo_enabled" ? std::string("stereo image")
+                                                                  : std::string("iteration-count normals")) + ")");
   } else if (name == "constant_DE_threshold") {
     if (parse_bool(value, b)) p->constant_de_threshold = b; else R.bad(name, value);
   } else if (name == "DE_thresh") {

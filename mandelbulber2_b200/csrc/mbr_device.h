@@ -135,11 +135,17 @@ struct DevScene {
   int32_t n_prims;         // primitives joined by union (F_EXT iteration only)
   int32_t pad2;
   DevPrim prim[MBR_MAX_PRIMITIVES];
+  // limit box and global folds (F_EXT iteration only)
+  int32_t limits, gbox, gsph, pad4;
+  double lim_min[3], lim_max[3];
+  double gbox_limit, gbox_value, gsph_fr2, gsph_mr2;  // spherical: outer^2, inner^2
+  float flim_min[3], flim_max[3];
+  float fgbox_limit, fgbox_value, fgsph_fr2, fgsph_mr2;
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 
 __host__ __device__ inline bool scene_extended(const DevScene &sc) {
-  return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0;
+  return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0 || sc.limits || sc.gbox || sc.gsph;
 }
 
 // Everything about one frame that is not the scene: camera, march and

@@ -480,6 +480,31 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
                      k);
   d.n_prims = sc.n_primitives;
   if (d.n_prims > 0) d.generic = 1;  // the union is evaluated by the reference-order iteration only
+  // limit box (fractparams.cpp:175-177) and global folds (fractparams.cpp:346-351)
+  if (!finite3(sc.limit_min) || !finite3(sc.limit_max) || !std::isfinite(sc.box_folding_limit) ||
+      !std::isfinite(sc.box_folding_value) || !std::isfinite(sc.spherical_folding_inner) ||
+      !std::isfinite(sc.spherical_folding_outer))
+    return set_err(ctx, MBR_EINVAL, "non-finite limit box or global fold parameter");
+  if (sc.spherical_folding && !(sc.spherical_folding_inner != 0.0))
+    return set_err(ctx, MBR_EINVAL, "spherical_folding_inner must be non-zero");
+  d.limits = sc.limits_enabled ? 1 : 0;
+  d.gbox = sc.box_folding ? 1 : 0;
+  d.gsph = sc.spherical_folding ? 1 : 0;
+  for (int i = 0; i < 3; i++) {
+    d.lim_min[i] = sc.limit_min[i];
+    d.lim_max[i] = sc.limit_max[i];
+    d.flim_min[i] = float(sc.limit_min[i]);
+    d.flim_max[i] = float(sc.limit_max[i]);
+  }
+  d.gbox_limit = sc.box_folding_limit;
+  d.gbox_value = sc.box_folding_value;
+  d.gsph_fr2 = sc.spherical_folding_outer * sc.spherical_folding_outer;
+  d.gsph_mr2 = sc.spherical_folding_inner * sc.spherical_folding_inner;
+  d.fgbox_limit = float(d.gbox_limit);
+  d.fgbox_value = float(d.gbox_value);
+  d.fgsph_fr2 = float(d.gsph_fr2);
+  d.fgsph_mr2 = float(d.gsph_mr2);
+  if (d.limits || d.gbox || d.gsph) d.generic = 1;  // the reference-order iteration carries them
   *out = d;
   return MBR_OK;
 }
@@ -886,6 +911,15 @@ void mbr_scene_defaults(mbr_scene *s) {
   for (int i = 0; i < 3; i++) s->fractal_constant_factor[i] = 1.0;
   mbr_fractal_defaults(&s->fractal[0], MBR_FORMULA_MANDELBULB);
   for (int i = 1; i < MBR_MAX_FRACTALS; i++) mbr_fractal_defaults(&s->fractal[i], MBR_FORMULA_NONE);
+  // initparameters.cpp:143-145, 199-204
+  for (int i = 0; i < 3; i++) {
+    s->limit_min[i] = -10.0;
+    s->limit_max[i] = 10.0;
+  }
+  s->box_folding_limit = 1.0;
+  s->box_folding_value = 2.0;
+  s->spherical_folding_inner = 0.5;
+  s->spherical_folding_outer = 1.0;
 }
 
 void mbr_camera_defaults(mbr_camera *c) {

@@ -349,7 +349,11 @@ __device__ double aux_shadow(const DevScene &sc, const DevFrame &fr, D3 q, doubl
   for (double i = start; i < distance; i += step) {
     const D3 point2 = d3ray(q, L, i);
     const double dist = de_eval<T, F, W>(sc, point2, thr, false, &it, tc);
-    if (soft) {  // :142-151
+    // a soft shadow ignores samples outside the limit box (:130-147)
+    const bool outside = F == F_EXT && sc.limits &&
+                         (point2.x < sc.lim_min[0] || point2.x > sc.lim_max[0] || point2.y < sc.lim_min[1] ||
+                          point2.y > sc.lim_max[1] || point2.z < sc.lim_min[2] || point2.z > sc.lim_max[2]);
+    if (soft && !outside) {  // :142-151
       double angle = (dist - double(dist_thresh_f)) / i;
       if (angle < 0) angle = 0;
       if (dist < double(dist_thresh_f)) angle = 0;

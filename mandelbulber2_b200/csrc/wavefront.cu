@@ -470,8 +470,10 @@ struct PrecHybT {
     const DevSlot &s = sc.slot[k];
     V4<float> z{e.zx, e.zy, e.zz, 0.0f};
     const V4<float> last = z;
-    const float tempDE = e.dr;
     float de = e.dr;
+    if (EXT) global_folds<float, false>(sc, z, e.r, de);
+    const V4<float> tempZ = z;
+    const float tempDE = de;
     if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs);
     if (s.add_c) {
       if (sc.julia) {
@@ -487,7 +489,7 @@ struct PrecHybT {
     if (sc.is_hybrid) {
       const double kw = s.d[P_WEIGHT];
       if (kw < 1.0) {
-        z = smooth4<float, false>(last, z, kw);
+        z = smooth4<float, false>(tempZ, z, kw);
         de = de * float(kw) + tempDE * float(1.0 - kw);
       }
     }
@@ -514,6 +516,13 @@ struct PrecHybT {
 
   __device__ static float distance(const State &e, const Params &fp, float detail, int &iters) {
     const DevScene &sc = *fp.sc;
+    if (EXT && sc.limits) {  // outside the limit box: its distance (the iteration is not used)
+      const float lbd = limit_box_distance<float>(sc, e.cx, e.cy, e.cz);
+      if (lbd > detail) {
+        iters = 0;
+        return lbd;
+      }
+    }
     iters = e.brk ? e.it : e.it + 1;
     const float r = e.r, DE = e.dr;
     float d;
@@ -1179,7 +1188,17 @@ struct ShadeStage {
     if (mode == 0) {
       shadow_de++;
       const bool soft = fr.soft_range > 0.0;
-      if (soft) {
+      bool outside = false;  // a soft shadow ignores samples outside the limit box (shader_aux_shadow.cpp:130-147)
+      if constexpr (P::kHyb) {
+        const DevScene &sc = *fp.sc;
+        if (soft && sc.limits) {
+          D qx, qy, qz;
+          point(qx, qy, qz);
+          outside = qx < sc.flim_min[0] || qx > sc.flim_max[0] || qy < sc.flim_min[1] || qy > sc.flim_max[1] ||
+                    qz < sc.flim_min[2] || qz > sc.flim_max[2];
+        }
+      }
+      if (soft && !outside) {
         D angle = (d - D(thr)) / t;
         if (angle < D(0)) angle = D(0);
         if (d < D(thr)) angle = D(0);

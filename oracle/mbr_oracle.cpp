@@ -92,6 +92,10 @@ struct OPrim {
 
 struct Seq {
   std::vector<OPrim> prims;
+  // limit box (fractparams.cpp:175-177) and global folds (:346-351)
+  bool limits = false, gbox = false, gsph = false;
+  double lim_min[3] = {-10, -10, -10}, lim_max[3] = {10, 10, 10};
+  double gbox_limit = 1.0, gbox_value = 2.0, gsph_inner = 0.5, gsph_outer = 1.0;
   bool is_hybrid = false, julia = false;
   int length = 0, n = 0, formula_maxiter = 250, min_n = 1;
   int de_function = 1, de_analytic = 1;
@@ -239,6 +243,17 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     if (!build_prim(sc.primitive[k], &op)) return false;
     s.prims.push_back(op);
   }
+  s.limits = sc.limits_enabled != 0;
+  s.gbox = sc.box_folding != 0;
+  s.gsph = sc.spherical_folding != 0;
+  for (int i = 0; i < 3; i++) {
+    s.lim_min[i] = sc.limit_min[i];
+    s.lim_max[i] = sc.limit_max[i];
+  }
+  s.gbox_limit = sc.box_folding_limit;
+  s.gbox_value = sc.box_folding_value;
+  s.gsph_inner = sc.spherical_folding_inner;
+  s.gsph_outer = sc.spherical_folding_outer;
   *out = s;
   return true;
 }
@@ -250,6 +265,10 @@ template <class S>
 struct V4 {
   S x, y, z, w;
 };
+template <class S, class K>
+inline V4<S> operator*(const V4<S> &v, const K &k) {  // CVector4 * double (algebra.hpp)
+  return V4<S>{v.x * k, v.y * k, v.z * k, v.w * k};
+}
 template <class S>
 inline S len4(const V4<S> &v) {  // CVector4::Length (algebra.hpp:401)
   return sqrt(v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w);
@@ -798,6 +817,30 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
     const int sequence = (i < seq.length) ? seq.seq[i] : seq.seq[0];  // GetSequence
     const Slot &sd = seq.slot[sequence];
     const SlotT<S> &f = slots[sequence];
+    if (seq.gbox) {  // BoxFolding (legacy_fractal_transforrms.cpp:43-75), compute_fractal.cpp:192-196
+      if (z.x > seq.gbox_limit) z.x = seq.gbox_value - z.x;
+      else if (z.x < -seq.gbox_limit) z.x = -seq.gbox_value - z.x;
+      if (z.y > seq.gbox_limit) z.y = seq.gbox_value - z.y;
+      else if (z.y < -seq.gbox_limit) z.y = -seq.gbox_value - z.y;
+      if (z.z > seq.gbox_limit) z.z = seq.gbox_value - z.z;
+      else if (z.z < -seq.gbox_limit) z.z = -seq.gbox_value - z.z;
+      r = len4(z);
+    }
+    if (seq.gsph) {  // SphericalFolding (:77-103), compute_fractal.cpp:198-202
+      const double fR2_2 = seq.gsph_outer * seq.gsph_outer;
+      const double mR2_2 = seq.gsph_inner * seq.gsph_inner;
+      const S r2_2 = r * r;
+      const double fold_factor1_2 = fR2_2 / mR2_2;
+      if (r2_2 < mR2_2) {
+        z = z * fold_factor1_2;
+        DE = DE * fold_factor1_2;
+      } else if (r2_2 < fR2_2) {
+        const S fold_factor2_2 = fR2_2 / r2_2;
+        z = z * fold_factor2_2;
+        DE = DE * fold_factor2_2;
+      }
+      r = len4(z);
+    }
     const V4<S> tempZ = z;
     const S tempAuxDE = DE;
     if (sd.weight > 0.0) {
@@ -894,6 +937,16 @@ inline void zero_tangents(Dual<N> &d) {
 template <class S>
 S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
                 int *iters_out) {
+  if (seq.limits) {  // the limit box early-out (calculate_distance.cpp:261-275)
+    S bx = std::max(px - seq.lim_max[0], -(px - seq.lim_min[0]));
+    S by = std::max(py - seq.lim_max[1], -(py - seq.lim_min[1]));
+    S bz = std::max(pz - seq.lim_max[2], -(pz - seq.lim_min[2]));
+    S limitBoxDist = std::max({bx, by, bz});
+    if (limitBoxDist > detailSize) {
+      if (iters_out) *iters_out = 0;  // the reference leaves out->iters unset here
+      return limitBoxDist;
+    }
+  }
   const int mult = (normalMode && seq.iter_thresh) ? 5 : 1;
   FractalOut<S> fo = compute<S>(seq, slots, px, py, pz, mult, -1);
   S distance = fo.distance;
@@ -1288,7 +1341,13 @@ struct Renderer {
     for (double i = start; i < distance; i += step) {
       const D3 point2 = add(q, mul(L, i));
       const double dist = de(point2, thr, false, nullptr, c);
-      if (bSoft) {  // :142-151
+      bool limitsReached = false;  // :130-140
+      if (seq.limits) {
+        if (point2.x < seq.lim_min[0] || point2.x > seq.lim_max[0] || point2.y < seq.lim_min[1] ||
+            point2.y > seq.lim_max[1] || point2.z < seq.lim_min[2] || point2.z > seq.lim_max[2])
+          limitsReached = true;
+      }
+      if (bSoft && !limitsReached) {  // :142-151
         double angle = (dist - dist_thresh) / i;
         if (angle < 0) angle = 0;
         if (dist < dist_thresh) angle = 0;
@@ -1657,6 +1716,14 @@ void oracle_scene_defaults(mbr_scene *s) {
   for (int i = 0; i < 3; i++) s->fractal_constant_factor[i] = 1.0;
   oracle_fractal_defaults(&s->fractal[0], MBR_FORMULA_MANDELBULB);
   for (int i = 1; i < MBR_MAX_FRACTALS; i++) oracle_fractal_defaults(&s->fractal[i], MBR_FORMULA_NONE);
+  for (int i = 0; i < 3; i++) {  // :143-145
+    s->limit_min[i] = -10.0;
+    s->limit_max[i] = 10.0;
+  }
+  s->box_folding_limit = 1.0;  // :199-204
+  s->box_folding_value = 2.0;
+  s->spherical_folding_inner = 0.5;
+  s->spherical_folding_outer = 1.0;
 }
 
 void oracle_camera_defaults(mbr_camera *c) {

@@ -189,7 +189,9 @@ int refp_distance(void *h, const double *pts, int n, double detail, int normal_m
   if (!p->prepared && refp_prepare(h)) return 1;
   for (int i = 0; i < n; i++) {
     sDistanceIn in(CVector3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), detail, normal_mode != 0);
-    sDistanceOut out;
+    // zero-initialised: the limit-box early-out (calculate_distance.cpp:268-273)
+    // returns without setting `iters`
+    sDistanceOut out{};
     dist[i] = CalculateDistance(*p->params, *p->fractals, in, &out, p->data.get());
     if (iters) iters[i] = out.iters;
   }

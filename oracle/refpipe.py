@@ -196,6 +196,15 @@ class RefPipeline:
         self.set("delta_DE_function", s.delta_de_function, KIND_INT)
         self.set("N", s.formula_maxiter, KIND_INT)
         self.set("repeat_from", s.repeat_from, KIND_INT)
+        self.set("limits_enabled", s.limits_enabled, KIND_BOOL)
+        self.set("limit_min", list(s.limit_min), KIND_VEC3)
+        self.set("limit_max", list(s.limit_max), KIND_VEC3)
+        self.set("box_folding", s.box_folding, KIND_BOOL)
+        self.set("box_folding_limit", s.box_folding_limit, KIND_DOUBLE)
+        self.set("box_folding_value", s.box_folding_value, KIND_DOUBLE)
+        self.set("spherical_folding", s.spherical_folding, KIND_BOOL)
+        self.set("spherical_folding_inner", s.spherical_folding_inner, KIND_DOUBLE)
+        self.set("spherical_folding_outer", s.spherical_folding_outer, KIND_DOUBLE)
         if hybrid:
             self.set_string("node_0001_definition", f"hybrid 1,1,{NODE_HYBRID},0,-1")
             for i in range(n):

@@ -112,6 +112,32 @@ def cases():
     s.fractal[2].dont_add_c_constant = 1
     s.repeat_from = 2
     out["hybrid_box_bulb_menger_repeat2"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.limits_enabled = 1
+    s.limit_min[:] = [-1.5, -0.8, -2.0]
+    s.limit_max[:] = [0.9, 1.2, 0.7]
+    out["box_limits"] = s
+    s = configs.mandelbulb_scene(8.0, 30)
+    s.box_folding = 1
+    s.box_folding_limit = 0.9
+    s.box_folding_value = 1.7
+    out["bulb_global_box_fold"] = s
+    s = configs.mandelbulb_scene(6.0, 30)
+    s.spherical_folding = 1
+    s.spherical_folding_inner = 0.4
+    s.spherical_folding_outer = 1.1
+    out["bulb_global_spherical_fold"] = s
+    s = configs.hybrid_scene()
+    s.box_folding = 1
+    s.spherical_folding = 1
+    s.limits_enabled = 1
+    s.limit_min[:] = [-1.0, -1.0, -0.6]
+    s.limit_max[:] = [1.0, 0.8, 1.0]
+    out["hybrid_folds_limits"] = s
+    s = abi.scene_defaults(abi.FORMULA_HYPERCOMPLEX)
+    s.formula_maxiter = 30
+    s.spherical_folding = 1
+    out["hypercomplex_spherical_fold"] = s
     return out
 
 
@@ -176,4 +202,8 @@ def render_cases():
     f.ifs_rotation_enabled = 1
     f.ifs_rotation[:] = [20.0, 0.0, 10.0]
     out.append(("ifs_menger", s, configs.camera((1.2, -2.2, 1.5), width=32, height=24), params()))
+    out.append(("box_limits_soft_shadow", cases_["box_limits"], configs.camera((0.0, -5.0, 0.5), width=40, height=24),
+                params(soft_shadow_cone=15.0)))
+    out.append(("bulb_global_folds", cases_["bulb_global_box_fold"],
+                configs.camera((0.3, -2.8, 0.4), width=32, height=24), params()))
     return out

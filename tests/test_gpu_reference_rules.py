@@ -229,3 +229,31 @@ def test_gamma_tables_stay_ordered_on_the_stream(renderer, engine):
     renderer.sync(s)
     for g, b in zip(gammas, got):
         assert np.array_equal(b["rgb8"].cpu().numpy(), want[g]), g
+
+
+@pytest.mark.parametrize("case", ["box_limits", "bulb_global_box_fold", "bulb_global_spherical_fold",
+                                  "hybrid_folds_limits"])
+def test_limit_box_and_global_folds(renderer, oracle, case):
+    """The limit box (calculate_distance.cpp:261-275; with a soft shadow,
+    shader_aux_shadow.cpp:130-147) and the global box and spherical folds
+    (compute_fractal.cpp:190-202): the oracle reproduces the reference's own
+    CalculateDistance and render worker bit for bit (tests/golden/
+    pipeline_kat.json, render_kat.json); every engine that takes these scenes
+    is held to the oracle.  The FP64 wavefront, batches and the allocation-free
+    path refuse them."""
+    from tests.golden.pipeline_cases import cases
+
+    from mandelbulber2_b200.render import MbrError
+
+    sc = cases()[case]
+    cam = configs.camera((0.0, -5.0, 0.5) if case == "box_limits" else (0.3, -2.8, 0.4), width=64, height=40)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    p.soft_shadow_cone = 15.0
+    o, _ = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.98
+    check_engines(renderer, sc, cam, p, o, case,
+                  engines=(abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64) + FP32_ENGINES)
+    with pytest.raises(MbrError) as e:
+        renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP64)
+    assert e.value.status == abi.MBR_EUNSUPPORTED

@@ -295,8 +295,8 @@ def test_reference_examples():
     """Every example scene the reference ships is read: none is malformed, and a
     scene is accepted exactly when the formulas it iterates are built here and
     none of the unsupported features appears.  Switches that change the
-    geometry, the march or the normals and are not built (the limit box, the
-    global folds, stereo, iteration-count normals) turn a scene away."""
+    image plane or the normals and are not built (stereo, iteration-count
+    normals) turn a scene away."""
     files = sorted(glob.glob(os.path.join(EXAMPLES, "**", "*.fract"), recursive=True))
     assert len(files) > 150
     ok = 0
@@ -307,7 +307,7 @@ def test_reference_examples():
         used = range(sc.n_fractals) if sc.hybrid_fractal_enable else range(1)
         formulas = {sc.fractal[i].formula for i in used} - {0}
         text = open(path, errors="replace").read()
-        for key in ("limits_enabled", "box_folding", "spherical_folding", "stereo_enabled", "slow_shading"):
+        for key in ("stereo_enabled", "slow_shading"):
             if f"\n{key} true;" in text:
                 assert not s.ok and any(u.startswith(key + " true") for u in s.unsupported()), (path, key)
         if s.ok:
@@ -316,7 +316,7 @@ def test_reference_examples():
             assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
         elif not formulas <= {2, 3, 4, 7, 8, 10, 11}:
             assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
-    assert ok >= 150, ok
+    assert ok >= 165, ok
 
 
 @pytest.mark.skipif(not EXAMPLES or not os.path.isdir(EXAMPLES), reason="reference example scenes not present")
