@@ -572,8 +572,13 @@ mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera, 
  *
  * MBR_OK: everything that changes the geometry is representable.
  * MBR_EUNSUPPORTED: the structs are filled, but the file uses geometry this
- * path does not build (another formula, boolean combinations, primitives,
- * transforms, forced delta DE); each is named in the report.  MBR_EINVAL: not a settings file, or a malformed value of a
+ * path does not build (another formula, boolean combinations, primitives
+ * combined other than by union, more than 8 primitives, a transform of the
+ * primitives group, formula and fractal transforms, forced delta DE,
+ * iteration-count normals, stereo images); each is named in the report.
+ * The eleven primitive kinds joined by union, advanced quality, the limits
+ * box and the global folds are read into the structs.
+ * MBR_EINVAL: not a settings file, or a malformed value of a
  * parameter read here.  The report (optional, NUL-terminated, truncated to
  * report_size) also lists the shading parameters outside the path that were
  * ignored, and how the main light and AO were mapped. */

@@ -243,8 +243,6 @@ def test_limit_box_and_global_folds(renderer, oracle, case):
     path refuse them."""
     from tests.golden.pipeline_cases import cases
 
-    from mandelbulber2_b200.render import MbrError
-
     sc = cases()[case]
     cam = configs.camera((0.0, -5.0, 0.5) if case == "box_limits" else (0.3, -2.8, 0.4), width=64, height=40)
     p = configs.base_params(5, 20.0)
