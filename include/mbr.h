@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MBR_ABI_VERSION 4
+#define MBR_ABI_VERSION 5
 
 /* Number of formula slots of one hybrid sequence (the reference's nine
  * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
@@ -57,18 +57,33 @@ typedef enum mbr_formula {
   MBR_FORMULA_MANDELBULB = 2,   /* formula/definition/fractal_mandelbulb.cpp:29-43 */
   MBR_FORMULA_MANDELBULB_POWER2 = 3, /* formula/definition/fractal_mandelbulb_power2.cpp:30-45 */
   MBR_FORMULA_HYPERCOMPLEX = 4, /* formula/definition/fractal_hypercomplex.cpp:30-45; 4-D: plain FP64 engines */
+  MBR_FORMULA_QUATERNION = 5,   /* formula/definition/fractal_quaternion.cpp:29-39 */
+  MBR_FORMULA_AEXION = 19,      /* formula/definition/fractal_aexion.cpp:29-59; 4-D: plain FP64 engines */
   MBR_FORMULA_KALEIDOSCOPIC_IFS = 10, /* formula/definition/fractal_kaleidoscopic_ifs.cpp:30-85 */
   MBR_FORMULA_XENODREAMBUIE = 11, /* formula/definition/fractal_xenodreambuie.cpp:30-49; Mandelbulb parameters */
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
   MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
 } mbr_formula;
 
-/* fractal::enumDEFunctionType (src/fractal_enums.h:47-60). */
+/* fractal::enumDEFunctionType (src/fractal_enums.h:47-60).  The Jos
+ * Kleinian function is taken with the delta DE only: its analytic form reads
+ * formula parameters that mbr_fractal does not carry. */
 typedef enum mbr_de_function {
   MBR_DE_FUNCTION_PREFERRED = 0,
   MBR_DE_FUNCTION_LINEAR = 1,
-  MBR_DE_FUNCTION_LOGARITHMIC = 2
+  MBR_DE_FUNCTION_LOGARITHMIC = 2,
+  MBR_DE_FUNCTION_PSEUDO_KLEINIAN = 3,
+  MBR_DE_FUNCTION_JOS_KLEINIAN = 4,
+  MBR_DE_FUNCTION_CUSTOM = 5,
+  MBR_DE_FUNCTION_MAX_AXIS = 6
 } mbr_de_function;
+
+/* fractal::enumDEMethod (src/fractal_enums.h:40-45), "delta_DE_method". */
+typedef enum mbr_de_method {
+  MBR_DE_METHOD_PREFERRED = 0,     /* each formula's own (all formulas built here are analytic) */
+  MBR_DE_METHOD_FORCE_DELTA = 1,   /* the delta DE of CalculateDistanceSimple */
+  MBR_DE_METHOD_FORCE_ANALYTIC = 2
+} mbr_de_method;
 
 /* Which kernel renders a frame. */
 typedef enum mbr_engine {
@@ -162,6 +177,13 @@ typedef struct mbr_fractal {
   double ifs_rotations[9][3];                /* default 0 */
   double ifs_distance[9];                    /* default 0 */
   double ifs_intensity[9];                   /* default 1 */
+  /* Aexion: "cadd" (sFractalAexion, fractal.cpp:118) */
+  double aexion_cadd;                        /* default -1.3 */
+  /* sFractalAnalyticDE (fractal.cpp:260-265) as the Aexion reads it */
+  int32_t analytic_de_enabled;               /* "analyticDE_enabled", default 1 */
+  int32_t reserved_ade;
+  double analytic_de_scale1;                 /* "analyticDE_scale_1", default 1 */
+  double analytic_de_offset1;                /* "analyticDE_offset_1", default 1 */
 } mbr_fractal;
 
 /* Primitive kinds (fractal::enumObjectType primitives, src/primitive.cpp) */
@@ -259,6 +281,18 @@ typedef struct mbr_scene {
   double box_folding_value;    /* default 2 */
   double spherical_folding_inner; /* default 0.5 */
   double spherical_folding_outer; /* default 1 */
+  /* "delta_DE_method" (mbr_de_method, default PREFERRED): with the delta DE,
+   * CalculateDistanceSimple (src/calculate_distance.cpp:607-760) runs the
+   * orbit at the point and at three points offset by deltaDE along x, y and
+   * z, each capped at the first orbit's iteration count, and divides the
+   * orbit radius by the gradient of |z|.  deltaDE = max(|p| 1e-14, f detail)
+   * with f = "deltade_relative_delta" under advanced quality, else 1e-5.
+   * Offsets of 1e-5 of the detail size need FP64 points: the plain FP64
+   * engines take it; the others return MBR_EUNSUPPORTED.  mbr_distance uses
+   * f = 1e-5 (a render without advanced quality). */
+  int32_t delta_de_method;
+  int32_t reserved_delta;
+  double deltade_relative_delta; /* default 0.01 (src/initparameters.cpp:166) */
 } mbr_scene;
 
 /* params::enumPerspectiveType (src/projection_3d.hpp:44-50): the view
@@ -574,10 +608,11 @@ mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camera *camera, 
  * MBR_EUNSUPPORTED: the structs are filled, but the file uses geometry this
  * path does not build (another formula, boolean combinations, primitives
  * combined other than by union, more than 8 primitives, a transform of the
- * primitives group, formula and fractal transforms, forced delta DE,
- * iteration-count normals, stereo images); each is named in the report.
- * The eleven primitive kinds joined by union, advanced quality, the limits
- * box and the global folds are read into the structs.
+ * primitives group, formula and fractal transforms, the analytic Jos
+ * Kleinian DE function, iteration-count normals, stereo images); each is
+ * named in the report.  The eleven primitive kinds joined by union, advanced
+ * quality, the limits box, the global folds and the DE method and function
+ * (the delta DE included) are read into the structs.
  * MBR_EINVAL: not a settings file, or a malformed value of a
  * parameter read here.  The report (optional, NUL-terminated, truncated to
  * report_size) also lists the shading parameters outside the path that were

@@ -24,12 +24,15 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 # mbr_formula (fractal::enumFractalFormula)
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
 FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS, FORMULA_XENODREAMBUIE = 3, 4, 10, 11
+FORMULA_QUATERNION, FORMULA_AEXION = 5, 19
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_primitive_type
 (PRIMITIVE_PLANE, PRIMITIVE_BOX, PRIMITIVE_SPHERE, PRIMITIVE_WATER, PRIMITIVE_TORUS, PRIMITIVE_CYLINDER,
  PRIMITIVE_CIRCLE, PRIMITIVE_RECTANGLE, PRIMITIVE_CONE, PRIMITIVE_PRISM, PRIMITIVE_ELLIPSOID) = range(1, 12)
 # mbr_de_function
-DE_PREFERRED, DE_LINEAR, DE_LOG = 0, 1, 2
+DE_PREFERRED, DE_LINEAR, DE_LOG, DE_PSEUDO_KLEINIAN, DE_JOS_KLEINIAN, DE_CUSTOM, DE_MAX_AXIS = range(7)
+# mbr_de_method
+DE_METHOD_PREFERRED, DE_METHOD_FORCE_DELTA, DE_METHOD_FORCE_ANALYTIC = range(3)
 # mbr_engine
 ENGINE_PLAIN_FP64, ENGINE_PLAIN_FP64_STRICT, ENGINE_PLAIN_MIXED, ENGINE_WAVEFRONT_FP32, ENGINE_WAVEFRONT_FP64, \
     ENGINE_WAVEFRONT_AUTO = range(6)
@@ -62,6 +65,8 @@ class Fractal(C.Structure):
         ("ifs_scale", C.c_double), ("ifs_rotation", D3), ("ifs_offset", D3), ("ifs_edge", D3),
         ("ifs_direction", D3 * 9), ("ifs_rotations", D3 * 9), ("ifs_distance", C.c_double * 9),
         ("ifs_intensity", C.c_double * 9),
+        ("aexion_cadd", C.c_double), ("analytic_de_enabled", C.c_int32), ("reserved_ade", C.c_int32),
+        ("analytic_de_scale1", C.c_double), ("analytic_de_offset1", C.c_double),
     ]
 
 
@@ -91,6 +96,7 @@ class Scene(C.Structure):
         ("reserved_folds", C.c_int32), ("limit_min", D3), ("limit_max", D3), ("box_folding_limit", C.c_double),
         ("box_folding_value", C.c_double), ("spherical_folding_inner", C.c_double),
         ("spherical_folding_outer", C.c_double),
+        ("delta_de_method", C.c_int32), ("reserved_delta", C.c_int32), ("deltade_relative_delta", C.c_double),
     ]
 
 

@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ De
                                                       const __grid_constant__ DevFrame fr,
                                                       const __grid_constant__ AdjointFrame af, const double *depth,
                                                       const uint8_t *hit, const float *dl_ddepth,
-                                                      const float *dl_dshade, double *grad) {
+                                                      const float *dl_dshade, double *partials) {
   const long long n = (long long)fr.width * fr.height;
   double acc[MBR_GRAD_COUNT];
 #pragma unroll
@@ -362,13 +362,31 @@ __global__ void __launch_bounds__(128) adjoint_kernel(const __grid_constant__ De
 #pragma unroll
     for (int k = 0; k < MBR_GRAD_COUNT; k++) acc[k] += wt * dt[k] + ws * ds[k];
   }
-  // warp reduction, then one atomic per warp and parameter
+  // warp reduction, then the block's warps in order: one partial sum per
+  // block and parameter, summed by adjoint_sum_kernel in block order, so the
+  // gradient does not depend on the order in which blocks ran
+  __shared__ double warp_sum[4][MBR_GRAD_COUNT];
 #pragma unroll
   for (int k = 0; k < MBR_GRAD_COUNT; k++) {
     double v = acc[k];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(grad + k, v);
+    if ((threadIdx.x & 31) == 0) warp_sum[threadIdx.x >> 5][k] = v;
   }
+  __syncthreads();
+  if (threadIdx.x < MBR_GRAD_COUNT) {
+    const int k = threadIdx.x;
+    partials[(long long)blockIdx.x * MBR_GRAD_COUNT + k] =
+        ((warp_sum[0][k] + warp_sum[1][k]) + warp_sum[2][k]) + warp_sum[3][k];
+  }
+}
+
+// grad[k] += the blocks' partial sums of parameter k, in block order.
+__global__ void adjoint_sum_kernel(const double *partials, int blocks, double *grad) {
+  const int k = threadIdx.x;
+  if (k >= MBR_GRAD_COUNT) return;
+  double v = 0.0;
+  for (int b = 0; b < blocks; b++) v += partials[(long long)b * MBR_GRAD_COUNT + k];
+  grad[k] += v;
 }
 
 }  // namespace mbr
@@ -392,6 +410,8 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the Mandelbox without rotations");
   if (sc->n_prims > 0 || sc->limits || sc->gbox || sc->gsph)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers scenes without primitives, limit box or global folds");
+  if (sc->delta_de || sc->de_final > DEF_IFS)
+    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the analytic linear and logarithmic DE functions");
   if (sc->is_hybrid || sc->has_w || sc->iter_thresh || sc->interior ||
       (sc->slot[0].formula != MBR_FORMULA_MANDELBULB && sc->slot[0].formula != MBR_FORMULA_MANDELBOX))
     return set_err(ctx, MBR_EUNSUPPORTED,
@@ -422,10 +442,14 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const long long n = (long long)fr.width * fr.height;
-  const int grid = int(std::min<long long>((n + 127) / 128, (long long)sms * 16));
+  const int grid = int(std::max<long long>(1, std::min<long long>((n + 127) / 128, (long long)sms * 16)));
+  double *partials = nullptr;
+  st = ctx_adjoint_partials(ctx, size_t(grid) * MBR_GRAD_COUNT * sizeof(double), &partials);
+  if (st != MBR_OK) return st;
   if (engine == MBR_ENGINE_PLAIN_FP64)
-    adjoint_kernel<double><<<grid, 128, 0, s>>>(*sc, fr, af, depth, hit, dl_ddepth, dl_dshade, grad);
+    adjoint_kernel<double><<<grid, 128, 0, s>>>(*sc, fr, af, depth, hit, dl_ddepth, dl_dshade, partials);
   else
-    adjoint_kernel<float><<<grid, 128, 0, s>>>(*sc, fr, af, depth, hit, dl_ddepth, dl_dshade, grad);
+    adjoint_kernel<float><<<grid, 128, 0, s>>>(*sc, fr, af, depth, hit, dl_ddepth, dl_dshade, partials);
+  adjoint_sum_kernel<<<1, 32, 0, s>>>(partials, grid, grad);
   return cuda_err(ctx, int(cudaGetLastError()), "adjoint kernel launch");
 }

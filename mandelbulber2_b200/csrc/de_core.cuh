@@ -253,6 +253,50 @@ __device__ __forceinline__ void f_hypercomplex(V4<T> &z, T r, T &DE) {
   z.w = nw;
 }
 
+// cFractalQuaternion::FormulaCode (fractal_quaternion.cpp:29-39)
+template <class T>
+__device__ __forceinline__ void f_quaternion(V4<T> &z, T r, T &DE) {
+  DE = DE * T(2.0) * r;
+  const T nx = z.x * z.x - z.y * z.y - z.z * z.z;
+  const T ny = T(2.0) * z.x * z.y;
+  const T nz = T(2.0) * z.x * z.z;
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+}
+
+// cFractalAexion::FormulaCode (fractal_aexion.cpp:29-59): at the orbit's
+// first iteration the point is folded into the tetrahedral frame and becomes
+// the orbit's c (aux.const_c, which the c-addition of other slots also reads);
+// 4-D, so the host sets has_w
+template <class T>
+__device__ __forceinline__ void f_aexion(V4<T> &z, T r, T &DE, const DevSlot &s, int i, V4<T> &c) {
+  V4<T> temp = z;
+  if (i == 0) {
+    const T cadd = T(s.d[P_AEX_CADD]);
+    temp.x = z.x + z.y + z.z;
+    temp.y = -z.x - z.y + z.z;
+    temp.z = -z.x + z.y - z.z;
+    temp.w = z.x - z.y - z.z;
+    z = V4<T>{m_abs(temp.x) + cadd, m_abs(temp.y) + cadd, m_abs(temp.z) + cadd, m_abs(temp.w) + cadd};
+    c = z;
+  }
+  T t = T(2.0) * z.w * z.z;
+  temp.x = z.x * z.x - z.y * z.y;
+  temp.y = t - temp.x;
+  temp.x = temp.x + t;
+  t = T(2.0) * z.x * z.y;
+  temp.z = z.z * z.z - z.w * z.w;
+  temp.w = t - temp.z;
+  temp.z = temp.z + t;
+  z = V4<T>{temp.x + c.x, temp.y + c.y, temp.z + c.z, temp.w + c.w};
+  if (s.d[P_ADE_ON] != 0.0) {
+    T de1 = T(1.1) * r;
+    de1 = de1 + (len4<T, true>(z) / r - de1) * T(s.d[P_ADE_SCALE1]);
+    DE = de1 * T(2.0) * DE + T(s.d[P_ADE_OFFSET1]);
+  }
+}
+
 // cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
 // over the enabled vectors of the scene's IFS block; the 4-vector terms with
 // w keep the reference's operations (its direction and offset have w = 0)
@@ -305,11 +349,15 @@ __device__ __forceinline__ void f_ifs(V4<T> &z, T &DE, const IfsBlock &b) {
 // EXT: the formulas beyond the three specialised ones and the Mandelbox
 // rotations are compiled in; kernels of scenes that use none of them (hybrids
 // of the three included) are built without that code.
+// i: the iteration (aux.i); c: the orbit's c (aux.const_c), which the Aexion
+// replaces at its first iteration.
 template <class T, bool W, bool EXT = false>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
-                                                 const MbRot *rot, const IfsBlock *ifs) {
+                                                 const MbRot *rot, const IfsBlock *ifs, int i, V4<T> &c) {
   if constexpr (EXT) {
     switch (formula) {
+      case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
+      case MBR_FORMULA_AEXION: f_aexion<T>(z, r, DE, s, i, c); break;
       case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
       case MBR_FORMULA_MANDELBOX: f_mandelbox<T, W, true>(z, DE, s, rot); break;
       case MBR_FORMULA_MANDELBULB_POWER2: f_bulb_pow2<T>(z, r, DE); break;
@@ -493,10 +541,6 @@ __device__ __noinline__ T prim_distance(const DevPrim &q, T wx, T wy, T wz) {
   return d * T(q.abs_scale);
 }
 
-// Compute<calcModeNormal> + CalculateDistanceSimple (analytic branch).
-// F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
-// the three specialised formulas) or F_EXT (generic with every formula and
-// the Mandelbox rotations).  W: 4-D state.
 // The limit box of CalculateDistance (calculate_distance.cpp:261-275): the
 // largest of the per-axis distances outside [lim_min, lim_max].
 template <class T>
@@ -550,24 +594,20 @@ __device__ __forceinline__ void global_folds(const DevScene &sc, V4<T> &z, T &r,
   }
 }
 
+// The orbit of Compute<calcModeNormal> and Compute<calcModeDeltaDE1>
+// (compute_fractal.cpp:170-492; the two modes iterate alike) from the point
+// (px, py, pz), at most maxN iterations.  Returns the loop index at exit (the
+// orbit's iteration count is one more) and leaves the final z, r = |z| (4-D),
+// the derivative DE and the orbit's maxiter flag.
 template <class T, int F, bool W>
-__device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
-                                           int *iters_out) {
-  if (F == F_EXT && sc.limits) {  // outside the limit box: its distance, no iteration
-    const T lbd = limit_box_distance<T>(sc, px, py, pz);
-    if (lbd > detail) {
-      *iters_out = 0;
-      return lbd;
-    }
-  }
-  const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
-  const int maxN = sc.formula_maxiter * mult;
-  V4<T> z{px, py, pz, W ? T(sc.w0) : T(0.0)};
-  const V4<T> c = z;
-  T r = len4<T, W>(z);
-  T DE = T(1.0);
+__device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T pz, int maxN, V4<T> &z, T &r, T &DE,
+                                             bool &maxiter) {
+  z = V4<T>{px, py, pz, W ? T(sc.w0) : T(0.0)};
+  V4<T> c = z;  // aux.const_c
+  r = len4<T, W>(z);
+  DE = T(1.0);
   V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)};
-  bool maxiter = true;
+  maxiter = true;
   int i;
   for (i = 0; i < maxN; i++) {
     lastZ = z;
@@ -581,7 +621,7 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
       if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs);
+      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c);
     }
     if (s.add_c) {
       if (sc.julia) {
@@ -614,33 +654,121 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
       break;
     }
   }
-  // final DE (compute_fractal.cpp:495-621)
-  T distance;
-  if (DE > T(0.0)) {
-    // 1 linear r/DE, 2 log, 3 IFS, 4 hybrid linear with offset
-    const int fn = (F <= 0 && sc.is_hybrid) ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
-    if (fn == 4) {
-      distance = (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
-    } else if (fn == 2) {
-      distance = (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
-    } else if (fn == 1) {
-      distance = r / DE;
-    } else if (fn == 3) {
-      distance = (r - T(2.0)) / DE;
-    } else {
-      distance = r;
+  return i;
+}
+
+// The final distance of an analytic orbit (compute_fractal.cpp:495-621).
+// The specialised iterations carry linear, logarithmic and IFS; the extended
+// one every DevDeFinal code.
+template <class T, int F, bool W>
+__device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE) {
+  if (!(DE > T(0.0))) return r;
+  if (F == F_EXT) {
+    switch (sc.de_final) {
+      case DEF_LINEAR_OFFSET: return (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
+      case DEF_LOG: return (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
+      case DEF_LINEAR: return r / DE;
+      case DEF_IFS: return (r - T(2.0)) / DE;
+      case DEF_PSEUDO_KLEINIAN: {  // aux.pseudoKleinianDE keeps its initial 1 (compute_fractal.cpp:120)
+        const T rxy = m_sqrt(z.x * z.x + z.y * z.y);
+        return smax(T(rxy - T(1.0)), T(m_abs(rxy * z.z) / r)) / DE;
+      }
+      case DEF_CUSTOM: return T(1000.0);  // aux.dist (:119)
+      case DEF_MAX_AXIS: {
+        const T rd = smax(m_abs(z.x), smax(m_abs(z.y), m_abs(z.z)));
+        return rd / DE;
+      }
+      case DEF_NONE: return T(-1.0);
+      default: return r;
+    }
+  }
+  // 1 linear r/DE, 2 log, 3 IFS, 4 hybrid linear with offset
+  const int fn = (F <= 0 && sc.is_hybrid) ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
+  if (fn == 4) return (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
+  if (fn == 2) return (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
+  if (fn == 1) return r / DE;
+  if (fn == 3) return (r - T(2.0)) / DE;
+  return r;
+}
+
+// CalculateDistanceSimple, delta-DE branch (calculate_distance.cpp:607-760):
+// the orbit radius at the point and at three points offset by deltaDE along
+// x, y and z, each capped at the first orbit's iteration count; the distance
+// divides the radius by the gradient of |z| through the sequence's DE
+// function.  FP64 only: the offsets are 1e-5 of the detail size.
+template <class T, bool W>
+__device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
+                                         int *iters_out, int *total_out) {
+  const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
+  const T plen = m_sqrt(px * px + py * py + pz * pz);  // fractIn.point.Length()
+  const T deltaDE = smax(T(plen * T(1e-14)), T(T(sc.delta_factor) * detail));
+  V4<T> z;
+  T r4, DE;
+  bool mx;
+  // Compute's delta-mode ending for the Jos Kleinian function
+  // (compute_fractal.cpp:627-638): z.y = min(z.y, foldingValue - z.y) with
+  // the default transf_spheres_enabled (true) and transf_folding_value (2)
+  const bool jos = sc.delta_fn == 4;
+  const int i1 = compute_orbit<T, F_EXT, W>(sc, px, py, pz, sc.formula_maxiter * mult, z, r4, DE, mx);
+  if (jos && T(2.0) - z.y < z.y) z.y = T(2.0) - z.y;
+  const T r = m_sqrt(z.x * z.x + z.y * z.y + z.z * z.z);  // fractOut.z.Length(): the 3-D part
+  const T zfx = z.x, zfy = z.y, zfz = z.z;
+  const int iters1 = i1 + 1;
+  int total = iters1;
+  bool out_maxiter = mx;
+  bool maxiter = mx;
+  if (!sc.limits) {
+    if (!sc.iter_thresh) maxiter = false;
+  } else {
+    if (normal_mode) maxiter = false;
+  }
+  T drv[3];
+  int last_iters = iters1;
+  for (int a = 0; a < 3; a++) {  // x, y, z offsets, each with forcedMaxiter = the first orbit's count
+    const int i = compute_orbit<T, F_EXT, W>(sc, a == 0 ? T(px + deltaDE) : T(px + T(0.0)),
+                                             a == 1 ? T(py + deltaDE) : T(py + T(0.0)),
+                                             a == 2 ? T(pz + deltaDE) : T(pz + T(0.0)), iters1, z, r4, DE, mx);
+    if (jos && T(2.0) - z.y < z.y) z.y = T(2.0) - z.y;
+    const T r2 = m_sqrt(z.x * z.x + z.y * z.y + z.z * z.z);
+    drv[a] = m_abs(T(r2 - r)) / deltaDE;
+    last_iters = i + 1;
+    total += last_iters;
+  }
+  const T dr = m_sqrt(drv[0] * drv[0] + drv[1] * drv[1] + drv[2] * drv[2]);
+  T distance = T(0.0);
+  if (dr > T(0.0)) {
+    switch (sc.delta_fn) {
+      case 1: distance = T(0.5) * r / dr; break;
+      case 2: distance = T(0.5) * r * m_log(r) / dr; break;
+      case 3: {  // the last offset orbit's z (:686-690)
+        const T rxy = m_sqrt(z.x * z.x + z.y * z.y);
+        distance = smax(T(rxy - T(0.92784)), T(m_abs(rxy * z.z) / r)) / dr;
+        break;
+      }
+      case 4: {
+        const T rxy = m_sqrt(z.x * z.x + z.z * z.z);
+        distance = (m_abs(rxy * z.y) / r) / dr;
+        maxiter = false;
+        break;
+      }
+      case 5: distance = r; break;
+      case 6: {  // the first orbit's z; dMax (common_math.cpp:74-83)
+        const T ax = m_abs(zfx), ay = m_abs(zfy), az = m_abs(zfz);
+        const T d0 = m_abs(drv[0]), d1 = m_abs(drv[1]), d2 = m_abs(drv[2]);
+        const T maxZ = (ax > ay) ? ((ax > az) ? ax : az) : ((ay > az) ? ay : az);
+        const T maxDr = (d0 > d1) ? ((d0 > d2) ? d0 : d2) : ((d1 > d2) ? d1 : d2);
+        distance = T(0.5) * maxZ / maxDr;
+        break;
+      }
+      default: break;
     }
   } else {
     distance = r;
   }
-  const int iters = i + 1;
-  *iters_out = iters;
-  // CalculateDistanceSimple post-processing (calculate_distance.cpp:561-605)
-  bool mx = maxiter;
-  if (!sc.iter_thresh) mx = false;
-  if (normal_mode) mx = false;
-  if (mx) distance = T(0.0);
-  if (iters < sc.min_n && distance < detail) distance = detail;
+  if (!sc.iter_thresh) out_maxiter = false;
+  if (normal_mode) out_maxiter = false;
+  if (out_maxiter) distance = T(0.0);
+  if (last_iters < sc.min_n && distance < detail) distance = detail;  // fractOut of the last offset orbit
   if (sc.interior) {
     if (!normal_mode) {
       if (distance < T(0.5) * detail || maxiter) distance = detail;
@@ -653,6 +781,65 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
   }
   if (distance < T(0.0)) distance = T(0.0);
   if (distance > T(10.0)) distance = T(10.0);
+  *iters_out = iters1;
+  if (total_out) *total_out = total;
+  return distance;
+}
+
+// CalculateDistance for one point: the limit box, CalculateDistanceSimple
+// (analytic or delta branch) and the union with the primitives.
+// F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
+// the three specialised formulas) or F_EXT (generic with every formula and
+// the Mandelbox rotations).  W: 4-D state.  *iters_out: the iteration count
+// of the (first) orbit; *total_out, when given: the iterations of all orbits.
+template <class T, int F, bool W>
+__device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
+                                           int *iters_out, int *total_out = nullptr) {
+  if (F == F_EXT && sc.limits) {  // outside the limit box: its distance, no iteration
+    const T lbd = limit_box_distance<T>(sc, px, py, pz);
+    if (lbd > detail) {
+      *iters_out = 0;
+      if (total_out) *total_out = 0;
+      return lbd;
+    }
+  }
+  T distance;
+  bool simple = true;
+  if constexpr (F == F_EXT && sizeof(T) == 8) {
+    if (sc.delta_de) {
+      distance = delta_distance<T, W>(sc, px, py, pz, detail, normal_mode, iters_out, total_out);
+      simple = false;
+    }
+  }
+  if (simple) {
+    const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
+    V4<T> z;
+    T r, DE;
+    bool maxiter;
+    const int i = compute_orbit<T, F, W>(sc, px, py, pz, sc.formula_maxiter * mult, z, r, DE, maxiter);
+    distance = final_distance<T, F, W>(sc, z, r, DE);
+    const int iters = i + 1;
+    *iters_out = iters;
+    if (total_out) *total_out = iters;
+    // CalculateDistanceSimple post-processing (calculate_distance.cpp:561-605)
+    bool mx = maxiter;
+    if (!sc.iter_thresh) mx = false;
+    if (normal_mode) mx = false;
+    if (mx) distance = T(0.0);
+    if (iters < sc.min_n && distance < detail) distance = detail;
+    if (sc.interior) {
+      if (!normal_mode) {
+        if (distance < T(0.5) * detail || maxiter) distance = detail;
+      } else {
+        if (distance < T(0.9) * detail) distance = detail - distance;
+      }
+    }
+    if (sc.iter_thresh && !normal_mode && !maxiter) {
+      if (distance < detail) distance = detail * T(1.01);
+    }
+    if (distance < T(0.0)) distance = T(0.0);
+    if (distance > T(10.0)) distance = T(10.0);
+  }
   if (F == F_EXT) {  // the union with the primitives (booleanAdd, calculate_distance.cpp:166-201)
     for (int k = 0; k < sc.n_prims; k++) {
       const T pd = prim_distance<T>(sc.prim[k], px, py, pz);

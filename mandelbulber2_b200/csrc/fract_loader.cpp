@@ -20,9 +20,10 @@
 // formulas and the hybrid sequence, the iteration and bailout settings,
 // camera, raymarching quality, the main light, AO and the 8-bit conversion.
 // Primitives joined by union (plane, box, sphere, water, torus, cylinder,
-// circle, rectangle, cone, prism, ellipsoid) are read into mbr_scene.primitive.  Geometry this path
+// circle, rectangle, cone, prism, ellipsoid) are read into mbr_scene.primitive, and so are the
+// DE method and function (the delta DE included).  Geometry this path
 // does not build (other formulas, boolean combinations, other primitives or
-// operators, transforms, forced delta DE) makes the call
+// operators, transforms) makes the call
 // return MBR_EUNSUPPORTED with each item named in the report; shading
 // parameters outside the path (materials, fog, glow, reflections, textures,
 // further lights) are counted and listed as ignored.
@@ -387,6 +388,14 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
     if (parse_vec3(value, v)) std::memcpy(f.mandelbox_offset, v, sizeof(v)); else R.bad(name, value);
   } else if (name == "transf_scale_3") {
     if (parse_double(value, d)) f.transf_scale3 = d; else R.bad(name, value);
+  } else if (name == "cadd") {  // Aexion (fractal.cpp:118)
+    if (parse_double(value, d)) f.aexion_cadd = d; else R.bad(name, value);
+  } else if (name == "analyticDE_enabled") {
+    if (parse_bool(value, b)) f.analytic_de_enabled = b; else R.bad(name, value);
+  } else if (name == "analyticDE_scale_1") {
+    if (parse_double(value, d)) f.analytic_de_scale1 = d; else R.bad(name, value);
+  } else if (name == "analyticDE_offset_1") {
+    if (parse_double(value, d)) f.analytic_de_offset1 = d; else R.bad(name, value);
   } else if (name == "mandelbox_rotations_enabled") {
     if (parse_bool(value, b)) f.mandelbox_rotations_enabled = b; else R.bad(name, value);
   } else if (name == "mandelbox_main_rotation_enabled") {
@@ -554,16 +563,16 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
   } else if (name == "linear_DE_offset") {
     if (parse_double(value, d)) sc->linear_de_offset = d; else R.bad(name, value);
   } else if (name == "delta_DE_function") {
-    if (parse_int(value, b) && b >= 0 && b <= 2) sc->delta_de_function = b;
-    else if (parse_int(value, b)) R.unsupported.push_back(name + " " + value + " (DE function)");
+    // 0 preferred, 1 linear, 2 logarithmic, 3 pseudo-Kleinian, 4 Jos Kleinian, 5 custom, 6 max axis
+    if (parse_int(value, b) && b >= 0 && b <= 6) sc->delta_de_function = b;
     else R.bad(name, value);
   } else if (name == "delta_DE_method") {
-    // 0 preferred (analytic for the three formulas), 1 forced delta, 2 forced analytic
-    if (parse_int(value, b)) {
-      if (b == 1) R.unsupported.push_back(name + " 1 (forced delta DE)");
-    } else {
-      R.bad(name, value);
-    }
+    // 0 preferred (analytic for every formula built here), 1 forced delta, 2 forced analytic
+    if (parse_int(value, b) && b >= 0 && b <= 2) sc->delta_de_method = b;
+    else R.bad(name, value);
+  } else if (name == "deltade_relative_delta") {
+    if (parse_double(value, d) && d > 0.0 && std::isfinite(d)) sc->deltade_relative_delta = d;
+    else R.bad(name, value);
   } else if (name == "iteration_threshold_mode") {
     if (parse_bool(value, b)) sc->iteration_threshold_mode = b; else R.bad(name, value);
   } else if (name == "interior_mode") {
@@ -840,10 +849,11 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     if (f == MBR_FORMULA_NONE) continue;
     if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE &&
         f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS &&
-        f != MBR_FORMULA_XENODREAMBUIE)
+        f != MBR_FORMULA_XENODREAMBUIE && f != MBR_FORMULA_QUATERNION && f != MBR_FORMULA_AEXION)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
                               " (formula not built here: 2 Mandelbulb, 3 Mandelbulb power 2, 4 hypercomplex, "
-                              "7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie are)");
+                              "5 quaternion, 7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie, "
+                              "19 aexion are)");
     if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && R.hybrid)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in a hybrid)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
@@ -962,6 +972,11 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     }
   }
 
+  // the analytic Jos Kleinian DE function reads formula parameters not carried here
+  if (scene->delta_de_function == MBR_DE_FUNCTION_JOS_KLEINIAN && scene->delta_de_method != MBR_DE_METHOD_FORCE_DELTA)
+    R.unsupported.push_back("delta_DE_function 4 (the analytic Jos Kleinian DE function)");
+  if (scene->delta_de_method == MBR_DE_METHOD_FORCE_DELTA)
+    append(rep, "note: delta_DE_method 1 (forced delta DE): the plain FP64 engines render it");
   for (const std::string &u : R.unsupported) append(rep, "unsupported: " + u);
   if (!R.ignored.empty()) {
     std::string s = "ignored: " + std::to_string(R.ignored.size()) + " parameters outside the DE path:";

@@ -32,6 +32,10 @@ enum SlotParam {
   P_SCALE3,
   P_BAILOUT,
   P_WEIGHT,
+  P_AEX_CADD,       // aexion cadd
+  P_ADE_ON,         // analyticDE enabled (0 or 1)
+  P_ADE_SCALE1,     // analyticDE scale1
+  P_ADE_OFFSET1,    // analyticDE offset1
   P_COUNT
 };
 
@@ -141,11 +145,37 @@ struct DevScene {
   double gbox_limit, gbox_value, gsph_fr2, gsph_mr2;  // spherical: outer^2, inner^2
   float flim_min[3], flim_max[3];
   float fgbox_limit, fgbox_value, fgsph_fr2, fgsph_mr2;
+  // the final distance of the orbit (DevDeFinal), and the delta DE
+  // (calculate_distance.cpp:607-760): its DE function (enumDEFunctionType)
+  // and offset factor (1e-5, or deltade_relative_delta under advanced
+  // quality; set per render)
+  int32_t de_final;
+  int32_t delta_de;
+  int32_t delta_fn;
+  int32_t pad5;
+  double delta_factor;
+  double delta_rel;
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 
+// The final distance of an analytic orbit (compute_fractal.cpp:495-621):
+// one code for the hybrid DEFunctionType and the non-hybrid
+// DEAnalyticFunction.  The first four are the ones the specialised
+// iterations carry; the others make a scene extended.
+enum DevDeFinal {
+  DEF_LINEAR = 1,         // r / DE
+  DEF_LOG = 2,            // 0.5 r log r / DE (0 for r <= 1)
+  DEF_IFS = 3,            // (r - 2) / DE
+  DEF_LINEAR_OFFSET = 4,  // hybrid linear: (r - linearDEOffset) / DE
+  DEF_PSEUDO_KLEINIAN = 5,// max(rxy - 1, |rxy z| / r) / DE (aux.pseudoKleinianDE stays 1)
+  DEF_CUSTOM = 6,         // aux.dist: 1000 for every formula built here
+  DEF_MAX_AXIS = 7,       // max |z_i| / DE
+  DEF_NONE = 8            // analyticFunctionNone: -1
+};
+
 __host__ __device__ inline bool scene_extended(const DevScene &sc) {
-  return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0 || sc.limits || sc.gbox || sc.gsph;
+  return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0 || sc.limits || sc.gbox || sc.gsph ||
+         sc.delta_de || sc.de_final > DEF_LINEAR_OFFSET;
 }
 
 // Everything about one frame that is not the scene: camera, march and

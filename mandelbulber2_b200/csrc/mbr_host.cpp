@@ -45,6 +45,8 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_HYPERCOMPLEX: *m = {2, 0, 10.0, 2}; return true;
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: *m = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
     case MBR_FORMULA_XENODREAMBUIE: *m = {2, 0, 10.0, 2}; return true;       // fractal_xenodreambuie.cpp:17-28
+    case MBR_FORMULA_QUATERNION: *m = {2, 0, 10.0, 2}; return true;          // fractal_quaternion.cpp:16-27
+    case MBR_FORMULA_AEXION: *m = {2, 2, 10000.0, 2}; return true;           // fractal_aexion.cpp:16-27
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -70,7 +72,8 @@ struct mbr_ctx {
   // scratch of the wavefront kernel (work counter + per-lane queue cursor)
   unsigned long long *d_work = nullptr;
   size_t work_words = 0;
-  void *adjoint_scratch = nullptr;
+  void *adjoint_scratch = nullptr;  // the adjoint's per-block partial sums
+  size_t adjoint_scratch_bytes = 0;
 };
 
 namespace mbr {
@@ -246,10 +249,12 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   if (!finite3(sc.julia_c) || !finite3(sc.fractal_constant_factor) || !std::isfinite(sc.initial_waxis) ||
       !std::isfinite(sc.linear_de_offset))
     return set_err(ctx, MBR_EINVAL, "non-finite scene vector");
-  if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED && sc.delta_de_function != MBR_DE_FUNCTION_LINEAR &&
-      sc.delta_de_function != MBR_DE_FUNCTION_LOGARITHMIC)
-    return set_err(ctx, MBR_EUNSUPPORTED, "delta_de_function %d is not supported (preferred, linear, log)",
-                   sc.delta_de_function);
+  if (sc.delta_de_function < MBR_DE_FUNCTION_PREFERRED || sc.delta_de_function > MBR_DE_FUNCTION_MAX_AXIS)
+    return set_err(ctx, MBR_EINVAL, "delta_de_function must be in [0, 6], got %d", sc.delta_de_function);
+  if (sc.delta_de_method < MBR_DE_METHOD_PREFERRED || sc.delta_de_method > MBR_DE_METHOD_FORCE_ANALYTIC)
+    return set_err(ctx, MBR_EINVAL, "delta_de_method must be in [0, 2], got %d", sc.delta_de_method);
+  if (!(sc.deltade_relative_delta > 0.0) || !std::isfinite(sc.deltade_relative_delta))
+    return set_err(ctx, MBR_EINVAL, "deltade_relative_delta must be finite and > 0");
   // Mandelbox rotations: slot 0 of a single-fractal scene
   for (int i = 0; i < (hybrid ? n : 1); i++) {
     const mbr_fractal &f = sc.fractal[i];
@@ -328,7 +333,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     }
     FormulaMeta m;
     if (!formula_meta(f.formula, &m))
-      return set_err(ctx, MBR_EUNSUPPORTED, "slot %d: formula %d is not supported (2, 7, 8)", i, f.formula);
+      return set_err(ctx, MBR_EUNSUPPORTED, "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 19)", i, f.formula);
     any = true;
     if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
     if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)
@@ -351,6 +356,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     s.check_bailout = hybrid ? (f.check_for_bailout != 0) : 1;
     bool addc = f.dont_add_c_constant == 0;
     if (m.cpixel == 1) addc = !addc;
+    if (m.cpixel == 2) addc = false;  // cpixelAlreadyHas: the formula adds c itself (:209-212)
     s.add_c = addc ? 1 : 0;
     double bailout;
     if (sc.use_default_bailout) {
@@ -379,6 +385,10 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     p[P_SCALE3] = f.transf_scale3;
     p[P_BAILOUT] = bailout;
     p[P_WEIGHT] = f.formula_weight;
+    p[P_AEX_CADD] = f.aexion_cadd;
+    p[P_ADE_ON] = f.analytic_de_enabled ? 1.0 : 0.0;
+    p[P_ADE_SCALE1] = f.analytic_de_scale1;
+    p[P_ADE_OFFSET1] = f.analytic_de_offset1;
     s.has_offset = (f.mandelbox_offset[0] != 0.0 || f.mandelbox_offset[1] != 0.0 || f.mandelbox_offset[2] != 0.0);
   }
   if (!any) return set_err(ctx, MBR_EINVAL, "scene has no formula");
@@ -437,17 +447,35 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     }
     d.de_analytic = (d.de_function == 2) ? 2 : 1;
     d.uniform_formula = 0;
+    // every formula built here is analytic, so only the forced method makes
+    // the sequence a delta-DE one (:463-464)
+    d.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+    static const int hyb_final[7] = {0, DEF_LINEAR_OFFSET, DEF_LOG, DEF_PSEUDO_KLEINIAN, 0, DEF_CUSTOM, DEF_MAX_AXIS};
+    d.de_final = hyb_final[d.de_function];
   } else {
     FormulaMeta m;
     formula_meta(d.slot[0].formula, &m);
     d.de_function = m.de_function;
     d.de_analytic = m.analytic;
-    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {
+    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {  // :477-500
       d.de_function = sc.delta_de_function;
-      d.de_analytic = (d.de_function == 2) ? 2 : 1;
+      static const int fn_analytic[7] = {1, 1, 2, 4, 5, 6, 7};  // enumDEAnalyticFunction
+      d.de_analytic = fn_analytic[d.de_function];
     }
+    d.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+    // enumDEAnalyticFunction -> DevDeFinal (Jos Kleinian: 0, refused below)
+    static const int an_final[8] = {DEF_NONE, DEF_LINEAR, DEF_LOG, DEF_IFS, DEF_PSEUDO_KLEINIAN, 0, DEF_CUSTOM,
+                                    DEF_MAX_AXIS};
+    d.de_final = an_final[d.de_analytic];
     d.uniform_formula = d.slot[0].formula;
   }
+  if (!d.delta_de && d.de_final == 0)
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "the analytic Jos Kleinian DE function reads formula parameters this build does not carry "
+                   "(the delta DE takes it)");
+  d.delta_fn = d.de_function;
+  d.delta_rel = sc.deltade_relative_delta;
+  d.delta_factor = 1e-5;
   d.formula_maxiter = sc.formula_maxiter;
   d.min_n = sc.min_n;
   d.iter_thresh = sc.iteration_threshold_mode ? 1 : 0;
@@ -463,7 +491,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   d.has_w = sc.initial_waxis != 0.0;
   for (int i = 0; i < n; i++) {
     const int f = d.slot[i].formula;
-    if (f == MBR_FORMULA_HYPERCOMPLEX) d.has_w = 1;  // z.w evolves from w = 0
+    if (f == MBR_FORMULA_HYPERCOMPLEX || f == MBR_FORMULA_AEXION) d.has_w = 1;  // z.w evolves from w = 0
     if (f != MBR_FORMULA_NONE && f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX &&
         f != MBR_FORMULA_MENGER_SPONGE)
       d.generic = 1;
@@ -505,6 +533,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   d.fgsph_fr2 = float(d.gsph_fr2);
   d.fgsph_mr2 = float(d.gsph_mr2);
   if (d.limits || d.gbox || d.gsph) d.generic = 1;  // the reference-order iteration carries them
+  if (d.delta_de || d.de_final > DEF_LINEAR_OFFSET) d.generic = 1;  // so do the delta DE and the other DE functions
   *out = d;
   return MBR_OK;
 }
@@ -785,6 +814,19 @@ mbr_status ctx_work(mbr_ctx *ctx, size_t words, unsigned long long **out) {
   return MBR_OK;
 }
 
+mbr_status ctx_adjoint_partials(mbr_ctx *ctx, size_t bytes, double **out) {
+  if (ctx->adjoint_scratch_bytes < bytes) {
+    if (ctx->adjoint_scratch) cudaFree(ctx->adjoint_scratch);
+    ctx->adjoint_scratch = nullptr;
+    ctx->adjoint_scratch_bytes = 0;
+    const int e = int(cudaMalloc(&ctx->adjoint_scratch, bytes));
+    if (e) return set_err(ctx, MBR_ENOMEM, "cudaMalloc(adjoint partials): %s", cudaGetErrorString(cudaError_t(e)));
+    ctx->adjoint_scratch_bytes = bytes;
+  }
+  *out = static_cast<double *>(ctx->adjoint_scratch);
+  return MBR_OK;
+}
+
 }  // namespace mbr
 
 // ============================================================================
@@ -895,6 +937,10 @@ void mbr_fractal_defaults(mbr_fractal *f, int formula) {
     f->ifs_direction[i][0] = 1.0;
     f->ifs_intensity[i] = 1.0;
   }
+  f->aexion_cadd = -1.3;        // initparameters.cpp:722
+  f->analytic_de_enabled = 1;   // :904-909
+  f->analytic_de_scale1 = 1.0;
+  f->analytic_de_offset1 = 1.0;
 }
 
 void mbr_scene_defaults(mbr_scene *s) {
@@ -920,6 +966,8 @@ void mbr_scene_defaults(mbr_scene *s) {
   s->box_folding_value = 2.0;
   s->spherical_folding_inner = 0.5;
   s->spherical_folding_outer = 1.0;
+  s->delta_de_method = MBR_DE_METHOD_PREFERRED;
+  s->deltade_relative_delta = 0.01;  // :166
 }
 
 void mbr_camera_defaults(mbr_camera *c) {
@@ -1028,10 +1076,23 @@ mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_p
   if (fp32 && ctx->scene.has_w)
     return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need a 3-D state: initial_waxis == 0 and no hypercomplex "
                                           "formula");
+  if (engine == MBR_ENGINE_PLAIN_MIXED && ctx->scene.delta_de)
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "the delta DE offsets points by 1e-5 of the detail size, which FP32 points do not resolve: use a "
+                   "plain FP64 engine");
+  // the delta DE's offset factor follows this render's advanced quality
+  // (calculate_distance.cpp:616-623); the scene is a launch parameter
+  DevScene scd;
+  const DevScene *scp = &ctx->scene;
+  if (ctx->scene.delta_de) {
+    scd = ctx->scene;
+    scd.delta_factor = params->advanced_quality ? scd.delta_rel : 1e-5;
+    scp = &scd;
+  }
   int e;
   switch (engine) {
-    case MBR_ENGINE_PLAIN_FP64: e = launch_plain_fp64(ctx->scene, fr, d, stream); break;
-    case MBR_ENGINE_PLAIN_FP64_STRICT: e = launch_plain_fp64_strict(ctx->scene, fr, d, stream); break;
+    case MBR_ENGINE_PLAIN_FP64: e = launch_plain_fp64(*scp, fr, d, stream); break;
+    case MBR_ENGINE_PLAIN_FP64_STRICT: e = launch_plain_fp64_strict(*scp, fr, d, stream); break;
     case MBR_ENGINE_PLAIN_MIXED: e = launch_plain_mixed(ctx->scene, fr, d, stream); break;
     case MBR_ENGINE_WAVEFRONT_FP32:
     case MBR_ENGINE_WAVEFRONT_FP64:
@@ -1081,6 +1142,8 @@ mbr_status mbr_distance(mbr_ctx *ctx, const double *points, int64_t n, double de
     case MBR_ENGINE_PLAIN_MIXED:
     case MBR_ENGINE_WAVEFRONT_FP32:
       if (ctx->scene.has_w) return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need initial_waxis == 0");
+      if (ctx->scene.delta_de)
+        return set_err(ctx, MBR_EUNSUPPORTED, "the delta DE needs FP64 points: use a plain FP64 engine");
       e = launch_distance_fp32(ctx->scene, points, n, detail_size, normal_mode, dist, iters, stream);
       break;
     default: return set_err(ctx, MBR_EINVAL, "unknown engine %d", engine);

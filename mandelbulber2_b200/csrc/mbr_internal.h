@@ -24,6 +24,8 @@ const mbr_scene *ctx_scene_src(mbr_ctx *ctx);
 mbr_tuning &ctx_tuning(mbr_ctx *ctx);
 int32_t *ctx_status(mbr_ctx *ctx);
 mbr_status ctx_work(mbr_ctx *ctx, size_t words, unsigned long long **out);
+// Device buffer of the adjoint's per-block partial sums, grown on demand.
+mbr_status ctx_adjoint_partials(mbr_ctx *ctx, size_t bytes, double **out);
 
 // wavefront.cu
 mbr_status render_wavefront(mbr_ctx *ctx, const DevScene &sc, const DevFrame &fr, const DevOutputs &out, int engine,

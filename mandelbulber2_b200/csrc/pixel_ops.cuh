@@ -199,10 +199,10 @@ enum { K_DE = 0, K_ITERS, K_MARCH, K_BINARY, K_NORMAL, K_SHADOW, K_AO, K_GI, K_P
 template <class T, int F, bool W>
 __device__ __forceinline__ double de_eval(const DevScene &sc, D3 q, double detail, bool normal_mode, int *iters,
                                           ThreadCount &tc) {
-  int it;
-  const T d = calc_distance<T, F, W>(sc, T(q.x), T(q.y), T(q.z), T(detail), normal_mode, &it);
+  int it, total;
+  const T d = calc_distance<T, F, W>(sc, T(q.x), T(q.y), T(q.z), T(detail), normal_mode, &it, &total);
   tc.de++;
-  tc.iters += unsigned(it);
+  tc.iters += unsigned(total);
   *iters = it;
   return double(d);
 }

@@ -474,7 +474,9 @@ struct PrecHybT {
     if (EXT) global_folds<float, false>(sc, z, e.r, de);
     const V4<float> tempZ = z;
     const float tempDE = de;
-    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs);
+    // the Aexion, the one formula that replaces c, is 4-D and never runs here
+    V4<float> c{e.cx, e.cy, e.cz, 0.0f};
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs, i, c);
     if (s.add_c) {
       if (sc.julia) {
         z.x = z.x + juliac_of<float>(sc, 0);
@@ -524,18 +526,7 @@ struct PrecHybT {
       }
     }
     iters = e.brk ? e.it : e.it + 1;
-    const float r = e.r, DE = e.dr;
-    float d;
-    if (DE > 0.0f) {
-      const int fn = sc.is_hybrid ? ((sc.de_function == 1) ? 4 : 2) : sc.de_analytic;
-      if (fn == 4) d = (r - sc.flinear_de_offset) / DE;
-      else if (fn == 2) d = (r > 1.0f) ? float(0.5f * r * logf(r) / DE) : 0.0f;
-      else if (fn == 1) d = r / DE;
-      else if (fn == 3) d = (r - 2.0f) / DE;
-      else d = r;
-    } else {
-      d = r;
-    }
+    float d = final_distance<float, EXT ? F_EXT : 0, false>(sc, V4<float>{e.zx, e.zy, e.zz, 0.0f}, e.r, e.dr);
     if (iters < sc.min_n && d < detail) d = detail;
     if (d < 0.0f) d = 0.0f;
     if (d > 10.0f) d = 10.0f;
@@ -1875,6 +1866,10 @@ static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFra
   if (sc.iter_thresh || sc.interior || sc.has_w)
     return set_err(ctx, MBR_EUNSUPPORTED,
                    "wavefront engine: iteration_threshold_mode, interior_mode and initial_waxis != 0 use the plain engines");
+  if (sc.delta_de)
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "wavefront engine: the delta DE offsets points by 1e-5 of the detail size, which FP32 points do "
+                   "not resolve; it runs on the plain FP64 engines");
   if (fr.refine != MBR_REFINE_REFERENCE)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: root refinement uses the plain engines");
   return MBR_OK;

@@ -46,7 +46,7 @@ thread_local OpTally g_tally;
 // ============================================================================
 struct FormulaInfo {
   int de_function;      // enumDEFunctionType
-  int cpixel;           // enumCPixelAddition: 0 enabled by default, 1 disabled by default
+  int cpixel;           // enumCPixelAddition: 0 enabled by default, 1 disabled by default, 2 already has
   double default_bailout;
   int analytic;         // enumDEAnalyticFunction
 };
@@ -57,6 +57,8 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_HYPERCOMPLEX: *fi = {2, 0, 10.0, 2}; return true;      // fractal_hypercomplex.cpp:17-28
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: *fi = {1, 1, 100.0, 3}; return true;  // fractal_kaleidoscopic_ifs.cpp:17-28
     case MBR_FORMULA_XENODREAMBUIE: *fi = {2, 0, 10.0, 2}; return true;       // fractal_xenodreambuie.cpp:17-28
+    case MBR_FORMULA_QUATERNION: *fi = {2, 0, 10.0, 2}; return true;          // fractal_quaternion.cpp:16-27
+    case MBR_FORMULA_AEXION: *fi = {2, 2, 10000.0, 2}; return true;           // fractal_aexion.cpp:16-27
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
     default: return false;
@@ -99,6 +101,10 @@ struct Seq {
   bool is_hybrid = false, julia = false;
   int length = 0, n = 0, formula_maxiter = 250, min_n = 1;
   int de_function = 1, de_analytic = 1;
+  // delta DE (calculate_distance.cpp:607-760): on, and the offset factor
+  // (1e-5, or deltade_relative_delta under advanced quality: set per render)
+  bool delta_de = false;
+  double delta_rel = 0.01, delta_factor = 1e-5;
   bool iter_thresh = false, interior = false;
   double julia_c[3] = {0, 0, 0}, cmul[3] = {1, 1, 1}, w0 = 0, linear_de_offset = 0;
   std::vector<int> seq;
@@ -135,6 +141,7 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     // c-constant rule :204-215
     bool addc = !(f.dont_add_c_constant != 0);
     if (fi.cpixel == 1) addc = !addc;
+    if (fi.cpixel == 2) addc = false;  // cpixelAlreadyHas (hybrid_fractal_sequences.cpp:209-212)
     sl.add_c = addc;
     if (sc.use_default_bailout) {  // :217-224
       if (hybrid) maxBailout = std::max(maxBailout, fi.default_bailout);
@@ -231,12 +238,19 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     formula_info(s.slot[0].formula, &fi);
     s.de_function = fi.de_function;
     s.de_analytic = fi.analytic;
-    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {
+    if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {  // :477-500
       s.de_function = sc.delta_de_function;
-      s.de_analytic = (s.de_function == 2) ? 2 : 1;
+      static const int fn_analytic[7] = {1, 1, 2, 4, 5, 6, 7};  // enumDEAnalyticFunction
+      s.de_analytic = fn_analytic[s.de_function];
     }
   }
-  if (s.de_function != 1 && s.de_function != 2) return false;
+  // every formula restated here is analytic: only the forced method makes
+  // the sequence a delta-DE one (:376-377, 463, 474)
+  s.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+  s.delta_rel = sc.deltade_relative_delta;
+  if (s.de_function < 1 || s.de_function > 6) return false;
+  // the analytic Jos Kleinian function reads formula parameters not carried here
+  if (!s.delta_de && (hybrid ? s.de_function == 4 : s.de_analytic == 5)) return false;
   if (sc.n_primitives < 0 || sc.n_primitives > MBR_MAX_PRIMITIVES) return false;
   for (int k = 0; k < sc.n_primitives; k++) {
     OPrim op;
@@ -711,6 +725,49 @@ inline void formula_hypercomplex(V4<S> &z, const S &r, S &DE) {
   z.w = nw;
 }
 
+// cFractalQuaternion::FormulaCode (fractal_quaternion.cpp:29-39)
+template <class S>
+inline void formula_quaternion(V4<S> &z, const S &r, S &DE) {
+  DE = DE * 2.0 * r;
+  const S nx = z.x * z.x - z.y * z.y - z.z * z.z;
+  const S ny = 2.0 * z.x * z.y;
+  const S nz = 2.0 * z.x * z.z;
+  z.x = nx;
+  z.y = ny;
+  z.z = nz;
+}
+
+// cFractalAexion::FormulaCode (fractal_aexion.cpp:29-59); c is aux.const_c,
+// replaced at the orbit's first iteration
+template <class S>
+inline void formula_aexion(V4<S> &z, const S &r, S &DE, const mbr_fractal &p, int i, V4<S> &c) {
+  V4<S> temp = z;
+  S t;
+  if (i == 0) {
+    t = p.aexion_cadd;
+    temp.x = z.x + z.y + z.z;
+    temp.y = -z.x - z.y + z.z;
+    temp.z = -z.x + z.y - z.z;
+    temp.w = z.x - z.y - z.z;
+    z = V4<S>{fabs(temp.x) + t, fabs(temp.y) + t, fabs(temp.z) + t, fabs(temp.w) + t};
+    c = z;
+  }
+  t = 2.0 * z.w * z.z;
+  temp.x = z.x * z.x - z.y * z.y;
+  temp.y = t - temp.x;
+  temp.x = temp.x + t;
+  t = 2.0 * z.x * z.y;
+  temp.z = z.z * z.z - z.w * z.w;
+  temp.w = t - temp.z;
+  temp.z = temp.z + t;
+  z = V4<S>{temp.x + c.x, temp.y + c.y, temp.z + c.z, temp.w + c.w};
+  if (p.analytic_de_enabled) {
+    S de1 = 1.1 * r;
+    de1 = de1 + (len4(z) / r - de1) * p.analytic_de_scale1;
+    DE = de1 * 2.0 * DE + p.analytic_de_offset1;
+  }
+}
+
 // cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
 template <class S>
 inline void formula_ifs(V4<S> &z, const SlotT<S> &f, S &DE) {
@@ -793,6 +850,7 @@ struct FractalOut {
   S distance;
   int iters;
   bool maxiter;
+  V4<S> z;  // the orbit's last z (fractOut.z)
 };
 
 // Compute<calcModeNormal> (compute_fractal.cpp:67-654), without global
@@ -804,7 +862,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   V4<S> z{px, py, pz, S(0.0)};
   z.w = S(seq.w0);
   out.maxiter = true;
-  const V4<S> const_c = z;
+  V4<S> const_c = z;  // aux.const_c (the Aexion replaces it)
   S r = len4(z);
   S DE = 1.0;
   V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ;
@@ -852,10 +910,13 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(z, r, DE); break;
         case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(z, f, DE); break;
         case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(z, f, r, DE); break;
+        case MBR_FORMULA_QUATERNION: formula_quaternion(z, r, DE); break;
+        case MBR_FORMULA_AEXION: formula_aexion(z, r, DE, sd.ifs, i, const_c); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
           out.maxiter = true;
+          out.z = z;
           return out;
         }
       }
@@ -899,18 +960,35 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
       break;
     }
   }
-  // final DE :495-621
+  // final DE :495-621 (aux.pseudoKleinianDE = 1 and aux.dist = 1000 keep
+  // their initial values :119-120 for every formula restated here)
   if (DE > 0.0) {
     if (seq.is_hybrid) {
-      if (seq.de_function == 1)
-        out.distance = (r - seq.linear_de_offset) / DE;
-      else
-        out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0);
+      switch (seq.de_function) {
+        case 1: out.distance = (r - seq.linear_de_offset) / DE; break;
+        case 2: out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0); break;
+        case 3: {
+          const S rxy = sqrt(z.x * z.x + z.y * z.y);
+          out.distance = std::max(S(rxy - 1.0), S(fabs(rxy * z.z) / r)) / DE;
+          break;
+        }
+        case 5: out.distance = 1000.0; break;
+        case 6: out.distance = std::max(fabs(z.x), std::max(fabs(z.y), fabs(z.z))) / DE; break;
+        default: out.distance = 0.0; break;
+      }
     } else {
       switch (seq.de_analytic) {
         case 2: out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0); break;
         case 1: out.distance = r / DE; break;
         case 3: out.distance = (r - 2.0) / DE; break;
+        case 4: {
+          const S rxy = sqrt(z.x * z.x + z.y * z.y);
+          out.distance = std::max(S(rxy - 1.0), S(fabs(rxy * z.z) / r)) / DE;
+          break;
+        }
+        case 6: out.distance = 1000.0; break;
+        case 7: out.distance = std::max(fabs(z.x), std::max(fabs(z.y), fabs(z.z))) / DE; break;
+        case 0: out.distance = -1.0; break;
         default: out.distance = r; break;
       }
     }
@@ -918,6 +996,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
     out.distance = r;
   }
   out.iters = i + 1;
+  out.z = z;
   return out;
 }
 
@@ -931,12 +1010,100 @@ inline void zero_tangents(Dual<N> &d) {
   for (int i = 0; i < N; i++) d.d[i] = 0.0;
 }
 
+// CalculateDistanceSimple, delta-DE branch (calculate_distance.cpp:607-760):
+// the orbit radius |z| (3-D) at the point and at three points offset by
+// deltaDE along x, y and z, the offset orbits capped at the first orbit's
+// iteration count (forcedMaxiter), the DE function of the sequence applied to
+// the radius and the gradient of |z|.  *iters_out: the first orbit's count;
+// *total_iters (when given): all four.
+static double delta_distance(const Seq &seq, const SlotT<double> *slots, double px, double py, double pz,
+                             double detailSize, bool normalMode, int mult, int *iters_out, int *total_iters = nullptr) {
+  const double plen = sqrt(px * px + py * py + pz * pz);
+  const double deltaDE = std::max(plen * 1e-14, seq.delta_factor * detailSize);
+  // Compute's delta-mode ending for the Jos Kleinian function
+  // (compute_fractal.cpp:627-638): z.y = min(z.y, foldingValue - z.y) with
+  // the default transf_spheres_enabled (true) and transf_folding_value (2)
+  auto jos_fold = [&](FractalOut<double> &f) {
+    if (seq.de_function == 4) f.z.y = std::min(f.z.y, 2.0 - f.z.y);
+  };
+  FractalOut<double> fo = compute<double>(seq, slots, px, py, pz, mult, -1);
+  jos_fold(fo);
+  const V4<double> zFromIters = fo.z;
+  const double r = sqrt(fo.z.x * fo.z.x + fo.z.y * fo.z.y + fo.z.z * fo.z.z);
+  bool out_maxiter = fo.maxiter;
+  bool maxiter = fo.maxiter;
+  const int iters1 = fo.iters;
+  int total = fo.iters;
+  if (!seq.limits) {
+    if (!seq.iter_thresh) maxiter = false;
+  } else {
+    if (normalMode) maxiter = false;
+  }
+  double drv[3];
+  for (int a = 0; a < 3; a++) {
+    fo = compute<double>(seq, slots, px + (a == 0 ? deltaDE : 0.0), py + (a == 1 ? deltaDE : 0.0),
+                         pz + (a == 2 ? deltaDE : 0.0), mult, iters1);
+    jos_fold(fo);
+    const double r2 = sqrt(fo.z.x * fo.z.x + fo.z.y * fo.z.y + fo.z.z * fo.z.z);
+    drv[a] = fabs(r2 - r) / deltaDE;
+    total += fo.iters;
+  }
+  const double dr = sqrt(drv[0] * drv[0] + drv[1] * drv[1] + drv[2] * drv[2]);
+  double distance = 0.0;
+  if (dr > 0) {
+    const V4<double> &z = fo.z;  // the last offset orbit (:686-698)
+    switch (seq.de_function) {
+      case 1: distance = 0.5 * r / dr; break;
+      case 2: distance = 0.5 * r * log(r) / dr; break;
+      case 3: {
+        const double rxy = sqrt(z.x * z.x + z.y * z.y);
+        distance = std::max(rxy - 0.92784, fabs(rxy * z.z) / r) / dr;
+        break;
+      }
+      case 4: {
+        const double rxy = sqrt(z.x * z.x + z.z * z.z);
+        distance = (fabs(rxy * z.y) / r) / dr;
+        maxiter = false;
+        break;
+      }
+      case 5: distance = r; break;
+      case 6: {  // dMax (common_math.cpp:74-83)
+        auto dmax3 = [](double a, double b, double c) { return (a > b) ? ((a > c) ? a : c) : ((b > c) ? b : c); };
+        const double maxZ = dmax3(fabs(zFromIters.x), fabs(zFromIters.y), fabs(zFromIters.z));
+        const double maxDr = dmax3(fabs(drv[0]), fabs(drv[1]), fabs(drv[2]));
+        distance = 0.5 * maxZ / maxDr;
+        break;
+      }
+      default: break;
+    }
+  } else {
+    distance = r;
+  }
+  if (!seq.iter_thresh) out_maxiter = false;
+  if (normalMode) out_maxiter = false;
+  if (out_maxiter) distance = 0.0;
+  if (fo.iters < seq.min_n && distance < detailSize) distance = detailSize;  // the last offset orbit's count
+  if (seq.interior && !normalMode) {
+    if (distance < 0.5 * detailSize || maxiter) distance = detailSize;
+  } else if (seq.interior && normalMode) {
+    if (distance < 0.9 * detailSize) distance = detailSize - distance;
+  }
+  if (seq.iter_thresh && !normalMode && !maxiter) {
+    if (distance < detailSize) distance = detailSize * 1.01;
+  }
+  if (distance < 0.0) distance = 0.0;
+  if (distance > 10.0) distance = 10.0;
+  if (iters_out) *iters_out = iters1;
+  if (total_iters) *total_iters = total;
+  return distance;
+}
+
 // CalculateDistanceSimple, analytic branch (calculate_distance.cpp:533-606),
 // reached through CalculateDistanceFromObjectsTree (:225-516) for the single
 // identity-transform node (pointLocal == point, distance *= 1).
 template <class S>
 S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
-                int *iters_out) {
+                int *iters_out, int *total_out = nullptr) {
   if (seq.limits) {  // the limit box early-out (calculate_distance.cpp:261-275)
     S bx = std::max(px - seq.lim_max[0], -(px - seq.lim_min[0]));
     S by = std::max(py - seq.lim_max[1], -(py - seq.lim_min[1]));
@@ -944,15 +1111,27 @@ S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double 
     S limitBoxDist = std::max({bx, by, bz});
     if (limitBoxDist > detailSize) {
       if (iters_out) *iters_out = 0;  // the reference leaves out->iters unset here
+      if (total_out) *total_out = 0;
       return limitBoxDist;
     }
   }
   const int mult = (normalMode && seq.iter_thresh) ? 5 : 1;
+  if constexpr (std::is_same<S, double>::value) {
+    if (seq.delta_de) {
+      S distance = delta_distance(seq, slots, px, py, pz, detailSize, normalMode, mult, iters_out, total_out);
+      for (const OPrim &op : seq.prims) {  // booleanAdd with the primitives
+        const double pd = prim_distance(op, px, py, pz);
+        if (pd < distance) distance = pd;
+      }
+      return distance;
+    }
+  }
   FractalOut<S> fo = compute<S>(seq, slots, px, py, pz, mult, -1);
   S distance = fo.distance;
   if (fo.maxiter) zero_tangents(distance);
   bool maxiter = fo.maxiter;
   if (iters_out) *iters_out = fo.iters;
+  if (total_out) *total_out = fo.iters;
   if (!seq.iter_thresh) maxiter = false;
   if (normalMode) maxiter = false;
   if (maxiter) distance = 0.0;
@@ -1156,10 +1335,10 @@ struct Renderer {
   bool want_normal = false;
 
   double de(D3 q, double detail, bool normalMode, int *iters, Counters &c) const {
-    int it = 0;
-    double d = calc_distance<double>(seq, slots.data(), q.x, q.y, q.z, detail, normalMode, &it);
+    int it = 0, total = 0;
+    double d = calc_distance<double>(seq, slots.data(), q.x, q.y, q.z, detail, normalMode, &it, &total);
     c.de++;
-    c.iters += it;
+    c.iters += total;
     if (iters) *iters = it;
     return d;
   }
@@ -1642,6 +1821,8 @@ static void to_rgb8(const float *rgb, const mbr_render_params &p, const std::vec
 static bool make_renderer(const mbr_scene *scene, const mbr_camera *cam, const mbr_render_params *params,
                           Renderer *R) {
   if (!build_sequence(*scene, &R->seq)) return false;
+  // the delta DE's offset factor (calculate_distance.cpp:616-623)
+  R->seq.delta_factor = params->advanced_quality ? R->seq.delta_rel : 1e-5;
   R->slots.clear();
   for (int i = 0; i < R->seq.n; i++) R->slots.push_back(make_slot<double>(R->seq.slot[i], false));
   R->p = *params;
@@ -1703,6 +1884,10 @@ void oracle_fractal_defaults(mbr_fractal *f, int formula) {
     f->ifs_direction[i][0] = 1.0;
     f->ifs_intensity[i] = 1.0;
   }
+  f->aexion_cadd = -1.3;        // initparameters.cpp:722
+  f->analytic_de_enabled = 1;   // :904-909
+  f->analytic_de_scale1 = 1.0;
+  f->analytic_de_offset1 = 1.0;
 }
 
 void oracle_scene_defaults(mbr_scene *s) {
@@ -1724,6 +1909,8 @@ void oracle_scene_defaults(mbr_scene *s) {
   s->box_folding_value = 2.0;
   s->spherical_folding_inner = 0.5;
   s->spherical_folding_outer = 1.0;
+  s->delta_de_method = MBR_DE_METHOD_PREFERRED;
+  s->deltade_relative_delta = 0.01;  // initparameters.cpp:166
 }
 
 void oracle_camera_defaults(mbr_camera *c) {
@@ -1929,6 +2116,7 @@ int oracle_formula_step(const mbr_scene *scene, int slot, double *z, double *r, 
     case MBR_FORMULA_HYPERCOMPLEX: formula_hypercomplex(v, *r, *de); break;
     case MBR_FORMULA_KALEIDOSCOPIC_IFS: formula_ifs(v, f, *de); break;
     case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(v, f, *r, *de); break;
+    case MBR_FORMULA_QUATERNION: formula_quaternion(v, *r, *de); break;
     default: return 1;
   }
   z[0] = v.x; z[1] = v.y; z[2] = v.z; z[3] = v.w;

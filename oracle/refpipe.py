@@ -167,6 +167,10 @@ class RefPipeline:
             self.set("mandelbox_folding_fixed_radius", f.mandelbox_folding_fixed_radius, KIND_DOUBLE, i)
             self.set("mandelbox_offset", list(f.mandelbox_offset), KIND_VEC3, i)
             self.set("transf_scale_3", f.transf_scale3, KIND_DOUBLE, i)
+            self.set("cadd", f.aexion_cadd, KIND_DOUBLE, i)
+            self.set("analyticDE_enabled", f.analytic_de_enabled, KIND_BOOL, i)
+            self.set("analyticDE_scale_1", f.analytic_de_scale1, KIND_DOUBLE, i)
+            self.set("analyticDE_offset_1", f.analytic_de_offset1, KIND_DOUBLE, i)
             self.set("mandelbox_rotations_enabled", f.mandelbox_rotations_enabled, KIND_BOOL, i)
             self.set("mandelbox_main_rotation_enabled", f.mandelbox_main_rotation_enabled, KIND_BOOL, i)
             self.set("mandelbox_rotation_main", list(f.mandelbox_rotation_main), KIND_VEC3, i)
@@ -194,6 +198,8 @@ class RefPipeline:
         self.set("interior_mode", s.interior_mode, KIND_BOOL)
         self.set("linear_DE_offset", s.linear_de_offset, KIND_DOUBLE)
         self.set("delta_DE_function", s.delta_de_function, KIND_INT)
+        self.set("delta_DE_method", s.delta_de_method, KIND_INT)
+        self.set("deltade_relative_delta", s.deltade_relative_delta, KIND_DOUBLE)
         self.set("N", s.formula_maxiter, KIND_INT)
         self.set("repeat_from", s.repeat_from, KIND_INT)
         self.set("limits_enabled", s.limits_enabled, KIND_BOOL)

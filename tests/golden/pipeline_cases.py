@@ -138,6 +138,74 @@ def cases():
     s.formula_maxiter = 30
     s.spherical_folding = 1
     out["hypercomplex_spherical_fold"] = s
+    # the delta DE (calculate_distance.cpp:607-760) with each DE function
+    for name, base, fn in (("bulb_delta_preferred", configs.mandelbulb_scene(8.0, 30), abi.DE_PREFERRED),
+                           ("box_delta_preferred", configs.mandelbox_scene(-1.5, 0.5, 30), abi.DE_PREFERRED),
+                           ("box_delta_log", configs.mandelbox_scene(-1.5, 0.5, 30), abi.DE_LOG),
+                           ("bulb_delta_pseudo_kleinian", configs.mandelbulb_scene(8.0, 30), abi.DE_PSEUDO_KLEINIAN),
+                           ("box_delta_jos_kleinian", configs.mandelbox_scene(-1.5, 0.5, 30), abi.DE_JOS_KLEINIAN),
+                           ("menger_delta_custom", configs.menger_scene(10), abi.DE_CUSTOM),
+                           ("box_delta_max_axis", configs.mandelbox_scene(2.0, 0.5, 30), abi.DE_MAX_AXIS)):
+        base.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+        base.delta_de_function = fn
+        out[name] = base
+    s = configs.hybrid_scene()
+    s.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+    s.min_n = 3
+    out["hybrid_delta"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+    s.interior_mode = 1
+    out["box_delta_interior"] = s
+    s = configs.mandelbox_scene(-1.5, 0.5, 30)
+    s.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+    s.iteration_threshold_mode = 1
+    s.limits_enabled = 1
+    out["box_delta_iter_thresh_limits"] = s
+    # the other analytic DE functions (compute_fractal.cpp:495-621)
+    for name, base, fn in (("bulb_pseudo_kleinian", configs.mandelbulb_scene(8.0, 30), abi.DE_PSEUDO_KLEINIAN),
+                           ("box_custom", configs.mandelbox_scene(-1.5, 0.5, 30), abi.DE_CUSTOM),
+                           ("box_max_axis", configs.mandelbox_scene(-1.5, 0.5, 30), abi.DE_MAX_AXIS)):
+        base.delta_de_function = fn
+        out[name] = base
+    s = configs.hybrid_scene()
+    s.delta_de_function = abi.DE_MAX_AXIS
+    out["hybrid_max_axis"] = s
+    s = configs.hybrid_scene()
+    s.delta_de_function = abi.DE_PSEUDO_KLEINIAN
+    out["hybrid_pseudo_kleinian"] = s
+    # quaternion (5) and aexion (19)
+    s = abi.scene_defaults(abi.FORMULA_QUATERNION)
+    s.formula_maxiter = 40
+    out["quaternion"] = s
+    s = abi.scene_defaults(abi.FORMULA_AEXION)
+    s.formula_maxiter = 40
+    out["aexion"] = s
+    s = abi.scene_defaults(abi.FORMULA_AEXION)
+    s.formula_maxiter = 30
+    s.fractal[0].aexion_cadd = -1.1
+    s.fractal[0].analytic_de_scale1 = 0.8
+    s.fractal[0].analytic_de_offset1 = 0.5
+    out["aexion_params"] = s
+    s = abi.scene_defaults(abi.FORMULA_AEXION)
+    s.formula_maxiter = 30
+    s.fractal[0].analytic_de_enabled = 0
+    out["aexion_no_analytic_de"] = s
+    s = abi.scene_defaults(abi.FORMULA_AEXION)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    s.formula_maxiter = 30
+    s.fractal[0].formula_iterations = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_QUATERNION)
+    out["hybrid_aexion_quaternion"] = s
+    s = abi.scene_defaults(abi.FORMULA_MANDELBULB)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    s.formula_maxiter = 30
+    s.fractal[0].bulb_power = 8.0
+    s.fractal[0].formula_iterations = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_QUATERNION)
+    out["hybrid_bulb_quaternion"] = s
     return out
 
 
@@ -206,4 +274,14 @@ def render_cases():
                 params(soft_shadow_cone=15.0)))
     out.append(("bulb_global_folds", cases_["bulb_global_box_fold"],
                 configs.camera((0.3, -2.8, 0.4), width=32, height=24), params()))
+    out.append(("box_delta_de", cases_["box_delta_preferred"], configs.camera((0.0, -6.0, 0.0), width=40, height=24),
+                params()))
+    s = abi.scene_defaults(abi.FORMULA_QUATERNION)
+    s.formula_maxiter = 30
+    out.append(("quaternion", s, configs.camera((0.3, -2.4, 0.8), width=32, height=24), params()))
+    sc, cam, p = configs.mandelbulb_512(32, 24, binary_steps=30)
+    sc.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+    sc.deltade_relative_delta = 0.02
+    p.advanced_quality = 1  # the offset is deltade_relative_delta of the detail size
+    out.append(("bulb_delta_de_advanced_quality", sc, cam, p))
     return out

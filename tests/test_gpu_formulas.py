@@ -134,3 +134,39 @@ def test_xenodreambuie(renderer, oracle):
         else:
             assert m["hit_mismatch"] <= 0.005, m
             assert m["depth_rel_median"] <= 1e-4, m
+
+
+def test_quaternion(renderer, oracle):
+    """Formula 5 (fractal_quaternion.cpp:29-39): +, -, * only, so the strict
+    FP64 kernel is bit-exact; 3-D, so every engine that takes extended
+    scenes renders it."""
+    sc, cam, p = scene(abi.FORMULA_QUATERNION)
+    cam.camera[:] = [0.3, -2.4, 0.8]
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.95
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED,
+                   abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
+        check(renderer, sc, cam, p, o, ost, engine, "quaternion")
+
+
+@pytest.mark.parametrize("case", ["aexion", "hybrid_aexion_quaternion"])
+def test_aexion(renderer, oracle, case):
+    """Formula 19 (fractal_aexion.cpp:29-59): 4-D, with the orbit's c replaced
+    at its first iteration; the plain FP64 engines render it (strict
+    bit-exact), the FP32 engines refuse its 4-D state."""
+    from mandelbulber2_b200.render import MbrError
+    from tests.golden.pipeline_cases import cases
+
+    sc = cases()[case]
+    _, cam, p = scene(abi.FORMULA_AEXION)
+    cam.camera[:] = [0.5, -3.5, 1.2]
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.95, float(np.mean(o["hit"]))
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64):
+        check(renderer, sc, cam, p, o, ost, engine, case)
+    for engine in (abi.ENGINE_PLAIN_MIXED, abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO):
+        with pytest.raises(MbrError) as e:
+            renderer.render(cam, p, engine)
+        assert e.value.status == abi.MBR_EUNSUPPORTED

@@ -244,7 +244,8 @@ def test_limit_box_and_global_folds(renderer, oracle, case):
     from tests.golden.pipeline_cases import cases
 
     sc = cases()[case]
-    cam = configs.camera((0.0, -5.0, 0.5) if case == "box_limits" else (0.3, -2.8, 0.4), width=64, height=40)
+    pos = {"box_limits": (0.0, -5.0, 0.5), "bulb_global_box_fold": (0.3, -6.0, 0.4)}.get(case, (0.3, -2.8, 0.4))
+    cam = configs.camera(pos, width=64, height=40)
     p = configs.base_params(5, 20.0)
     p.ao_rays = 4
     p.soft_shadow_cone = 15.0
@@ -255,3 +256,133 @@ def test_limit_box_and_global_folds(renderer, oracle, case):
     with pytest.raises(MbrError) as e:
         renderer.render(cam, p, abi.ENGINE_WAVEFRONT_FP64)
     assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+# Formulas without transcendental functions (the Mandelbox, the Menger
+# sponge) run the same IEEE operations on the strict FP64 engine as in the
+# oracle, so their distances are bit-identical; the Mandelbulb's asin, atan2,
+# sincos and pow differ from the host's libm by an ulp here and there.
+def _exact(case):
+    return "bulb" not in case and "hybrid" not in case
+
+
+def _rel(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+@pytest.mark.parametrize("case", ["box_delta_preferred", "bulb_delta_pseudo_kleinian", "box_delta_jos_kleinian",
+                                  "box_delta_max_axis", "hybrid_delta", "box_delta_iter_thresh_limits"])
+def test_delta_de_distances(renderer, oracle, case):
+    """The delta DE (calculate_distance.cpp:607-760) through mbr_distance
+    against the oracle (which equals the reference's own CalculateDistance on
+    these scenes, tests/golden/pipeline_kat.json).  The strict FP64 engine is
+    bit-identical on the Mandelbox and Menger scenes.  The difference quotient
+    over offsets of 1e-5 of the detail size magnifies an ulp of |z| about
+    1e7-fold (the max-axis function, one derivative component, more), so the
+    FMA engine and the Mandelbulb scenes are held, over the points whose
+    orbit escapes within N iterations, to median relative error <= 1e-6 and
+    95th percentile <= 1e-3, with iteration counts identical on >= 99.9 % of
+    them.  Longer orbits (the set's interior, iterated up to 5 x N for the
+    normals in iteration-threshold mode) are chaotic: there an ulp decides
+    the result on either engine, so they are not compared.  FP32 engines
+    refuse the delta DE."""
+    from tests.golden.pipeline_cases import cases
+
+    sc = cases()[case]
+    renderer.set_scene(sc)
+    rng = np.random.default_rng(11)
+    pts = rng.uniform(-2.0, 2.0, size=(4096, 3))
+    for det in (1e-3, 0.05):
+        for nm in (False, True):
+            od, oit = oracle.distance(sc, pts, det, nm)
+            for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64):
+                d, it = renderer.distance(torch.from_numpy(pts), det, nm, engine)
+                d, it = d.cpu().numpy(), it.cpu().numpy()
+                if engine == abi.ENGINE_PLAIN_FP64_STRICT and _exact(case):
+                    assert np.array_equal(d, od) and np.array_equal(it, oit), (case, det, nm)
+                    continue
+                esc = oit <= sc.formula_maxiter
+                rel = _rel(d[esc], od[esc])
+                print(case, det, nm, abi.ENGINE_NAMES[engine], "escaping", int(esc.sum()), "rel median",
+                      np.median(rel), "p95", np.percentile(rel, 95), "iters", np.mean(it[esc] == oit[esc]))
+                assert esc.sum() >= 256
+                assert np.median(rel) <= 1e-6 and np.percentile(rel, 95) <= 1e-3, (case, det, nm, engine)
+                assert np.mean(it[esc] == oit[esc]) >= 0.999, (case, det, nm, engine)
+    with pytest.raises(MbrError) as e:
+        renderer.distance(torch.from_numpy(pts), 1e-3, False, abi.ENGINE_PLAIN_MIXED)
+    assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("case", ["box_delta_de", "bulb_delta_de_advanced_quality"])
+def test_delta_de_frames(renderer, oracle, case):
+    """Frames with the delta DE on the plain FP64 engines against the oracle
+    (whose render worker equals the reference's on these frames,
+    tests/golden/render_kat.json): bit-identical on the strict engine for the
+    Mandelbox; otherwise hits and iteration counts identical on >= 99.5 % of
+    the pixels (the delta quotient's magnified rounding moves a few march
+    steps) and depth within 1e-6 on >= 99 % of the common hits.  The other
+    engines refuse delta-DE scenes."""
+    from tests.golden.pipeline_cases import render_cases
+
+    _, sc, cam, p = [c for c in render_cases() if c[0] == case][0]
+    cam.width, cam.height = 96, 64
+    p.ao_rays = 4
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.98
+    renderer.set_scene(sc)
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64):
+        fr = renderer.render(cam, p, engine, outputs=NAMES)
+        g = {k: v.cpu().numpy() for k, v in fr.buffers.items()}
+        if engine == abi.ENGINE_PLAIN_FP64_STRICT and _exact(case):
+            for k in ("depth", "iters", "hit", "normal", "ao", "rgb8"):
+                assert np.array_equal(g[k], o[k]), (case, k)
+            for k in ("de_evals", "formula_iterations", "march_steps", "normal_evals", "ao_evals"):
+                assert fr.stats[k] == ost[k], (case, k, fr.stats[k], ost[k])
+            continue
+        m = compare(g, o)
+        print(case, abi.ENGINE_NAMES[engine], m)
+        assert m["hit_iters_match"] >= 0.995, (engine, m)
+        assert m["depth_rel_le_1e-4"] >= 0.99, (engine, m)
+        both = g["hit"].astype(bool) & o["hit"].astype(bool)
+        assert np.mean(_rel(g["depth"][both], o["depth"][both]) <= 1e-6) >= 0.99, engine
+    for engine in (abi.ENGINE_PLAIN_MIXED, abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_FP64,
+                   abi.ENGINE_WAVEFRONT_AUTO):
+        with pytest.raises(MbrError) as e:
+            renderer.render(cam, p, engine)
+        assert e.value.status == abi.MBR_EUNSUPPORTED, engine
+
+
+@pytest.mark.parametrize("case", ["bulb_pseudo_kleinian", "box_max_axis", "hybrid_max_axis", "hybrid_pseudo_kleinian"])
+def test_other_analytic_de_functions(renderer, oracle, case):
+    """The pseudo-Kleinian and max-axis analytic DE functions
+    (compute_fractal.cpp:495-621) on every engine that takes extended scenes;
+    the strict FP64 engine equals the oracle bit for bit on Mandelbox
+    distances; on the Mandelbulb ones (whose libm functions differ by an ulp
+    here and there) it agrees within 1e-8 on >= 99.9 % of the points whose
+    orbit escapes (interior orbits are chaotic)."""
+    from tests.golden.pipeline_cases import cases
+
+    sc = cases()[case]
+    renderer.set_scene(sc)
+    rng = np.random.default_rng(12)
+    pts = rng.uniform(-2.0, 2.0, size=(4096, 3))
+    od, oit = oracle.distance(sc, pts, 1e-3, False)
+    d, it = renderer.distance(torch.from_numpy(pts), 1e-3, False, abi.ENGINE_PLAIN_FP64_STRICT)
+    d, it = d.cpu().numpy(), it.cpu().numpy()
+    if _exact(case):
+        assert np.array_equal(d, od) and np.array_equal(it, oit), case
+    else:
+        esc = oit <= sc.formula_maxiter
+        rel = _rel(d[esc], od[esc])
+        print(case, "escaping", int(esc.sum()), "rel median", np.median(rel), "max", rel.max(),
+              "iters", np.mean(it[esc] == oit[esc]))
+        assert esc.sum() >= 256
+        assert np.mean(rel <= 1e-8) >= 0.999 and np.mean(it[esc] == oit[esc]) >= 0.999, case
+    cam = configs.camera((0.0, -3.0, 0.3) if "bulb" in case or "hybrid" in case else (0.0, -6.0, 0.0), width=64,
+                         height=40)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    o, _ = oracle.render(sc, cam, p)
+    assert 0.02 < float(np.mean(o["hit"])) < 0.98, float(np.mean(o["hit"]))
+    check_engines(renderer, sc, cam, p, o, case,
+                  engines=(abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64) + FP32_ENGINES)

@@ -78,9 +78,12 @@ def test_camera_rotation_matches_oracle(oracle):
 @pytest.mark.parametrize("mutate,status", [
     (lambda s: setattr(s, "n_fractals", 0), abi.MBR_EINVAL),
     (lambda s: setattr(s, "formula_maxiter", 0), abi.MBR_EINVAL),
-    (lambda s: setattr(s.fractal[0], "formula", 5), abi.MBR_EUNSUPPORTED),
+    (lambda s: setattr(s.fractal[0], "formula", 6), abi.MBR_EUNSUPPORTED),
     (lambda s: setattr(s.fractal[0], "formula_weight", 1.5), abi.MBR_EINVAL),
-    (lambda s: setattr(s, "delta_de_function", 3), abi.MBR_EUNSUPPORTED),
+    (lambda s: setattr(s, "delta_de_function", 7), abi.MBR_EINVAL),
+    (lambda s: setattr(s, "delta_de_function", abi.DE_JOS_KLEINIAN), abi.MBR_EUNSUPPORTED),  # analytic Jos Kleinian
+    (lambda s: setattr(s, "delta_de_method", 3), abi.MBR_EINVAL),
+    (lambda s: setattr(s, "deltade_relative_delta", 0.0), abi.MBR_EINVAL),
     (lambda s: (setattr(s.fractal[0], "formula", 8), setattr(s.fractal[0], "mandelbox_folding_min_radius", 0.0)),
      abi.MBR_EINVAL),
     (lambda s: (setattr(s.fractal[0], "formula", 8), setattr(s.fractal[0], "mandelbox_folding_limit", -1.0)),

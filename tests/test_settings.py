@@ -212,13 +212,13 @@ def test_unsupported_geometry_is_named():
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nprimitive_prism_1_boolean_operator 0;\n"
                     "boolean_operators true;\n"
-                    "delta_DE_method 1;\nhybrid_fractal_enable true;\n"
+                    "delta_DE_function 4;\nhybrid_fractal_enable true;\n"
                     "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
     for key in ("primitive_prism_1_boolean_operator 0", "boolean_operators",
-                "delta_DE_method 1", "Mandelbox rotations in a hybrid"):
+                "delta_DE_function 4", "Mandelbox rotations in a hybrid"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
     s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
@@ -312,9 +312,9 @@ def test_reference_examples():
                 assert not s.ok and any(u.startswith(key + " true") for u in s.unsupported()), (path, key)
         if s.ok:
             ok += 1
-            assert formulas <= {2, 3, 4, 7, 8, 10, 11}, (path, formulas)
+            assert formulas <= {2, 3, 4, 5, 7, 8, 10, 11, 19}, (path, formulas)
             assert sc.formula_maxiter >= 1 and s.camera.width >= 5 and s.camera.height >= 5
-        elif not formulas <= {2, 3, 4, 7, 8, 10, 11}:
+        elif not formulas <= {2, 3, 4, 5, 7, 8, 10, 11, 19}:
             assert any("formula not built here" in u for u in s.unsupported()), (path, s.report)
     assert ok >= 165, ok
 
@@ -365,3 +365,24 @@ def test_malformed_text_never_crashes():
         assert s.status in (abi.MBR_OK, abi.MBR_EINVAL, abi.MBR_EUNSUPPORTED)
         assert isinstance(s.report, str)
     assert abi.MBR_EINVAL in statuses
+
+
+def test_delta_de_settings():
+    """delta_DE_method, delta_DE_function and deltade_relative_delta are read
+    into the scene (the delta DE renders on the plain FP64 engines); the Jos
+    Kleinian function is taken with the delta DE only."""
+    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\ndelta_DE_method 1;\n"
+                                  "delta_DE_function 3;\ndeltade_relative_delta 0,02;\n")
+    assert s.ok, s.report
+    assert s.scene.delta_de_method == abi.DE_METHOD_FORCE_DELTA
+    assert s.scene.delta_de_function == abi.DE_PSEUDO_KLEINIAN
+    assert s.scene.deltade_relative_delta == 0.02
+    assert "forced delta DE" in s.report
+    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\ndelta_DE_method 1;\n"
+                                  "delta_DE_function 4;\n")
+    assert s.ok, s.report
+    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\ndelta_DE_function 6;\n")
+    assert s.ok and s.scene.delta_de_function == abi.DE_MAX_AXIS, s.report
+    for bad in ("delta_DE_method 3;", "delta_DE_function 7;", "deltade_relative_delta 0;"):
+        s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\n" + bad + "\n")
+        assert s.status == abi.MBR_EINVAL, (bad, s.report)
