@@ -385,7 +385,12 @@ typedef struct mbr_render_params {
    * each step by the absolute and relative bounds below instead of step <= 3
    * (:819-834).  Defaults from src/initparameters.cpp:159-165. */
   int32_t advanced_quality;     /* default 0 */
-  int32_t reserved_aq;
+  /* "slow_shading": normals from the gradient of the orbit's iteration count
+   * over an 11 x 11 x 11 lattice of points CalcDelta apart, each weighted by
+   * 1 + N - iterations (src/shader_calculate_normals.cpp:83-106); plain
+   * engines, scenes without primitives.  Default 0 (the six-sample DE
+   * gradient). */
+  int32_t slow_shading;
   double detail_size_min;       /* default 1e-12 */
   double detail_size_max;       /* default 1 */
   double abs_min_marching_step; /* default 1e-15 */

@@ -122,7 +122,7 @@ class RenderParams(C.Structure):
         ("gamma", C.c_double), ("saturation", C.c_double), ("hdr", C.c_int32), ("row_end", C.c_int32),
         ("soft_shadow_cone", C.c_double), ("penetrating", C.c_int32), ("ao_fast", C.c_int32),
         ("ao_quality", C.c_int32), ("ao_fast_tune", C.c_double),
-        ("advanced_quality", C.c_int32), ("reserved_aq", C.c_int32), ("detail_size_min", C.c_double),
+        ("advanced_quality", C.c_int32), ("slow_shading", C.c_int32), ("detail_size_min", C.c_double),
         ("detail_size_max", C.c_double), ("abs_min_marching_step", C.c_double),
         ("abs_max_marching_step", C.c_double), ("rel_min_marching_step", C.c_double),
         ("rel_max_marching_step", C.c_double),

@@ -403,6 +403,8 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
     return set_err(ctx, MBR_EINVAL, "the adjoint differentiates a camera given by position and angles (use_angles = 1)");
   if (camera->perspective_type != MBR_PROJECTION_THREE_POINT)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the three-point projection");
+  if (params->slow_shading)
+    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint differentiates the six-sample normals (no slow shading)");
   if (params->advanced_quality || params->constant_de_threshold)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers thresholds proportional to the distance (no advanced "
                                           "quality clamps, no constant threshold)");

@@ -650,14 +650,13 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     if (parse_double(value, d)) sc->spherical_folding_inner = d; else R.bad(name, value);
   } else if (name == "spherical_folding_outer") {
     if (parse_double(value, d)) sc->spherical_folding_outer = d; else R.bad(name, value);
-  } else if (name == "stereo_enabled" || name == "slow_shading") {
-    // switches that change the image plane (stereo, render_worker.cpp:107-108,
-    // 158-161, 268) or the normals (iteration-count normals,
-    // shader_calculate_normals.cpp:82-109): refused when on
+  } else if (name == "slow_shading") {  // iteration-count normals (shader_calculate_normals.cpp:83-106)
+    if (parse_bool(value, b)) p->slow_shading = b; else R.bad(name, value);
+  } else if (name == "stereo_enabled") {
+    // a switch that changes the image plane (stereo, render_worker.cpp:107-108,
+    // 158-161, 268): refused when on
     if (!parse_bool(value, b)) R.bad(name, value);
-    else if (b) R.unsupported.push_back(name + " true (" +
-                                        (name == "stereo_enabled" ? std::string("stereo image")
-                                                                  : std::string("iteration-count normals")) + ")");
+    else if (b) R.unsupported.push_back(name + " true (stereo image)");
   } else if (name == "constant_DE_threshold") {
     if (parse_bool(value, b)) p->constant_de_threshold = b; else R.bad(name, value);
   } else if (name == "DE_thresh") {

@@ -231,7 +231,7 @@ struct DevFrame {
   const uint16_t *gamma;  // 65536-entry table (device)
   // advanced quality: threshold clamps and march step limits (render_worker.cpp:671-675, 819-834)
   int32_t adv_quality;
-  int32_t pad3;
+  int32_t slow_shading;  // normals from the iteration-count gradient (plain engines, F_EXT kernels)
   double detail_size_min, detail_size_max;
   double abs_step_min, abs_step_max, rel_step_min, rel_step_max;
 };

@@ -717,6 +717,7 @@ mbr_status build_frame(mbr_ctx *ctx, const mbr_camera &cam, const mbr_render_par
   f.saturation = float(p.saturation);
   f.hdr = p.hdr ? 1 : 0;
   f.adv_quality = p.advanced_quality ? 1 : 0;
+  f.slow_shading = p.slow_shading ? 1 : 0;
   f.detail_size_min = p.detail_size_min;
   f.detail_size_max = p.detail_size_max;
   f.abs_step_min = p.abs_min_marching_step;
@@ -1076,6 +1077,9 @@ mbr_status mbr_render(mbr_ctx *ctx, const mbr_camera *camera, const mbr_render_p
   if (fp32 && ctx->scene.has_w)
     return set_err(ctx, MBR_EUNSUPPORTED, "FP32 engines need a 3-D state: initial_waxis == 0 and no hypercomplex "
                                           "formula");
+  if (params->slow_shading && ctx->scene.n_prims > 0)
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "slow shading takes its normals from the fractal's orbit; with primitives a hit may lie on one");
   if (engine == MBR_ENGINE_PLAIN_MIXED && ctx->scene.delta_de)
     return set_err(ctx, MBR_EUNSUPPORTED,
                    "the delta DE offsets points by 1e-5 of the detail size, which FP32 points do not resolve: use a "

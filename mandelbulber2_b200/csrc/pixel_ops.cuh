@@ -312,8 +312,50 @@ __device__ MarchOut ray_marching(const DevScene &sc, const DevFrame &fr, D3 star
   return o;
 }
 
+// CalculateNormals with slowShading (shader_calculate_normals.cpp:83-106):
+// the orbit (Compute, no normal mode) at an 11 x 11 x 11 lattice of points
+// q + (i, j, k) delta, i, j, k = -1, -0.8, ... accumulated in steps of 0.2
+// as the reference's loops do, delta = CalcDelta(q) * smoothness; the normal
+// is the sum of the lattice offsets weighted by 1 + N - iterations.  Every
+// orbit counts as one distance evaluation.
+template <class T, bool W>
+__device__ __noinline__ D3 slow_normals(const DevScene &sc, const DevFrame &fr, D3 q, double thr, ThreadCount &tc) {
+  double delta = calc_delta(fr, q) * fr.smoothness;
+  if (sc.interior) delta = thr * 0.2 * fr.smoothness;
+  D3 n{0.0, 0.0, 0.0};
+  for (double px = -1.0; px <= 1.0; px += 0.2) {
+    for (double py = -1.0; py <= 1.0; py += 0.2) {
+      for (double pz = -1.0; pz <= 1.0; pz += 0.2) {
+        const D3 p3{q.x + px * delta, q.y + py * delta, q.z + pz * delta};
+        V4<T> z;
+        T r, DE;
+        bool mx;
+        const int i = compute_orbit<T, F_EXT, W>(sc, T(p3.x), T(p3.y), T(p3.z), sc.formula_maxiter, z, r, DE, mx);
+        const double pd = double(1 + sc.formula_maxiter - (i + 1));
+        n.x = n.x + px * pd;
+        n.y = n.y + py * pd;
+        n.z = n.z + pz * pd;
+        tc.de++;
+        tc.iters += unsigned(i + 1);
+      }
+    }
+  }
+  return n;
+}
+
 template <class T, int F, bool W>
 __device__ D3 normals(const DevScene &sc, const DevFrame &fr, D3 q, double thr, ThreadCount &tc) {
+  if constexpr (F == F_EXT) {
+    if (fr.slow_shading) {
+      D3 n = slow_normals<T, W>(sc, fr, q, thr, tc);
+      if (fabs(n.x) < 1e-50 && fabs(n.y) < 1e-50 && fabs(n.z) < 1e-50)
+        n = D3{1.0, 0.0, 0.0};
+      else
+        n = d3norm(n);
+      if (!(isfinite(n.x) && isfinite(n.y) && isfinite(n.z))) n = D3{1.0, 0.0, 0.0};
+      return n;
+    }
+  }
   double delta = thr * fr.smoothness;
   if (sc.interior) delta = thr * 0.2 * fr.smoothness;
   int it;

@@ -227,7 +227,7 @@ int launch_plain_t(const DevScene &sc, const DevFrame &fr, const DevOutputs &out
   const dim3 block(128);
   const dim3 grid((fr.width + 15) / 16, (fr.row1 - fr.row0 + 7) / 8);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const bool ext = scene_extended(sc);
+  const bool ext = scene_extended(sc) || fr.slow_shading;  // slow shading is compiled into F_EXT kernels only
   const int F = sc.is_hybrid ? 0 : sc.uniform_formula;
   if (sc.has_w) {
     if constexpr (sizeof(T) == 8) {

@@ -1872,6 +1872,9 @@ static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFra
                    "not resolve; it runs on the plain FP64 engines");
   if (fr.refine != MBR_REFINE_REFERENCE)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: root refinement uses the plain engines");
+  if (fr.slow_shading)
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: slow shading (iteration-count normals) uses the plain "
+                                          "engines");
   return MBR_OK;
 }
 
@@ -2503,10 +2506,10 @@ extern "C" mbr_status mbr_render_noalloc(const mbr_scene *scene, const mbr_camer
   if (st != MBR_OK) return noalloc_fail(err, err_len, st, msg);
   fr.want_normal = out->normal != nullptr;
   if (sc.is_hybrid || sc.generic || sc.iter_thresh || sc.interior || sc.has_w || fr.gi_samples > 0 ||
-      fr.refine != MBR_REFINE_REFERENCE)
+      fr.refine != MBR_REFINE_REFERENCE || fr.slow_shading)
     return noalloc_fail(err, err_len, MBR_EUNSUPPORTED,
                         "the wavefront engine renders non-hybrid Mandelbulb, Mandelbox and Menger scenes without GI, "
-                        "root refinement, iteration threshold, interior mode or initial w");
+                        "root refinement, iteration threshold, interior mode, initial w or slow shading");
   const long long total = (long long)fr.width * (fr.row1 - fr.row0);  // row-linear queue: no tile padding
   const int per = ((fr.shading_enable && fr.shadow_enable) ? 1 : 0) + ao_tasks(fr);
   const size_t need = scratch_bytes(total, per);

@@ -1478,6 +1478,30 @@ struct Renderer {
 
   // CalculateNormals fast path (shader_calculate_normals.cpp:40-125)
   D3 normals(D3 q, double thr, Counters &c, uint64_t *counter) const {
+    if (p.slow_shading) {  // shader_calculate_normals.cpp:83-106
+      double delta = calc_delta(q) * p.smoothness;
+      if (seq.interior) delta = thr * 0.2 * p.smoothness;
+      D3 n{0.0, 0.0, 0.0};
+      for (double px = -1.0; px <= 1.0; px += 0.2)
+        for (double py = -1.0; py <= 1.0; py += 0.2)
+          for (double pz = -1.0; pz <= 1.0; pz += 0.2) {
+            const D3 p3{q.x + px * delta, q.y + py * delta, q.z + pz * delta};
+            const FractalOut<double> fo = compute<double>(seq, slots.data(), p3.x, p3.y, p3.z, 1, -1);
+            const double pd = double(1 + seq.formula_maxiter - fo.iters);
+            n.x = n.x + px * pd;
+            n.y = n.y + py * pd;
+            n.z = n.z + pz * pd;
+            c.de++;
+            c.iters += fo.iters;
+            *counter += 1;
+          }
+      if (fabs(n.x) < 1e-50 && fabs(n.y) < 1e-50 && fabs(n.z) < 1e-50)
+        n = D3{1.0, 0.0, 0.0};
+      else
+        n = normalize(n);
+      if (!(isfinite(n.x) && isfinite(n.y) && isfinite(n.z))) n = D3{1.0, 0.0, 0.0};
+      return n;
+    }
     double delta = thr * p.smoothness;
     if (seq.interior) delta = thr * 0.2 * p.smoothness;
     const uint64_t before = c.de;

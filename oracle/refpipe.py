@@ -243,6 +243,7 @@ class RefPipeline:
             self.set("constant_DE_threshold", p.constant_de_threshold, KIND_BOOL)
             self.set("DE_thresh", p.de_thresh, KIND_DOUBLE)
             self.set("advanced_quality", p.advanced_quality, KIND_BOOL)
+            self.set("slow_shading", p.slow_shading, KIND_BOOL)
             self.set("detail_size_min", p.detail_size_min, KIND_DOUBLE)
             self.set("detail_size_max", p.detail_size_max, KIND_DOUBLE)
             self.set("abs_min_marching_step", p.abs_min_marching_step, KIND_DOUBLE)

@@ -279,6 +279,10 @@ def render_cases():
     s = abi.scene_defaults(abi.FORMULA_QUATERNION)
     s.formula_maxiter = 30
     out.append(("quaternion", s, configs.camera((0.3, -2.4, 0.8), width=32, height=24), params()))
+    out.append(("bulb_slow_shading", configs.mandelbulb_scene(8.0, 20), configs.camera((0.4, -2.2, 0.9), width=24,
+                height=16), params(slow_shading=1)))
+    out.append(("box_slow_shading", configs.mandelbox_scene(-1.5, 0.5, 20),
+                configs.camera((0.0, -6.0, 0.0), width=24, height=16), params(slow_shading=1)))
     sc, cam, p = configs.mandelbulb_512(32, 24, binary_steps=30)
     sc.delta_de_method = abi.DE_METHOD_FORCE_DELTA
     sc.deltade_relative_delta = 0.02

@@ -386,3 +386,40 @@ def test_other_analytic_de_functions(renderer, oracle, case):
     assert 0.02 < float(np.mean(o["hit"])) < 0.98, float(np.mean(o["hit"]))
     check_engines(renderer, sc, cam, p, o, case,
                   engines=(abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64) + FP32_ENGINES)
+
+
+@pytest.mark.parametrize("case", ["bulb_slow_shading", "box_slow_shading"])
+def test_slow_shading(renderer, oracle, case):
+    """Iteration-count normals (shader_calculate_normals.cpp:83-106): the
+    gradient of 1 + N - iterations over an 11^3 lattice of orbits around the
+    hit.  The oracle equals the reference's render worker on these frames
+    (tests/golden/render_kat.json); the strict FP64 engine equals the oracle
+    bit for bit on the Mandelbox, the other plain engines are held to their
+    bars, and the wavefront engines refuse slow shading."""
+    from tests.golden.pipeline_cases import render_cases
+
+    _, sc, cam, p = [c for c in render_cases() if c[0] == case][0]
+    cam.width, cam.height = 64, 40
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.98
+    renderer.set_scene(sc)
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED):
+        fr = renderer.render(cam, p, engine, outputs=NAMES)
+        g = {k: v.cpu().numpy() for k, v in fr.buffers.items()}
+        m = compare(g, o)
+        print(case, abi.ENGINE_NAMES[engine], m)
+        if engine == abi.ENGINE_PLAIN_FP64_STRICT and _exact(case):
+            for k in NAMES:
+                assert np.array_equal(g[k], o[k]), (case, k)
+            assert fr.stats["normal_evals"] == ost["normal_evals"]
+        elif engine != abi.ENGINE_PLAIN_MIXED:
+            assert m["hit_iters_match"] >= 0.999 and m["depth_rel_le_1e-9"] >= 0.999, m
+            assert m["normal_deg_p99"] <= 1e-3, m
+        else:
+            assert m["hit_mismatch"] <= 0.005 and m["depth_rel_median"] <= 1e-4, m
+            # FP32 orbits near the bailout shift some lattice points' iteration counts
+            assert m["normal_deg_median"] <= 1.0, m
+    for engine in (abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_FP64, abi.ENGINE_WAVEFRONT_AUTO):
+        with pytest.raises(MbrError) as e:
+            renderer.render(cam, p, engine)
+        assert e.value.status == abi.MBR_EUNSUPPORTED
