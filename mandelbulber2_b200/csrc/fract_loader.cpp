@@ -842,6 +842,12 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     if (R.formula[i] != MBR_FORMULA_NONE) last = i + 1;
   }
   scene->n_fractals = R.hybrid ? (last > 0 ? last : 1) : 1;
+  // the scene holds one IFS block and one Mandelbox-rotation block
+  int n_ifs = 0, n_box = 0;
+  for (int i = 0; i < scene->n_fractals && (R.hybrid || i == 0); i++) {
+    if (R.formula[i] == MBR_FORMULA_KALEIDOSCOPIC_IFS) n_ifs++;
+    if (R.formula[i] == MBR_FORMULA_MANDELBOX) n_box++;
+  }
   for (int i = 0; i < scene->n_fractals; i++) {
     const int f = R.formula[i];
     if (!R.hybrid && i > 0) break;
@@ -853,12 +859,13 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
                               " (formula not built here: 2 Mandelbulb, 3 Mandelbulb power 2, 4 hypercomplex, "
                               "5 quaternion, 7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie, "
                               "19 aexion are)");
-    if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && R.hybrid)
-      R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in a hybrid)");
+    if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && n_ifs > 1)
+      R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in more than one slot)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
-    if (f == MBR_FORMULA_MANDELBOX && R.hybrid &&
+    if (f == MBR_FORMULA_MANDELBOX && n_box > 1 &&
         (scene->fractal[i].mandelbox_rotations_enabled || scene->fractal[i].mandelbox_main_rotation_enabled))
-      R.unsupported.push_back("fractal_" + std::to_string(i + 1) + " rotations (Mandelbox rotations in a hybrid)");
+      R.unsupported.push_back("fractal_" + std::to_string(i + 1) +
+                              " rotations (Mandelbox rotations with more than one Mandelbox slot)");
   }
   if (!R.hybrid && R.formula[0] == MBR_FORMULA_NONE) R.unsupported.push_back("formula_1 0 (no fractal)");
   // enabled primitives join the fractal by union (MigrateToObjectsTree, settings.cpp:2866-2940)

@@ -255,13 +255,20 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     return set_err(ctx, MBR_EINVAL, "delta_de_method must be in [0, 2], got %d", sc.delta_de_method);
   if (!(sc.deltade_relative_delta > 0.0) || !std::isfinite(sc.deltade_relative_delta))
     return set_err(ctx, MBR_EINVAL, "deltade_relative_delta must be finite and > 0");
-  // Mandelbox rotations: slot 0 of a single-fractal scene
+  // Mandelbox rotations and the kaleidoscopic IFS: the scene holds one block
+  // of each, for its single Mandelbox slot and its single IFS slot
+  int n_box = 0, n_ifs = 0;
+  for (int i = 0; i < (hybrid ? n : 1); i++) {
+    if (sc.fractal[i].formula == MBR_FORMULA_MANDELBOX) n_box++;
+    if (sc.fractal[i].formula == MBR_FORMULA_KALEIDOSCOPIC_IFS) n_ifs++;
+  }
   for (int i = 0; i < (hybrid ? n : 1); i++) {
     const mbr_fractal &f = sc.fractal[i];
     const bool rot = f.mandelbox_rotations_enabled || f.mandelbox_main_rotation_enabled;
     if (!rot || f.formula != MBR_FORMULA_MANDELBOX) continue;
-    if (hybrid)
-      return set_err(ctx, MBR_EUNSUPPORTED, "Mandelbox rotations are supported in single-fractal scenes only");
+    if (n_box > 1)
+      return set_err(ctx, MBR_EUNSUPPORTED,
+                     "Mandelbox rotations are supported when the sequence has one Mandelbox slot");
     bool ok = finite3(f.mandelbox_rotation_main);
     for (int a = 0; a < 3; a++) ok = ok && finite3(f.mandelbox_rotation_neg[a]) && finite3(f.mandelbox_rotation_pos[a]);
     if (!ok) return set_err(ctx, MBR_EINVAL, "non-finite Mandelbox rotation angle");
@@ -278,11 +285,11 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     mandelbox_rotation(f.mandelbox_rotation_main, r.mm, &zero);
     r.main_zero = zero ? 1 : 0;
   }
-  // kaleidoscopic IFS: slot 0 of a single-fractal scene
   for (int i = 0; i < (hybrid ? n : 1); i++) {
     const mbr_fractal &f = sc.fractal[i];
     if (f.formula != MBR_FORMULA_KALEIDOSCOPIC_IFS) continue;
-    if (hybrid) return set_err(ctx, MBR_EUNSUPPORTED, "the kaleidoscopic IFS is supported in single-fractal scenes only");
+    if (n_ifs > 1)
+      return set_err(ctx, MBR_EUNSUPPORTED, "the kaleidoscopic IFS is supported in one slot of a sequence");
     IfsBlock &b = d.ifs;
     b.abs_x = f.ifs_abs_x ? 1 : 0;
     b.abs_y = f.ifs_abs_y ? 1 : 0;

@@ -174,6 +174,29 @@ def cases():
     s = configs.hybrid_scene()
     s.delta_de_function = abi.DE_PSEUDO_KLEINIAN
     out["hybrid_pseudo_kleinian"] = s
+    # the IFS and a rotated Mandelbox inside hybrids
+    s = abi.scene_defaults(abi.FORMULA_MANDELBOX)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 3
+    s.formula_maxiter = 30
+    s.fractal[0].mandelbox_scale = -1.7
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_KALEIDOSCOPIC_IFS)
+    f = s.fractal[1]
+    f.ifs_menger_sponge_mode = 1
+    f.ifs_scale = 3.0
+    f.ifs_rotation_enabled = 1
+    f.ifs_rotation[:] = [8.0, 0.0, 4.0]
+    abi.fractal_defaults(s.fractal[2], abi.FORMULA_MANDELBULB_POWER2)
+    out["hybrid_box_ifs_pow2"] = s
+    s = configs.hybrid_scene()
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBOX)
+    s.fractal[1].formula_iterations = 3
+    s.fractal[1].mandelbox_scale = -1.6
+    s.fractal[1].mandelbox_rotations_enabled = 1
+    s.fractal[1].mandelbox_rotation_neg[0][:] = [12.0, 0.0, 3.0]
+    s.fractal[1].mandelbox_main_rotation_enabled = 1
+    s.fractal[1].mandelbox_rotation_main[:] = [5.0, 9.0, -4.0]
+    out["hybrid_bulb_rotated_box"] = s
     # quaternion (5) and aexion (19)
     s = abi.scene_defaults(abi.FORMULA_QUATERNION)
     s.formula_maxiter = 40

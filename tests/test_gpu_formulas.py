@@ -170,3 +170,26 @@ def test_aexion(renderer, oracle, case):
         with pytest.raises(MbrError) as e:
             renderer.render(cam, p, engine)
         assert e.value.status == abi.MBR_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("case", ["hybrid_box_ifs_pow2", "hybrid_bulb_rotated_box"])
+def test_ifs_and_rotated_mandelbox_in_hybrids(renderer, oracle, case):
+    """A hybrid with its one kaleidoscopic IFS slot, and one with its one
+    (rotated) Mandelbox slot: the scene's IFS and rotation blocks belong to
+    that slot.  Strict FP64 is bit-exact where the sequence has no
+    transcendental function; every engine that takes hybrids is held to its
+    bar."""
+    from tests.golden.pipeline_cases import cases
+
+    sc = cases()[case]
+    cam = configs.camera((0.4, -3.0, 0.9), width=96, height=64)
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    assert 0.05 < float(np.mean(o["hit"])) < 0.95, float(np.mean(o["hit"]))
+    engines = [abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED, abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_AUTO]
+    if "bulb_rotated" not in case:
+        engines.insert(0, abi.ENGINE_PLAIN_FP64_STRICT)
+    for engine in engines:
+        check(renderer, sc, cam, p, o, ost, engine, case)

@@ -212,13 +212,13 @@ def test_unsupported_geometry_is_named():
     assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nprimitive_prism_1_boolean_operator 0;\n"
                     "boolean_operators true;\n"
-                    "delta_DE_function 4;\nhybrid_fractal_enable true;\n"
+                    "delta_DE_function 4;\nhybrid_fractal_enable true;\nformula_2 8;\n"
                     "[fractal_1]\nmandelbox_rotations_enabled true;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
     u = " | ".join(s.unsupported())
     for key in ("primitive_prism_1_boolean_operator 0", "boolean_operators",
-                "delta_DE_function 4", "Mandelbox rotations in a hybrid"):
+                "delta_DE_function 4", "Mandelbox rotations with more than one Mandelbox slot"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
     s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
