@@ -40,6 +40,8 @@ extern "C" {
 #define MBR_SEQUENCE_LENGTH 1250
 /* primitives joined to the fractal by union (at most this many) */
 #define MBR_MAX_PRIMITIVES 8
+/* nodes of an explicit objects tree */
+#define MBR_MAX_NODES 16
 
 typedef enum mbr_status {
   MBR_OK = 0,
@@ -235,6 +237,44 @@ typedef struct mbr_primitive {
   double triangle_height;     /* prism ("trangle_height"): default 1 */
 } mbr_primitive;
 
+/* enumNodeType (src/object_node_type.h:11-19). */
+typedef enum mbr_node_type {
+  MBR_NODE_FRACTAL = 1,      /* one formula slot, iterated alone */
+  MBR_NODE_PRIMITIVE = 2,    /* one primitive */
+  MBR_NODE_BOOLEAN_ADD = 11, /* union of the children (smooth union where a child asks for it) */
+  MBR_NODE_BOOLEAN_MUL = 12, /* intersection of the children */
+  MBR_NODE_BOOLEAN_SUB = 13  /* the first child minus the others */
+} mbr_node_type;
+
+/* One node of an explicit objects tree (cObjectsTree::sNodeData,
+ * src/objects_tree.h:24-48; the node_NNNN_* parameters of
+ * src/initparameters.cpp:2102-2125).  Nodes are listed in the order
+ * CalculateDistanceFromObjectsTree walks them (src/calculate_distance.cpp:
+ * 225-516): preorder, a boolean node's children following it one level
+ * deeper.  The node's transform (position, rotation in degrees, uniform
+ * scale) composes with its ancestors' (objects_tree.cpp:285-330); a leaf
+ * repeats in its own frame.  A PRIMITIVE node's local transform is the
+ * mbr_primitive's own position, rotation, scale and repeat. */
+typedef struct mbr_node {
+  int32_t type;                 /* mbr_node_type */
+  int32_t level;                /* 0 for the top nodes */
+  int32_t index;                /* FRACTAL: the slot of mbr_scene.fractal; PRIMITIVE: of mbr_scene.primitive */
+  int32_t enabled;              /* default 1; a disabled node takes its subtree with it */
+  double position[3];
+  double rotation[3];           /* degrees */
+  double scale;                 /* default 1 */
+  double repeat[3];             /* default 0: no tiling */
+  double detail_level_multiplier; /* default 1 */
+  double smooth_combine_distance; /* default 0.1 */
+  int32_t smooth_combine;       /* smooth union with what precedes it in a union, default 0 */
+  int32_t formula_maxiter;      /* FRACTAL: default 250 */
+  int32_t julia_mode;           /* FRACTAL: default 0 */
+  int32_t reserved;
+  double julia_c[3];            /* FRACTAL */
+  double fractal_constant_factor[3]; /* FRACTAL: default (1,1,1) */
+  double initial_waxis;         /* FRACTAL: default 0 */
+} mbr_node;
+
 /* The fractal part of a scene: one fractal (or hybrid) object node with the
  * general fractal parameters of src/initparameters.cpp:128-157 and the node
  * parameters of :2102-2125.  The objects tree holds exactly this one node at
@@ -293,6 +333,16 @@ typedef struct mbr_scene {
   int32_t delta_de_method;
   int32_t reserved_delta;
   double deltade_relative_delta; /* default 0.01 (src/initparameters.cpp:166) */
+  /* An explicit objects tree: with n_nodes > 0 the nodes replace the default
+   * tree (the fractal or hybrid node and the primitives joined by union).
+   * FRACTAL nodes iterate their slot alone, with the node's iteration limit,
+   * julia and constant-factor settings (hybrid_fractal_enable must be 0);
+   * the general settings above (bailout, DE method and function, minN,
+   * interior and iteration-threshold modes, limits, global folds) hold for
+   * every node.  Explicit trees run on the plain engines. */
+  int32_t n_nodes;              /* 0..MBR_MAX_NODES, default 0 */
+  int32_t reserved_nodes;
+  mbr_node node[MBR_MAX_NODES];
 } mbr_scene;
 
 /* params::enumPerspectiveType (src/projection_3d.hpp:44-50): the view

@@ -15,6 +15,9 @@ LIB_PATH = os.path.join(HERE, "libmbr.so")
 MBR_MAX_FRACTALS = 9
 MBR_SEQUENCE_LENGTH = 1250
 MBR_MAX_PRIMITIVES = 8
+MBR_MAX_NODES = 16
+# mbr_node_type
+NODE_FRACTAL, NODE_PRIMITIVE, NODE_BOOLEAN_ADD, NODE_BOOLEAN_MUL, NODE_BOOLEAN_SUB = 1, 2, 11, 12, 13
 
 # mbr_status
 MBR_OK, MBR_EINVAL, MBR_ECUDA, MBR_ETIMEOUT, MBR_ENOMEM, MBR_EUNSUPPORTED = range(6)
@@ -83,6 +86,28 @@ class Primitive(C.Structure):
     ]
 
 
+class Node(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("level", C.c_int32), ("index", C.c_int32), ("enabled", C.c_int32),
+        ("position", D3), ("rotation", D3), ("scale", C.c_double), ("repeat", D3),
+        ("detail_level_multiplier", C.c_double), ("smooth_combine_distance", C.c_double),
+        ("smooth_combine", C.c_int32), ("formula_maxiter", C.c_int32), ("julia_mode", C.c_int32),
+        ("reserved", C.c_int32), ("julia_c", D3), ("fractal_constant_factor", D3), ("initial_waxis", C.c_double),
+    ]
+
+
+def node_defaults(node_type: int, index: int = 0, level: int = 0) -> Node:
+    """A node with the reference's node defaults (initparameters.cpp:2102-2125)."""
+    n = Node()
+    n.type, n.index, n.level, n.enabled = node_type, index, level, 1
+    n.scale = 1.0
+    n.detail_level_multiplier = 1.0
+    n.smooth_combine_distance = 0.1
+    n.formula_maxiter = 250
+    n.fractal_constant_factor[:] = [1.0, 1.0, 1.0]
+    return n
+
+
 class Scene(C.Structure):
     _fields_ = [
         ("n_fractals", C.c_int32), ("hybrid_fractal_enable", C.c_int32), ("formula_maxiter", C.c_int32),
@@ -97,6 +122,7 @@ class Scene(C.Structure):
         ("box_folding_value", C.c_double), ("spherical_folding_inner", C.c_double),
         ("spherical_folding_outer", C.c_double),
         ("delta_de_method", C.c_int32), ("reserved_delta", C.c_int32), ("deltade_relative_delta", C.c_double),
+        ("n_nodes", C.c_int32), ("reserved_nodes", C.c_int32), ("node", Node * MBR_MAX_NODES),
     ]
 
 

@@ -410,8 +410,9 @@ extern "C" mbr_status mbr_adjoint(mbr_ctx *ctx, const mbr_camera *camera, const 
                                           "quality clamps, no constant threshold)");
   if (sc->mbrot.folds || sc->mbrot.main)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the Mandelbox without rotations");
-  if (sc->n_prims > 0 || sc->limits || sc->gbox || sc->gsph)
-    return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers scenes without primitives, limit box or global folds");
+  if (sc->n_prims > 0 || sc->n_nodes > 0 || sc->limits || sc->gbox || sc->gsph)
+    return set_err(ctx, MBR_EUNSUPPORTED,
+                   "the adjoint covers scenes without primitives, objects tree, limit box or global folds");
   if (sc->delta_de || sc->de_final > DEF_IFS)
     return set_err(ctx, MBR_EUNSUPPORTED, "the adjoint covers the analytic linear and logarithmic DE functions");
   if (sc->is_hybrid || sc->has_w || sc->iter_thresh || sc->interior ||

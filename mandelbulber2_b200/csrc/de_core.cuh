@@ -403,6 +403,16 @@ template <class T>
 __device__ __forceinline__ T juliac_of(const DevScene &sc, int k) {
   return T(sc.julia_c[k] * sc.cmul[k]);
 }
+// the same for a fractal node of an explicit tree
+template <class T>
+__device__ __forceinline__ T node_cmul(const DevNode &nd, int k) {
+  if constexpr (sizeof(T) == 8) return T(nd.cmul[k]);
+  else return T(nd.fcmul[k]);
+}
+template <class T>
+__device__ __forceinline__ T node_juliac(const DevNode &nd, int k) {
+  return T(nd.julia_c[k] * nd.cmul[k]);
+}
 
 // std::max(a, b) of the reference: b when a < b, else a.
 template <class T>
@@ -599,10 +609,10 @@ __device__ __forceinline__ void global_folds(const DevScene &sc, V4<T> &z, T &r,
 // (px, py, pz), at most maxN iterations.  Returns the loop index at exit (the
 // orbit's iteration count is one more) and leaves the final z, r = |z| (4-D),
 // the derivative DE and the orbit's maxiter flag.
-template <class T, int F, bool W>
+template <class T, int F, bool W, bool TREE = false>
 __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T pz, int maxN, V4<T> &z, T &r, T &DE,
-                                             bool &maxiter) {
-  z = V4<T>{px, py, pz, W ? T(sc.w0) : T(0.0)};
+                                             bool &maxiter, const DevNode *nd = nullptr) {
+  z = V4<T>{px, py, pz, W ? T(TREE ? nd->w0 : sc.w0) : T(0.0)};
   V4<T> c = z;  // aux.const_c
   r = len4<T, W>(z);
   DE = T(1.0);
@@ -611,7 +621,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
   int i;
   for (i = 0; i < maxN; i++) {
     lastZ = z;
-    const int k = (F > 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0]));
+    const int k = TREE ? nd->slot : ((F > 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0])));
     const DevSlot &s = sc.slot[k];
     if (F == F_EXT) global_folds<T, W>(sc, z, r, DE);
     const V4<T> tempZ = z;
@@ -624,18 +634,18 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
       formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c);
     }
     if (s.add_c) {
-      if (sc.julia) {
-        z.x = z.x + juliac_of<T>(sc, 0);
-        z.y = z.y + juliac_of<T>(sc, 1);
-        z.z = z.z + juliac_of<T>(sc, 2);
+      if (TREE ? nd->julia : sc.julia) {
+        z.x = z.x + (TREE ? node_juliac<T>(*nd, 0) : juliac_of<T>(sc, 0));
+        z.y = z.y + (TREE ? node_juliac<T>(*nd, 1) : juliac_of<T>(sc, 1));
+        z.z = z.z + (TREE ? node_juliac<T>(*nd, 2) : juliac_of<T>(sc, 2));
       } else {
-        z.x = z.x + c.x * cmul_of<T>(sc, 0);
-        z.y = z.y + c.y * cmul_of<T>(sc, 1);
-        z.z = z.z + c.z * cmul_of<T>(sc, 2);
+        z.x = z.x + c.x * (TREE ? node_cmul<T>(*nd, 0) : cmul_of<T>(sc, 0));
+        z.y = z.y + c.y * (TREE ? node_cmul<T>(*nd, 1) : cmul_of<T>(sc, 1));
+        z.z = z.z + c.z * (TREE ? node_cmul<T>(*nd, 2) : cmul_of<T>(sc, 2));
         if (W) z.w = z.w + c.w;
       }
     }
-    if (F <= 0 && sc.is_hybrid) {
+    if (!TREE && F <= 0 && sc.is_hybrid) {
       const double kw = s.d[P_WEIGHT];
       if (kw < 1.0) {
         z = smooth4<T, W>(tempZ, z, kw);
@@ -661,10 +671,10 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
 // The specialised iterations carry linear, logarithmic and IFS; the extended
 // one every DevDeFinal code.
 template <class T, int F, bool W>
-__device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE) {
+__device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE, int de_final = -1) {
   if (!(DE > T(0.0))) return r;
   if (F == F_EXT) {
-    switch (sc.de_final) {
+    switch (de_final >= 0 ? de_final : sc.de_final) {
       case DEF_LINEAR_OFFSET: return (r - (sizeof(T) == 8 ? T(sc.linear_de_offset) : T(sc.flinear_de_offset))) / DE;
       case DEF_LOG: return (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
       case DEF_LINEAR: return r / DE;
@@ -696,9 +706,11 @@ __device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, 
 // x, y and z, each capped at the first orbit's iteration count; the distance
 // divides the radius by the gradient of |z| through the sequence's DE
 // function.  FP64 only: the offsets are 1e-5 of the detail size.
-template <class T, bool W>
+template <class T, bool W, bool TREE = false>
 __device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
-                                         int *iters_out, int *total_out) {
+                                         int *iters_out, int *total_out, const DevNode *nd = nullptr) {
+  const int maxN = TREE ? nd->maxN : sc.formula_maxiter;
+  const int delta_fn = TREE ? nd->delta_fn : sc.delta_fn;
   const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
   const T plen = m_sqrt(px * px + py * py + pz * pz);  // fractIn.point.Length()
   const T deltaDE = smax(T(plen * T(1e-14)), T(T(sc.delta_factor) * detail));
@@ -708,8 +720,8 @@ __device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T
   // Compute's delta-mode ending for the Jos Kleinian function
   // (compute_fractal.cpp:627-638): z.y = min(z.y, foldingValue - z.y) with
   // the default transf_spheres_enabled (true) and transf_folding_value (2)
-  const bool jos = sc.delta_fn == 4;
-  const int i1 = compute_orbit<T, F_EXT, W>(sc, px, py, pz, sc.formula_maxiter * mult, z, r4, DE, mx);
+  const bool jos = delta_fn == 4;
+  const int i1 = compute_orbit<T, F_EXT, W, TREE>(sc, px, py, pz, maxN * mult, z, r4, DE, mx, nd);
   if (jos && T(2.0) - z.y < z.y) z.y = T(2.0) - z.y;
   const T r = m_sqrt(z.x * z.x + z.y * z.y + z.z * z.z);  // fractOut.z.Length(): the 3-D part
   const T zfx = z.x, zfy = z.y, zfz = z.z;
@@ -725,9 +737,10 @@ __device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T
   T drv[3];
   int last_iters = iters1;
   for (int a = 0; a < 3; a++) {  // x, y, z offsets, each with forcedMaxiter = the first orbit's count
-    const int i = compute_orbit<T, F_EXT, W>(sc, a == 0 ? T(px + deltaDE) : T(px + T(0.0)),
-                                             a == 1 ? T(py + deltaDE) : T(py + T(0.0)),
-                                             a == 2 ? T(pz + deltaDE) : T(pz + T(0.0)), iters1, z, r4, DE, mx);
+    const int i = compute_orbit<T, F_EXT, W, TREE>(sc, a == 0 ? T(px + deltaDE) : T(px + T(0.0)),
+                                                   a == 1 ? T(py + deltaDE) : T(py + T(0.0)),
+                                                   a == 2 ? T(pz + deltaDE) : T(pz + T(0.0)), iters1, z, r4, DE, mx,
+                                                   nd);
     if (jos && T(2.0) - z.y < z.y) z.y = T(2.0) - z.y;
     const T r2 = m_sqrt(z.x * z.x + z.y * z.y + z.z * z.z);
     drv[a] = m_abs(T(r2 - r)) / deltaDE;
@@ -737,7 +750,7 @@ __device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T
   const T dr = m_sqrt(drv[0] * drv[0] + drv[1] * drv[1] + drv[2] * drv[2]);
   T distance = T(0.0);
   if (dr > T(0.0)) {
-    switch (sc.delta_fn) {
+    switch (delta_fn) {
       case 1: distance = T(0.5) * r / dr; break;
       case 2: distance = T(0.5) * r * m_log(r) / dr; break;
       case 3: {  // the last offset orbit's z (:686-690)
@@ -786,8 +799,149 @@ __device__ __noinline__ T delta_distance(const DevScene &sc, T px, T py, T pz, T
   return distance;
 }
 
-// CalculateDistance for one point: the limit box, CalculateDistanceSimple
-// (analytic or delta branch) and the union with the primitives.
+// CalculateDistanceSimple (calculate_distance.cpp:533-760): the delta
+// branch (FP64) or the analytic branch, with its post-processing.  TREE: for
+// the fractal node nd of an explicit tree (its slot, iteration limit, julia
+// and constant factor, DE function).
+template <class T, int F, bool W, bool TREE = false>
+__device__ __forceinline__ T calc_distance_simple(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
+                                                  int *iters_out, int *total_out, const DevNode *nd = nullptr) {
+  if constexpr (F == F_EXT && sizeof(T) == 8) {
+    if (TREE ? nd->delta_de : sc.delta_de)
+      return delta_distance<T, W, TREE>(sc, px, py, pz, detail, normal_mode, iters_out, total_out, nd);
+  }
+  const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
+  V4<T> z;
+  T r, DE;
+  bool maxiter;
+  const int i = compute_orbit<T, F, W, TREE>(sc, px, py, pz, (TREE ? nd->maxN : sc.formula_maxiter) * mult, z, r,
+                                             DE, maxiter, nd);
+  T distance = final_distance<T, F, W>(sc, z, r, DE, TREE ? nd->de_final : -1);
+  const int iters = i + 1;
+  *iters_out = iters;
+  if (total_out) *total_out = iters;
+  // CalculateDistanceSimple post-processing (calculate_distance.cpp:561-605)
+  bool mx = maxiter;
+  if (!sc.iter_thresh) mx = false;
+  if (normal_mode) mx = false;
+  if (mx) distance = T(0.0);
+  if (iters < sc.min_n && distance < detail) distance = detail;
+  if (sc.interior) {
+    if (!normal_mode) {
+      if (distance < T(0.5) * detail || maxiter) distance = detail;
+    } else {
+      if (distance < T(0.9) * detail) distance = detail - distance;
+    }
+  }
+  if (sc.iter_thresh && !normal_mode && !maxiter) {
+    if (distance < detail) distance = detail * T(1.01);
+  }
+  if (distance < T(0.0)) distance = T(0.0);
+  if (distance > T(10.0)) distance = T(10.0);
+  return distance;
+}
+
+// mergeChildIntoParent (calculate_distance.cpp:103-204) on the distance and
+// the smooth-combine settings: intersection takes the larger distance,
+// subtraction pushes the first operand's surface 1.5 detail sizes out where a
+// later operand is within one detail size, union takes the smaller or, for a
+// child that asks for it, the smooth union (opSmoothUnion, math_utilities.h:99-103).
+template <class T>
+struct TreeFrame {
+  T dist, detail, smooth_dist;
+  int type;
+  bool smooth;
+};
+template <class T>
+__device__ __forceinline__ void tree_merge(T cd, bool csmooth, T csdist, TreeFrame<T> &p) {
+  if (p.type == MBR_NODE_BOOLEAN_MUL) {
+    if (cd > p.dist) p.dist = cd;
+  } else if (p.type == MBR_NODE_BOOLEAN_SUB) {
+    if (p.dist >= T(1e19)) {
+      p.dist = cd;
+    } else if (p.detail > T(0.0) && cd < p.detail) {
+      const T limitDist = p.detail * T(1.5);
+      if (cd < limitDist) {
+        p.dist = limitDist;
+      } else {
+        const T adjusted = smax(T(limitDist - cd), p.dist);
+        p.dist = (adjusted < T(0.0)) ? T(0.0) : adjusted;
+      }
+    }
+  } else {
+    if (csmooth && p.dist < T(1e19)) {
+      const T k = csdist, d1 = cd, d2 = p.dist;
+      const T t = T(0.5) + T(0.5) * (d2 - d1) / k;
+      const T h = (t < T(0.0)) ? T(0.0) : ((t > T(1.0)) ? T(1.0) : t);
+      p.dist = (d2 * (T(1.0) - h) + d1 * h) - k * h * (T(1.0) - h);
+    } else if (cd < p.dist) {
+      p.dist = cd;
+    }
+  }
+}
+
+// CalculateDistanceFromObjectsTree (calculate_distance.cpp:225-516) over the
+// scene's explicit tree: each node's world-to-local transform, repeat in its
+// own frame, detail size / (absScale * detail multiplier); boolean groups on
+// a stack of at most 9 levels; the leaves' iterations summed.
+template <class T, bool W>
+__device__ __noinline__ T tree_distance(const DevScene &sc, T px, T py, T pz, T detail, bool normal_mode,
+                                        int *iters_out, int *total_out) {
+  TreeFrame<T> st[10];
+  st[0] = TreeFrame<T>{T(1e20), detail, T(0.1), MBR_NODE_BOOLEAN_ADD, false};
+  int sl = 0, total_iters = 0, total_all = 0;
+  for (int n = 0; n < sc.n_nodes; n++) {
+    const DevNode &nd = sc.node[n];
+    const double *m = nd.w2l;
+    T lx = T(m[0]) * px + T(m[1]) * py + T(m[2]) * pz + T(m[3]);
+    T ly = T(m[4]) * px + T(m[5]) * py + T(m[6]) * pz + T(m[7]);
+    T lz = T(m[8]) * px + T(m[9]) * py + T(m[10]) * pz + T(m[11]);
+    if (nd.has_repeat) {
+      lx = repeat_mod(lx, T(nd.repeat[0]));
+      ly = repeat_mod(ly, T(nd.repeat[1]));
+      lz = repeat_mod(lz, T(nd.repeat[2]));
+    }
+    T nodeDetail;
+    if (nd.abs_scale > 0.0 && nd.detail_mult > 0.0) nodeDetail = detail / T(nd.abs_scale) / T(nd.detail_mult);
+    else if (nd.abs_scale > 0.0) nodeDetail = detail / T(nd.abs_scale);
+    else if (nd.detail_mult > 0.0) nodeDetail = detail / T(nd.detail_mult);
+    else nodeDetail = detail;
+    while (sl > nd.level) {
+      const TreeFrame<T> child = st[sl];
+      sl--;
+      tree_merge<T>(child.dist, child.smooth, child.smooth_dist, st[sl]);
+    }
+    T distance;
+    int leaf_iters = 0, leaf_total = 0;
+    if (nd.type == MBR_NODE_FRACTAL) {
+      distance = calc_distance_simple<T, F_EXT, W, true>(sc, lx, ly, lz, nodeDetail, normal_mode, &leaf_iters,
+                                                         &leaf_total, &nd);
+      distance = distance * T(nd.abs_scale);
+    } else if (nd.type == MBR_NODE_PRIMITIVE) {
+      distance = prim_distance<T>(sc.prim[nd.prim], px, py, pz);
+    } else {
+      sl++;
+      st[sl] = TreeFrame<T>{nd.type == MBR_NODE_BOOLEAN_MUL ? T(-1e20) : T(1e20), nodeDetail, T(nd.smooth_dist),
+                            nd.type, nd.smooth != 0};
+      continue;
+    }
+    tree_merge<T>(distance, nd.smooth != 0, T(nd.smooth_dist), st[sl]);
+    total_iters += leaf_iters;
+    total_all += leaf_total;
+  }
+  while (sl > 0) {
+    const TreeFrame<T> child = st[sl];
+    sl--;
+    tree_merge<T>(child.dist, child.smooth, child.smooth_dist, st[sl]);
+  }
+  *iters_out = total_iters;
+  if (total_out) *total_out = total_all;
+  return st[0].dist;
+}
+
+// CalculateDistance for one point: the limit box, then the objects tree -
+// the scene's explicit tree (F_EXT), or the default one: CalculateDistanceSimple
+// of the fractal or hybrid node and the union with the primitives.
 // F: fixed formula id (non-hybrid scene), 0 (generic: the sequence table over
 // the three specialised formulas) or F_EXT (generic with every formula and
 // the Mandelbox rotations).  W: 4-D state.  *iters_out: the iteration count
@@ -803,43 +957,10 @@ __device__ __forceinline__ T calc_distance(const DevScene &sc, T px, T py, T pz,
       return lbd;
     }
   }
-  T distance;
-  bool simple = true;
-  if constexpr (F == F_EXT && sizeof(T) == 8) {
-    if (sc.delta_de) {
-      distance = delta_distance<T, W>(sc, px, py, pz, detail, normal_mode, iters_out, total_out);
-      simple = false;
-    }
+  if constexpr (F == F_EXT) {
+    if (sc.n_nodes > 0) return tree_distance<T, W>(sc, px, py, pz, detail, normal_mode, iters_out, total_out);
   }
-  if (simple) {
-    const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
-    V4<T> z;
-    T r, DE;
-    bool maxiter;
-    const int i = compute_orbit<T, F, W>(sc, px, py, pz, sc.formula_maxiter * mult, z, r, DE, maxiter);
-    distance = final_distance<T, F, W>(sc, z, r, DE);
-    const int iters = i + 1;
-    *iters_out = iters;
-    if (total_out) *total_out = iters;
-    // CalculateDistanceSimple post-processing (calculate_distance.cpp:561-605)
-    bool mx = maxiter;
-    if (!sc.iter_thresh) mx = false;
-    if (normal_mode) mx = false;
-    if (mx) distance = T(0.0);
-    if (iters < sc.min_n && distance < detail) distance = detail;
-    if (sc.interior) {
-      if (!normal_mode) {
-        if (distance < T(0.5) * detail || maxiter) distance = detail;
-      } else {
-        if (distance < T(0.9) * detail) distance = detail - distance;
-      }
-    }
-    if (sc.iter_thresh && !normal_mode && !maxiter) {
-      if (distance < detail) distance = detail * T(1.01);
-    }
-    if (distance < T(0.0)) distance = T(0.0);
-    if (distance > T(10.0)) distance = T(10.0);
-  }
+  T distance = calc_distance_simple<T, F, W>(sc, px, py, pz, detail, normal_mode, iters_out, total_out);
   if (F == F_EXT) {  // the union with the primitives (booleanAdd, calculate_distance.cpp:166-201)
     for (int k = 0; k < sc.n_prims; k++) {
       const T pd = prim_distance<T>(sc.prim[k], px, py, pz);

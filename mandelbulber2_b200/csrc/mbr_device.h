@@ -110,6 +110,27 @@ struct DevPrim {
   double pn[3], tri;    // prism: (sin a, cos a, sin a) of half its angle a, triangle height * sin a
 };
 
+// One node of an explicit objects tree as the walk reads it
+// (cObjectsTree::sNodeDataForRendering, objects_tree.h:50-80), built on the
+// host: the world-to-local matrix of its accumulated transform, its scale,
+// repeat and detail multiplier, the smooth-union settings, and for a fractal
+// node its own sequence settings (one slot iterated alone).
+struct DevNode {
+  int32_t type, level, smooth, has_repeat;
+  double w2l[12];
+  double abs_scale, detail_mult, smooth_dist;
+  double repeat[3];     // repeat / absScale
+  // FRACTAL
+  int32_t slot, maxN, julia, has_w;
+  int32_t de_final, de_analytic, delta_de, delta_fn;
+  double julia_c[3];    // julia_c
+  double cmul[3];       // fractal_constant_factor
+  double w0;
+  float fcmul[3], pad_f;
+  // PRIMITIVE: its record in DevScene::prim
+  int32_t prim, pad;
+};
+
 struct DevScene {
   int32_t n;
   int32_t is_hybrid;
@@ -155,6 +176,10 @@ struct DevScene {
   int32_t pad5;
   double delta_factor;
   double delta_rel;
+  // an explicit objects tree (F_EXT iteration only)
+  int32_t n_nodes;
+  int32_t pad6;
+  DevNode node[MBR_MAX_NODES];
   uint8_t seq[MBR_SEQUENCE_LENGTH];
 };
 
@@ -175,7 +200,7 @@ enum DevDeFinal {
 
 __host__ __device__ inline bool scene_extended(const DevScene &sc) {
   return sc.generic || sc.mbrot.folds || sc.mbrot.main || sc.n_prims > 0 || sc.limits || sc.gbox || sc.gsph ||
-         sc.delta_de || sc.de_final > DEF_LINEAR_OFFSET;
+         sc.delta_de || sc.de_final > DEF_LINEAR_OFFSET || sc.n_nodes > 0;
 }
 
 // Everything about one frame that is not the scene: camera, march and

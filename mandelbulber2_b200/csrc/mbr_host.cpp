@@ -125,10 +125,54 @@ static void mandelbox_rotation(const double deg[3], double m[9], bool *zero, boo
 
 static void rotate_axis(double *m, bool *zero, int axis, double angle);
 
+static const double kIdentity44[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+
+// A node's localToWorld under its parent's (objects_tree.cpp:285-330):
+// W = P * [R^T s | t], R from SetRotation2(rotation * pi/180), row-major 4x4.
+static void node_world(const double P[16], const double pos[3], const double rot[3], double scale, double W[16]) {
+  double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  bool zero = true;
+  const double k = kPi / 180.0;
+  rotate_axis(R, &zero, 2, rot[2] * k);
+  rotate_axis(R, &zero, 1, rot[1] * k);
+  rotate_axis(R, &zero, 0, rot[0] * k);
+  const double L[16] = {R[0] * scale, R[3] * scale, R[6] * scale, pos[0],  //
+                        R[1] * scale, R[4] * scale, R[7] * scale, pos[1],  //
+                        R[2] * scale, R[5] * scale, R[8] * scale, pos[2],  //
+                        0.0,          0.0,          0.0,          1.0};
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++)
+      W[r * 4 + c] = P[r * 4 + 0] * L[c] + P[r * 4 + 1] * L[4 + c] + P[r * 4 + 2] * L[8 + c] + P[r * 4 + 3] * L[12 + c];
+}
+
+// CMatrix44::InverseAffine (algebra.cpp:528-576) of W into rows 1-3 of m
+// (m must hold zeros), and the world scale |first row of W|
+static void world_to_local(const double W[16], double m[12], double *abs_scale) {
+  const double ws = std::sqrt(W[0] * W[0] + W[1] * W[1] + W[2] * W[2]);
+  const double s2 = ws * ws;
+  if (ws > 1e-12) {
+    m[0] = W[0] / s2;
+    m[1] = W[4] / s2;
+    m[2] = W[8] / s2;
+    m[4] = W[1] / s2;
+    m[5] = W[5] / s2;
+    m[6] = W[9] / s2;
+    m[8] = W[2] / s2;
+    m[9] = W[6] / s2;
+    m[10] = W[10] / s2;
+  }
+  const double tx = W[3], ty = W[7], tz = W[11];
+  m[3] = -(W[0] * tx + W[4] * ty + W[8] * tz) / s2;
+  m[7] = -(W[1] * tx + W[5] * ty + W[9] * tz) / s2;
+  m[11] = -(W[2] * tx + W[6] * ty + W[10] * tz) / s2;
+  *abs_scale = std::fabs(ws);
+}
+
 // A primitive's node as the distance reads it: localToWorld = [R^T s | t] with
-// R from SetRotation2(rotation * pi/180), accumulated under identity parents,
-// then InverseAffine (objects_tree.cpp:290-385, algebra.cpp:477-576).
-static bool build_prim(const mbr_primitive &q, DevPrim *o) {
+// R from SetRotation2(rotation * pi/180), accumulated under the parent
+// transform P (identity groups for the default objects tree), then
+// InverseAffine (objects_tree.cpp:290-385, algebra.cpp:477-576).
+static bool build_prim(const mbr_primitive &q, DevPrim *o, const double P[16] = kIdentity44) {
   std::memset(o, 0, sizeof(*o));
   const bool finite = finite3(q.position) && finite3(q.rotation) && finite3(q.repeat) && finite3(q.size) &&
                       finite3(q.limits_min) && finite3(q.limits_max) && std::isfinite(q.scale) &&
@@ -145,40 +189,9 @@ static bool build_prim(const mbr_primitive &q, DevPrim *o) {
   if (q.type == MBR_PRIMITIVE_CONE && !(q.height != 0.0)) return false;
   if (q.type == MBR_PRIMITIVE_ELLIPSOID && !(q.size[0] != 0.0 && q.size[1] != 0.0 && q.size[2] != 0.0)) return false;
   if (q.type == MBR_PRIMITIVE_WATER && !(q.length != 0.0)) return false;
-  double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-  bool zero = true;
-  const double k = kPi / 180.0;
-  rotate_axis(R, &zero, 2, q.rotation[2] * k);
-  rotate_axis(R, &zero, 1, q.rotation[1] * k);
-  rotate_axis(R, &zero, 0, q.rotation[0] * k);
-  const double sc = q.scale;
-  const double L[16] = {R[0] * sc, R[3] * sc, R[6] * sc, q.position[0],  //
-                        R[1] * sc, R[4] * sc, R[7] * sc, q.position[1],  //
-                        R[2] * sc, R[5] * sc, R[8] * sc, q.position[2],  //
-                        0.0,       0.0,       0.0,       1.0};
-  static const double I[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
   double W[16];
-  for (int r = 0; r < 4; r++)
-    for (int c = 0; c < 4; c++)
-      W[r * 4 + c] = I[r * 4 + 0] * L[c] + I[r * 4 + 1] * L[4 + c] + I[r * 4 + 2] * L[8 + c] + I[r * 4 + 3] * L[12 + c];
-  const double ws = std::sqrt(W[0] * W[0] + W[1] * W[1] + W[2] * W[2]);
-  const double s2 = ws * ws;
-  if (ws > 1e-12) {
-    o->m[0] = W[0] / s2;
-    o->m[1] = W[4] / s2;
-    o->m[2] = W[8] / s2;
-    o->m[4] = W[1] / s2;
-    o->m[5] = W[5] / s2;
-    o->m[6] = W[9] / s2;
-    o->m[8] = W[2] / s2;
-    o->m[9] = W[6] / s2;
-    o->m[10] = W[10] / s2;
-  }
-  const double tx = W[3], ty = W[7], tz = W[11];
-  o->m[3] = -(W[0] * tx + W[4] * ty + W[8] * tz) / s2;
-  o->m[7] = -(W[1] * tx + W[5] * ty + W[9] * tz) / s2;
-  o->m[11] = -(W[2] * tx + W[6] * ty + W[10] * tz) / s2;
-  o->abs_scale = std::fabs(ws);
+  node_world(P, q.position, q.rotation, q.scale, W);
+  world_to_local(W, o->m, &o->abs_scale);
   for (int i = 0; i < 3; i++) o->repeat[i] = q.repeat[i] / o->abs_scale;
   o->has_repeat = std::sqrt(o->repeat[0] * o->repeat[0] + o->repeat[1] * o->repeat[1] + o->repeat[2] * o->repeat[2]) > 0.0;
   o->type = q.type;
@@ -228,6 +241,139 @@ static bool build_prim(const mbr_primitive &q, DevPrim *o) {
   return true;
 }
 
+// ---- explicit objects tree -----------------------------------------------------
+// The node list's shape (cObjectsTree, objects_tree.cpp:185-245): levels
+// start at 0 and go down by at most one per node, only a boolean group has
+// children, a disabled node drops its subtree.  live[i]: node i is walked.
+static mbr_status tree_shape(mbr_ctx *ctx, const mbr_scene &sc, bool live[MBR_MAX_NODES]) {
+  int skip = -1, prev_level = -1;
+  bool prev_group = false;
+  for (int i = 0; i < sc.n_nodes; i++) {
+    const mbr_node &q = sc.node[i];
+    const bool group =
+        q.type == MBR_NODE_BOOLEAN_ADD || q.type == MBR_NODE_BOOLEAN_MUL || q.type == MBR_NODE_BOOLEAN_SUB;
+    if (!group && q.type != MBR_NODE_FRACTAL && q.type != MBR_NODE_PRIMITIVE)
+      return set_err(ctx, MBR_EINVAL, "node %d: type must be FRACTAL, PRIMITIVE or a boolean group, got %d", i,
+                     q.type);
+    if (q.level < 0 || q.level > 8 || q.level > prev_level + 1)
+      return set_err(ctx, MBR_EINVAL, "node %d: level must be in [0, 8] and at most one below the node before", i);
+    if (q.level == prev_level + 1 && i > 0 && !prev_group)
+      return set_err(ctx, MBR_EINVAL, "node %d: only a boolean group has children", i);
+    prev_level = q.level;
+    prev_group = group;
+    if (skip >= 0 && q.level > skip) continue;
+    skip = -1;
+    if (!q.enabled) {
+      skip = q.level;
+      continue;
+    }
+    if (q.type == MBR_NODE_FRACTAL && (q.index < 0 || q.index >= sc.n_fractals))
+      return set_err(ctx, MBR_EINVAL, "node %d: fractal index must be in [0, n_fractals)", i);
+    if (q.type == MBR_NODE_PRIMITIVE && (q.index < 0 || q.index >= sc.n_primitives))
+      return set_err(ctx, MBR_EINVAL, "node %d: primitive index must be in [0, n_primitives)", i);
+    if (!finite3(q.position) || !finite3(q.rotation) || !finite3(q.repeat) || !std::isfinite(q.scale) ||
+        !std::isfinite(q.detail_level_multiplier) || !std::isfinite(q.smooth_combine_distance) ||
+        !finite3(q.julia_c) || !finite3(q.fractal_constant_factor) || !std::isfinite(q.initial_waxis))
+      return set_err(ctx, MBR_EINVAL, "node %d: non-finite value", i);
+    if (group || q.type == MBR_NODE_FRACTAL) {
+      if (!(std::fabs(q.scale) > 1e-12)) return set_err(ctx, MBR_EINVAL, "node %d: |scale| must be > 1e-12", i);
+    }
+    if (q.smooth_combine && !(q.smooth_combine_distance != 0.0))
+      return set_err(ctx, MBR_EINVAL, "node %d: smooth_combine_distance must be non-zero", i);
+    if (q.type == MBR_NODE_FRACTAL && (q.formula_maxiter < 1 || q.formula_maxiter > 9999))
+      return set_err(ctx, MBR_EINVAL, "node %d: formula_maxiter must be in [1, 9999]", i);
+    live[i] = true;
+  }
+  return MBR_OK;
+}
+
+// cObjectsTree::GetNodeDataListForRendering (objects_tree.cpp:185-410) into
+// the scene: per walked node its world matrix (the parent's times its own)
+// inverted, |world scale|, repeat / |world scale|; a fractal node's slot with
+// the sequence settings CreateSequence gives a non-hybrid node (iteration
+// limit, julia, constant factor, w, DE selection, hybrid_fractal_sequences.cpp:
+// 377-500); a primitive node's record in d->prim under the accumulated
+// transform (one record per primitive node).
+static mbr_status build_tree(mbr_ctx *ctx, const mbr_scene &sc, const bool live[MBR_MAX_NODES], DevScene *d) {
+  double Wl[9][16];
+  int nn = 0, np = 0;
+  for (int i = 0; i < sc.n_nodes; i++) {
+    if (!live[i]) continue;
+    const mbr_node &q = sc.node[i];
+    DevNode &o = d->node[nn];
+    std::memset(&o, 0, sizeof(o));
+    o.type = q.type;
+    o.level = q.level;
+    o.smooth = q.smooth_combine ? 1 : 0;
+    o.smooth_dist = q.smooth_combine_distance;
+    o.detail_mult = q.detail_level_multiplier;
+    const double *P = (q.level == 0) ? kIdentity44 : Wl[q.level - 1];
+    if (q.type == MBR_NODE_PRIMITIVE) {
+      if (np >= MBR_MAX_PRIMITIVES)
+        return set_err(ctx, MBR_EUNSUPPORTED, "an objects tree holds at most %d primitive nodes", MBR_MAX_PRIMITIVES);
+      const mbr_primitive &pq = sc.primitive[q.index];
+      if (!build_prim(pq, &d->prim[np], P))
+        return set_err(ctx, MBR_EINVAL,
+                       "primitive %d: type must be 1..8, every value finite, |scale| > 1e-12, iterations in "
+                       "[0, 100] and a water length != 0",
+                       q.index);
+      node_world(P, pq.position, pq.rotation, pq.scale, Wl[q.level]);
+      const DevPrim &pr = d->prim[np];
+      for (int k = 0; k < 12; k++) o.w2l[k] = pr.m[k];
+      o.abs_scale = pr.abs_scale;
+      for (int k = 0; k < 3; k++) o.repeat[k] = pr.repeat[k];
+      o.has_repeat = pr.has_repeat;
+      o.prim = np++;
+    } else {
+      node_world(P, q.position, q.rotation, q.scale, Wl[q.level]);
+      world_to_local(Wl[q.level], o.w2l, &o.abs_scale);
+      for (int k = 0; k < 3; k++) o.repeat[k] = q.repeat[k] / o.abs_scale;
+      o.has_repeat =
+          std::sqrt(o.repeat[0] * o.repeat[0] + o.repeat[1] * o.repeat[1] + o.repeat[2] * o.repeat[2]) > 0.0;
+    }
+    if (q.type == MBR_NODE_FRACTAL) {
+      const int slot = q.index;
+      FormulaMeta m;
+      formula_meta(d->slot[slot].formula, &m);  // validated with the slots
+      o.slot = slot;
+      o.maxN = q.formula_maxiter;
+      o.julia = q.julia_mode ? 1 : 0;
+      for (int k = 0; k < 3; k++) {
+        o.julia_c[k] = q.julia_c[k];
+        o.cmul[k] = q.fractal_constant_factor[k];
+        o.fcmul[k] = float(q.fractal_constant_factor[k]);
+      }
+      o.w0 = q.initial_waxis;
+      const int f = d->slot[slot].formula;
+      o.has_w = (q.initial_waxis != 0.0 || f == MBR_FORMULA_HYPERCOMPLEX || f == MBR_FORMULA_AEXION) ? 1 : 0;
+      if (o.has_w) d->has_w = 1;
+      int de_function = m.de_function, de_analytic = m.analytic;
+      if (sc.delta_de_function != MBR_DE_FUNCTION_PREFERRED) {
+        static const int fn_analytic[7] = {1, 1, 2, 4, 5, 6, 7};  // enumDEAnalyticFunction
+        de_function = sc.delta_de_function;
+        de_analytic = fn_analytic[de_function];
+      }
+      static const int an_final[8] = {DEF_NONE, DEF_LINEAR, DEF_LOG, DEF_IFS, DEF_PSEUDO_KLEINIAN, 0, DEF_CUSTOM,
+                                      DEF_MAX_AXIS};
+      o.de_analytic = de_analytic;
+      o.de_final = an_final[de_analytic];
+      o.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+      o.delta_fn = de_function;
+      if (!o.delta_de && o.de_final == 0)
+        return set_err(ctx, MBR_EUNSUPPORTED,
+                       "node %d: the analytic Jos Kleinian DE function reads formula parameters this build does "
+                       "not carry (the delta DE takes it)",
+                       i);
+    }
+    nn++;
+  }
+  if (nn == 0) return set_err(ctx, MBR_EINVAL, "every node of the objects tree is disabled");
+  d->n_nodes = nn;
+  d->n_prims = np;
+  d->generic = 1;  // the tree is walked by the reference-order iteration only
+  return MBR_OK;
+}
+
 // ---- scene -------------------------------------------------------------------
 // Validates `sc` and flattens it into a DevScene.  Restates CollectSequenceData
 // and CreateSequence for the single fractal (or hybrid) node of the default
@@ -255,20 +401,39 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     return set_err(ctx, MBR_EINVAL, "delta_de_method must be in [0, 2], got %d", sc.delta_de_method);
   if (!(sc.deltade_relative_delta > 0.0) || !std::isfinite(sc.deltade_relative_delta))
     return set_err(ctx, MBR_EINVAL, "deltade_relative_delta must be finite and > 0");
+  // the slots the scene iterates: the fractal (or the hybrid sequence's
+  // slots) of the default objects tree, or the slots that the enabled fractal
+  // nodes of an explicit tree name
+  if (sc.n_nodes < 0 || sc.n_nodes > MBR_MAX_NODES)
+    return set_err(ctx, MBR_EINVAL, "n_nodes must be in [0, %d], got %d", MBR_MAX_NODES, sc.n_nodes);
+  const bool tree = sc.n_nodes > 0;
+  if (tree && hybrid)
+    return set_err(ctx, MBR_EUNSUPPORTED, "an explicit objects tree takes non-hybrid fractal nodes");
+  bool used[MBR_MAX_FRACTALS] = {};
+  for (int i = 0; i < (hybrid ? n : 1); i++) used[i] = true;
+  bool live[MBR_MAX_NODES] = {};
+  if (tree) {
+    mbr_status st = tree_shape(ctx, sc, live);
+    if (st != MBR_OK) return st;
+    for (int i = 0; i < sc.n_nodes; i++)
+      if (live[i] && sc.node[i].type == MBR_NODE_FRACTAL) used[sc.node[i].index] = true;
+  }
   // Mandelbox rotations and the kaleidoscopic IFS: the scene holds one block
   // of each, for its single Mandelbox slot and its single IFS slot
   int n_box = 0, n_ifs = 0;
-  for (int i = 0; i < (hybrid ? n : 1); i++) {
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++) {
+    if (!used[i]) continue;
     if (sc.fractal[i].formula == MBR_FORMULA_MANDELBOX) n_box++;
     if (sc.fractal[i].formula == MBR_FORMULA_KALEIDOSCOPIC_IFS) n_ifs++;
   }
-  for (int i = 0; i < (hybrid ? n : 1); i++) {
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++) {
+    if (!used[i]) continue;
     const mbr_fractal &f = sc.fractal[i];
     const bool rot = f.mandelbox_rotations_enabled || f.mandelbox_main_rotation_enabled;
     if (!rot || f.formula != MBR_FORMULA_MANDELBOX) continue;
     if (n_box > 1)
       return set_err(ctx, MBR_EUNSUPPORTED,
-                     "Mandelbox rotations are supported when the sequence has one Mandelbox slot");
+                     "Mandelbox rotations are supported when the scene iterates one Mandelbox slot");
     bool ok = finite3(f.mandelbox_rotation_main);
     for (int a = 0; a < 3; a++) ok = ok && finite3(f.mandelbox_rotation_neg[a]) && finite3(f.mandelbox_rotation_pos[a]);
     if (!ok) return set_err(ctx, MBR_EINVAL, "non-finite Mandelbox rotation angle");
@@ -285,11 +450,12 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     mandelbox_rotation(f.mandelbox_rotation_main, r.mm, &zero);
     r.main_zero = zero ? 1 : 0;
   }
-  for (int i = 0; i < (hybrid ? n : 1); i++) {
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++) {
+    if (!used[i]) continue;
     const mbr_fractal &f = sc.fractal[i];
     if (f.formula != MBR_FORMULA_KALEIDOSCOPIC_IFS) continue;
     if (n_ifs > 1)
-      return set_err(ctx, MBR_EUNSUPPORTED, "the kaleidoscopic IFS is supported in one slot of a sequence");
+      return set_err(ctx, MBR_EUNSUPPORTED, "the kaleidoscopic IFS is supported in one slot of a scene");
     IfsBlock &b = d.ifs;
     b.abs_x = f.ifs_abs_x ? 1 : 0;
     b.abs_y = f.ifs_abs_y ? 1 : 0;
@@ -330,7 +496,8 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   d.is_hybrid = hybrid ? 1 : 0;
   double maxBailout = 0.0;
   bool any = false;
-  for (int i = 0; i < n; i++) {
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++) {
+    if (!used[i]) continue;
     const mbr_fractal &f = sc.fractal[i];
     DevSlot &s = d.slot[i];
     s.formula = f.formula;
@@ -401,7 +568,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   if (!any) return set_err(ctx, MBR_EINVAL, "scene has no formula");
   if (hybrid && sc.use_default_bailout)
     for (int i = 0; i < n; i++) d.slot[i].d[P_BAILOUT] = maxBailout;
-  for (int i = 0; i < n; i++)
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++)
     for (int k = 0; k < P_COUNT; k++) d.slot[i].f[k] = float(d.slot[i].d[k]);
 
   // the sequence (hybrid_fractal_sequences.cpp:296-370)
@@ -496,7 +663,8 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   }
   d.w0 = sc.initial_waxis;
   d.has_w = sc.initial_waxis != 0.0;
-  for (int i = 0; i < n; i++) {
+  for (int i = 0; i < MBR_MAX_FRACTALS; i++) {
+    if (!used[i]) continue;
     const int f = d.slot[i].formula;
     if (f == MBR_FORMULA_HYPERCOMPLEX || f == MBR_FORMULA_AEXION) d.has_w = 1;  // z.w evolves from w = 0
     if (f != MBR_FORMULA_NONE && f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX &&
@@ -541,6 +709,10 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
   d.fgsph_mr2 = float(d.gsph_mr2);
   if (d.limits || d.gbox || d.gsph) d.generic = 1;  // the reference-order iteration carries them
   if (d.delta_de || d.de_final > DEF_LINEAR_OFFSET) d.generic = 1;  // so do the delta DE and the other DE functions
+  if (tree) {
+    mbr_status st = build_tree(ctx, sc, live, &d);
+    if (st != MBR_OK) return st;
+  }
   *out = d;
   return MBR_OK;
 }

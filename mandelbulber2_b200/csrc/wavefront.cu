@@ -1872,6 +1872,8 @@ static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFra
                    "not resolve; it runs on the plain FP64 engines");
   if (fr.refine != MBR_REFINE_REFERENCE)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: root refinement uses the plain engines");
+  if (sc.n_nodes > 0)
+    return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: explicit objects trees use the plain engines");
   if (fr.slow_shading)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: slow shading (iteration-count normals) uses the plain "
                                           "engines");

@@ -17,6 +17,7 @@
 #include <cstdint>
 #include <cstring>
 #include <type_traits>
+#include <memory>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -92,8 +93,11 @@ struct OPrim {
   double repeat[3];  // node repeat / absScale (calculate_distance.cpp:277-282)
 };
 
+struct OTree;  // an explicit objects tree (below)
+
 struct Seq {
   std::vector<OPrim> prims;
+  std::shared_ptr<OTree> tree;  // set when the scene lists nodes
   // limit box (fractparams.cpp:175-177) and global folds (:346-351)
   bool limits = false, gbox = false, gsph = false;
   double lim_min[3] = {-10, -10, -10}, lim_max[3] = {10, 10, 10};
@@ -112,6 +116,7 @@ struct Seq {
 };
 
 static bool build_prim(const mbr_primitive &q, OPrim *o);
+static bool build_tree(const mbr_scene &sc, Seq *s);
 
 // Returns false for scenes the restatement does not cover.
 static bool build_sequence(const mbr_scene &sc, Seq *out) {
@@ -268,6 +273,7 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
   s.gbox_value = sc.box_folding_value;
   s.gsph_inner = sc.spherical_folding_inner;
   s.gsph_outer = sc.spherical_folding_outer;
+  if (!build_tree(sc, &s)) return false;
   *out = s;
   return true;
 }
@@ -360,6 +366,45 @@ static bool build_prim(const mbr_primitive &q, OPrim *o) {
 
 // std::max
 static inline double dmax(double a, double b) { return (a < b) ? b : a; }
+
+// One component of CVector3::repeatMod (algebra.hpp:106-115)
+static inline double repeat_mod(double p, double v) {
+  double t = p - v * 0.5;
+  t = (v > 0.0) ? fmod(t, v) : t;
+  t = t + v;
+  t = (v > 0.0) ? fmod(t, v) : t;
+  return t - v * 0.5;
+}
+
+// A node's local-to-world matrix composed with its parent's
+// (objects_tree.cpp:285-330): W = P * [R s | t], R from SetRotation2 of the
+// rotation in degrees
+static void node_world(const double P[4][4], const double pos[3], const double rot[3], double scale,
+                       double W[4][4]) {
+  double R[9];
+  bool zero;
+  mb_rotation(rot, R, &zero, false, M_PI / 180.0);
+  const double L[4][4] = {{R[0] * scale, R[3] * scale, R[6] * scale, pos[0]},
+                          {R[1] * scale, R[4] * scale, R[7] * scale, pos[1]},
+                          {R[2] * scale, R[5] * scale, R[8] * scale, pos[2]},
+                          {0.0, 0.0, 0.0, 1.0}};
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) W[r][c] = P[r][0] * L[0][c] + P[r][1] * L[1][c] + P[r][2] * L[2][c] + P[r][3] * L[3][c];
+}
+
+// CMatrix44::InverseAffine (algebra.cpp:528-576) into rows 1-3, and the
+// world scale (the norm of the first row)
+static void inverse_affine(const double W[4][4], double m[12], double *abs_scale) {
+  const double ws = sqrt(W[0][0] * W[0][0] + W[0][1] * W[0][1] + W[0][2] * W[0][2]);
+  const double sSq = ws * ws;
+  for (int i = 0; i < 12; i++) m[i] = 0.0;
+  if (ws > 1e-12) {
+    for (int r = 0; r < 3; r++)
+      for (int c = 0; c < 3; c++) m[r * 4 + c] = W[c][r] / sSq;
+  }
+  for (int r = 0; r < 3; r++) m[r * 4 + 3] = -(W[0][r] * W[0][3] + W[1][r] * W[1][3] + W[2][r] * W[2][3]) / sSq;
+  *abs_scale = fabs(ws);
+}
 
 // Limits box of a primitive (primitive.cpp, e.g. :490-495)
 static inline double limit_box(const mbr_primitive &q, double x, double y, double z, double dist) {
@@ -1098,33 +1143,14 @@ static double delta_distance(const Seq &seq, const SlotT<double> *slots, double 
   return distance;
 }
 
-// CalculateDistanceSimple, analytic branch (calculate_distance.cpp:533-606),
-// reached through CalculateDistanceFromObjectsTree (:225-516) for the single
-// identity-transform node (pointLocal == point, distance *= 1).
+// CalculateDistanceSimple (calculate_distance.cpp:533-760): the delta branch
+// (FP64) or the analytic branch, with its post-processing.
 template <class S>
-S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
-                int *iters_out, int *total_out = nullptr) {
-  if (seq.limits) {  // the limit box early-out (calculate_distance.cpp:261-275)
-    S bx = std::max(px - seq.lim_max[0], -(px - seq.lim_min[0]));
-    S by = std::max(py - seq.lim_max[1], -(py - seq.lim_min[1]));
-    S bz = std::max(pz - seq.lim_max[2], -(pz - seq.lim_min[2]));
-    S limitBoxDist = std::max({bx, by, bz});
-    if (limitBoxDist > detailSize) {
-      if (iters_out) *iters_out = 0;  // the reference leaves out->iters unset here
-      if (total_out) *total_out = 0;
-      return limitBoxDist;
-    }
-  }
+S calc_distance_simple(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
+                       int *iters_out, int *total_out) {
   const int mult = (normalMode && seq.iter_thresh) ? 5 : 1;
   if constexpr (std::is_same<S, double>::value) {
-    if (seq.delta_de) {
-      S distance = delta_distance(seq, slots, px, py, pz, detailSize, normalMode, mult, iters_out, total_out);
-      for (const OPrim &op : seq.prims) {  // booleanAdd with the primitives
-        const double pd = prim_distance(op, px, py, pz);
-        if (pd < distance) distance = pd;
-      }
-      return distance;
-    }
+    if (seq.delta_de) return delta_distance(seq, slots, px, py, pz, detailSize, normalMode, mult, iters_out, total_out);
   }
   FractalOut<S> fo = compute<S>(seq, slots, px, py, pz, mult, -1);
   S distance = fo.distance;
@@ -1146,6 +1172,234 @@ S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double 
   }
   if (distance < 0.0) distance = 0.0;
   if (distance > 10.0) distance = 10.0;
+  return distance;
+}
+
+// One node of an explicit objects tree as the walk reads it
+// (cObjectsTree::sNodeDataForRendering, objects_tree.h:50-80): the world-to-
+// local matrix of its accumulated transform, its scale and repeat, and for a
+// fractal node its own sequence (the scene's general settings with the
+// node's slot, iteration limit, julia and constant factor).
+struct ONode {
+  int type = 0, level = 0;
+  double w2l[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+  double abs_scale = 1.0, detail_mult = 1.0, smooth_dist = 0.1;
+  double repeat[3] = {0, 0, 0};  // repeat / absScale
+  bool smooth = false;
+  OPrim prim;                    // PRIMITIVE: its world transform, repeat and scale
+  std::shared_ptr<Seq> seq;      // FRACTAL
+  std::vector<SlotT<double>> slots;
+};
+struct OTree {
+  std::vector<ONode> nodes;
+};
+
+// cObjectsTree::GetNodeDataListForRendering (objects_tree.cpp:185-410) for
+// the listed nodes: a disabled node drops its subtree, every node's world
+// matrix is its parent's times its own, and a fractal node's sequence is
+// built from the scene with that node's slot and settings.
+static bool build_tree(const mbr_scene &sc, Seq *s) {
+  if (sc.n_nodes <= 0) return true;
+  if (sc.n_nodes > MBR_MAX_NODES || sc.hybrid_fractal_enable) return false;
+  auto tree = std::make_shared<OTree>();
+  double Wl[12][4][4];
+  static const double I[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+  int skip = -1, prev_level = -1, prev_type = 0;
+  for (int i = 0; i < sc.n_nodes; i++) {
+    const mbr_node &n = sc.node[i];
+    const bool group = n.type == MBR_NODE_BOOLEAN_ADD || n.type == MBR_NODE_BOOLEAN_MUL || n.type == MBR_NODE_BOOLEAN_SUB;
+    if (n.level < 0 || n.level > 8 || n.level > prev_level + 1) return false;
+    if (n.level == prev_level + 1 && i > 0 && prev_type != 1) return false;  // only a group has children
+    prev_level = n.level;
+    prev_type = group ? 1 : 0;
+    if (skip >= 0 && n.level > skip) continue;
+    skip = -1;
+    if (!n.enabled) {
+      skip = n.level;
+      continue;
+    }
+    ONode nd;
+    nd.type = n.type;
+    nd.level = n.level;
+    nd.detail_mult = n.detail_level_multiplier;
+    nd.smooth = n.smooth_combine != 0;
+    nd.smooth_dist = n.smooth_combine_distance;
+    const double(*P)[4] = (n.level == 0) ? I : Wl[n.level - 1];
+    const mbr_primitive *q = nullptr;
+    if (n.type == MBR_NODE_PRIMITIVE) {
+      if (n.index < 0 || n.index >= sc.n_primitives) return false;
+      q = &sc.primitive[n.index];
+      node_world(P, q->position, q->rotation, q->scale, Wl[n.level]);
+    } else {
+      node_world(P, n.position, n.rotation, n.scale, Wl[n.level]);
+    }
+    inverse_affine(Wl[n.level], nd.w2l, &nd.abs_scale);
+    const double *rep = q ? q->repeat : n.repeat;
+    for (int k = 0; k < 3; k++) nd.repeat[k] = rep[k] / nd.abs_scale;
+    if (n.type == MBR_NODE_FRACTAL) {
+      if (n.index < 0 || n.index >= MBR_MAX_FRACTALS) return false;
+      mbr_scene t = sc;
+      t.n_nodes = 0;
+      t.n_primitives = 0;
+      t.hybrid_fractal_enable = 0;
+      t.n_fractals = 1;
+      t.fractal[0] = sc.fractal[n.index];
+      t.formula_maxiter = n.formula_maxiter;
+      t.julia_mode = n.julia_mode;
+      for (int k = 0; k < 3; k++) {
+        t.julia_c[k] = n.julia_c[k];
+        t.fractal_constant_factor[k] = n.fractal_constant_factor[k];
+      }
+      t.initial_waxis = n.initial_waxis;
+      auto seq = std::make_shared<Seq>();
+      if (!build_sequence(t, seq.get())) return false;
+      nd.seq = seq;
+      nd.slots.push_back(make_slot<double>(seq->slot[0], false));
+    } else if (n.type == MBR_NODE_PRIMITIVE) {
+      nd.prim.q = *q;
+      for (int k = 0; k < 12; k++) nd.prim.w2l[k] = nd.w2l[k];
+      nd.prim.abs_scale = nd.abs_scale;
+      for (int k = 0; k < 3; k++) nd.prim.repeat[k] = nd.repeat[k];
+    } else if (!group) {
+      return false;
+    }
+    tree->nodes.push_back(nd);
+  }
+  s->tree = tree;
+  return true;
+}
+
+// mergeChildIntoParent (calculate_distance.cpp:103-204) on the distance and
+// the smooth-combine settings (the closest-object bookkeeping is for shading)
+struct OFrame {
+  double dist = 1e20, detail = 0.0, smooth_dist = 0.1;
+  int level = 0, type = MBR_NODE_BOOLEAN_ADD;
+  bool smooth = false;
+};
+static void merge_child(const OFrame &child, OFrame *parent) {
+  const double cd = child.dist;
+  switch (parent->type) {
+    case MBR_NODE_BOOLEAN_MUL:
+      if (cd > parent->dist) parent->dist = cd;
+      break;
+    case MBR_NODE_BOOLEAN_SUB:
+      if (parent->dist >= 1e19) {
+        parent->dist = cd;
+      } else if (parent->detail > 0 && cd < parent->detail) {
+        const double limitDist = parent->detail * 1.5;
+        if (cd < limitDist) {
+          parent->dist = limitDist;
+        } else {
+          const double adjusted = std::max(limitDist - cd, parent->dist);
+          parent->dist = (adjusted < 0) ? 0 : adjusted;
+        }
+      }
+      break;
+    default:
+      if (child.smooth && parent->dist < 1e19) {  // opSmoothUnion (math_utilities.h:99-103)
+        const double k = child.smooth_dist, d1 = cd, d2 = parent->dist;
+        const double t = 0.5 + 0.5 * (d2 - d1) / k;
+        const double h = (t < 0.0) ? 0.0 : ((t > 1.0) ? 1.0 : t);
+        parent->dist = (d2 * (1.0 - h) + d1 * h) - k * h * (1.0 - h);
+      } else if (cd < parent->dist) {
+        parent->dist = cd;
+      }
+      break;
+  }
+}
+
+// CalculateDistanceFromObjectsTree (calculate_distance.cpp:225-516) over an
+// explicit tree: each enabled node's world-to-local transform, repeat in its
+// own frame and detail size / (absScale * detail multiplier), boolean groups
+// on a stack of at most 10 levels.  iters: the leaves' iterations summed.
+static double tree_distance(const Seq &seq, double px, double py, double pz, double detailSize, bool normalMode,
+                            int *iters_out, int *total_out) {
+  OFrame st[10];
+  st[0].dist = 1e20;
+  st[0].level = 0;
+  st[0].type = MBR_NODE_BOOLEAN_ADD;
+  st[0].detail = detailSize;
+  int sl = 0, total_iters = 0, total_all = 0;
+  for (const ONode &nd : seq.tree->nodes) {
+    const double *m = nd.w2l;
+    double lx = m[0] * px + m[1] * py + m[2] * pz + m[3];
+    double ly = m[4] * px + m[5] * py + m[6] * pz + m[7];
+    double lz = m[8] * px + m[9] * py + m[10] * pz + m[11];
+    if (sqrt(nd.repeat[0] * nd.repeat[0] + nd.repeat[1] * nd.repeat[1] + nd.repeat[2] * nd.repeat[2]) > 0.0) {
+      lx = repeat_mod(lx, nd.repeat[0]);
+      ly = repeat_mod(ly, nd.repeat[1]);
+      lz = repeat_mod(lz, nd.repeat[2]);
+    }
+    double nodeDetail;
+    if (nd.abs_scale > 0.0 && nd.detail_mult > 0.0) nodeDetail = detailSize / nd.abs_scale / nd.detail_mult;
+    else if (nd.abs_scale > 0.0) nodeDetail = detailSize / nd.abs_scale;
+    else if (nd.detail_mult > 0.0) nodeDetail = detailSize / nd.detail_mult;
+    else nodeDetail = detailSize;
+    if (nd.level < sl) {
+      while (sl > nd.level) {
+        const OFrame child = st[sl];
+        sl--;
+        merge_child(child, &st[sl]);
+      }
+    }
+    double distance = 1e20;
+    int leafIters = 0, leafTotal = 0;
+    if (nd.type == MBR_NODE_FRACTAL) {
+      distance = calc_distance_simple<double>(*nd.seq, nd.slots.data(), lx, ly, lz, nodeDetail, normalMode,
+                                              &leafIters, &leafTotal);
+      distance *= nd.abs_scale;
+    } else if (nd.type == MBR_NODE_PRIMITIVE) {
+      distance = prim_distance(nd.prim, px, py, pz);
+    } else {
+      sl++;
+      st[sl].dist = (nd.type == MBR_NODE_BOOLEAN_MUL) ? -1e20 : 1e20;
+      st[sl].level = nd.level;
+      st[sl].type = nd.type;
+      st[sl].detail = nodeDetail;
+      st[sl].smooth = nd.smooth;
+      st[sl].smooth_dist = nd.smooth_dist;
+      continue;
+    }
+    OFrame leaf;
+    leaf.dist = distance;
+    leaf.detail = nodeDetail;
+    leaf.smooth = nd.smooth;
+    leaf.smooth_dist = nd.smooth_dist;
+    merge_child(leaf, &st[sl]);
+    total_iters += leafIters;
+    total_all += leafTotal;
+  }
+  while (sl > 0) {
+    const OFrame child = st[sl];
+    sl--;
+    merge_child(child, &st[sl]);
+  }
+  if (iters_out) *iters_out = total_iters;
+  if (total_out) *total_out = total_all;
+  return st[0].dist;
+}
+
+// CalculateDistance: the limit box early-out, then the objects tree - the
+// explicit one, or the default (the fractal node, identity transform, and
+// the primitives joined by union, calculate_distance.cpp:166-201).
+template <class S>
+S calc_distance(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, double detailSize, bool normalMode,
+                int *iters_out, int *total_out = nullptr) {
+  if (seq.limits) {  // the limit box early-out (calculate_distance.cpp:261-275)
+    S bx = std::max(px - seq.lim_max[0], -(px - seq.lim_min[0]));
+    S by = std::max(py - seq.lim_max[1], -(py - seq.lim_min[1]));
+    S bz = std::max(pz - seq.lim_max[2], -(pz - seq.lim_min[2]));
+    S limitBoxDist = std::max({bx, by, bz});
+    if (limitBoxDist > detailSize) {
+      if (iters_out) *iters_out = 0;  // the reference leaves out->iters unset here
+      if (total_out) *total_out = 0;
+      return limitBoxDist;
+    }
+  }
+  if constexpr (std::is_same<S, double>::value) {
+    if (seq.tree) return tree_distance(seq, px, py, pz, detailSize, normalMode, iters_out, total_out);
+  }
+  S distance = calc_distance_simple<S>(seq, slots, px, py, pz, detailSize, normalMode, iters_out, total_out);
   if constexpr (std::is_same<S, double>::value) {  // booleanAdd with the primitives (calculate_distance.cpp:166-201)
     for (const OPrim &op : seq.prims) {
       const double pd = prim_distance(op, px, py, pz);

@@ -31,6 +31,8 @@
 #include "src/material.h"
 #include "src/objects_tree.h"
 #include "src/parameters.hpp"
+#include "src/primitive_item.h"
+#include "src/primitives.h"
 #include "src/render_data.hpp"
 #include "src/render_worker.hpp"
 #include "src/scheduler.hpp"
@@ -117,6 +119,18 @@ int refp_set_string(void *h, int fractal, const char *name, const char *value) {
 int refp_add_node(void *h, int id) {
   Pipeline *p = static_cast<Pipeline *>(h);
   InitNodeParams(id, p->par);
+  p->prepared = false;
+  return 0;
+}
+
+// Adds the parameters of primitive_<type>_<id> with their defaults
+// (InitPrimitiveParams, initparameters.cpp:1313-1420).
+int refp_add_primitive(void *h, const char *type_name, int id) {
+  Pipeline *p = static_cast<Pipeline *>(h);
+  const QString name(type_name);
+  const fractal::enumObjectType t = cPrimitives::PrimitiveNameToEnum(name);
+  const sPrimitiveItem item(t, id, QString("primitive_%1_%2").arg(name).arg(id), name);
+  InitPrimitiveParams(item, p->par);
   p->prepared = false;
   return 0;
 }

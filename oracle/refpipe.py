@@ -25,6 +25,10 @@ _P = C.c_void_p
 
 KIND_INT, KIND_DOUBLE, KIND_BOOL, KIND_VEC3 = 0, 1, 2, 3
 NODE_FRACTAL, NODE_HYBRID = 1, 10  # enumNodeType (object_node_type.h:11-19)
+NODE_FRACTAL_T, NODE_PRIMITIVE_T = 1, 2
+# mbr_primitive_type -> the reference's primitive type names (primitives.cpp:60-100)
+PRIMITIVE_NAMES = {1: "plane", 2: "box", 3: "sphere", 4: "water", 5: "torus", 6: "cylinder", 7: "circle",
+                   8: "rectangle", 9: "cone", 10: "prism", 11: "ellipsoid"}
 
 
 def available() -> bool:
@@ -45,6 +49,7 @@ class RefPipeline:
             L.refp_set.argtypes = [_P, C.c_int, C.c_char_p, C.c_int, _P]
             L.refp_set_string.argtypes = [_P, C.c_int, C.c_char_p, C.c_char_p]
             L.refp_add_node.argtypes = [_P, C.c_int]
+            L.refp_add_primitive.argtypes = [_P, C.c_char_p, C.c_int]
             L.refp_prepare.argtypes = [_P]
             L.refp_distance.argtypes = [_P, _P, C.c_int, C.c_double, C.c_int, _P, _P]
             L.refp_compute.argtypes = [_P, _P, C.c_int, C.c_int, _P, _P, _P, _P]
@@ -82,6 +87,82 @@ class RefPipeline:
 
     def add_node(self, node_id: int) -> None:
         self.L.refp_add_node(self.h, node_id)
+
+    def add_primitive(self, type_name: str, pid: int) -> None:
+        self.L.refp_add_primitive(self.h, type_name.encode(), pid)
+
+    def _primitive(self, q, pid: int, object_id: int) -> str:
+        """primitive_<type>_<pid>: the mbr_primitive's shape parameters (its
+        transform goes to its node)."""
+        name = PRIMITIVE_NAMES[q.type]
+        self.add_primitive(name, pid)
+        pre = f"primitive_{name}_{pid}_"
+        self.set(pre + "enabled", 1, KIND_BOOL)
+        self.set(pre + "object_id", object_id, KIND_INT)
+        for key, kind, val in (("empty", KIND_BOOL, q.empty), ("limits_enable", KIND_BOOL, q.limits_enable),
+                               ("caps", KIND_BOOL, q.caps), ("iterations", KIND_INT, q.iterations),
+                               ("size", KIND_VEC3, list(q.size)), ("radius", KIND_DOUBLE, q.radius),
+                               ("height", KIND_DOUBLE, q.height), ("width", KIND_DOUBLE, q.width),
+                               ("tube_radius", KIND_DOUBLE, q.tube_radius),
+                               ("radius_lpow", KIND_DOUBLE, q.radius_lpow),
+                               ("tube_radius_lpow", KIND_DOUBLE, q.tube_radius_lpow),
+                               ("rounding", KIND_DOUBLE, q.rounding), ("wall_thickness", KIND_DOUBLE, q.wall_thickness),
+                               ("limits_min", KIND_VEC3, list(q.limits_min)),
+                               ("limits_max", KIND_VEC3, list(q.limits_max)),
+                               ("relative_amplitude", KIND_DOUBLE, q.relative_amplitude),
+                               ("length", KIND_DOUBLE, q.length), ("anim_speed", KIND_DOUBLE, q.anim_speed),
+                               ("anim_progression_speed", KIND_DOUBLE, q.anim_progression_speed),
+                               ("prism_angle", KIND_DOUBLE, q.prism_angle),
+                               ("trangle_height", KIND_DOUBLE, q.triangle_height)):
+            try:
+                self.set(pre + key, val, kind)
+            except KeyError:  # not a parameter of this kind of primitive
+                pass
+        return name
+
+    def _tree(self, s) -> None:
+        """The scene's explicit objects tree as node_NNNN_* parameters: node i
+        (0-based) gets id i + 1 and display order i; its parent is the nearest
+        preceding node one level up."""
+        parents = []
+        for i in range(s.n_nodes):
+            nd = s.node[i]
+            nid = i + 1
+            if nid > 1:
+                self.add_node(nid)
+            while len(parents) > nd.level:
+                parents.pop()
+            parent = parents[-1] if parents else 0
+            pre = f"node_{nid:04d}_"
+            if nd.type == NODE_FRACTAL_T:
+                name, oid = "fractal", nd.index + 1
+            elif nd.type == NODE_PRIMITIVE_T:
+                q = s.primitive[nd.index]
+                oid = 200 + i
+                name = self._primitive(q, nd.index + 1, oid)
+                self.set(pre + "position", list(q.position), KIND_VEC3)
+                self.set(pre + "rotation", list(q.rotation), KIND_VEC3)
+                self.set(pre + "scale", q.scale, KIND_DOUBLE)
+                self.set(pre + "repeat", list(q.repeat), KIND_VEC3)
+            else:
+                name, oid = "group", 100 + i
+            self.set_string(pre + "definition", f"{name} {nid},{nid},{nd.type},{parent},{oid},{i}")
+            if nd.type != NODE_PRIMITIVE_T:
+                self.set(pre + "position", list(nd.position), KIND_VEC3)
+                self.set(pre + "rotation", list(nd.rotation), KIND_VEC3)
+                self.set(pre + "scale", nd.scale, KIND_DOUBLE)
+                self.set(pre + "repeat", list(nd.repeat), KIND_VEC3)
+            self.set(pre + "enabled", nd.enabled, KIND_BOOL)
+            self.set(pre + "detail_level_multiplier", nd.detail_level_multiplier, KIND_DOUBLE)
+            self.set(pre + "smooth_de_combine_enable", nd.smooth_combine, KIND_BOOL)
+            self.set(pre + "smooth_de_combine_distance", nd.smooth_combine_distance, KIND_DOUBLE)
+            self.set(pre + "formula_maxiter", nd.formula_maxiter, KIND_INT)
+            self.set(pre + "julia_mode", nd.julia_mode, KIND_BOOL)
+            self.set(pre + "julia_c", list(nd.julia_c), KIND_VEC3)
+            self.set(pre + "fractal_constant_factor", list(nd.fractal_constant_factor), KIND_VEC3)
+            self.set(pre + "initial_waxis", nd.initial_waxis, KIND_DOUBLE)
+            if nd.type in (11, 12, 13):
+                parents.append(nid)
 
     def prepare(self) -> None:
         if self.L.refp_prepare(self.h):
@@ -147,7 +228,7 @@ class RefPipeline:
         hybrid, settings.cpp:2700-2800)."""
         s = scene
         hybrid = bool(s.hybrid_fractal_enable)
-        n = s.n_fractals if hybrid else 1
+        n = s.n_fractals if (hybrid or s.n_nodes > 0) else 1
         for i in range(n):
             f = s.fractal[i]
             self.set("formula", f.formula, KIND_INT, i)
@@ -211,18 +292,21 @@ class RefPipeline:
         self.set("spherical_folding", s.spherical_folding, KIND_BOOL)
         self.set("spherical_folding_inner", s.spherical_folding_inner, KIND_DOUBLE)
         self.set("spherical_folding_outer", s.spherical_folding_outer, KIND_DOUBLE)
-        if hybrid:
-            self.set_string("node_0001_definition", f"hybrid 1,1,{NODE_HYBRID},0,-1")
-            for i in range(n):
-                nid = i + 2
-                self.add_node(nid)
-                self.set_string(f"node_{nid:04d}_definition", f"fractal {i + 1},{nid},{NODE_FRACTAL},1,{i + 1}")
-        node = "node_0001_"
-        self.set(node + "formula_maxiter", s.formula_maxiter, KIND_INT)
-        self.set(node + "julia_mode", s.julia_mode, KIND_BOOL)
-        self.set(node + "julia_c", list(s.julia_c), KIND_VEC3)
-        self.set(node + "fractal_constant_factor", list(s.fractal_constant_factor), KIND_VEC3)
-        self.set(node + "initial_waxis", s.initial_waxis, KIND_DOUBLE)
+        if s.n_nodes > 0:
+            self._tree(s)
+        else:
+            if hybrid:
+                self.set_string("node_0001_definition", f"hybrid 1,1,{NODE_HYBRID},0,-1")
+                for i in range(n):
+                    nid = i + 2
+                    self.add_node(nid)
+                    self.set_string(f"node_{nid:04d}_definition", f"fractal {i + 1},{nid},{NODE_FRACTAL},1,{i + 1}")
+            node = "node_0001_"
+            self.set(node + "formula_maxiter", s.formula_maxiter, KIND_INT)
+            self.set(node + "julia_mode", s.julia_mode, KIND_BOOL)
+            self.set(node + "julia_c", list(s.julia_c), KIND_VEC3)
+            self.set(node + "fractal_constant_factor", list(s.fractal_constant_factor), KIND_VEC3)
+            self.set(node + "initial_waxis", s.initial_waxis, KIND_DOUBLE)
         if camera is not None:
             c = camera
             self.set("camera", list(c.camera), KIND_VEC3)

@@ -14,6 +14,79 @@ def _box(**kw):
     return s
 
 
+def _node(node_type, index=0, level=0, pos=(0.0, 0.0, 0.0), rot=(0.0, 0.0, 0.0), scale=1.0, **kw):
+    n = abi.node_defaults(node_type, index, level)
+    n.position[:] = list(pos)
+    n.rotation[:] = list(rot)
+    n.scale = scale
+    for k, v in kw.items():
+        if isinstance(v, (list, tuple)):
+            getattr(n, k)[:] = list(v)
+        else:
+            setattr(n, k, v)
+    return n
+
+
+def _tree_scene(slots, prims, nodes, **kw):
+    s = abi.scene_defaults(slots[0][0])
+    s.n_fractals = len(slots)
+    for i, (formula, fkw) in enumerate(slots):
+        abi.fractal_defaults(s.fractal[i], formula)
+        for k, v in fkw.items():
+            setattr(s.fractal[i], k, v)
+    s.n_primitives = len(prims)
+    for i, (ptype, pkw) in enumerate(prims):
+        s.primitive[i] = abi.primitive_defaults(ptype)
+        for k, v in pkw.items():
+            if isinstance(v, (list, tuple)):
+                getattr(s.primitive[i], k)[:] = list(v)
+            else:
+                setattr(s.primitive[i], k, v)
+    s.n_nodes = len(nodes)
+    for i, n in enumerate(nodes):
+        s.node[i] = n
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def _trees():
+    F, P = abi.NODE_FRACTAL, abi.NODE_PRIMITIVE
+    ADD, MUL, SUB = abi.NODE_BOOLEAN_ADD, abi.NODE_BOOLEAN_MUL, abi.NODE_BOOLEAN_SUB
+    box = (abi.FORMULA_MANDELBOX, {"mandelbox_scale": -1.5})
+    bulb = (abi.FORMULA_MANDELBULB, {"bulb_power": 8.0})
+    menger = (abi.FORMULA_MENGER_SPONGE, {})
+    t = {}
+    t["tree_two_fractals"] = _tree_scene(
+        [box, bulb], [],
+        [_node(F, 0, 0, pos=(0.9, 0.0, 0.0), scale=0.5, formula_maxiter=30),
+         _node(F, 1, 0, pos=(-0.8, 0.1, 0.0), rot=(10.0, 20.0, 0.0), scale=0.7, formula_maxiter=20)])
+    t["tree_intersection"] = _tree_scene(
+        [box], [(abi.PRIMITIVE_SPHERE, {"radius": 1.4})],
+        [_node(MUL), _node(F, 0, 1, formula_maxiter=30), _node(P, 0, 1)])
+    t["tree_subtraction"] = _tree_scene(
+        [bulb], [(abi.PRIMITIVE_BOX, {"size": [0.8, 0.8, 3.0], "position": [0.3, 0.0, 0.0], "rotation": [0.0, 0.0, 30.0]})],
+        [_node(SUB), _node(F, 0, 1, formula_maxiter=20), _node(P, 0, 1)])
+    t["tree_smooth_nested"] = _tree_scene(
+        [box, menger], [(abi.PRIMITIVE_TORUS, {"radius": 0.9, "tube_radius": 0.25}),
+                        (abi.PRIMITIVE_CYLINDER, {"radius": 0.3, "height": 2.5})],
+        [_node(ADD, pos=(0.1, -0.2, 0.05), rot=(5.0, 0.0, 15.0), scale=1.2),
+         _node(F, 0, 1, scale=0.6, formula_maxiter=25, julia_mode=1, julia_c=[0.2, -0.1, 0.3]),
+         _node(P, 0, 1, smooth_combine=1, smooth_combine_distance=0.3),
+         _node(MUL, 0, 1, pos=(0.0, 0.4, 0.0)),
+         _node(F, 1, 2, scale=0.8, formula_maxiter=8, fractal_constant_factor=[1.1, 1.0, 0.9]),
+         _node(P, 1, 2, rot=(90.0, 0.0, 0.0))])
+    t["tree_repeat_detail"] = _tree_scene(
+        [bulb], [(abi.PRIMITIVE_PLANE, {"position": [0.0, 0.0, -1.2]})],
+        [_node(F, 0, 0, scale=0.3, repeat=[1.0, 1.0, 0.0], detail_level_multiplier=2.0, formula_maxiter=15),
+         _node(P, 0, 0)])
+    t["tree_disabled_branch"] = _tree_scene(
+        [box, bulb], [(abi.PRIMITIVE_SPHERE, {"radius": 0.5}), (abi.PRIMITIVE_SPHERE, {"radius": 0.4, "position": [1.5, 0.0, 0.0]})],
+        [_node(ADD), _node(F, 0, 1, formula_maxiter=30), _node(MUL, 0, 1, enabled=0), _node(F, 1, 2),
+         _node(P, 0, 2), _node(P, 1, 1)])
+    return t
+
+
 def cases():
     out = {}
     out["bulb_p8"] = configs.mandelbulb_scene(8.0, 250)
@@ -197,6 +270,9 @@ def cases():
     s.fractal[1].mandelbox_main_rotation_enabled = 1
     s.fractal[1].mandelbox_rotation_main[:] = [5.0, 9.0, -4.0]
     out["hybrid_bulb_rotated_box"] = s
+    # explicit objects trees (calculate_distance.cpp:225-516)
+    for name, tree in _trees().items():
+        out[name] = tree
     # quaternion (5) and aexion (19)
     s = abi.scene_defaults(abi.FORMULA_QUATERNION)
     s.formula_maxiter = 40
@@ -311,4 +387,11 @@ def render_cases():
     sc.deltade_relative_delta = 0.02
     p.advanced_quality = 1  # the offset is deltade_relative_delta of the detail size
     out.append(("bulb_delta_de_advanced_quality", sc, cam, p))
+    trees = _trees()
+    out.append(("tree_intersection", trees["tree_intersection"], configs.camera((0.3, -3.5, 1.2), width=32, height=24),
+                params()))
+    out.append(("tree_smooth_nested", trees["tree_smooth_nested"],
+                configs.camera((1.0, -10.0, 2.0), width=32, height=24), params()))
+    out.append(("tree_subtraction", trees["tree_subtraction"], configs.camera((0.0, -3.0, 0.3), width=32, height=24),
+                params(soft_shadow_cone=15.0)))
     return out
