@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define MBR_ABI_VERSION 5
+#define MBR_ABI_VERSION 6
 
 /* Number of formula slots of one hybrid sequence (the reference's nine
  * fractal tabs; "repeat_from" is limited to 1..9, src/initparameters.cpp:151). */
@@ -64,7 +64,9 @@ typedef enum mbr_formula {
   MBR_FORMULA_KALEIDOSCOPIC_IFS = 10, /* formula/definition/fractal_kaleidoscopic_ifs.cpp:30-85 */
   MBR_FORMULA_XENODREAMBUIE = 11, /* formula/definition/fractal_xenodreambuie.cpp:30-49; Mandelbulb parameters */
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
-  MBR_FORMULA_MANDELBOX = 8     /* formula/definition/fractal_mandelbox.cpp:31-107 */
+  MBR_FORMULA_MANDELBOX = 8,    /* formula/definition/fractal_mandelbox.cpp:31-107 */
+  /* formulas whose parameters are passed by settings key (mbr_fractal.param) */
+  MBR_FORMULA_PSEUDO_KLEINIAN = 103 /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
 } mbr_formula;
 
 /* fractal::enumDEFunctionType (src/fractal_enums.h:47-60).  The Jos
@@ -127,6 +129,16 @@ typedef enum mbr_refine {
  * that the three supported formulas read.  Angles are in degrees, as in the
  * settings file; the library converts them like
  * sFractal::RecalculateFractalParams (src/fractal.cpp:653-678). */
+/* One formula parameter by its settings key (see mbr_fractal.param).
+ * Integers and booleans (0 / 1) use value[0]; vectors use value[0..2];
+ * rotations are vectors of angles in degrees. */
+#define MBR_MAX_FORMULA_PARAMS 48
+#define MBR_PARAM_KEY_LEN 48
+typedef struct mbr_formula_param {
+  char key[MBR_PARAM_KEY_LEN];               /* NUL-terminated */
+  double value[3];
+} mbr_formula_param;
+
 typedef struct mbr_fractal {
   int32_t formula;                 /* mbr_formula */
   int32_t formula_iterations;      /* "formula_iterations", default 1 */
@@ -186,6 +198,16 @@ typedef struct mbr_fractal {
   int32_t reserved_ade;
   double analytic_de_scale1;                 /* "analyticDE_scale_1", default 1 */
   double analytic_de_offset1;                /* "analyticDE_offset_1", default 1 */
+  /* Formula parameters by settings key, for the formulas listed after the
+   * Mandelbox in mbr_formula: each entry names one parameter of the fractal
+   * container (sFractal, src/fractal.cpp:47-720, e.g.
+   * "transf_addition_constant_0777", "analyticDE_tweak_005") and its value;
+   * a parameter not listed keeps the reference's default
+   * (InitFractalParams, src/initparameters.cpp:700-1300).  A key the slot's
+   * formula does not read makes mbr_scene_set fail with MBR_EINVAL. */
+  int32_t n_params;                          /* 0..MBR_MAX_FORMULA_PARAMS */
+  int32_t reserved_params;
+  mbr_formula_param param[MBR_MAX_FORMULA_PARAMS];
 } mbr_fractal;
 
 /* Primitive kinds (fractal::enumObjectType primitives, src/primitive.cpp) */

@@ -28,6 +28,10 @@ STATUS_NAMES = {0: "MBR_OK", 1: "MBR_EINVAL", 2: "MBR_ECUDA", 3: "MBR_ETIMEOUT",
 FORMULA_NONE, FORMULA_MANDELBULB, FORMULA_MENGER_SPONGE, FORMULA_MANDELBOX = 0, 2, 7, 8
 FORMULA_MANDELBULB_POWER2, FORMULA_HYPERCOMPLEX, FORMULA_KALEIDOSCOPIC_IFS, FORMULA_XENODREAMBUIE = 3, 4, 10, 11
 FORMULA_QUATERNION, FORMULA_AEXION = 5, 19
+# formulas whose parameters are passed by settings key (Fractal.param)
+FORMULA_PSEUDO_KLEINIAN = 103
+MBR_MAX_FORMULA_PARAMS = 48
+MBR_PARAM_KEY_LEN = 48
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)
 # mbr_primitive_type
 (PRIMITIVE_PLANE, PRIMITIVE_BOX, PRIMITIVE_SPHERE, PRIMITIVE_WATER, PRIMITIVE_TORUS, PRIMITIVE_CYLINDER,
@@ -50,6 +54,10 @@ GRAD_CAMERA_X, GRAD_CAMERA_Y, GRAD_CAMERA_Z, GRAD_YAW, GRAD_COUNT = 3, 4, 5, 6, 
 D3 = C.c_double * 3
 
 
+class FormulaParam(C.Structure):
+    _fields_ = [("key", C.c_char * MBR_PARAM_KEY_LEN), ("value", D3)]
+
+
 class Fractal(C.Structure):
     _fields_ = [
         ("formula", C.c_int32), ("formula_iterations", C.c_int32), ("formula_start_iteration", C.c_int32),
@@ -70,7 +78,31 @@ class Fractal(C.Structure):
         ("ifs_intensity", C.c_double * 9),
         ("aexion_cadd", C.c_double), ("analytic_de_enabled", C.c_int32), ("reserved_ade", C.c_int32),
         ("analytic_de_scale1", C.c_double), ("analytic_de_offset1", C.c_double),
+        ("n_params", C.c_int32), ("reserved_params", C.c_int32),
+        ("param", FormulaParam * MBR_MAX_FORMULA_PARAMS),
     ]
+
+    def set_param(self, key: str, value) -> None:
+        """Sets formula parameter `key` (the reference's settings name) to a
+        number, a bool or a 3-vector, replacing an earlier value of the key."""
+        v = list(value) if isinstance(value, (list, tuple)) else [float(value), 0.0, 0.0]
+        k = key.encode()
+        if len(k) >= MBR_PARAM_KEY_LEN:
+            raise ValueError(f"parameter key longer than {MBR_PARAM_KEY_LEN - 1} bytes: {key}")
+        for i in range(self.n_params):
+            if self.param[i].key == k:
+                self.param[i].value[:] = [float(x) for x in v]
+                return
+        if self.n_params >= MBR_MAX_FORMULA_PARAMS:
+            raise ValueError("too many formula parameters")
+        p = self.param[self.n_params]
+        p.key = k
+        p.value[:] = [float(x) for x in v]
+        self.n_params += 1
+
+    def params(self) -> dict:
+        """The listed formula parameters, key -> (x, y, z)."""
+        return {self.param[i].key.decode(): tuple(self.param[i].value) for i in range(self.n_params)}
 
 
 class Primitive(C.Structure):

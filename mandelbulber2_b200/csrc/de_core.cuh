@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include "formula_params.h"
 #include "mbr_device.h"
 
 namespace mbr {
@@ -297,6 +298,109 @@ __device__ __forceinline__ void f_aexion(V4<T> &z, T r, T &DE, const DevSlot &s,
   }
 }
 
+// std::max(a, b) of the reference: b when a < b, else a.
+template <class T>
+__device__ __forceinline__ T smax(T a, T b) {
+  return (a < b) ? b : a;
+}
+
+// sign() of math_utilities.h:65-67: -1, 0 or 1
+template <class T>
+__device__ __forceinline__ T sgn_of(T v) {
+  return (T(0.0) < v) ? T(1.0) : ((v < T(0.0)) ? T(-1.0) : T(0.0));
+}
+
+// cFractalPseudoKleinian::FormulaCode (fractal_pseudo_kleinian.cpp:30-202)
+// from the slot's keyed block (PseudoKleinianX); the aux.color terms are not
+// computed.  pk: aux.pseudoKleinianDE, which the pseudo-Kleinian DE function
+// reads.
+template <class T>
+__device__ __noinline__ void f_pseudo_kleinian(V4<T> &z, T &DE, T &pk, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (x[PKX_SPH_INV] != 0.0 && i >= int(x[PKX_START_X]) && i < int(x[PKX_STOP_1])) {  // :33-44
+    z.x = z.x + T(x[PKX_OFFSET000]);
+    z.y = z.y + T(x[PKX_OFFSET000 + 1]);
+    z.z = z.z + T(x[PKX_OFFSET000 + 2]);
+    const T rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const T q = T(x[PKX_MAXR2]) / rr;
+    z.x = z.x * q;
+    z.y = z.y * q;
+    z.z = z.z * q;
+    z.w = z.w * q;
+    z.x = z.x + T(x[PKX_ADD_A000] - x[PKX_OFFSET000]);
+    z.y = z.y + T(x[PKX_ADD_A000 + 1] - x[PKX_OFFSET000 + 1]);
+    z.z = z.z + T(x[PKX_ADD_A000 + 2] - x[PKX_OFFSET000 + 2]);
+    DE = DE * (T(x[PKX_MAXR2]) / rr) + T(x[PKX_DE_OFFSET0]);
+  }
+  if (x[PKX_PRISM] != 0.0 && i >= int(x[PKX_START_P]) && i < int(x[PKX_STOP_P1])) {  // prism shape :47-75
+    z.y = m_abs(z.y);
+    z.z = m_abs(z.z);
+    const T dot1 = (z.x * T(-0.86602540378443864676372317075294) + z.y * T(0.5)) * T(x[PKX_SCALE]);
+    T t = smax(T(0.0), dot1);
+    z.x = z.x - t * T(-1.73205080756887729352744634150587);
+    z.y = m_abs(T(z.y - t));
+    if (z.y > z.z) {
+      t = z.y;
+      z.y = z.z;
+      z.z = t;
+    }
+    z.x = z.x - T(x[PKX_CMUL000] * 0.86602540378443864676372317075294);
+    z.y = z.y - T(x[PKX_CMUL000 + 1] * 1.5);
+    z.z = z.z - T(x[PKX_CMUL000 + 2] * 1.5);
+    if (z.z > z.x) {
+      t = z.z;
+      z.z = z.x;
+      z.x = t;
+    }
+    if (z.x > T(0.0)) {
+      z.y = smax(T(0.0), z.y);
+      z.z = smax(T(0.0), z.z);
+    }
+  }
+  if (x[PKX_ABS_BOX] != 0.0 && i >= int(x[PKX_START_E]) && i < int(x[PKX_STOP_E])) {  // abs box fold :78-91
+    const T ax = T(x[PKX_ADD111]), ay = T(x[PKX_ADD111 + 1]), az = T(x[PKX_ADD111 + 2]);
+    z.x = m_abs(T(z.x + ax)) - m_abs(T(z.x - ax)) - z.x;
+    z.y = m_abs(T(z.y + ay)) - m_abs(T(z.y - ay)) - z.y;
+    if (x[PKX_ABS_BOX_Z] != 0.0) z.z = m_abs(T(z.z + az)) - m_abs(T(z.z - az)) - z.z;
+  }
+  if (x[PKX_BOX] != 0.0 && i >= int(x[PKX_START_A]) && i < int(x[PKX_STOP_A])) {  // box fold :94-115
+    const T limit = T(x[PKX_MB_LIMIT]), value = T(x[PKX_MB_VALUE]);
+    if (m_abs(z.x) > limit) z.x = sgn_of(z.x) * value - z.x;
+    if (m_abs(z.y) > limit) z.y = sgn_of(z.y) * value - z.y;
+    const T zLimit = T(x[PKX_MB_LIMIT] * x[PKX_SCALE1]);
+    const T zValue = T(x[PKX_MB_VALUE] * x[PKX_SCALE1]);
+    if (m_abs(z.z) > zLimit) z.z = sgn_of(z.z) * zValue - z.z;
+  }
+  if (i >= int(x[PKX_START_C]) && i < int(x[PKX_STOP_C])) {  // the Kleinian fold :118-138
+    const T cx = T(x[PKX_CSIZE]), cy = T(x[PKX_CSIZE + 1]), cz = T(x[PKX_CSIZE + 2]);
+    V4<T> t = z;
+    if (z.x > cx) t.x = cx;
+    if (z.x < -cx) t.x = -cx;
+    if (z.y > cy) t.y = cy;
+    if (z.y < -cy) t.y = -cy;
+    if (z.z > cz) t.z = cz;
+    if (z.z < -cz) t.z = -cz;
+    z.x = t.x * T(2.0) - z.x;
+    z.y = t.y * T(2.0) - z.y;
+    z.z = t.z * T(2.0) - z.z;
+    z.w = t.w * T(2.0) - z.w;
+    const T k = smax(T(T(x[PKX_MINR05]) / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), T(1.0));
+    z.x = z.x * k;
+    z.y = z.y * k;
+    z.z = z.z * k;
+    z.w = z.w * k;
+    if (x[PKX_FLIP_Z] != 0.0) z.z = -z.z;
+    if (x[PKX_FLIP_W] != 0.0) z.w = -z.w;
+    DE = DE * (k + T(x[PKX_TWEAK005]));
+    pk = T(x[PKX_DE_SCALE1]);
+  }
+  if (x[PKX_ROT_ON] != 0.0 && i >= int(x[PKX_START_R]) && i < int(x[PKX_STOP_R]) && x[PKX_ROT] == 0.0)
+    z = mb_turn<T>(x + PKX_ROT + 1, false, z);  // :141-144 (the matrix's zero flag first)
+  z.x = z.x + T(x[PKX_ADD000]);  // :147
+  z.y = z.y + T(x[PKX_ADD000 + 1]);
+  z.z = z.z + T(x[PKX_ADD000 + 2]);
+}
+
 // cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
 // over the enabled vectors of the scene's IFS block; the 4-vector terms with
 // w keep the reference's operations (its direction and offset have w = 0)
@@ -353,9 +457,10 @@ __device__ __forceinline__ void f_ifs(V4<T> &z, T &DE, const IfsBlock &b) {
 // replaces at its first iteration.
 template <class T, bool W, bool EXT = false>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
-                                                 const MbRot *rot, const IfsBlock *ifs, int i, V4<T> &c) {
+                                                 const MbRot *rot, const IfsBlock *ifs, int i, V4<T> &c, T &pk) {
   if constexpr (EXT) {
     switch (formula) {
+      case MBR_FORMULA_PSEUDO_KLEINIAN: f_pseudo_kleinian<T>(z, DE, pk, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
       case MBR_FORMULA_AEXION: f_aexion<T>(z, r, DE, s, i, c); break;
       case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;
@@ -414,11 +519,6 @@ __device__ __forceinline__ T node_juliac(const DevNode &nd, int k) {
   return T(nd.julia_c[k] * nd.cmul[k]);
 }
 
-// std::max(a, b) of the reference: b when a < b, else a.
-template <class T>
-__device__ __forceinline__ T smax(T a, T b) {
-  return (a < b) ? b : a;
-}
 
 // One component of CVector3::repeatMod (algebra.hpp:106-115): ((p - v/2) % v
 // + v) % v - v/2, with % the fmod of a positive period.
@@ -611,15 +711,17 @@ __device__ __forceinline__ void global_folds(const DevScene &sc, V4<T> &z, T &r,
 // the derivative DE and the orbit's maxiter flag.
 template <class T, int F, bool W, bool TREE = false>
 __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T pz, int maxN, V4<T> &z, T &r, T &DE,
-                                             bool &maxiter, const DevNode *nd = nullptr) {
+                                             bool &maxiter, const DevNode *nd = nullptr, T *pk_out = nullptr) {
   z = V4<T>{px, py, pz, W ? T(TREE ? nd->w0 : sc.w0) : T(0.0)};
   V4<T> c = z;  // aux.const_c
   r = len4<T, W>(z);
   DE = T(1.0);
-  V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)};
+  T pk = T(1.0);  // aux.pseudoKleinianDE (compute_fractal.cpp:120)
+  V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)}, lastLastZ = lastZ;
   maxiter = true;
   int i;
   for (i = 0; i < maxN; i++) {
+    lastLastZ = lastZ;
     lastZ = z;
     const int k = TREE ? nd->slot : ((F > 0) ? 0 : ((i < sc.length) ? int(sc.seq[i]) : int(sc.seq[0])));
     const DevSlot &s = sc.slot[k];
@@ -631,7 +733,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
       if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c);
+      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c, pk);
     }
     if (s.add_c) {
       if (TREE ? nd->julia : sc.julia) {
@@ -663,7 +765,17 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
       maxiter = false;
       break;
     }
+    // the convergence bailout of pseudo- and Jos-Kleinian formulas
+    // (compute_fractal.cpp:323-336; hybrid_fractal_sequences.cpp:242-246)
+    if (F == F_EXT && s.check_bailout && s.add_bail) {
+      maxiter = false;
+      const T lim = T(0.1 / s.d[P_BAILOUT]);
+      if (len4<T, W>(V4<T>{z.x - lastZ.x, z.y - lastZ.y, z.z - lastZ.z, z.w - lastZ.w}) / r < lim) break;
+      if (len4<T, W>(V4<T>{z.x - lastLastZ.x, z.y - lastLastZ.y, z.z - lastLastZ.z, z.w - lastLastZ.w}) / r < lim)
+        break;
+    }
   }
+  if (pk_out) *pk_out = pk;
   return i;
 }
 
@@ -671,7 +783,8 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
 // The specialised iterations carry linear, logarithmic and IFS; the extended
 // one every DevDeFinal code.
 template <class T, int F, bool W>
-__device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE, int de_final = -1) {
+__device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE, int de_final = -1,
+                                            T pk = T(1.0)) {
   if (!(DE > T(0.0))) return r;
   if (F == F_EXT) {
     switch (de_final >= 0 ? de_final : sc.de_final) {
@@ -679,9 +792,9 @@ __device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, 
       case DEF_LOG: return (r > T(1.0)) ? T(T(0.5) * r * m_log(r) / DE) : T(0.0);
       case DEF_LINEAR: return r / DE;
       case DEF_IFS: return (r - T(2.0)) / DE;
-      case DEF_PSEUDO_KLEINIAN: {  // aux.pseudoKleinianDE keeps its initial 1 (compute_fractal.cpp:120)
+      case DEF_PSEUDO_KLEINIAN: {  // pk: aux.pseudoKleinianDE, 1 unless a pseudo-Kleinian formula set it
         const T rxy = m_sqrt(z.x * z.x + z.y * z.y);
-        return smax(T(rxy - T(1.0)), T(m_abs(rxy * z.z) / r)) / DE;
+        return smax(T(rxy - pk), T(m_abs(rxy * z.z) / r)) / DE;
       }
       case DEF_CUSTOM: return T(1000.0);  // aux.dist (:119)
       case DEF_MAX_AXIS: {
@@ -812,11 +925,11 @@ __device__ __forceinline__ T calc_distance_simple(const DevScene &sc, T px, T py
   }
   const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
   V4<T> z;
-  T r, DE;
+  T r, DE, pk;
   bool maxiter;
   const int i = compute_orbit<T, F, W, TREE>(sc, px, py, pz, (TREE ? nd->maxN : sc.formula_maxiter) * mult, z, r,
-                                             DE, maxiter, nd);
-  T distance = final_distance<T, F, W>(sc, z, r, DE, TREE ? nd->de_final : -1);
+                                             DE, maxiter, nd, &pk);
+  T distance = final_distance<T, F, W>(sc, z, r, DE, TREE ? nd->de_final : -1, pk);
   const int iters = i + 1;
   *iters_out = iters;
   if (total_out) *total_out = iters;

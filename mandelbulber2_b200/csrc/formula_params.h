@@ -1,0 +1,229 @@
+// formula_params.h - the formulas whose parameters come by settings key
+// (mbr_fractal.param): for each, the keys it reads with the reference's
+// defaults (InitFractalParams, src/initparameters.cpp) and the layout of the
+// values in a slot's parameter block DevSlot::x.
+//
+// A value's kind fixes how many x[] entries it takes: an int, a double or a
+// bool (0 / 1) one; a vector three; a rotation ten - the zero flag of
+// CRotationMatrix and the 3x3 matrix of SetRotation2(angles * pi / 180)
+// (src/algebra.cpp:296-302, as sFractal::RecalculateFractalParams builds
+// transformCommon.rotationMatrix, src/fractal.cpp:696), row-major.
+#pragma once
+#include <cmath>
+
+#include "../../include/mbr.h"
+
+#define MBR_SLOT_X 64  // entries of a slot's keyed parameter block
+
+namespace mbr {
+
+enum ParamKind { PK_INT = 0, PK_DOUBLE = 1, PK_BOOL = 2, PK_VEC3 = 3, PK_ROT = 4 };
+
+// cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
+// 30-202): sphere inversion, prism shape, abs-box and box folds, the
+// Kleinian fold, rotation and offset.  The box fold reads the slot's
+// mandelbox_folding_limit / _value and the Kleinian fold its
+// analytic_de_scale1 (mbr_fractal fields, after the keyed block).
+enum PseudoKleinianX {
+  PKX_SPH_INV = 0,                  // transf_sphere_inversion_enabled_false
+  PKX_START_X = 1,                  // transf_start_iterations_X
+  PKX_STOP_1 = 2,                   // transf_stop_iterations_1
+  PKX_OFFSET000 = 3,                // transf_offset_000 (3)
+  PKX_MAXR2 = 6,                    // transf_maxR2_1
+  PKX_ADD_A000 = 7,                 // transf_addition_constantA_000 (3)
+  PKX_DE_OFFSET0 = 10,              // analyticDE_offset_0
+  PKX_PRISM = 11,                   // transf_function_enabledP_false
+  PKX_START_P = 12,                 // transf_start_iterations_P
+  PKX_STOP_P1 = 13,                 // transf_stop_iterations_P1
+  PKX_SCALE = 14,                   // transf_scale
+  PKX_CMUL000 = 15,                 // transf_constant_multiplier_000 (3)
+  PKX_ABS_BOX = 18,                 // transf_function_enabledBy_false
+  PKX_START_E = 19,                 // transf_start_iterations_E
+  PKX_STOP_E = 20,                  // transf_stop_iterations_E
+  PKX_ADD111 = 21,                  // transf_addition_constant_111 (3)
+  PKX_ABS_BOX_Z = 24,               // transf_function_enabledBy
+  PKX_BOX = 25,                     // transf_function_enabledBx_false
+  PKX_START_A = 26,                 // transf_start_iterations_A
+  PKX_STOP_A = 27,                  // transf_stop_iterations_A
+  PKX_SCALE1 = 28,                  // transf_scale_1
+  PKX_CSIZE = 29,                   // transf_addition_constant_0777 (3)
+  PKX_START_C = 32,                 // transf_start_iterations_C
+  PKX_STOP_C = 33,                  // transf_stop_iterations_C
+  PKX_MINR05 = 34,                  // transf_minimum_radius_05
+  PKX_FLIP_Z = 35,                  // transf_function_enabledN_false
+  PKX_FLIP_W = 36,                  // transf_function_enabledw_false
+  PKX_TWEAK005 = 37,                // analyticDE_tweak_005
+  PKX_ROT_ON = 38,                  // transf_function_enabledR_false
+  PKX_START_R = 39,                 // transf_start_iterations_R
+  PKX_STOP_R = 40,                  // transf_stop_iterations_R
+  PKX_ROT = 41,                     // transf_rotation (10)
+  PKX_ADD000 = 51,                  // transf_addition_constant (3)
+  PKX_KEYED_END = 54,               // the keyed block ends here
+  PKX_MB_LIMIT = 54,                // mandelbox_folding_limit (mbr_fractal field)
+  PKX_MB_VALUE = 55,                // mandelbox_folding_value (mbr_fractal field)
+  PKX_DE_SCALE1 = 56,               // analyticDE_scale_1 (mbr_fractal analytic_de_scale1)
+  PKX_COUNT = 57
+};
+static_assert(PKX_COUNT <= MBR_SLOT_X, "pseudo-Kleinian block exceeds the slot's parameter block");
+
+#ifndef __CUDA_ARCH__
+struct FormulaKey {
+  const char *key;
+  int kind;
+  double def[3];
+  int x;  // first x[] entry
+};
+
+constexpr int param_kind_size(int kind) { return kind == PK_VEC3 ? 3 : (kind == PK_ROT ? 10 : 1); }
+
+// true when the table's entries follow one another in x[] from 0 to end
+template <int N>
+constexpr bool keys_contiguous(const FormulaKey (&t)[N], int end) {
+  int o = 0;
+  for (int i = 0; i < N; i++) {
+    if (t[i].x != o) return false;
+    o += param_kind_size(t[i].kind);
+  }
+  return o == end;
+}
+
+constexpr FormulaKey kPseudoKleinianKeys[] = {
+    {"transf_sphere_inversion_enabled_false", PK_BOOL, {0, 0, 0}, PKX_SPH_INV},
+    {"transf_start_iterations_X", PK_INT, {0, 0, 0}, PKX_START_X},
+    {"transf_stop_iterations_1", PK_INT, {1, 0, 0}, PKX_STOP_1},
+    {"transf_offset_000", PK_VEC3, {0, 0, 0}, PKX_OFFSET000},
+    {"transf_maxR2_1", PK_DOUBLE, {1, 0, 0}, PKX_MAXR2},
+    {"transf_addition_constantA_000", PK_VEC3, {0, 0, 0}, PKX_ADD_A000},
+    {"analyticDE_offset_0", PK_DOUBLE, {0, 0, 0}, PKX_DE_OFFSET0},
+    {"transf_function_enabledP_false", PK_BOOL, {0, 0, 0}, PKX_PRISM},
+    {"transf_start_iterations_P", PK_INT, {0, 0, 0}, PKX_START_P},
+    {"transf_stop_iterations_P1", PK_INT, {1, 0, 0}, PKX_STOP_P1},
+    {"transf_scale", PK_DOUBLE, {1, 0, 0}, PKX_SCALE},
+    {"transf_constant_multiplier_000", PK_VEC3, {0, 0, 0}, PKX_CMUL000},
+    {"transf_function_enabledBy_false", PK_BOOL, {0, 0, 0}, PKX_ABS_BOX},
+    {"transf_start_iterations_E", PK_INT, {0, 0, 0}, PKX_START_E},
+    {"transf_stop_iterations_E", PK_INT, {250, 0, 0}, PKX_STOP_E},
+    {"transf_addition_constant_111", PK_VEC3, {1, 1, 1}, PKX_ADD111},
+    {"transf_function_enabledBy", PK_BOOL, {1, 0, 0}, PKX_ABS_BOX_Z},
+    {"transf_function_enabledBx_false", PK_BOOL, {0, 0, 0}, PKX_BOX},
+    {"transf_start_iterations_A", PK_INT, {0, 0, 0}, PKX_START_A},
+    {"transf_stop_iterations_A", PK_INT, {250, 0, 0}, PKX_STOP_A},
+    {"transf_scale_1", PK_DOUBLE, {1, 0, 0}, PKX_SCALE1},
+    {"transf_addition_constant_0777", PK_VEC3, {0.7, 0.7, 0.7}, PKX_CSIZE},
+    {"transf_start_iterations_C", PK_INT, {0, 0, 0}, PKX_START_C},
+    {"transf_stop_iterations_C", PK_INT, {250, 0, 0}, PKX_STOP_C},
+    {"transf_minimum_radius_05", PK_DOUBLE, {0.5, 0, 0}, PKX_MINR05},
+    {"transf_function_enabledN_false", PK_BOOL, {0, 0, 0}, PKX_FLIP_Z},
+    {"transf_function_enabledw_false", PK_BOOL, {0, 0, 0}, PKX_FLIP_W},
+    {"analyticDE_tweak_005", PK_DOUBLE, {0.05, 0, 0}, PKX_TWEAK005},
+    {"transf_function_enabledR_false", PK_BOOL, {0, 0, 0}, PKX_ROT_ON},
+    {"transf_start_iterations_R", PK_INT, {0, 0, 0}, PKX_START_R},
+    {"transf_stop_iterations_R", PK_INT, {250, 0, 0}, PKX_STOP_R},
+    {"transf_rotation", PK_ROT, {0, 0, 0}, PKX_ROT},
+    {"transf_addition_constant", PK_VEC3, {0, 0, 0}, PKX_ADD000},
+};
+static_assert(keys_contiguous(kPseudoKleinianKeys, PKX_KEYED_END), "pseudo-Kleinian keys and x[] layout disagree");
+
+struct KeyTable {
+  const FormulaKey *keys;
+  int n;
+};
+
+// the key table of a keyed formula; n = 0 for the others
+inline KeyTable formula_keys(int formula) {
+  switch (formula) {
+    case MBR_FORMULA_PSEUDO_KLEINIAN:
+      return {kPseudoKleinianKeys, int(sizeof(kPseudoKleinianKeys) / sizeof(kPseudoKleinianKeys[0]))};
+    default: return {nullptr, 0};
+  }
+}
+
+// The entry of `key` in the table, or -1.
+inline int find_key(const KeyTable &t, const char *key) {
+  for (int i = 0; i < t.n; i++) {
+    const char *a = t.keys[i].key;
+    const char *b = key;
+    while (*a && *a == *b) {
+      a++;
+      b++;
+    }
+    if (*a == 0 && *b == 0) return i;
+  }
+  return -1;
+}
+
+// CRotationMatrix::SetRotation2(deg * M_PI_180) (src/algebra.cpp:198-247,
+// 296-302): from the identity, rotations about z, y and x by the vector's z,
+// y and x angles multiplied onto the right, each skipped for a zero angle.
+// out[0]: 1 when every angle is zero (RotateVector returns its argument),
+// out[1..9]: the matrix, row-major.
+inline void keyed_rotation(const double deg[3], double *out) {
+  const double k = 0.01745329251994329576923690768489;  // M_PI_180 (fractal.h:45-46)
+  double m[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  bool zero = true;
+  for (int axis = 2; axis >= 0; axis--) {
+    const double a = deg[axis] * k;
+    if (a == 0.0) continue;
+    const double sn = std::sin(a), cs = std::cos(a);
+    double r[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (axis == 0) { r[0] = 1.0; r[4] = cs; r[8] = cs; r[5] = -sn; r[7] = sn; }
+    if (axis == 1) { r[4] = 1.0; r[8] = cs; r[0] = cs; r[6] = -sn; r[2] = sn; }
+    if (axis == 2) { r[8] = 1.0; r[0] = cs; r[4] = cs; r[1] = -sn; r[3] = sn; }
+    double t[9];
+    for (int row = 0; row < 3; row++)
+      for (int col = 0; col < 3; col++)
+        t[row * 3 + col] = m[row * 3 + 0] * r[col] + m[row * 3 + 1] * r[3 + col] + m[row * 3 + 2] * r[6 + col];
+    for (int j = 0; j < 9; j++) m[j] = t[j];
+    zero = false;
+  }
+  out[0] = zero ? 1.0 : 0.0;
+  for (int j = 0; j < 9; j++) out[1 + j] = m[j];
+}
+
+// One value into x[] as its kind stores it: an int truncated toward zero
+// (as cParameterContainer::Set<int> of the double), a bool 0 / 1.
+inline void put_keyed(const FormulaKey &k, const double *v, double *x) {
+  switch (k.kind) {
+    case PK_INT: x[k.x] = double(int(v[0])); break;
+    case PK_BOOL: x[k.x] = v[0] != 0.0 ? 1.0 : 0.0; break;
+    case PK_VEC3: x[k.x] = v[0]; x[k.x + 1] = v[1]; x[k.x + 2] = v[2]; break;
+    case PK_ROT: keyed_rotation(v, x + k.x); break;
+    default: x[k.x] = v[0]; break;
+  }
+}
+
+// The parameter block of a keyed formula: every key's default, then the
+// values f.param lists, then the values the formula reads from mbr_fractal's
+// named fields.  Returns -1 when the block is filled, else the index of the
+// first entry of f.param that is malformed (a key without its NUL, one the
+// formula does not read, a non-finite value or an int out of range); -2 when
+// n_params is out of range.
+inline int pack_keyed(const mbr_fractal &f, double *x) {
+  for (int j = 0; j < MBR_SLOT_X; j++) x[j] = 0.0;
+  const KeyTable t = formula_keys(f.formula);
+  if (f.n_params < 0 || f.n_params > MBR_MAX_FORMULA_PARAMS) return -2;
+  for (int i = 0; i < t.n; i++) put_keyed(t.keys[i], t.keys[i].def, x);
+  for (int j = 0; j < f.n_params; j++) {
+    const mbr_formula_param &q = f.param[j];
+    bool terminated = false;
+    for (int c = 0; c < MBR_PARAM_KEY_LEN; c++)
+      if (q.key[c] == 0) terminated = true;
+    if (!terminated) return j;
+    const int i = find_key(t, q.key);
+    if (i < 0) return j;
+    const int nv = t.keys[i].kind == PK_VEC3 || t.keys[i].kind == PK_ROT ? 3 : 1;
+    for (int c = 0; c < nv; c++)
+      if (!std::isfinite(q.value[c])) return j;
+    if (t.keys[i].kind == PK_INT && !(q.value[0] > -2147483648.0 && q.value[0] < 2147483648.0)) return j;
+    put_keyed(t.keys[i], q.value, x);
+  }
+  if (f.formula == MBR_FORMULA_PSEUDO_KLEINIAN) {
+    x[PKX_MB_LIMIT] = f.mandelbox_folding_limit;
+    x[PKX_MB_VALUE] = f.mandelbox_folding_value;
+    x[PKX_DE_SCALE1] = f.analytic_de_scale1;
+  }
+  return -1;
+}
+#endif
+
+}  // namespace mbr

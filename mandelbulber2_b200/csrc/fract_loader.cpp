@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "../../include/mbr.h"
+#include "formula_params.h"
 
 namespace {
 
@@ -459,7 +460,38 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
   } else if (name == "formula_stop_iteration") {
     if (parse_int(value, b)) f.formula_stop_iteration = b; else R.bad(name, value);
   } else {
-    R.ignored.push_back("fractal_" + std::to_string(slot + 1) + "." + name);
+    // a parameter the slot's formula reads by key (formula_params.h)
+    const mbr::KeyTable t = mbr::formula_keys(R.formula[slot]);
+    const int k = mbr::find_key(t, name.c_str());
+    if (k < 0) {
+      R.ignored.push_back("fractal_" + std::to_string(slot + 1) + "." + name);
+      return;
+    }
+    double val[3] = {0.0, 0.0, 0.0};
+    bool ok;
+    switch (t.keys[k].kind) {
+      case mbr::PK_INT: ok = parse_int(value, b); val[0] = b; break;
+      case mbr::PK_BOOL: ok = parse_bool(value, b); val[0] = b; break;
+      case mbr::PK_VEC3:
+      case mbr::PK_ROT: ok = parse_vec3(value, val); break;
+      default: ok = parse_double(value, val[0]); break;
+    }
+    if (!ok) {
+      R.bad(name, value);
+      return;
+    }
+    int j = 0;
+    while (j < f.n_params && std::strcmp(f.param[j].key, name.c_str()) != 0) j++;
+    if (j == f.n_params) {
+      if (f.n_params == MBR_MAX_FORMULA_PARAMS) {
+        R.unsupported.push_back("fractal_" + std::to_string(slot + 1) + "." + name + " (more than " +
+                                std::to_string(MBR_MAX_FORMULA_PARAMS) + " formula parameters)");
+        return;
+      }
+      std::snprintf(f.param[j].key, MBR_PARAM_KEY_LEN, "%s", name.c_str());
+      f.n_params++;
+    }
+    std::memcpy(f.param[j].value, val, sizeof(val));
   }
 }
 
@@ -854,11 +886,12 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     if (f == MBR_FORMULA_NONE) continue;
     if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE &&
         f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS &&
-        f != MBR_FORMULA_XENODREAMBUIE && f != MBR_FORMULA_QUATERNION && f != MBR_FORMULA_AEXION)
+        f != MBR_FORMULA_XENODREAMBUIE && f != MBR_FORMULA_QUATERNION && f != MBR_FORMULA_AEXION &&
+        mbr::formula_keys(f).n == 0)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " " + std::to_string(f) +
                               " (formula not built here: 2 Mandelbulb, 3 Mandelbulb power 2, 4 hypercomplex, "
                               "5 quaternion, 7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie, "
-                              "19 aexion are)");
+                              "19 aexion, 103 pseudo-Kleinian are)");
     if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && n_ifs > 1)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in more than one slot)");
     if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");

@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include "../../include/mbr.h"
+#include "formula_params.h"
 
 namespace mbr {
 
@@ -44,8 +45,11 @@ struct DevSlot {
   int32_t add_c;
   int32_t check_bailout;
   int32_t has_offset;
+  int32_t add_bail;      // the formula's DE function is pseudo- or Jos-Kleinian: the convergence bailout
+  int32_t pad_slot;
   double d[P_COUNT];
   float f[P_COUNT];
+  double x[MBR_SLOT_X];  // a keyed formula's parameter block (formula_params.h)
 };
 
 // Mandelbox rotations of slot 0 of a single-fractal scene (sFractalMandelbox

@@ -49,6 +49,7 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_AEXION: *m = {2, 2, 10000.0, 2}; return true;           // fractal_aexion.cpp:16-27
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
+    case MBR_FORMULA_PSEUDO_KLEINIAN: *m = {3, 1, 100.0, 4}; return true;  // fractal_pseudo_kleinian.cpp:17-28
     default: return false;
   }
 }
@@ -507,7 +508,8 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     }
     FormulaMeta m;
     if (!formula_meta(f.formula, &m))
-      return set_err(ctx, MBR_EUNSUPPORTED, "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 19)", i, f.formula);
+      return set_err(ctx, MBR_EUNSUPPORTED,
+                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 19, 103)", i, f.formula);
     any = true;
     if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
     if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)
@@ -532,6 +534,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     if (m.cpixel == 1) addc = !addc;
     if (m.cpixel == 2) addc = false;  // cpixelAlreadyHas: the formula adds c itself (:209-212)
     s.add_c = addc ? 1 : 0;
+    s.add_bail = (m.de_function == 3 || m.de_function == 4) ? 1 : 0;  // hybrid_fractal_sequences.cpp:242-246
     double bailout;
     if (sc.use_default_bailout) {
       bailout = m.bailout;
@@ -564,6 +567,14 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     p[P_ADE_SCALE1] = f.analytic_de_scale1;
     p[P_ADE_OFFSET1] = f.analytic_de_offset1;
     s.has_offset = (f.mandelbox_offset[0] != 0.0 || f.mandelbox_offset[1] != 0.0 || f.mandelbox_offset[2] != 0.0);
+    // the keyed parameters (formula_params.h); any other formula takes none
+    const int bad = pack_keyed(f, s.x);
+    if (bad == -2) return set_err(ctx, MBR_EINVAL, "slot %d: n_params must be in [0, %d]", i, MBR_MAX_FORMULA_PARAMS);
+    if (bad >= 0)
+      return set_err(ctx, MBR_EINVAL,
+                     "slot %d: param[%d] (\"%.*s\") is not a parameter formula %d reads, or its value is not "
+                     "finite (an int within 32 bits)",
+                     i, bad, MBR_PARAM_KEY_LEN, f.param[bad].key, f.formula);
   }
   if (!any) return set_err(ctx, MBR_EINVAL, "scene has no formula");
   if (hybrid && sc.use_default_bailout)

@@ -24,6 +24,9 @@
 #endif
 
 #include "../include/mbr.h"
+// the keyed formulas' parameter tables and defaults (the settings keys and
+// values of InitFractalParams, a format both sides must read alike)
+#include "../mandelbulber2_b200/csrc/formula_params.h"
 #include "oracle_scalar.hpp"
 
 namespace oracle {
@@ -62,6 +65,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_AEXION: *fi = {2, 2, 10000.0, 2}; return true;           // fractal_aexion.cpp:16-27
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
+    case MBR_FORMULA_PSEUDO_KLEINIAN: *fi = {3, 1, 100.0, 4}; return true;  // fractal_pseudo_kleinian.cpp:17-28
     default: return false;
   }
 }
@@ -74,6 +78,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
 struct Slot {
   int formula = 0;
   bool add_c = false, check_bailout = true;
+  bool add_bail = false;  // pseudo- / Jos-Kleinian DE function: the convergence bailout
   double weight = 1.0, bailout = 10.0;
   int iterations = 1, start = 0, stop = 250;
   double power = 9, alpha = 0, beta = 0;
@@ -148,6 +153,7 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
     if (fi.cpixel == 1) addc = !addc;
     if (fi.cpixel == 2) addc = false;  // cpixelAlreadyHas (hybrid_fractal_sequences.cpp:209-212)
     sl.add_c = addc;
+    sl.add_bail = fi.de_function == 3 || fi.de_function == 4;  // hybrid_fractal_sequences.cpp:242-246
     if (sc.use_default_bailout) {  // :217-224
       if (hybrid) maxBailout = std::max(maxBailout, fi.default_bailout);
       else sl.bailout = fi.default_bailout;
@@ -175,6 +181,8 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
       }
     for (int k = 0; k < 3; k++) sl.mb_main_deg[k] = f.mandelbox_rotation_main[k];
     sl.ifs = f;
+    double keyed[MBR_SLOT_X];
+    if (mbr::pack_keyed(f, keyed) != -1) return false;  // a key the formula does not read
   }
   if (hybrid && sc.use_default_bailout)
     for (int i = 0; i < n; i++) s.slot[i].bailout = maxBailout;  // :253-259
@@ -578,6 +586,7 @@ struct SlotT {
   // kaleidoscopic IFS (sFractalIFS after RecalculateFractalParams, fractal.cpp:655-661)
   bool ifs_abs[3], ifs_enabled[9], ifs_menger, ifs_rot_on, ifs_edge_on, ifs_main_zero, ifs_rot_zero[9];
   double ifs_scale, ifs_offset[3], ifs_edge[3], ifs_main[9], ifs_rot[9][9], ifs_dir[9][3], ifs_dist[9], ifs_int[9];
+  double x[MBR_SLOT_X];   // a keyed formula's parameters (formula_params.h layout)
 };
 enum { TAN_POWER = 0, TAN_SCALE = 1, TAN_MR2 = 2, TAN_X = 3, TAN_Y = 4, TAN_Z = 5 };
 
@@ -638,6 +647,7 @@ SlotT<S> make_slot(const Slot &s, bool tangents) {
     t.ifs_dist[i] = f.ifs_distance[i];
     t.ifs_int[i] = f.ifs_intensity[i];
   }
+  mbr::pack_keyed(f, t.x);  // validated when the sequence was built
   return t;
 }
 
@@ -754,6 +764,99 @@ inline void formula_xenodreambuie(V4<S> &z, const SlotT<S> &f, const S &r, S &DE
   z.x = rp * cos(th) * sph;
   z.y = rp * sin(th) * sph;
   z.z = rp * cos(ph);
+}
+
+// cFractalPseudoKleinian::FormulaCode (fractal_pseudo_kleinian.cpp:30-202)
+// without the aux.color terms; pk is aux.pseudoKleinianDE.
+template <class S>
+inline void formula_pseudo_kleinian(V4<S> &z, const SlotT<S> &f, S &DE, S &pk, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  if (x[PKX_SPH_INV] != 0.0 && i >= int(x[PKX_START_X]) && i < int(x[PKX_STOP_1])) {  // :33-44
+    z.x = z.x + x[PKX_OFFSET000];
+    z.y = z.y + x[PKX_OFFSET000 + 1];
+    z.z = z.z + x[PKX_OFFSET000 + 2];
+    z.w = z.w + 0.0;
+    const S rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const S q = x[PKX_MAXR2] / rr;
+    z.x = z.x * q;
+    z.y = z.y * q;
+    z.z = z.z * q;
+    z.w = z.w * q;
+    z.x = z.x + (x[PKX_ADD_A000] - x[PKX_OFFSET000]);
+    z.y = z.y + (x[PKX_ADD_A000 + 1] - x[PKX_OFFSET000 + 1]);
+    z.z = z.z + (x[PKX_ADD_A000 + 2] - x[PKX_OFFSET000 + 2]);
+    z.w = z.w + (0.0 - 0.0);
+    DE = DE * (x[PKX_MAXR2] / rr) + x[PKX_DE_OFFSET0];
+  }
+  if (x[PKX_PRISM] != 0.0 && i >= int(x[PKX_START_P]) && i < int(x[PKX_STOP_P1])) {  // :47-75
+    const double kSqrt34 = 0.86602540378443864676372317075294, kSqrt3 = 1.73205080756887729352744634150587;
+    z.y = fabs(z.y);
+    z.z = fabs(z.z);
+    const S dot1 = (z.x * -kSqrt34 + z.y * 0.5) * x[PKX_SCALE];
+    S t = std::max(S(0.0), dot1);
+    z.x = z.x - t * -kSqrt3;
+    z.y = fabs(z.y - t);
+    if (z.y > z.z) {
+      t = z.y;
+      z.y = z.z;
+      z.z = t;
+    }
+    z.x = z.x - x[PKX_CMUL000] * kSqrt34;
+    z.y = z.y - x[PKX_CMUL000 + 1] * 1.5;
+    z.z = z.z - x[PKX_CMUL000 + 2] * 1.5;
+    z.w = z.w - 1.0 * 0.0;
+    if (z.z > z.x) {
+      t = z.z;
+      z.z = z.x;
+      z.x = t;
+    }
+    if (z.x > 0.0) {
+      z.y = std::max(S(0.0), z.y);
+      z.z = std::max(S(0.0), z.z);
+    }
+  }
+  if (x[PKX_ABS_BOX] != 0.0 && i >= int(x[PKX_START_E]) && i < int(x[PKX_STOP_E])) {  // :78-91
+    z.x = fabs(z.x + x[PKX_ADD111]) - fabs(z.x - x[PKX_ADD111]) - z.x;
+    z.y = fabs(z.y + x[PKX_ADD111 + 1]) - fabs(z.y - x[PKX_ADD111 + 1]) - z.y;
+    if (x[PKX_ABS_BOX_Z] != 0.0) z.z = fabs(z.z + x[PKX_ADD111 + 2]) - fabs(z.z - x[PKX_ADD111 + 2]) - z.z;
+  }
+  if (x[PKX_BOX] != 0.0 && i >= int(x[PKX_START_A]) && i < int(x[PKX_STOP_A])) {  // :94-115
+    if (fabs(z.x) > x[PKX_MB_LIMIT]) z.x = S(double(sgn(val(z.x)))) * x[PKX_MB_VALUE] - z.x;
+    if (fabs(z.y) > x[PKX_MB_LIMIT]) z.y = S(double(sgn(val(z.y)))) * x[PKX_MB_VALUE] - z.y;
+    const double zLimit = x[PKX_MB_LIMIT] * x[PKX_SCALE1];
+    const double zValue = x[PKX_MB_VALUE] * x[PKX_SCALE1];
+    if (fabs(z.z) > zLimit) z.z = S(double(sgn(val(z.z)))) * zValue - z.z;
+  }
+  if (i >= int(x[PKX_START_C]) && i < int(x[PKX_STOP_C])) {  // :118-138
+    const double cx = x[PKX_CSIZE], cy = x[PKX_CSIZE + 1], cz = x[PKX_CSIZE + 2];
+    V4<S> t = z;
+    if (z.x > cx) t.x = cx;
+    if (z.x < -cx) t.x = -cx;
+    if (z.y > cy) t.y = cy;
+    if (z.y < -cy) t.y = -cy;
+    if (z.z > cz) t.z = cz;
+    if (z.z < -cz) t.z = -cz;
+    z.x = t.x * 2.0 - z.x;
+    z.y = t.y * 2.0 - z.y;
+    z.z = t.z * 2.0 - z.z;
+    z.w = t.w * 2.0 - z.w;
+    const S k = std::max(S(x[PKX_MINR05] / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), S(1.0));
+    z.x = z.x * k;
+    z.y = z.y * k;
+    z.z = z.z * k;
+    z.w = z.w * k;
+    if (x[PKX_FLIP_Z] != 0.0) z.z = -z.z;
+    if (x[PKX_FLIP_W] != 0.0) z.w = -z.w;
+    DE = DE * (k + x[PKX_TWEAK005]);
+    pk = x[PKX_DE_SCALE1];
+  }
+  if (x[PKX_ROT_ON] != 0.0 && i >= int(x[PKX_START_R]) && i < int(x[PKX_STOP_R]))  // :141-144
+    z = mb_turn(x + PKX_ROT + 1, x[PKX_ROT] != 0.0, false, z);
+  z.x = z.x + x[PKX_ADD000];  // :147
+  z.y = z.y + x[PKX_ADD000 + 1];
+  z.z = z.z + x[PKX_ADD000 + 2];
+  z.w = z.w + 0.0;
 }
 
 // cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45)
@@ -910,12 +1013,14 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   V4<S> const_c = z;  // aux.const_c (the Aexion replaces it)
   S r = len4(z);
   S DE = 1.0;
-  V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ;
+  S pk = 1.0;  // aux.pseudoKleinianDE (:120)
+  V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ, lastLastZ = lastZ;
   int maxN = seq.formula_maxiter * maxiterMultiplier;
   if (forcedMaxiter >= 0) maxN = forcedMaxiter;
   int i;
   for (i = 0; i < maxN; i++) {
     lastGoodZ = lastZ;
+    lastLastZ = lastZ;
     lastZ = z;
     const int sequence = (i < seq.length) ? seq.seq[i] : seq.seq[0];  // GetSequence
     const Slot &sd = seq.slot[sequence];
@@ -957,6 +1062,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_XENODREAMBUIE: formula_xenodreambuie(z, f, r, DE); break;
         case MBR_FORMULA_QUATERNION: formula_quaternion(z, r, DE); break;
         case MBR_FORMULA_AEXION: formula_aexion(z, r, DE, sd.ifs, i, const_c); break;
+        case MBR_FORMULA_PSEUDO_KLEINIAN: formula_pseudo_kleinian(z, f, DE, pk, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
@@ -999,14 +1105,21 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         out.maxiter = false;
         break;
       }
+      if (sd.add_bail) {  // :323-336
+        out.maxiter = false;
+        const V4<S> d1{z.x - lastZ.x, z.y - lastZ.y, z.z - lastZ.z, z.w - lastZ.w};
+        if (len4(d1) / r < 0.1 / sd.bailout) break;
+        const V4<S> d2{z.x - lastLastZ.x, z.y - lastLastZ.y, z.z - lastLastZ.z, z.w - lastLastZ.w};
+        if (len4(d2) / r < 0.1 / sd.bailout) break;
+      }
     }
     if (nan4(z)) {  // :487-491
       z = lastGoodZ;
       break;
     }
   }
-  // final DE :495-621 (aux.pseudoKleinianDE = 1 and aux.dist = 1000 keep
-  // their initial values :119-120 for every formula restated here)
+  // final DE :495-621 (aux.dist = 1000 keeps its initial value :119 for
+  // every formula restated here; aux.pseudoKleinianDE is pk)
   if (DE > 0.0) {
     if (seq.is_hybrid) {
       switch (seq.de_function) {
@@ -1014,7 +1127,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case 2: out.distance = (r > 1.0) ? S(0.5 * r * log(r) / DE) : S(0.0); break;
         case 3: {
           const S rxy = sqrt(z.x * z.x + z.y * z.y);
-          out.distance = std::max(S(rxy - 1.0), S(fabs(rxy * z.z) / r)) / DE;
+          out.distance = std::max(S(rxy - pk), S(fabs(rxy * z.z) / r)) / DE;
           break;
         }
         case 5: out.distance = 1000.0; break;
@@ -1028,7 +1141,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case 3: out.distance = (r - 2.0) / DE; break;
         case 4: {
           const S rxy = sqrt(z.x * z.x + z.y * z.y);
-          out.distance = std::max(S(rxy - 1.0), S(fabs(rxy * z.z) / r)) / DE;
+          out.distance = std::max(S(rxy - pk), S(fabs(rxy * z.z) / r)) / DE;
           break;
         }
         case 6: out.distance = 1000.0; break;

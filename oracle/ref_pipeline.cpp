@@ -103,6 +103,23 @@ int refp_set(void *h, int fractal, const char *name, int kind, const double *v) 
   return 0;
 }
 
+// The kind refp_set takes for a parameter of the main container (fractal <
+// 0) or of fractal slot `fractal`: 0 int, 1 double, 2 bool, 3 vector; -1 when
+// the container has no such parameter or it is of another type.
+int refp_param_kind(void *h, int fractal, const char *name) {
+  Pipeline *p = static_cast<Pipeline *>(h);
+  std::shared_ptr<cParameterContainer> c = fractal < 0 ? p->par : p->fract->at(fractal);
+  const QString n(name);
+  if (!c->IfExists(n)) return -1;
+  switch (c->GetVarType(n)) {
+    case parameterContainer::typeInt: return 0;
+    case parameterContainer::typeDouble: return 1;
+    case parameterContainer::typeBool: return 2;
+    case parameterContainer::typeVector3: return 3;
+    default: return -1;
+  }
+}
+
 // Sets a string parameter (node definitions, enumerations by name).
 int refp_set_string(void *h, int fractal, const char *name, const char *value) {
   Pipeline *p = static_cast<Pipeline *>(h);

@@ -48,6 +48,7 @@ class RefPipeline:
             L.refp_free.argtypes = [_P]
             L.refp_set.argtypes = [_P, C.c_int, C.c_char_p, C.c_int, _P]
             L.refp_set_string.argtypes = [_P, C.c_int, C.c_char_p, C.c_char_p]
+            L.refp_param_kind.argtypes = [_P, C.c_int, C.c_char_p]
             L.refp_add_node.argtypes = [_P, C.c_int]
             L.refp_add_primitive.argtypes = [_P, C.c_char_p, C.c_int]
             L.refp_prepare.argtypes = [_P]
@@ -272,6 +273,14 @@ class RefPipeline:
                     self.set(f"IFS_rotations_{k}", list(f.ifs_rotations[k]), KIND_VEC3, i)
                     self.set(f"IFS_distance_{k}", f.ifs_distance[k], KIND_DOUBLE, i)
                     self.set(f"IFS_intensity_{k}", f.ifs_intensity[k], KIND_DOUBLE, i)
+            # the keyed formula parameters: ints, bools and doubles as their
+            # container holds them (a rotation is a vector of degrees)
+            for j in range(f.n_params):
+                key = f.param[j].key.decode()
+                kind = self.L.refp_param_kind(self.h, i, key.encode())
+                if kind < 0:
+                    raise KeyError(f"fractal {i}: no parameter {key}")
+                self.set(key, list(f.param[j].value) if kind == KIND_VEC3 else f.param[j].value[0], kind, i)
         self.set("use_default_bailout", s.use_default_bailout, KIND_BOOL)
         self.set("bailout", s.bailout, KIND_DOUBLE)
         self.set("minN", s.min_n, KIND_INT)

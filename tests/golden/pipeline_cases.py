@@ -87,6 +87,46 @@ def _trees():
     return t
 
 
+def _pk(maxiter=30, **params):
+    s = abi.scene_defaults(abi.FORMULA_PSEUDO_KLEINIAN)
+    s.formula_maxiter = maxiter
+    for k, v in params.items():
+        s.fractal[0].set_param(k, v)
+    return s
+
+
+def _pseudo_kleinian_cases():
+    t = {}
+    t["pk_default"] = _pk()
+    t["pk_params"] = _pk(analyticDE_tweak_005=0.076923, transf_addition_constant_0777=[0.173077, 0.307692, 1.0],
+                         transf_minimum_radius_05=0.230769)
+    t["pk_sphere_inversion"] = _pk(transf_sphere_inversion_enabled_false=1, transf_stop_iterations_1=2,
+                                   transf_offset_000=[0.1, -0.2, 0.3], transf_maxR2_1=1.3,
+                                   transf_addition_constantA_000=[0.05, 0.0, -0.1], analyticDE_offset_0=0.2)
+    t["pk_prism"] = _pk(transf_function_enabledP_false=1, transf_stop_iterations_P1=3, transf_scale=1.2,
+                        transf_constant_multiplier_000=[0.3, 0.2, 0.1])
+    t["pk_box_folds"] = _pk(transf_function_enabledBy_false=1, transf_function_enabledBy=0,
+                            transf_addition_constant_111=[0.9, 1.1, 1.0], transf_stop_iterations_E=5,
+                            transf_function_enabledBx_false=1, transf_scale_1=1.3, transf_start_iterations_A=1)
+    s = _pk(transf_function_enabledR_false=1, transf_rotation=[10.0, 20.0, 30.0], transf_start_iterations_R=2,
+            transf_addition_constant=[0.1, 0.0, -0.05], transf_function_enabledN_false=1,
+            transf_start_iterations_C=1, transf_stop_iterations_C=20)
+    s.fractal[0].analytic_de_scale1 = 0.7
+    s.fractal[0].mandelbox_folding_limit = 0.9
+    t["pk_rotation_flip_scale"] = s
+    s = _pk(20)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    s.fractal[0].formula_iterations = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBOX)
+    s.fractal[1].mandelbox_scale = -1.5
+    t["hybrid_pk_box"] = s
+    s = _pk(25)
+    s.delta_de_method = abi.DE_METHOD_FORCE_DELTA
+    t["pk_delta"] = s
+    return t
+
+
 def cases():
     out = {}
     out["bulb_p8"] = configs.mandelbulb_scene(8.0, 250)
@@ -273,6 +313,8 @@ def cases():
     # explicit objects trees (calculate_distance.cpp:225-516)
     for name, tree in _trees().items():
         out[name] = tree
+    # the pseudo-Kleinian (103), parameters by settings key
+    out.update(_pseudo_kleinian_cases())
     # quaternion (5) and aexion (19)
     s = abi.scene_defaults(abi.FORMULA_QUATERNION)
     s.formula_maxiter = 40
@@ -387,6 +429,11 @@ def render_cases():
     sc.deltade_relative_delta = 0.02
     p.advanced_quality = 1  # the offset is deltade_relative_delta of the detail size
     out.append(("bulb_delta_de_advanced_quality", sc, cam, p))
+    s = _pk(60, analyticDE_tweak_005=0.076923, transf_addition_constant_0777=[0.173077, 0.307692, 1.0],
+            transf_minimum_radius_05=0.230769)
+    cam = configs.camera((2.12066528836305, -3.70836995527439, 1.90220668159675),
+                         target=(2.12183734234493, -3.70761659259838, 1.90598160360012), width=32, height=24)
+    out.append(("pseudo_kleinian", s, cam, params()))
     trees = _trees()
     out.append(("tree_intersection", trees["tree_intersection"], configs.camera((0.3, -3.5, 1.2), width=32, height=24),
                 params()))

@@ -34,7 +34,8 @@ def test_struct_layout_matches_c(tmp_path):
     prog = tmp_path / "sizes.c"
     structs = {"mbr_fractal": abi.Fractal, "mbr_scene": abi.Scene, "mbr_camera": abi.Camera,
                "mbr_render_params": abi.RenderParams, "mbr_stats": abi.Stats, "mbr_outputs": abi.Outputs,
-               "mbr_job": abi.Job, "mbr_tuning": abi.Tuning}
+               "mbr_job": abi.Job, "mbr_tuning": abi.Tuning, "mbr_formula_param": abi.FormulaParam,
+               "mbr_node": abi.Node, "mbr_primitive": abi.Primitive}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

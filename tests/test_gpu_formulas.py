@@ -193,3 +193,63 @@ def test_ifs_and_rotated_mandelbox_in_hybrids(renderer, oracle, case):
         engines.insert(0, abi.ENGINE_PLAIN_FP64_STRICT)
     for engine in engines:
         check(renderer, sc, cam, p, o, ost, engine, case)
+
+
+PK_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk_box_folds", "pk_rotation_flip_scale",
+            "hybrid_pk_box", "pk_delta"]
+
+
+@pytest.mark.parametrize("case", PK_CASES)
+def test_pseudo_kleinian_distances(renderer, oracle, case):
+    """Formula 103 (fractal_pseudo_kleinian.cpp:30-202) with its parameters by
+    settings key, the pseudo-Kleinian DE state and the convergence bailout
+    (compute_fractal.cpp:323-336): the oracle equals the reference's own
+    CalculateDistance on these scenes (tests/golden/pipeline_kat.json).  The
+    formula uses +, -, *, / and fabs only (the rotation matrix is built on the
+    host), so the strict FP64 engine equals the oracle bit for bit, iteration
+    counts included.  The FMA and mixed engines are reported; their orbits
+    never escape (the convergence bailout ends them), so an FMA's rounding can
+    end one an iteration apart and no tight per-point bar holds: they are held
+    to a median relative error of 1e-6 (FMA) / 1e-3 (FP32)."""
+    from tests.golden.pipeline_cases import cases
+
+    sc = cases()[case]
+    renderer.set_scene(sc)
+    pts = np.random.default_rng(31).uniform(-2.0, 2.0, size=(4096, 3))
+    import torch
+    for det in (1e-3, 0.05):
+        for nm in (False, True):
+            od, oit = oracle.distance(sc, pts, det, nm)
+            d, it = renderer.distance(torch.from_numpy(pts), det, nm, abi.ENGINE_PLAIN_FP64_STRICT)
+            assert np.array_equal(d.cpu().numpy(), od) and np.array_equal(it.cpu().numpy(), oit), (case, det, nm)
+            engines = [abi.ENGINE_PLAIN_FP64] + ([] if "delta" in case else [abi.ENGINE_PLAIN_MIXED])
+            for engine in engines:
+                d, it = renderer.distance(torch.from_numpy(pts), det, nm, engine)
+                d, it = d.cpu().numpy(), it.cpu().numpy()
+                rel = np.abs(d - od) / np.maximum(np.abs(od), 1e-300)
+                print(case, det, nm, abi.ENGINE_NAMES[engine], "rel median", np.median(rel), "p90",
+                      np.percentile(rel, 90), "iters", np.mean(it == oit))
+                assert np.median(rel) <= (1e-6 if engine == abi.ENGINE_PLAIN_FP64 else 1e-3), (case, engine)
+
+
+def test_pseudo_kleinian_frames(renderer, oracle):
+    """An interior view of the pseudo-Kleinian (the settings of the
+    reference's example 'pseudo kleinian 002', whose frame the oracle
+    reproduces bit for bit, tests/golden/render_kat.json): strict FP64
+    bit-exact, FP64 and mixed engines to their bars; the wavefront engines
+    refuse the formula."""
+    from mandelbulber2_b200.render import MbrError
+    from tests.golden.pipeline_cases import render_cases
+
+    _, sc, cam, _ = [c for c in render_cases() if c[0] == "pseudo_kleinian"][0]
+    cam.width, cam.height = 96, 64
+    p = configs.base_params(5, 20.0)
+    p.ao_rays = 4
+    renderer.set_scene(sc)
+    o, ost = oracle.render(sc, cam, p)
+    for engine in (abi.ENGINE_PLAIN_FP64_STRICT, abi.ENGINE_PLAIN_FP64, abi.ENGINE_PLAIN_MIXED):
+        check(renderer, sc, cam, p, o, ost, engine, "pseudo_kleinian")
+    for engine in (abi.ENGINE_WAVEFRONT_FP32, abi.ENGINE_WAVEFRONT_FP64, abi.ENGINE_WAVEFRONT_AUTO):
+        with pytest.raises(MbrError) as e:
+            renderer.render(cam, p, engine)
+        assert e.value.status == abi.MBR_EUNSUPPORTED

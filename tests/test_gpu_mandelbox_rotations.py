@@ -68,7 +68,10 @@ def test_rotated_distance_strict_bit_exact(renderer, oracle):
     assert np.array_equal(d.cpu().numpy(), od)
 
 
-def test_rotations_in_a_hybrid_are_refused(renderer):
+def test_rotations_with_two_mandelbox_slots_are_refused(renderer):
+    """The scene carries one Mandelbox rotation block: a hybrid whose one
+    Mandelbox slot is rotated is accepted, one with two Mandelbox slots and
+    rotations is refused."""
     from mandelbulber2_b200.render import MbrError
 
     sc = configs.hybrid_scene()
@@ -76,6 +79,8 @@ def test_rotations_in_a_hybrid_are_refused(renderer):
     sc.fractal[0].formula_iterations = 2
     sc.fractal[0].mandelbox_main_rotation_enabled = 1
     sc.fractal[0].mandelbox_rotation_main[:] = MAIN
+    renderer.set_scene(sc)
+    sc.fractal[1] = configs.mandelbox_scene().fractal[0]
     with pytest.raises(MbrError) as e:
         renderer.set_scene(sc)
     assert e.value.status == abi.MBR_EUNSUPPORTED

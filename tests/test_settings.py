@@ -206,10 +206,10 @@ def test_invalid_files(text, what):
 
 
 def test_unsupported_geometry_is_named():
-    txt = HEADER + ("[main_parameters]\nformula_1 103;\n")
+    txt = HEADER + ("[main_parameters]\nformula_1 104;\n")
     s = settings.load_from_string(txt)
     assert s.status == abi.MBR_EUNSUPPORTED
-    assert any(u.startswith("formula_1 103") for u in s.unsupported()), s.report
+    assert any(u.startswith("formula_1 104") for u in s.unsupported()), s.report
     txt = HEADER + ("[main_parameters]\nformula_1 8;\nprimitive_prism_1_enabled true;\nprimitive_prism_1_boolean_operator 0;\n"
                     "boolean_operators true;\n"
                     "delta_DE_function 4;\nhybrid_fractal_enable true;\nformula_2 8;\n"
@@ -221,7 +221,7 @@ def test_unsupported_geometry_is_named():
                 "delta_DE_function 4", "Mandelbox rotations with more than one Mandelbox slot"):
         assert key in u, (key, s.report)
     # a slot that a single-fractal scene does not iterate may name any formula
-    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 103;\n")
+    s = settings.load_from_string(HEADER + "[main_parameters]\nformula_1 8;\nformula_2 104;\n")
     assert s.ok, s.report
 
 
