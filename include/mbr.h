@@ -66,7 +66,9 @@ typedef enum mbr_formula {
   MBR_FORMULA_MENGER_SPONGE = 7,/* formula/definition/fractal_menger_sponge.cpp:30-71 */
   MBR_FORMULA_MANDELBOX = 8,    /* formula/definition/fractal_mandelbox.cpp:31-107 */
   /* formulas whose parameters are passed by settings key (mbr_fractal.param) */
-  MBR_FORMULA_PSEUDO_KLEINIAN = 103 /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
+  MBR_FORMULA_BOX_FOLD_BULB_POW2 = 16, /* formula/definition/fractal_box_fold_bulb_pow2.cpp:27-76 (delta DE) */
+  MBR_FORMULA_MENGER_MOD1 = 61,       /* formula/definition/fractal_menger_mod1.cpp:29-103 */
+  MBR_FORMULA_PSEUDO_KLEINIAN = 103   /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
 } mbr_formula;
 
 /* fractal::enumDEFunctionType (src/fractal_enums.h:47-60).  The Jos

@@ -401,6 +401,112 @@ __device__ __noinline__ void f_pseudo_kleinian(V4<T> &z, T &DE, T &pk, const Dev
   z.z = z.z + T(x[PKX_ADD000 + 2]);
 }
 
+// cFractalBoxFoldBulbPow2::FormulaCode (fractal_box_fold_bulb_pow2.cpp:27-76):
+// a box fold, the fixed spherical fold (min radius^2 0.25, fixed 1), then the
+// power-2 bulb with its z factor; a delta-DE formula (its analytic DE terms
+// apply only under a forced analytic method)
+template <class T>
+__device__ __noinline__ void f_box_fold_bulb_pow2(V4<T> &z, T r, T &DE, const DevSlot &s) {
+  const double *x = s.x;
+  const double ff = x[BFX_FOLD];
+  if (m_abs(z.x) > T(ff)) z.x = T(double(sgn_of(z.x)) * ff * 2.0) - z.x;
+  if (m_abs(z.y) > T(ff)) z.y = T(double(sgn_of(z.y)) * ff * 2.0) - z.y;
+  if (m_abs(z.z) > T(ff)) z.z = T(double(sgn_of(z.z)) * ff * 2.0) - z.z;
+  const T r2 = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+  if (r2 < T(0.25)) {
+    z.x = z.x * T(4.0);
+    z.y = z.y * T(4.0);
+    z.z = z.z * T(4.0);
+    z.w = z.w * T(4.0);
+    DE = DE * T(4.0);
+  } else if (r2 < T(1.0)) {
+    const T f2 = T(1.0) / r2;
+    z.x = z.x * f2;
+    z.y = z.y * f2;
+    z.z = z.z * f2;
+    z.w = z.w * f2;
+    DE = DE * f2;
+  }
+  z.x = z.x * T(2.0);
+  z.y = z.y * T(2.0);
+  z.z = z.z * T(2.0);
+  z.w = z.w * T(2.0);
+  const T x2 = z.x * z.x, y2 = z.y * z.y, z2 = z.z * z.z;
+  const T temp = T(1.0) - z2 / (x2 + y2);
+  const T nx = (x2 - y2) * temp;
+  const T ny = T(2.0) * z.x * z.y * temp;
+  const T nz = T(-2.0) * z.z * m_sqrt(T(x2 + y2));
+  z.x = nx;
+  z.y = ny;
+  z.z = nz * T(x[BFX_ZFACTOR]);
+  if (x[BFX_ADE_ON] != 0.0)  // :67-73
+    DE = (DE + T(1.0)) * T(5.0) * r * T(x[BFX_ADE_SCALE1]) *
+             T(sqrt(x[BFX_ZFACTOR] * x[BFX_ZFACTOR] + 2.0 + x[BFX_ADE_OFFSET2])) +
+         T(x[BFX_ADE_OFFSET1]);
+}
+
+// cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
+// aux.color terms left out
+template <class T>
+__device__ __noinline__ void f_menger_mod1(V4<T> &z, T &DE, const DevSlot &s, int i) {
+  const double *x = s.x;
+  z = V4<T>{m_abs(z.x), m_abs(z.y), m_abs(z.z), m_abs(z.w)};
+  T t;
+  if (z.x < z.y) {
+    t = z.y;
+    z.y = z.x;
+    z.x = t;
+  }
+  if (z.x < z.z) {
+    t = z.z;
+    z.z = z.x;
+    z.x = t;
+  }
+  if (z.y < z.z) {
+    t = z.z;
+    z.z = z.y;
+    z.y = t;
+  }
+  const T s3 = T(x[MMX_SCALE3]);
+  z.x = z.x * s3;
+  z.y = z.y * s3;
+  z.z = z.z * s3;
+  z.w = z.w * s3;
+  z.x = z.x - T(2.0 * x[MMX_CM111]);
+  z.y = z.y - T(2.0 * x[MMX_CM111 + 1]);
+  if (z.z > T(1.0)) z.z = z.z - T(2.0 * x[MMX_CM111 + 2]);
+  DE = DE * s3;
+  if (x[MMX_ROT_ON] != 0.0 && i >= int(x[MMX_START]) && i < int(x[MMX_STOP])) {
+    if (x[MMX_ROT] == 0.0) z = mb_turn<T>(x + MMX_ROT + 1, false, z);
+    DE = DE * T(x[MMX_SCALED1]) + T(x[MMX_OFFSET1]);
+  }
+  z.x = z.x + T(x[MMX_ADD000]);
+  z.y = z.y + T(x[MMX_ADD000 + 1]);
+  z.z = z.z + T(x[MMX_ADD000 + 2]);
+  if (x[MMX_BOX_OFF] != 0.0 && i >= int(x[MMX_START_A]) && i < int(x[MMX_STOP_A])) {  // box offset :74-89
+    const V4<T> t0 = z;
+    z.x = sgn_of(z.x) * T(x[MMX_ADD_A000]) + z.x;
+    z.y = sgn_of(z.y) * T(x[MMX_ADD_A000 + 1]) + z.y;
+    z.z = sgn_of(z.z) * T(x[MMX_ADD_A000 + 2]) + z.z;
+    if (x[MMX_AVG_SCALE] != 0.0) {
+      const T tempL = len4<T, true>(t0);
+      const T avgScale = len4<T, true>(z) / tempL;
+      DE = DE * avgScale + T(1.0);
+    }
+  }
+  if (x[MMX_BLEND] != 0.0) {  // :91-102
+    const bool a = i == int(x[MMX_INT_A]), b = i == int(x[MMX_INT_B]);
+    const T sc1 = T(x[MMX_SCALE1]), oA = T(x[MMX_OFFSET]), oB = T(x[MMX_OFFSET0]);
+    const V4<T> zA = a ? z : V4<T>{T(0.0), T(0.0), T(0.0), T(0.0)};
+    const V4<T> zB = b ? z : V4<T>{T(0.0), T(0.0), T(0.0), T(0.0)};
+    z.x = z.x * sc1 + zA.x * oA + zB.x * oB;
+    z.y = z.y * sc1 + zA.y * oA + zB.y * oB;
+    z.z = z.z * sc1 + zA.z * oA + zB.z * oB;
+    z.w = z.w * sc1 + zA.w * oA + zB.w * oB;
+    DE = DE * sc1;
+  }
+}
+
 // cFractalKaleidoscopicIfs::FormulaCode (fractal_kaleidoscopic_ifs.cpp:30-85)
 // over the enabled vectors of the scene's IFS block; the 4-vector terms with
 // w keep the reference's operations (its direction and offset have w = 0)
@@ -461,6 +567,8 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
   if constexpr (EXT) {
     switch (formula) {
       case MBR_FORMULA_PSEUDO_KLEINIAN: f_pseudo_kleinian<T>(z, DE, pk, s, i); break;
+      case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
+      case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
       case MBR_FORMULA_AEXION: f_aexion<T>(z, r, DE, s, i, c); break;
       case MBR_FORMULA_MANDELBULB: f_mandelbulb<T>(z, r, DE, s); break;

@@ -7,7 +7,10 @@
 // bool (0 / 1) one; a vector three; a rotation ten - the zero flag of
 // CRotationMatrix and the 3x3 matrix of SetRotation2(angles * pi / 180)
 // (src/algebra.cpp:296-302, as sFractal::RecalculateFractalParams builds
-// transformCommon.rotationMatrix, src/fractal.cpp:696), row-major.
+// transformCommon.rotationMatrix, src/fractal.cpp:696), row-major.  A NAMED
+// entry takes one value from a named mbr_fractal field that holds the same
+// parameter (mandelbox_folding_limit, transf_scale3, ...): such keys come
+// through those fields, never through mbr_fractal.param.
 #pragma once
 #include <cmath>
 
@@ -17,7 +20,17 @@
 
 namespace mbr {
 
-enum ParamKind { PK_INT = 0, PK_DOUBLE = 1, PK_BOOL = 2, PK_VEC3 = 3, PK_ROT = 4 };
+enum ParamKind { PK_INT = 0, PK_DOUBLE = 1, PK_BOOL = 2, PK_VEC3 = 3, PK_ROT = 4, PK_NAMED = 5 };
+
+// the named mbr_fractal fields a NAMED entry reads
+enum NamedField {
+  NF_MB_LIMIT = 0,   // mandelbox_folding_limit
+  NF_MB_VALUE,       // mandelbox_folding_value
+  NF_MB_SCALE,       // mandelbox_scale
+  NF_ADE_SCALE1,     // analytic_de_scale1 (analyticDE_scale_1)
+  NF_ADE_OFFSET1,    // analytic_de_offset1 (analyticDE_offset_1)
+  NF_SCALE3          // transf_scale3 (transf_scale_3)
+};
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
 // 30-202): sphere inversion, prism shape, abs-box and box folds, the
@@ -58,13 +71,48 @@ enum PseudoKleinianX {
   PKX_STOP_R = 40,                  // transf_stop_iterations_R
   PKX_ROT = 41,                     // transf_rotation (10)
   PKX_ADD000 = 51,                  // transf_addition_constant (3)
-  PKX_KEYED_END = 54,               // the keyed block ends here
-  PKX_MB_LIMIT = 54,                // mandelbox_folding_limit (mbr_fractal field)
-  PKX_MB_VALUE = 55,                // mandelbox_folding_value (mbr_fractal field)
-  PKX_DE_SCALE1 = 56,               // analyticDE_scale_1 (mbr_fractal analytic_de_scale1)
+  PKX_MB_LIMIT = 54,                // mandelbox_folding_limit (named)
+  PKX_MB_VALUE = 55,                // mandelbox_folding_value (named)
+  PKX_DE_SCALE1 = 56,               // analyticDE_scale_1 (named)
   PKX_COUNT = 57
 };
 static_assert(PKX_COUNT <= MBR_SLOT_X, "pseudo-Kleinian block exceeds the slot's parameter block");
+
+// cFractalBoxFoldBulbPow2 (formula/definition/fractal_box_fold_bulb_pow2.cpp:27-76)
+enum BoxFoldBulbPow2X {
+  BFX_FOLD = 0,      // boxfold_bulbpow2_folding_factor
+  BFX_ZFACTOR = 1,   // boxfold_bulbpow2_z_factor
+  BFX_ADE_ON = 2,    // analyticDE_enabled_false
+  BFX_ADE_OFFSET2 = 3,  // analyticDE_offset_2
+  BFX_ADE_SCALE1 = 4,   // analyticDE_scale_1 (named)
+  BFX_ADE_OFFSET1 = 5,  // analyticDE_offset_1 (named)
+  BFX_COUNT = 6
+};
+
+// cFractalMengerMod1 (formula/definition/fractal_menger_mod1.cpp:29-103)
+enum MengerMod1X {
+  MMX_CM111 = 0,     // transf_constant_multiplier_111 (3)
+  MMX_ROT_ON = 3,    // transf_rotation_enabled
+  MMX_START = 4,     // transf_start_iterations
+  MMX_STOP = 5,      // transf_stop_iterations
+  MMX_ROT = 6,       // transf_rotation (10)
+  MMX_SCALED1 = 16,  // transf_scaleD_1
+  MMX_OFFSET1 = 17,  // transf_offset_1
+  MMX_ADD000 = 18,   // transf_addition_constant (3)
+  MMX_BOX_OFF = 21,  // transf_function_enabledx_false
+  MMX_START_A = 22,  // transf_start_iterations_A
+  MMX_STOP_A = 23,   // transf_stop_iterations_A
+  MMX_ADD_A000 = 24, // transf_addition_constantA_000 (3)
+  MMX_AVG_SCALE = 27,  // transf_function_enabledA_false
+  MMX_BLEND = 28,    // transf_function_enabled_false
+  MMX_INT_A = 29,    // transf_int_A
+  MMX_INT_B = 30,    // transf_int_B
+  MMX_SCALE1 = 31,   // transf_scale_1
+  MMX_OFFSET = 32,   // transf_offset
+  MMX_OFFSET0 = 33,  // transf_offset_0
+  MMX_SCALE3 = 34,   // transf_scale_3 (named)
+  MMX_COUNT = 35
+};
 
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
@@ -121,8 +169,45 @@ constexpr FormulaKey kPseudoKleinianKeys[] = {
     {"transf_stop_iterations_R", PK_INT, {250, 0, 0}, PKX_STOP_R},
     {"transf_rotation", PK_ROT, {0, 0, 0}, PKX_ROT},
     {"transf_addition_constant", PK_VEC3, {0, 0, 0}, PKX_ADD000},
+    {"mandelbox_folding_limit", PK_NAMED, {NF_MB_LIMIT, 0, 0}, PKX_MB_LIMIT},
+    {"mandelbox_folding_value", PK_NAMED, {NF_MB_VALUE, 0, 0}, PKX_MB_VALUE},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1, 0, 0}, PKX_DE_SCALE1},
 };
-static_assert(keys_contiguous(kPseudoKleinianKeys, PKX_KEYED_END), "pseudo-Kleinian keys and x[] layout disagree");
+static_assert(keys_contiguous(kPseudoKleinianKeys, PKX_COUNT), "pseudo-Kleinian keys and x[] layout disagree");
+
+constexpr FormulaKey kBoxFoldBulbPow2Keys[] = {
+    {"boxfold_bulbpow2_folding_factor", PK_DOUBLE, {2, 0, 0}, BFX_FOLD},
+    {"boxfold_bulbpow2_z_factor", PK_DOUBLE, {5, 0, 0}, BFX_ZFACTOR},
+    {"analyticDE_enabled_false", PK_BOOL, {0, 0, 0}, BFX_ADE_ON},
+    {"analyticDE_offset_2", PK_DOUBLE, {1, 0, 0}, BFX_ADE_OFFSET2},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1, 0, 0}, BFX_ADE_SCALE1},
+    {"analyticDE_offset_1", PK_NAMED, {NF_ADE_OFFSET1, 0, 0}, BFX_ADE_OFFSET1},
+};
+static_assert(keys_contiguous(kBoxFoldBulbPow2Keys, BFX_COUNT), "box fold bulb pow 2 keys and layout disagree");
+
+constexpr FormulaKey kMengerMod1Keys[] = {
+    {"transf_constant_multiplier_111", PK_VEC3, {1, 1, 1}, MMX_CM111},
+    {"transf_rotation_enabled", PK_BOOL, {0, 0, 0}, MMX_ROT_ON},
+    {"transf_start_iterations", PK_INT, {0, 0, 0}, MMX_START},
+    {"transf_stop_iterations", PK_INT, {250, 0, 0}, MMX_STOP},
+    {"transf_rotation", PK_ROT, {0, 0, 0}, MMX_ROT},
+    {"transf_scaleD_1", PK_DOUBLE, {1, 0, 0}, MMX_SCALED1},
+    {"transf_offset_1", PK_DOUBLE, {1, 0, 0}, MMX_OFFSET1},
+    {"transf_addition_constant", PK_VEC3, {0, 0, 0}, MMX_ADD000},
+    {"transf_function_enabledx_false", PK_BOOL, {0, 0, 0}, MMX_BOX_OFF},
+    {"transf_start_iterations_A", PK_INT, {0, 0, 0}, MMX_START_A},
+    {"transf_stop_iterations_A", PK_INT, {250, 0, 0}, MMX_STOP_A},
+    {"transf_addition_constantA_000", PK_VEC3, {0, 0, 0}, MMX_ADD_A000},
+    {"transf_function_enabledA_false", PK_BOOL, {0, 0, 0}, MMX_AVG_SCALE},
+    {"transf_function_enabled_false", PK_BOOL, {0, 0, 0}, MMX_BLEND},
+    {"transf_int_A", PK_INT, {0, 0, 0}, MMX_INT_A},
+    {"transf_int_B", PK_INT, {0, 0, 0}, MMX_INT_B},
+    {"transf_scale_1", PK_DOUBLE, {1, 0, 0}, MMX_SCALE1},
+    {"transf_offset", PK_DOUBLE, {0, 0, 0}, MMX_OFFSET},
+    {"transf_offset_0", PK_DOUBLE, {0, 0, 0}, MMX_OFFSET0},
+    {"transf_scale_3", PK_NAMED, {NF_SCALE3, 0, 0}, MMX_SCALE3},
+};
+static_assert(keys_contiguous(kMengerMod1Keys, MMX_COUNT), "Menger mod 1 keys and layout disagree");
 
 struct KeyTable {
   const FormulaKey *keys;
@@ -134,13 +219,19 @@ inline KeyTable formula_keys(int formula) {
   switch (formula) {
     case MBR_FORMULA_PSEUDO_KLEINIAN:
       return {kPseudoKleinianKeys, int(sizeof(kPseudoKleinianKeys) / sizeof(kPseudoKleinianKeys[0]))};
+    case MBR_FORMULA_BOX_FOLD_BULB_POW2:
+      return {kBoxFoldBulbPow2Keys, int(sizeof(kBoxFoldBulbPow2Keys) / sizeof(kBoxFoldBulbPow2Keys[0]))};
+    case MBR_FORMULA_MENGER_MOD1:
+      return {kMengerMod1Keys, int(sizeof(kMengerMod1Keys) / sizeof(kMengerMod1Keys[0]))};
     default: return {nullptr, 0};
   }
 }
 
-// The entry of `key` in the table, or -1.
+// The entry of `key` in the table, or -1 (also for a NAMED entry, whose
+// value comes from its mbr_fractal field).
 inline int find_key(const KeyTable &t, const char *key) {
   for (int i = 0; i < t.n; i++) {
+    if (t.keys[i].kind == PK_NAMED) continue;
     const char *a = t.keys[i].key;
     const char *b = key;
     while (*a && *a == *b) {
@@ -180,6 +271,17 @@ inline void keyed_rotation(const double deg[3], double *out) {
   for (int j = 0; j < 9; j++) out[1 + j] = m[j];
 }
 
+inline double named_field(const mbr_fractal &f, int id) {
+  switch (id) {
+    case NF_MB_LIMIT: return f.mandelbox_folding_limit;
+    case NF_MB_VALUE: return f.mandelbox_folding_value;
+    case NF_MB_SCALE: return f.mandelbox_scale;
+    case NF_ADE_SCALE1: return f.analytic_de_scale1;
+    case NF_ADE_OFFSET1: return f.analytic_de_offset1;
+    default: return f.transf_scale3;
+  }
+}
+
 // One value into x[] as its kind stores it: an int truncated toward zero
 // (as cParameterContainer::Set<int> of the double), a bool 0 / 1.
 inline void put_keyed(const FormulaKey &k, const double *v, double *x) {
@@ -192,9 +294,8 @@ inline void put_keyed(const FormulaKey &k, const double *v, double *x) {
   }
 }
 
-// The parameter block of a keyed formula: every key's default, then the
-// values f.param lists, then the values the formula reads from mbr_fractal's
-// named fields.  Returns -1 when the block is filled, else the index of the
+// The parameter block of a keyed formula: every key's default (a NAMED
+// entry's field), then the values f.param lists.  Returns -1 when the block is filled, else the index of the
 // first entry of f.param that is malformed (a key without its NUL, one the
 // formula does not read, a non-finite value or an int out of range); -2 when
 // n_params is out of range.
@@ -202,7 +303,10 @@ inline int pack_keyed(const mbr_fractal &f, double *x) {
   for (int j = 0; j < MBR_SLOT_X; j++) x[j] = 0.0;
   const KeyTable t = formula_keys(f.formula);
   if (f.n_params < 0 || f.n_params > MBR_MAX_FORMULA_PARAMS) return -2;
-  for (int i = 0; i < t.n; i++) put_keyed(t.keys[i], t.keys[i].def, x);
+  for (int i = 0; i < t.n; i++) {
+    if (t.keys[i].kind == PK_NAMED) x[t.keys[i].x] = named_field(f, int(t.keys[i].def[0]));
+    else put_keyed(t.keys[i], t.keys[i].def, x);
+  }
   for (int j = 0; j < f.n_params; j++) {
     const mbr_formula_param &q = f.param[j];
     bool terminated = false;
@@ -216,11 +320,6 @@ inline int pack_keyed(const mbr_fractal &f, double *x) {
       if (!std::isfinite(q.value[c])) return j;
     if (t.keys[i].kind == PK_INT && !(q.value[0] > -2147483648.0 && q.value[0] < 2147483648.0)) return j;
     put_keyed(t.keys[i], q.value, x);
-  }
-  if (f.formula == MBR_FORMULA_PSEUDO_KLEINIAN) {
-    x[PKX_MB_LIMIT] = f.mandelbox_folding_limit;
-    x[PKX_MB_VALUE] = f.mandelbox_folding_value;
-    x[PKX_DE_SCALE1] = f.analytic_de_scale1;
   }
   return -1;
 }

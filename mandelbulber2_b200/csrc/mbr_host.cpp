@@ -34,6 +34,7 @@ struct FormulaMeta {
   int cpixel;        // 0 enabled by default, 1 disabled by default
   double bailout;    // default bailout
   int analytic;      // enumDEAnalyticFunction
+  int delta;         // DEType: 1 deltaDEType, 0 analyticDEType
 };
 // cAbstractFractal metadata of the formula classes (fractal_mandelbulb.cpp:16-27,
 // fractal_mandelbulb_power2.cpp:17-28, fractal_hypercomplex.cpp:17-28,
@@ -50,6 +51,8 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_MANDELBOX: *m = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *m = {1, 1, 10.0, 3}; return true;
     case MBR_FORMULA_PSEUDO_KLEINIAN: *m = {3, 1, 100.0, 4}; return true;  // fractal_pseudo_kleinian.cpp:17-28
+    case MBR_FORMULA_BOX_FOLD_BULB_POW2: *m = {1, 0, 10000.0, 1, 1}; return true;  // fractal_box_fold_bulb_pow2.cpp:14-25
+    case MBR_FORMULA_MENGER_MOD1: *m = {1, 1, 10.0, 3}; return true;  // fractal_menger_mod1.cpp:16-27
     default: return false;
   }
 }
@@ -358,7 +361,9 @@ static mbr_status build_tree(mbr_ctx *ctx, const mbr_scene &sc, const bool live[
                                       DEF_MAX_AXIS};
       o.de_analytic = de_analytic;
       o.de_final = an_final[de_analytic];
-      o.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+      // DEType and the forcing switches (hybrid_fractal_sequences.cpp:466-474)
+      o.delta_de = (m.delta || sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA) &&
+                   sc.delta_de_method != MBR_DE_METHOD_FORCE_ANALYTIC;
       o.delta_fn = de_function;
       if (!o.delta_de && o.de_final == 0)
         return set_err(ctx, MBR_EUNSUPPORTED,
@@ -509,7 +514,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     FormulaMeta m;
     if (!formula_meta(f.formula, &m))
       return set_err(ctx, MBR_EUNSUPPORTED,
-                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 19, 103)", i, f.formula);
+                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 16, 19, 61, 103)", i, f.formula);
     any = true;
     if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
     if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)
@@ -632,9 +637,15 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     }
     d.de_analytic = (d.de_function == 2) ? 2 : 1;
     d.uniform_formula = 0;
-    // every formula built here is analytic, so only the forced method makes
-    // the sequence a delta-DE one (:463-464)
-    d.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+    // a delta-DE formula in any slot makes the sequence a delta-DE one, and
+    // the forcing switches override (:450-464)
+    bool any_delta = false;
+    for (int i = 0; i < n; i++) {
+      FormulaMeta m;
+      if (formula_meta(d.slot[i].formula, &m) && m.delta) any_delta = true;
+    }
+    d.delta_de = (any_delta || sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA) &&
+                 sc.delta_de_method != MBR_DE_METHOD_FORCE_ANALYTIC;
     static const int hyb_final[7] = {0, DEF_LINEAR_OFFSET, DEF_LOG, DEF_PSEUDO_KLEINIAN, 0, DEF_CUSTOM, DEF_MAX_AXIS};
     d.de_final = hyb_final[d.de_function];
   } else {
@@ -647,7 +658,9 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
       static const int fn_analytic[7] = {1, 1, 2, 4, 5, 6, 7};  // enumDEAnalyticFunction
       d.de_analytic = fn_analytic[d.de_function];
     }
-    d.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+    // DEType and the forcing switches (:466-474)
+    d.delta_de = (m.delta || sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA) &&
+                 sc.delta_de_method != MBR_DE_METHOD_FORCE_ANALYTIC;
     // enumDEAnalyticFunction -> DevDeFinal (Jos Kleinian: 0, refused below)
     static const int an_final[8] = {DEF_NONE, DEF_LINEAR, DEF_LOG, DEF_IFS, DEF_PSEUDO_KLEINIAN, 0, DEF_CUSTOM,
                                     DEF_MAX_AXIS};

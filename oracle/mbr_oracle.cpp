@@ -53,6 +53,7 @@ struct FormulaInfo {
   int cpixel;           // enumCPixelAddition: 0 enabled by default, 1 disabled by default, 2 already has
   double default_bailout;
   int analytic;         // enumDEAnalyticFunction
+  int delta;            // DEType: 1 deltaDEType
 };
 static bool formula_info(int formula, FormulaInfo *fi) {
   switch (formula) {
@@ -65,7 +66,9 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_AEXION: *fi = {2, 2, 10000.0, 2}; return true;           // fractal_aexion.cpp:16-27
     case MBR_FORMULA_MANDELBOX: *fi = {1, 0, 100.0, 1}; return true;
     case MBR_FORMULA_MENGER_SPONGE: *fi = {1, 1, 10.0, 3}; return true;
-    case MBR_FORMULA_PSEUDO_KLEINIAN: *fi = {3, 1, 100.0, 4}; return true;  // fractal_pseudo_kleinian.cpp:17-28
+    case MBR_FORMULA_PSEUDO_KLEINIAN: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian.cpp:17-28
+    case MBR_FORMULA_BOX_FOLD_BULB_POW2: *fi = {1, 0, 10000.0, 1, 1}; return true;  // fractal_box_fold_bulb_pow2.cpp:14-25
+    case MBR_FORMULA_MENGER_MOD1: *fi = {1, 1, 10.0, 3, 0}; return true;  // fractal_menger_mod1.cpp:16-27
     default: return false;
   }
 }
@@ -257,9 +260,15 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
       s.de_analytic = fn_analytic[s.de_function];
     }
   }
-  // every formula restated here is analytic: only the forced method makes
-  // the sequence a delta-DE one (:376-377, 463, 474)
-  s.delta_de = sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA;
+  // a delta-DE formula among the iterated slots, then the forcing switches
+  // (:376-377, 412-421, 450-474)
+  bool any_delta = false;
+  for (int i = 0; i < n; i++) {
+    FormulaInfo fi;
+    if (s.slot[i].formula != MBR_FORMULA_NONE && formula_info(s.slot[i].formula, &fi) && fi.delta) any_delta = true;
+  }
+  s.delta_de = (any_delta || sc.delta_de_method == MBR_DE_METHOD_FORCE_DELTA) &&
+               sc.delta_de_method != MBR_DE_METHOD_FORCE_ANALYTIC;
   s.delta_rel = sc.deltade_relative_delta;
   if (s.de_function < 1 || s.de_function > 6) return false;
   // the analytic Jos Kleinian function reads formula parameters not carried here
@@ -859,6 +868,101 @@ inline void formula_pseudo_kleinian(V4<S> &z, const SlotT<S> &f, S &DE, S &pk, i
   z.w = z.w + 0.0;
 }
 
+// cFractalBoxFoldBulbPow2::FormulaCode (fractal_box_fold_bulb_pow2.cpp:27-76)
+template <class S>
+inline void formula_box_fold_bulb_pow2(V4<S> &z, const SlotT<S> &f, const S &r, S &DE) {
+  using namespace mbr;
+  const double *x = f.x;
+  const double ff = x[BFX_FOLD];
+  if (fabs(z.x) > ff) z.x = S(double(sgn(val(z.x))) * ff * 2.0) - z.x;
+  if (fabs(z.y) > ff) z.y = S(double(sgn(val(z.y))) * ff * 2.0) - z.y;
+  if (fabs(z.z) > ff) z.z = S(double(sgn(val(z.z))) * ff * 2.0) - z.z;
+  const double fR2_2 = 1.0, mR2_2 = 0.25;
+  const S r2_2 = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+  const double tglad_factor1_2 = fR2_2 / mR2_2;
+  if (r2_2 < mR2_2) {
+    z = z * tglad_factor1_2;
+    DE = DE * tglad_factor1_2;
+  } else if (r2_2 < fR2_2) {
+    const S tglad_factor2_2 = fR2_2 / r2_2;
+    z = z * tglad_factor2_2;
+    DE = DE * tglad_factor2_2;
+  }
+  z = z * 2.0;
+  const S x2 = z.x * z.x, y2 = z.y * z.y, z2 = z.z * z.z;
+  const S temp = 1.0 - z2 / (x2 + y2);
+  V4<S> t;
+  t.x = (x2 - y2) * temp;
+  t.y = 2.0 * z.x * z.y * temp;
+  t.z = -2.0 * z.z * sqrt(x2 + y2);
+  t.w = z.w;
+  z = t;
+  z.z = z.z * x[BFX_ZFACTOR];
+  if (x[BFX_ADE_ON] != 0.0)  // :67-73
+    DE = (DE + 1.0) * 5.0 * r * x[BFX_ADE_SCALE1] *
+             sqrt(x[BFX_ZFACTOR] * x[BFX_ZFACTOR] + 2.0 + x[BFX_ADE_OFFSET2]) +
+         x[BFX_ADE_OFFSET1];
+}
+
+// cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
+// aux.color terms left out
+template <class S>
+inline void formula_menger_mod1(V4<S> &z, const SlotT<S> &f, S &DE, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  z = V4<S>{fabs(z.x), fabs(z.y), fabs(z.z), fabs(z.w)};
+  S temp;
+  if (z.x < z.y) {
+    temp = z.y;
+    z.y = z.x;
+    z.x = temp;
+  }
+  if (z.x < z.z) {
+    temp = z.z;
+    z.z = z.x;
+    z.x = temp;
+  }
+  if (z.y < z.z) {
+    temp = z.z;
+    z.z = z.y;
+    z.y = temp;
+  }
+  z = z * x[MMX_SCALE3];
+  z.x = z.x - 2.0 * x[MMX_CM111];
+  z.y = z.y - 2.0 * x[MMX_CM111 + 1];
+  if (z.z > 1.0) z.z = z.z - 2.0 * x[MMX_CM111 + 2];
+  DE = DE * x[MMX_SCALE3];
+  if (x[MMX_ROT_ON] != 0.0 && i >= int(x[MMX_START]) && i < int(x[MMX_STOP])) {
+    z = mb_turn(x + MMX_ROT + 1, x[MMX_ROT] != 0.0, false, z);
+    DE = DE * x[MMX_SCALED1] + x[MMX_OFFSET1];
+  }
+  z.x = z.x + x[MMX_ADD000];
+  z.y = z.y + x[MMX_ADD000 + 1];
+  z.z = z.z + x[MMX_ADD000 + 2];
+  z.w = z.w + 0.0;
+  if (x[MMX_BOX_OFF] != 0.0 && i >= int(x[MMX_START_A]) && i < int(x[MMX_STOP_A])) {  // box offset :74-89
+    const V4<S> t = z;
+    z.x = S(double(sgn(val(z.x)))) * x[MMX_ADD_A000] + z.x;
+    z.y = S(double(sgn(val(z.y)))) * x[MMX_ADD_A000 + 1] + z.y;
+    z.z = S(double(sgn(val(z.z)))) * x[MMX_ADD_A000 + 2] + z.z;
+    if (x[MMX_AVG_SCALE] != 0.0) {
+      const S tempL = len4(t);
+      const S avgScale = len4(z) / tempL;
+      DE = DE * avgScale + 1.0;
+    }
+  }
+  if (x[MMX_BLEND] != 0.0) {  // :91-102
+    const bool a = i == int(x[MMX_INT_A]), b = i == int(x[MMX_INT_B]);
+    const V4<S> zA = a ? z : V4<S>{S(0.0), S(0.0), S(0.0), S(0.0)};
+    const V4<S> zB = b ? z : V4<S>{S(0.0), S(0.0), S(0.0), S(0.0)};
+    z.x = z.x * x[MMX_SCALE1] + zA.x * x[MMX_OFFSET] + zB.x * x[MMX_OFFSET0];
+    z.y = z.y * x[MMX_SCALE1] + zA.y * x[MMX_OFFSET] + zB.y * x[MMX_OFFSET0];
+    z.z = z.z * x[MMX_SCALE1] + zA.z * x[MMX_OFFSET] + zB.z * x[MMX_OFFSET0];
+    z.w = z.w * x[MMX_SCALE1] + zA.w * x[MMX_OFFSET] + zB.w * x[MMX_OFFSET0];
+    DE = DE * x[MMX_SCALE1];
+  }
+}
+
 // cFractalHypercomplex::FormulaCode (fractal_hypercomplex.cpp:30-45)
 template <class S>
 inline void formula_hypercomplex(V4<S> &z, const S &r, S &DE) {
@@ -1063,6 +1167,8 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_QUATERNION: formula_quaternion(z, r, DE); break;
         case MBR_FORMULA_AEXION: formula_aexion(z, r, DE, sd.ifs, i, const_c); break;
         case MBR_FORMULA_PSEUDO_KLEINIAN: formula_pseudo_kleinian(z, f, DE, pk, i); break;
+        case MBR_FORMULA_BOX_FOLD_BULB_POW2: formula_box_fold_bulb_pow2(z, f, r, DE); break;
+        case MBR_FORMULA_MENGER_MOD1: formula_menger_mod1(z, f, DE, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

@@ -127,6 +127,44 @@ def _pseudo_kleinian_cases():
     return t
 
 
+def _keyed(formula, maxiter=30, **params):
+    s = abi.scene_defaults(formula)
+    s.formula_maxiter = maxiter
+    for k, v in params.items():
+        s.fractal[0].set_param(k, v)
+    return s
+
+
+def _keyed_formula_cases():
+    """Box fold bulb pow 2 (16, a delta-DE formula) and Menger mod 1 (61)."""
+    t = {}
+    t["bfbp2_default"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2, 20)
+    t["bfbp2_params"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2, 20, boxfold_bulbpow2_folding_factor=1.6,
+                               boxfold_bulbpow2_z_factor=4.0)
+    s = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2, 20, analyticDE_enabled_false=1, analyticDE_offset_2=0.5)
+    s.delta_de_method = abi.DE_METHOD_FORCE_ANALYTIC
+    s.fractal[0].analytic_de_scale1 = 0.8
+    s.fractal[0].analytic_de_offset1 = 0.3
+    t["bfbp2_forced_analytic"] = s
+    t["menger_mod1_default"] = _keyed(abi.FORMULA_MENGER_MOD1, 12)
+    s = _keyed(abi.FORMULA_MENGER_MOD1, 12, transf_constant_multiplier_111=[1.1, 0.9, 1.0],
+               transf_rotation_enabled=1, transf_rotation=[5.0, 10.0, -15.0], transf_start_iterations=1,
+               transf_scaleD_1=1.1, transf_offset_1=0.5, transf_addition_constant=[0.05, 0.0, -0.02])
+    s.fractal[0].transf_scale3 = 2.8
+    t["menger_mod1_rotation"] = s
+    t["menger_mod1_box_offset_blend"] = _keyed(
+        abi.FORMULA_MENGER_MOD1, 12, transf_function_enabledx_false=1, transf_addition_constantA_000=[0.1, 0.2, 0.0],
+        transf_function_enabledA_false=1, transf_stop_iterations_A=6, transf_function_enabled_false=1,
+        transf_int_A=2, transf_int_B=3, transf_scale_1=0.95, transf_offset=0.1, transf_offset_0=-0.05)
+    s = _keyed(abi.FORMULA_MENGER_MOD1, 15)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    s.fractal[0].formula_iterations = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_BOX_FOLD_BULB_POW2)
+    t["hybrid_menger_mod1_bfbp2"] = s
+    return t
+
+
 def cases():
     out = {}
     out["bulb_p8"] = configs.mandelbulb_scene(8.0, 250)
@@ -315,6 +353,7 @@ def cases():
         out[name] = tree
     # the pseudo-Kleinian (103), parameters by settings key
     out.update(_pseudo_kleinian_cases())
+    out.update(_keyed_formula_cases())
     # quaternion (5) and aexion (19)
     s = abi.scene_defaults(abi.FORMULA_QUATERNION)
     s.formula_maxiter = 40

@@ -195,22 +195,26 @@ def test_ifs_and_rotated_mandelbox_in_hybrids(renderer, oracle, case):
         check(renderer, sc, cam, p, o, ost, engine, case)
 
 
-PK_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk_box_folds", "pk_rotation_flip_scale",
-            "hybrid_pk_box", "pk_delta"]
+KEYED_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk_box_folds",
+               "pk_rotation_flip_scale", "hybrid_pk_box", "pk_delta", "bfbp2_default", "bfbp2_params",
+               "bfbp2_forced_analytic", "menger_mod1_default", "menger_mod1_rotation",
+               "menger_mod1_box_offset_blend", "hybrid_menger_mod1_bfbp2"]
 
 
-@pytest.mark.parametrize("case", PK_CASES)
-def test_pseudo_kleinian_distances(renderer, oracle, case):
-    """Formula 103 (fractal_pseudo_kleinian.cpp:30-202) with its parameters by
-    settings key, the pseudo-Kleinian DE state and the convergence bailout
-    (compute_fractal.cpp:323-336): the oracle equals the reference's own
-    CalculateDistance on these scenes (tests/golden/pipeline_kat.json).  The
-    formula uses +, -, *, / and fabs only (the rotation matrix is built on the
-    host), so the strict FP64 engine equals the oracle bit for bit, iteration
-    counts included.  The FMA and mixed engines are reported; their orbits
-    never escape (the convergence bailout ends them), so an FMA's rounding can
-    end one an iteration apart and no tight per-point bar holds: they are held
-    to a median relative error of 1e-6 (FMA) / 1e-3 (FP32)."""
+@pytest.mark.parametrize("case", KEYED_CASES)
+def test_keyed_formula_distances(renderer, oracle, case):
+    """The formulas whose parameters come by settings key: the pseudo-Kleinian
+    (103, fractal_pseudo_kleinian.cpp:30-202, with its DE state and the
+    convergence bailout of compute_fractal.cpp:323-336), the box fold bulb
+    pow 2 (16, a delta-DE formula) and Menger mod 1 (61).  The oracle equals
+    the reference's own CalculateDistance on these scenes
+    (tests/golden/pipeline_kat.json).  The formulas use +, -, *, /, sqrt and
+    fabs only (rotation matrices are built on the host), so the strict FP64
+    engine equals the oracle bit for bit, iteration counts included.  The FMA
+    and mixed engines are held to a median relative error of 1e-6 (FMA) and
+    1e-3 (FP32): pseudo-Kleinian orbits never escape (the convergence bailout
+    ends them) and an FMA's rounding can end one an iteration apart, so no
+    tight per-point bar holds for them.  FP32 engines refuse the delta DE."""
     from tests.golden.pipeline_cases import cases
 
     sc = cases()[case]
@@ -222,7 +226,8 @@ def test_pseudo_kleinian_distances(renderer, oracle, case):
             od, oit = oracle.distance(sc, pts, det, nm)
             d, it = renderer.distance(torch.from_numpy(pts), det, nm, abi.ENGINE_PLAIN_FP64_STRICT)
             assert np.array_equal(d.cpu().numpy(), od) and np.array_equal(it.cpu().numpy(), oit), (case, det, nm)
-            engines = [abi.ENGINE_PLAIN_FP64] + ([] if "delta" in case else [abi.ENGINE_PLAIN_MIXED])
+            delta = "delta" in case or ("bfbp2" in case and "analytic" not in case)
+            engines = [abi.ENGINE_PLAIN_FP64] + ([] if delta else [abi.ENGINE_PLAIN_MIXED])
             for engine in engines:
                 d, it = renderer.distance(torch.from_numpy(pts), det, nm, engine)
                 d, it = d.cpu().numpy(), it.cpu().numpy()
