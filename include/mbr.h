@@ -68,7 +68,9 @@ typedef enum mbr_formula {
   /* formulas whose parameters are passed by settings key (mbr_fractal.param) */
   MBR_FORMULA_BOX_FOLD_BULB_POW2 = 16, /* formula/definition/fractal_box_fold_bulb_pow2.cpp:27-76 (delta DE) */
   MBR_FORMULA_MENGER_MOD1 = 61,       /* formula/definition/fractal_menger_mod1.cpp:29-103 */
-  MBR_FORMULA_PSEUDO_KLEINIAN = 103   /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
+  MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 = 125, /* formula/definition/fractal_box_fold_bulb_pow2_v2.cpp:29-146 */
+  MBR_FORMULA_PSEUDO_KLEINIAN = 103,  /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
+  MBR_FORMULA_ABOX_MOD11 = 119        /* formula/definition/fractal_abox_mod11.cpp:34-250 */
 } mbr_formula;
 
 /* fractal::enumDEFunctionType (src/fractal_enums.h:47-60).  The Jos

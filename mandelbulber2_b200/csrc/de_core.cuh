@@ -304,6 +304,31 @@ __device__ __forceinline__ T smax(T a, T b) {
   return (a < b) ? b : a;
 }
 
+// The orbit state of sExtendedAux that keyed formulas carry from one
+// iteration to the next (compute_fractal.cpp:118-127): pk =
+// aux.pseudoKleinianDE (initially 1), scale = aux.actualScale (initially the
+// Mandelbox scale of the sequence's first slot), scaleA = aux.actualScaleA
+// (initially 0).
+template <class T>
+struct AuxX {
+  T pk, scale, scaleA;
+  V4<T> c;  // aux.c (initially the point), which aboxMod11's alternate c-addition permutes
+};
+
+// (x, y, z) reordered as mandelbulbMulti.orderOfXYZ says (enumMulti_OrderOfXYZ,
+// fractal.h:282-289): xyz, xzy, yxz, yzx, zxy, zyx; w kept
+template <class T>
+__device__ __forceinline__ V4<T> order_xyz(const V4<T> &v, int order) {
+  switch (order) {
+    case 1: return V4<T>{v.x, v.z, v.y, v.w};
+    case 2: return V4<T>{v.y, v.x, v.z, v.w};
+    case 3: return V4<T>{v.y, v.z, v.x, v.w};
+    case 4: return V4<T>{v.z, v.x, v.y, v.w};
+    case 5: return V4<T>{v.z, v.y, v.x, v.w};
+    default: return v;
+  }
+}
+
 // sign() of math_utilities.h:65-67: -1, 0 or 1
 template <class T>
 __device__ __forceinline__ T sgn_of(T v) {
@@ -445,6 +470,168 @@ __device__ __noinline__ void f_box_fold_bulb_pow2(V4<T> &z, T r, T &DE, const De
          T(x[BFX_ADE_OFFSET1]);
 }
 
+// cFractalBoxFoldBulbPow2V2::FormulaCode (fractal_box_fold_bulb_pow2_v2.cpp:
+// 29-146), the aux.color terms left out: tglad fold, spherical fold, a scale
+// that may vary from one iteration to the next (scaleA = aux.actualScaleA),
+// the power-2 bulb with its z factor
+template <class T>
+__device__ __noinline__ void f_box_fold_bulb_pow2_v2(V4<T> &z, T &DE, T &scaleA, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (i >= int(x[B2X_START_B]) && i < int(x[B2X_STOP_B])) {  // tglad fold :35-45
+    const T ax = T(x[B2X_ADD111]), ay = T(x[B2X_ADD111 + 1]), az = T(x[B2X_ADD111 + 2]);
+    z.x = m_abs(T(z.x + ax)) - m_abs(T(z.x - ax)) - z.x;
+    z.y = m_abs(T(z.y + ay)) - m_abs(T(z.y - ay)) - z.y;
+    z.z = m_abs(T(z.z + az)) - m_abs(T(z.z - az)) - z.z;
+  }
+  if (i >= int(x[B2X_START_S]) && i < int(x[B2X_STOP_S])) {  // spherical fold :48-67
+    const T rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const T ox = T(x[B2X_MB_OFFSET]), oy = T(x[B2X_MB_OFFSET + 1]), oz = T(x[B2X_MB_OFFSET + 2]);
+    z.x = z.x + ox;
+    z.y = z.y + oy;
+    z.z = z.z + oz;
+    if (rr < T(x[B2X_MINR2])) {
+      const T f1 = T(x[B2X_MAXR2] / x[B2X_MINR2]);
+      z.x = z.x * f1;
+      z.y = z.y * f1;
+      z.z = z.z * f1;
+      z.w = z.w * f1;
+      DE = DE * f1;
+    } else if (rr < T(x[B2X_MAXR2])) {
+      const T f2 = T(x[B2X_MAXR2]) / rr;
+      z.x = z.x * f2;
+      z.y = z.y * f2;
+      z.z = z.z * f2;
+      z.w = z.w * f2;
+      DE = DE * f2;
+    }
+    z.x = z.x - ox;
+    z.y = z.y - oy;
+    z.z = z.z - oz;
+  }
+  if (i >= int(x[B2X_START_C]) && i < int(x[B2X_STOP_C])) {  // scale :70-88
+    const T useScale = scaleA + T(x[B2X_SCALE]);
+    z.x = z.x * useScale;
+    z.y = z.y * useScale;
+    z.z = z.z * useScale;
+    z.w = z.w * useScale;
+    DE = DE * m_abs(useScale);
+    if (i >= int(x[B2X_START_X]) && i < int(x[B2X_STOP_X])) {
+      const T vary = T(x[B2X_SCALE_VARY]) * (m_abs(scaleA) - T(x[B2X_SCALE_B1]));
+      scaleA = (x[B2X_VARY_M] != 0.0) ? T(-vary) : T(scaleA - vary);
+    }
+  }
+  if (i >= int(x[B2X_START_A]) && i < int(x[B2X_STOP_A])) {  // :90-110
+    const T r = len4<T, true>(z);
+    DE = r * DE * T(16.0) * T(x[B2X_ADE_SCALE1]) *
+             T(sqrt(x[B2X_ZFACTOR] * x[B2X_ZFACTOR] + 2.0 + x[B2X_ADE_OFFSET2])) /
+             T(1.73205080756887729352744634150587) +
+         T(x[B2X_ADE_OFFSET1]);
+    z.x = z.x * T(2.0);
+    z.y = z.y * T(2.0);
+    z.z = z.z * T(2.0);
+    z.w = z.w * T(2.0);
+    const T x2 = z.x * z.x, y2 = z.y * z.y, z2 = z.z * z.z;
+    const T temp = T(1.0) - z2 / (x2 + y2);
+    const T nx = (x2 - y2) * temp;
+    const T ny = T(2.0) * z.x * z.y * temp;
+    const T nz = T(-2.0) * z.z * m_sqrt(T(x2 + y2));
+    z.x = nx;
+    z.y = ny;
+    z.z = nz * T(x[B2X_ZFACTOR]);
+  }
+}
+
+// cFractalAboxMod11::FormulaCode (fractal_abox_mod11.cpp:34-250), the
+// aux.color terms left out: a scale that varies with |aux.actualScale|, tglad
+// fold, the smooth fold, a swap, a spherical fold whose inner radius follows
+// a curve over the iterations, scale, offset, c-addition (optionally of aux.c
+// permuted every iteration), rotation and a tweak scale.  c: aux.const_c.
+template <class T>
+__device__ __noinline__ void f_abox_mod11(V4<T> &z, T &DE, AuxX<T> &ax, const V4<T> &c, const DevSlot &s, int i) {
+  const double *x = s.x;
+  ax.scale = T(x[ABX_MB_SCALE] + x[ABX_SCALE_VARY] * (fabs(double(ax.scale)) - 1.0));  // :36-37
+  if (i >= int(x[ABX_START_B]) && i < int(x[ABX_STOP_B])) {  // tglad fold :41-55
+    const T ax0 = T(x[ABX_ADD111]), ay = T(x[ABX_ADD111 + 1]), az = T(x[ABX_ADD111 + 2]);
+    z.x = m_abs(T(z.x + ax0)) - m_abs(T(z.x - ax0)) - z.x;
+    z.y = m_abs(T(z.y + ay)) - m_abs(T(z.y - ay)) - z.y;
+    if (x[ABX_FOLD_Z] != 0.0) z.z = m_abs(T(z.z + az)) - m_abs(T(z.z - az)) - z.z;
+  }
+  if (x[ABX_FOLD_D] != 0.0 && i >= int(x[ABX_START_D]) && i < int(x[ABX_STOP_D1])) {  // :56-77
+    T *zc[3] = {&z.x, &z.y, &z.z};
+    T add[3];
+    for (int a = 0; a < 3; a++) {
+      const double lim = x[ABX_ADD111 + a], len = 2.0 * lim, tS = 1.0 / len;
+      const T v = *zc[a], av = m_abs(v);
+      add[a] = T(0.0);
+      if (av < T(lim)) add[a] = v * v * T(tS);
+      if (av > T(lim) && av < T(len)) add[a] = (T(len) - av) * (T(len) - av) * T(tS);
+      add[a] = add[a] * T(x[ABX_SCALE3D + a]);
+    }
+    for (int a = 0; a < 3; a++) *zc[a] = *zc[a] - sgn_of(*zc[a]) * add[a];
+  }
+  if (x[ABX_SWAP] != 0.0) z = V4<T>{z.z, z.y, z.x, z.w};  // :79-82
+  if (i >= int(x[ABX_START_S]) && i < int(x[ABX_STOP_S])) {  // spherical fold :85-174
+    const double para = abox_mod11_para(x, i);
+    const T rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const T ox = T(x[ABX_MB_OFFSET]), oy = T(x[ABX_MB_OFFSET + 1]), oz = T(x[ABX_MB_OFFSET + 2]);
+    z.x = z.x + ox;
+    z.y = z.y + oy;
+    z.z = z.z + oz;
+    if (rr < T(para)) {
+      const T f1 = T(x[ABX_MAXR2] / para);
+      z.x = z.x * f1;
+      z.y = z.y * f1;
+      z.z = z.z * f1;
+      z.w = z.w * f1;
+      DE = DE * f1;
+    } else if (rr < T(x[ABX_MAXR2])) {
+      const T f2 = T(x[ABX_MAXR2]) / rr;
+      z.x = z.x * f2;
+      z.y = z.y * f2;
+      z.z = z.z * f2;
+      z.w = z.w * f2;
+      DE = DE * f2;
+    }
+    z.x = z.x - ox;
+    z.y = z.y - oy;
+    z.z = z.z - oz;
+  }
+  if (i >= int(x[ABX_START_A]) && i < int(x[ABX_STOP_A])) {  // scale :177-186
+    z.x = z.x * ax.scale;
+    z.y = z.y * ax.scale;
+    z.z = z.z * ax.scale;
+    z.w = z.w * ax.scale;
+    if (x[ABX_ADE_ON] == 0.0) DE = DE * m_abs(ax.scale) + T(1.0);
+    else DE = DE * m_abs(ax.scale) * T(x[ABX_ADE_SCALE1]) + T(x[ABX_ADE_OFFSET1]);
+  }
+  z.x = z.x + T(x[ABX_ADD000]);  // :188
+  z.y = z.y + T(x[ABX_ADD000 + 1]);
+  z.z = z.z + T(x[ABX_ADD000 + 2]);
+  if (x[ABX_ADDC] != 0.0 && i >= int(x[ABX_START_E]) && i < int(x[ABX_STOP_E])) {  // :191-225
+    V4<T> t;
+    if (x[ABX_ALTERNATE] != 0.0) {
+      t = order_xyz(ax.c, int(x[ABX_ORDER]));
+      ax.c = t;
+    } else {
+      t = order_xyz(c, int(x[ABX_ORDER]));
+    }
+    z.x = z.x + t.x * T(x[ABX_CM111]);
+    z.y = z.y + t.y * T(x[ABX_CM111 + 1]);
+    z.z = z.z + t.z * T(x[ABX_CM111 + 2]);
+    z.w = z.w + t.w * T(1.0);
+  }
+  if (x[ABX_ROT_ON] != 0.0 && i >= int(x[ABX_START_R]) && i < int(x[ABX_STOP_R]) && x[ABX_ROT] == 0.0)
+    z = mb_turn<T>(x + ABX_ROT + 1, false, z);  // :227-232
+  if (i >= int(x[ABX_START_C]) && i < int(x[ABX_STOP_C1])) {  // tweak scale :234-239
+    const T g = T(x[ABX_SCALE_G1]);
+    z.x = z.x * g;
+    z.y = z.y * g;
+    z.z = z.z * g;
+    z.w = z.w * g;
+    DE = DE * T(fabs(x[ABX_SCALE_G1]));
+  }
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -563,10 +750,13 @@ __device__ __forceinline__ void f_ifs(V4<T> &z, T &DE, const IfsBlock &b) {
 // replaces at its first iteration.
 template <class T, bool W, bool EXT = false>
 __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &DE, const DevSlot &s,
-                                                 const MbRot *rot, const IfsBlock *ifs, int i, V4<T> &c, T &pk) {
+                                                 const MbRot *rot, const IfsBlock *ifs, int i, V4<T> &c,
+                                                 AuxX<T> &ax) {
   if constexpr (EXT) {
     switch (formula) {
-      case MBR_FORMULA_PSEUDO_KLEINIAN: f_pseudo_kleinian<T>(z, DE, pk, s, i); break;
+      case MBR_FORMULA_PSEUDO_KLEINIAN: f_pseudo_kleinian<T>(z, DE, ax.pk, s, i); break;
+      case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: f_box_fold_bulb_pow2_v2<T>(z, DE, ax.scaleA, s, i); break;
+      case MBR_FORMULA_ABOX_MOD11: f_abox_mod11<T>(z, DE, ax, c, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
@@ -824,7 +1014,9 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
   V4<T> c = z;  // aux.const_c
   r = len4<T, W>(z);
   DE = T(1.0);
-  T pk = T(1.0);  // aux.pseudoKleinianDE (compute_fractal.cpp:120)
+  AuxX<T> ax{T(1.0), T(0.0), T(0.0), z};
+  if (F == F_EXT)  // aux.actualScale: the Mandelbox scale of the sequence's first slot (compute_fractal.cpp:97-98, 123)
+    ax.scale = T(sc.slot[TREE ? nd->slot : int(sc.seq[0])].d[P_MB_SCALE]);
   V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)}, lastLastZ = lastZ;
   maxiter = true;
   int i;
@@ -841,7 +1033,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
       if (F == MBR_FORMULA_MANDELBOX) f_mandelbox<T, W>(z, DE, s);
       if (F == MBR_FORMULA_MENGER_SPONGE) f_menger<T, W>(z, DE, s);
     } else if (s.d[P_WEIGHT] > 0.0) {
-      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c, pk);
+      formula_dispatch<T, W, F == F_EXT>(s.formula, z, r, DE, s, &sc.mbrot, &sc.ifs, i, c, ax);
     }
     if (s.add_c) {
       if (TREE ? nd->julia : sc.julia) {
@@ -883,7 +1075,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
         break;
     }
   }
-  if (pk_out) *pk_out = pk;
+  if (pk_out) *pk_out = ax.pk;
   return i;
 }
 

@@ -16,11 +16,17 @@
 
 #include "../../include/mbr.h"
 
-#define MBR_SLOT_X 64  // entries of a slot's keyed parameter block
+#define MBR_SLOT_X 80  // entries of a slot's keyed parameter block
+
+#ifdef __CUDACC__
+#define MBR_HD __host__ __device__
+#else
+#define MBR_HD
+#endif
 
 namespace mbr {
 
-enum ParamKind { PK_INT = 0, PK_DOUBLE = 1, PK_BOOL = 2, PK_VEC3 = 3, PK_ROT = 4, PK_NAMED = 5 };
+enum ParamKind { PK_INT = 0, PK_DOUBLE = 1, PK_BOOL = 2, PK_VEC3 = 3, PK_ROT = 4, PK_NAMED = 5, PK_NAMED3 = 6 };
 
 // the named mbr_fractal fields a NAMED entry reads
 enum NamedField {
@@ -29,8 +35,16 @@ enum NamedField {
   NF_MB_SCALE,       // mandelbox_scale
   NF_ADE_SCALE1,     // analytic_de_scale1 (analyticDE_scale_1)
   NF_ADE_OFFSET1,    // analytic_de_offset1 (analyticDE_offset_1)
-  NF_SCALE3          // transf_scale3 (transf_scale_3)
+  NF_SCALE3,         // transf_scale3 (transf_scale_3)
+  NF_MB_OFFSET       // mandelbox_offset (a vector: NAMED3)
 };
+
+// formulas that carry orbit state (AuxX) or end orbits by the convergence
+// bailout: the FP32 wavefront's iteration does not carry them
+inline MBR_HD bool keyed_formula_has_state(int formula) {
+  return formula == MBR_FORMULA_PSEUDO_KLEINIAN || formula == MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 ||
+         formula == MBR_FORMULA_ABOX_MOD11;
+}
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
 // 30-202): sphere inversion, prism shape, abs-box and box folds, the
@@ -114,6 +128,133 @@ enum MengerMod1X {
   MMX_COUNT = 35
 };
 
+// cFractalBoxFoldBulbPow2V2 (formula/definition/fractal_box_fold_bulb_pow2_v2.cpp:29-146)
+enum BoxFoldBulbPow2V2X {
+  B2X_ADD111 = 0,     // transf_addition_constant_111 (3)
+  B2X_START_B = 3,    // transf_start_iterations_B
+  B2X_STOP_B = 4,     // transf_stop_iterations_B
+  B2X_START_S = 5,    // transf_start_iterations_S
+  B2X_STOP_S = 6,     // transf_stop_iterations_S
+  B2X_MINR2 = 7,      // transf_minR2_p25
+  B2X_MAXR2 = 8,      // transf_maxR2_1
+  B2X_START_C = 9,    // transf_start_iterations_C
+  B2X_STOP_C = 10,    // transf_stop_iterations_C
+  B2X_SCALE = 11,     // transf_scale
+  B2X_START_X = 12,   // transf_start_iterations_X
+  B2X_STOP_X = 13,    // transf_stop_iterations_X
+  B2X_SCALE_VARY = 14,  // transf_scale_vary_0
+  B2X_SCALE_B1 = 15,  // transf_scaleB_1
+  B2X_VARY_M = 16,    // transf_function_enabledM_false
+  B2X_START_A = 17,   // transf_start_iterations_A
+  B2X_STOP_A = 18,    // transf_stop_iterations_A
+  B2X_ZFACTOR = 19,   // boxfold_bulbpow2_z_factor
+  B2X_ADE_OFFSET2 = 20,  // analyticDE_offset_2
+  B2X_MB_OFFSET = 21,    // mandelbox_offset (named, 3)
+  B2X_ADE_SCALE1 = 24,   // analyticDE_scale_1 (named)
+  B2X_ADE_OFFSET1 = 25,  // analyticDE_offset_1 (named)
+  B2X_COUNT = 26
+};
+
+// cFractalAboxMod11 (formula/definition/fractal_abox_mod11.cpp:34-250)
+enum AboxMod11X {
+  ABX_SCALE_VARY = 0,   // mandelbox_vary_scale_vary
+  ABX_ADD111 = 1,       // transf_addition_constant_111 (3)
+  ABX_START_B = 4,      // transf_start_iterations_B
+  ABX_STOP_B = 5,       // transf_stop_iterations_B
+  ABX_FOLD_Z = 6,       // transf_function_enabled
+  ABX_FOLD_D = 7,       // transf_function_enabled_false
+  ABX_START_D = 8,      // transf_start_iterations_D
+  ABX_STOP_D1 = 9,      // transf_stop_iterations_D1
+  ABX_SCALE3D = 10,     // transf_scale3D_000 (3)
+  ABX_SWAP = 13,        // transf_function_enabledSw_false
+  ABX_START_S = 14,     // transf_start_iterations_S
+  ABX_STOP_S = 15,      // transf_stop_iterations_S
+  ABX_PARA = 16,        // transf_function_enabledy_false
+  ABX_CP_LINEAR = 17,   // Cpara_enabledLinear
+  ABX_CP_PARA00 = 18,   // Cpara_para00
+  ABX_CP_PARAA = 19,    // Cpara_paraA
+  ABX_CP_PARAB = 20,    // Cpara_paraB
+  ABX_CP_PARAC = 21,    // Cpara_paraC
+  ABX_CP_ITERA = 22,    // Cpara_iterA
+  ABX_CP_ITERB = 23,    // Cpara_iterB
+  ABX_CP_ITERC = 24,    // Cpara_iterC
+  ABX_CP_CURVES = 25,   // Cpara_enabledCurves
+  ABX_CP_PARAB_ON = 26, // Cpara_enabledParab_false
+  ABX_CP_OFFSET0 = 27,  // Cpara_parab_offset0
+  ABX_CP_SLOPE = 28,    // Cpara_parab_slope
+  ABX_CP_SCALE = 29,    // Cpara_parab_scale
+  ABX_MINR2 = 30,       // transf_minR2_p25
+  ABX_MAXR2 = 31,       // transf_maxR2_1
+  ABX_START_A = 32,     // transf_start_iterations_A
+  ABX_STOP_A = 33,      // transf_stop_iterations_A
+  ABX_ADE_ON = 34,      // analyticDE_enabled_false
+  ABX_ADD000 = 35,      // transf_addition_constant (3)
+  ABX_ADDC = 38,        // transf_addCpixel_enabled_false
+  ABX_START_E = 39,     // transf_start_iterations_E
+  ABX_STOP_E = 40,      // transf_stop_iterations_E
+  ABX_ALTERNATE = 41,   // transf_alternate_enabled_false
+  ABX_ORDER = 42,       // mandelbulbMulti_order_of_xyz
+  ABX_CM111 = 43,       // transf_constant_multiplier_111 (3)
+  ABX_ROT_ON = 46,      // transf_rotation_enabled
+  ABX_START_R = 47,     // transf_start_iterations_R
+  ABX_STOP_R = 48,      // transf_stop_iterations_R
+  ABX_ROT = 49,         // transf_rotation (10)
+  ABX_START_C = 59,     // transf_start_iterations_C
+  ABX_STOP_C1 = 60,     // transf_stop_iterations_C1
+  ABX_SCALE_G1 = 61,    // transf_scaleG_1
+  ABX_MB_OFFSET = 62,   // mandelbox_offset (named, 3)
+  ABX_MB_SCALE = 65,    // mandelbox_scale (named)
+  ABX_ADE_SCALE1 = 66,  // analyticDE_scale_1 (named)
+  ABX_ADE_OFFSET1 = 67, // analyticDE_offset_1 (named)
+  ABX_COUNT = 68
+};
+static_assert(ABX_COUNT <= MBR_SLOT_X, "Abox mod 11 block exceeds the slot's parameter block");
+
+// aboxMod11's parameter curve (fractal_abox_mod11.cpp:96-156): the value
+// added to the minimum radius^2 of the spherical fold at iteration i, in
+// double precision as the reference computes it (it depends on i only)
+inline MBR_HD double abox_mod11_para(const double *x, int i) {
+  double para = 0.0, paraAddP0 = 0.0;
+  if (x[ABX_PARA] != 0.0) {
+    if (x[ABX_CP_LINEAR] != 0.0) {
+      const int iterA = int(x[ABX_CP_ITERA]), iterB = int(x[ABX_CP_ITERB]), iterC = int(x[ABX_CP_ITERC]);
+      para = x[ABX_CP_PARA00];
+      const double temp0 = para, tempA = x[ABX_CP_PARAA], tempB = x[ABX_CP_PARAB], tempC = x[ABX_CP_PARAC];
+      const double lengthAB = double(iterB - iterA);
+      const double lengthBC = double(iterC - iterB);
+      const double grade1 = (tempA - temp0) / double(iterA);
+      const double grade2 = (tempB - tempA) / lengthAB;
+      const double grade3 = (tempC - tempB) / lengthBC;
+      if (i < iterA) para = temp0 + (double(i) * grade1);
+      if (i < iterB && i >= iterA) para = tempA + double(i - iterA) * grade2;
+      if (i >= iterB) para = tempB + double(i - iterB) * grade3;
+      if (x[ABX_CP_CURVES] != 0.0) {
+        double paraAdd = 0.0, paraIt;
+        if (lengthAB > 2.0 * double(iterA)) {
+          const double curve1 = (grade2 - grade1) / (4.0 * double(iterA));
+          const double tempL = lengthAB - double(iterA);
+          const double curve2 = (grade3 - grade2) / (4.0 * tempL);
+          if (i < 2 * iterA) {
+            paraIt = tempA - fabs(tempA - double(i));
+            paraAdd = paraIt * paraIt * curve1;
+          }
+          if (i >= 2 * iterA && double(i) < double(iterB) + tempL) {
+            paraIt = tempB - fabs(tempB * double(i));
+            paraAdd = paraIt * paraIt * curve2;
+          }
+          para += paraAdd;
+        }
+      }
+    }
+    paraAddP0 = 0.0;
+    if (x[ABX_CP_PARAB_ON] != 0.0)
+      paraAddP0 = x[ABX_CP_OFFSET0] + (double(i) * x[ABX_CP_SLOPE]) + (double(i * i) * 0.001 * x[ABX_CP_SCALE]);
+  }
+  para += paraAddP0 + x[ABX_MINR2];
+  return para;
+}
+
+
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
   const char *key;
@@ -122,7 +263,9 @@ struct FormulaKey {
   int x;  // first x[] entry
 };
 
-constexpr int param_kind_size(int kind) { return kind == PK_VEC3 ? 3 : (kind == PK_ROT ? 10 : 1); }
+constexpr int param_kind_size(int kind) {
+  return (kind == PK_VEC3 || kind == PK_NAMED3) ? 3 : (kind == PK_ROT ? 10 : 1);
+}
 
 // true when the table's entries follow one another in x[] from 0 to end
 template <int N>
@@ -209,6 +352,85 @@ constexpr FormulaKey kMengerMod1Keys[] = {
 };
 static_assert(keys_contiguous(kMengerMod1Keys, MMX_COUNT), "Menger mod 1 keys and layout disagree");
 
+constexpr FormulaKey kBoxFoldBulbPow2V2Keys[] = {
+    {"transf_addition_constant_111", PK_VEC3, {1, 1, 1}, B2X_ADD111},
+    {"transf_start_iterations_B", PK_INT, {0, 0, 0}, B2X_START_B},
+    {"transf_stop_iterations_B", PK_INT, {250, 0, 0}, B2X_STOP_B},
+    {"transf_start_iterations_S", PK_INT, {0, 0, 0}, B2X_START_S},
+    {"transf_stop_iterations_S", PK_INT, {250, 0, 0}, B2X_STOP_S},
+    {"transf_minR2_p25", PK_DOUBLE, {0.25, 0, 0}, B2X_MINR2},
+    {"transf_maxR2_1", PK_DOUBLE, {1, 0, 0}, B2X_MAXR2},
+    {"transf_start_iterations_C", PK_INT, {0, 0, 0}, B2X_START_C},
+    {"transf_stop_iterations_C", PK_INT, {250, 0, 0}, B2X_STOP_C},
+    {"transf_scale", PK_DOUBLE, {1, 0, 0}, B2X_SCALE},
+    {"transf_start_iterations_X", PK_INT, {0, 0, 0}, B2X_START_X},
+    {"transf_stop_iterations_X", PK_INT, {250, 0, 0}, B2X_STOP_X},
+    {"transf_scale_vary_0", PK_DOUBLE, {0, 0, 0}, B2X_SCALE_VARY},
+    {"transf_scaleB_1", PK_DOUBLE, {1, 0, 0}, B2X_SCALE_B1},
+    {"transf_function_enabledM_false", PK_BOOL, {0, 0, 0}, B2X_VARY_M},
+    {"transf_start_iterations_A", PK_INT, {0, 0, 0}, B2X_START_A},
+    {"transf_stop_iterations_A", PK_INT, {250, 0, 0}, B2X_STOP_A},
+    {"boxfold_bulbpow2_z_factor", PK_DOUBLE, {5, 0, 0}, B2X_ZFACTOR},
+    {"analyticDE_offset_2", PK_DOUBLE, {1, 0, 0}, B2X_ADE_OFFSET2},
+    {"mandelbox_offset", PK_NAMED3, {NF_MB_OFFSET, 0, 0}, B2X_MB_OFFSET},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1, 0, 0}, B2X_ADE_SCALE1},
+    {"analyticDE_offset_1", PK_NAMED, {NF_ADE_OFFSET1, 0, 0}, B2X_ADE_OFFSET1},
+};
+static_assert(keys_contiguous(kBoxFoldBulbPow2V2Keys, B2X_COUNT), "box fold bulb pow 2 V2 keys and layout disagree");
+
+constexpr FormulaKey kAboxMod11Keys[] = {
+    {"mandelbox_vary_scale_vary", PK_DOUBLE, {0, 0, 0}, ABX_SCALE_VARY},
+    {"transf_addition_constant_111", PK_VEC3, {1, 1, 1}, ABX_ADD111},
+    {"transf_start_iterations_B", PK_INT, {0, 0, 0}, ABX_START_B},
+    {"transf_stop_iterations_B", PK_INT, {250, 0, 0}, ABX_STOP_B},
+    {"transf_function_enabled", PK_BOOL, {1, 0, 0}, ABX_FOLD_Z},
+    {"transf_function_enabled_false", PK_BOOL, {0, 0, 0}, ABX_FOLD_D},
+    {"transf_start_iterations_D", PK_INT, {0, 0, 0}, ABX_START_D},
+    {"transf_stop_iterations_D1", PK_INT, {1, 0, 0}, ABX_STOP_D1},
+    {"transf_scale3D_000", PK_VEC3, {0, 0, 0}, ABX_SCALE3D},
+    {"transf_function_enabledSw_false", PK_BOOL, {0, 0, 0}, ABX_SWAP},
+    {"transf_start_iterations_S", PK_INT, {0, 0, 0}, ABX_START_S},
+    {"transf_stop_iterations_S", PK_INT, {250, 0, 0}, ABX_STOP_S},
+    {"transf_function_enabledy_false", PK_BOOL, {0, 0, 0}, ABX_PARA},
+    {"Cpara_enabledLinear", PK_BOOL, {1, 0, 0}, ABX_CP_LINEAR},
+    {"Cpara_para00", PK_DOUBLE, {0, 0, 0}, ABX_CP_PARA00},
+    {"Cpara_paraA", PK_DOUBLE, {1, 0, 0}, ABX_CP_PARAA},
+    {"Cpara_paraB", PK_DOUBLE, {1, 0, 0}, ABX_CP_PARAB},
+    {"Cpara_paraC", PK_DOUBLE, {1, 0, 0}, ABX_CP_PARAC},
+    {"Cpara_iterA", PK_INT, {250, 0, 0}, ABX_CP_ITERA},
+    {"Cpara_iterB", PK_INT, {250, 0, 0}, ABX_CP_ITERB},
+    {"Cpara_iterC", PK_INT, {250, 0, 0}, ABX_CP_ITERC},
+    {"Cpara_enabledCurves", PK_BOOL, {1, 0, 0}, ABX_CP_CURVES},
+    {"Cpara_enabledParab_false", PK_BOOL, {0, 0, 0}, ABX_CP_PARAB_ON},
+    {"Cpara_parab_offset0", PK_DOUBLE, {0, 0, 0}, ABX_CP_OFFSET0},
+    {"Cpara_parab_slope", PK_DOUBLE, {0, 0, 0}, ABX_CP_SLOPE},
+    {"Cpara_parab_scale", PK_DOUBLE, {0, 0, 0}, ABX_CP_SCALE},
+    {"transf_minR2_p25", PK_DOUBLE, {0.25, 0, 0}, ABX_MINR2},
+    {"transf_maxR2_1", PK_DOUBLE, {1, 0, 0}, ABX_MAXR2},
+    {"transf_start_iterations_A", PK_INT, {0, 0, 0}, ABX_START_A},
+    {"transf_stop_iterations_A", PK_INT, {250, 0, 0}, ABX_STOP_A},
+    {"analyticDE_enabled_false", PK_BOOL, {0, 0, 0}, ABX_ADE_ON},
+    {"transf_addition_constant", PK_VEC3, {0, 0, 0}, ABX_ADD000},
+    {"transf_addCpixel_enabled_false", PK_BOOL, {0, 0, 0}, ABX_ADDC},
+    {"transf_start_iterations_E", PK_INT, {0, 0, 0}, ABX_START_E},
+    {"transf_stop_iterations_E", PK_INT, {250, 0, 0}, ABX_STOP_E},
+    {"transf_alternate_enabled_false", PK_BOOL, {0, 0, 0}, ABX_ALTERNATE},
+    {"mandelbulbMulti_order_of_xyz", PK_INT, {0, 0, 0}, ABX_ORDER},
+    {"transf_constant_multiplier_111", PK_VEC3, {1, 1, 1}, ABX_CM111},
+    {"transf_rotation_enabled", PK_BOOL, {0, 0, 0}, ABX_ROT_ON},
+    {"transf_start_iterations_R", PK_INT, {0, 0, 0}, ABX_START_R},
+    {"transf_stop_iterations_R", PK_INT, {250, 0, 0}, ABX_STOP_R},
+    {"transf_rotation", PK_ROT, {0, 0, 0}, ABX_ROT},
+    {"transf_start_iterations_C", PK_INT, {0, 0, 0}, ABX_START_C},
+    {"transf_stop_iterations_C1", PK_INT, {1, 0, 0}, ABX_STOP_C1},
+    {"transf_scaleG_1", PK_DOUBLE, {1, 0, 0}, ABX_SCALE_G1},
+    {"mandelbox_offset", PK_NAMED3, {NF_MB_OFFSET, 0, 0}, ABX_MB_OFFSET},
+    {"mandelbox_scale", PK_NAMED, {NF_MB_SCALE, 0, 0}, ABX_MB_SCALE},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1, 0, 0}, ABX_ADE_SCALE1},
+    {"analyticDE_offset_1", PK_NAMED, {NF_ADE_OFFSET1, 0, 0}, ABX_ADE_OFFSET1},
+};
+static_assert(keys_contiguous(kAboxMod11Keys, ABX_COUNT), "Abox mod 11 keys and layout disagree");
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -223,6 +445,10 @@ inline KeyTable formula_keys(int formula) {
       return {kBoxFoldBulbPow2Keys, int(sizeof(kBoxFoldBulbPow2Keys) / sizeof(kBoxFoldBulbPow2Keys[0]))};
     case MBR_FORMULA_MENGER_MOD1:
       return {kMengerMod1Keys, int(sizeof(kMengerMod1Keys) / sizeof(kMengerMod1Keys[0]))};
+    case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2:
+      return {kBoxFoldBulbPow2V2Keys, int(sizeof(kBoxFoldBulbPow2V2Keys) / sizeof(kBoxFoldBulbPow2V2Keys[0]))};
+    case MBR_FORMULA_ABOX_MOD11:
+      return {kAboxMod11Keys, int(sizeof(kAboxMod11Keys) / sizeof(kAboxMod11Keys[0]))};
     default: return {nullptr, 0};
   }
 }
@@ -231,7 +457,7 @@ inline KeyTable formula_keys(int formula) {
 // value comes from its mbr_fractal field).
 inline int find_key(const KeyTable &t, const char *key) {
   for (int i = 0; i < t.n; i++) {
-    if (t.keys[i].kind == PK_NAMED) continue;
+    if (t.keys[i].kind == PK_NAMED || t.keys[i].kind == PK_NAMED3) continue;
     const char *a = t.keys[i].key;
     const char *b = key;
     while (*a && *a == *b) {
@@ -304,8 +530,13 @@ inline int pack_keyed(const mbr_fractal &f, double *x) {
   const KeyTable t = formula_keys(f.formula);
   if (f.n_params < 0 || f.n_params > MBR_MAX_FORMULA_PARAMS) return -2;
   for (int i = 0; i < t.n; i++) {
-    if (t.keys[i].kind == PK_NAMED) x[t.keys[i].x] = named_field(f, int(t.keys[i].def[0]));
-    else put_keyed(t.keys[i], t.keys[i].def, x);
+    if (t.keys[i].kind == PK_NAMED) {
+      x[t.keys[i].x] = named_field(f, int(t.keys[i].def[0]));
+    } else if (t.keys[i].kind == PK_NAMED3) {  // mandelbox_offset, the one vector field
+      for (int c = 0; c < 3; c++) x[t.keys[i].x + c] = f.mandelbox_offset[c];
+    } else {
+      put_keyed(t.keys[i], t.keys[i].def, x);
+    }
   }
   for (int j = 0; j < f.n_params; j++) {
     const mbr_formula_param &q = f.param[j];

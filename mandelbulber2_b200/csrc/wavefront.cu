@@ -476,8 +476,8 @@ struct PrecHybT {
     const float tempDE = de;
     // the Aexion, the one formula that replaces c, is 4-D and never runs here
     V4<float> c{e.cx, e.cy, e.cz, 0.0f};
-    float pk = 1.0f;  // pseudo-Kleinian formulas do not run here (check_supported)
-    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs, i, c, pk);
+    AuxX<float> ax{1.0f, 0.0f, 0.0f, c};  // formulas with orbit state do not run here (check_supported)
+    if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs, i, c, ax);
     if (s.add_c) {
       if (sc.julia) {
         z.x = z.x + juliac_of<float>(sc, 0);
@@ -1876,10 +1876,10 @@ static mbr_status check_supported(mbr_ctx *ctx, const DevScene &sc, const DevFra
   if (sc.n_nodes > 0)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: explicit objects trees use the plain engines");
   for (int k = 0; k < MBR_MAX_FRACTALS; k++)
-    if (sc.slot[k].add_bail || sc.slot[k].formula == MBR_FORMULA_PSEUDO_KLEINIAN)
+    if (sc.slot[k].add_bail || keyed_formula_has_state(sc.slot[k].formula))
       return set_err(ctx, MBR_EUNSUPPORTED,
-                     "wavefront engine: pseudo-Kleinian formulas (their convergence bailout and DE state) use the "
-                     "plain engines");
+                     "wavefront engine: formulas with a convergence bailout or orbit state (pseudo-Kleinian, "
+                     "Abox mod 11, box fold bulb pow 2 V2) use the plain engines");
   if (fr.slow_shading)
     return set_err(ctx, MBR_EUNSUPPORTED, "wavefront engine: slow shading (iteration-count normals) uses the plain "
                                           "engines");

@@ -69,6 +69,8 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_PSEUDO_KLEINIAN: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian.cpp:17-28
     case MBR_FORMULA_BOX_FOLD_BULB_POW2: *fi = {1, 0, 10000.0, 1, 1}; return true;  // fractal_box_fold_bulb_pow2.cpp:14-25
     case MBR_FORMULA_MENGER_MOD1: *fi = {1, 1, 10.0, 3, 0}; return true;  // fractal_menger_mod1.cpp:16-27
+    case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: *fi = {2, 0, 100.0, 2, 0}; return true;  // fractal_box_fold_bulb_pow2_v2.cpp:16-27
+    case MBR_FORMULA_ABOX_MOD11: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_abox_mod11.cpp:21-32
     default: return false;
   }
 }
@@ -904,6 +906,159 @@ inline void formula_box_fold_bulb_pow2(V4<S> &z, const SlotT<S> &f, const S &r, 
          x[BFX_ADE_OFFSET1];
 }
 
+// cFractalBoxFoldBulbPow2V2::FormulaCode (fractal_box_fold_bulb_pow2_v2.cpp:
+// 29-146) without the aux.color terms; scaleA is aux.actualScaleA
+template <class S>
+inline void formula_box_fold_bulb_pow2_v2(V4<S> &z, const SlotT<S> &f, S &DE, S &scaleA, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  if (i >= int(x[B2X_START_B]) && i < int(x[B2X_STOP_B])) {  // :35-45
+    z.x = fabs(z.x + x[B2X_ADD111]) - fabs(z.x - x[B2X_ADD111]) - z.x;
+    z.y = fabs(z.y + x[B2X_ADD111 + 1]) - fabs(z.y - x[B2X_ADD111 + 1]) - z.y;
+    z.z = fabs(z.z + x[B2X_ADD111 + 2]) - fabs(z.z - x[B2X_ADD111 + 2]) - z.z;
+  }
+  if (i >= int(x[B2X_START_S]) && i < int(x[B2X_STOP_S])) {  // :48-67
+    const S rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    z.x = z.x + x[B2X_MB_OFFSET];
+    z.y = z.y + x[B2X_MB_OFFSET + 1];
+    z.z = z.z + x[B2X_MB_OFFSET + 2];
+    z.w = z.w + 0.0;
+    if (rr < x[B2X_MINR2]) {
+      const double tglad_factor1 = x[B2X_MAXR2] / x[B2X_MINR2];
+      z = z * tglad_factor1;
+      DE = DE * tglad_factor1;
+    } else if (rr < x[B2X_MAXR2]) {
+      const S tglad_factor2 = x[B2X_MAXR2] / rr;
+      z = z * tglad_factor2;
+      DE = DE * tglad_factor2;
+    }
+    z.x = z.x - x[B2X_MB_OFFSET];
+    z.y = z.y - x[B2X_MB_OFFSET + 1];
+    z.z = z.z - x[B2X_MB_OFFSET + 2];
+    z.w = z.w - 0.0;
+  }
+  if (i >= int(x[B2X_START_C]) && i < int(x[B2X_STOP_C])) {  // :70-88
+    const S useScale = scaleA + x[B2X_SCALE];
+    z = z * useScale;
+    DE = DE * fabs(useScale);
+    if (i >= int(x[B2X_START_X]) && i < int(x[B2X_STOP_X])) {
+      const S vary = x[B2X_SCALE_VARY] * (fabs(scaleA) - x[B2X_SCALE_B1]);
+      if (x[B2X_VARY_M] != 0.0) scaleA = -vary;
+      else scaleA = scaleA - vary;
+    }
+  }
+  if (i >= int(x[B2X_START_A]) && i < int(x[B2X_STOP_A])) {  // :90-110
+    const S r = len4(z);
+    DE = r * DE * 16.0 * x[B2X_ADE_SCALE1] * sqrt(x[B2X_ZFACTOR] * x[B2X_ZFACTOR] + 2.0 + x[B2X_ADE_OFFSET2]) /
+             1.73205080756887729352744634150587 +
+         x[B2X_ADE_OFFSET1];
+    z = z * 2.0;
+    const S x2 = z.x * z.x, y2 = z.y * z.y, z2 = z.z * z.z;
+    const S temp = 1.0 - z2 / (x2 + y2);
+    V4<S> t;
+    t.x = (x2 - y2) * temp;
+    t.y = 2.0 * z.x * z.y * temp;
+    t.z = -2.0 * z.z * sqrt(x2 + y2);
+    t.w = z.w;
+    z = t;
+    z.z = z.z * x[B2X_ZFACTOR];
+  }
+}
+
+// (x, y, z) in the order of enumMulti_OrderOfXYZ (fractal.h:282-289)
+template <class S>
+inline V4<S> order_xyz(const V4<S> &v, int order) {
+  switch (order) {
+    case 1: return V4<S>{v.x, v.z, v.y, v.w};
+    case 2: return V4<S>{v.y, v.x, v.z, v.w};
+    case 3: return V4<S>{v.y, v.z, v.x, v.w};
+    case 4: return V4<S>{v.z, v.x, v.y, v.w};
+    case 5: return V4<S>{v.z, v.y, v.x, v.w};
+    default: return v;
+  }
+}
+
+// cFractalAboxMod11::FormulaCode (fractal_abox_mod11.cpp:34-250) without the
+// aux.color terms; actualScale and auxC are aux.actualScale and aux.c, c is
+// aux.const_c
+template <class S>
+inline void formula_abox_mod11(V4<S> &z, const SlotT<S> &f, S &DE, S &actualScale, V4<S> &auxC, const V4<S> &c,
+                               int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  actualScale = x[ABX_MB_SCALE] + x[ABX_SCALE_VARY] * (fabs(actualScale) - 1.0);
+  if (i >= int(x[ABX_START_B]) && i < int(x[ABX_STOP_B])) {
+    z.x = fabs(z.x + x[ABX_ADD111]) - fabs(z.x - x[ABX_ADD111]) - z.x;
+    z.y = fabs(z.y + x[ABX_ADD111 + 1]) - fabs(z.y - x[ABX_ADD111 + 1]) - z.y;
+    if (x[ABX_FOLD_Z] != 0.0) z.z = fabs(z.z + x[ABX_ADD111 + 2]) - fabs(z.z - x[ABX_ADD111 + 2]) - z.z;
+  }
+  if (x[ABX_FOLD_D] != 0.0 && i >= int(x[ABX_START_D]) && i < int(x[ABX_STOP_D1])) {
+    const double limit[3] = {x[ABX_ADD111], x[ABX_ADD111 + 1], x[ABX_ADD111 + 2]};
+    S add[3] = {S(0.0), S(0.0), S(0.0)};
+    const S zz[3] = {z.x, z.y, z.z};
+    for (int a = 0; a < 3; a++) {
+      const double length = 2.0 * limit[a];
+      const double tgladS = 1.0 / length;
+      if (fabs(zz[a]) < limit[a]) add[a] = zz[a] * zz[a] * tgladS;
+      if (fabs(zz[a]) > limit[a] && fabs(zz[a]) < length) add[a] = (length - fabs(zz[a])) * (length - fabs(zz[a])) * tgladS;
+    }
+    for (int a = 0; a < 3; a++) add[a] = add[a] * x[ABX_SCALE3D + a];
+    z.x = (z.x - (S(double(sgn(val(z.x)))) * (add[0])));
+    z.y = (z.y - (S(double(sgn(val(z.y)))) * (add[1])));
+    z.z = (z.z - (S(double(sgn(val(z.z)))) * (add[2])));
+  }
+  if (x[ABX_SWAP] != 0.0) z = V4<S>{z.z, z.y, z.x, z.w};
+  if (i >= int(x[ABX_START_S]) && i < int(x[ABX_STOP_S])) {
+    const double para = abox_mod11_para(x, i);
+    const S rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    z.x = z.x + x[ABX_MB_OFFSET];
+    z.y = z.y + x[ABX_MB_OFFSET + 1];
+    z.z = z.z + x[ABX_MB_OFFSET + 2];
+    z.w = z.w + 0.0;
+    if (rr < para) {
+      const double tglad_factor1 = x[ABX_MAXR2] / para;
+      z = z * tglad_factor1;
+      DE = DE * tglad_factor1;
+    } else if (rr < x[ABX_MAXR2]) {
+      const S tglad_factor2 = x[ABX_MAXR2] / rr;
+      z = z * tglad_factor2;
+      DE = DE * tglad_factor2;
+    }
+    z.x = z.x - x[ABX_MB_OFFSET];
+    z.y = z.y - x[ABX_MB_OFFSET + 1];
+    z.z = z.z - x[ABX_MB_OFFSET + 2];
+    z.w = z.w - 0.0;
+  }
+  if (i >= int(x[ABX_START_A]) && i < int(x[ABX_STOP_A])) {
+    z = z * actualScale;
+    if (x[ABX_ADE_ON] == 0.0) DE = DE * fabs(actualScale) + 1.0;
+    else DE = DE * fabs(actualScale) * x[ABX_ADE_SCALE1] + x[ABX_ADE_OFFSET1];
+  }
+  z.x = z.x + x[ABX_ADD000];
+  z.y = z.y + x[ABX_ADD000 + 1];
+  z.z = z.z + x[ABX_ADD000 + 2];
+  z.w = z.w + 0.0;
+  if (x[ABX_ADDC] != 0.0 && i >= int(x[ABX_START_E]) && i < int(x[ABX_STOP_E])) {
+    V4<S> t;
+    if (x[ABX_ALTERNATE] != 0.0) {
+      t = order_xyz(auxC, int(x[ABX_ORDER]));
+      auxC = t;
+    } else {
+      t = order_xyz(c, int(x[ABX_ORDER]));
+    }
+    z.x = z.x + t.x * x[ABX_CM111];
+    z.y = z.y + t.y * x[ABX_CM111 + 1];
+    z.z = z.z + t.z * x[ABX_CM111 + 2];
+    z.w = z.w + t.w * 1.0;
+  }
+  if (x[ABX_ROT_ON] != 0.0 && i >= int(x[ABX_START_R]) && i < int(x[ABX_STOP_R]))
+    z = mb_turn(x + ABX_ROT + 1, x[ABX_ROT] != 0.0, false, z);
+  if (i >= int(x[ABX_START_C]) && i < int(x[ABX_STOP_C1])) {
+    z = z * x[ABX_SCALE_G1];
+    DE = DE * fabs(x[ABX_SCALE_G1]);
+  }
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class S>
@@ -1118,6 +1273,10 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   S r = len4(z);
   S DE = 1.0;
   S pk = 1.0;  // aux.pseudoKleinianDE (:120)
+  S scaleA = 0.0;  // aux.actualScaleA (:124)
+  // aux.actualScale: the Mandelbox scale of the first sequence slot (:97-98, 123)
+  S actualScale = seq.length > 0 ? S(seq.slot[seq.seq[0]].mb_scale) : S(seq.slot[0].mb_scale);
+  V4<S> auxC = z;  // aux.c (:107)
   V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ, lastLastZ = lastZ;
   int maxN = seq.formula_maxiter * maxiterMultiplier;
   if (forcedMaxiter >= 0) maxN = forcedMaxiter;
@@ -1169,6 +1328,8 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_PSEUDO_KLEINIAN: formula_pseudo_kleinian(z, f, DE, pk, i); break;
         case MBR_FORMULA_BOX_FOLD_BULB_POW2: formula_box_fold_bulb_pow2(z, f, r, DE); break;
         case MBR_FORMULA_MENGER_MOD1: formula_menger_mod1(z, f, DE, i); break;
+        case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: formula_box_fold_bulb_pow2_v2(z, f, DE, scaleA, i); break;
+        case MBR_FORMULA_ABOX_MOD11: formula_abox_mod11(z, f, DE, actualScale, auxC, const_c, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

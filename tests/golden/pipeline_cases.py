@@ -162,6 +162,41 @@ def _keyed_formula_cases():
     s.fractal[0].formula_iterations = 2
     abi.fractal_defaults(s.fractal[1], abi.FORMULA_BOX_FOLD_BULB_POW2)
     t["hybrid_menger_mod1_bfbp2"] = s
+    t["bfbp2v2_default"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20)
+    s = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale=1.2, transf_scale_vary_0=0.1,
+               transf_start_iterations_X=1, transf_scaleB_1=0.9, transf_minR2_p25=0.2, transf_maxR2_1=1.1,
+               boxfold_bulbpow2_z_factor=4.5, transf_addition_constant_111=[1.0, 0.9, 1.1])
+    s.fractal[0].mandelbox_offset[:] = [0.1, 0.0, -0.05]
+    s.fractal[0].analytic_de_scale1 = 0.9
+    t["bfbp2v2_vary"] = s
+    s = _keyed(abi.FORMULA_ABOX_MOD11, 25)
+    s.fractal[0].mandelbox_scale = -1.8
+    t["abox_mod11_default"] = s
+    s = _keyed(abi.FORMULA_ABOX_MOD11, 25, mandelbox_vary_scale_vary=0.1, transf_function_enabled_false=1,
+               transf_stop_iterations_D1=4, transf_scale3D_000=[0.3, 0.2, 0.1], transf_function_enabledSw_false=1,
+               transf_addition_constant=[0.1, 0.0, 0.05], transf_rotation_enabled=1,
+               transf_rotation=[0.0, 15.0, 5.0], transf_stop_iterations_C1=3, transf_scaleG_1=0.97)
+    s.fractal[0].mandelbox_scale = 2.2
+    s.fractal[0].mandelbox_offset[:] = [0.05, -0.1, 0.0]
+    t["abox_mod11_folds"] = s
+    s = _keyed(abi.FORMULA_ABOX_MOD11, 25, transf_function_enabledy_false=1, Cpara_para00=0.1, Cpara_paraA=0.3,
+               Cpara_paraB=0.2, Cpara_paraC=0.25, Cpara_iterA=3, Cpara_iterB=12, Cpara_iterC=20,
+               Cpara_enabledParab_false=1, Cpara_parab_offset0=0.01, Cpara_parab_slope=0.002, Cpara_parab_scale=0.5,
+               analyticDE_enabled_false=1, transf_addCpixel_enabled_false=1, transf_alternate_enabled_false=1,
+               mandelbulbMulti_order_of_xyz=3, transf_constant_multiplier_111=[0.9, 1.0, 1.1])
+    s.fractal[0].mandelbox_scale = -1.7
+    s.fractal[0].analytic_de_scale1 = 1.1
+    s.fractal[0].analytic_de_offset1 = 0.5
+    t["abox_mod11_curve_c"] = s
+    s = _keyed(abi.FORMULA_ABOX_MOD11, 20, transf_addCpixel_enabled_false=1, mandelbulbMulti_order_of_xyz=5,
+               mandelbox_vary_scale_vary=0.05)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBULB)
+    s.fractal[1].bulb_power = 3.0
+    t["hybrid_abox_mod11_bulb"] = s
+    t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
+                                 transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t
 
 
