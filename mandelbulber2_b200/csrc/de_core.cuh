@@ -312,6 +312,7 @@ __device__ __forceinline__ T smax(T a, T b) {
 template <class T>
 struct AuxX {
   T pk, scale, scaleA;
+  T pn;     // aux.pos_neg (initially 1)
   V4<T> c;  // aux.c (initially the point), which aboxMod11's alternate c-addition permutes
 };
 
@@ -632,6 +633,97 @@ __device__ __noinline__ void f_abox_mod11(V4<T> &z, T &DE, AuxX<T> &ax, const V4
   }
 }
 
+// cFractalPseudoKleinianMod4::FormulaCode (fractal_pseudo_kleinian_mod4.cpp:
+// 29-145) without the aux.color terms; pk and pos_neg are
+// aux.pseudoKleinianDE and aux.pos_neg
+template <class T>
+__device__ __noinline__ void f_pseudo_kleinian_mod4(V4<T> &z, T &DE, AuxX<T> &ax, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (x[P4X_SPH_INV] != 0.0 && i >= int(x[P4X_START_X]) && i < int(x[P4X_STOP_1])) {  // :37-47
+    z.x = z.x + T(x[P4X_OFFSET000]);
+    z.y = z.y + T(x[P4X_OFFSET000 + 1]);
+    z.z = z.z + T(x[P4X_OFFSET000 + 2]);
+    const T rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const T q = T(x[P4X_SCALE_G1]) / rr;
+    z.x = z.x * q;
+    z.y = z.y * q;
+    z.z = z.z * q;
+    z.w = z.w * q;
+    DE = DE * (T(x[P4X_SCALE_G1]) / rr);
+    z.x = z.x + T(x[P4X_ADD_P000] - x[P4X_OFFSET000]);
+    z.y = z.y + T(x[P4X_ADD_P000 + 1] - x[P4X_OFFSET000 + 1]);
+    z.z = z.z + T(x[P4X_ADD_P000 + 2] - x[P4X_OFFSET000 + 2]);
+    const T a1 = T(x[P4X_SCALE_A1]);
+    z.x = z.x * a1;
+    z.y = z.y * a1;
+    z.z = z.z * a1;
+    z.w = z.w * a1;
+    DE = DE * a1;
+  }
+  if (i >= int(x[P4X_START_M]) && i < int(x[P4X_STOP_M])) {  // box offset :49-55
+    z.x = z.x - T(x[P4X_CM000]) * sgn_of(z.x);
+    z.y = z.y - T(x[P4X_CM000 + 1]) * sgn_of(z.y);
+    z.z = z.z - T(x[P4X_CM000 + 2]) * sgn_of(z.z);
+  }
+  {  // the Kleinian fold :58-66
+    const T cx = T(x[P4X_CSIZE]), cy = T(x[P4X_CSIZE + 1]), cz = T(x[P4X_CSIZE + 2]);
+    z.x = m_abs(T(z.x + cx)) - m_abs(T(z.x - cx)) - z.x;
+    z.y = m_abs(T(z.y + cy)) - m_abs(T(z.y - cy)) - z.y;
+    z.z = m_abs(T(z.z + cz)) - m_abs(T(z.z - cz)) - z.z;
+    z.w = m_abs(z.w) - m_abs(z.w) - z.w;
+    const T k = smax(T(T(x[P4X_MINR05]) / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), T(1.0));
+    z.x = z.x * k;
+    z.y = z.y * k;
+    z.z = z.z * k;
+    z.w = z.w * k;
+    DE = DE * (k + T(x[P4X_TWEAK005]));
+    ax.pk = T(x[P4X_DE_SCALE1]);
+  }
+  z.x = z.x + T(x[P4X_ADD000]);
+  z.y = z.y + T(x[P4X_ADD000 + 1]);
+  z.z = z.z + T(x[P4X_ADD000 + 2]);
+  if (x[P4X_G_ON] != 0.0 && i >= int(x[P4X_START_G]) && i < int(x[P4X_STOP_G])) {  // :70-78
+    z.x = z.x + ax.pn * T(x[P4X_ADD_A000]);
+    z.y = z.y + ax.pn * T(x[P4X_ADD_A000 + 1]);
+    z.z = z.z + ax.pn * T(x[P4X_ADD_A000 + 2]);
+    ax.pn = ax.pn * T(x[P4X_SCALE_NEG1]);
+  }
+  if (x[P4X_F_ON] != 0.0 && i >= int(x[P4X_START_F]) && i < int(x[P4X_STOP_F])) {  // :80-85
+    const T ox = T(x[P4X_OFFSET_A000]), oy = T(x[P4X_OFFSET_A000 + 1]), oz = T(x[P4X_OFFSET_A000 + 2]);
+    z.x = m_abs(T(z.x + ox)) - m_abs(T(z.x - ox)) - z.x;
+    z.y = m_abs(T(z.y + oy)) - m_abs(T(z.y - oy)) - z.y;
+    z.z = m_abs(T(z.z + oz)) - m_abs(T(z.z - oz)) - z.z;
+    z.w = m_abs(z.w) - m_abs(z.w) - z.w;
+  }
+  if (x[P4X_N_ON] != 0.0 && i >= int(x[P4X_START_N]) && i < int(x[P4X_STOP_N])) {  // :87-127
+    T t;
+    z.x = m_abs(z.x);
+    z.y = m_abs(z.y);
+    if (x[P4X_SWAP_A] != 0.0) {
+      t = z.x;
+      z.x = z.y;
+      z.y = t;
+    }
+    t = z.x;
+    z.x = z.x + z.y - T(x[P4X_OFFSET0]);
+    z.y = t - z.y - T(x[P4X_OFFSET_A0]);
+    if (x[P4X_BX_F] != 0.0 && i >= int(x[P4X_START_O]) && i < int(x[P4X_STOP_O])) z.x = -m_abs(z.x);
+    if (x[P4X_BX] != 0.0 && i >= int(x[P4X_START_P]) && i < int(x[P4X_STOP_P])) z.y = -m_abs(z.y);
+    t = z.x;
+    z.x = z.x + z.y;
+    z.y = t - z.y;
+    z.x = z.x * T(0.5);
+    z.y = z.y * T(0.5);
+    if (x[P4X_AX] != 0.0 && i >= int(x[P4X_START_R]) && i < int(x[P4X_STOP_R]))
+      z.x = T(x[P4X_OFFSET1]) - m_abs(T(z.x + T(x[P4X_OFFSET1])));
+    if (x[P4X_AX_F] != 0.0 && i >= int(x[P4X_START_RV]) && i < int(x[P4X_STOP_RV]))
+      z.y = T(x[P4X_OFFSET_A1]) - m_abs(T(z.y + T(x[P4X_OFFSET_A1])));
+  }
+  if (x[P4X_FLIP_X] != 0.0) z.x = -z.x;
+  if (x[P4X_FLIP_Y] != 0.0) z.y = -z.y;
+  if (x[P4X_FLIP_Z] != 0.0) z.z = -z.z;
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -757,6 +849,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_PSEUDO_KLEINIAN: f_pseudo_kleinian<T>(z, DE, ax.pk, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: f_box_fold_bulb_pow2_v2<T>(z, DE, ax.scaleA, s, i); break;
       case MBR_FORMULA_ABOX_MOD11: f_abox_mod11<T>(z, DE, ax, c, s, i); break;
+      case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: f_pseudo_kleinian_mod4<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
@@ -1014,7 +1107,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
   V4<T> c = z;  // aux.const_c
   r = len4<T, W>(z);
   DE = T(1.0);
-  AuxX<T> ax{T(1.0), T(0.0), T(0.0), z};
+  AuxX<T> ax{T(1.0), T(0.0), T(0.0), T(1.0), z};
   if (F == F_EXT)  // aux.actualScale: the Mandelbox scale of the sequence's first slot (compute_fractal.cpp:97-98, 123)
     ax.scale = T(sc.slot[TREE ? nd->slot : int(sc.seq[0])].d[P_MB_SCALE]);
   V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)}, lastLastZ = lastZ;

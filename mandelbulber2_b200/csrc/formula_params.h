@@ -43,7 +43,7 @@ enum NamedField {
 // bailout: the FP32 wavefront's iteration does not carry them
 inline MBR_HD bool keyed_formula_has_state(int formula) {
   return formula == MBR_FORMULA_PSEUDO_KLEINIAN || formula == MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 ||
-         formula == MBR_FORMULA_ABOX_MOD11;
+         formula == MBR_FORMULA_ABOX_MOD11 || formula == MBR_FORMULA_PSEUDO_KLEINIAN_MOD4;
 }
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
@@ -255,6 +255,58 @@ inline MBR_HD double abox_mod11_para(const double *x, int i) {
 }
 
 
+// cFractalPseudoKleinianMod4 (formula/definition/fractal_pseudo_kleinian_mod4.cpp:29-145)
+enum PseudoKleinianMod4X {
+  P4X_SPH_INV = 0,       // transf_sphere_inversion_enabled_false
+  P4X_START_X = 1,       // transf_start_iterations_X
+  P4X_STOP_1 = 2,        // transf_stop_iterations_1
+  P4X_OFFSET000 = 3,     // transf_offset_000 (3)
+  P4X_SCALE_G1 = 6,      // transf_scaleG_1
+  P4X_ADD_P000 = 7,      // transf_addition_constantP_000 (3)
+  P4X_SCALE_A1 = 10,      // transf_scaleA_1
+  P4X_START_M = 11,       // transf_start_iterations_M
+  P4X_STOP_M = 12,        // transf_stop_iterations_M
+  P4X_CM000 = 13,         // transf_constant_multiplier_000 (3)
+  P4X_CSIZE = 16,         // transf_addition_constant_0777 (3)
+  P4X_MINR05 = 19,        // transf_minimum_radius_05
+  P4X_TWEAK005 = 20,      // analyticDE_tweak_005
+  P4X_ADD000 = 21,        // transf_addition_constant (3)
+  P4X_G_ON = 24,          // transf_function_enabledG_false
+  P4X_START_G = 25,       // transf_start_iterations_G
+  P4X_STOP_G = 26,        // transf_stop_iterations_G
+  P4X_ADD_A000 = 27,      // transf_addition_constantA_000 (3)
+  P4X_SCALE_NEG1 = 30,    // transf_scale_neg1
+  P4X_F_ON = 31,          // transf_function_enabledF_false
+  P4X_START_F = 32,       // transf_start_iterations_F
+  P4X_STOP_F = 33,        // transf_stop_iterations_F
+  P4X_OFFSET_A000 = 34,   // transf_offsetA_000 (3)
+  P4X_N_ON = 37,          // transf_function_enabledN_false
+  P4X_START_N = 38,       // transf_start_iterations_N
+  P4X_STOP_N = 39,        // transf_stop_iterations_N
+  P4X_SWAP_A = 40,        // transf_function_enabledA_false
+  P4X_OFFSET0 = 41,       // transf_offset_0
+  P4X_OFFSET_A0 = 42,     // transf_offsetA_0
+  P4X_BX_F = 43,          // transf_function_enabledBx_false
+  P4X_START_O = 44,       // transf_start_iterations_O
+  P4X_STOP_O = 45,        // transf_stop_iterations_O
+  P4X_BX = 46,            // transf_function_enabledBx
+  P4X_START_P = 47,       // transf_start_iterations_P
+  P4X_STOP_P = 48,        // transf_stop_iterations_P
+  P4X_AX = 49,            // transf_function_enabledAx
+  P4X_START_R = 50,       // transf_start_iterations_R
+  P4X_STOP_R = 51,        // transf_stop_iterations_R
+  P4X_OFFSET1 = 52,       // transf_offset_1
+  P4X_AX_F = 53,          // transf_function_enabledAx_false
+  P4X_START_RV = 54,      // transf_start_iterations_RV
+  P4X_STOP_RV = 55,       // transf_stop_iterations_RV
+  P4X_OFFSET_A1 = 56,     // transf_offsetA_1
+  P4X_FLIP_X = 57,        // transf_function_enabledx_false
+  P4X_FLIP_Y = 58,        // transf_function_enabledy_false
+  P4X_FLIP_Z = 59,        // transf_function_enabledz_false
+  P4X_DE_SCALE1 = 60,     // analyticDE_scale_1 (named)
+  P4X_COUNT = 61
+};
+
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
   const char *key;
@@ -431,6 +483,57 @@ constexpr FormulaKey kAboxMod11Keys[] = {
 };
 static_assert(keys_contiguous(kAboxMod11Keys, ABX_COUNT), "Abox mod 11 keys and layout disagree");
 
+constexpr FormulaKey kPseudoKleinianMod4Keys[] = {
+    {"transf_sphere_inversion_enabled_false", PK_BOOL, {0,0,0}, P4X_SPH_INV},
+    {"transf_start_iterations_X", PK_INT, {0,0,0}, P4X_START_X},
+    {"transf_stop_iterations_1", PK_INT, {1,0,0}, P4X_STOP_1},
+    {"transf_offset_000", PK_VEC3, {0,0,0}, P4X_OFFSET000},
+    {"transf_scaleG_1", PK_DOUBLE, {1,0,0}, P4X_SCALE_G1},
+    {"transf_addition_constantP_000", PK_VEC3, {0,0,0}, P4X_ADD_P000},
+    {"transf_scaleA_1", PK_DOUBLE, {1,0,0}, P4X_SCALE_A1},
+    {"transf_start_iterations_M", PK_INT, {0,0,0}, P4X_START_M},
+    {"transf_stop_iterations_M", PK_INT, {250,0,0}, P4X_STOP_M},
+    {"transf_constant_multiplier_000", PK_VEC3, {0,0,0}, P4X_CM000},
+    {"transf_addition_constant_0777", PK_VEC3, {0.7,0.7,0.7}, P4X_CSIZE},
+    {"transf_minimum_radius_05", PK_DOUBLE, {0.5,0,0}, P4X_MINR05},
+    {"analyticDE_tweak_005", PK_DOUBLE, {0.05,0,0}, P4X_TWEAK005},
+    {"transf_addition_constant", PK_VEC3, {0,0,0}, P4X_ADD000},
+    {"transf_function_enabledG_false", PK_BOOL, {0,0,0}, P4X_G_ON},
+    {"transf_start_iterations_G", PK_INT, {0,0,0}, P4X_START_G},
+    {"transf_stop_iterations_G", PK_INT, {250,0,0}, P4X_STOP_G},
+    {"transf_addition_constantA_000", PK_VEC3, {0,0,0}, P4X_ADD_A000},
+    {"transf_scale_neg1", PK_DOUBLE, {-1,0,0}, P4X_SCALE_NEG1},
+    {"transf_function_enabledF_false", PK_BOOL, {0,0,0}, P4X_F_ON},
+    {"transf_start_iterations_F", PK_INT, {0,0,0}, P4X_START_F},
+    {"transf_stop_iterations_F", PK_INT, {250,0,0}, P4X_STOP_F},
+    {"transf_offsetA_000", PK_VEC3, {0,0,0}, P4X_OFFSET_A000},
+    {"transf_function_enabledN_false", PK_BOOL, {0,0,0}, P4X_N_ON},
+    {"transf_start_iterations_N", PK_INT, {0,0,0}, P4X_START_N},
+    {"transf_stop_iterations_N", PK_INT, {250,0,0}, P4X_STOP_N},
+    {"transf_function_enabledA_false", PK_BOOL, {0,0,0}, P4X_SWAP_A},
+    {"transf_offset_0", PK_DOUBLE, {0,0,0}, P4X_OFFSET0},
+    {"transf_offsetA_0", PK_DOUBLE, {0,0,0}, P4X_OFFSET_A0},
+    {"transf_function_enabledBx_false", PK_BOOL, {0,0,0}, P4X_BX_F},
+    {"transf_start_iterations_O", PK_INT, {0,0,0}, P4X_START_O},
+    {"transf_stop_iterations_O", PK_INT, {250,0,0}, P4X_STOP_O},
+    {"transf_function_enabledBx", PK_BOOL, {1,0,0}, P4X_BX},
+    {"transf_start_iterations_P", PK_INT, {0,0,0}, P4X_START_P},
+    {"transf_stop_iterations_P", PK_INT, {250,0,0}, P4X_STOP_P},
+    {"transf_function_enabledAx", PK_BOOL, {1,0,0}, P4X_AX},
+    {"transf_start_iterations_R", PK_INT, {0,0,0}, P4X_START_R},
+    {"transf_stop_iterations_R", PK_INT, {250,0,0}, P4X_STOP_R},
+    {"transf_offset_1", PK_DOUBLE, {1,0,0}, P4X_OFFSET1},
+    {"transf_function_enabledAx_false", PK_BOOL, {0,0,0}, P4X_AX_F},
+    {"transf_start_iterations_RV", PK_INT, {0,0,0}, P4X_START_RV},
+    {"transf_stop_iterations_RV", PK_INT, {250,0,0}, P4X_STOP_RV},
+    {"transf_offsetA_1", PK_DOUBLE, {1,0,0}, P4X_OFFSET_A1},
+    {"transf_function_enabledx_false", PK_BOOL, {0,0,0}, P4X_FLIP_X},
+    {"transf_function_enabledy_false", PK_BOOL, {0,0,0}, P4X_FLIP_Y},
+    {"transf_function_enabledz_false", PK_BOOL, {0,0,0}, P4X_FLIP_Z},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1,0,0}, P4X_DE_SCALE1},
+};
+static_assert(keys_contiguous(kPseudoKleinianMod4Keys, P4X_COUNT), "pseudo-Kleinian mod 4 keys and layout disagree");
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -449,6 +552,8 @@ inline KeyTable formula_keys(int formula) {
       return {kBoxFoldBulbPow2V2Keys, int(sizeof(kBoxFoldBulbPow2V2Keys) / sizeof(kBoxFoldBulbPow2V2Keys[0]))};
     case MBR_FORMULA_ABOX_MOD11:
       return {kAboxMod11Keys, int(sizeof(kAboxMod11Keys) / sizeof(kAboxMod11Keys[0]))};
+    case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4:
+      return {kPseudoKleinianMod4Keys, int(sizeof(kPseudoKleinianMod4Keys) / sizeof(kPseudoKleinianMod4Keys[0]))};
     default: return {nullptr, 0};
   }
 }

@@ -71,6 +71,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_MENGER_MOD1: *fi = {1, 1, 10.0, 3, 0}; return true;  // fractal_menger_mod1.cpp:16-27
     case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: *fi = {2, 0, 100.0, 2, 0}; return true;  // fractal_box_fold_bulb_pow2_v2.cpp:16-27
     case MBR_FORMULA_ABOX_MOD11: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_abox_mod11.cpp:21-32
+    case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian_mod4.cpp:17-28
     default: return false;
   }
 }
@@ -965,6 +966,85 @@ inline void formula_box_fold_bulb_pow2_v2(V4<S> &z, const SlotT<S> &f, S &DE, S 
   }
 }
 
+// cFractalPseudoKleinianMod4::FormulaCode (fractal_pseudo_kleinian_mod4.cpp:
+// 29-145) without the aux.color terms
+template <class S>
+inline void formula_pseudo_kleinian_mod4(V4<S> &z, const SlotT<S> &f, S &DE, S &pk, S &posNeg, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  if (x[P4X_SPH_INV] != 0.0 && i >= int(x[P4X_START_X]) && i < int(x[P4X_STOP_1])) {
+    z.x = z.x + x[P4X_OFFSET000];
+    z.y = z.y + x[P4X_OFFSET000 + 1];
+    z.z = z.z + x[P4X_OFFSET000 + 2];
+    z.w = z.w + 0.0;
+    const S rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    z = z * S(x[P4X_SCALE_G1] / rr);
+    DE = DE * (x[P4X_SCALE_G1] / rr);
+    z.x = z.x + (x[P4X_ADD_P000] - x[P4X_OFFSET000]);
+    z.y = z.y + (x[P4X_ADD_P000 + 1] - x[P4X_OFFSET000 + 1]);
+    z.z = z.z + (x[P4X_ADD_P000 + 2] - x[P4X_OFFSET000 + 2]);
+    z.w = z.w + (0.0 - 0.0);
+    z = z * x[P4X_SCALE_A1];
+    DE = DE * x[P4X_SCALE_A1];
+  }
+  if (i >= int(x[P4X_START_M]) && i < int(x[P4X_STOP_M])) {
+    z.x = z.x - x[P4X_CM000] * S(double(sgn(val(z.x))));
+    z.y = z.y - x[P4X_CM000 + 1] * S(double(sgn(val(z.y))));
+    z.z = z.z - x[P4X_CM000 + 2] * S(double(sgn(val(z.z))));
+  }
+  z.x = fabs(z.x + x[P4X_CSIZE]) - fabs(z.x - x[P4X_CSIZE]) - z.x;
+  z.y = fabs(z.y + x[P4X_CSIZE + 1]) - fabs(z.y - x[P4X_CSIZE + 1]) - z.y;
+  z.z = fabs(z.z + x[P4X_CSIZE + 2]) - fabs(z.z - x[P4X_CSIZE + 2]) - z.z;
+  z.w = fabs(z.w + 0.0) - fabs(z.w - 0.0) - z.w;
+  const S k = std::max(S(x[P4X_MINR05] / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), S(1.0));
+  z = z * k;
+  DE = DE * (k + x[P4X_TWEAK005]);
+  pk = x[P4X_DE_SCALE1];
+  z.x = z.x + x[P4X_ADD000];
+  z.y = z.y + x[P4X_ADD000 + 1];
+  z.z = z.z + x[P4X_ADD000 + 2];
+  z.w = z.w + 0.0;
+  if (x[P4X_G_ON] != 0.0 && i >= int(x[P4X_START_G]) && i < int(x[P4X_STOP_G])) {
+    z.x = z.x + posNeg * x[P4X_ADD_A000];
+    z.y = z.y + posNeg * x[P4X_ADD_A000 + 1];
+    z.z = z.z + posNeg * x[P4X_ADD_A000 + 2];
+    posNeg = posNeg * x[P4X_SCALE_NEG1];
+  }
+  if (x[P4X_F_ON] != 0.0 && i >= int(x[P4X_START_F]) && i < int(x[P4X_STOP_F])) {
+    z.x = fabs(z.x + x[P4X_OFFSET_A000]) - fabs(z.x - x[P4X_OFFSET_A000]) - z.x;
+    z.y = fabs(z.y + x[P4X_OFFSET_A000 + 1]) - fabs(z.y - x[P4X_OFFSET_A000 + 1]) - z.y;
+    z.z = fabs(z.z + x[P4X_OFFSET_A000 + 2]) - fabs(z.z - x[P4X_OFFSET_A000 + 2]) - z.z;
+    z.w = fabs(z.w + 0.0) - fabs(z.w - 0.0) - z.w;
+  }
+  if (x[P4X_N_ON] != 0.0 && i >= int(x[P4X_START_N]) && i < int(x[P4X_STOP_N])) {
+    S t;
+    z.x = fabs(z.x);
+    z.y = fabs(z.y);
+    if (x[P4X_SWAP_A] != 0.0) {
+      t = z.x;
+      z.x = z.y;
+      z.y = t;
+    }
+    t = z.x;
+    z.x = z.x + z.y - x[P4X_OFFSET0];
+    z.y = t - z.y - x[P4X_OFFSET_A0];
+    if (x[P4X_BX_F] != 0.0 && i >= int(x[P4X_START_O]) && i < int(x[P4X_STOP_O])) z.x = -fabs(z.x);
+    if (x[P4X_BX] != 0.0 && i >= int(x[P4X_START_P]) && i < int(x[P4X_STOP_P])) z.y = -fabs(z.y);
+    t = z.x;
+    z.x = z.x + z.y;
+    z.y = t - z.y;
+    z.x = z.x * 0.5;
+    z.y = z.y * 0.5;
+    if (x[P4X_AX] != 0.0 && i >= int(x[P4X_START_R]) && i < int(x[P4X_STOP_R]))
+      z.x = x[P4X_OFFSET1] - fabs(z.x + x[P4X_OFFSET1]);
+    if (x[P4X_AX_F] != 0.0 && i >= int(x[P4X_START_RV]) && i < int(x[P4X_STOP_RV]))
+      z.y = x[P4X_OFFSET_A1] - fabs(z.y + x[P4X_OFFSET_A1]);
+  }
+  if (x[P4X_FLIP_X] != 0.0) z.x = -z.x;
+  if (x[P4X_FLIP_Y] != 0.0) z.y = -z.y;
+  if (x[P4X_FLIP_Z] != 0.0) z.z = -z.z;
+}
+
 // (x, y, z) in the order of enumMulti_OrderOfXYZ (fractal.h:282-289)
 template <class S>
 inline V4<S> order_xyz(const V4<S> &v, int order) {
@@ -1277,6 +1357,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   // aux.actualScale: the Mandelbox scale of the first sequence slot (:97-98, 123)
   S actualScale = seq.length > 0 ? S(seq.slot[seq.seq[0]].mb_scale) : S(seq.slot[0].mb_scale);
   V4<S> auxC = z;  // aux.c (:107)
+  S posNeg = 1.0;  // aux.pos_neg (:109)
   V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ, lastLastZ = lastZ;
   int maxN = seq.formula_maxiter * maxiterMultiplier;
   if (forcedMaxiter >= 0) maxN = forcedMaxiter;
@@ -1330,6 +1411,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_MENGER_MOD1: formula_menger_mod1(z, f, DE, i); break;
         case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: formula_box_fold_bulb_pow2_v2(z, f, DE, scaleA, i); break;
         case MBR_FORMULA_ABOX_MOD11: formula_abox_mod11(z, f, DE, actualScale, auxC, const_c, i); break;
+        case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: formula_pseudo_kleinian_mod4(z, f, DE, pk, posNeg, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

@@ -195,6 +195,17 @@ def _keyed_formula_cases():
     abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBULB)
     s.fractal[1].bulb_power = 3.0
     t["hybrid_abox_mod11_bulb"] = s
+    t["pkm4_default"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_MOD4, 30)
+    t["pkm4_sphere_box"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_MOD4, 30, transf_sphere_inversion_enabled_false=1,
+                                  transf_stop_iterations_1=2, transf_offset_000=[0.1, 0.0, -0.1], transf_scaleG_1=1.2,
+                                  transf_addition_constantP_000=[0.0, 0.05, 0.0], transf_scaleA_1=0.9,
+                                  transf_constant_multiplier_000=[0.1, 0.05, 0.0], transf_start_iterations_M=1)
+    t["pkm4_fold_n"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_MOD4, 30, transf_function_enabledG_false=1,
+                              transf_addition_constantA_000=[0.05, 0.02, 0.0], transf_function_enabledF_false=1,
+                              transf_offsetA_000=[0.9, 1.0, 1.1], transf_function_enabledN_false=1,
+                              transf_function_enabledA_false=1, transf_offset_0=0.1, transf_offsetA_0=0.05,
+                              transf_function_enabledBx_false=1, transf_function_enabledAx_false=1,
+                              transf_offsetA_1=0.8, transf_function_enabledz_false=1)
     t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
                                  transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t
