@@ -211,6 +211,12 @@ struct Reader {
   int hybrid = 0, boolean_ops = 0;
   int formula[kSlots];
   int slot_enable[kSlots];
+  // formula transforms (formula_position/_rotation/_scale/_repeat of each
+  // slot) and the legacy global fractal transform (fractal_position,
+  // fractal_rotation, repeat; MigrateLegacyParamsToFractal,
+  // settings.cpp:2372-2401, copies a non-default one into every slot)
+  double f_pos[kSlots][3] = {}, f_rot[kSlots][3] = {}, f_rep[kSlots][3] = {}, f_scale[kSlots];
+  double g_pos[3] = {0, 0, 0}, g_rot[3] = {0, 0, 0}, g_rep[3] = {0, 0, 0};
   int ao_enabled = 0, ao_mode = 2;
   double ao_intensity = 1.0;
   int ao_quality = 4;
@@ -228,6 +234,7 @@ struct Reader {
     for (int i = 0; i < kSlots; i++) {
       formula[i] = i == 0 ? MBR_FORMULA_MANDELBULB : MBR_FORMULA_NONE;
       slot_enable[i] = 1;
+      f_scale[i] = 1.0;
     }
   }
 
@@ -541,11 +548,12 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
       return;
     }
     if (base == "formula_position" || base == "formula_rotation" || base == "formula_repeat") {
-      if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (formula transform)");
+      double *dst = base == "formula_position" ? R.f_pos[slot] : (base == "formula_rotation" ? R.f_rot[slot] : R.f_rep[slot]);
+      if (parse_vec3(value, v)) std::memcpy(dst, v, sizeof(v)); else R.bad(name, value);
       return;
     }
     if (base == "formula_scale") {
-      if (parse_double(value, d) && d != 1.0) R.unsupported.push_back(name + " (formula transform)");
+      if (parse_double(value, d)) R.f_scale[slot] = d; else R.bad(name, value);
       return;
     }
     // julia_mode_K, julia_c_K, fractal_constant_factor_K, initial_waxis_K,
@@ -613,7 +621,8 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     // the transform of the group that holds the primitives (settings.cpp:3113-3117)
     if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (primitive group transform)");
   } else if (name == "fractal_position" || name == "fractal_rotation" || name == "repeat") {
-    if (parse_vec3(value, v) && nonzero3(v)) R.unsupported.push_back(name + " (fractal transform)");
+    double *dst = name == "fractal_position" ? R.g_pos : (name == "fractal_rotation" ? R.g_rot : R.g_rep);
+    if (parse_vec3(value, v)) std::memcpy(dst, v, sizeof(v)); else R.bad(name, value);
   } else if (name == "formula_code") {
     R.unsupported.push_back(name + " (custom formula code)");
   // camera and image
@@ -1017,6 +1026,57 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
     R.unsupported.push_back("delta_DE_function 4 (the analytic Jos Kleinian DE function)");
   if (scene->delta_de_method == MBR_DE_METHOD_FORCE_DELTA)
     append(rep, "note: delta_DE_method 1 (forced delta DE): the plain FP64 engines render it");
+  // the fractal's transform: a single fractal becomes the fractal node of
+  // an explicit objects tree with the primitives beside it in the root union
+  // (MigrateToObjectsTree with CopyFormulaTransform, settings.cpp:2471-2481,
+  // 2713-2730, 2866-2940); hybrids and boolean combinations keep refusing it
+  for (int i = 0; i < kSlots; i++) {
+    for (int k = 0; k < 3; k++) {
+      if (nonzero3(R.g_pos)) R.f_pos[i][k] = R.g_pos[k];
+      if (nonzero3(R.g_rot)) R.f_rot[i][k] = R.g_rot[k];
+      if (nonzero3(R.g_rep)) R.f_rep[i][k] = R.g_rep[k];
+    }
+  }
+  const int iterated = R.hybrid ? scene->n_fractals : 1;
+  bool transformed = false;
+  for (int i = 0; i < iterated; i++)
+    if (nonzero3(R.f_pos[i]) || nonzero3(R.f_rot[i]) || nonzero3(R.f_rep[i]) || R.f_scale[i] != 1.0) transformed = true;
+  if (transformed && (R.hybrid || R.boolean_ops)) {
+    R.unsupported.push_back("formula or fractal transform of a hybrid or boolean combination");
+  } else if (transformed) {
+    if (!(std::fabs(R.f_scale[0]) > 1e-12)) {
+      R.unsupported.push_back("formula_scale_1 0 (degenerate formula transform)");
+    } else {
+      mbr_node &n = scene->node[0];
+      std::memset(&n, 0, sizeof(n));
+      n.type = MBR_NODE_FRACTAL;
+      n.index = 0;
+      n.enabled = 1;
+      std::memcpy(n.position, R.f_pos[0], sizeof(n.position));
+      std::memcpy(n.rotation, R.f_rot[0], sizeof(n.rotation));
+      std::memcpy(n.repeat, R.f_rep[0], sizeof(n.repeat));
+      n.scale = R.f_scale[0];
+      n.detail_level_multiplier = 1.0;
+      n.smooth_combine_distance = 0.1;
+      n.formula_maxiter = scene->formula_maxiter;
+      n.julia_mode = scene->julia_mode;
+      std::memcpy(n.julia_c, scene->julia_c, sizeof(n.julia_c));
+      std::memcpy(n.fractal_constant_factor, scene->fractal_constant_factor, sizeof(n.fractal_constant_factor));
+      n.initial_waxis = scene->initial_waxis;
+      scene->n_nodes = 1;
+      for (int k = 0; k < scene->n_primitives; k++) {
+        mbr_node &q = scene->node[scene->n_nodes++];
+        std::memset(&q, 0, sizeof(q));
+        q.type = MBR_NODE_PRIMITIVE;
+        q.index = k;
+        q.enabled = 1;
+        q.scale = 1.0;
+        q.detail_level_multiplier = 1.0;
+        q.smooth_combine_distance = 0.1;
+      }
+      append(rep, "note: the fractal's transform makes the scene an explicit objects tree (plain engines)");
+    }
+  }
   for (const std::string &u : R.unsupported) append(rep, "unsupported: " + u);
   if (!R.ignored.empty()) {
     std::string s = "ignored: " + std::to_string(R.ignored.size()) + " parameters outside the DE path:";

@@ -116,3 +116,30 @@ def test_oracle_tree_transform_moves_the_object(oracle):
     d1, i1 = oracle.distance(tree, t + s * pts, 1e-3, False)
     assert np.array_equal(i0, i1)
     np.testing.assert_allclose(d1, s * d0, rtol=1e-12, atol=1e-15)
+
+
+def test_settings_transform_of_a_single_fractal_becomes_a_tree():
+    """A legacy file's formula transform (formula_position_1, ..._rotation_1,
+    ..._scale_1, ..._repeat_1; a non-default fractal_position / _rotation /
+    repeat overrides them, settings.cpp:2372-2401) becomes the fractal node
+    of an explicit tree, with the file's primitives beside it in the root
+    union; a hybrid with a transform stays refused."""
+    from mandelbulber2_b200 import settings
+
+    head = "# Mandelbulber settings file\n# version 2.33\n# only modified parameters\n"
+    txt = head + ("[main_parameters]\nformula_1 8;\nN 30;\nfractal_rotation 0 -90 0;\n"
+                  "primitive_sphere_1_enabled true;\nprimitive_sphere_1_radius 0,5;\n"
+                  "formula_position_1 0 0 1;\nformula_scale_1 0,5;\nformula_repeat_1 3 0 0;\n")
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    sc = s.scene
+    assert sc.n_nodes == 2 and sc.n_primitives == 1
+    n = sc.node[0]
+    assert n.type == abi.NODE_FRACTAL and n.level == 0 and n.formula_maxiter == 30
+    assert list(n.position) == [0.0, 0.0, 1.0] and list(n.rotation) == [0.0, -90.0, 0.0]
+    assert n.scale == 0.5 and list(n.repeat) == [3.0, 0.0, 0.0]
+    assert sc.node[1].type == abi.NODE_PRIMITIVE and sc.node[1].index == 0
+    scene_sequence(sc)
+    s = settings.load_from_string(head + "[main_parameters]\nformula_1 8;\nformula_2 2;\nhybrid_fractal_enable true;\n"
+                                  "fractal_position 1 0 0;\n")
+    assert s.status == abi.MBR_EUNSUPPORTED
