@@ -69,6 +69,7 @@ typedef enum mbr_formula {
   MBR_FORMULA_BOX_FOLD_BULB_POW2 = 16, /* formula/definition/fractal_box_fold_bulb_pow2.cpp:27-76 (delta DE) */
   MBR_FORMULA_MENGER_MOD1 = 61,       /* formula/definition/fractal_menger_mod1.cpp:29-103 */
   MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 = 125, /* formula/definition/fractal_box_fold_bulb_pow2_v2.cpp:29-146 */
+  MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE = 101, /* formula/definition/fractal_pseudo_kleinian_std_de.cpp:29-215 (custom DE) */
   MBR_FORMULA_PSEUDO_KLEINIAN = 103,  /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
   MBR_FORMULA_ABOX_MOD11 = 119,       /* formula/definition/fractal_abox_mod11.cpp:34-250 */
   MBR_FORMULA_PSEUDO_KLEINIAN_MOD4 = 217 /* formula/definition/fractal_pseudo_kleinian_mod4.cpp:29-145 */

@@ -313,6 +313,7 @@ template <class T>
 struct AuxX {
   T pk, scale, scaleA;
   T pn;     // aux.pos_neg (initially 1)
+  T dist;   // aux.dist, the custom DE (initially 1000)
   V4<T> c;  // aux.c (initially the point), which aboxMod11's alternate c-addition permutes
 };
 
@@ -724,6 +725,176 @@ __device__ __noinline__ void f_pseudo_kleinian_mod4(V4<T> &z, T &DE, AuxX<T> &ax
   if (x[P4X_FLIP_Z] != 0.0) z.z = -z.z;
 }
 
+// the tetrahedral frame turn of Benesi's transforms (SQRT_1_3, SQRT_2_3,
+// SQRT_1_2 of abstract_fractal.h:30-32): into the frame and back
+template <class T>
+__device__ __forceinline__ V4<T> benesi_in(const V4<T> &z) {
+  const T t = z.x * T(0.81649658092772603273242802490196) - z.z * T(0.57735026918962576450914878050196);
+  return V4<T>{(t - z.y) * T(0.70710678118654752440084436210485), (t + z.y) * T(0.70710678118654752440084436210485),
+               z.x * T(0.57735026918962576450914878050196) + z.z * T(0.81649658092772603273242802490196), z.w};
+}
+template <class T>
+__device__ __forceinline__ V4<T> benesi_out(const V4<T> &z) {
+  const T t = (z.y + z.x) * T(0.70710678118654752440084436210485);
+  return V4<T>{z.z * T(0.57735026918962576450914878050196) + t * T(0.81649658092772603273242802490196),
+               (z.y - z.x) * T(0.70710678118654752440084436210485),
+               z.z * T(0.81649658092772603273242802490196) - t * T(0.57735026918962576450914878050196), z.w};
+}
+
+// cFractalPseudoKleinianStdDE::FormulaCode (fractal_pseudo_kleinian_std_de.cpp:
+// 29-215) without the aux.color terms: prism, rotation, Benesi's T1 and the
+// T1 mod, an abs fold, a Menger fold, the Kleinian fold (two variants) and
+// the custom distance aux.dist (ax.dist)
+template <class T>
+__device__ __noinline__ void f_pseudo_kleinian_std_de(V4<T> &z, T &DE, AuxX<T> &ax, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (x[PSX_P_ON] != 0.0 && i >= int(x[PSX_START_P]) && i < int(x[PSX_STOP_P1])) {  // prism :38-58
+    z.y = m_abs(z.y);
+    z.z = m_abs(z.z);
+    const T dot1 = (z.x * T(-0.86602540378443864676372317075294) + z.y * T(0.5)) * T(x[PSX_SCALE]);
+    T t = smax(T(0.0), dot1);
+    z.x = z.x - t * T(-1.73205080756887729352744634150587);
+    z.y = m_abs(T(z.y - t));
+    if (z.y > z.z) {
+      t = z.y;
+      z.y = z.z;
+      z.z = t;
+    }
+    z.x = z.x - T(x[PSX_CM000] * 0.86602540378443864676372317075294);
+    z.y = z.y - T(x[PSX_CM000 + 1] * 1.5);
+    z.z = z.z - T(x[PSX_CM000 + 2] * 1.5);
+    if (z.z > z.x) {
+      t = z.z;
+      z.z = z.x;
+      z.x = t;
+    }
+    if (z.x > T(0.0)) {
+      z.y = smax(T(0.0), z.y);
+      z.z = smax(T(0.0), z.z);
+    }
+  }
+  if (x[PSX_R_ON] != 0.0 && i >= int(x[PSX_START_R]) && i < int(x[PSX_STOP_R]) && x[PSX_ROT] == 0.0)
+    z = mb_turn<T>(x + PSX_ROT + 1, false, z);  // :60-63
+  if (x[PSX_T1_ON] != 0.0 && i >= int(x[PSX_START]) && i < int(x[PSX_STOP_T1])) {  // benesi T1 :65-83
+    z = benesi_in(z);
+    const T tempL = len4<T, true>(z);
+    z = V4<T>{m_abs(z.x) * T(x[PSX_S222]), m_abs(z.y) * T(x[PSX_S222 + 1]), m_abs(z.z) * T(x[PSX_S222 + 2]),
+              m_abs(z.w)};
+    const T avgScale = len4<T, true>(z) / tempL;
+    DE = DE * avgScale + T(1.0);
+    z = benesi_out(z);
+    z.x = z.x - T(x[PSX_OFF200]);
+    z.y = z.y - T(x[PSX_OFF200 + 1]);
+    z.z = z.z - T(x[PSX_OFF200 + 2]);
+  }
+  if (x[PSX_TM_ON] != 0.0 && i >= int(x[PSX_START_D]) && i < int(x[PSX_STOP_TM1])) {  // benesi T1 mod :85-104
+    z = benesi_in(z);
+    const T tempL = len4<T, true>(z);
+    z = V4<T>{m_abs(z.x) * T(x[PSX_S333]), m_abs(z.y) * T(x[PSX_S333 + 1]), m_abs(z.z) * T(x[PSX_S333 + 2]),
+              m_abs(z.w)};
+    const T avgScale = len4<T, true>(z) / tempL;
+    DE = DE * avgScale + T(1.0);
+    const T ax0 = T(x[PSX_ADD111]), ay = T(x[PSX_ADD111 + 1]), az = T(x[PSX_ADD111 + 2]);
+    z.x = m_abs(T(z.x + ax0)) - m_abs(T(z.x - ax0)) - z.x;
+    z.y = m_abs(T(z.y + ay)) - m_abs(T(z.y - ay)) - z.y;
+    z.z = m_abs(T(z.z + az)) - m_abs(T(z.z - az)) - z.z;
+    z.w = m_abs(z.w) - m_abs(z.w) - z.w;
+    z = benesi_out(z);
+  }
+  if (x[PSX_F_ON] != 0.0 && i >= int(x[PSX_START_F]) && i < int(x[PSX_STOP_F])) {  // :106-127
+    T ta = T(0.0), tb = T(0.0);
+    if (x[PSX_F_AX] != 0.0) ta = m_abs(T(z.x + T(x[PSX_OFFF000])));
+    if (x[PSX_F_X] != 0.0) tb = m_abs(T(z.x - T(x[PSX_OFF000])));
+    z.x = ta - tb - (z.x * T(x[PSX_S111]));
+    ta = T(0.0);
+    tb = T(0.0);
+    if (x[PSX_F_AY] != 0.0) ta = m_abs(T(z.y + T(x[PSX_OFFF000 + 1])));
+    if (x[PSX_F_Y] != 0.0) tb = m_abs(T(z.y - T(x[PSX_OFF000 + 1])));
+    z.y = ta - tb - (z.y * T(x[PSX_S111 + 1]));
+    ta = T(0.0);
+    tb = T(0.0);
+    if (x[PSX_F_AZ] != 0.0) ta = m_abs(T(z.z + T(x[PSX_OFFF000 + 2])));
+    if (x[PSX_F_Z] != 0.0) tb = m_abs(T(z.z - T(x[PSX_OFF000 + 2])));
+    z.z = ta - tb - (z.z * T(x[PSX_S111 + 2]));
+  }
+  if (x[PSX_M_ON] != 0.0 && i >= int(x[PSX_START_M]) && i < int(x[PSX_STOP_M])) {  // Menger fold :129-142
+    z = V4<T>{m_abs(z.x), m_abs(z.y), m_abs(z.z), m_abs(z.w)};
+    T t;
+    if (z.x - z.y < T(0.0)) {
+      t = z.y;
+      z.y = z.x;
+      z.x = t;
+    }
+    if (z.x - z.z < T(0.0)) {
+      t = z.z;
+      z.z = z.x;
+      z.x = t;
+    }
+    if (z.y - z.z < T(0.0)) {
+      t = z.z;
+      z.z = z.y;
+      z.y = t;
+    }
+    const T s3 = T(x[PSX_SCALE3]);
+    z.x = z.x * s3;
+    z.y = z.y * s3;
+    z.z = z.z * s3;
+    z.w = z.w * s3;
+    z.x = z.x - T(2.0 * x[PSX_CMA111]);
+    z.y = z.y - T(2.0 * x[PSX_CMA111 + 1]);
+    if (z.z > T(1.0)) z.z = z.z - T(2.0 * x[PSX_CMA111 + 2]);
+    DE = DE * T(x[PSX_SCALE3] * x[PSX_SCALE_A1]);
+    z.x = z.x + T(x[PSX_ADD_A000]);
+    z.y = z.y + T(x[PSX_ADD_A000 + 1]);
+    z.z = z.z + T(x[PSX_ADD_A000 + 2]);
+  }
+  if (x[PSX_FLIP_Z] != 0.0) z.z = -z.z;
+  const T cx = T(x[PSX_CSIZE]), cy = T(x[PSX_CSIZE + 1]), cz = T(x[PSX_CSIZE + 2]);
+  if (x[PSX_AW] != 0.0 && i >= int(x[PSX_START_C]) && i < int(x[PSX_STOP_C])) {  // :148-166
+    V4<T> t = z;
+    if (z.x > cx) t.x = cx;
+    if (z.x < -cx) t.x = -cx;
+    if (z.y > cy) t.y = cy;
+    if (z.y < -cy) t.y = -cy;
+    if (z.z > cz) t.z = cz;
+    if (z.z < -cz) t.z = -cz;
+    const T b1 = T(x[PSX_SCALE_B1]);
+    z.x = z.x * b1;
+    z.y = z.y * b1;
+    z.z = z.z * b1;
+    z.w = z.w * b1;
+    DE = DE * T(fabs(x[PSX_SCALE_B1]));
+    z.x = t.x * T(2.0) - z.x;
+    z.y = t.y * T(2.0) - z.y;
+    z.z = t.z * T(2.0) - z.z;
+    z.w = t.w * T(2.0) - z.w;
+    const T k = smax(T(T(x[PSX_MINR05]) / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), T(1.0));
+    z.x = z.x * k;
+    z.y = z.y * k;
+    z.z = z.z * k;
+    z.w = z.w * k;
+    DE = DE * (k + T(x[PSX_TWEAK005]));
+  }
+  if (x[PSX_AYF] != 0.0 && i >= int(x[PSX_START_B]) && i < int(x[PSX_STOP_B])) {  // :167-181
+    if (z.x > cx) z.x = T(x[PSX_CSIZE] * 2.0) - z.x;
+    if (z.x < -cx) z.x = T(-x[PSX_CSIZE] * 2.0) - z.x;
+    if (z.y > cy) z.y = T(x[PSX_CSIZE + 1] * 2.0) - z.y;
+    if (z.y < -cy) z.y = T(-x[PSX_CSIZE + 1] * 2.0) - z.y;
+    if (z.z > cz) z.z = T(x[PSX_CSIZE + 2] * 2.0) - z.z;
+    if (z.z < -cz) z.z = T(-x[PSX_CSIZE + 2] * 2.0) - z.z;
+    const T k = smax(T(T(x[PSX_MINR05]) / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), T(1.0));
+    z.x = z.x * k;
+    z.y = z.y * k;
+    z.z = z.z * k;
+    z.w = z.w * k;
+    DE = DE * (k + T(x[PSX_TWEAK005]));
+  }
+  z.x = z.x + T(x[PSX_ADD000]);  // :182
+  z.y = z.y + T(x[PSX_ADD000 + 1]);
+  z.z = z.z + T(x[PSX_ADD000 + 2]);
+  ax.dist = m_sqrt(T(z.x * z.x + z.y * z.y)) / DE;  // :183
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -850,6 +1021,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: f_box_fold_bulb_pow2_v2<T>(z, DE, ax.scaleA, s, i); break;
       case MBR_FORMULA_ABOX_MOD11: f_abox_mod11<T>(z, DE, ax, c, s, i); break;
       case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: f_pseudo_kleinian_mod4<T>(z, DE, ax, s, i); break;
+      case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: f_pseudo_kleinian_std_de<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;
@@ -1102,12 +1274,13 @@ __device__ __forceinline__ void global_folds(const DevScene &sc, V4<T> &z, T &r,
 // the derivative DE and the orbit's maxiter flag.
 template <class T, int F, bool W, bool TREE = false>
 __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T pz, int maxN, V4<T> &z, T &r, T &DE,
-                                             bool &maxiter, const DevNode *nd = nullptr, T *pk_out = nullptr) {
+                                             bool &maxiter, const DevNode *nd = nullptr, T *pk_out = nullptr,
+                                             T *dist_out = nullptr) {
   z = V4<T>{px, py, pz, W ? T(TREE ? nd->w0 : sc.w0) : T(0.0)};
   V4<T> c = z;  // aux.const_c
   r = len4<T, W>(z);
   DE = T(1.0);
-  AuxX<T> ax{T(1.0), T(0.0), T(0.0), T(1.0), z};
+  AuxX<T> ax{T(1.0), T(0.0), T(0.0), T(1.0), T(1000.0), z};
   if (F == F_EXT)  // aux.actualScale: the Mandelbox scale of the sequence's first slot (compute_fractal.cpp:97-98, 123)
     ax.scale = T(sc.slot[TREE ? nd->slot : int(sc.seq[0])].d[P_MB_SCALE]);
   V4<T> lastZ{T(0.0), T(0.0), T(0.0), T(0.0)}, lastLastZ = lastZ;
@@ -1169,6 +1342,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
     }
   }
   if (pk_out) *pk_out = ax.pk;
+  if (dist_out) *dist_out = ax.dist;
   return i;
 }
 
@@ -1177,7 +1351,7 @@ __device__ __forceinline__ int compute_orbit(const DevScene &sc, T px, T py, T p
 // one every DevDeFinal code.
 template <class T, int F, bool W>
 __device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, T r, T DE, int de_final = -1,
-                                            T pk = T(1.0)) {
+                                            T pk = T(1.0), T dist = T(1000.0)) {
   if (!(DE > T(0.0))) return r;
   if (F == F_EXT) {
     switch (de_final >= 0 ? de_final : sc.de_final) {
@@ -1189,7 +1363,7 @@ __device__ __forceinline__ T final_distance(const DevScene &sc, const V4<T> &z, 
         const T rxy = m_sqrt(z.x * z.x + z.y * z.y);
         return smax(T(rxy - pk), T(m_abs(rxy * z.z) / r)) / DE;
       }
-      case DEF_CUSTOM: return T(1000.0);  // aux.dist (:119)
+      case DEF_CUSTOM: return dist;  // aux.dist: 1000 unless a formula set it (:119)
       case DEF_MAX_AXIS: {
         const T rd = smax(m_abs(z.x), smax(m_abs(z.y), m_abs(z.z)));
         return rd / DE;
@@ -1318,11 +1492,11 @@ __device__ __forceinline__ T calc_distance_simple(const DevScene &sc, T px, T py
   }
   const int mult = (normal_mode && sc.iter_thresh) ? 5 : 1;
   V4<T> z;
-  T r, DE, pk;
+  T r, DE, pk, cdist;
   bool maxiter;
   const int i = compute_orbit<T, F, W, TREE>(sc, px, py, pz, (TREE ? nd->maxN : sc.formula_maxiter) * mult, z, r,
-                                             DE, maxiter, nd, &pk);
-  T distance = final_distance<T, F, W>(sc, z, r, DE, TREE ? nd->de_final : -1, pk);
+                                             DE, maxiter, nd, &pk, &cdist);
+  T distance = final_distance<T, F, W>(sc, z, r, DE, TREE ? nd->de_final : -1, pk, cdist);
   const int iters = i + 1;
   *iters_out = iters;
   if (total_out) *total_out = iters;

@@ -16,7 +16,7 @@
 
 #include "../../include/mbr.h"
 
-#define MBR_SLOT_X 80  // entries of a slot's keyed parameter block
+#define MBR_SLOT_X 96  // entries of a slot's keyed parameter block
 
 #ifdef __CUDACC__
 #define MBR_HD __host__ __device__
@@ -43,7 +43,8 @@ enum NamedField {
 // bailout: the FP32 wavefront's iteration does not carry them
 inline MBR_HD bool keyed_formula_has_state(int formula) {
   return formula == MBR_FORMULA_PSEUDO_KLEINIAN || formula == MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 ||
-         formula == MBR_FORMULA_ABOX_MOD11 || formula == MBR_FORMULA_PSEUDO_KLEINIAN_MOD4;
+         formula == MBR_FORMULA_ABOX_MOD11 || formula == MBR_FORMULA_PSEUDO_KLEINIAN_MOD4 ||
+         formula == MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE;
 }
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
@@ -307,6 +308,62 @@ enum PseudoKleinianMod4X {
   P4X_COUNT = 61
 };
 
+// cFractalPseudoKleinianStdDE (formula/definition/fractal_pseudo_kleinian_std_de.cpp:29-215)
+enum PseudoKleinianStdDEX {
+  PSX_P_ON = 0,        // transf_function_enabledP_false
+  PSX_START_P = 1,     // transf_start_iterations_P
+  PSX_STOP_P1 = 2,     // transf_stop_iterations_P1
+  PSX_SCALE = 3,       // transf_scale
+  PSX_CM000 = 4,       // transf_constant_multiplier_000 (3)
+  PSX_R_ON = 7,        // transf_function_enabledR_false
+  PSX_START_R = 8,     // transf_start_iterations_R
+  PSX_STOP_R = 9,      // transf_stop_iterations_R
+  PSX_ROT = 10,         // transf_rotation (10)
+  PSX_T1_ON = 20,       // transf_benesi_T1_enabled_false
+  PSX_START = 21,       // transf_start_iterations
+  PSX_STOP_T1 = 22,     // transf_stop_iterationsT_1
+  PSX_S222 = 23,        // transf_scale3D_222 (3)
+  PSX_OFF200 = 26,      // transf_offset_200 (3)
+  PSX_TM_ON = 29,       // transf_function_enabledx_false
+  PSX_START_D = 30,     // transf_start_iterations_D
+  PSX_STOP_TM1 = 31,    // transf_stop_iterationsTM_1
+  PSX_S333 = 32,        // transf_scale3D_333 (3)
+  PSX_ADD111 = 35,      // transf_addition_constant_111 (3)
+  PSX_F_ON = 38,        // transf_function_enabledF_false
+  PSX_START_F = 39,     // transf_start_iterations_F
+  PSX_STOP_F = 40,      // transf_stop_iterations_F
+  PSX_F_AX = 41,        // transf_function_enabledAx
+  PSX_F_X = 42,         // transf_function_enabledx
+  PSX_F_AY = 43,        // transf_function_enabledAy
+  PSX_F_Y = 44,         // transf_function_enabledy
+  PSX_F_AZ = 45,        // transf_function_enabledAz
+  PSX_F_Z = 46,         // transf_function_enabledz
+  PSX_OFFF000 = 47,     // transf_offsetF_000 (3)
+  PSX_OFF000 = 50,      // transf_offset_000 (3)
+  PSX_S111 = 53,        // transf_scale3D_111 (3)
+  PSX_M_ON = 56,        // transf_function_enabled
+  PSX_START_M = 57,     // transf_start_iterations_M
+  PSX_STOP_M = 58,      // transf_stop_iterations_M
+  PSX_CMA111 = 59,      // transf_constant_multiplierA_111 (3)
+  PSX_SCALE_A1 = 62,    // transf_scaleA_1
+  PSX_ADD_A000 = 63,    // transf_addition_constantA_000 (3)
+  PSX_FLIP_Z = 66,      // transf_function_enabledN_false
+  PSX_AW = 67,          // transf_function_enabledAw
+  PSX_START_C = 68,     // transf_start_iterations_C
+  PSX_STOP_C = 69,      // transf_stop_iterations_C
+  PSX_CSIZE = 70,       // transf_addition_constant_0777 (3)
+  PSX_SCALE_B1 = 73,    // transf_scaleB_1
+  PSX_MINR05 = 74,      // transf_minimum_radius_05
+  PSX_TWEAK005 = 75,    // analyticDE_tweak_005
+  PSX_AYF = 76,         // transf_function_enabledAy_false
+  PSX_START_B = 77,     // transf_start_iterations_B
+  PSX_STOP_B = 78,      // transf_stop_iterations_B
+  PSX_ADD000 = 79,      // transf_addition_constant (3)
+  PSX_SCALE3 = 82,      // transf_scale_3 (named)
+  PSX_COUNT = 83
+};
+static_assert(PSX_COUNT <= MBR_SLOT_X, "pseudo-Kleinian std DE block exceeds the slot's parameter block");
+
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
   const char *key;
@@ -534,6 +591,60 @@ constexpr FormulaKey kPseudoKleinianMod4Keys[] = {
 };
 static_assert(keys_contiguous(kPseudoKleinianMod4Keys, P4X_COUNT), "pseudo-Kleinian mod 4 keys and layout disagree");
 
+constexpr FormulaKey kPseudoKleinianStdDEKeys[] = {
+    {"transf_function_enabledP_false", PK_BOOL, {0,0,0}, PSX_P_ON},
+    {"transf_start_iterations_P", PK_INT, {0,0,0}, PSX_START_P},
+    {"transf_stop_iterations_P1", PK_INT, {1,0,0}, PSX_STOP_P1},
+    {"transf_scale", PK_DOUBLE, {1,0,0}, PSX_SCALE},
+    {"transf_constant_multiplier_000", PK_VEC3, {0,0,0}, PSX_CM000},
+    {"transf_function_enabledR_false", PK_BOOL, {0,0,0}, PSX_R_ON},
+    {"transf_start_iterations_R", PK_INT, {0,0,0}, PSX_START_R},
+    {"transf_stop_iterations_R", PK_INT, {250,0,0}, PSX_STOP_R},
+    {"transf_rotation", PK_ROT, {0,0,0}, PSX_ROT},
+    {"transf_benesi_T1_enabled_false", PK_BOOL, {0,0,0}, PSX_T1_ON},
+    {"transf_start_iterations", PK_INT, {0,0,0}, PSX_START},
+    {"transf_stop_iterationsT_1", PK_INT, {1,0,0}, PSX_STOP_T1},
+    {"transf_scale3D_222", PK_VEC3, {2,2,2}, PSX_S222},
+    {"transf_offset_200", PK_VEC3, {2,0,0}, PSX_OFF200},
+    {"transf_function_enabledx_false", PK_BOOL, {0,0,0}, PSX_TM_ON},
+    {"transf_start_iterations_D", PK_INT, {0,0,0}, PSX_START_D},
+    {"transf_stop_iterationsTM_1", PK_INT, {1,0,0}, PSX_STOP_TM1},
+    {"transf_scale3D_333", PK_VEC3, {3,3,3}, PSX_S333},
+    {"transf_addition_constant_111", PK_VEC3, {1,1,1}, PSX_ADD111},
+    {"transf_function_enabledF_false", PK_BOOL, {0,0,0}, PSX_F_ON},
+    {"transf_start_iterations_F", PK_INT, {0,0,0}, PSX_START_F},
+    {"transf_stop_iterations_F", PK_INT, {250,0,0}, PSX_STOP_F},
+    {"transf_function_enabledAx", PK_BOOL, {1,0,0}, PSX_F_AX},
+    {"transf_function_enabledx", PK_BOOL, {1,0,0}, PSX_F_X},
+    {"transf_function_enabledAy", PK_BOOL, {1,0,0}, PSX_F_AY},
+    {"transf_function_enabledy", PK_BOOL, {1,0,0}, PSX_F_Y},
+    {"transf_function_enabledAz", PK_BOOL, {1,0,0}, PSX_F_AZ},
+    {"transf_function_enabledz", PK_BOOL, {1,0,0}, PSX_F_Z},
+    {"transf_offsetF_000", PK_VEC3, {0,0,0}, PSX_OFFF000},
+    {"transf_offset_000", PK_VEC3, {0,0,0}, PSX_OFF000},
+    {"transf_scale3D_111", PK_VEC3, {1,1,1}, PSX_S111},
+    {"transf_function_enabled", PK_BOOL, {1,0,0}, PSX_M_ON},
+    {"transf_start_iterations_M", PK_INT, {0,0,0}, PSX_START_M},
+    {"transf_stop_iterations_M", PK_INT, {250,0,0}, PSX_STOP_M},
+    {"transf_constant_multiplierA_111", PK_VEC3, {1,1,1}, PSX_CMA111},
+    {"transf_scaleA_1", PK_DOUBLE, {1,0,0}, PSX_SCALE_A1},
+    {"transf_addition_constantA_000", PK_VEC3, {0,0,0}, PSX_ADD_A000},
+    {"transf_function_enabledN_false", PK_BOOL, {0,0,0}, PSX_FLIP_Z},
+    {"transf_function_enabledAw", PK_BOOL, {1,0,0}, PSX_AW},
+    {"transf_start_iterations_C", PK_INT, {0,0,0}, PSX_START_C},
+    {"transf_stop_iterations_C", PK_INT, {250,0,0}, PSX_STOP_C},
+    {"transf_addition_constant_0777", PK_VEC3, {0.7,0.7,0.7}, PSX_CSIZE},
+    {"transf_scaleB_1", PK_DOUBLE, {1,0,0}, PSX_SCALE_B1},
+    {"transf_minimum_radius_05", PK_DOUBLE, {0.5,0,0}, PSX_MINR05},
+    {"analyticDE_tweak_005", PK_DOUBLE, {0.05,0,0}, PSX_TWEAK005},
+    {"transf_function_enabledAy_false", PK_BOOL, {0,0,0}, PSX_AYF},
+    {"transf_start_iterations_B", PK_INT, {0,0,0}, PSX_START_B},
+    {"transf_stop_iterations_B", PK_INT, {250,0,0}, PSX_STOP_B},
+    {"transf_addition_constant", PK_VEC3, {0,0,0}, PSX_ADD000},
+    {"transf_scale_3", PK_NAMED, {NF_SCALE3,0,0}, PSX_SCALE3},
+};
+static_assert(keys_contiguous(kPseudoKleinianStdDEKeys, PSX_COUNT), "pseudo-Kleinian std DE keys and layout disagree");
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -554,6 +665,8 @@ inline KeyTable formula_keys(int formula) {
       return {kAboxMod11Keys, int(sizeof(kAboxMod11Keys) / sizeof(kAboxMod11Keys[0]))};
     case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4:
       return {kPseudoKleinianMod4Keys, int(sizeof(kPseudoKleinianMod4Keys) / sizeof(kPseudoKleinianMod4Keys[0]))};
+    case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE:
+      return {kPseudoKleinianStdDEKeys, int(sizeof(kPseudoKleinianStdDEKeys) / sizeof(kPseudoKleinianStdDEKeys[0]))};
     default: return {nullptr, 0};
   }
 }

@@ -56,6 +56,7 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: *m = {2, 0, 100.0, 2}; return true;  // fractal_box_fold_bulb_pow2_v2.cpp:16-27
     case MBR_FORMULA_ABOX_MOD11: *m = {1, 0, 100.0, 1}; return true;  // fractal_abox_mod11.cpp:21-32
     case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: *m = {3, 1, 100.0, 4}; return true;  // fractal_pseudo_kleinian_mod4.cpp:17-28
+    case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *m = {5, 1, 100.0, 6}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
     default: return false;
   }
 }
@@ -517,7 +518,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     FormulaMeta m;
     if (!formula_meta(f.formula, &m))
       return set_err(ctx, MBR_EUNSUPPORTED,
-                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 16, 19, 61, 103, 119, 125, 217)", i, f.formula);
+                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 16, 19, 61, 101, 103, 119, 125, 217)", i, f.formula);
     any = true;
     if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
     if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)
@@ -635,6 +636,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
           maxCount = count[i];
           d.de_function = i;
         }
+      if (count[MBR_DE_FUNCTION_CUSTOM] > 0) d.de_function = MBR_DE_FUNCTION_CUSTOM;  // a custom-DE formula wins (:425-429)
     } else {
       d.de_function = sc.delta_de_function;
     }

@@ -476,7 +476,7 @@ struct PrecHybT {
     const float tempDE = de;
     // the Aexion, the one formula that replaces c, is 4-D and never runs here
     V4<float> c{e.cx, e.cy, e.cz, 0.0f};
-    AuxX<float> ax{1.0f, 0.0f, 0.0f, 1.0f, c};  // formulas with orbit state do not run here (check_supported)
+    AuxX<float> ax{1.0f, 0.0f, 0.0f, 1.0f, 1000.0f, c};  // formulas with orbit state do not run here (check_supported)
     if (s.d[P_WEIGHT] > 0.0) formula_dispatch<float, false, EXT>(s.formula, z, e.r, de, s, &sc.mbrot, &sc.ifs, i, c, ax);
     if (s.add_c) {
       if (sc.julia) {

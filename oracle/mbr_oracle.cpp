@@ -72,6 +72,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: *fi = {2, 0, 100.0, 2, 0}; return true;  // fractal_box_fold_bulb_pow2_v2.cpp:16-27
     case MBR_FORMULA_ABOX_MOD11: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_abox_mod11.cpp:21-32
     case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian_mod4.cpp:17-28
+    case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *fi = {5, 1, 100.0, 6, 0}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
     default: return false;
   }
 }
@@ -249,6 +250,7 @@ static bool build_sequence(const mbr_scene &sc, Seq *out) {
           maxCount = count[i];
           s.de_function = i;
         }
+      if (count[5] > 0) s.de_function = 5;  // a custom-DE formula wins (:425-429)
     } else {
       s.de_function = sc.delta_de_function;
     }
@@ -1045,6 +1047,142 @@ inline void formula_pseudo_kleinian_mod4(V4<S> &z, const SlotT<S> &f, S &DE, S &
   if (x[P4X_FLIP_Z] != 0.0) z.z = -z.z;
 }
 
+// Benesi's tetrahedral frame turns (abstract_fractal.h:30-32 constants)
+template <class S>
+inline V4<S> benesi_in(const V4<S> &z) {
+  const double s13 = 0.57735026918962576450914878050196, s12 = 0.70710678118654752440084436210485,
+               s23 = 0.81649658092772603273242802490196;
+  const S t = z.x * s23 - z.z * s13;
+  return V4<S>{(t - z.y) * s12, (t + z.y) * s12, z.x * s13 + z.z * s23, z.w};
+}
+template <class S>
+inline V4<S> benesi_out(const V4<S> &z) {
+  const double s13 = 0.57735026918962576450914878050196, s12 = 0.70710678118654752440084436210485,
+               s23 = 0.81649658092772603273242802490196;
+  const S t = (z.y + z.x) * s12;
+  return V4<S>{z.z * s13 + t * s23, (z.y - z.x) * s12, z.z * s23 - t * s13, z.w};
+}
+
+// cFractalPseudoKleinianStdDE::FormulaCode (fractal_pseudo_kleinian_std_de.cpp:
+// 29-215) without the aux.color terms; dist is aux.dist
+template <class S>
+inline void formula_pseudo_kleinian_std_de(V4<S> &z, const SlotT<S> &f, S &DE, S &dist, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  if (x[PSX_P_ON] != 0.0 && i >= int(x[PSX_START_P]) && i < int(x[PSX_STOP_P1])) {
+    const double kSqrt34 = 0.86602540378443864676372317075294, kSqrt3 = 1.73205080756887729352744634150587;
+    z.y = fabs(z.y);
+    z.z = fabs(z.z);
+    const S dot1 = (z.x * -kSqrt34 + z.y * 0.5) * x[PSX_SCALE];
+    S t = std::max(S(0.0), dot1);
+    z.x = z.x - t * -kSqrt3;
+    z.y = fabs(z.y - t);
+    if (z.y > z.z) std::swap(z.y, z.z);
+    z.x = z.x - x[PSX_CM000] * kSqrt34;
+    z.y = z.y - x[PSX_CM000 + 1] * 1.5;
+    z.z = z.z - x[PSX_CM000 + 2] * 1.5;
+    z.w = z.w - 1.0 * 0.0;
+    if (z.z > z.x) std::swap(z.z, z.x);
+    if (z.x > 0.0) {
+      z.y = std::max(S(0.0), z.y);
+      z.z = std::max(S(0.0), z.z);
+    }
+  }
+  if (x[PSX_R_ON] != 0.0 && i >= int(x[PSX_START_R]) && i < int(x[PSX_STOP_R]))
+    z = mb_turn(x + PSX_ROT + 1, x[PSX_ROT] != 0.0, false, z);
+  if (x[PSX_T1_ON] != 0.0 && i >= int(x[PSX_START]) && i < int(x[PSX_STOP_T1])) {
+    z = benesi_in(z);
+    const S tempL = len4(z);
+    z = V4<S>{fabs(z.x) * x[PSX_S222], fabs(z.y) * x[PSX_S222 + 1], fabs(z.z) * x[PSX_S222 + 2], fabs(z.w) * 1.0};
+    const S avgScale = len4(z) / tempL;
+    DE = DE * avgScale + 1.0;
+    z = benesi_out(z);
+    z.x = z.x - x[PSX_OFF200];
+    z.y = z.y - x[PSX_OFF200 + 1];
+    z.z = z.z - x[PSX_OFF200 + 2];
+    z.w = z.w - 0.0;
+  }
+  if (x[PSX_TM_ON] != 0.0 && i >= int(x[PSX_START_D]) && i < int(x[PSX_STOP_TM1])) {
+    z = benesi_in(z);
+    const S tempL = len4(z);
+    z = V4<S>{fabs(z.x) * x[PSX_S333], fabs(z.y) * x[PSX_S333 + 1], fabs(z.z) * x[PSX_S333 + 2], fabs(z.w) * 1.0};
+    const S avgScale = len4(z) / tempL;
+    DE = DE * avgScale + 1.0;
+    z.x = fabs(z.x + x[PSX_ADD111]) - fabs(z.x - x[PSX_ADD111]) - z.x;
+    z.y = fabs(z.y + x[PSX_ADD111 + 1]) - fabs(z.y - x[PSX_ADD111 + 1]) - z.y;
+    z.z = fabs(z.z + x[PSX_ADD111 + 2]) - fabs(z.z - x[PSX_ADD111 + 2]) - z.z;
+    z.w = fabs(z.w + 0.0) - fabs(z.w - 0.0) - z.w;
+    z = benesi_out(z);
+  }
+  if (x[PSX_F_ON] != 0.0 && i >= int(x[PSX_START_F]) && i < int(x[PSX_STOP_F])) {
+    S ta = S(0.0), tb = S(0.0);
+    if (x[PSX_F_AX] != 0.0) ta = fabs(z.x + x[PSX_OFFF000]);
+    if (x[PSX_F_X] != 0.0) tb = fabs(z.x - x[PSX_OFF000]);
+    z.x = ta - tb - (z.x * x[PSX_S111]);
+    ta = S(0.0);
+    tb = S(0.0);
+    if (x[PSX_F_AY] != 0.0) ta = fabs(z.y + x[PSX_OFFF000 + 1]);
+    if (x[PSX_F_Y] != 0.0) tb = fabs(z.y - x[PSX_OFF000 + 1]);
+    z.y = ta - tb - (z.y * x[PSX_S111 + 1]);
+    ta = S(0.0);
+    tb = S(0.0);
+    if (x[PSX_F_AZ] != 0.0) ta = fabs(z.z + x[PSX_OFFF000 + 2]);
+    if (x[PSX_F_Z] != 0.0) tb = fabs(z.z - x[PSX_OFF000 + 2]);
+    z.z = ta - tb - (z.z * x[PSX_S111 + 2]);
+  }
+  if (x[PSX_M_ON] != 0.0 && i >= int(x[PSX_START_M]) && i < int(x[PSX_STOP_M])) {
+    z = V4<S>{fabs(z.x), fabs(z.y), fabs(z.z), fabs(z.w)};
+    if (z.x - z.y < 0.0) std::swap(z.y, z.x);
+    if (z.x - z.z < 0.0) std::swap(z.z, z.x);
+    if (z.y - z.z < 0.0) std::swap(z.z, z.y);
+    z = z * x[PSX_SCALE3];
+    z.x = z.x - 2.0 * x[PSX_CMA111];
+    z.y = z.y - 2.0 * x[PSX_CMA111 + 1];
+    if (z.z > 1.0) z.z = z.z - 2.0 * x[PSX_CMA111 + 2];
+    DE = DE * (x[PSX_SCALE3] * x[PSX_SCALE_A1]);
+    z.x = z.x + x[PSX_ADD_A000];
+    z.y = z.y + x[PSX_ADD_A000 + 1];
+    z.z = z.z + x[PSX_ADD_A000 + 2];
+    z.w = z.w + 0.0;
+  }
+  if (x[PSX_FLIP_Z] != 0.0) z.z = -z.z;
+  const double cx = x[PSX_CSIZE], cy = x[PSX_CSIZE + 1], cz = x[PSX_CSIZE + 2];
+  if (x[PSX_AW] != 0.0 && i >= int(x[PSX_START_C]) && i < int(x[PSX_STOP_C])) {
+    V4<S> t = z;
+    if (z.x > cx) t.x = cx;
+    if (z.x < -cx) t.x = -cx;
+    if (z.y > cy) t.y = cy;
+    if (z.y < -cy) t.y = -cy;
+    if (z.z > cz) t.z = cz;
+    if (z.z < -cz) t.z = -cz;
+    z = z * x[PSX_SCALE_B1];
+    DE = DE * fabs(x[PSX_SCALE_B1]);
+    z.x = t.x * 2.0 - z.x;
+    z.y = t.y * 2.0 - z.y;
+    z.z = t.z * 2.0 - z.z;
+    z.w = t.w * 2.0 - z.w;
+    const S k = std::max(S(x[PSX_MINR05] / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), S(1.0));
+    z = z * k;
+    DE = DE * (k + x[PSX_TWEAK005]);
+  }
+  if (x[PSX_AYF] != 0.0 && i >= int(x[PSX_START_B]) && i < int(x[PSX_STOP_B])) {
+    if (z.x > cx) z.x = cx * 2.0 - z.x;
+    if (z.x < -cx) z.x = -cx * 2.0 - z.x;
+    if (z.y > cy) z.y = cy * 2.0 - z.y;
+    if (z.y < -cy) z.y = -cy * 2.0 - z.y;
+    if (z.z > cz) z.z = cz * 2.0 - z.z;
+    if (z.z < -cz) z.z = -cz * 2.0 - z.z;
+    const S k = std::max(S(x[PSX_MINR05] / (z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w)), S(1.0));
+    z = z * k;
+    DE = DE * (k + x[PSX_TWEAK005]);
+  }
+  z.x = z.x + x[PSX_ADD000];
+  z.y = z.y + x[PSX_ADD000 + 1];
+  z.z = z.z + x[PSX_ADD000 + 2];
+  z.w = z.w + 0.0;
+  dist = sqrt(z.x * z.x + z.y * z.y) / DE;
+}
+
 // (x, y, z) in the order of enumMulti_OrderOfXYZ (fractal.h:282-289)
 template <class S>
 inline V4<S> order_xyz(const V4<S> &v, int order) {
@@ -1358,6 +1496,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
   S actualScale = seq.length > 0 ? S(seq.slot[seq.seq[0]].mb_scale) : S(seq.slot[0].mb_scale);
   V4<S> auxC = z;  // aux.c (:107)
   S posNeg = 1.0;  // aux.pos_neg (:109)
+  S auxDist = 1000.0;  // aux.dist (:119)
   V4<S> lastZ{S(0.0), S(0.0), S(0.0), S(0.0)}, lastGoodZ = lastZ, lastLastZ = lastZ;
   int maxN = seq.formula_maxiter * maxiterMultiplier;
   if (forcedMaxiter >= 0) maxN = forcedMaxiter;
@@ -1412,6 +1551,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_BOX_FOLD_BULB_POW2_V2: formula_box_fold_bulb_pow2_v2(z, f, DE, scaleA, i); break;
         case MBR_FORMULA_ABOX_MOD11: formula_abox_mod11(z, f, DE, actualScale, auxC, const_c, i); break;
         case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: formula_pseudo_kleinian_mod4(z, f, DE, pk, posNeg, i); break;
+        case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: formula_pseudo_kleinian_std_de(z, f, DE, auxDist, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;
@@ -1479,7 +1619,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
           out.distance = std::max(S(rxy - pk), S(fabs(rxy * z.z) / r)) / DE;
           break;
         }
-        case 5: out.distance = 1000.0; break;
+        case 5: out.distance = auxDist; break;
         case 6: out.distance = std::max(fabs(z.x), std::max(fabs(z.y), fabs(z.z))) / DE; break;
         default: out.distance = 0.0; break;
       }
@@ -1493,7 +1633,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
           out.distance = std::max(S(rxy - pk), S(fabs(rxy * z.z) / r)) / DE;
           break;
         }
-        case 6: out.distance = 1000.0; break;
+        case 6: out.distance = auxDist; break;
         case 7: out.distance = std::max(fabs(z.x), std::max(fabs(z.y), fabs(z.z))) / DE; break;
         case 0: out.distance = -1.0; break;
         default: out.distance = r; break;

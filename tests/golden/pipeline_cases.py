@@ -206,6 +206,25 @@ def _keyed_formula_cases():
                               transf_function_enabledA_false=1, transf_offset_0=0.1, transf_offsetA_0=0.05,
                               transf_function_enabledBx_false=1, transf_function_enabledAx_false=1,
                               transf_offsetA_1=0.8, transf_function_enabledz_false=1)
+    t["pksd_default"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_STD_DE, 30)
+    t["pksd_benesi"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_STD_DE, 30, transf_benesi_T1_enabled_false=1,
+                              transf_stop_iterationsT_1=2, transf_scale3D_222=[2.0, 1.9, 2.1],
+                              transf_offset_200=[1.9, 0.1, 0.0], transf_function_enabledx_false=1,
+                              transf_start_iterations_D=1, transf_stop_iterationsTM_1=3,
+                              transf_function_enabledR_false=1, transf_rotation=[10.0, 0.0, 20.0])
+    t["pksd_folds"] = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_STD_DE, 30, transf_function_enabledF_false=1,
+                             transf_offsetF_000=[0.5, 0.4, 0.3], transf_offset_000=[0.2, 0.1, 0.0],
+                             transf_function_enabledAy=0, transf_function_enabledP_false=1,
+                             transf_stop_iterations_P1=2, transf_constant_multiplier_000=[0.2, 0.1, 0.1],
+                             transf_stop_iterations_M=2, transf_scaleA_1=0.9, transf_function_enabledAy_false=1,
+                             transf_start_iterations_B=3, transf_scaleB_1=1.05, transf_function_enabledN_false=1)
+    s = _keyed(abi.FORMULA_PSEUDO_KLEINIAN_STD_DE, 20)
+    s.hybrid_fractal_enable = 1
+    s.n_fractals = 2
+    abi.fractal_defaults(s.fractal[1], abi.FORMULA_MANDELBOX)
+    s.fractal[1].formula_iterations = 2
+    s.fractal[1].mandelbox_scale = -1.5
+    t["hybrid_pksd_box"] = s
     t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
                                  transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t

@@ -200,7 +200,8 @@ KEYED_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk
                "bfbp2_forced_analytic", "menger_mod1_default", "menger_mod1_rotation",
                "menger_mod1_box_offset_blend", "hybrid_menger_mod1_bfbp2", "bfbp2v2_default", "bfbp2v2_vary",
                "bfbp2v2_vary_m", "abox_mod11_default", "abox_mod11_folds", "abox_mod11_curve_c",
-               "hybrid_abox_mod11_bulb", "pkm4_default", "pkm4_sphere_box", "pkm4_fold_n"]
+               "hybrid_abox_mod11_bulb", "pkm4_default", "pkm4_sphere_box", "pkm4_fold_n", "pksd_default",
+               "pksd_benesi", "pksd_folds", "hybrid_pksd_box"]
 
 
 @pytest.mark.parametrize("case", KEYED_CASES)
