@@ -217,6 +217,11 @@ struct Reader {
   // settings.cpp:2372-2401, copies a non-default one into every slot)
   double f_pos[kSlots][3] = {}, f_rot[kSlots][3] = {}, f_rep[kSlots][3] = {}, f_scale[kSlots];
   double g_pos[3] = {0, 0, 0}, g_rot[3] = {0, 0, 0}, g_rep[3] = {0, 0, 0};
+  // the per-fractal node parameters of a boolean combination (the fractal
+  // containers' julia_mode, julia_c, fractal_constant_factor, initial_waxis,
+  // formula_maxiter; initparameters.cpp:705-715) and boolean_operator_K
+  int f_julia[kSlots] = {}, f_maxiter[kSlots], bool_op[kSlots + 1], bool_op_set[kSlots + 1] = {};
+  double f_julia_c[kSlots][3] = {}, f_cmul[kSlots][3], f_w0[kSlots] = {};
   int ao_enabled = 0, ao_mode = 2;
   double ao_intensity = 1.0;
   int ao_quality = 4;
@@ -235,6 +240,8 @@ struct Reader {
       formula[i] = i == 0 ? MBR_FORMULA_MANDELBULB : MBR_FORMULA_NONE;
       slot_enable[i] = 1;
       f_scale[i] = 1.0;
+      f_maxiter[i] = 250;
+      for (int k = 0; k < 3; k++) f_cmul[i][k] = 1.0;
     }
   }
 
@@ -371,6 +378,28 @@ void read_primitive_param(Reader &R, const std::string &full, const std::string 
   }
 }
 
+// A fractal container's node parameter (julia_mode, julia_c,
+// fractal_constant_factor, initial_waxis, formula_maxiter) of slot `slot`:
+// true when `base` is one of them.
+bool read_node_param(Reader &R, int slot, const std::string &base, const std::string &value) {
+  int b;
+  double d, v[3];
+  if (base == "julia_mode") {
+    if (parse_bool(value, b)) R.f_julia[slot] = b; else R.bad(base, value);
+  } else if (base == "julia_c") {
+    if (parse_vec3(value, v)) std::memcpy(R.f_julia_c[slot], v, sizeof(v)); else R.bad(base, value);
+  } else if (base == "fractal_constant_factor") {
+    if (parse_vec3(value, v)) std::memcpy(R.f_cmul[slot], v, sizeof(v)); else R.bad(base, value);
+  } else if (base == "initial_waxis") {
+    if (parse_double(value, d)) R.f_w0[slot] = d; else R.bad(base, value);
+  } else if (base == "formula_maxiter") {
+    if (parse_int(value, b)) R.f_maxiter[slot] = b; else R.bad(base, value);
+  } else {
+    return false;
+  }
+  return true;
+}
+
 void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &name, const std::string &value) {
   mbr_fractal &f = sc->fractal[slot];
   double d;
@@ -466,6 +495,8 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
     if (parse_int(value, b)) f.formula_start_iteration = b; else R.bad(name, value);
   } else if (name == "formula_stop_iteration") {
     if (parse_int(value, b)) f.formula_stop_iteration = b; else R.bad(name, value);
+  } else if (read_node_param(R, slot, name, value)) {
+    // a node parameter of the fractal container
   } else {
     // a parameter the slot's formula reads by key (formula_params.h)
     const mbr::KeyTable t = mbr::formula_keys(R.formula[slot]);
@@ -503,6 +534,82 @@ void read_fractal_param(Reader &R, mbr_scene *sc, int slot, const std::string &n
 }
 
 bool nonzero3(const double v[3]) { return v[0] != 0.0 || v[1] != 0.0 || v[2] != 0.0; }
+
+// A node of an explicit objects tree with InitNodeParams' defaults
+// (initparameters.cpp:2102-2125).
+mbr_node tree_node(int type, int level, int index) {
+  mbr_node n;
+  std::memset(&n, 0, sizeof(n));
+  n.type = type;
+  n.level = level;
+  n.index = index;
+  n.enabled = 1;
+  n.scale = 1.0;
+  n.detail_level_multiplier = 1.0;
+  n.smooth_combine_distance = 0.1;
+  n.formula_maxiter = 250;
+  for (int k = 0; k < 3; k++) n.fractal_constant_factor[k] = 1.0;
+  return n;
+}
+
+// The legacy boolean mode (MigrateToObjectsTree, settings.cpp:2608-2712): the
+// m slots with a formula combine left to right, ((f1 op f2) op f3) ..., each
+// operator a group (boolean_operator_K: 0 intersection, 2 subtraction, else
+// union; a missing one takes boolean_operator_1's value, else union), each
+// fractal a node with its slot's formula transform (CopyFormulaTransform) and
+// node parameters (CopyOneFractalParams; formula_maxiter is N for files
+// before 2.29, settings.cpp:1721-1733), disabled when its fractal_enable_K is
+// false.  The file's primitives join by union at the root.
+void build_boolean_tree(Reader &R, mbr_scene *scene) {
+  int en[kSlots], m = 0;
+  for (int i = 0; i < kSlots; i++)
+    if (R.formula[i] != MBR_FORMULA_NONE) en[m++] = i;
+  if (m == 0) return;
+  const int npr = scene->n_primitives;
+  const int root_shift = npr > 0 ? 1 : 0;
+  const int count = (2 * m - 1) + root_shift + npr;
+  if (count > MBR_MAX_NODES || (m - 1) + root_shift > 8) {
+    R.unsupported.push_back("boolean_operators with " + std::to_string(m) + " fractals and " + std::to_string(npr) +
+                            " primitives (more than " + std::to_string(MBR_MAX_NODES) + " tree nodes)");
+    return;
+  }
+  const int default_op = R.bool_op_set[1] ? R.bool_op[1] : 1;
+  auto op_type = [&](int j) {  // the group joining fractals 0..j-1 with fractal j (ToNodeType, :2418-2426)
+    int idx = en[j];
+    if (idx < 1) idx = 1;
+    const int op = R.bool_op_set[idx] ? R.bool_op[idx] : default_op;
+    return op == 0 ? MBR_NODE_BOOLEAN_MUL : (op == 2 ? MBR_NODE_BOOLEAN_SUB : MBR_NODE_BOOLEAN_ADD);
+  };
+  auto fractal_node = [&](int j, int level) {
+    const int k = en[j];
+    mbr_node n = tree_node(MBR_NODE_FRACTAL, level, k);
+    n.enabled = R.slot_enable[k] ? 1 : 0;
+    std::memcpy(n.position, R.f_pos[k], sizeof(n.position));
+    std::memcpy(n.rotation, R.f_rot[k], sizeof(n.rotation));
+    std::memcpy(n.repeat, R.f_rep[k], sizeof(n.repeat));
+    n.scale = R.f_scale[k];
+    n.formula_maxiter = R.version < 2.29 ? R.N : R.f_maxiter[k];
+    n.julia_mode = R.f_julia[k];
+    std::memcpy(n.julia_c, R.f_julia_c[k], sizeof(n.julia_c));
+    std::memcpy(n.fractal_constant_factor, R.f_cmul[k], sizeof(n.fractal_constant_factor));
+    n.initial_waxis = R.f_w0[k];
+    return n;
+  };
+  int nn = 0;
+  if (root_shift) scene->node[nn++] = tree_node(MBR_NODE_BOOLEAN_ADD, 0, 0);
+  if (m == 1) {
+    scene->node[nn++] = fractal_node(0, root_shift);
+  } else {
+    // preorder: the groups from the root inward, then fractals 0 and 1 in
+    // the innermost group, then fractal j in the group that joins it
+    for (int j = m - 1; j >= 1; j--) scene->node[nn++] = tree_node(op_type(j), root_shift + (m - 1 - j), 0);
+    scene->node[nn++] = fractal_node(0, root_shift + m - 1);
+    scene->node[nn++] = fractal_node(1, root_shift + m - 1);
+    for (int j = 2; j < m; j++) scene->node[nn++] = fractal_node(j, root_shift + m - j);
+  }
+  for (int k = 0; k < npr; k++) scene->node[nn++] = tree_node(MBR_NODE_PRIMITIVE, 1, k);
+  scene->n_nodes = nn;
+}
 
 void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_params *p, std::string name,
                      std::string value) {
@@ -558,9 +665,17 @@ void read_main_param(Reader &R, mbr_scene *sc, mbr_camera *cam, mbr_render_param
     }
     // julia_mode_K, julia_c_K, fractal_constant_factor_K, initial_waxis_K,
     // formula_maxiter_K, boolean_operator_K: read by the boolean combination only
-    if (base == "julia_mode" || base == "julia_c" || base == "fractal_constant_factor" ||
-        base == "initial_waxis" || base == "formula_maxiter" || base == "boolean_operator" ||
-        base == "formula_material_id") {
+    if (read_node_param(R, slot, base, value)) return;
+    if (base == "boolean_operator") {
+      if (parse_int(value, b)) {
+        R.bool_op[slot + 1] = b;
+        R.bool_op_set[slot + 1] = 1;
+      } else {
+        R.bad(name, value);
+      }
+      return;
+    }
+    if (base == "formula_material_id") {
       R.ignored.push_back(name);
       return;
     }
@@ -875,23 +990,26 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
 
   // formulas: a single fractal renders slot 1; a hybrid iterates every slot
   // whose formula is not none (MigrateToObjectsTree, settings.cpp:2716-2830)
-  if (R.boolean_ops) R.unsupported.push_back("boolean_operators (boolean combination of fractals)");
+  // a boolean combination of the slots with a formula (MigrateToObjectsTree,
+  // settings.cpp:2608-2712) becomes an explicit objects tree (below)
+  const bool boolean = R.boolean_ops && !R.hybrid;
+  if (R.boolean_ops && R.hybrid) R.unsupported.push_back("boolean_operators with a hybrid (boolean combination of fractals)");
   scene->hybrid_fractal_enable = R.hybrid;
   int last = 0;
   for (int i = 0; i < kSlots; i++) {
     scene->fractal[i].formula = R.formula[i];
     if (R.formula[i] != MBR_FORMULA_NONE) last = i + 1;
   }
-  scene->n_fractals = R.hybrid ? (last > 0 ? last : 1) : 1;
+  scene->n_fractals = (R.hybrid || boolean) ? (last > 0 ? last : 1) : 1;
   // the scene holds one IFS block and one Mandelbox-rotation block
   int n_ifs = 0, n_box = 0;
-  for (int i = 0; i < scene->n_fractals && (R.hybrid || i == 0); i++) {
+  for (int i = 0; i < scene->n_fractals && (R.hybrid || boolean || i == 0); i++) {
     if (R.formula[i] == MBR_FORMULA_KALEIDOSCOPIC_IFS) n_ifs++;
     if (R.formula[i] == MBR_FORMULA_MANDELBOX) n_box++;
   }
   for (int i = 0; i < scene->n_fractals; i++) {
     const int f = R.formula[i];
-    if (!R.hybrid && i > 0) break;
+    if (!R.hybrid && !boolean && i > 0) break;
     if (f == MBR_FORMULA_NONE) continue;
     if (f != MBR_FORMULA_MANDELBULB && f != MBR_FORMULA_MANDELBOX && f != MBR_FORMULA_MENGER_SPONGE &&
         f != MBR_FORMULA_MANDELBULB_POWER2 && f != MBR_FORMULA_HYPERCOMPLEX && f != MBR_FORMULA_KALEIDOSCOPIC_IFS &&
@@ -904,7 +1022,7 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
                               "101 pseudo-Kleinian std DE, 119 Abox mod 11, 125 box fold bulb pow 2 V2, 217 pseudo-Kleinian mod 4 are)");
     if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && n_ifs > 1)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in more than one slot)");
-    if (!R.slot_enable[i]) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
+    if (!R.slot_enable[i] && !boolean) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");
     if (f == MBR_FORMULA_MANDELBOX && n_box > 1 &&
         (scene->fractal[i].mandelbox_rotations_enabled || scene->fractal[i].mandelbox_main_rotation_enabled))
       R.unsupported.push_back("fractal_" + std::to_string(i + 1) +
@@ -1041,7 +1159,9 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
   bool transformed = false;
   for (int i = 0; i < iterated; i++)
     if (nonzero3(R.f_pos[i]) || nonzero3(R.f_rot[i]) || nonzero3(R.f_rep[i]) || R.f_scale[i] != 1.0) transformed = true;
-  if (transformed && (R.hybrid || R.boolean_ops)) {
+  if (boolean) {
+    build_boolean_tree(R, scene);
+  } else if (transformed && (R.hybrid || R.boolean_ops)) {
     R.unsupported.push_back("formula or fractal transform of a hybrid or boolean combination");
   } else if (transformed) {
     if (!(std::fabs(R.f_scale[0]) > 1e-12)) {

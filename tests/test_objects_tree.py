@@ -143,3 +143,29 @@ def test_settings_transform_of_a_single_fractal_becomes_a_tree():
     s = settings.load_from_string(head + "[main_parameters]\nformula_1 8;\nformula_2 2;\nhybrid_fractal_enable true;\n"
                                   "fractal_position 1 0 0;\n")
     assert s.status == abi.MBR_EUNSUPPORTED
+
+
+def test_settings_boolean_mode_becomes_a_tree():
+    """The legacy boolean mode (boolean_operators): the slots with a formula
+    combine left to right as nested groups (boolean_operator_K: 0
+    intersection, 2 subtraction, else union; a missing operator takes
+    boolean_operator_1's value), each fractal node with its own iteration
+    limit (N before version 2.29) and julia settings; primitives join by
+    union at the root."""
+    from mandelbulber2_b200 import settings
+
+    head = "# Mandelbulber settings file\n# version 2.26\n# only modified parameters\n"
+    txt = head + ("[main_parameters]\nboolean_operators true;\nboolean_operator_1 2;\nN 20;\n"
+                  "formula_1 8;\nformula_2 2;\nformula_3 7;\njulia_mode_2 true;\njulia_c_2 0,1 0,2 0,3;\n"
+                  "formula_position_3 0 0 1;\nprimitive_plane_1_enabled true;\n")
+    s = settings.load_from_string(txt)
+    assert s.ok, s.report
+    sc = s.scene
+    kinds = [(sc.node[i].type, sc.node[i].level, sc.node[i].index) for i in range(sc.n_nodes)]
+    SUB, ADD, F, P = abi.NODE_BOOLEAN_SUB, abi.NODE_BOOLEAN_ADD, abi.NODE_FRACTAL, abi.NODE_PRIMITIVE
+    # root union with the plane; ((box - bulb) - menger): operators 1 and 2 both take operator 1's value
+    assert kinds == [(ADD, 0, 0), (SUB, 1, 0), (SUB, 2, 0), (F, 3, 0), (F, 3, 1), (F, 2, 2), (P, 1, 0)], kinds
+    assert all(sc.node[i].formula_maxiter == 20 for i in (3, 4, 5))
+    assert sc.node[4].julia_mode == 1 and list(sc.node[4].julia_c) == [0.1, 0.2, 0.3]
+    assert list(sc.node[5].position) == [0.0, 0.0, 1.0]
+    scene_sequence(sc)
