@@ -67,6 +67,7 @@ typedef enum mbr_formula {
   MBR_FORMULA_MANDELBOX = 8,    /* formula/definition/fractal_mandelbox.cpp:31-107 */
   /* formulas whose parameters are passed by settings key (mbr_fractal.param) */
   MBR_FORMULA_BOX_FOLD_BULB_POW2 = 16, /* formula/definition/fractal_box_fold_bulb_pow2.cpp:27-76 (delta DE) */
+  MBR_FORMULA_GENERALIZED_FOLD_BOX = 37, /* formula/definition/fractal_generalized_fold_box.cpp:31-245 */
   MBR_FORMULA_MENGER_MOD1 = 61,       /* formula/definition/fractal_menger_mod1.cpp:29-103 */
   MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 = 125, /* formula/definition/fractal_box_fold_bulb_pow2_v2.cpp:29-146 */
   MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE = 101, /* formula/definition/fractal_pseudo_kleinian_std_de.cpp:29-215 (custom DE) */

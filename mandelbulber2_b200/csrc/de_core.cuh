@@ -895,6 +895,123 @@ __device__ __noinline__ void f_pseudo_kleinian_std_de(V4<T> &z, T &DE, AuxX<T> &
   ax.dist = m_sqrt(T(z.x * z.x + z.y * z.y)) / DE;  // :183
 }
 
+// three-vector helpers of the generalized fold box (CVector3 Dot, Cross)
+template <class T>
+struct G3 {
+  T x, y, z;
+};
+template <class T>
+__device__ __forceinline__ T g3dot(const G3<T> &a, const G3<T> &b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+
+// cFractalGeneralizedFoldBox::FormulaCode (fractal_generalized_fold_box.cpp:
+// 31-245), the aux.color terms left out: a fold in the planes of a
+// polyhedron (mirror, rotation line or inversion point, above the melt
+// layer), then the Mandelbox sphere fold, main rotation and scale
+template <class T>
+__device__ __noinline__ void f_generalized_fold_box(V4<T> &z, T &DE, const DevSlot &s) {
+  const double *x = s.x;
+  const int sides = int(x[GFX_SIDES]);
+  const T solid = T(x[GFX_SOLID]), melt = T(x[GFX_MELT]);
+  auto nv = [&](int i) { return G3<T>{T(x[GFX_NV + 3 * i]), T(x[GFX_NV + 3 * i + 1]), T(x[GFX_NV + 3 * i + 2])}; };
+  G3<T> zz{z.x, z.y, z.z};
+  G3<T> L = zz;
+  T a = T(1.0);
+  int side = -1;
+  for (int i = 0; i < sides; i++) {  // the closest plane cutting the line origin..z
+    const T b = solid, c = g3dot(L, nv(i));
+    if ((c > T(0.0)) && ((a * c) > b)) {
+      side = i;
+      a = b / c;
+    }
+  }
+  if (side != -1) {
+    const int side_m = side;
+    const G3<T> Nm = nv(side_m);
+    const T dm = g3dot(zz, Nm) - solid;
+    const G3<T> Xm{zz.x - Nm.x * dm, zz.y - Nm.y * dm, zz.z - Nm.z * dm};
+    L = G3<T>{Xm.x - Nm.x, Xm.y - Nm.y, Xm.z - Nm.z};
+    G3<T> Y = Nm;
+    a = T(1.0);
+    side = -1;
+    for (int i = 0; i < sides; i++) {
+      if (i != side_m) {
+        const T b = solid - g3dot(Y, nv(i)), c = g3dot(L, nv(i));
+        if ((c > T(0.0)) && ((a * c) > b)) {
+          side = i;
+          a = b / c;
+        }
+      }
+    }
+    G3<T> target;
+    if (side != -1) {  // rotation check
+      const G3<T> Xmr{Y.x + L.x * a, Y.y + L.y * a, Y.z + L.z * a};
+      const int side_r = side;
+      const G3<T> Nr = nv(side_r);
+      G3<T> Lr{Nm.y * Nr.z - Nm.z * Nr.y, -Nm.x * Nr.z + Nm.z * Nr.x, Nm.x * Nr.y - Nm.y * Nr.x};
+      T a_rmin = (g3dot(zz, Lr) - g3dot(Xmr, Lr)) / (g3dot(Lr, Lr));
+      if (a_rmin < T(0.0)) {
+        a_rmin = -a_rmin;
+        Lr = G3<T>{Lr.x * T(-1.0), Lr.y * T(-1.0), Lr.z * T(-1.0)};
+      }
+      const G3<T> Xr{Xmr.x + Lr.x * a_rmin, Xmr.y + Lr.y * a_rmin, Xmr.z + Lr.z * a_rmin};
+      L = G3<T>{Xr.x - Xmr.x, Xr.y - Xmr.y, Xr.z - Xmr.z};
+      Y = Xmr;
+      a = T(1.0);
+      side = -1;
+      for (int i = 0; i < sides; i++) {
+        if ((i != side_m) && (i != side_r)) {
+          const T b = solid - g3dot(Y, nv(i)), c = g3dot(L, nv(i));
+          if ((c > T(0.0)) && ((a * c) > b)) {
+            side = i;
+            a = b / c;
+          }
+        }
+      }
+      target = (side != -1) ? G3<T>{Y.x + L.x * a, Y.y + L.y * a, Y.z + L.z * a} : Xr;
+    } else {
+      target = Xm;
+    }
+    const G3<T> z2X{target.x - zz.x, target.y - zz.y, target.z - zz.z};
+    if (g3dot(z2X, z2X) > (melt * melt)) {  // above the melt layer
+      const T mag = m_sqrt(g3dot(z2X, z2X));
+      const T k = T(2.0) * (mag - melt) / (mag + T(.00000001));
+      zz = G3<T>{zz.x + z2X.x * k, zz.y + z2X.y * k, zz.z + z2X.z * k};
+    }
+  }
+  const T r2 = g3dot(zz, zz);
+  z.x = zz.x + T(x[GFX_MB_OFFSET]);
+  z.y = zz.y + T(x[GFX_MB_OFFSET + 1]);
+  z.z = zz.z + T(x[GFX_MB_OFFSET + 2]);
+  const double mR2 = x[GFX_MB_MINR] * x[GFX_MB_MINR], fR2 = x[GFX_MB_FIXEDR] * x[GFX_MB_FIXEDR];
+  if (r2 < T(mR2)) {
+    const T f1 = T(fR2 / mR2);
+    z.x = z.x * f1;
+    z.y = z.y * f1;
+    z.z = z.z * f1;
+    z.w = z.w * f1;
+    DE = DE * f1;
+  } else if (r2 < T(fR2)) {
+    const T f2 = T(fR2) / r2;
+    z.x = z.x * f2;
+    z.y = z.y * f2;
+    z.z = z.z * f2;
+    z.w = z.w * f2;
+    DE = DE * f2;
+  }
+  z.x = z.x - T(x[GFX_MB_OFFSET]);
+  z.y = z.y - T(x[GFX_MB_OFFSET + 1]);
+  z.z = z.z - T(x[GFX_MB_OFFSET + 2]);
+  if (x[GFX_MAIN_ON] != 0.0 && x[GFX_MAIN_ROT] == 0.0) z = mb_turn<T>(x + GFX_MAIN_ROT + 1, false, z);
+  const T sc = T(x[GFX_MB_SCALE]);
+  z.x = z.x * sc;
+  z.y = z.y * sc;
+  z.z = z.z * sc;
+  z.w = z.w * sc;
+  DE = DE * T(fabs(x[GFX_MB_SCALE])) + T(1.0);
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -1022,6 +1139,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_ABOX_MOD11: f_abox_mod11<T>(z, DE, ax, c, s, i); break;
       case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: f_pseudo_kleinian_mod4<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: f_pseudo_kleinian_std_de<T>(z, DE, ax, s, i); break;
+      case MBR_FORMULA_GENERALIZED_FOLD_BOX: f_generalized_fold_box<T>(z, DE, s); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;

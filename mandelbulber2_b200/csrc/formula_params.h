@@ -36,7 +36,9 @@ enum NamedField {
   NF_ADE_SCALE1,     // analytic_de_scale1 (analyticDE_scale_1)
   NF_ADE_OFFSET1,    // analytic_de_offset1 (analyticDE_offset_1)
   NF_SCALE3,         // transf_scale3 (transf_scale_3)
-  NF_MB_OFFSET       // mandelbox_offset (a vector: NAMED3)
+  NF_MB_OFFSET,      // mandelbox_offset (a vector: NAMED3)
+  NF_MB_MIN_R,       // mandelbox_folding_min_radius
+  NF_MB_FIXED_R      // mandelbox_folding_fixed_radius
 };
 
 // formulas that carry orbit state (AuxX) or end orbits by the convergence
@@ -364,6 +366,27 @@ enum PseudoKleinianStdDEX {
 };
 static_assert(PSX_COUNT <= MBR_SLOT_X, "pseudo-Kleinian std DE block exceeds the slot's parameter block");
 
+// cFractalGeneralizedFoldBox (formula/definition/fractal_generalized_fold_box.cpp:31-245):
+// the keyed block, then the main rotation and the fold planes of the chosen
+// polyhedron, derived on the host as sFractal's constructor and
+// RecalculateFractalParams derive them (fractal.cpp:663, 713-818)
+enum GeneralizedFoldBoxX {
+  GFX_TYPE = 0,       // mandelbox_generalized_fold_type
+  GFX_SOLID = 1,      // mandelbox_solid
+  GFX_MELT = 2,       // mandelbox_melt
+  GFX_MB_SCALE = 3,   // mandelbox_scale (named)
+  GFX_MB_MINR = 4,    // mandelbox_folding_min_radius (named)
+  GFX_MB_FIXEDR = 5,  // mandelbox_folding_fixed_radius (named)
+  GFX_MB_OFFSET = 6,  // mandelbox_offset (named, 3)
+  GFX_KEYED_END = 9,
+  GFX_MAIN_ON = 9,    // mandelbox_main_rotation_enabled
+  GFX_MAIN_ROT = 10,  // SetRotation2 of mandelbox_rotation_main (10)
+  GFX_SIDES = 20,     // planes of the polyhedron
+  GFX_NV = 21,        // their unit normals (up to 20 x 3)
+  GFX_COUNT = 81
+};
+static_assert(GFX_COUNT <= MBR_SLOT_X, "generalized fold box block exceeds the slot's parameter block");
+
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
   const char *key;
@@ -645,6 +668,80 @@ constexpr FormulaKey kPseudoKleinianStdDEKeys[] = {
 };
 static_assert(keys_contiguous(kPseudoKleinianStdDEKeys, PSX_COUNT), "pseudo-Kleinian std DE keys and layout disagree");
 
+constexpr FormulaKey kGeneralizedFoldBoxKeys[] = {
+    {"mandelbox_generalized_fold_type", PK_INT, {0, 0, 0}, GFX_TYPE},
+    {"mandelbox_solid", PK_DOUBLE, {1, 0, 0}, GFX_SOLID},
+    {"mandelbox_melt", PK_DOUBLE, {0, 0, 0}, GFX_MELT},
+    {"mandelbox_scale", PK_NAMED, {NF_MB_SCALE, 0, 0}, GFX_MB_SCALE},
+    {"mandelbox_folding_min_radius", PK_NAMED, {NF_MB_MIN_R, 0, 0}, GFX_MB_MINR},
+    {"mandelbox_folding_fixed_radius", PK_NAMED, {NF_MB_FIXED_R, 0, 0}, GFX_MB_FIXEDR},
+    {"mandelbox_offset", PK_NAMED3, {NF_MB_OFFSET, 0, 0}, GFX_MB_OFFSET},
+};
+static_assert(keys_contiguous(kGeneralizedFoldBoxKeys, GFX_KEYED_END), "generalized fold box keys and layout disagree");
+
+// The fold planes of enumGeneralizedFoldBoxType `type` (fractal.h:66-76) into
+// nv (x, y, z per plane), as sFractal's constructor builds them
+// (fractal.cpp:713-818); returns the number of planes.  An unknown type is
+// the tetrahedron, the switch's default.
+inline int generalized_fold_box_planes(int type, double *nv) {
+  const double pi = 3.14159265358979323846;
+  const double s = 1.0 / std::sqrt(3.0);
+  const double tet[8][3] = {{s, s, -s}, {s, -s, s}, {-s, s, s}, {-s, -s, -s},
+                            {s, s, s}, {-s, -s, s}, {-s, s, -s}, {s, -s, -s}};
+  const double cube[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+  int n = 0;
+  auto put = [&](double a, double b, double c) {
+    nv[3 * n] = a;
+    nv[3 * n + 1] = b;
+    nv[3 * n + 2] = c;
+    n++;
+  };
+  const double aa = ((1.0 + std::sqrt(5.0)) / 2.0);
+  const double bb = (1.0 / std::sqrt(aa * aa + 1.0));
+  const double ff = std::sqrt(aa * aa + 1.0 / (aa * aa));
+  const double cc = aa / ff;
+  const double dd = 1.0 / aa / ff;
+  switch (type) {
+    case 1:  // cube
+      for (int i = 0; i < 6; i++) put(cube[i][0], cube[i][1], cube[i][2]);
+      break;
+    case 2:  // octahedron
+      for (int i = 0; i < 8; i++) put(tet[i][0], tet[i][1], tet[i][2]);
+      break;
+    case 3:  // dodecahedron
+      put(0, bb, aa * bb); put(0, bb, -aa * bb); put(0, -bb, aa * bb); put(0, -bb, -aa * bb);
+      put(bb, aa * bb, 0); put(bb, -aa * bb, 0); put(-bb, aa * bb, 0); put(-bb, -aa * bb, 0);
+      put(aa * bb, 0, bb); put(-aa * bb, 0, bb); put(aa * bb, 0, -bb); put(-aa * bb, 0, -bb);
+      break;
+    case 4:  // octahedron and cube
+      for (int i = 0; i < 8; i++) put(tet[i][0], tet[i][1], tet[i][2]);
+      for (int i = 0; i < 6; i++) put(cube[i][0], cube[i][1], cube[i][2]);
+      break;
+    case 5:  // icosahedron
+      for (int i = 0; i < 8; i++) put(tet[i][0], tet[i][1], tet[i][2]);
+      put(0, dd, cc); put(0, dd, -cc); put(0, -dd, cc); put(0, -dd, -cc);
+      put(cc, 0, dd); put(cc, 0, -dd); put(-cc, 0, dd); put(-cc, 0, -dd);
+      put(dd, cc, 0); put(dd, -cc, 0); put(-dd, cc, 0); put(-dd, -cc, 0);
+      break;
+    case 6: {  // hexagonal prism
+      const double tha = pi * 2.0 / 6.0;
+      put(0, 0, 1); put(0, 0, -1);
+      for (int k = 0; k < 6; k++) put(std::cos(tha * k), std::sin(tha * k), 0);
+      break;
+    }
+    case 7: {  // pentagonal prism
+      const double tha5 = pi * 2.0 / 5.0;
+      put(0, 0, 1); put(0, 0, -1);
+      for (int k = 0; k < 5; k++) put(std::cos(tha5 * k), std::sin(tha5 * k), 0);
+      break;
+    }
+    default:  // tetrahedron
+      for (int i = 0; i < 4; i++) put(tet[i][0], tet[i][1], tet[i][2]);
+      break;
+  }
+  return n;
+}
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -667,6 +764,8 @@ inline KeyTable formula_keys(int formula) {
       return {kPseudoKleinianMod4Keys, int(sizeof(kPseudoKleinianMod4Keys) / sizeof(kPseudoKleinianMod4Keys[0]))};
     case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE:
       return {kPseudoKleinianStdDEKeys, int(sizeof(kPseudoKleinianStdDEKeys) / sizeof(kPseudoKleinianStdDEKeys[0]))};
+    case MBR_FORMULA_GENERALIZED_FOLD_BOX:
+      return {kGeneralizedFoldBoxKeys, int(sizeof(kGeneralizedFoldBoxKeys) / sizeof(kGeneralizedFoldBoxKeys[0]))};
     default: return {nullptr, 0};
   }
 }
@@ -722,6 +821,8 @@ inline double named_field(const mbr_fractal &f, int id) {
     case NF_MB_SCALE: return f.mandelbox_scale;
     case NF_ADE_SCALE1: return f.analytic_de_scale1;
     case NF_ADE_OFFSET1: return f.analytic_de_offset1;
+    case NF_MB_MIN_R: return f.mandelbox_folding_min_radius;
+    case NF_MB_FIXED_R: return f.mandelbox_folding_fixed_radius;
     default: return f.transf_scale3;
   }
 }
@@ -769,6 +870,11 @@ inline int pack_keyed(const mbr_fractal &f, double *x) {
       if (!std::isfinite(q.value[c])) return j;
     if (t.keys[i].kind == PK_INT && !(q.value[0] > -2147483648.0 && q.value[0] < 2147483648.0)) return j;
     put_keyed(t.keys[i], q.value, x);
+  }
+  if (f.formula == MBR_FORMULA_GENERALIZED_FOLD_BOX) {  // the derived part of its block
+    x[GFX_MAIN_ON] = f.mandelbox_main_rotation_enabled ? 1.0 : 0.0;
+    keyed_rotation(f.mandelbox_rotation_main, x + GFX_MAIN_ROT);
+    x[GFX_SIDES] = generalized_fold_box_planes(int(x[GFX_TYPE]), x + GFX_NV);
   }
   return -1;
 }

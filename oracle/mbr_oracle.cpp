@@ -73,6 +73,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_ABOX_MOD11: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_abox_mod11.cpp:21-32
     case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian_mod4.cpp:17-28
     case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *fi = {5, 1, 100.0, 6, 0}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
+    case MBR_FORMULA_GENERALIZED_FOLD_BOX: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_generalized_fold_box.cpp:17-29
     default: return false;
   }
 }
@@ -1047,6 +1048,112 @@ inline void formula_pseudo_kleinian_mod4(V4<S> &z, const SlotT<S> &f, S &DE, S &
   if (x[P4X_FLIP_Z] != 0.0) z.z = -z.z;
 }
 
+// cFractalGeneralizedFoldBox::FormulaCode (fractal_generalized_fold_box.cpp:
+// 31-245) without the aux.color terms
+template <class S>
+inline void formula_generalized_fold_box(V4<S> &z, const SlotT<S> &f, S &DE) {
+  using namespace mbr;
+  const double *x = f.x;
+  struct V3 {
+    S x, y, z;
+  };
+  auto dot = [](const V3 &a, const V3 &b) { return a.x * b.x + a.y * b.y + a.z * b.z; };
+  auto nv = [&](int i) { return V3{S(x[GFX_NV + 3 * i]), S(x[GFX_NV + 3 * i + 1]), S(x[GFX_NV + 3 * i + 2])}; };
+  const int sides = int(x[GFX_SIDES]);
+  const double melt = x[GFX_MELT], solid = x[GFX_SOLID];
+  V3 zXYZ{z.x, z.y, z.z};
+  V3 L = zXYZ;
+  S a = 1.0;
+  int side = -1;
+  for (int i = 0; i < sides; i++) {
+    const S b = solid;
+    const S c = dot(L, nv(i));
+    if ((c > 0.0) && ((a * c) > b)) {
+      side = i;
+      a = b / c;
+    }
+  }
+  if (side != -1) {
+    const int side_m = side;
+    const V3 Nm = nv(side_m);
+    const S dm = dot(zXYZ, Nm) - solid;
+    const V3 Xm{zXYZ.x - Nm.x * dm, zXYZ.y - Nm.y * dm, zXYZ.z - Nm.z * dm};
+    L = V3{Xm.x - Nm.x, Xm.y - Nm.y, Xm.z - Nm.z};
+    V3 Y = Nm;
+    a = 1.0;
+    side = -1;
+    for (int i = 0; i < sides; i++) {
+      if (i != side_m) {
+        const S b = solid - dot(Y, nv(i));
+        const S c = dot(L, nv(i));
+        if ((c > 0.0) && ((a * c) > b)) {
+          side = i;
+          a = b / c;
+        }
+      }
+    }
+    V3 target;
+    if (side != -1) {
+      const V3 Xmr{Y.x + L.x * a, Y.y + L.y * a, Y.z + L.z * a};
+      const int side_r = side;
+      const V3 Nr = nv(side_r);
+      V3 Lr{Nm.y * Nr.z - Nm.z * Nr.y, -Nm.x * Nr.z + Nm.z * Nr.x, Nm.x * Nr.y - Nm.y * Nr.x};
+      S a_rmin = (dot(zXYZ, Lr) - dot(Xmr, Lr)) / (dot(Lr, Lr));
+      if (a_rmin < 0.0) {
+        a_rmin = -a_rmin;
+        Lr = V3{Lr.x * -1.0, Lr.y * -1.0, Lr.z * -1.0};
+      }
+      const V3 Xr{Xmr.x + Lr.x * a_rmin, Xmr.y + Lr.y * a_rmin, Xmr.z + Lr.z * a_rmin};
+      L = V3{Xr.x - Xmr.x, Xr.y - Xmr.y, Xr.z - Xmr.z};
+      Y = Xmr;
+      a = 1.0;
+      side = -1;
+      for (int i = 0; i < sides; i++) {
+        if ((i != side_m) && (i != side_r)) {
+          const S b = solid - dot(Y, nv(i));
+          const S c = dot(L, nv(i));
+          if ((c > 0.0) && ((a * c) > b)) {
+            side = i;
+            a = b / c;
+          }
+        }
+      }
+      target = (side != -1) ? V3{Y.x + L.x * a, Y.y + L.y * a, Y.z + L.z * a} : Xr;
+    } else {
+      target = Xm;
+    }
+    const V3 z2X{target.x - zXYZ.x, target.y - zXYZ.y, target.z - zXYZ.z};
+    if (dot(z2X, z2X) > (melt * melt)) {
+      const S mag = sqrt(dot(z2X, z2X));
+      const S k = 2.0 * (mag - melt) / (mag + .00000001);
+      zXYZ = V3{zXYZ.x + z2X.x * k, zXYZ.y + z2X.y * k, zXYZ.z + z2X.z * k};
+    }
+  }
+  const S r2 = dot(zXYZ, zXYZ);
+  z = V4<S>{zXYZ.x, zXYZ.y, zXYZ.z, z.w};
+  z.x = z.x + x[GFX_MB_OFFSET];
+  z.y = z.y + x[GFX_MB_OFFSET + 1];
+  z.z = z.z + x[GFX_MB_OFFSET + 2];
+  z.w = z.w + 0.0;
+  const double mR2 = x[GFX_MB_MINR] * x[GFX_MB_MINR], fR2 = x[GFX_MB_FIXEDR] * x[GFX_MB_FIXEDR];
+  const double factor1 = fR2 / mR2;
+  if (r2 < mR2) {
+    z = z * factor1;
+    DE = DE * factor1;
+  } else if (r2 < fR2) {
+    const S f2 = fR2 / r2;
+    z = z * f2;
+    DE = DE * f2;
+  }
+  z.x = z.x - x[GFX_MB_OFFSET];
+  z.y = z.y - x[GFX_MB_OFFSET + 1];
+  z.z = z.z - x[GFX_MB_OFFSET + 2];
+  z.w = z.w - 0.0;
+  if (x[GFX_MAIN_ON] != 0.0) z = mb_turn(x + GFX_MAIN_ROT + 1, x[GFX_MAIN_ROT] != 0.0, false, z);
+  z = z * x[GFX_MB_SCALE];
+  DE = DE * fabs(x[GFX_MB_SCALE]) + 1.0;
+}
+
 // Benesi's tetrahedral frame turns (abstract_fractal.h:30-32 constants)
 template <class S>
 inline V4<S> benesi_in(const V4<S> &z) {
@@ -1552,6 +1659,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_ABOX_MOD11: formula_abox_mod11(z, f, DE, actualScale, auxC, const_c, i); break;
         case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: formula_pseudo_kleinian_mod4(z, f, DE, pk, posNeg, i); break;
         case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: formula_pseudo_kleinian_std_de(z, f, DE, auxDist, i); break;
+        case MBR_FORMULA_GENERALIZED_FOLD_BOX: formula_generalized_fold_box(z, f, DE); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

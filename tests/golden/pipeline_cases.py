@@ -225,6 +225,17 @@ def _keyed_formula_cases():
     s.fractal[1].formula_iterations = 2
     s.fractal[1].mandelbox_scale = -1.5
     t["hybrid_pksd_box"] = s
+    for gtype in range(8):
+        s = _keyed(abi.FORMULA_GENERALIZED_FOLD_BOX, 25, mandelbox_generalized_fold_type=gtype,
+                   mandelbox_melt=0.05 * (gtype % 3), mandelbox_solid=1.0 - 0.05 * (gtype % 2))
+        s.fractal[0].mandelbox_scale = -1.5 if gtype % 2 else 2.0
+        t[f"gfb_type{gtype}"] = s
+    s = _keyed(abi.FORMULA_GENERALIZED_FOLD_BOX, 25, mandelbox_generalized_fold_type=5)
+    s.fractal[0].mandelbox_main_rotation_enabled = 1
+    s.fractal[0].mandelbox_rotation_main[:] = [5.0, -10.0, 20.0]
+    s.fractal[0].mandelbox_offset[:] = [0.1, 0.0, 0.0]
+    s.fractal[0].mandelbox_folding_min_radius = 0.4
+    t["gfb_rotated"] = s
     t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
                                  transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t

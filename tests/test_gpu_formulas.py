@@ -201,7 +201,7 @@ KEYED_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk
                "menger_mod1_box_offset_blend", "hybrid_menger_mod1_bfbp2", "bfbp2v2_default", "bfbp2v2_vary",
                "bfbp2v2_vary_m", "abox_mod11_default", "abox_mod11_folds", "abox_mod11_curve_c",
                "hybrid_abox_mod11_bulb", "pkm4_default", "pkm4_sphere_box", "pkm4_fold_n", "pksd_default",
-               "pksd_benesi", "pksd_folds", "hybrid_pksd_box"]
+               "pksd_benesi", "pksd_folds", "hybrid_pksd_box"] + [f"gfb_type{k}" for k in range(8)] + ["gfb_rotated"]
 
 
 @pytest.mark.parametrize("case", KEYED_CASES)
