@@ -1012,6 +1012,83 @@ __device__ __noinline__ void f_generalized_fold_box(V4<T> &z, T &DE, const DevSl
   DE = DE * T(fabs(x[GFX_MB_SCALE])) + T(1.0);
 }
 
+// cFractalMandelbulbPupuku::FormulaCode (fractal_mandelbulb_pupuku.cpp:29-144):
+// a Mandelbulb with optional pre-folds, acos latitude, sin/cos swap, polar
+// scalings and a y fold; dist is aux.dist (set when its own DE block is on)
+template <class T>
+__device__ __noinline__ void f_mandelbulb_pupuku(V4<T> &z, T r, T &DE, T &dist, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (x[PPX_P_ON] != 0.0 && i >= int(x[PPX_START_P]) && i < int(x[PPX_STOP_P])) {  // :34-45
+    if (x[PPX_CX] != 0.0) z.x = m_abs(z.x);
+    if (x[PPX_CY] != 0.0) z.y = m_abs(z.y);
+    if (x[PPX_CZ] != 0.0) z.z = m_abs(z.z);
+    z.x = z.x + T(x[PPX_OFFSET_A000]);
+    z.y = z.y + T(x[PPX_OFFSET_A000 + 1]);
+    z.z = z.z + T(x[PPX_OFFSET_A000 + 2]);
+    if (x[PPX_T_ON] != 0.0) r = len4<T, true>(z);
+  }
+  T t = (x[PPX_SW] == 0.0) ? m_asin(T(z.z / r)) : m_acos(T(z.z / r));
+  const T power = T(x[PPX_POWER]);
+  const T th = (t + T(x[PPX_BETA])) * power * T(x[PPX_SCALE_A1]);
+  T ph = (m_atan2(z.y, z.x) + T(x[PPX_ALPHA])) * power * T(x[PPX_SCALE_B1]);
+  T rp = m_pow(r, T(x[PPX_POWER] - x[PPX_OFFSET1]));
+  T sth, cth;
+  m_sincos(th, &sth, &cth);
+  if (x[PPX_X_ON] != 0.0 && i >= int(x[PPX_START_X]) && i < int(x[PPX_STOP_X])) {  // :53-57
+    if (cth < T(0.0)) ph = ph + T(3.14159265358979323846);
+  }
+  DE = rp * DE * m_abs(power) + T(x[PPX_ADE_OFFSET1]);
+  rp = rp * r;
+  T zth;
+  if (x[PPX_D_ON] == 0.0) {
+    t = cth;
+    zth = sth;
+  } else {
+    t = sth;
+    zth = cth;
+  }
+  T sph, cph;
+  m_sincos(ph, &sph, &cph);
+  if (x[PPX_B_ON] != 0.0 && i >= int(x[PPX_START_B]) && i < int(x[PPX_STOP_B]))
+    z.x = (T(1.0) + (t - T(1.0)) * T(x[PPX_SCALE_B0])) * cph;
+  else
+    z.x = t * cph;
+  if (x[PPX_A_ON] != 0.0 && i >= int(x[PPX_START_A]) && i < int(x[PPX_STOP_A]))
+    z.y = (T(1.0) + (t - T(1.0)) * T(x[PPX_SCALE_A0])) * sph;
+  else
+    z.y = t * sph;
+  z.z = zth;
+  z.x = z.x * rp;
+  z.y = z.y * rp;
+  z.z = z.z * rp;
+  z.w = z.w * rp;
+  if (x[PPX_BZ] != 0.0) {  // min(z.y, offset0 - z.y)
+    const T o = T(x[PPX_OFFSET0]) - z.y;
+    if (o < z.y) z.y = o;
+  }
+  z.x = z.x + T(x[PPX_OFFSET000]);
+  z.y = z.y + T(x[PPX_OFFSET000 + 1]);
+  z.z = z.z + T(x[PPX_OFFSET000 + 2]);
+  if (i >= int(x[PPX_START_S]) && i < int(x[PPX_STOP_S])) {
+    const T c1 = T(x[PPX_SCALE_C1]);
+    z.x = z.x * c1;
+    z.y = z.y * c1;
+    z.z = z.z * c1;
+    z.w = z.w * c1;
+    DE = DE * T(fabs(x[PPX_SCALE_C1]));
+  }
+  if (x[PPX_ADE_ON] != 0.0) DE = DE * T(x[PPX_ADE_SCALE1]) + T(x[PPX_ADE_OFFSET0]);
+  if (x[PPX_C_ON] != 0.0) {  // :120-143
+    T de0 = len4<T, true>(z);
+    de0 = (de0 > T(1.0)) ? T(T(0.5) * m_log(de0) * de0 / DE) : T(0.0);
+    if (x[PPX_E_ON] == 0.0 || !(i >= int(x[PPX_START_E]) && i < int(x[PPX_STOP_E]))) {
+      dist = de0;
+    } else if (de0 < dist) {
+      dist = de0;
+    }
+  }
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -1140,6 +1217,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: f_pseudo_kleinian_mod4<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: f_pseudo_kleinian_std_de<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_GENERALIZED_FOLD_BOX: f_generalized_fold_box<T>(z, DE, s); break;
+      case MBR_FORMULA_MANDELBULB_PUPUKU: f_mandelbulb_pupuku<T>(z, r, DE, ax.dist, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;

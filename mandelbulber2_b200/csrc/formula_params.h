@@ -38,7 +38,10 @@ enum NamedField {
   NF_SCALE3,         // transf_scale3 (transf_scale_3)
   NF_MB_OFFSET,      // mandelbox_offset (a vector: NAMED3)
   NF_MB_MIN_R,       // mandelbox_folding_min_radius
-  NF_MB_FIXED_R      // mandelbox_folding_fixed_radius
+  NF_MB_FIXED_R,     // mandelbox_folding_fixed_radius
+  NF_POWER,          // bulb_power (power)
+  NF_ALPHA,          // bulb_alpha_angle_offset, in radians (fractal.cpp:677)
+  NF_BETA            // bulb_beta_angle_offset, in radians (fractal.cpp:678)
 };
 
 // formulas that carry orbit state (AuxX) or end orbits by the convergence
@@ -46,7 +49,7 @@ enum NamedField {
 inline MBR_HD bool keyed_formula_has_state(int formula) {
   return formula == MBR_FORMULA_PSEUDO_KLEINIAN || formula == MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 ||
          formula == MBR_FORMULA_ABOX_MOD11 || formula == MBR_FORMULA_PSEUDO_KLEINIAN_MOD4 ||
-         formula == MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE;
+         formula == MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE || formula == MBR_FORMULA_MANDELBULB_PUPUKU;
 }
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
@@ -386,6 +389,52 @@ enum GeneralizedFoldBoxX {
   GFX_COUNT = 81
 };
 static_assert(GFX_COUNT <= MBR_SLOT_X, "generalized fold box block exceeds the slot's parameter block");
+
+// cFractalMandelbulbPupuku (formula/definition/fractal_mandelbulb_pupuku.cpp:29-144)
+enum MandelbulbPupukuX {
+  PPX_P_ON = 0,        // transf_function_enabledP_false
+  PPX_START_P = 1,     // transf_start_iterations_P
+  PPX_STOP_P = 2,      // transf_stop_iterations_P
+  PPX_CX = 3,          // transf_function_enabledCx_false
+  PPX_CY = 4,          // transf_function_enabledCy_false
+  PPX_CZ = 5,          // transf_function_enabledCz_false
+  PPX_OFFSET_A000 = 6, // transf_offsetA_000 (3)
+  PPX_T_ON = 9,        // transf_function_enabledT_false
+  PPX_SW = 10,          // transf_function_enabledSw_false
+  PPX_SCALE_A1 = 11,    // transf_scaleA_1
+  PPX_SCALE_B1 = 12,    // transf_scaleB_1
+  PPX_OFFSET1 = 13,     // transf_offset_1
+  PPX_X_ON = 14,        // transf_function_enabledX_false
+  PPX_START_X = 15,     // transf_start_iterations_X
+  PPX_STOP_X = 16,      // transf_stop_iterations_X
+  PPX_D_ON = 17,        // transf_function_enabledD_false
+  PPX_B_ON = 18,        // transf_function_enabledB_false
+  PPX_START_B = 19,     // transf_start_iterations_B
+  PPX_STOP_B = 20,      // transf_stop_iterations_B
+  PPX_SCALE_B0 = 21,    // transf_scaleB_0
+  PPX_A_ON = 22,        // transf_function_enabledA_false
+  PPX_START_A = 23,     // transf_start_iterations_A
+  PPX_STOP_A = 24,      // transf_stop_iterations_A
+  PPX_SCALE_A0 = 25,    // transf_scaleA_0
+  PPX_BZ = 26,          // transf_function_enabledBz_false
+  PPX_OFFSET0 = 27,     // transf_offset_0
+  PPX_OFFSET000 = 28,   // transf_offset_000 (3)
+  PPX_START_S = 31,     // transf_start_iterations_S
+  PPX_STOP_S = 32,      // transf_stop_iterations_S
+  PPX_SCALE_C1 = 33,    // transf_scaleC_1
+  PPX_ADE_ON = 34,      // analyticDE_enabled_false
+  PPX_ADE_OFFSET0 = 35, // analyticDE_offset_0
+  PPX_C_ON = 36,        // transf_function_enabledC_false
+  PPX_E_ON = 37,        // transf_function_enabledE_false
+  PPX_START_E = 38,     // transf_start_iterations_E
+  PPX_STOP_E = 39,      // transf_stop_iterations_E
+  PPX_POWER = 40,       // power (named)
+  PPX_ALPHA = 41,       // alpha_angle_offset (named)
+  PPX_BETA = 42,        // beta_angle_offset (named)
+  PPX_ADE_SCALE1 = 43,  // analyticDE_scale_1 (named)
+  PPX_ADE_OFFSET1 = 44, // analyticDE_offset_1 (named)
+  PPX_COUNT = 45
+};
 
 #ifndef __CUDA_ARCH__
 struct FormulaKey {
@@ -742,6 +791,51 @@ inline int generalized_fold_box_planes(int type, double *nv) {
   return n;
 }
 
+constexpr FormulaKey kMandelbulbPupukuKeys[] = {
+    {"transf_function_enabledP_false", PK_BOOL, {0,0,0}, PPX_P_ON},
+    {"transf_start_iterations_P", PK_INT, {0,0,0}, PPX_START_P},
+    {"transf_stop_iterations_P", PK_INT, {250,0,0}, PPX_STOP_P},
+    {"transf_function_enabledCx_false", PK_BOOL, {0,0,0}, PPX_CX},
+    {"transf_function_enabledCy_false", PK_BOOL, {0,0,0}, PPX_CY},
+    {"transf_function_enabledCz_false", PK_BOOL, {0,0,0}, PPX_CZ},
+    {"transf_offsetA_000", PK_VEC3, {0,0,0}, PPX_OFFSET_A000},
+    {"transf_function_enabledT_false", PK_BOOL, {0,0,0}, PPX_T_ON},
+    {"transf_function_enabledSw_false", PK_BOOL, {0,0,0}, PPX_SW},
+    {"transf_scaleA_1", PK_DOUBLE, {1,0,0}, PPX_SCALE_A1},
+    {"transf_scaleB_1", PK_DOUBLE, {1,0,0}, PPX_SCALE_B1},
+    {"transf_offset_1", PK_DOUBLE, {1,0,0}, PPX_OFFSET1},
+    {"transf_function_enabledX_false", PK_BOOL, {0,0,0}, PPX_X_ON},
+    {"transf_start_iterations_X", PK_INT, {0,0,0}, PPX_START_X},
+    {"transf_stop_iterations_X", PK_INT, {250,0,0}, PPX_STOP_X},
+    {"transf_function_enabledD_false", PK_BOOL, {0,0,0}, PPX_D_ON},
+    {"transf_function_enabledB_false", PK_BOOL, {0,0,0}, PPX_B_ON},
+    {"transf_start_iterations_B", PK_INT, {0,0,0}, PPX_START_B},
+    {"transf_stop_iterations_B", PK_INT, {250,0,0}, PPX_STOP_B},
+    {"transf_scaleB_0", PK_DOUBLE, {0,0,0}, PPX_SCALE_B0},
+    {"transf_function_enabledA_false", PK_BOOL, {0,0,0}, PPX_A_ON},
+    {"transf_start_iterations_A", PK_INT, {0,0,0}, PPX_START_A},
+    {"transf_stop_iterations_A", PK_INT, {250,0,0}, PPX_STOP_A},
+    {"transf_scaleA_0", PK_DOUBLE, {0,0,0}, PPX_SCALE_A0},
+    {"transf_function_enabledBz_false", PK_BOOL, {0,0,0}, PPX_BZ},
+    {"transf_offset_0", PK_DOUBLE, {0,0,0}, PPX_OFFSET0},
+    {"transf_offset_000", PK_VEC3, {0,0,0}, PPX_OFFSET000},
+    {"transf_start_iterations_S", PK_INT, {0,0,0}, PPX_START_S},
+    {"transf_stop_iterations_S", PK_INT, {250,0,0}, PPX_STOP_S},
+    {"transf_scaleC_1", PK_DOUBLE, {1,0,0}, PPX_SCALE_C1},
+    {"analyticDE_enabled_false", PK_BOOL, {0,0,0}, PPX_ADE_ON},
+    {"analyticDE_offset_0", PK_DOUBLE, {0,0,0}, PPX_ADE_OFFSET0},
+    {"transf_function_enabledC_false", PK_BOOL, {0,0,0}, PPX_C_ON},
+    {"transf_function_enabledE_false", PK_BOOL, {0,0,0}, PPX_E_ON},
+    {"transf_start_iterations_E", PK_INT, {0,0,0}, PPX_START_E},
+    {"transf_stop_iterations_E", PK_INT, {250,0,0}, PPX_STOP_E},
+    {"power", PK_NAMED, {NF_POWER,0,0}, PPX_POWER},
+    {"alpha_angle_offset", PK_NAMED, {NF_ALPHA,0,0}, PPX_ALPHA},
+    {"beta_angle_offset", PK_NAMED, {NF_BETA,0,0}, PPX_BETA},
+    {"analyticDE_scale_1", PK_NAMED, {NF_ADE_SCALE1,0,0}, PPX_ADE_SCALE1},
+    {"analyticDE_offset_1", PK_NAMED, {NF_ADE_OFFSET1,0,0}, PPX_ADE_OFFSET1},
+};
+static_assert(keys_contiguous(kMandelbulbPupukuKeys, PPX_COUNT), "Mandelbulb Pupuku keys and layout disagree");
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -766,6 +860,8 @@ inline KeyTable formula_keys(int formula) {
       return {kPseudoKleinianStdDEKeys, int(sizeof(kPseudoKleinianStdDEKeys) / sizeof(kPseudoKleinianStdDEKeys[0]))};
     case MBR_FORMULA_GENERALIZED_FOLD_BOX:
       return {kGeneralizedFoldBoxKeys, int(sizeof(kGeneralizedFoldBoxKeys) / sizeof(kGeneralizedFoldBoxKeys[0]))};
+    case MBR_FORMULA_MANDELBULB_PUPUKU:
+      return {kMandelbulbPupukuKeys, int(sizeof(kMandelbulbPupukuKeys) / sizeof(kMandelbulbPupukuKeys[0]))};
     default: return {nullptr, 0};
   }
 }
@@ -823,6 +919,9 @@ inline double named_field(const mbr_fractal &f, int id) {
     case NF_ADE_OFFSET1: return f.analytic_de_offset1;
     case NF_MB_MIN_R: return f.mandelbox_folding_min_radius;
     case NF_MB_FIXED_R: return f.mandelbox_folding_fixed_radius;
+    case NF_POWER: return f.bulb_power;
+    case NF_ALPHA: return f.bulb_alpha_angle_offset * 0.01745329251994329576923690768489;
+    case NF_BETA: return f.bulb_beta_angle_offset * 0.01745329251994329576923690768489;
     default: return f.transf_scale3;
   }
 }

@@ -74,6 +74,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: *fi = {3, 1, 100.0, 4, 0}; return true;  // fractal_pseudo_kleinian_mod4.cpp:17-28
     case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *fi = {5, 1, 100.0, 6, 0}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
     case MBR_FORMULA_GENERALIZED_FOLD_BOX: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_generalized_fold_box.cpp:17-29
+    case MBR_FORMULA_MANDELBULB_PUPUKU: *fi = {2, 0, 10.0, 2, 0}; return true;  // fractal_mandelbulb_pupuku.cpp:16-27
     default: return false;
   }
 }
@@ -1154,6 +1155,74 @@ inline void formula_generalized_fold_box(V4<S> &z, const SlotT<S> &f, S &DE) {
   DE = DE * fabs(x[GFX_MB_SCALE]) + 1.0;
 }
 
+// cFractalMandelbulbPupuku::FormulaCode (fractal_mandelbulb_pupuku.cpp:29-144);
+// r is aux.r (the formula may replace it), dist is aux.dist
+template <class S>
+inline void formula_mandelbulb_pupuku(V4<S> &z, const SlotT<S> &f, S r, S &DE, S &dist, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  S t;
+  if (x[PPX_P_ON] != 0.0 && i >= int(x[PPX_START_P]) && i < int(x[PPX_STOP_P])) {
+    if (x[PPX_CX] != 0.0) z.x = fabs(z.x);
+    if (x[PPX_CY] != 0.0) z.y = fabs(z.y);
+    if (x[PPX_CZ] != 0.0) z.z = fabs(z.z);
+    z.x = z.x + x[PPX_OFFSET_A000];
+    z.y = z.y + x[PPX_OFFSET_A000 + 1];
+    z.z = z.z + x[PPX_OFFSET_A000 + 2];
+    z.w = z.w + 0.0;
+    if (x[PPX_T_ON] != 0.0) r = len4(z);
+  }
+  if (x[PPX_SW] == 0.0) t = asin(z.z / r);
+  else t = acos(z.z / r);
+  const S th = (t + x[PPX_BETA]) * x[PPX_POWER] * x[PPX_SCALE_A1];
+  S ph = (atan2(z.y, z.x) + x[PPX_ALPHA]) * x[PPX_POWER] * x[PPX_SCALE_B1];
+  S rp = pow(r, S(x[PPX_POWER] - x[PPX_OFFSET1]));
+  if (x[PPX_X_ON] != 0.0 && i >= int(x[PPX_START_X]) && i < int(x[PPX_STOP_X])) {
+    if (cos(th) < 0.0) ph = ph + M_PI;
+  }
+  DE = rp * DE * fabs(x[PPX_POWER]) + x[PPX_ADE_OFFSET1];
+  rp = rp * r;
+  S zth;
+  if (x[PPX_D_ON] == 0.0) {
+    t = cos(th);
+    zth = sin(th);
+  } else {
+    t = sin(th);
+    zth = cos(th);
+  }
+  if (x[PPX_B_ON] != 0.0 && i >= int(x[PPX_START_B]) && i < int(x[PPX_STOP_B]))
+    z.x = (1.0 + (t - 1.0) * x[PPX_SCALE_B0]) * cos(ph);
+  else
+    z.x = t * cos(ph);
+  if (x[PPX_A_ON] != 0.0 && i >= int(x[PPX_START_A]) && i < int(x[PPX_STOP_A]))
+    z.y = (1.0 + (t - 1.0) * x[PPX_SCALE_A0]) * sin(ph);
+  else
+    z.y = t * sin(ph);
+  z.z = zth;
+  z = z * rp;
+  if (x[PPX_BZ] != 0.0) z.y = std::min(z.y, S(x[PPX_OFFSET0] - z.y));
+  z.x = z.x + x[PPX_OFFSET000];
+  z.y = z.y + x[PPX_OFFSET000 + 1];
+  z.z = z.z + x[PPX_OFFSET000 + 2];
+  z.w = z.w + 0.0;
+  if (i >= int(x[PPX_START_S]) && i < int(x[PPX_STOP_S])) {
+    z = z * x[PPX_SCALE_C1];
+    DE = DE * fabs(x[PPX_SCALE_C1]);
+  }
+  if (x[PPX_ADE_ON] != 0.0) DE = DE * x[PPX_ADE_SCALE1] + x[PPX_ADE_OFFSET0];
+  if (x[PPX_C_ON] != 0.0) {
+    S de0 = len4(z);
+    if (de0 > 1.0) de0 = 0.5 * log(de0) * de0 / DE;
+    else de0 = 0.0;
+    if (x[PPX_E_ON] == 0.0) {
+      dist = de0;
+    } else {
+      if (i >= int(x[PPX_START_E]) && i < int(x[PPX_STOP_E])) dist = std::min(dist, de0);
+      else dist = de0;
+    }
+  }
+}
+
 // Benesi's tetrahedral frame turns (abstract_fractal.h:30-32 constants)
 template <class S>
 inline V4<S> benesi_in(const V4<S> &z) {
@@ -1660,6 +1729,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_PSEUDO_KLEINIAN_MOD4: formula_pseudo_kleinian_mod4(z, f, DE, pk, posNeg, i); break;
         case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: formula_pseudo_kleinian_std_de(z, f, DE, auxDist, i); break;
         case MBR_FORMULA_GENERALIZED_FOLD_BOX: formula_generalized_fold_box(z, f, DE); break;
+        case MBR_FORMULA_MANDELBULB_PUPUKU: formula_mandelbulb_pupuku(z, f, r, DE, auxDist, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

@@ -236,6 +236,22 @@ def _keyed_formula_cases():
     s.fractal[0].mandelbox_offset[:] = [0.1, 0.0, 0.0]
     s.fractal[0].mandelbox_folding_min_radius = 0.4
     t["gfb_rotated"] = s
+    s = _keyed(abi.FORMULA_MANDELBULB_PUPUKU, 30)
+    s.fractal[0].bulb_power = 6.0
+    t["pupuku_default"] = s
+    s = _keyed(abi.FORMULA_MANDELBULB_PUPUKU, 30, transf_function_enabledP_false=1, transf_function_enabledCx_false=1,
+               transf_offsetA_000=[0.1, 0.0, 0.0], transf_function_enabledT_false=1, transf_function_enabledSw_false=1,
+               transf_scaleA_1=1.1, transf_function_enabledX_false=1, transf_function_enabledB_false=1,
+               transf_scaleB_0=0.3, transf_function_enabledBz_false=1, transf_offset_0=0.2,
+               transf_scaleC_1=0.95, analyticDE_enabled_false=1, analyticDE_offset_0=0.1)
+    s.fractal[0].bulb_power = 5.0
+    s.fractal[0].bulb_alpha_angle_offset = 10.0
+    t["pupuku_options"] = s
+    s = _keyed(abi.FORMULA_MANDELBULB_PUPUKU, 30, transf_function_enabledC_false=1, transf_function_enabledE_false=1,
+               transf_start_iterations_E=2, transf_function_enabledD_false=1)
+    s.fractal[0].bulb_power = 4.0
+    s.delta_de_function = abi.DE_CUSTOM
+    t["pupuku_custom_de"] = s
     t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
                                  transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t
