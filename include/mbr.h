@@ -71,6 +71,7 @@ typedef enum mbr_formula {
   MBR_FORMULA_MENGER_MOD1 = 61,       /* formula/definition/fractal_menger_mod1.cpp:29-103 */
   MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 = 125, /* formula/definition/fractal_box_fold_bulb_pow2_v2.cpp:29-146 */
   MBR_FORMULA_MANDELBULB_PUPUKU = 266, /* formula/definition/fractal_mandelbulb_pupuku.cpp:29-144 */
+  MBR_FORMULA_DIFS_HEXTGRID2 = 608,   /* formula/definition/fractal_difs_hextgrid2.cpp:30-138 (custom DE) */
   MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE = 101, /* formula/definition/fractal_pseudo_kleinian_std_de.cpp:29-215 (custom DE) */
   MBR_FORMULA_PSEUDO_KLEINIAN = 103,  /* formula/definition/fractal_pseudo_kleinian.cpp:30-202 */
   MBR_FORMULA_ABOX_MOD11 = 119,       /* formula/definition/fractal_abox_mod11.cpp:34-250 */

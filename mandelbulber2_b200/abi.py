@@ -32,6 +32,7 @@ FORMULA_QUATERNION, FORMULA_AEXION = 5, 19
 FORMULA_BOX_FOLD_BULB_POW2, FORMULA_MENGER_MOD1, FORMULA_PSEUDO_KLEINIAN = 16, 61, 103
 FORMULA_BOX_FOLD_BULB_POW2_V2, FORMULA_ABOX_MOD11, FORMULA_PSEUDO_KLEINIAN_MOD4 = 125, 119, 217
 FORMULA_PSEUDO_KLEINIAN_STD_DE, FORMULA_GENERALIZED_FOLD_BOX, FORMULA_MANDELBULB_PUPUKU = 101, 37, 266
+FORMULA_DIFS_HEXTGRID2 = 608
 MBR_MAX_FORMULA_PARAMS = 48
 MBR_PARAM_KEY_LEN = 48
 PROJECTION_THREE_POINT, PROJECTION_FISH_EYE, PROJECTION_EQUIRECTANGULAR, PROJECTION_FISH_EYE_CUT = range(4)

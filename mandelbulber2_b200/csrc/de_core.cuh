@@ -1089,6 +1089,73 @@ __device__ __noinline__ void f_mandelbulb_pupuku(V4<T> &z, T r, T &DE, T &dist, 
   }
 }
 
+// cFractalDIFSHextgrid2::FormulaCode (fractal_difs_hextgrid2.cpp:30-138), the
+// aux.color terms left out: a hexagonal grid distance into aux.dist (a
+// custom-DE formula) after sphere inversion, a tiling fold, a varying scale
+// (scaleA = aux.actualScaleA), offset and rotation
+template <class T>
+__device__ __noinline__ void f_difs_hextgrid2(V4<T> &z, T &DE, AuxX<T> &ax, const DevSlot &s, int i) {
+  const double *x = s.x;
+  if (x[HGX_SPH_INV] != 0.0 && i >= int(x[HGX_START_X]) && i < int(x[HGX_STOP_1])) {  // :35-45
+    z.x = z.x + T(x[HGX_OFFSET000]);
+    z.y = z.y + T(x[HGX_OFFSET000 + 1]);
+    z.z = z.z + T(x[HGX_OFFSET000 + 2]);
+    const T rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    const T q = T(x[HGX_SCALE_G1]) / rr;
+    z.x = z.x * q;
+    z.y = z.y * q;
+    z.z = z.z * q;
+    z.w = z.w * q;
+    DE = DE * (T(x[HGX_SCALE_G1]) / rr);
+    z.x = z.x + T(x[HGX_ADD000] - x[HGX_OFFSET000]);
+    z.y = z.y + T(x[HGX_ADD000 + 1] - x[HGX_OFFSET000 + 1]);
+    z.z = z.z + T(x[HGX_ADD000 + 2] - x[HGX_OFFSET000 + 2]);
+    const T a1 = T(x[HGX_SCALE_A1]);
+    z.x = z.x * a1;
+    z.y = z.y * a1;
+    z.z = z.z * a1;
+    z.w = z.w * a1;
+    DE = DE * a1;
+  }
+  if (x[HGX_C_ON] != 0.0 && i >= int(x[HGX_START_C]) && i < int(x[HGX_STOP_C1])) {  // :46-54
+    T tp = T(x[HGX_OFFSET2]);
+    z.x = T(fmod(m_abs(z.x) + tp, T(T(2.0) * tp))) - tp;
+    tp = T(x[HGX_OFFSETA2]);
+    z.y = T(fmod(m_abs(z.y) + tp, T(T(2.0) * tp))) - tp;
+  }
+  if (i >= int(x[HGX_START_S]) && i < int(x[HGX_STOP_S])) {  // scale :56-71
+    const T useScale = ax.scaleA + T(x[HGX_SCALE2]);
+    z.x = z.x * useScale;
+    z.y = z.y * useScale;
+    z.z = z.z * useScale;
+    z.w = z.w * useScale;
+    DE = DE * m_abs(useScale);
+    if (x[HGX_K_ON] != 0.0 && i >= int(x[HGX_START_K]) && i < int(x[HGX_STOP_K])) {
+      const T vary = T(x[HGX_SCALE_VARY]) * (m_abs(ax.scaleA) - T(x[HGX_SCALE_C1]));
+      ax.scaleA = ax.scaleA - vary;
+    }
+  }
+  z.x = z.x + T(x[HGX_OFFSET001]);  // :73
+  z.y = z.y + T(x[HGX_OFFSET001 + 1]);
+  z.z = z.z + T(x[HGX_OFFSET001 + 2]);
+  if (x[HGX_R_ON] != 0.0 && i >= int(x[HGX_START_R]) && i < int(x[HGX_STOP_R]) && x[HGX_ROT] == 0.0)
+    z = mb_turn<T>(x + HGX_ROT + 1, false, z);  // :75-80
+  if (i >= int(x[HGX_START]) && i < int(x[HGX_STOP])) {  // the grid :84-105
+    const T size = T(x[HGX_SCALE1]), cosPi6 = T(x[HGX_COS6]);
+    const T zx = z.x, zy = z.y, zz = z.z / T(x[HGX_SCALE_F1]);
+    const T yFloor = m_abs(T(zy - size * T(floor(zy / size + T(0.5)))));
+    const T xFloor =
+        m_abs(T(zx - size * T(1.5) / cosPi6 * T(floor(zx / size / T(1.5) * cosPi6 + T(0.5)))));
+    const T gridMax = smax(yFloor, T(xFloor * cosPi6 + yFloor * T(x[HGX_SIN6])));
+    const T gm = gridMax - size * T(0.5);
+    const T gridMin = (yFloor < gm) ? yFloor : gm;  // std::min
+    T hexD = (x[HGX_J_ON] == 0.0) ? m_sqrt(T(gridMin * gridMin + zz * zz)) : smax(m_abs(gridMin), m_abs(zz));
+    hexD = hexD - T(x[HGX_OFFSET0005]);
+    const T d = hexD / (DE + T(1.0));
+    if (d < ax.dist) ax.dist = d;
+  }
+}
+
 // cFractalMengerMod1::FormulaCode (fractal_menger_mod1.cpp:29-103), the
 // aux.color terms left out
 template <class T>
@@ -1218,6 +1285,7 @@ __device__ __forceinline__ void formula_dispatch(int formula, V4<T> &z, T r, T &
       case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: f_pseudo_kleinian_std_de<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_GENERALIZED_FOLD_BOX: f_generalized_fold_box<T>(z, DE, s); break;
       case MBR_FORMULA_MANDELBULB_PUPUKU: f_mandelbulb_pupuku<T>(z, r, DE, ax.dist, s, i); break;
+      case MBR_FORMULA_DIFS_HEXTGRID2: f_difs_hextgrid2<T>(z, DE, ax, s, i); break;
       case MBR_FORMULA_BOX_FOLD_BULB_POW2: f_box_fold_bulb_pow2<T>(z, r, DE, s); break;
       case MBR_FORMULA_MENGER_MOD1: f_menger_mod1<T>(z, DE, s, i); break;
       case MBR_FORMULA_QUATERNION: f_quaternion<T>(z, r, DE); break;

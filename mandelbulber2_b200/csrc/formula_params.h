@@ -49,7 +49,8 @@ enum NamedField {
 inline MBR_HD bool keyed_formula_has_state(int formula) {
   return formula == MBR_FORMULA_PSEUDO_KLEINIAN || formula == MBR_FORMULA_BOX_FOLD_BULB_POW2_V2 ||
          formula == MBR_FORMULA_ABOX_MOD11 || formula == MBR_FORMULA_PSEUDO_KLEINIAN_MOD4 ||
-         formula == MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE || formula == MBR_FORMULA_MANDELBULB_PUPUKU;
+         formula == MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE || formula == MBR_FORMULA_MANDELBULB_PUPUKU ||
+         formula == MBR_FORMULA_DIFS_HEXTGRID2;
 }
 
 // cFractalPseudoKleinian (formula/definition/fractal_pseudo_kleinian.cpp:
@@ -434,6 +435,45 @@ enum MandelbulbPupukuX {
   PPX_ADE_SCALE1 = 43,  // analyticDE_scale_1 (named)
   PPX_ADE_OFFSET1 = 44, // analyticDE_offset_1 (named)
   PPX_COUNT = 45
+};
+
+// cFractalDIFSHextgrid2 (formula/definition/fractal_difs_hextgrid2.cpp:30-138)
+enum DIFSHextgrid2X {
+  HGX_SPH_INV = 0,     // transf_sphere_inversion_enabled_false
+  HGX_START_X = 1,     // transf_start_iterations_X
+  HGX_STOP_1 = 2,      // transf_stop_iterations_1
+  HGX_OFFSET000 = 3,   // transf_offset_000 (3)
+  HGX_SCALE_G1 = 6,    // transf_scaleG_1
+  HGX_ADD000 = 7,      // transf_addition_constant (3)
+  HGX_SCALE_A1 = 10,    // transf_scaleA_1
+  HGX_C_ON = 11,        // transf_function_enabledC_false
+  HGX_START_C = 12,     // transf_start_iterations_C
+  HGX_STOP_C1 = 13,     // transf_stop_iterations_C1
+  HGX_OFFSET2 = 14,     // transf_offset_2
+  HGX_OFFSETA2 = 15,    // transf_offsetA_2
+  HGX_START_S = 16,     // transf_start_iterations_S
+  HGX_STOP_S = 17,      // transf_stop_iterations_S
+  HGX_SCALE2 = 18,      // transf_scale_2
+  HGX_K_ON = 19,        // transf_function_enabledK_false
+  HGX_START_K = 20,     // transf_start_iterations_K
+  HGX_STOP_K = 21,      // transf_stop_iterations_K
+  HGX_SCALE_VARY = 22,  // transf_scale_vary_0
+  HGX_SCALE_C1 = 23,    // transf_scaleC_1
+  HGX_OFFSET001 = 24,   // transf_offset_001 (3)
+  HGX_R_ON = 27,        // transf_function_enabledR_false
+  HGX_START_R = 28,     // transf_start_iterations_R
+  HGX_STOP_R = 29,      // transf_stop_iterations_R
+  HGX_ROT = 30,         // transf_rotation (10)
+  HGX_START = 40,       // transf_start_iterations
+  HGX_STOP = 41,        // transf_stop_iterations
+  HGX_SCALE1 = 42,      // transf_scale_1
+  HGX_SCALE_F1 = 43,    // transf_scaleF_1
+  HGX_J_ON = 44,        // transf_function_enabledJ_false
+  HGX_OFFSET0005 = 45,  // transf_offset_0005
+  HGX_KEYED_END = 46,
+  HGX_COS6 = 46,          // cos(pi / 6), host libm
+  HGX_SIN6 = 47,          // sin(pi / 6), host libm
+  HGX_COUNT = 48
 };
 
 #ifndef __CUDA_ARCH__
@@ -836,6 +876,41 @@ constexpr FormulaKey kMandelbulbPupukuKeys[] = {
 };
 static_assert(keys_contiguous(kMandelbulbPupukuKeys, PPX_COUNT), "Mandelbulb Pupuku keys and layout disagree");
 
+constexpr FormulaKey kDIFSHextgrid2Keys[] = {
+    {"transf_sphere_inversion_enabled_false", PK_BOOL, {0,0,0}, HGX_SPH_INV},
+    {"transf_start_iterations_X", PK_INT, {0,0,0}, HGX_START_X},
+    {"transf_stop_iterations_1", PK_INT, {1,0,0}, HGX_STOP_1},
+    {"transf_offset_000", PK_VEC3, {0,0,0}, HGX_OFFSET000},
+    {"transf_scaleG_1", PK_DOUBLE, {1,0,0}, HGX_SCALE_G1},
+    {"transf_addition_constant", PK_VEC3, {0,0,0}, HGX_ADD000},
+    {"transf_scaleA_1", PK_DOUBLE, {1,0,0}, HGX_SCALE_A1},
+    {"transf_function_enabledC_false", PK_BOOL, {0,0,0}, HGX_C_ON},
+    {"transf_start_iterations_C", PK_INT, {0,0,0}, HGX_START_C},
+    {"transf_stop_iterations_C1", PK_INT, {1,0,0}, HGX_STOP_C1},
+    {"transf_offset_2", PK_DOUBLE, {2,0,0}, HGX_OFFSET2},
+    {"transf_offsetA_2", PK_DOUBLE, {2,0,0}, HGX_OFFSETA2},
+    {"transf_start_iterations_S", PK_INT, {0,0,0}, HGX_START_S},
+    {"transf_stop_iterations_S", PK_INT, {250,0,0}, HGX_STOP_S},
+    {"transf_scale_2", PK_DOUBLE, {2,0,0}, HGX_SCALE2},
+    {"transf_function_enabledK_false", PK_BOOL, {0,0,0}, HGX_K_ON},
+    {"transf_start_iterations_K", PK_INT, {0,0,0}, HGX_START_K},
+    {"transf_stop_iterations_K", PK_INT, {250,0,0}, HGX_STOP_K},
+    {"transf_scale_vary_0", PK_DOUBLE, {0,0,0}, HGX_SCALE_VARY},
+    {"transf_scaleC_1", PK_DOUBLE, {1,0,0}, HGX_SCALE_C1},
+    {"transf_offset_001", PK_VEC3, {0,0,1}, HGX_OFFSET001},
+    {"transf_function_enabledR_false", PK_BOOL, {0,0,0}, HGX_R_ON},
+    {"transf_start_iterations_R", PK_INT, {0,0,0}, HGX_START_R},
+    {"transf_stop_iterations_R", PK_INT, {250,0,0}, HGX_STOP_R},
+    {"transf_rotation", PK_ROT, {0,0,0}, HGX_ROT},
+    {"transf_start_iterations", PK_INT, {0,0,0}, HGX_START},
+    {"transf_stop_iterations", PK_INT, {250,0,0}, HGX_STOP},
+    {"transf_scale_1", PK_DOUBLE, {1,0,0}, HGX_SCALE1},
+    {"transf_scaleF_1", PK_DOUBLE, {1,0,0}, HGX_SCALE_F1},
+    {"transf_function_enabledJ_false", PK_BOOL, {0,0,0}, HGX_J_ON},
+    {"transf_offset_0005", PK_DOUBLE, {0.005,0,0}, HGX_OFFSET0005},
+};
+static_assert(keys_contiguous(kDIFSHextgrid2Keys, HGX_KEYED_END), "DIFS hextgrid2 keys and layout disagree");
+
 struct KeyTable {
   const FormulaKey *keys;
   int n;
@@ -862,6 +937,8 @@ inline KeyTable formula_keys(int formula) {
       return {kGeneralizedFoldBoxKeys, int(sizeof(kGeneralizedFoldBoxKeys) / sizeof(kGeneralizedFoldBoxKeys[0]))};
     case MBR_FORMULA_MANDELBULB_PUPUKU:
       return {kMandelbulbPupukuKeys, int(sizeof(kMandelbulbPupukuKeys) / sizeof(kMandelbulbPupukuKeys[0]))};
+    case MBR_FORMULA_DIFS_HEXTGRID2:
+      return {kDIFSHextgrid2Keys, int(sizeof(kDIFSHextgrid2Keys) / sizeof(kDIFSHextgrid2Keys[0]))};
     default: return {nullptr, 0};
   }
 }
@@ -969,6 +1046,10 @@ inline int pack_keyed(const mbr_fractal &f, double *x) {
       if (!std::isfinite(q.value[c])) return j;
     if (t.keys[i].kind == PK_INT && !(q.value[0] > -2147483648.0 && q.value[0] < 2147483648.0)) return j;
     put_keyed(t.keys[i], q.value, x);
+  }
+  if (f.formula == MBR_FORMULA_DIFS_HEXTGRID2) {  // its constants, computed on the host as the reference computes them
+    x[HGX_COS6] = std::cos(3.14159265358979323846 / 6.0);
+    x[HGX_SIN6] = std::sin(3.14159265358979323846 / 6.0);
   }
   if (f.formula == MBR_FORMULA_GENERALIZED_FOLD_BOX) {  // the derived part of its block
     x[GFX_MAIN_ON] = f.mandelbox_main_rotation_enabled ? 1.0 : 0.0;

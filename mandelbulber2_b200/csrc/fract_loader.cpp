@@ -1020,7 +1020,7 @@ extern "C" mbr_status mbr_fract_parse(const char *text, mbr_scene *scene, mbr_ca
                               "5 quaternion, 7 Menger sponge, 8 Mandelbox, 10 kaleidoscopic IFS, 11 xenodreambuie, "
                               "16 box fold bulb pow 2, 19 aexion, 37 generalized fold box, 61 Menger mod 1, 103 pseudo-Kleinian, "
                               "101 pseudo-Kleinian std DE, 119 Abox mod 11, 125 box fold bulb pow 2 V2, 217 pseudo-Kleinian mod 4, "
-                              "266 Mandelbulb Pupuku are)");
+                              "266 Mandelbulb Pupuku, 608 DIFS hextgrid2 are)");
     if (f == MBR_FORMULA_KALEIDOSCOPIC_IFS && n_ifs > 1)
       R.unsupported.push_back("formula_" + std::to_string(i + 1) + " 10 (kaleidoscopic IFS in more than one slot)");
     if (!R.slot_enable[i] && !boolean) R.unsupported.push_back("fractal_enable_" + std::to_string(i + 1) + " false");

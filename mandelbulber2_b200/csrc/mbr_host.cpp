@@ -59,6 +59,7 @@ bool formula_meta(int formula, FormulaMeta *m) {
     case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *m = {5, 1, 100.0, 6}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
     case MBR_FORMULA_GENERALIZED_FOLD_BOX: *m = {1, 0, 100.0, 1}; return true;  // fractal_generalized_fold_box.cpp:17-29
     case MBR_FORMULA_MANDELBULB_PUPUKU: *m = {2, 0, 10.0, 2}; return true;  // fractal_mandelbulb_pupuku.cpp:16-27
+    case MBR_FORMULA_DIFS_HEXTGRID2: *m = {5, 1, 100.0, 6}; return true;  // fractal_difs_hextgrid2.cpp:18-29
     default: return false;
   }
 }
@@ -520,7 +521,7 @@ mbr_status build_scene(mbr_ctx *ctx, const mbr_scene &sc, DevScene *out) {
     FormulaMeta m;
     if (!formula_meta(f.formula, &m))
       return set_err(ctx, MBR_EUNSUPPORTED,
-                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 16, 19, 37, 61, 101, 103, 119, 125, 217, 266)", i, f.formula);
+                     "slot %d: formula %d is not supported (2, 3, 4, 5, 7, 8, 10, 11, 16, 19, 37, 61, 101, 103, 119, 125, 217, 266, 608)", i, f.formula);
     any = true;
     if (f.formula_iterations < 1) return set_err(ctx, MBR_EINVAL, "slot %d: formula_iterations < 1", i);
     if (f.formula_start_iteration < 0 || f.formula_stop_iteration < 0)

@@ -75,6 +75,7 @@ static bool formula_info(int formula, FormulaInfo *fi) {
     case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: *fi = {5, 1, 100.0, 6, 0}; return true;  // fractal_pseudo_kleinian_std_de.cpp:16-27
     case MBR_FORMULA_GENERALIZED_FOLD_BOX: *fi = {1, 0, 100.0, 1, 0}; return true;  // fractal_generalized_fold_box.cpp:17-29
     case MBR_FORMULA_MANDELBULB_PUPUKU: *fi = {2, 0, 10.0, 2, 0}; return true;  // fractal_mandelbulb_pupuku.cpp:16-27
+    case MBR_FORMULA_DIFS_HEXTGRID2: *fi = {5, 1, 100.0, 6, 0}; return true;  // fractal_difs_hextgrid2.cpp:18-29
     default: return false;
   }
 }
@@ -1223,6 +1224,64 @@ inline void formula_mandelbulb_pupuku(V4<S> &z, const SlotT<S> &f, S r, S &DE, S
   }
 }
 
+// cFractalDIFSHextgrid2::FormulaCode (fractal_difs_hextgrid2.cpp:30-138)
+// without the aux.color terms; scaleA and dist are aux.actualScaleA, aux.dist
+template <class S>
+inline void formula_difs_hextgrid2(V4<S> &z, const SlotT<S> &f, S &DE, S &scaleA, S &dist, int i) {
+  using namespace mbr;
+  const double *x = f.x;
+  if (x[HGX_SPH_INV] != 0.0 && i >= int(x[HGX_START_X]) && i < int(x[HGX_STOP_1])) {
+    z.x = z.x + x[HGX_OFFSET000];
+    z.y = z.y + x[HGX_OFFSET000 + 1];
+    z.z = z.z + x[HGX_OFFSET000 + 2];
+    z.w = z.w + 0.0;
+    const S rr = z.x * z.x + z.y * z.y + z.z * z.z + z.w * z.w;
+    z = z * S(x[HGX_SCALE_G1] / rr);
+    DE = DE * (x[HGX_SCALE_G1] / rr);
+    z.x = z.x + (x[HGX_ADD000] - x[HGX_OFFSET000]);
+    z.y = z.y + (x[HGX_ADD000 + 1] - x[HGX_OFFSET000 + 1]);
+    z.z = z.z + (x[HGX_ADD000 + 2] - x[HGX_OFFSET000 + 2]);
+    z.w = z.w + (0.0 - 0.0);
+    z = z * x[HGX_SCALE_A1];
+    DE = DE * x[HGX_SCALE_A1];
+  }
+  if (x[HGX_C_ON] != 0.0 && i >= int(x[HGX_START_C]) && i < int(x[HGX_STOP_C1])) {
+    double Tp = x[HGX_OFFSET2];
+    z.x = S(fmod(val(fabs(z.x) + Tp), 2.0 * Tp)) - Tp;
+    Tp = x[HGX_OFFSETA2];
+    z.y = S(fmod(val(fabs(z.y) + Tp), 2.0 * Tp)) - Tp;
+  }
+  if (i >= int(x[HGX_START_S]) && i < int(x[HGX_STOP_S])) {
+    const S useScale = scaleA + x[HGX_SCALE2];
+    z = z * useScale;
+    DE = DE * fabs(useScale);
+    if (x[HGX_K_ON] != 0.0 && i >= int(x[HGX_START_K]) && i < int(x[HGX_STOP_K])) {
+      const S vary = x[HGX_SCALE_VARY] * (fabs(scaleA) - x[HGX_SCALE_C1]);
+      scaleA = scaleA - vary;
+    }
+  }
+  z.x = z.x + x[HGX_OFFSET001];
+  z.y = z.y + x[HGX_OFFSET001 + 1];
+  z.z = z.z + x[HGX_OFFSET001 + 2];
+  z.w = z.w + 0.0;
+  if (x[HGX_R_ON] != 0.0 && i >= int(x[HGX_START_R]) && i < int(x[HGX_STOP_R]))
+    z = mb_turn(x + HGX_ROT + 1, x[HGX_ROT] != 0.0, false, z);
+  if (i >= int(x[HGX_START]) && i < int(x[HGX_STOP])) {
+    const double size = x[HGX_SCALE1], cosPi6 = x[HGX_COS6];
+    V4<S> zc = z;
+    zc.z = zc.z / x[HGX_SCALE_F1];
+    const S yFloor = fabs(zc.y - size * S(floor(val(zc.y / size + 0.5))));
+    const S xFloor = fabs(zc.x - size * 1.5 / cosPi6 * S(floor(val(zc.x / size / 1.5 * cosPi6 + 0.5))));
+    const S gridMax = std::max(yFloor, S(xFloor * cosPi6 + yFloor * x[HGX_SIN6]));
+    const S gridMin = std::min(S(gridMax - size * 0.5), yFloor);
+    S hexD;
+    if (x[HGX_J_ON] == 0.0) hexD = sqrt(gridMin * gridMin + zc.z * zc.z);
+    else hexD = std::max(S(fabs(gridMin)), S(fabs(zc.z)));
+    hexD = hexD - x[HGX_OFFSET0005];
+    dist = std::min(dist, S(hexD / (DE + 1.0)));
+  }
+}
+
 // Benesi's tetrahedral frame turns (abstract_fractal.h:30-32 constants)
 template <class S>
 inline V4<S> benesi_in(const V4<S> &z) {
@@ -1730,6 +1789,7 @@ FractalOut<S> compute(const Seq &seq, const SlotT<S> *slots, S px, S py, S pz, i
         case MBR_FORMULA_PSEUDO_KLEINIAN_STD_DE: formula_pseudo_kleinian_std_de(z, f, DE, auxDist, i); break;
         case MBR_FORMULA_GENERALIZED_FOLD_BOX: formula_generalized_fold_box(z, f, DE); break;
         case MBR_FORMULA_MANDELBULB_PUPUKU: formula_mandelbulb_pupuku(z, f, r, DE, auxDist, i); break;
+        case MBR_FORMULA_DIFS_HEXTGRID2: formula_difs_hextgrid2(z, f, DE, scaleA, auxDist, i); break;
         default: {  // :228-238
           out.distance = 10.0;
           out.iters = 1;

@@ -252,6 +252,12 @@ def _keyed_formula_cases():
     s.fractal[0].bulb_power = 4.0
     s.delta_de_function = abi.DE_CUSTOM
     t["pupuku_custom_de"] = s
+    t["hextgrid2_default"] = _keyed(abi.FORMULA_DIFS_HEXTGRID2, 20)
+    t["hextgrid2_options"] = _keyed(abi.FORMULA_DIFS_HEXTGRID2, 20, transf_function_enabledC_false=1,
+                                    transf_stop_iterations_C1=3, transf_offset_2=1.5, transf_function_enabledK_false=1,
+                                    transf_scale_vary_0=0.1, transf_function_enabledR_false=1,
+                                    transf_rotation=[0.0, 10.0, 30.0], transf_scaleF_1=1.2,
+                                    transf_function_enabledJ_false=1, transf_scale_1=0.8)
     t["bfbp2v2_vary_m"] = _keyed(abi.FORMULA_BOX_FOLD_BULB_POW2_V2, 20, transf_scale_vary_0=0.2,
                                  transf_function_enabledM_false=1, transf_stop_iterations_A=8)
     return t

@@ -201,14 +201,15 @@ KEYED_CASES = ["pk_default", "pk_params", "pk_sphere_inversion", "pk_prism", "pk
                "menger_mod1_box_offset_blend", "hybrid_menger_mod1_bfbp2", "bfbp2v2_default", "bfbp2v2_vary",
                "bfbp2v2_vary_m", "abox_mod11_default", "abox_mod11_folds", "abox_mod11_curve_c",
                "hybrid_abox_mod11_bulb", "pkm4_default", "pkm4_sphere_box", "pkm4_fold_n", "pksd_default",
-               "pksd_benesi", "pksd_folds", "hybrid_pksd_box"] + [f"gfb_type{k}" for k in range(8)] + ["gfb_rotated", "pupuku_default", "pupuku_options", "pupuku_custom_de"]
+               "pksd_benesi", "pksd_folds", "hybrid_pksd_box"] + [f"gfb_type{k}" for k in range(8)] + ["gfb_rotated", "pupuku_default", "pupuku_options", "pupuku_custom_de",
+                                                             "hextgrid2_default", "hextgrid2_options"]
 
 
 # formulas whose orbits at random points are chaotic in every engine that
 # rounds differently from the strict one (folds that branch on the sign or
 # the order of coordinates, no escape): their FMA and FP32 distances there
 # are reported, and their frames are held to the frame bars below
-CHAOTIC = ("pksd_", "gfb_")
+CHAOTIC = ("pksd_", "gfb_", "hextgrid2_")
 
 
 @pytest.mark.parametrize("case", KEYED_CASES)
